@@ -1,0 +1,149 @@
+/*
+ * sympack_b200.h — C ABI of the B200-native supernodal Cholesky factor / solve.
+ *
+ * The reference (symPACK v2.0) exposes its solver only as the C++ template
+ * class symPACKMatrix2D<Ptr, Idx, T> (include/sympack/symPACKMatrix2D.hpp:2618-2627,
+ * base interface include/sympack/symPACKMatrixBase.hpp:51-63).  Its only extern "C"
+ * functions are symPACK_Init / symPACK_Finalize / symPACK_Rank / symPACK_cuda_setup
+ * (include/sympack.hpp:25-36).  Each entry point below replaces one method of that
+ * class one-for-one, with plain pointers and sizes so that a ctypes / cgo / JNI
+ * binding needs no C++ types:
+ *
+ *   spb_create            symPACKMatrix2D::Init(symPACKOptions&)               2D.hpp:2649
+ *   spb_symbolic          symPACKMatrix2D::SymbolicFactorization(DistSparseMatrix&) 2D.hpp:2699
+ *   spb_distribute        symPACKMatrix2D::DistributeMatrix(DistSparseMatrix&)  2D.hpp:6337
+ *   spb_factorize         symPACKMatrix2D::Factorize()                          2D.hpp:6579
+ *   spb_solve             symPACKMatrix2D::Solve(T* RHS, int nrhs, int rhs_size) 2D.hpp:6643
+ *   spb_get_solution      symPACKMatrix2D::GetSolution(T* B, int nrhs)          2D.hpp:6713
+ *   spb_get_ordering      symPACKMatrixBase::GetOrdering()                      symPACKMatrixBase.hpp:96-103
+ *   spb_get_supernodes    symPACKMatrixBase::GetSupernodalPartition() / GetSupMembership()
+ *   spb_get_etree         symPACKMatrixBase::GetETree()
+ *
+ * Conventions (same as the reference): the input matrix is the lower triangle,
+ * diagonal included, in 1-based compressed-column form with rows sorted per
+ * column (DistSparseMatrix<T>, DistSparseMatrix.hpp:49-63); right-hand sides and
+ * solutions are column-major n x nrhs in the ORIGINAL ordering.  Solve keeps the
+ * solution inside the handle until GetSolution copies it out.
+ *
+ * Errors are status codes instead of exceptions / spins: a non-SPD pivot (where
+ * the reference throws "Matrix is not HPD." and then spins in gdb_lock,
+ * 2D.hpp:1097-1100) returns SPB_ERR_NOT_SPD with the failing supernode and
+ * column available from spb_get_status.
+ *
+ * A handle owns all of its device memory and one CUDA stream; it is not
+ * thread-safe.  All host pointers are read or written synchronously.
+ */
+#ifndef SYMPACK_B200_H
+#define SYMPACK_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SPB_OK 0
+#define SPB_ERR_INVALID (-1)   /* bad argument or malformed matrix */
+#define SPB_ERR_NOT_SPD (-2)   /* non-positive pivot during Factorize */
+#define SPB_ERR_OOM (-3)       /* device allocation failed */
+#define SPB_ERR_CUDA (-4)      /* any other CUDA runtime failure */
+#define SPB_ERR_STATE (-5)     /* call out of order (e.g. Solve before Factorize) */
+#define SPB_ERR_STRUCTURE (-6) /* inconsistent symbolic structure detected on the device */
+#define SPB_ERR_TIMEOUT (-7)   /* a bounded device wait expired */
+#define SPB_ERR_NOT_CONVERGED (-8) /* iterative refinement did not reach its tolerance */
+
+#define SPB_ORDERING_MMD 0
+#define SPB_ORDERING_NATURAL 1
+#define SPB_ORDERING_USER 2
+
+#define SPB_PRECISION_FP64 0      /* plain FP64 factor and solve (the drop-in path) */
+#define SPB_PRECISION_FP32_IR 1   /* FP32 factor + FP64 iterative refinement */
+
+typedef struct spb_handle spb_handle;
+
+/* Mirrors the symPACKOptions fields this path uses (Types.hpp:106-201). */
+typedef struct spb_options {
+  int ordering;            /* SPB_ORDERING_* ("-ordering", default MMD) */
+  int nrelax0, nrelax1, nrelax2; /* supernode relaxation sizes (8, 32, 64) */
+  int max_snode;           /* "-b": maximum supernode width, 0 = unlimited (driver default) */
+  double zrelax0, zrelax1, zrelax2; /* relaxation zero fractions (0.8, 0.1, 0.05) */
+  const int32_t* user_perm; /* SPB_ORDERING_USER: 1-based new->old permutation */
+  int device;              /* CUDA device ordinal */
+  int precision;           /* SPB_PRECISION_* */
+  double ir_tolerance;     /* backward-error target of refinement (1e-12) */
+  int ir_max_iter;         /* refinement iteration cap */
+  int verbose;
+} spb_options;
+
+typedef struct spb_info {
+  int32_t n;
+  int32_t nsuper;
+  int32_t nlevels;         /* height of the supernodal elimination tree */
+  int32_t max_width;
+  int64_t nnz_a;           /* entries of the input lower triangle */
+  int64_t nnz_l;           /* sum of column counts (reference "NNZ in L factor") */
+  int64_t lindx_size;      /* total row-structure entries */
+  int64_t arena_bytes;     /* device bytes of the factor panels */
+  int64_t device_bytes;    /* all device bytes held by the handle */
+  double flops_stat;       /* sum of column counts squared (reference "Flops" statistic) */
+  double flops_exec;       /* flops the kernel sequence executes */
+  int32_t ncells;          /* reference 2D cells (K, I) */
+  int32_t nblocks;         /* reference contiguous-row blocks */
+  int32_t ir_iterations;   /* refinement steps of the last solve */
+  int32_t pad;
+  double backward_error;   /* componentwise-free backward error of the last solve, if computed */
+} spb_info;
+
+void spb_default_options(spb_options* opt);
+int spb_create(const spb_options* opt, spb_handle** out);
+void spb_destroy(spb_handle* h);
+const char* spb_last_error(const spb_handle* h);
+
+/* SymbolicFactorization: structure only (values not needed). */
+int spb_symbolic(spb_handle* h, int32_t n, const int64_t* colptr, const int32_t* rowind);
+/* DistributeMatrix: values in the same order as rowind (host or device pointer). */
+int spb_distribute(spb_handle* h, const double* nzval);
+int spb_distribute_device(spb_handle* h, const double* d_nzval);
+/* Factorize. */
+int spb_factorize(spb_handle* h);
+/* Solve: host RHS (column-major, leading dimension ldb >= n); the solution stays in the handle. */
+int spb_solve(spb_handle* h, const double* rhs, int32_t nrhs, int64_t ldb);
+/* GetSolution: copy the last solution to host B (column-major, leading dimension ldb). */
+int spb_get_solution(spb_handle* h, double* B, int32_t nrhs, int64_t ldb);
+/* Solve with device-resident right-hand sides and solution (both n x nrhs, leading dimension ld). */
+int spb_solve_device(spb_handle* h, const double* d_rhs, double* d_x, int32_t nrhs, int64_t ld);
+
+/* Introspection for parity checks (arrays sized from spb_get_info). */
+int spb_get_info(spb_handle* h, spb_info* info);
+int spb_get_ordering(spb_handle* h, int32_t* perm, int32_t* invp);           /* n each, 1-based */
+int spb_get_mmd_invp(spb_handle* h, int32_t* invp);                          /* n, before postordering */
+int spb_get_etree(spb_handle* h, int32_t* parent);                           /* n, postordered, 0 = root */
+int spb_get_colcounts(spb_handle* h, int32_t* cc_fund, int32_t* cc_relaxed); /* n each */
+int spb_get_supernodes(spb_handle* h, int32_t* xsuper, int32_t* supmember);  /* nsuper+1, n */
+int spb_get_structure(spb_handle* h, int64_t* xlindx, int32_t* lindx);       /* nsuper+1, lindx_size */
+/* Cells (K, I) in the reference's construction order and their row blocks. */
+int spb_get_cells(spb_handle* h, int32_t* cell_I, int32_t* cell_K, int32_t* cell_nrows,
+                  int32_t* cell_first_block, int32_t* cell_nblocks, int32_t* block_first_row,
+                  int32_t* block_nrows);
+/* Factor: per supernode, the h x w panel column-major with leading dimension h,
+ * entries above the diagonal of the diagonal block set to zero.  Size = sum h*w. */
+int spb_get_factor(spb_handle* h, double* out);
+/* Status of the last factorization: code, supernode (0-based), column (0-based, permuted). */
+int spb_get_status(spb_handle* h, int32_t* code, int32_t* supernode, int32_t* column);
+
+/* Rutherford-Boeing input boundary, replacing ReadMatrix / ReadHB_PARA
+ * (include/sympack/utility.hpp:1274-1481, 1695-1727) for one rank.  spb_rb_info
+ * reports the size; spb_rb_read fills colptr (n+1), rowind (nnz) and, if not
+ * NULL, nzval (nnz), each column's rows sorted.  spb_rb_write writes a real
+ * symmetric ("rsa") lower-triangle file in the (8I10) / (4E20.12) layout that
+ * reader expects. */
+int spb_rb_info(const char* path, int32_t* n, int64_t* nnz);
+int spb_rb_read(const char* path, int64_t* colptr, int32_t* rowind, double* nzval);
+int spb_rb_write(const char* path, const char* title, int32_t n, const int64_t* colptr, const int32_t* rowind,
+                 const double* nzval);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SYMPACK_B200_H */

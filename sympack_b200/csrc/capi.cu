@@ -1,0 +1,541 @@
+// extern "C" boundary of the supernodal Cholesky path (declared in
+// include/sympack_b200.h).  A handle plays the role of one symPACKMatrix2D
+// object at one rank: it owns the symbolic analysis (host), the device plan,
+// the factor arena in HBM, and a CUDA graph replaying the factorization.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <exception>
+#include <new>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/sympack_b200.h"
+#include "kernels.cuh"
+#include "plan.hpp"
+#include "symbolic.hpp"
+
+using spb::dev::Status;
+
+struct spb_handle {
+  spb_options opt{};
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  bool have_symbolic = false, have_values = false, factored = false, have_solution = false;
+  spb::Symbolic sym;
+  spb::Plan plan;
+  spb::Cells cells;
+  bool cells_built = false;
+  int64_t nnz_a = 0;
+  std::vector<int64_t> colptr;
+  std::vector<int32_t> rowind;
+  std::vector<int32_t> level_off;  // level l covers dlevel_sn[level_off[l] .. level_off[l+1])
+  // device buffers
+  double* dL = nullptr;
+  spb::SnMeta* dmeta = nullptr;
+  int32_t* drows = nullptr;
+  int32_t* dsupm = nullptr;
+  int64_t* damap = nullptr;
+  double* dA = nullptr;
+  int32_t* dsmall = nullptr;
+  spb::PanelItem* dpanel = nullptr;
+  spb::TileItem* dtiles = nullptr;
+  int32_t* dinvp0 = nullptr;
+  int32_t* dlevel_sn = nullptr;
+  Status* dstatus = nullptr;
+  double* dX = nullptr;
+  double* dB = nullptr;
+  int64_t x_cap = 0;  // doubles available in dX and dB
+  int x_nrhs = 0;
+  int64_t device_bytes = 0;
+  cudaGraphExec_t fgraph = nullptr;
+  std::vector<void*> allocs;
+};
+
+namespace {
+
+int fail(spb_handle* h, int code, const std::string& msg) {
+  if (h) h->err = msg;
+  return code;
+}
+
+int cuda_fail(spb_handle* h, cudaError_t e, const char* what) {
+  std::string msg = std::string(what) + ": " + cudaGetErrorString(e);
+  cudaGetLastError();
+  return fail(h, e == cudaErrorMemoryAllocation ? SPB_ERR_OOM : SPB_ERR_CUDA, msg);
+}
+
+#define SPB_CK(h, call)                                   \
+  do {                                                    \
+    cudaError_t _e = (call);                              \
+    if (_e != cudaSuccess) return cuda_fail(h, _e, #call); \
+  } while (0)
+
+template <class T>
+cudaError_t dalloc(spb_handle* h, T** p, size_t count) {
+  *p = nullptr;
+  if (count == 0) count = 1;
+  cudaError_t e = cudaMalloc((void**)p, count * sizeof(T));
+  if (e == cudaSuccess) {
+    h->allocs.push_back((void*)*p);
+    h->device_bytes += (int64_t)(count * sizeof(T));
+  }
+  return e;
+}
+
+void release_device(spb_handle* h) {
+  if (h->fgraph) {
+    cudaGraphExecDestroy(h->fgraph);
+    h->fgraph = nullptr;
+  }
+  for (void* p : h->allocs) cudaFree(p);
+  h->allocs.clear();
+  h->device_bytes = 0;
+  h->dL = nullptr;
+  h->dX = h->dB = nullptr;
+  h->x_cap = 0;
+}
+
+spb::dev::FactorArgs factor_args(spb_handle* h) {
+  spb::dev::FactorArgs a;
+  a.L = h->dL;
+  a.meta = h->dmeta;
+  a.rows = h->drows;
+  a.supmember = h->dsupm;
+  a.status = h->dstatus;
+  return a;
+}
+
+// Issue the factorization steps on the handle's stream (captured into a graph).
+void enqueue_factor(spb_handle* h) {
+  const spb::Plan& P = h->plan;
+  spb::dev::FactorArgs a = factor_args(h);
+  for (const spb::Step& st : P.steps) {
+    switch (st.kind) {
+      case spb::StepKind::FactorSmall:
+        spb::dev::launch_factor_small(h->stream, a, h->dsmall + st.begin, st.count, st.arg);
+        break;
+      case spb::StepKind::PotrfDiag:
+        spb::dev::launch_potrf_diag(h->stream, a, h->dpanel + st.begin, st.count);
+        break;
+      case spb::StepKind::TrsmRows:
+        spb::dev::launch_trsm_rows(h->stream, a, h->dpanel + st.begin, st.count);
+        break;
+      case spb::StepKind::Gemm:
+        spb::dev::launch_gemm(h->stream, a, h->dtiles + st.begin, st.count, st.tile);
+        break;
+    }
+  }
+}
+
+int check_handle(spb_handle* h) { return h ? SPB_OK : SPB_ERR_INVALID; }
+
+int ensure_rhs_capacity(spb_handle* h, int nrhs) {
+  int64_t need = (int64_t)h->sym.n * nrhs;
+  if (need <= h->x_cap) return SPB_OK;
+  for (double** p : {&h->dX, &h->dB}) {
+    if (*p) {
+      auto it = std::find(h->allocs.begin(), h->allocs.end(), (void*)*p);
+      if (it != h->allocs.end()) h->allocs.erase(it);
+      cudaFree(*p);
+      h->device_bytes -= h->x_cap * (int64_t)sizeof(double);
+      *p = nullptr;
+    }
+  }
+  h->x_cap = 0;
+  SPB_CK(h, dalloc(h, &h->dX, need));
+  SPB_CK(h, dalloc(h, &h->dB, need));
+  h->x_cap = need;
+  return SPB_OK;
+}
+
+// Forward and backward sweeps over the levels on permuted X (n x nrhs, ld n).
+void enqueue_solve(spb_handle* h, int nrhs) {
+  const spb::Plan& P = h->plan;
+  for (int c0 = 0; c0 < nrhs; c0 += 64) {
+    spb::dev::SolveArgs a;
+    a.L = h->dL;
+    a.meta = h->dmeta;
+    a.rows = h->drows;
+    a.X = h->dX + (int64_t)c0 * h->sym.n;
+    a.ldx = h->sym.n;
+    a.nrhs = std::min(64, nrhs - c0);
+    for (int l = 0; l < P.nlevels; ++l)
+      spb::dev::launch_solve_forward(h->stream, a, h->dlevel_sn + h->level_off[l], h->level_off[l + 1] - h->level_off[l]);
+    for (int l = P.nlevels - 1; l >= 0; --l)
+      spb::dev::launch_solve_backward(h->stream, a, h->dlevel_sn + h->level_off[l], h->level_off[l + 1] - h->level_off[l]);
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+void spb_default_options(spb_options* o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof(*o));
+  o->ordering = SPB_ORDERING_MMD;
+  o->nrelax0 = 8;
+  o->nrelax1 = 32;
+  o->nrelax2 = 64;
+  o->max_snode = 0;
+  o->zrelax0 = 0.8;
+  o->zrelax1 = 0.1;
+  o->zrelax2 = 0.05;
+  o->user_perm = nullptr;
+  o->device = 0;
+  o->precision = SPB_PRECISION_FP64;
+  o->ir_tolerance = 1e-12;
+  o->ir_max_iter = 30;
+  o->verbose = 0;
+}
+
+int spb_create(const spb_options* opt, spb_handle** out) {
+  if (!out) return SPB_ERR_INVALID;
+  *out = nullptr;
+  spb_handle* h = new (std::nothrow) spb_handle();
+  if (!h) return SPB_ERR_OOM;
+  if (opt) h->opt = *opt;
+  else spb_default_options(&h->opt);
+  if (h->opt.ordering < 0 || h->opt.ordering > 2 || h->opt.precision < 0 || h->opt.precision > 1) {
+    delete h;
+    return SPB_ERR_INVALID;
+  }
+  h->device = h->opt.device;
+  cudaError_t e = cudaSetDevice(h->device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    delete h;
+    return e == cudaErrorMemoryAllocation ? SPB_ERR_OOM : SPB_ERR_CUDA;
+  }
+  spb::dev::init_kernel_attributes();
+  *out = h;
+  return SPB_OK;
+}
+
+void spb_destroy(spb_handle* h) {
+  if (!h) return;
+  cudaSetDevice(h->device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  release_device(h);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+}
+
+const char* spb_last_error(const spb_handle* h) { return h ? h->err.c_str() : "null handle"; }
+
+int spb_symbolic(spb_handle* h, int32_t n, const int64_t* colptr, const int32_t* rowind) {
+  if (check_handle(h)) return SPB_ERR_INVALID;
+  if (n <= 0 || !colptr || !rowind) return fail(h, SPB_ERR_INVALID, "symbolic: empty matrix or null pointer");
+  SPB_CK(h, cudaSetDevice(h->device));
+  release_device(h);
+  h->have_symbolic = h->have_values = h->factored = h->have_solution = false;
+  h->cells_built = false;
+  try {
+    h->nnz_a = colptr[n] - 1;
+    h->colptr.assign(colptr, colptr + n + 1);
+    h->rowind.assign(rowind, rowind + h->nnz_a);
+    spb::RelaxParams rp;
+    rp.nrelax0 = h->opt.nrelax0;
+    rp.nrelax1 = h->opt.nrelax1;
+    rp.nrelax2 = h->opt.nrelax2;
+    rp.maxSize = h->opt.max_snode;
+    rp.zrelax0 = h->opt.zrelax0;
+    rp.zrelax1 = h->opt.zrelax1;
+    rp.zrelax2 = h->opt.zrelax2;
+    if (rp.maxSize > 0) {  // RelaxationParameters::SetMaxSize (Types.hpp:63-70)
+      rp.nrelax0 = std::min(rp.nrelax0, rp.maxSize);
+      rp.nrelax1 = std::min(rp.nrelax1, rp.maxSize);
+      rp.nrelax2 = std::min(rp.nrelax2, rp.maxSize);
+    }
+    h->sym = spb::symbolic_factorization(n, colptr, rowind, (spb::OrderingKind)h->opt.ordering, rp, h->opt.user_perm);
+    h->plan = spb::build_plan(h->sym);
+  } catch (const std::invalid_argument& e) {
+    return fail(h, SPB_ERR_INVALID, e.what());
+  } catch (const std::bad_alloc&) {
+    return fail(h, SPB_ERR_OOM, "symbolic: host allocation failed");
+  } catch (const std::exception& e) {
+    return fail(h, SPB_ERR_STRUCTURE, e.what());
+  }
+  std::vector<int64_t> amap;
+  try {
+    amap = spb::build_assembly_map(h->sym, h->plan, colptr, rowind);
+  } catch (const std::exception& e) {
+    return fail(h, SPB_ERR_STRUCTURE, e.what());
+  }
+  const spb::Plan& P = h->plan;
+  std::vector<int32_t> lsn, invp0(n);
+  h->level_off.assign(P.nlevels + 1, 0);
+  for (int l = 0; l < P.nlevels; ++l) {
+    h->level_off[l] = (int32_t)lsn.size();
+    lsn.insert(lsn.end(), P.level_sn[l].begin(), P.level_sn[l].end());
+  }
+  h->level_off[P.nlevels] = (int32_t)lsn.size();
+  for (int i = 0; i < n; ++i) invp0[i] = h->sym.invp[i] - 1;
+
+  SPB_CK(h, dalloc(h, &h->dL, P.arena_elems));
+  SPB_CK(h, dalloc(h, &h->dmeta, P.meta.size()));
+  SPB_CK(h, dalloc(h, &h->drows, P.rows.size()));
+  SPB_CK(h, dalloc(h, &h->dsupm, P.supmember0.size()));
+  SPB_CK(h, dalloc(h, &h->damap, amap.size()));
+  SPB_CK(h, dalloc(h, &h->dA, (size_t)h->nnz_a));
+  SPB_CK(h, dalloc(h, &h->dsmall, P.small_items.size()));
+  SPB_CK(h, dalloc(h, &h->dpanel, P.panel_items.size()));
+  SPB_CK(h, dalloc(h, &h->dtiles, P.tile_items.size()));
+  SPB_CK(h, dalloc(h, &h->dinvp0, invp0.size()));
+  SPB_CK(h, dalloc(h, &h->dlevel_sn, lsn.size()));
+  SPB_CK(h, dalloc(h, &h->dstatus, 1));
+  auto up = [&](void* d, const void* s, size_t bytes) {
+    return bytes ? cudaMemcpyAsync(d, s, bytes, cudaMemcpyHostToDevice, h->stream) : cudaSuccess;
+  };
+  SPB_CK(h, up(h->dmeta, P.meta.data(), P.meta.size() * sizeof(spb::SnMeta)));
+  SPB_CK(h, up(h->drows, P.rows.data(), P.rows.size() * 4));
+  SPB_CK(h, up(h->dsupm, P.supmember0.data(), P.supmember0.size() * 4));
+  SPB_CK(h, up(h->damap, amap.data(), amap.size() * 8));
+  SPB_CK(h, up(h->dsmall, P.small_items.data(), P.small_items.size() * 4));
+  SPB_CK(h, up(h->dpanel, P.panel_items.data(), P.panel_items.size() * sizeof(spb::PanelItem)));
+  SPB_CK(h, up(h->dtiles, P.tile_items.data(), P.tile_items.size() * sizeof(spb::TileItem)));
+  SPB_CK(h, up(h->dinvp0, invp0.data(), invp0.size() * 4));
+  SPB_CK(h, up(h->dlevel_sn, lsn.data(), lsn.size() * 4));
+  SPB_CK(h, cudaMemsetAsync(h->dstatus, 0, sizeof(Status), h->stream));
+  SPB_CK(h, cudaStreamSynchronize(h->stream));
+  h->have_symbolic = true;
+  return SPB_OK;
+}
+
+static int distribute_common(spb_handle* h) {
+  const spb::Plan& P = h->plan;
+  SPB_CK(h, cudaMemsetAsync(h->dL, 0, P.arena_elems * sizeof(double), h->stream));
+  SPB_CK(h, cudaMemsetAsync(h->dstatus, 0, sizeof(Status), h->stream));
+  spb::dev::launch_assemble(h->stream, h->dL, h->damap, h->dA, h->nnz_a);
+  SPB_CK(h, cudaGetLastError());
+  SPB_CK(h, cudaStreamSynchronize(h->stream));
+  h->have_values = true;
+  h->factored = h->have_solution = false;
+  return SPB_OK;
+}
+
+int spb_distribute(spb_handle* h, const double* nzval) {
+  if (check_handle(h)) return SPB_ERR_INVALID;
+  if (!h->have_symbolic) return fail(h, SPB_ERR_STATE, "distribute: call spb_symbolic first");
+  if (!nzval) return fail(h, SPB_ERR_INVALID, "distribute: null values");
+  SPB_CK(h, cudaSetDevice(h->device));
+  SPB_CK(h, cudaMemcpyAsync(h->dA, nzval, h->nnz_a * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  return distribute_common(h);
+}
+
+int spb_distribute_device(spb_handle* h, const double* d_nzval) {
+  if (check_handle(h)) return SPB_ERR_INVALID;
+  if (!h->have_symbolic) return fail(h, SPB_ERR_STATE, "distribute: call spb_symbolic first");
+  if (!d_nzval) return fail(h, SPB_ERR_INVALID, "distribute: null values");
+  SPB_CK(h, cudaSetDevice(h->device));
+  SPB_CK(h, cudaMemcpyAsync(h->dA, d_nzval, h->nnz_a * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+  return distribute_common(h);
+}
+
+int spb_factorize(spb_handle* h) {
+  if (check_handle(h)) return SPB_ERR_INVALID;
+  if (!h->have_values) return fail(h, SPB_ERR_STATE, "factorize: call spb_distribute first");
+  if (h->factored) return fail(h, SPB_ERR_STATE, "factorize: values already factored; distribute again");
+  SPB_CK(h, cudaSetDevice(h->device));
+  if (!h->fgraph && !h->plan.steps.empty()) {
+    cudaGraph_t g;
+    SPB_CK(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    enqueue_factor(h);
+    cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+    if (e != cudaSuccess) return cuda_fail(h, e, "factorize: graph capture");
+    e = cudaGraphInstantiate(&h->fgraph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return cuda_fail(h, e, "factorize: graph instantiate");
+  }
+  if (h->fgraph) SPB_CK(h, cudaGraphLaunch(h->fgraph, h->stream));
+  Status st;
+  SPB_CK(h, cudaMemcpyAsync(&st, h->dstatus, sizeof(st), cudaMemcpyDeviceToHost, h->stream));
+  SPB_CK(h, cudaStreamSynchronize(h->stream));
+  h->factored = true;
+  if (st.code == 1) {
+    char msg[128];
+    snprintf(msg, sizeof msg, "Matrix is not HPD: non-positive pivot in supernode %d, column %d", st.supernode + 1,
+             st.column + 1);
+    return fail(h, SPB_ERR_NOT_SPD, msg);
+  }
+  if (st.code != 0) return fail(h, SPB_ERR_STRUCTURE, "factorize: update row missing from target structure");
+  return SPB_OK;
+}
+
+int spb_solve_device(spb_handle* h, const double* d_rhs, double* d_x, int32_t nrhs, int64_t ld) {
+  if (check_handle(h)) return SPB_ERR_INVALID;
+  if (!h->factored) return fail(h, SPB_ERR_STATE, "solve: call spb_factorize first");
+  const int n = h->sym.n;
+  if (nrhs <= 0 || ld < n || !d_rhs || !d_x) return fail(h, SPB_ERR_INVALID, "solve: bad right-hand side");
+  SPB_CK(h, cudaSetDevice(h->device));
+  int rc = ensure_rhs_capacity(h, nrhs);
+  if (rc) return rc;
+  spb::dev::launch_permute_in(h->stream, h->dX, n, d_rhs, ld, h->dinvp0, n, nrhs);
+  enqueue_solve(h, nrhs);
+  spb::dev::launch_permute_out(h->stream, d_x, ld, h->dX, n, h->dinvp0, n, nrhs);
+  SPB_CK(h, cudaGetLastError());
+  SPB_CK(h, cudaStreamSynchronize(h->stream));
+  return SPB_OK;
+}
+
+int spb_solve(spb_handle* h, const double* rhs, int32_t nrhs, int64_t ldb) {
+  if (check_handle(h)) return SPB_ERR_INVALID;
+  if (!h->factored) return fail(h, SPB_ERR_STATE, "solve: call spb_factorize first");
+  const int n = h->sym.n;
+  if (nrhs <= 0 || ldb < n || !rhs) return fail(h, SPB_ERR_INVALID, "solve: bad right-hand side");
+  SPB_CK(h, cudaSetDevice(h->device));
+  int rc = ensure_rhs_capacity(h, nrhs);
+  if (rc) return rc;
+  SPB_CK(h, cudaMemcpy2DAsync(h->dB, (size_t)n * 8, rhs, (size_t)ldb * 8, (size_t)n * 8, nrhs, cudaMemcpyHostToDevice,
+                              h->stream));
+  spb::dev::launch_permute_in(h->stream, h->dX, n, h->dB, n, h->dinvp0, n, nrhs);
+  enqueue_solve(h, nrhs);
+  SPB_CK(h, cudaGetLastError());
+  SPB_CK(h, cudaStreamSynchronize(h->stream));
+  h->have_solution = true;
+  h->x_nrhs = nrhs;
+  return SPB_OK;
+}
+
+int spb_get_solution(spb_handle* h, double* B, int32_t nrhs, int64_t ldb) {
+  if (check_handle(h)) return SPB_ERR_INVALID;
+  if (!h->have_solution) return fail(h, SPB_ERR_STATE, "get_solution: call spb_solve first");
+  const int n = h->sym.n;
+  if (!B || nrhs <= 0 || nrhs > h->x_nrhs || ldb < n) return fail(h, SPB_ERR_INVALID, "get_solution: bad output");
+  SPB_CK(h, cudaSetDevice(h->device));
+  spb::dev::launch_permute_out(h->stream, h->dB, n, h->dX, n, h->dinvp0, n, nrhs);
+  SPB_CK(h, cudaMemcpy2DAsync(B, (size_t)ldb * 8, h->dB, (size_t)n * 8, (size_t)n * 8, nrhs, cudaMemcpyDeviceToHost,
+                              h->stream));
+  SPB_CK(h, cudaStreamSynchronize(h->stream));
+  return SPB_OK;
+}
+
+int spb_get_info(spb_handle* h, spb_info* info) {
+  if (check_handle(h) || !info) return SPB_ERR_INVALID;
+  if (!h->have_symbolic) return fail(h, SPB_ERR_STATE, "info: no symbolic factorization");
+  std::memset(info, 0, sizeof(*info));
+  const spb::Plan& P = h->plan;
+  if (!h->cells_built) {
+    h->cells = spb::build_cells(h->sym);
+    h->cells_built = true;
+  }
+  info->n = h->sym.n;
+  info->nsuper = P.nsuper;
+  info->nlevels = P.nlevels;
+  int mw = 0;
+  for (const auto& m : P.meta) mw = std::max(mw, m.w);
+  info->max_width = mw;
+  info->nnz_a = h->nnz_a;
+  info->nnz_l = h->sym.nnzL_stat;
+  info->lindx_size = (int64_t)h->sym.lindx.size();
+  info->arena_bytes = P.arena_elems * 8;
+  info->device_bytes = h->device_bytes;
+  info->flops_stat = h->sym.flops_stat;
+  info->flops_exec = P.exec_flops;
+  info->ncells = (int32_t)h->cells.cells.size();
+  info->nblocks = (int32_t)h->cells.block_first_row.size();
+  return SPB_OK;
+}
+
+int spb_get_ordering(spb_handle* h, int32_t* perm, int32_t* invp) {
+  if (check_handle(h)) return SPB_ERR_INVALID;
+  if (!h->have_symbolic) return fail(h, SPB_ERR_STATE, "no symbolic factorization");
+  if (perm) std::copy(h->sym.perm.begin(), h->sym.perm.end(), perm);
+  if (invp) std::copy(h->sym.invp.begin(), h->sym.invp.end(), invp);
+  return SPB_OK;
+}
+
+int spb_get_mmd_invp(spb_handle* h, int32_t* invp) {
+  if (check_handle(h)) return SPB_ERR_INVALID;
+  if (!h->have_symbolic) return fail(h, SPB_ERR_STATE, "no symbolic factorization");
+  if (invp) std::copy(h->sym.mmd_invp.begin(), h->sym.mmd_invp.end(), invp);
+  return SPB_OK;
+}
+
+int spb_get_etree(spb_handle* h, int32_t* parent) {
+  if (check_handle(h)) return SPB_ERR_INVALID;
+  if (!h->have_symbolic) return fail(h, SPB_ERR_STATE, "no symbolic factorization");
+  if (parent) std::copy(h->sym.parent.begin(), h->sym.parent.end(), parent);
+  return SPB_OK;
+}
+
+int spb_get_colcounts(spb_handle* h, int32_t* cc_fund, int32_t* cc_relaxed) {
+  if (check_handle(h)) return SPB_ERR_INVALID;
+  if (!h->have_symbolic) return fail(h, SPB_ERR_STATE, "no symbolic factorization");
+  if (cc_fund) std::copy(h->sym.cc_fund.begin(), h->sym.cc_fund.end(), cc_fund);
+  if (cc_relaxed) std::copy(h->sym.cc.begin(), h->sym.cc.end(), cc_relaxed);
+  return SPB_OK;
+}
+
+int spb_get_supernodes(spb_handle* h, int32_t* xsuper, int32_t* supmember) {
+  if (check_handle(h)) return SPB_ERR_INVALID;
+  if (!h->have_symbolic) return fail(h, SPB_ERR_STATE, "no symbolic factorization");
+  if (xsuper) std::copy(h->sym.xsuper.begin(), h->sym.xsuper.end(), xsuper);
+  if (supmember) std::copy(h->sym.supmember.begin(), h->sym.supmember.end(), supmember);
+  return SPB_OK;
+}
+
+int spb_get_structure(spb_handle* h, int64_t* xlindx, int32_t* lindx) {
+  if (check_handle(h)) return SPB_ERR_INVALID;
+  if (!h->have_symbolic) return fail(h, SPB_ERR_STATE, "no symbolic factorization");
+  if (xlindx) std::copy(h->sym.xlindx.begin(), h->sym.xlindx.end(), xlindx);
+  if (lindx) std::copy(h->sym.lindx.begin(), h->sym.lindx.end(), lindx);
+  return SPB_OK;
+}
+
+int spb_get_cells(spb_handle* h, int32_t* cI, int32_t* cK, int32_t* cnr, int32_t* cfb, int32_t* cnb, int32_t* bfr,
+                  int32_t* bnr) {
+  if (check_handle(h)) return SPB_ERR_INVALID;
+  if (!h->have_symbolic) return fail(h, SPB_ERR_STATE, "no symbolic factorization");
+  if (!h->cells_built) {
+    h->cells = spb::build_cells(h->sym);
+    h->cells_built = true;
+  }
+  const auto& C = h->cells;
+  for (size_t i = 0; i < C.cells.size(); ++i) {
+    if (cI) cI[i] = C.cells[i].I;
+    if (cK) cK[i] = C.cells[i].K;
+    if (cnr) cnr[i] = C.cells[i].nrows;
+    if (cfb) cfb[i] = C.cells[i].first_block;
+    if (cnb) cnb[i] = C.cells[i].nblocks;
+  }
+  if (bfr) std::copy(C.block_first_row.begin(), C.block_first_row.end(), bfr);
+  if (bnr) std::copy(C.block_nrows.begin(), C.block_nrows.end(), bnr);
+  return SPB_OK;
+}
+
+int spb_get_factor(spb_handle* h, double* out) {
+  if (check_handle(h) || !out) return SPB_ERR_INVALID;
+  if (!h->factored) return fail(h, SPB_ERR_STATE, "get_factor: call spb_factorize first");
+  SPB_CK(h, cudaSetDevice(h->device));
+  const spb::Plan& P = h->plan;
+  std::vector<double> arena(P.arena_elems);
+  SPB_CK(h, cudaMemcpy(arena.data(), h->dL, P.arena_elems * 8, cudaMemcpyDeviceToHost));
+  int64_t pos = 0;
+  for (const auto& m : P.meta) {
+    for (int c = 0; c < m.w; ++c)
+      for (int r = 0; r < m.h; ++r) out[pos + r + (int64_t)c * m.h] = (r < c) ? 0.0 : arena[m.off + r + (int64_t)c * m.ld];
+    pos += (int64_t)m.h * m.w;
+  }
+  return SPB_OK;
+}
+
+int spb_get_status(spb_handle* h, int32_t* code, int32_t* supernode, int32_t* column) {
+  if (check_handle(h)) return SPB_ERR_INVALID;
+  if (!h->have_symbolic) return fail(h, SPB_ERR_STATE, "no symbolic factorization");
+  SPB_CK(h, cudaSetDevice(h->device));
+  Status st;
+  SPB_CK(h, cudaMemcpy(&st, h->dstatus, sizeof(st), cudaMemcpyDeviceToHost));
+  if (code) *code = st.code;
+  if (supernode) *supernode = st.supernode;
+  if (column) *column = st.column;
+  return SPB_OK;
+}
+
+}  // extern "C"

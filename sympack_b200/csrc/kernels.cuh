@@ -1,0 +1,55 @@
+// Device kernels of the supernodal Cholesky factor and solve (sm_100a).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "plan.hpp"
+
+namespace spb {
+namespace dev {
+
+// Status word shared by all kernels of one handle.  The first failure wins.
+struct Status {
+  int32_t code;        // 0 ok, 1 not SPD, 2 structure error
+  int32_t supernode;   // 0-based supernode of the failing pivot
+  int32_t column;      // 0-based permuted column of the failing pivot
+  int32_t pad;
+};
+
+// Arguments shared by the factor kernels.
+struct FactorArgs {
+  double* L;                 // factor arena
+  const SnMeta* meta;        // nsuper
+  const int32_t* rows;       // concatenated 0-based row lists
+  const int32_t* supmember;  // 0-based supernode of each permuted column
+  Status* status;
+};
+
+// Must run once per process (per device) before the first launch or capture.
+void init_kernel_attributes();
+void launch_assemble(cudaStream_t st, double* L, const int64_t* dst, const double* vals, int64_t nnz);
+void launch_factor_small(cudaStream_t st, const FactorArgs& a, const int32_t* items, int count, int smem_bytes);
+void launch_potrf_diag(cudaStream_t st, const FactorArgs& a, const PanelItem* items, int count);
+void launch_trsm_rows(cudaStream_t st, const FactorArgs& a, const PanelItem* items, int count);
+void launch_gemm(cudaStream_t st, const FactorArgs& a, const TileItem* items, int count, int tile);
+
+// Solve on the permuted right-hand sides X (n x nrhs, column-major, leading dimension ldx).
+struct SolveArgs {
+  const double* L;
+  const SnMeta* meta;
+  const int32_t* rows;
+  double* X;
+  int64_t ldx;
+  int nrhs;
+};
+void launch_solve_forward(cudaStream_t st, const SolveArgs& a, const int32_t* sn, int count);
+void launch_solve_backward(cudaStream_t st, const SolveArgs& a, const int32_t* sn, int count);
+
+// X[invp[i], c] = B[i, c]   and   B[i, c] = X[invp[i], c]
+void launch_permute_in(cudaStream_t st, double* X, int64_t ldx, const double* B, int64_t ldb,
+                       const int32_t* invp0, int n, int nrhs);
+void launch_permute_out(cudaStream_t st, double* B, int64_t ldb, const double* X, int64_t ldx,
+                        const int32_t* invp0, int n, int nrhs);
+
+}  // namespace dev
+}  // namespace spb

@@ -1,0 +1,163 @@
+#include "plan.hpp"
+
+#include <algorithm>
+#include <stdexcept>
+
+namespace spb {
+
+static int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
+
+Plan build_plan(const Symbolic& sym, const PlanParams& prm) {
+  Plan P;
+  P.n = sym.n;
+  P.nsuper = sym.nsuper();
+  const int ns = P.nsuper;
+  P.meta.resize(ns);
+  P.rows.resize(sym.lindx.size());
+  for (size_t k = 0; k < sym.lindx.size(); ++k) P.rows[k] = sym.lindx[k] - 1;
+  P.lindx_total = (int64_t)sym.lindx.size();
+  P.supmember0.resize(sym.n);
+  for (int i = 0; i < sym.n; ++i) P.supmember0[i] = sym.supmember[i] - 1;
+
+  int64_t off = 0;
+  for (int s = 0; s < ns; ++s) {
+    SnMeta& m = P.meta[s];
+    m.fc = sym.xsuper[s] - 1;
+    m.w = sym.xsuper[s + 1] - sym.xsuper[s];
+    m.h = (int32_t)(sym.xlindx[s + 1] - sym.xlindx[s]);
+    m.ld = (int32_t)round_up(m.h, 4);
+    m.off = off;
+    m.lidx = sym.xlindx[s] - 1;
+    off += round_up((int64_t)m.ld * m.w, 32);
+  }
+  P.arena_elems = off;
+
+  // supernodal elimination tree and height levels
+  P.sparent.assign(ns, -1);
+  for (int s = 0; s < ns; ++s) {
+    int lc = sym.xsuper[s + 1] - 1;  // 1-based last column
+    int pc = sym.parent[lc - 1];
+    P.sparent[s] = pc ? sym.supmember[pc - 1] - 1 : -1;
+  }
+  P.level.assign(ns, 0);
+  for (int s = 0; s < ns; ++s)  // children precede parents in postorder
+    if (P.sparent[s] >= 0) P.level[P.sparent[s]] = std::max(P.level[P.sparent[s]], P.level[s] + 1);
+  int H = 0;
+  for (int s = 0; s < ns; ++s) H = std::max(H, P.level[s] + 1);
+  P.nlevels = H;
+  P.level_sn.assign(H, {});
+  for (int s = 0; s < ns; ++s) P.level_sn[P.level[s]].push_back(s);
+
+  P.is_big.assign(ns, 0);
+  for (int s = 0; s < ns; ++s) {
+    const SnMeta& m = P.meta[s];
+    bool small = m.w <= prm.small_max_w && (int64_t)m.h * m.w * 8 <= prm.small_max_bytes;
+    P.is_big[s] = small ? 0 : 1;
+    double w = m.w, mm = m.h - m.w;
+    P.exec_flops += w * w * w / 3.0 + mm * w * w + mm * mm * w;
+  }
+
+  const int T = prm.tile_ext_small;
+  auto push_tiles = [&](int s, int mode, int rbeg, int rend, int cbeg, int cend, int k0, int kn,
+                        bool lower_only) {
+    // tiles of the (rend-rbeg) x (cend-cbeg) product; rows/cols counted from rbeg/cbeg
+    for (int cj = cbeg; cj < cend; cj += T)
+      for (int ri = rbeg; ri < rend; ri += T) {
+        // skip tiles entirely above the diagonal of a symmetric product
+        if (lower_only && (ri - rbeg) + T <= (cj - cbeg)) continue;
+        TileItem t;
+        t.s = s;
+        t.mode = mode;
+        t.a_row0 = ri;
+        t.b_row0 = cj;
+        t.k0 = k0;
+        t.kn = kn;
+        t.mrows = std::min(T, rend - ri);
+        t.ncols = std::min(T, cend - cj);
+        P.tile_items.push_back(t);
+      }
+  };
+
+  for (int L = 0; L < H; ++L) {
+    const auto& sns = P.level_sn[L];
+    // 1. fused small panels
+    {
+      Step st{StepKind::FactorSmall, (int32_t)P.small_items.size(), 0, 0, 0};
+      for (int s : sns)
+        if (!P.is_big[s]) {
+          P.small_items.push_back(s);
+          st.arg = std::max<int32_t>(st.arg, P.meta[s].h * P.meta[s].w * 8);
+        }
+      st.count = (int32_t)P.small_items.size() - st.begin;
+      if (st.count) P.steps.push_back(st);
+    }
+    // 2. blocked factorization of big panels, all big panels of the level in lockstep
+    int maxw = 0;
+    for (int s : sns)
+      if (P.is_big[s]) maxw = std::max(maxw, P.meta[s].w);
+    for (int c0 = 0; c0 < maxw; c0 += prm.nb) {
+      Step pd{StepKind::PotrfDiag, (int32_t)P.panel_items.size(), 0, c0, 0};
+      for (int s : sns) {
+        if (!P.is_big[s] || c0 >= P.meta[s].w) continue;
+        P.panel_items.push_back(PanelItem{s, c0, std::min(prm.nb, P.meta[s].w - c0), -1});
+      }
+      pd.count = (int32_t)P.panel_items.size() - pd.begin;
+      if (pd.count) P.steps.push_back(pd);
+      Step pt{StepKind::TrsmRows, (int32_t)P.panel_items.size(), 0, c0, 0};
+      for (int s : sns) {
+        if (!P.is_big[s]) continue;
+        const SnMeta& m = P.meta[s];
+        if (c0 >= m.w) continue;
+        int nbk = std::min(prm.nb, m.w - c0);
+        for (int r = c0 + nbk; r < m.h; r += 64) P.panel_items.push_back(PanelItem{s, c0, nbk, r});
+      }
+      pt.count = (int32_t)P.panel_items.size() - pt.begin;
+      if (pt.count) P.steps.push_back(pt);
+      Step gs{StepKind::Gemm, (int32_t)P.tile_items.size(), 0, 0, T};
+      for (int s : sns) {
+        if (!P.is_big[s]) continue;
+        const SnMeta& m = P.meta[s];
+        if (c0 >= m.w) continue;
+        int nbk = std::min(prm.nb, m.w - c0);
+        int c1 = c0 + nbk;
+        if (c1 >= m.w) continue;
+        push_tiles(s, 0, c1, m.h, c1, m.w, c0, nbk, true);
+      }
+      gs.count = (int32_t)P.tile_items.size() - gs.begin;
+      if (gs.count) P.steps.push_back(gs);
+    }
+    // 3. external Schur-complement updates of every panel of the level
+    {
+      Step gs{StepKind::Gemm, (int32_t)P.tile_items.size(), 0, 0, T};
+      for (int s : sns) {
+        const SnMeta& m = P.meta[s];
+        if (m.h > m.w) push_tiles(s, 1, m.w, m.h, m.w, m.h, 0, m.w, true);
+      }
+      gs.count = (int32_t)P.tile_items.size() - gs.begin;
+      if (gs.count) P.steps.push_back(gs);
+    }
+  }
+  return P;
+}
+
+std::vector<int64_t> build_assembly_map(const Symbolic& sym, const Plan& P, const int64_t* colptr,
+                                        const int32_t* rowind) {
+  const int n = sym.n;
+  const int64_t nnz = colptr[n] - 1;
+  std::vector<int64_t> dst(nnz);
+  for (int c = 1; c <= n; ++c)
+    for (int64_t p = colptr[c - 1]; p < colptr[c]; ++p) {
+      int r = rowind[p - 1];
+      int pr = sym.invp[r - 1] - 1, pc = sym.invp[c - 1] - 1;
+      if (pr < pc) std::swap(pr, pc);
+      int s = P.supmember0[pc];
+      const SnMeta& m = P.meta[s];
+      const int32_t* rl = P.rows.data() + m.lidx;
+      const int32_t* it = std::lower_bound(rl, rl + m.h, pr);
+      if (it == rl + m.h || *it != pr) throw std::runtime_error("assembly: entry outside the symbolic structure");
+      dst[p - 1] = m.off + (int64_t)(pc - m.fc) * m.ld + (it - rl);
+    }
+  return dst;
+}
+
+}  // namespace spb

@@ -1,0 +1,113 @@
+// Device plan: how the supernodal factor is laid out in HBM and in which order
+// the hot-path kernels visit it.  Built once per sparsity structure on the host
+// from the symbolic result; reused by every numeric factorization and solve.
+//
+// Layout.  Supernode s owns one column-major panel of h_s x w_s doubles (the
+// diagonal block followed by every off-diagonal row of its structure), with a
+// leading dimension ld_s >= h_s padded to a multiple of 4 and a panel offset
+// that is a multiple of 32 elements (256 B).  This is the reference's set of
+// cells (K, s) (symPACKMatrix2D.hpp:499-944) stored contiguously: cell (K, s)
+// is the run of panel rows whose global row falls in supernode K.
+//
+// Schedule.  The supernodal elimination tree is levelled by height (leaves at
+// level 0).  Supernodes of one level never depend on each other, so one level
+// is: factor all of its panels, then scatter all of their Schur-complement
+// updates into ancestors.  This is the reference's FACTOR -> TRSM ->
+// UPDATE2D_COMP dependency chain (symPACKMatrix2D.hpp:3893-3997) collapsed to
+// supernode granularity.
+#pragma once
+#include <cstdint>
+#include <vector>
+
+#include "symbolic.hpp"
+
+namespace spb {
+
+// Panel descriptor (device-visible).
+struct SnMeta {
+  int32_t fc;    // first column, 0-based (permuted numbering)
+  int32_t w;     // width (number of columns)
+  int32_t h;     // rows, including the w x w diagonal block
+  int32_t ld;    // leading dimension of the panel
+  int64_t off;   // element offset of the panel in the factor arena
+  int64_t lidx;  // offset of this supernode's row list in the device row array
+};
+
+// One tile of a Schur-complement product  C = A * B^T  over panel columns
+// [k0, k0+kn) of supernode s, rows a_row0.. of A and b_row0.. of B (panel rows).
+//  mode 0: in-panel update, C is subtracted from panel(s) rows a_row0+i, columns b_row0+j
+//  mode 1: external update, C is scatter-subtracted into the ancestors that own
+//          global rows lindx_s[a_row0+i] x lindx_s[b_row0+j]
+struct TileItem {
+  int32_t s;
+  int32_t mode;
+  int32_t a_row0;
+  int32_t b_row0;
+  int32_t k0;
+  int32_t kn;
+  int32_t mrows;  // valid rows in this tile (<= tile height)
+  int32_t ncols;  // valid columns in this tile (<= tile width)
+};
+
+// One launch of the factorization sequence.
+enum class StepKind : int32_t {
+  FactorSmall = 0,   // fused POTRF + TRSM of whole panels in shared memory (items = supernode ids)
+  PotrfDiag = 1,     // POTRF of one 64-column diagonal block of a wide panel (PanelItem, row0 = -1)
+  TrsmRows = 2,      // TRSM of 64-row tiles below that block (PanelItem)
+  Gemm = 3,          // TileItem list (in-panel or external update)
+};
+struct Step {
+  StepKind kind;
+  int32_t begin;  // range into the matching item array
+  int32_t count;
+  int32_t arg;    // PotrfDiag/TrsmRows: column block start c0; FactorSmall: shared-memory bytes
+  int32_t tile;   // Gemm: tile edge (64 or 128)
+};
+
+// Panel-block work: supernode s, column block [c0, c0+nb), row tile starting at row0.
+struct PanelItem {
+  int32_t s;
+  int32_t c0;
+  int32_t nb;
+  int32_t row0;   // first panel row of the row tile (>= c0+nb); -1 for the diagonal block
+};
+
+struct Plan {
+  int n = 0;
+  int nsuper = 0;
+  int nlevels = 0;
+  int64_t arena_elems = 0;      // total doubles in the factor arena
+  int64_t lindx_total = 0;
+  std::vector<SnMeta> meta;     // nsuper
+  std::vector<int32_t> rows;    // concatenated 0-based row lists (device copy)
+  std::vector<int32_t> supmember0;  // 0-based supernode of each (permuted) column
+  std::vector<int32_t> sparent;     // supernodal etree parent (0-based, -1 root)
+  std::vector<int32_t> level;       // height level of each supernode
+  std::vector<std::vector<int32_t>> level_sn;  // supernodes per level
+  // factorization sequence
+  std::vector<int32_t> small_items;  // supernode ids for FactorSmall steps
+  std::vector<PanelItem> panel_items;
+  std::vector<TileItem> tile_items;
+  std::vector<Step> steps;
+  // executed flop count of the sequence (w^3/3 + m w^2 + m^2 w per supernode)
+  double exec_flops = 0.0;
+  // solve: supernodes of each level (shared with level_sn); big ones flagged
+  std::vector<uint8_t> is_big;
+};
+
+// Tunables of the plan.
+struct PlanParams {
+  int small_max_w = 32;          // widest panel handled by the fused small-panel kernel
+  int small_max_bytes = 96 * 1024;
+  int nb = 64;                   // column block of the blocked panel factorization
+  int tile_ext_small = 64;       // tile edge for external updates
+};
+
+Plan build_plan(const Symbolic& s, const PlanParams& p = PlanParams());
+
+// Destination of each entry of A's lower triangle (input order) in the arena,
+// DistributeMatrix (symPACKMatrix2D.hpp:6336-6576) done once per structure.
+std::vector<int64_t> build_assembly_map(const Symbolic& s, const Plan& plan, const int64_t* colptr,
+                                        const int32_t* rowind);
+
+}  // namespace spb

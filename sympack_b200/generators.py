@@ -1,0 +1,138 @@
+"""Seeded synthetic SPD matrices of the shapes the benchmarks and tests use.
+
+Every generator returns the lower triangle, diagonal included, as 1-based CSC
+(colptr int64, rowind int32 sorted per column, nzval float64) — the input
+convention of symPACK's DistSparseMatrix.  Grid points are numbered x fastest.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+
+def _coo_to_lower_csc(n, rows, cols, vals):
+    """rows >= cols (0-based) -> 1-based lower CSC with rows sorted per column."""
+    order = np.lexsort((rows, cols))
+    rows, cols, vals = rows[order], cols[order], vals[order]
+    colptr = np.zeros(n + 1, np.int64)
+    np.add.at(colptr, cols + 1, 1)
+    colptr = np.cumsum(colptr) + 1
+    colptr[0] = 1
+    return colptr.astype(np.int64), (rows + 1).astype(np.int32), vals.astype(np.float64)
+
+
+def _grid_edges(dims, offsets):
+    """Pairs (i, j), i < j, of grid points joined by one of the given offsets.
+    dims = (nx, ny[, nz]); offsets are (dx, dy[, dz]) tuples."""
+    dims = tuple(int(d) for d in dims) + (1,) * (3 - len(dims))
+    nx, ny, nz = dims
+    idx = np.arange(nx * ny * nz, dtype=np.int64).reshape(nz, ny, nx)
+    pi, pj = [], []
+    for off in offsets:
+        off = tuple(off) + (0,) * (3 - len(off))
+        src, dst = [], []
+        for d, size in ((off[2], nz), (off[1], ny), (off[0], nx)):
+            if d >= 0:
+                src.append(slice(0, size - d))
+                dst.append(slice(d, size))
+            else:
+                src.append(slice(-d, size))
+                dst.append(slice(0, size + d))
+        a, b = idx[tuple(src)].ravel(), idx[tuple(dst)].ravel()
+        pi.append(np.minimum(a, b))
+        pj.append(np.maximum(a, b))
+    if not pi:
+        return np.empty(0, np.int64), np.empty(0, np.int64)
+    return np.concatenate(pi), np.concatenate(pj)
+
+
+def _forward_offsets(ndim, full):
+    """Half of the stencil's neighbour offsets (one of each +/- pair)."""
+    rng = (-1, 0, 1)
+    offs = []
+    if ndim == 2:
+        cand = [(dx, dy) for dy in rng for dx in rng]
+    else:
+        cand = [(dx, dy, dz) for dz in rng for dy in rng for dx in rng]
+    for o in cand:
+        if not any(o):
+            continue
+        if not full and sum(abs(v) for v in o) != 1:
+            continue
+        # keep the lexicographically positive representative of +/- o
+        rev = tuple(reversed(o))
+        if rev > tuple(0 for _ in o):
+            offs.append(o)
+    return offs
+
+
+def laplacian_2d(nx: int, ny: int, shift: float = 0.0):
+    """5-point Dirichlet Laplacian: diagonal 4 + shift, neighbours -1."""
+    n = nx * ny
+    i, j = _grid_edges((nx, ny), _forward_offsets(2, False))
+    rows = np.concatenate([np.arange(n), j])
+    cols = np.concatenate([np.arange(n), i])
+    vals = np.concatenate([np.full(n, 4.0 + shift), -np.ones(len(i))])
+    return (n, *_coo_to_lower_csc(n, rows, cols, vals))
+
+
+def laplacian_3d(nx: int, ny: int, nz: int, shift: float = 0.0):
+    """7-point Dirichlet Laplacian: diagonal 6 + shift, neighbours -1."""
+    n = nx * ny * nz
+    i, j = _grid_edges((nx, ny, nz), _forward_offsets(3, False))
+    rows = np.concatenate([np.arange(n), j])
+    cols = np.concatenate([np.arange(n), i])
+    vals = np.concatenate([np.full(n, 6.0 + shift), -np.ones(len(i))])
+    return (n, *_coo_to_lower_csc(n, rows, cols, vals))
+
+
+def _dominant(n, i, j, off, delta):
+    absum = np.zeros(n)
+    np.add.at(absum, i, np.abs(off))
+    np.add.at(absum, j, np.abs(off))
+    diag = absum * (1.0 + delta)
+    diag[diag == 0] = 1.0
+    rows = np.concatenate([np.arange(n), j])
+    cols = np.concatenate([np.arange(n), i])
+    vals = np.concatenate([diag, off])
+    return (n, *_coo_to_lower_csc(n, rows, cols, vals))
+
+
+def stencil27(nx: int, ny: int, nz: int, delta: float, seed: int = 0):
+    """27-point stencil: off-diagonals U[-1, 0) from seed, diagonal = |row sum| (1 + delta)."""
+    n = nx * ny * nz
+    i, j = _grid_edges((nx, ny, nz), _forward_offsets(3, True))
+    rng = np.random.default_rng(seed)
+    off = -rng.uniform(0.0, 1.0, size=len(i))  # in (-1, 0]
+    off[off == 0.0] = -0.5
+    return _dominant(n, i, j, off, delta)
+
+
+def random_graph_spd(n: int, avg_degree: float = 10.0, dominance: float = 1.05, seed: int = 0):
+    """Random sparse graph, off-diagonals U[-1, 0), diagonal = dominance * |row sum|."""
+    rng = np.random.default_rng(seed)
+    m = int(n * avg_degree / 2)
+    a = rng.integers(0, n, size=m)
+    b = rng.integers(0, n, size=m)
+    keep = a != b
+    a, b = a[keep], b[keep]
+    lo, hi = np.minimum(a, b), np.maximum(a, b)
+    key = np.unique(lo.astype(np.int64) * n + hi)
+    lo, hi = key // n, key % n
+    off = -rng.uniform(0.0, 1.0, size=len(lo))
+    off[off == 0.0] = -0.5
+    return _dominant(n, lo, hi, off, dominance - 1.0)
+
+
+def config_matrix(name: str, **kw):
+    """Named workloads: 'lap2d_64' (n=4096), 'lap3d_60' (n=216,000, shift 1e-3),
+    'st27_80' (n=512,000, delta from kw), plus scaled-down variants 'lap3d_<k>', 'st27_<k>'."""
+    if name.startswith("lap2d_"):
+        k = int(name.split("_")[1])
+        return laplacian_2d(k, k)
+    if name.startswith("lap3d_"):
+        k = int(name.split("_")[1])
+        return laplacian_3d(k, k, k, shift=kw.get("shift", 1e-3))
+    if name.startswith("st27_"):
+        k = int(name.split("_")[1])
+        return stencil27(k, k, k, delta=kw.get("delta", 1e-2), seed=kw.get("seed", 0))
+    raise ValueError(name)
