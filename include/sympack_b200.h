@@ -68,7 +68,7 @@ typedef struct spb_options {
   int max_snode;           /* "-b": maximum supernode width, 0 = unlimited (driver default) */
   double zrelax0, zrelax1, zrelax2; /* relaxation zero fractions (0.8, 0.1, 0.05) */
   const int32_t* user_perm; /* SPB_ORDERING_USER: 1-based new->old permutation */
-  int device;              /* CUDA device ordinal */
+  int device;              /* CUDA device ordinal; < 0 = host-only handle (symbolic analysis only) */
   int precision;           /* SPB_PRECISION_* */
   double ir_tolerance;     /* backward-error target of refinement (1e-12) */
   int ir_max_iter;         /* refinement iteration cap */

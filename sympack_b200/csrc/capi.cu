@@ -206,6 +206,10 @@ int spb_create(const spb_options* opt, spb_handle** out) {
     return SPB_ERR_INVALID;
   }
   h->device = h->opt.device;
+  if (h->device < 0) {  // host-only handle: symbolic analysis and introspection, no CUDA
+    *out = h;
+    return SPB_OK;
+  }
   cudaError_t e = cudaSetDevice(h->device);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) {
@@ -220,6 +224,10 @@ int spb_create(const spb_options* opt, spb_handle** out) {
 
 void spb_destroy(spb_handle* h) {
   if (!h) return;
+  if (h->device < 0) {
+    delete h;
+    return;
+  }
   cudaSetDevice(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
   release_device(h);
@@ -232,8 +240,10 @@ const char* spb_last_error(const spb_handle* h) { return h ? h->err.c_str() : "n
 int spb_symbolic(spb_handle* h, int32_t n, const int64_t* colptr, const int32_t* rowind) {
   if (check_handle(h)) return SPB_ERR_INVALID;
   if (n <= 0 || !colptr || !rowind) return fail(h, SPB_ERR_INVALID, "symbolic: empty matrix or null pointer");
-  SPB_CK(h, cudaSetDevice(h->device));
-  release_device(h);
+  if (h->device >= 0) {
+    SPB_CK(h, cudaSetDevice(h->device));
+    release_device(h);
+  }
   h->have_symbolic = h->have_values = h->factored = h->have_solution = false;
   h->cells_built = false;
   try {
@@ -267,6 +277,10 @@ int spb_symbolic(spb_handle* h, int32_t n, const int64_t* colptr, const int32_t*
     amap = spb::build_assembly_map(h->sym, h->plan, colptr, rowind);
   } catch (const std::exception& e) {
     return fail(h, SPB_ERR_STRUCTURE, e.what());
+  }
+  if (h->device < 0) {
+    h->have_symbolic = true;
+    return SPB_OK;
   }
   const spb::Plan& P = h->plan;
   std::vector<int32_t> lsn, invp0(n);
@@ -322,6 +336,7 @@ static int distribute_common(spb_handle* h) {
 
 int spb_distribute(spb_handle* h, const double* nzval) {
   if (check_handle(h)) return SPB_ERR_INVALID;
+  if (h->device < 0) return fail(h, SPB_ERR_STATE, "host-only handle (device < 0) has no numeric phase");
   if (!h->have_symbolic) return fail(h, SPB_ERR_STATE, "distribute: call spb_symbolic first");
   if (!nzval) return fail(h, SPB_ERR_INVALID, "distribute: null values");
   SPB_CK(h, cudaSetDevice(h->device));
@@ -331,6 +346,7 @@ int spb_distribute(spb_handle* h, const double* nzval) {
 
 int spb_distribute_device(spb_handle* h, const double* d_nzval) {
   if (check_handle(h)) return SPB_ERR_INVALID;
+  if (h->device < 0) return fail(h, SPB_ERR_STATE, "host-only handle (device < 0) has no numeric phase");
   if (!h->have_symbolic) return fail(h, SPB_ERR_STATE, "distribute: call spb_symbolic first");
   if (!d_nzval) return fail(h, SPB_ERR_INVALID, "distribute: null values");
   SPB_CK(h, cudaSetDevice(h->device));
@@ -340,6 +356,7 @@ int spb_distribute_device(spb_handle* h, const double* d_nzval) {
 
 int spb_factorize(spb_handle* h) {
   if (check_handle(h)) return SPB_ERR_INVALID;
+  if (h->device < 0) return fail(h, SPB_ERR_STATE, "host-only handle (device < 0) has no numeric phase");
   if (!h->have_values) return fail(h, SPB_ERR_STATE, "factorize: call spb_distribute first");
   if (h->factored) return fail(h, SPB_ERR_STATE, "factorize: values already factored; distribute again");
   SPB_CK(h, cudaSetDevice(h->device));
@@ -370,6 +387,7 @@ int spb_factorize(spb_handle* h) {
 
 int spb_solve_device(spb_handle* h, const double* d_rhs, double* d_x, int32_t nrhs, int64_t ld) {
   if (check_handle(h)) return SPB_ERR_INVALID;
+  if (h->device < 0) return fail(h, SPB_ERR_STATE, "host-only handle (device < 0) has no numeric phase");
   if (!h->factored) return fail(h, SPB_ERR_STATE, "solve: call spb_factorize first");
   const int n = h->sym.n;
   if (nrhs <= 0 || ld < n || !d_rhs || !d_x) return fail(h, SPB_ERR_INVALID, "solve: bad right-hand side");
@@ -386,6 +404,7 @@ int spb_solve_device(spb_handle* h, const double* d_rhs, double* d_x, int32_t nr
 
 int spb_solve(spb_handle* h, const double* rhs, int32_t nrhs, int64_t ldb) {
   if (check_handle(h)) return SPB_ERR_INVALID;
+  if (h->device < 0) return fail(h, SPB_ERR_STATE, "host-only handle (device < 0) has no numeric phase");
   if (!h->factored) return fail(h, SPB_ERR_STATE, "solve: call spb_factorize first");
   const int n = h->sym.n;
   if (nrhs <= 0 || ldb < n || !rhs) return fail(h, SPB_ERR_INVALID, "solve: bad right-hand side");
@@ -405,6 +424,7 @@ int spb_solve(spb_handle* h, const double* rhs, int32_t nrhs, int64_t ldb) {
 
 int spb_get_solution(spb_handle* h, double* B, int32_t nrhs, int64_t ldb) {
   if (check_handle(h)) return SPB_ERR_INVALID;
+  if (h->device < 0) return fail(h, SPB_ERR_STATE, "host-only handle (device < 0) has no numeric phase");
   if (!h->have_solution) return fail(h, SPB_ERR_STATE, "get_solution: call spb_solve first");
   const int n = h->sym.n;
   if (!B || nrhs <= 0 || nrhs > h->x_nrhs || ldb < n) return fail(h, SPB_ERR_INVALID, "get_solution: bad output");
@@ -512,6 +532,7 @@ int spb_get_cells(spb_handle* h, int32_t* cI, int32_t* cK, int32_t* cnr, int32_t
 
 int spb_get_factor(spb_handle* h, double* out) {
   if (check_handle(h) || !out) return SPB_ERR_INVALID;
+  if (h->device < 0) return fail(h, SPB_ERR_STATE, "host-only handle (device < 0) has no numeric phase");
   if (!h->factored) return fail(h, SPB_ERR_STATE, "get_factor: call spb_factorize first");
   SPB_CK(h, cudaSetDevice(h->device));
   const spb::Plan& P = h->plan;
@@ -528,6 +549,7 @@ int spb_get_factor(spb_handle* h, double* out) {
 
 int spb_get_status(spb_handle* h, int32_t* code, int32_t* supernode, int32_t* column) {
   if (check_handle(h)) return SPB_ERR_INVALID;
+  if (h->device < 0) return fail(h, SPB_ERR_STATE, "host-only handle (device < 0) has no numeric phase");
   if (!h->have_symbolic) return fail(h, SPB_ERR_STATE, "no symbolic factorization");
   SPB_CK(h, cudaSetDevice(h->device));
   Status st;
