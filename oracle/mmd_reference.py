@@ -1,0 +1,60 @@
+"""ORACLE — the reference's own MMD Fortran (src/ordmmd.F, genmmd.F, mmdint.F,
+mmdelm.F, mmdupd.F, mmdnum.F), translated by oracle/f77_to_c.py and compiled
+into oracle/_ref/libmmd_ref.so.  Building needs the reference sources
+(present in the development container only); the built library may travel.
+Called exactly as Ordering::MMD calls it (src/Ordering.cpp:103-218): the
+expanded graph without diagonal, iwsiz = 4n, invp taken as the result."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+REF_SRC = Path("/root/reference/src")
+FILES = ["ordmmd.F", "genmmd.F", "mmdint.F", "mmdelm.F", "mmdupd.F", "mmdnum.F"]
+OUT_C = HERE / "_ref" / "mmd_ref.c"
+OUT_SO = HERE / "_ref" / "libmmd_ref.so"
+_lib = None
+
+
+def available() -> bool:
+    return OUT_SO.exists() or all((REF_SRC / f).exists() for f in FILES)
+
+
+def build(force: bool = False) -> Path:
+    if OUT_SO.exists() and not force:
+        return OUT_SO
+    if not all((REF_SRC / f).exists() for f in FILES):
+        raise FileNotFoundError("reference MMD sources not present")
+    OUT_SO.parent.mkdir(exist_ok=True)
+    from . import f77_to_c
+    OUT_C.write_text(f77_to_c.translate([str(REF_SRC / f) for f in FILES]))
+    tmp = OUT_SO.with_suffix(".tmp.so")
+    subprocess.run(["gcc", "-O2", "-fPIC", "-shared", "-Wno-unused-label", "-o", str(tmp), str(OUT_C)], check=True)
+    os.replace(tmp, OUT_SO)
+    return OUT_SO
+
+
+def ordmmd(n: int, xadj, adj) -> np.ndarray:
+    """invp (1-based) of the reference MMD on a graph given as 1-based xadj/adj."""
+    global _lib
+    if _lib is None:
+        _lib = C.CDLL(str(build()))
+    P = C.POINTER(C.c_int32)
+    xadj = np.ascontiguousarray(xadj, np.int32)
+    adj = np.ascontiguousarray(adj, np.int32).copy()  # destroyed by genmmd
+    invp = np.zeros(n, np.int32)
+    perm = np.zeros(n, np.int32)
+    iwsiz = C.c_int32(4 * n)
+    iwork = np.zeros(4 * n, np.int32)
+    N, nadj, nofsub, iflag = C.c_int32(n), C.c_int32(len(adj)), C.c_int32(0), C.c_int32(0)
+    _lib.ordmmd_(C.byref(N), C.byref(nadj), xadj.ctypes.data_as(P), adj.ctypes.data_as(P),
+                 invp.ctypes.data_as(P), perm.ctypes.data_as(P), C.byref(iwsiz), iwork.ctypes.data_as(P),
+                 C.byref(nofsub), C.byref(iflag))
+    if iflag.value != 0:
+        raise RuntimeError(f"ordmmd iflag={iflag.value}")
+    return invp
