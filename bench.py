@@ -1,0 +1,399 @@
+"""Benchmark of the supernodal Cholesky factor + solve hot path.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (one GPU): 3D 7-point Laplacian on a 60^3 grid with diagonal shift
+1e-3 (n = 216,000), FP64, MMD ordering, right-hand sides standard-normal from
+seed 0 with nrhs in {1, 16}.  Synthetic data of that shape; the factor arena
+(1.4 GB) is far larger than L2, so no flush is needed between steps.
+
+One step = DistributeMatrix (values already in HBM) + Factorize + Solve(nrhs=1)
++ Solve(nrhs=16).  `value` is factor TFLOP/s using the reference's own flop
+statistic (sum of squared column counts); solves/s, backward errors, p50/p99
+step latency, a roofline of the dominant kernel, the end-to-end number through
+the host-buffer API and the CPU baseline ride on the same JSON line.
+
+Multi-GPU: one factorization does not shard, so N ranks run N independent
+replicas (weak scaling); timings are the max over ranks.
+
+--impl reference times the CPU restatement of the reference's numeric path
+(oracle/, OpenBLAS on all host cores) on the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = "3D 7-point Laplacian 60^3 + 1e-3 I (n=216000), FP64, MMD, nrhs 1 and 16"
+METRIC = "factor TFLOP/s (FP64 supernodal Cholesky, flops = sum of squared column counts)"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--grid", type=int, default=60, help="grid edge of the 3D Laplacian (60 = the named workload)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def build_matrix(k):
+    from sympack_b200 import generators as G
+    return G.laplacian_3d(k, k, k, shift=1e-3)
+
+
+def backward_error(A, x, b):
+    """||b - A x||_inf / (||A||_inf ||x||_inf + ||b||_inf), per right-hand side (max)."""
+    r = b - A.matvec(x)
+    n = A.size
+    cols = np.repeat(np.arange(n), np.diff(A.colptr))
+    rows = A.rowind - 1
+    rowsum = np.zeros(n)
+    np.add.at(rowsum, rows, np.abs(A.nzvalLocal))
+    off = rows != cols
+    np.add.at(rowsum, cols[off], np.abs(A.nzvalLocal[off]))
+    anorm = rowsum.max()
+    r2, x2, b2 = r.reshape(n, -1), x.reshape(n, -1), b.reshape(n, -1)
+    eta = np.abs(r2).max(0) / (anorm * np.abs(x2).max(0) + np.abs(b2).max(0))
+    return float(eta.max())
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, f[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_fp64_peak(torch, dev):
+    """cuBLAS DGEMM throughput on this GPU (TFLOP/s): the FP64 tensor-pipe denominator."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device=dev)
+    b = torch.randn(n, n, dtype=torch.float64, device=dev)
+    for _ in range(3):
+        torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 0.0
+    for _ in range(5):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        torch.cuda.synchronize()
+        best = max(best, 2.0 * n ** 3 / (s.elapsed_time(e) * 1e-3) / 1e12)
+    del a, b
+    torch.cuda.empty_cache()
+    return best
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "MEASURED_PEAKS.json"
+    except (OSError, ValueError):
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def cpu_baseline_run(n, cp, ri, v, sym, flops, steps=1, warmup=0):
+    """CPU restatement of the reference numeric path (oracle, OpenBLAS, all host cores)."""
+    from oracle import numeric
+    cores = os.cpu_count() or 1
+    f = numeric.OracleFactor(n, sym, threads=cores)
+    rng = np.random.default_rng(0)
+    b1 = rng.standard_normal((n, 1))
+    b16 = rng.standard_normal((n, 16))
+    fac, s1, s16 = [], [], []
+    for it in range(warmup + steps):
+        f.distribute(cp, ri, v)
+        t0 = time.perf_counter()
+        f.factorize()
+        t1 = time.perf_counter()
+        f.solve(b1)
+        t2 = time.perf_counter()
+        f.solve(b16)
+        t3 = time.perf_counter()
+        if it >= warmup:
+            fac.append(t1 - t0)
+            s1.append(t2 - t1)
+            s16.append(t3 - t2)
+    return dict(tflops=flops / (sum(fac) / len(fac)) / 1e12, factor_s=sum(fac) / len(fac),
+                solve1_s=sum(s1) / len(s1), solve16_s=sum(s16) / len(s16), cores=cores,
+                step_s=[a + b + c for a, b, c in zip(fac, s1, s16)])
+
+
+def host_symbolic(n, cp, ri):
+    from sympack_b200 import DistSparseMatrix, symPACKMatrix2D, symPACKOptions
+    A = DistSparseMatrix.from_lower_csc(n, cp, ri, np.zeros(len(ri)))
+    M = symPACKMatrix2D()
+    M.Init(symPACKOptions(device=-1))
+    M.SymbolicFactorization(A)
+    _, invp = M.GetOrdering()
+    xl, li = M.GetStructure()
+    sym = dict(xsuper=M.GetSupernodalPartition(), xlindx=xl, lindx=li, supmember=M.GetSupMembership(), invp=invp)
+    return sym, M.info().flops_stat
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    n, cp, ri, v = build_matrix(args.grid)
+    sym, flops = host_symbolic(n, cp, ri)
+    r = cpu_baseline_run(n, cp, ri, v, sym, flops, steps=args.steps, warmup=args.warmup)
+    st = r["step_s"]
+    line = {
+        "impl": "reference", "metric": METRIC, "value": r["tflops"], "unit": "TFLOP/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(st) / len(st),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "n": n, "flops_stat": flops},
+        "solves_per_s": {"nrhs1": 1.0 / r["solve1_s"], "nrhs16": 16.0 / r["solve16_s"]},
+        "cpu_baseline": {"value": r["tflops"], "unit": "TFLOP/s", "cores": r["cores"], "kind": "port",
+                         "sample": "full factorization + nrhs 1 and 16 solves of the workload per step; "
+                                   "CPU restatement of the reference 2D cell algorithm over OpenBLAS"},
+        "e2e": {"value": r["tflops"], "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    from sympack_b200 import DistSparseMatrix, symPACKMatrix2D, symPACKOptions
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+
+    n, cp, ri, v = build_matrix(args.grid)
+    A = DistSparseMatrix.from_lower_csc(n, cp, ri, v)
+    M = symPACKMatrix2D()
+    M.Init(symPACKOptions(device=local))
+    t0 = time.perf_counter()
+    M.SymbolicFactorization(A)
+    symb_s = time.perf_counter() - t0
+    info = M.info()
+    flops = info.flops_stat
+    stream = torch.cuda.current_stream(dev)
+    M.SetStream(stream.cuda_stream)
+
+    rng = np.random.default_rng(0)
+    b1 = rng.standard_normal((n, 1))
+    b16 = np.asfortranarray(rng.standard_normal((n, 16)))
+    d_vals = torch.from_numpy(A.nzvalLocal).to(dev)
+    d_b1 = torch.from_numpy(b1).to(dev)
+    d_b16 = torch.from_numpy(np.ascontiguousarray(b16.T)).to(dev)  # column-major n x 16
+    d_x1 = torch.empty_like(d_b1)
+    d_x16 = torch.empty_like(d_b16)
+
+    def step():
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        ev[0].record(stream)
+        M.DistributeMatrixDevice(d_vals.data_ptr())
+        M.Factorize()
+        ev[1].record(stream)
+        M.SolveDevice(d_b1.data_ptr(), d_x1.data_ptr(), 1, n)
+        ev[2].record(stream)
+        M.SolveDevice(d_b16.data_ptr(), d_x16.data_ptr(), 16, n)
+        ev[3].record(stream)
+        return ev
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        step()
+    barrier()
+    sampler = ClockSampler(local)
+    sampler.start()
+    barrier()
+    evs = [step() for _ in range(args.steps)]
+    barrier()
+    clocks = sampler.stop()
+    fac = [e[0].elapsed_time(e[1]) for e in evs]
+    s1 = [e[1].elapsed_time(e[2]) for e in evs]
+    s16 = [e[2].elapsed_time(e[3]) for e in evs]
+    tot = [e[0].elapsed_time(e[3]) for e in evs]
+    sums = torch.tensor([sum(fac), sum(s1), sum(s16), sum(tot)], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(sums, op=dist.ReduceOp.MAX)
+    fac_ms, s1_ms, s16_ms, tot_ms = (float(x) for x in sums.cpu())
+
+    x1 = d_x1.cpu().numpy()
+    x16 = np.asfortranarray(d_x16.cpu().numpy().T)
+    bwd1 = backward_error(A, x1, b1)
+    bwd16 = backward_error(A, x16, b16)
+
+    # end to end through the host-buffer API (pinned host values / RHS, solution read back)
+    h_vals = torch.from_numpy(A.nzvalLocal).pin_memory()
+    h_b16 = torch.from_numpy(np.ascontiguousarray(b16.T)).pin_memory()
+    h_out = torch.empty_like(h_b16).pin_memory()
+    from sympack_b200 import _native as Nn
+    import ctypes as C
+    lib = Nn.load()
+    dp = lambda t: C.cast(C.c_void_p(t.data_ptr()), Nn._DP)
+
+    def e2e_step():
+        s = torch.cuda.Event(enable_timing=True)
+        e = torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        for rc in (lib.spb_distribute(M._h, dp(h_vals)), lib.spb_factorize(M._h),
+                   lib.spb_solve(M._h, dp(h_b16), 16, n), lib.spb_get_solution(M._h, dp(h_out), 16, n)):
+            if rc != 0:
+                raise RuntimeError(f"e2e call failed ({rc}): {lib.spb_last_error(M._h).decode()}")
+        e.record(stream)
+        return s, e
+
+    for _ in range(max(1, args.warmup)):
+        e2e_step()
+    barrier()
+    e2e_ev = [e2e_step() for _ in range(args.steps)]
+    barrier()
+    e2e_ms = torch.tensor([sum(s.elapsed_time(e) for s, e in e2e_ev)], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(e2e_ms, op=dist.ReduceOp.MAX)
+    e2e_ms = float(e2e_ms.cpu())
+    bwd_e2e = backward_error(A, np.asfortranarray(h_out.numpy().T), b16)
+
+    # one profiled step (eager launches with per-launch CUDA events) for the roofline
+    M.SetProfiling(True)
+    M.DistributeMatrixDevice(d_vals.data_ptr())
+    M.Factorize()
+    M.SolveDevice(d_b16.data_ptr(), d_x16.data_ptr(), 16, n)
+    prof = M.GetProfile()
+    M.SetProfiling(False)
+    peaks, peak_src = measured_peaks()
+    fp64_peak = measured_fp64_peak(torch, dev)
+    factor_kinds = ["factor_small", "potrf_diag", "trsm_rows", "gemm_simt", "gemm_dmma"]
+    top = max(factor_kinds, key=lambda k: prof[k]["ms"])
+    tp = prof[top]
+    roofline = {"kernel": top, "bound": "tensor", "achieved": tp["flops"] / (tp["ms"] * 1e-3) / 1e12,
+                "peak": fp64_peak, "unit": "TFLOP/s", "traffic": None,
+                "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (no FP64 figure in "
+                               + peak_src + ")",
+                "launches": tp["launches"], "share_of_factor": tp["ms"] / sum(prof[k]["ms"] for k in factor_kinds)}
+    roofline["frac"] = roofline["achieved"] / roofline["peak"]
+    sf, sb = prof["solve_forward"], prof["solve_backward"]
+    roofline_solve = {"kernel": "solve_forward+solve_backward", "bound": "hbm", "unit": "GB/s",
+                      "achieved": (sf["bytes"] + sb["bytes"]) / ((sf["ms"] + sb["ms"]) * 1e-3) / 1e9,
+                      "peak": peaks.get("hbm_gbs"), "peak_source": peak_src, "nrhs": 16}
+    roofline_solve["frac"] = roofline_solve["achieved"] / roofline_solve["peak"]
+    kernels = {k: {"ms": round(p["ms"], 4), "launches": p["launches"]} for k, p in prof.items() if p["launches"]}
+
+    cpu = None
+    if world == 1 and rank == 0 and not args.no_cpu_baseline:
+        sym = dict(xsuper=M.GetSupernodalPartition(), xlindx=M.GetStructure()[0], lindx=M.GetStructure()[1],
+                   supmember=M.GetSupMembership(), invp=M.GetOrdering()[1])
+        r = cpu_baseline_run(n, cp, ri, v, sym, flops, steps=1, warmup=0)
+        cpu = {"value": r["tflops"], "unit": "TFLOP/s", "cores": r["cores"], "kind": "port",
+               "sample": "one full factorization of the workload (+ nrhs 1 and 16 solves, timed separately); "
+                         "CPU restatement of the reference 2D cell algorithm over OpenBLAS",
+               "factor_s": r["factor_s"], "solve1_s": r["solve1_s"], "solve16_s": r["solve16_s"]}
+
+    K = args.steps
+    launches_per_step = 1 + info.factor_launches + 4 + 4
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": world * flops * K / (fac_ms * 1e-3) / 1e12, "unit": "TFLOP/s",
+            "n_gpus": world, "steps": K, "warmup": args.warmup, "ms_per_step": tot_ms / K,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "n": n, "nnz_L": info.nnz_l, "flops_stat": flops,
+                       "flops_exec": info.flops_exec, "nsuper": info.nsuper, "etree_levels": info.nlevels,
+                       "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+                       "l2": "no flush: factor arena %.2f GB >> 126 MB L2" % (info.arena_bytes / 1e9),
+                       "symbolic_s": symb_s},
+            "factor_ms": fac_ms / K,
+            "solves_per_s": {"nrhs1": world * K / (s1_ms * 1e-3), "nrhs16": world * 16 * K / (s16_ms * 1e-3)},
+            "solve_ms": {"nrhs1": s1_ms / K, "nrhs16": s16_ms / K},
+            "backward_error": {"nrhs1": bwd1, "nrhs16": bwd16, "e2e_nrhs16": bwd_e2e},
+            "latency_ms": {"p50": float(np.percentile(tot, 50)), "p99": float(np.percentile(tot, 99))},
+            "roofline": roofline, "roofline_solve": roofline_solve, "kernels_profiled_step": kernels,
+            "cpu_baseline": cpu,
+            "e2e": {"value": world * flops * K / (e2e_ms * 1e-3) / 1e12, "unit": "TFLOP/s",
+                    "h2d_bytes_per_step": int(A.nnz * 8 + n * 16 * 8), "d2h_bytes_per_step": int(n * 16 * 8),
+                    "ms_per_step": e2e_ms / K,
+                    "note": "DistributeMatrix from pinned host values + Factorize + Solve(16 host RHS) + GetSolution"},
+            "clocks": clocks,
+            "gpu_launches": launches_per_step * K,
+        }
+        print(json.dumps(line), flush=True)
+    M.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

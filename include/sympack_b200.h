@@ -90,7 +90,7 @@ typedef struct spb_info {
   int32_t ncells;          /* reference 2D cells (K, I) */
   int32_t nblocks;         /* reference contiguous-row blocks */
   int32_t ir_iterations;   /* refinement steps of the last solve */
-  int32_t pad;
+  int32_t factor_launches; /* kernels in the factorization graph */
   double backward_error;   /* componentwise-free backward error of the last solve, if computed */
 } spb_info;
 
@@ -130,6 +130,45 @@ int spb_get_cells(spb_handle* h, int32_t* cell_I, int32_t* cell_K, int32_t* cell
 int spb_get_factor(spb_handle* h, double* out);
 /* Status of the last factorization: code, supernode (0-based), column (0-based, permuted). */
 int spb_get_status(spb_handle* h, int32_t* code, int32_t* supernode, int32_t* column);
+
+/* Bound on every device-side wait of the persistent solve kernels, in polls
+ * about 128 ns apart (default 2^24, a couple of seconds).  A wait that runs out
+ * records a timeout; the call returns SPB_ERR_TIMEOUT and the context stays usable. */
+int spb_set_wait_limit(spb_handle* h, int64_t polls);
+/* Test hook for failure detection: make the forward solve expect one more
+ * incoming update for `supernode` than any task delivers (its wait then runs
+ * out); -1 restores the true counts. */
+int spb_debug_stall(spb_handle* h, int32_t supernode);
+/* Reset the device status word (after a reported failure). */
+int spb_clear_status(spb_handle* h);
+
+/* Run every later call of this handle on the caller's CUDA stream (a
+ * cudaStream_t passed as void*; NULL returns to the handle's own stream).  Calls
+ * still return only when their work is complete. */
+int spb_set_stream(spb_handle* h, void* stream);
+
+/* Profiling: with profiling on, spb_factorize launches its steps eagerly with a
+ * CUDA event pair around each launch, and spb_solve / spb_solve_device time each
+ * sweep; spb_get_profile returns per kernel kind the device milliseconds of the
+ * last profiled call, the launches, and the algorithmic flops (factor kinds) or
+ * bytes (solve kinds: every panel element read once per sweep). */
+#define SPB_KIND_ASSEMBLE 0
+#define SPB_KIND_FACTOR_SMALL 1
+#define SPB_KIND_POTRF_DIAG 2
+#define SPB_KIND_TRSM_ROWS 3
+#define SPB_KIND_GEMM_SIMT 4
+#define SPB_KIND_GEMM_DMMA 5
+#define SPB_KIND_SOLVE_FORWARD 6
+#define SPB_KIND_SOLVE_BACKWARD 7
+#define SPB_KIND_COUNT 8
+typedef struct spb_profile {
+  double ms[SPB_KIND_COUNT];
+  double flops[SPB_KIND_COUNT];
+  double bytes[SPB_KIND_COUNT];
+  int32_t launches[SPB_KIND_COUNT];
+} spb_profile;
+int spb_set_profiling(spb_handle* h, int on);
+int spb_get_profile(spb_handle* h, spb_profile* out);
 
 /* Rutherford-Boeing input boundary, replacing ReadMatrix / ReadHB_PARA
  * (include/sympack/utility.hpp:1274-1481, 1695-1727) for one rank.  spb_rb_info

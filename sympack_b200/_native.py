@@ -62,8 +62,21 @@ class spb_info(C.Structure):
         ("ncells", C.c_int32),
         ("nblocks", C.c_int32),
         ("ir_iterations", C.c_int32),
-        ("pad", C.c_int32),
+        ("factor_launches", C.c_int32),
         ("backward_error", C.c_double),
+    ]
+
+
+KIND_NAMES = ["assemble", "factor_small", "potrf_diag", "trsm_rows", "gemm_simt", "gemm_dmma",
+              "solve_forward", "solve_backward"]
+
+
+class spb_profile(C.Structure):
+    _fields_ = [
+        ("ms", C.c_double * 8),
+        ("flops", C.c_double * 8),
+        ("bytes", C.c_double * 8),
+        ("launches", C.c_int32 * 8),
     ]
 
 
@@ -94,6 +107,12 @@ SIGNATURES = [
     ("spb_get_cells", C.c_int, [_P, _I32P, _I32P, _I32P, _I32P, _I32P, _I32P, _I32P]),
     ("spb_get_factor", C.c_int, [_P, _DP]),
     ("spb_get_status", C.c_int, [_P, _I32P, _I32P, _I32P]),
+    ("spb_set_wait_limit", C.c_int, [_P, C.c_int64]),
+    ("spb_debug_stall", C.c_int, [_P, C.c_int32]),
+    ("spb_clear_status", C.c_int, [_P]),
+    ("spb_set_stream", C.c_int, [_P, _P]),
+    ("spb_set_profiling", C.c_int, [_P, C.c_int]),
+    ("spb_get_profile", C.c_int, [_P, C.POINTER(spb_profile)]),
     ("spb_rb_info", C.c_int, [C.c_char_p, _I32P, _I64P]),
     ("spb_rb_read", C.c_int, [C.c_char_p, _I64P, _I32P, _DP]),
     ("spb_rb_write", C.c_int, [C.c_char_p, C.c_char_p, C.c_int32, _I64P, _I32P, _DP]),

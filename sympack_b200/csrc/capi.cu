@@ -23,7 +23,8 @@ using spb::dev::Status;
 struct spb_handle {
   spb_options opt{};
   int device = 0;
-  cudaStream_t stream = nullptr;
+  cudaStream_t stream = nullptr;      // stream every call runs on
+  cudaStream_t own_stream = nullptr;  // created by spb_create
   std::string err;
   bool have_symbolic = false, have_values = false, factored = false, have_solution = false;
   spb::Symbolic sym;
@@ -46,6 +47,11 @@ struct spb_handle {
   spb::TileItem* dtiles = nullptr;
   int32_t* dinvp0 = nullptr;
   int32_t* dlevel_sn = nullptr;
+  spb::SolveTask* dfwd = nullptr;
+  spb::SolveTask* dbwd = nullptr;
+  int32_t* dexpected = nullptr;
+  int32_t* dsparent = nullptr;
+  int32_t* dsync = nullptr;  // [fwd counter, bwd counter, arrived[ns], fwd blkdone[ns], bwd blkdone[ns]]
   Status* dstatus = nullptr;
   double* dX = nullptr;
   double* dB = nullptr;
@@ -54,6 +60,12 @@ struct spb_handle {
   int64_t device_bytes = 0;
   cudaGraphExec_t fgraph = nullptr;
   std::vector<void*> allocs;
+  // profiling: per-launch event pairs, per-kind totals of the last profiled call
+  long long wait_limit = 1LL << 24;  // ~2 s of polling per device wait
+  int stall_supernode = -1;          // test hook: extra expected arrival nobody delivers
+  bool profiling = false;
+  spb_profile prof{};
+  std::vector<cudaEvent_t> events;
 };
 
 namespace {
@@ -134,6 +146,69 @@ void enqueue_factor(spb_handle* h) {
 
 int check_handle(spb_handle* h) { return h ? SPB_OK : SPB_ERR_INVALID; }
 
+cudaError_t ensure_events(spb_handle* h, size_t count) {
+  while (h->events.size() < count) {
+    cudaEvent_t e;
+    cudaError_t err = cudaEventCreate(&e);
+    if (err != cudaSuccess) return err;
+    h->events.push_back(e);
+  }
+  return cudaSuccess;
+}
+
+int step_kind(const spb::Step& st) {
+  switch (st.kind) {
+    case spb::StepKind::FactorSmall: return SPB_KIND_FACTOR_SMALL;
+    case spb::StepKind::PotrfDiag: return SPB_KIND_POTRF_DIAG;
+    case spb::StepKind::TrsmRows: return SPB_KIND_TRSM_ROWS;
+    default: return st.tile == 128 ? SPB_KIND_GEMM_DMMA : SPB_KIND_GEMM_SIMT;
+  }
+}
+
+void clear_kinds(spb_handle* h, int first, int last) {
+  for (int k = first; k <= last; ++k) {
+    h->prof.ms[k] = h->prof.flops[k] = h->prof.bytes[k] = 0.0;
+    h->prof.launches[k] = 0;
+  }
+}
+
+// Eager factorization with one event pair per launch (profiling mode).
+int factor_profiled(spb_handle* h) {
+  const spb::Plan& P = h->plan;
+  SPB_CK(h, ensure_events(h, 2 * P.steps.size()));
+  spb::dev::FactorArgs a = factor_args(h);
+  for (size_t k = 0; k < P.steps.size(); ++k) {
+    const spb::Step& st = P.steps[k];
+    SPB_CK(h, cudaEventRecord(h->events[2 * k], h->stream));
+    switch (st.kind) {
+      case spb::StepKind::FactorSmall:
+        spb::dev::launch_factor_small(h->stream, a, h->dsmall + st.begin, st.count, st.arg);
+        break;
+      case spb::StepKind::PotrfDiag:
+        spb::dev::launch_potrf_diag(h->stream, a, h->dpanel + st.begin, st.count);
+        break;
+      case spb::StepKind::TrsmRows:
+        spb::dev::launch_trsm_rows(h->stream, a, h->dpanel + st.begin, st.count);
+        break;
+      case spb::StepKind::Gemm:
+        spb::dev::launch_gemm(h->stream, a, h->dtiles + st.begin, st.count, st.tile);
+        break;
+    }
+    SPB_CK(h, cudaEventRecord(h->events[2 * k + 1], h->stream));
+  }
+  SPB_CK(h, cudaStreamSynchronize(h->stream));
+  clear_kinds(h, SPB_KIND_FACTOR_SMALL, SPB_KIND_GEMM_DMMA);
+  for (size_t k = 0; k < P.steps.size(); ++k) {
+    float ms = 0.f;
+    SPB_CK(h, cudaEventElapsedTime(&ms, h->events[2 * k], h->events[2 * k + 1]));
+    int kind = step_kind(P.steps[k]);
+    h->prof.ms[kind] += ms;
+    h->prof.flops[kind] += P.step_flops[k];
+    h->prof.launches[kind] += 1;
+  }
+  return SPB_OK;
+}
+
 int ensure_rhs_capacity(spb_handle* h, int nrhs) {
   int64_t need = (int64_t)h->sym.n * nrhs;
   if (need <= h->x_cap) return SPB_OK;
@@ -153,22 +228,78 @@ int ensure_rhs_capacity(spb_handle* h, int nrhs) {
   return SPB_OK;
 }
 
-// Forward and backward sweeps over the levels on permuted X (n x nrhs, ld n).
+// Forward and backward persistent sweeps on the permuted X (n x nrhs, ld n),
+// 64 right-hand sides per pass.
 void enqueue_solve(spb_handle* h, int nrhs) {
   const spb::Plan& P = h->plan;
+  const int ns = P.nsuper;
   for (int c0 = 0; c0 < nrhs; c0 += 64) {
-    spb::dev::SolveArgs a;
+    cudaMemsetAsync(h->dsync, 0, sizeof(int32_t) * (2 + 3 * (size_t)ns), h->stream);
+    spb::dev::PSolveArgs a;
     a.L = h->dL;
     a.meta = h->dmeta;
     a.rows = h->drows;
+    a.supmember = h->dsupm;
+    a.sparent = h->dsparent;
     a.X = h->dX + (int64_t)c0 * h->sym.n;
     a.ldx = h->sym.n;
     a.nrhs = std::min(64, nrhs - c0);
-    for (int l = 0; l < P.nlevels; ++l)
-      spb::dev::launch_solve_forward(h->stream, a, h->dlevel_sn + h->level_off[l], h->level_off[l + 1] - h->level_off[l]);
-    for (int l = P.nlevels - 1; l >= 0; --l)
-      spb::dev::launch_solve_backward(h->stream, a, h->dlevel_sn + h->level_off[l], h->level_off[l + 1] - h->level_off[l]);
+    a.expected = h->dexpected;
+    a.arrived = h->dsync + 2;
+    a.status = h->dstatus;
+    const size_t e0 = 4 * (size_t)(c0 / 64);
+    a.tasks = h->dfwd;
+    a.ntasks = (int)P.fwd_tasks.size();
+    a.counter = h->dsync;
+    a.blkdone = h->dsync + 2 + ns;
+    if (h->profiling) cudaEventRecord(h->events[e0], h->stream);
+    spb::dev::launch_solve_persistent(h->stream, a, true);
+    if (h->profiling) cudaEventRecord(h->events[e0 + 1], h->stream);
+    a.tasks = h->dbwd;
+    a.ntasks = (int)P.bwd_tasks.size();
+    a.counter = h->dsync + 1;
+    a.blkdone = h->dsync + 2 + 2 * ns;
+    if (h->profiling) cudaEventRecord(h->events[e0 + 2], h->stream);
+    spb::dev::launch_solve_persistent(h->stream, a, false);
+    if (h->profiling) cudaEventRecord(h->events[e0 + 3], h->stream);
   }
+}
+
+// Per-sweep device times of the last profiled solve.
+int collect_solve_profile(spb_handle* h, int nrhs) {
+  if (!h->profiling) return SPB_OK;
+  SPB_CK(h, cudaStreamSynchronize(h->stream));
+  clear_kinds(h, SPB_KIND_SOLVE_FORWARD, SPB_KIND_SOLVE_BACKWARD);
+  for (int c0 = 0, i = 0; c0 < nrhs; c0 += 64, ++i) {
+    float f = 0.f, b = 0.f;
+    SPB_CK(h, cudaEventElapsedTime(&f, h->events[4 * i], h->events[4 * i + 1]));
+    SPB_CK(h, cudaEventElapsedTime(&b, h->events[4 * i + 2], h->events[4 * i + 3]));
+    const double rhs_bytes = 16.0 * h->sym.n * std::min(64, nrhs - c0);  // X read and written once
+    h->prof.ms[SPB_KIND_SOLVE_FORWARD] += f;
+    h->prof.ms[SPB_KIND_SOLVE_BACKWARD] += b;
+    h->prof.bytes[SPB_KIND_SOLVE_FORWARD] += h->plan.solve_sweep_bytes + rhs_bytes;
+    h->prof.bytes[SPB_KIND_SOLVE_BACKWARD] += h->plan.solve_sweep_bytes + rhs_bytes;
+    h->prof.launches[SPB_KIND_SOLVE_FORWARD] += 1;
+    h->prof.launches[SPB_KIND_SOLVE_BACKWARD] += 1;
+  }
+  return SPB_OK;
+}
+
+// Status word after a solve: device waits are bounded, report their expiry.
+int check_solve_status(spb_handle* h) {
+  Status st;
+  SPB_CK(h, cudaMemcpyAsync(&st, h->dstatus, sizeof(st), cudaMemcpyDeviceToHost, h->stream));
+  SPB_CK(h, cudaStreamSynchronize(h->stream));
+  if (st.code == 3) {
+    // the context is intact: clear the word so the next solve can run
+    SPB_CK(h, cudaMemsetAsync(h->dstatus, 0, sizeof(Status), h->stream));
+    SPB_CK(h, cudaStreamSynchronize(h->stream));
+    char msg[96];
+    snprintf(msg, sizeof msg, "solve: a device wait expired (supernode %d)", st.supernode + 1);
+    return fail(h, SPB_ERR_TIMEOUT, msg);
+  }
+  if (st.code != 0 && st.code != 1) return fail(h, SPB_ERR_STRUCTURE, "solve: device status error");
+  return SPB_OK;
 }
 
 }  // namespace
@@ -211,7 +342,8 @@ int spb_create(const spb_options* opt, spb_handle** out) {
     return SPB_OK;
   }
   cudaError_t e = cudaSetDevice(h->device);
-  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking);
+  h->stream = h->own_stream;
   if (e != cudaSuccess) {
     cudaGetLastError();
     delete h;
@@ -231,7 +363,8 @@ void spb_destroy(spb_handle* h) {
   cudaSetDevice(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
   release_device(h);
-  if (h->stream) cudaStreamDestroy(h->stream);
+  for (cudaEvent_t e : h->events) cudaEventDestroy(e);
+  if (h->own_stream) cudaStreamDestroy(h->own_stream);
   delete h;
 }
 
@@ -303,6 +436,11 @@ int spb_symbolic(spb_handle* h, int32_t n, const int64_t* colptr, const int32_t*
   SPB_CK(h, dalloc(h, &h->dtiles, P.tile_items.size()));
   SPB_CK(h, dalloc(h, &h->dinvp0, invp0.size()));
   SPB_CK(h, dalloc(h, &h->dlevel_sn, lsn.size()));
+  SPB_CK(h, dalloc(h, &h->dfwd, P.fwd_tasks.size()));
+  SPB_CK(h, dalloc(h, &h->dbwd, P.bwd_tasks.size()));
+  SPB_CK(h, dalloc(h, &h->dexpected, P.fwd_pending.size()));
+  SPB_CK(h, dalloc(h, &h->dsparent, P.sparent.size()));
+  SPB_CK(h, dalloc(h, &h->dsync, 2 + 3 * (size_t)P.nsuper));
   SPB_CK(h, dalloc(h, &h->dstatus, 1));
   auto up = [&](void* d, const void* s, size_t bytes) {
     return bytes ? cudaMemcpyAsync(d, s, bytes, cudaMemcpyHostToDevice, h->stream) : cudaSuccess;
@@ -316,6 +454,10 @@ int spb_symbolic(spb_handle* h, int32_t n, const int64_t* colptr, const int32_t*
   SPB_CK(h, up(h->dtiles, P.tile_items.data(), P.tile_items.size() * sizeof(spb::TileItem)));
   SPB_CK(h, up(h->dinvp0, invp0.data(), invp0.size() * 4));
   SPB_CK(h, up(h->dlevel_sn, lsn.data(), lsn.size() * 4));
+  SPB_CK(h, up(h->dfwd, P.fwd_tasks.data(), P.fwd_tasks.size() * sizeof(spb::SolveTask)));
+  SPB_CK(h, up(h->dbwd, P.bwd_tasks.data(), P.bwd_tasks.size() * sizeof(spb::SolveTask)));
+  SPB_CK(h, up(h->dexpected, P.fwd_pending.data(), P.fwd_pending.size() * 4));
+  SPB_CK(h, up(h->dsparent, P.sparent.data(), P.sparent.size() * 4));
   SPB_CK(h, cudaMemsetAsync(h->dstatus, 0, sizeof(Status), h->stream));
   SPB_CK(h, cudaStreamSynchronize(h->stream));
   h->have_symbolic = true;
@@ -326,9 +468,22 @@ static int distribute_common(spb_handle* h) {
   const spb::Plan& P = h->plan;
   SPB_CK(h, cudaMemsetAsync(h->dL, 0, P.arena_elems * sizeof(double), h->stream));
   SPB_CK(h, cudaMemsetAsync(h->dstatus, 0, sizeof(Status), h->stream));
+  if (h->profiling) {
+    SPB_CK(h, ensure_events(h, 2));
+    SPB_CK(h, cudaEventRecord(h->events[0], h->stream));
+  }
   spb::dev::launch_assemble(h->stream, h->dL, h->damap, h->dA, h->nnz_a);
   SPB_CK(h, cudaGetLastError());
+  if (h->profiling) SPB_CK(h, cudaEventRecord(h->events[1], h->stream));
   SPB_CK(h, cudaStreamSynchronize(h->stream));
+  if (h->profiling) {
+    float ms = 0.f;
+    SPB_CK(h, cudaEventElapsedTime(&ms, h->events[0], h->events[1]));
+    clear_kinds(h, SPB_KIND_ASSEMBLE, SPB_KIND_ASSEMBLE);
+    h->prof.ms[SPB_KIND_ASSEMBLE] = ms;
+    h->prof.bytes[SPB_KIND_ASSEMBLE] = (double)h->nnz_a * 24.0;  // value + index read, value written
+    h->prof.launches[SPB_KIND_ASSEMBLE] = 1;
+  }
   h->have_values = true;
   h->factored = h->have_solution = false;
   return SPB_OK;
@@ -360,7 +515,10 @@ int spb_factorize(spb_handle* h) {
   if (!h->have_values) return fail(h, SPB_ERR_STATE, "factorize: call spb_distribute first");
   if (h->factored) return fail(h, SPB_ERR_STATE, "factorize: values already factored; distribute again");
   SPB_CK(h, cudaSetDevice(h->device));
-  if (!h->fgraph && !h->plan.steps.empty()) {
+  if (h->profiling) {
+    int rc = factor_profiled(h);
+    if (rc) return rc;
+  } else if (!h->fgraph && !h->plan.steps.empty()) {
     cudaGraph_t g;
     SPB_CK(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
     enqueue_factor(h);
@@ -370,7 +528,7 @@ int spb_factorize(spb_handle* h) {
     cudaGraphDestroy(g);
     if (e != cudaSuccess) return cuda_fail(h, e, "factorize: graph instantiate");
   }
-  if (h->fgraph) SPB_CK(h, cudaGraphLaunch(h->fgraph, h->stream));
+  if (h->fgraph && !h->profiling) SPB_CK(h, cudaGraphLaunch(h->fgraph, h->stream));
   Status st;
   SPB_CK(h, cudaMemcpyAsync(&st, h->dstatus, sizeof(st), cudaMemcpyDeviceToHost, h->stream));
   SPB_CK(h, cudaStreamSynchronize(h->stream));
@@ -394,12 +552,14 @@ int spb_solve_device(spb_handle* h, const double* d_rhs, double* d_x, int32_t nr
   SPB_CK(h, cudaSetDevice(h->device));
   int rc = ensure_rhs_capacity(h, nrhs);
   if (rc) return rc;
+  if (h->profiling) SPB_CK(h, ensure_events(h, 4 * (size_t)((nrhs + 63) / 64)));
   spb::dev::launch_permute_in(h->stream, h->dX, n, d_rhs, ld, h->dinvp0, n, nrhs);
   enqueue_solve(h, nrhs);
+  rc = collect_solve_profile(h, nrhs);
+  if (rc) return rc;
   spb::dev::launch_permute_out(h->stream, d_x, ld, h->dX, n, h->dinvp0, n, nrhs);
   SPB_CK(h, cudaGetLastError());
-  SPB_CK(h, cudaStreamSynchronize(h->stream));
-  return SPB_OK;
+  return check_solve_status(h);
 }
 
 int spb_solve(spb_handle* h, const double* rhs, int32_t nrhs, int64_t ldb) {
@@ -413,10 +573,14 @@ int spb_solve(spb_handle* h, const double* rhs, int32_t nrhs, int64_t ldb) {
   if (rc) return rc;
   SPB_CK(h, cudaMemcpy2DAsync(h->dB, (size_t)n * 8, rhs, (size_t)ldb * 8, (size_t)n * 8, nrhs, cudaMemcpyHostToDevice,
                               h->stream));
+  if (h->profiling) SPB_CK(h, ensure_events(h, 4 * (size_t)((nrhs + 63) / 64)));
   spb::dev::launch_permute_in(h->stream, h->dX, n, h->dB, n, h->dinvp0, n, nrhs);
   enqueue_solve(h, nrhs);
+  rc = collect_solve_profile(h, nrhs);
+  if (rc) return rc;
   SPB_CK(h, cudaGetLastError());
-  SPB_CK(h, cudaStreamSynchronize(h->stream));
+  rc = check_solve_status(h);
+  if (rc) return rc;
   h->have_solution = true;
   h->x_nrhs = nrhs;
   return SPB_OK;
@@ -460,6 +624,7 @@ int spb_get_info(spb_handle* h, spb_info* info) {
   info->flops_exec = P.exec_flops;
   info->ncells = (int32_t)h->cells.cells.size();
   info->nblocks = (int32_t)h->cells.block_first_row.size();
+  info->factor_launches = (int32_t)P.steps.size();
   return SPB_OK;
 }
 
@@ -544,6 +709,53 @@ int spb_get_factor(spb_handle* h, double* out) {
       for (int r = 0; r < m.h; ++r) out[pos + r + (int64_t)c * m.h] = (r < c) ? 0.0 : arena[m.off + r + (int64_t)c * m.ld];
     pos += (int64_t)m.h * m.w;
   }
+  return SPB_OK;
+}
+
+int spb_set_wait_limit(spb_handle* h, int64_t polls) {
+  if (check_handle(h) || polls <= 0) return SPB_ERR_INVALID;
+  h->wait_limit = polls;
+  return SPB_OK;
+}
+
+int spb_debug_stall(spb_handle* h, int32_t supernode) {
+  if (check_handle(h)) return SPB_ERR_INVALID;
+  if (!h->have_symbolic || h->device < 0) return fail(h, SPB_ERR_STATE, "debug_stall: needs a device handle");
+  const int ns = h->plan.nsuper;
+  if (supernode >= ns) return fail(h, SPB_ERR_INVALID, "debug_stall: supernode out of range");
+  std::vector<int32_t> e = h->plan.fwd_pending;
+  if (supernode >= 0) e[supernode] += 1;
+  SPB_CK(h, cudaMemcpyAsync(h->dexpected, e.data(), e.size() * 4, cudaMemcpyHostToDevice, h->stream));
+  SPB_CK(h, cudaStreamSynchronize(h->stream));
+  h->stall_supernode = supernode;
+  return SPB_OK;
+}
+
+int spb_clear_status(spb_handle* h) {
+  if (check_handle(h)) return SPB_ERR_INVALID;
+  if (!h->have_symbolic || h->device < 0) return fail(h, SPB_ERR_STATE, "clear_status: needs a device handle");
+  SPB_CK(h, cudaMemsetAsync(h->dstatus, 0, sizeof(Status), h->stream));
+  SPB_CK(h, cudaStreamSynchronize(h->stream));
+  return SPB_OK;
+}
+
+int spb_set_stream(spb_handle* h, void* stream) {
+  if (check_handle(h)) return SPB_ERR_INVALID;
+  if (h->device < 0) return fail(h, SPB_ERR_STATE, "host-only handle (device < 0) has no stream");
+  SPB_CK(h, cudaStreamSynchronize(h->stream));
+  h->stream = stream ? (cudaStream_t)stream : h->own_stream;
+  return SPB_OK;
+}
+
+int spb_set_profiling(spb_handle* h, int on) {
+  if (check_handle(h)) return SPB_ERR_INVALID;
+  h->profiling = on != 0;
+  return SPB_OK;
+}
+
+int spb_get_profile(spb_handle* h, spb_profile* out) {
+  if (check_handle(h) || !out) return SPB_ERR_INVALID;
+  *out = h->prof;
   return SPB_OK;
 }
 

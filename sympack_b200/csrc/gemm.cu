@@ -1,0 +1,275 @@
+// Schur-complement products of the supernodal factorization (sm_100a):
+//   C = A * B^T over panel columns [k0, k0 + kn) of one supernode, followed by
+//   either an in-panel subtraction (mode 0) or a scatter-subtraction into the
+//   ancestor panels that own the rows and columns of C (mode 1).  This is the
+//   blockCell_t::update of symPACKMatrix2D.hpp:1180-1469 (GEMM into a buffer,
+//   then the src_to_tgt_offset / colindx scatter of 2D.hpp:1395-1466), fused so
+//   that C never leaves the SM.
+//
+// Two tile engines share one epilogue:
+//   k_gemm_dmma  128 x 128 tiles on the FP64 tensor pipe (mma.sync m16n8k4 .f64),
+//                3-stage cp.async pipeline, 8 warps of 64 x 32
+//   k_gemm_simt   64 x 64 tiles with FP64 FMA, for narrow updates
+// The epilogue stages C in shared memory and walks it column by column, so
+// consecutive threads touch consecutive target rows (coalesced atomics).
+#include <climits>
+
+#include "kernels.cuh"
+
+namespace spb {
+namespace dev {
+
+namespace {
+
+__device__ __forceinline__ void report_status(Status* st, int code, int s, int col) {
+  if (atomicCAS(&st->code, 0, code) == 0) {
+    st->supernode = s;
+    st->column = col;
+  }
+}
+
+__device__ __forceinline__ int find_row(const int32_t* __restrict__ rl, int h, int row) {
+  int lo = 0, hi = h;
+  while (lo < hi) {
+    int mid = (lo + hi) >> 1;
+    if (rl[mid] < row) lo = mid + 1;
+    else hi = mid;
+  }
+  return (lo < h && rl[lo] == row) ? lo : -1;
+}
+
+// Apply a BM x BN tile of C held in shared memory (column-major, leading dimension ldc).
+template <int BM, int BN, int NT>
+__device__ void tile_epilogue(const FactorArgs& a, const TileItem& it, const SnMeta& m, const double* Cs,
+                              int ldc, int* Rr, int* Rc, int* Tc, int* Pos) {
+  const int tid = threadIdx.x;
+  double* g = a.L + m.off;
+  if (it.mode == 0) {
+    const int64_t ld = m.ld;
+    for (int idx = tid; idx < BM * BN; idx += NT) {
+      int c = idx / BM, r = idx - c * BM;
+      if (r < it.mrows && c < it.ncols) {
+        int gr = it.a_row0 + r, gc = it.b_row0 + c;
+        if (gr >= gc) g[gr + (int64_t)gc * ld] -= Cs[r + c * ldc];
+      }
+    }
+    return;
+  }
+  const int32_t* rl = a.rows + m.lidx;
+  for (int i = tid; i < BM; i += NT) Rr[i] = i < it.mrows ? rl[it.a_row0 + i] : INT_MAX;
+  for (int i = tid; i < BN; i += NT) {
+    int rc = i < it.ncols ? rl[it.b_row0 + i] : INT_MAX;
+    Rc[i] = rc;
+    Tc[i] = i < it.ncols ? a.supmember[rc] : -1;
+  }
+  __syncthreads();
+  int c = 0;
+  while (c < it.ncols) {
+    const int t = Tc[c];
+    int ce = c + 1;
+    while (ce < it.ncols && Tc[ce] == t) ++ce;
+    const SnMeta mt = a.meta[t];
+    for (int i = tid; i < BM; i += NT) {
+      int pos = -1;
+      if (i < it.mrows && Rr[i] >= Rc[c]) {
+        pos = find_row(a.rows + mt.lidx, mt.h, Rr[i]);
+        if (pos < 0) report_status(a.status, 2, it.s, Rr[i]);
+      }
+      Pos[i] = pos;
+    }
+    __syncthreads();
+    double* gt = a.L + mt.off;
+    const int ncol = ce - c;
+    for (int idx = tid; idx < ncol * BM; idx += NT) {
+      int cc = c + idx / BM, r = idx % BM;
+      int p = Pos[r];
+      if (p >= 0 && Rr[r] >= Rc[cc]) atomicAdd(gt + (int64_t)(Rc[cc] - mt.fc) * mt.ld + p, -Cs[r + cc * ldc]);
+    }
+    __syncthreads();
+    c = ce;
+  }
+}
+
+}  // namespace
+
+namespace {
+
+// ---- 128 x 128 FP64 tensor-core tile ------------------------------------------
+constexpr int kDM = 128, kDN = 128, kDK = 16, kDStages = 3, kDLds = 132, kDLdc = 130, kDThreads = 256;
+constexpr size_t kDPipeBytes = (size_t)kDStages * 2 * kDK * kDLds * sizeof(double);
+constexpr size_t kDCBytes = (size_t)kDN * kDLdc * sizeof(double);
+constexpr size_t kDMainBytes = kDPipeBytes > kDCBytes ? kDPipeBytes : kDCBytes;
+constexpr size_t kDSmemBytes = kDMainBytes + 4 * 128 * sizeof(int);
+
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem, int src_bytes) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(src_bytes));
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+// D = A(16x4, row) * B(4x8, col) + D, FP64.  Fragment ownership (lane = 4*g + t):
+//   a0 = A[g][t], a1 = A[g+8][t], b0 = B[t][g],
+//   d0 = D[g][2t], d1 = D[g][2t+1], d2 = D[g+8][2t], d3 = D[g+8][2t+1].
+__device__ __forceinline__ void dmma_16x8x4(double* d, double a0, double a1, double b0) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};\n"
+      : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+      : "d"(a0), "d"(a1), "d"(b0));
+}
+
+__global__ void __launch_bounds__(kDThreads, 1) k_gemm_dmma(FactorArgs a, const TileItem* __restrict__ items) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double* pipe = reinterpret_cast<double*>(smem_raw);
+  double* Cs = reinterpret_cast<double*>(smem_raw);  // reused once the main loop is done
+  int* ints = reinterpret_cast<int*>(smem_raw + kDMainBytes);
+  const TileItem it = items[blockIdx.x];
+  const SnMeta m = a.meta[it.s];
+  const double* g = a.L + m.off;
+  const int64_t ld = m.ld;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wm = warp & 1, wn = warp >> 1;  // 2 x 4 warps, 64 x 32 each
+  const int gq = lane >> 2, tq = lane & 3;
+
+  auto load_stage = [&](int stage, int kk) {
+    double* As = pipe + (size_t)stage * 2 * kDK * kDLds;
+    double* Bs = As + kDK * kDLds;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      int e = tid + q * kDThreads;  // 0 .. 2047: (column, row) of a 16 x 128 operand slab
+      int col = e >> 7, r = e & 127;
+      int k = kk + col;
+      bool kok = k < it.kn;
+      int64_t coff = (int64_t)(it.k0 + (kok ? k : 0)) * ld;
+      bool aok = kok && r < it.mrows;
+      bool bok = kok && r < it.ncols;
+      cp_async8(As + col * kDLds + r, aok ? g + it.a_row0 + r + coff : g, aok ? 8 : 0);
+      cp_async8(Bs + col * kDLds + r, bok ? g + it.b_row0 + r + coff : g, bok ? 8 : 0);
+    }
+  };
+
+  double acc[4][4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc[i][j][q] = 0.0;
+
+  const int nk = (it.kn + kDK - 1) / kDK;
+#pragma unroll
+  for (int s = 0; s < kDStages - 1; ++s) {
+    if (s < nk) load_stage(s, s * kDK);
+    cp_commit();
+  }
+  for (int kt = 0; kt < nk; ++kt) {
+    cp_wait<kDStages - 2>();
+    __syncthreads();
+    const int nxt = kt + kDStages - 1;
+    if (nxt < nk) load_stage(nxt % kDStages, nxt * kDK);
+    cp_commit();
+    const double* As = pipe + (size_t)(kt % kDStages) * 2 * kDK * kDLds;
+    const double* Bs = As + kDK * kDLds;
+#pragma unroll
+    for (int ks = 0; ks < kDK; ks += 4) {
+      double af[4][2], bf[4];
+      const double* Ak = As + (ks + tq) * kDLds + wm * 64 + gq;
+      const double* Bk = Bs + (ks + tq) * kDLds + wn * 32 + gq;
+#pragma unroll
+      for (int mi = 0; mi < 4; ++mi) {
+        af[mi][0] = Ak[mi * 16];
+        af[mi][1] = Ak[mi * 16 + 8];
+      }
+#pragma unroll
+      for (int ni = 0; ni < 4; ++ni) bf[ni] = Bk[ni * 8];
+#pragma unroll
+      for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni) dmma_16x8x4(acc[mi][ni], af[mi][0], af[mi][1], bf[ni]);
+    }
+  }
+  cp_wait<0>();
+  __syncthreads();
+#pragma unroll
+  for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+    for (int ni = 0; ni < 4; ++ni) {
+      int r0 = wm * 64 + mi * 16 + gq, c0 = wn * 32 + ni * 8 + 2 * tq;
+      Cs[r0 + c0 * kDLdc] = acc[mi][ni][0];
+      Cs[r0 + (c0 + 1) * kDLdc] = acc[mi][ni][1];
+      Cs[r0 + 8 + c0 * kDLdc] = acc[mi][ni][2];
+      Cs[r0 + 8 + (c0 + 1) * kDLdc] = acc[mi][ni][3];
+    }
+  __syncthreads();
+  tile_epilogue<kDM, kDN, kDThreads>(a, it, m, Cs, kDLdc, ints, ints + 128, ints + 256, ints + 384);
+}
+
+// ---- 64 x 64 FP64 FMA tile --------------------------------------------------------
+constexpr int kSLdc = 65;
+constexpr size_t kSCBytes = (size_t)64 * kSLdc * sizeof(double);
+constexpr size_t kSSmemBytes = kSCBytes + 4 * 64 * sizeof(int);
+
+__global__ void __launch_bounds__(256) k_gemm_simt(FactorArgs a, const TileItem* __restrict__ items) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double(*As)[64] = reinterpret_cast<double(*)[64]>(smem_raw);
+  double(*Bs)[64] = reinterpret_cast<double(*)[64]>(smem_raw + 16 * 64 * sizeof(double));
+  double* Cs = reinterpret_cast<double*>(smem_raw);
+  int* ints = reinterpret_cast<int*>(smem_raw + kSCBytes);
+  const TileItem it = items[blockIdx.x];
+  const SnMeta m = a.meta[it.s];
+  const double* g = a.L + m.off;
+  const int64_t ld = m.ld;
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  double acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+  for (int kk = 0; kk < it.kn; kk += 16) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      int e = tid + 256 * q, kq = e >> 6, r = e & 63, k = kk + kq;
+      const int64_t col = (int64_t)(it.k0 + k) * ld;
+      As[kq][r] = (r < it.mrows && k < it.kn) ? g[it.a_row0 + r + col] : 0.0;
+      Bs[kq][r] = (r < it.ncols && k < it.kn) ? g[it.b_row0 + r + col] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kq = 0; kq < 16; ++kq) {
+      double av[4], bv[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) av[i] = As[kq][ty + 16 * i];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) bv[j] = Bs[kq][tx + 16 * j];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = fma(av[i], bv[j], acc[i][j]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) Cs[(ty + 16 * i) + (tx + 16 * j) * kSLdc] = acc[i][j];
+  __syncthreads();
+  tile_epilogue<64, 64, 256>(a, it, m, Cs, kSLdc, ints, ints + 64, ints + 128, ints + 192);
+}
+
+}  // namespace
+
+void init_gemm_attributes() {
+  cudaFuncSetAttribute(k_gemm_dmma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDSmemBytes);
+}
+
+void launch_gemm(cudaStream_t st, const FactorArgs& a, const TileItem* items, int count, int tile) {
+  if (count <= 0) return;
+  if (tile == 128) k_gemm_dmma<<<count, kDThreads, kDSmemBytes, st>>>(a, items);
+  else k_gemm_simt<<<count, 256, kSSmemBytes, st>>>(a, items);
+}
+
+}  // namespace dev
+}  // namespace spb

@@ -10,7 +10,7 @@ namespace dev {
 
 // Status word shared by all kernels of one handle.  The first failure wins.
 struct Status {
-  int32_t code;        // 0 ok, 1 not SPD, 2 structure error
+  int32_t code;        // 0 ok, 1 not SPD, 2 structure error, 3 device wait timed out
   int32_t supernode;   // 0-based supernode of the failing pivot
   int32_t column;      // 0-based permuted column of the failing pivot
   int32_t pad;
@@ -27,23 +27,38 @@ struct FactorArgs {
 
 // Must run once per process (per device) before the first launch or capture.
 void init_kernel_attributes();
+void init_gemm_attributes();
 void launch_assemble(cudaStream_t st, double* L, const int64_t* dst, const double* vals, int64_t nnz);
 void launch_factor_small(cudaStream_t st, const FactorArgs& a, const int32_t* items, int count, int smem_bytes);
 void launch_potrf_diag(cudaStream_t st, const FactorArgs& a, const PanelItem* items, int count);
 void launch_trsm_rows(cudaStream_t st, const FactorArgs& a, const PanelItem* items, int count);
 void launch_gemm(cudaStream_t st, const FactorArgs& a, const TileItem* items, int count, int tile);
 
-// Solve on the permuted right-hand sides X (n x nrhs, column-major, leading dimension ldx).
-struct SolveArgs {
+// Solves work on the permuted right-hand sides X (n x nrhs, column-major, leading dimension ldx).
+
+// Persistent sweeps (one launch each).  counter, arrived and blkdone must be
+// zero at launch; expected[s] is the number of forward off-diagonal tiles that
+// write rows of supernode s.
+struct PSolveArgs {
   const double* L;
   const SnMeta* meta;
   const int32_t* rows;
+  const int32_t* supmember;
+  const int32_t* sparent;
   double* X;
   int64_t ldx;
-  int nrhs;
+  int nrhs;  // <= 64
+  const SolveTask* tasks;
+  int ntasks;
+  int32_t* counter;
+  const int32_t* expected;
+  int32_t* arrived;
+  int32_t* blkdone;
+  Status* status;
+  long long spin_limit;  // polls (about 128 ns apart) before a wait gives up
 };
-void launch_solve_forward(cudaStream_t st, const SolveArgs& a, const int32_t* sn, int count);
-void launch_solve_backward(cudaStream_t st, const SolveArgs& a, const int32_t* sn, int count);
+void init_solve_attributes();
+void launch_solve_persistent(cudaStream_t st, const PSolveArgs& a, bool forward);
 
 // X[invp[i], c] = B[i, c]   and   B[i, c] = X[invp[i], c]
 void launch_permute_in(cudaStream_t st, double* X, int64_t ldx, const double* B, int64_t ldb,

@@ -57,14 +57,13 @@ Plan build_plan(const Symbolic& sym, const PlanParams& prm) {
     P.exec_flops += w * w * w / 3.0 + mm * w * w + mm * mm * w;
   }
 
-  const int T = prm.tile_ext_small;
-  auto push_tiles = [&](int s, int mode, int rbeg, int rend, int cbeg, int cend, int k0, int kn,
-                        bool lower_only) {
-    // tiles of the (rend-rbeg) x (cend-cbeg) product; rows/cols counted from rbeg/cbeg
+  // Tiles of a (rend-rbeg) x (cend-cbeg) product, rows/cols counted from rbeg/cbeg;
+  // tiles entirely above the diagonal of a symmetric product are skipped.
+  auto push_tiles = [&](std::vector<TileItem>& out, int T, int s, int mode, int rbeg, int rend, int cbeg, int cend,
+                        int k0, int kn) {
     for (int cj = cbeg; cj < cend; cj += T)
       for (int ri = rbeg; ri < rend; ri += T) {
-        // skip tiles entirely above the diagonal of a symmetric product
-        if (lower_only && (ri - rbeg) + T <= (cj - cbeg)) continue;
+        if ((ri - rbeg) + T <= (cj - cbeg)) continue;
         TileItem t;
         t.s = s;
         t.mode = mode;
@@ -74,9 +73,24 @@ Plan build_plan(const Symbolic& sym, const PlanParams& prm) {
         t.kn = kn;
         t.mrows = std::min(T, rend - ri);
         t.ncols = std::min(T, cend - cj);
-        P.tile_items.push_back(t);
+        out.push_back(t);
       }
   };
+  // Emit the tiles of one phase as (up to) two launches: 64-wide FMA tiles and
+  // 128-wide tensor-core tiles.
+  std::vector<TileItem> t64, t128;
+  auto flush_gemm = [&]() {
+    for (int pass = 0; pass < 2; ++pass) {
+      std::vector<TileItem>& v = pass ? t128 : t64;
+      if (v.empty()) continue;
+      Step gs{StepKind::Gemm, (int32_t)P.tile_items.size(), (int32_t)v.size(), 0, pass ? 128 : 64};
+      P.tile_items.insert(P.tile_items.end(), v.begin(), v.end());
+      P.steps.push_back(gs);
+      v.clear();
+    }
+  };
+  auto pick = [&](int rows) -> std::vector<TileItem>& { return rows >= prm.big_tile_rows ? t128 : t64; };
+  auto tile_of = [&](int rows) { return rows >= prm.big_tile_rows ? 128 : 64; };
 
   for (int L = 0; L < H; ++L) {
     const auto& sns = P.level_sn[L];
@@ -109,11 +123,10 @@ Plan build_plan(const Symbolic& sym, const PlanParams& prm) {
         const SnMeta& m = P.meta[s];
         if (c0 >= m.w) continue;
         int nbk = std::min(prm.nb, m.w - c0);
-        for (int r = c0 + nbk; r < m.h; r += 64) P.panel_items.push_back(PanelItem{s, c0, nbk, r});
+        for (int r = c0 + nbk; r < m.h; r += 128) P.panel_items.push_back(PanelItem{s, c0, nbk, r});
       }
       pt.count = (int32_t)P.panel_items.size() - pt.begin;
       if (pt.count) P.steps.push_back(pt);
-      Step gs{StepKind::Gemm, (int32_t)P.tile_items.size(), 0, 0, T};
       for (int s : sns) {
         if (!P.is_big[s]) continue;
         const SnMeta& m = P.meta[s];
@@ -121,21 +134,70 @@ Plan build_plan(const Symbolic& sym, const PlanParams& prm) {
         int nbk = std::min(prm.nb, m.w - c0);
         int c1 = c0 + nbk;
         if (c1 >= m.w) continue;
-        push_tiles(s, 0, c1, m.h, c1, m.w, c0, nbk, true);
+        int rows = m.h - c1;
+        push_tiles(pick(rows), tile_of(rows), s, 0, c1, m.h, c1, m.w, c0, nbk);
       }
-      gs.count = (int32_t)P.tile_items.size() - gs.begin;
-      if (gs.count) P.steps.push_back(gs);
+      flush_gemm();
     }
     // 3. external Schur-complement updates of every panel of the level
-    {
-      Step gs{StepKind::Gemm, (int32_t)P.tile_items.size(), 0, 0, T};
-      for (int s : sns) {
-        const SnMeta& m = P.meta[s];
-        if (m.h > m.w) push_tiles(s, 1, m.w, m.h, m.w, m.h, 0, m.w, true);
-      }
-      gs.count = (int32_t)P.tile_items.size() - gs.begin;
-      if (gs.count) P.steps.push_back(gs);
+    for (int s : sns) {
+      const SnMeta& m = P.meta[s];
+      int rows = m.h - m.w;
+      if (rows > 0) push_tiles(pick(rows), tile_of(rows), s, 1, m.w, m.h, m.w, m.h, 0, m.w);
     }
+    flush_gemm();
+  }
+  // algorithmic flops per step
+  P.step_flops.assign(P.steps.size(), 0.0);
+  for (size_t k = 0; k < P.steps.size(); ++k) {
+    const Step& st = P.steps[k];
+    double f = 0.0;
+    for (int i = st.begin; i < st.begin + st.count; ++i) {
+      if (st.kind == StepKind::FactorSmall) {
+        const SnMeta& m = P.meta[P.small_items[i]];
+        double w = m.w, mm = m.h - m.w;
+        f += w * w * w / 3.0 + mm * w * w;
+      } else if (st.kind == StepKind::PotrfDiag) {
+        double nb = P.panel_items[i].nb;
+        f += nb * nb * nb / 3.0;
+      } else if (st.kind == StepKind::TrsmRows) {
+        const PanelItem& it = P.panel_items[i];
+        double rows = std::min(128, P.meta[it.s].h - it.row0);
+        f += rows * it.nb * it.nb;
+      } else {
+        const TileItem& t = P.tile_items[i];
+        // pairs (r, c) of the tile with panel row >= panel column
+        double pairs = 0.0;
+        for (int c = 0; c < t.ncols; ++c) {
+          int lo = std::max(0, t.b_row0 + c - t.a_row0);
+          if (lo < t.mrows) pairs += t.mrows - lo;
+        }
+        f += 2.0 * t.kn * pairs;
+      }
+    }
+    P.step_flops[k] = f;
+  }
+  for (const SnMeta& m : P.meta) P.solve_sweep_bytes += 8.0 * m.h * m.w;
+
+  // persistent solve task lists
+  P.fwd_pending.assign(ns, 0);
+  for (int s = 0; s < ns; ++s) {
+    const SnMeta& m = P.meta[s];
+    const int nblk = (m.w + 63) / 64, noff = (m.h - m.w + 63) / 64;
+    for (int t = 0; t < nblk; ++t) P.fwd_tasks.push_back(SolveTask{s, t});
+    for (int u = 0; u < noff; ++u) {
+      P.fwd_tasks.push_back(SolveTask{s, -u - 1});
+      int r0 = m.w + 64 * u, r1 = std::min(m.h, r0 + 64), last = -1;
+      for (int r = r0; r < r1; ++r) {
+        int t = P.supmember0[P.rows[m.lidx + r]];
+        if (t != last) P.fwd_pending[t]++;
+        last = t;
+      }
+    }
+  }
+  for (int s = ns - 1; s >= 0; --s) {
+    const int nblk = (P.meta[s].w + 63) / 64;
+    for (int t = nblk - 1; t >= 0; --t) P.bwd_tasks.push_back(SolveTask{s, t});
   }
   return P;
 }

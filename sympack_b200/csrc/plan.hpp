@@ -53,7 +53,7 @@ struct TileItem {
 enum class StepKind : int32_t {
   FactorSmall = 0,   // fused POTRF + TRSM of whole panels in shared memory (items = supernode ids)
   PotrfDiag = 1,     // POTRF of one 64-column diagonal block of a wide panel (PanelItem, row0 = -1)
-  TrsmRows = 2,      // TRSM of 64-row tiles below that block (PanelItem)
+  TrsmRows = 2,      // TRSM of 128-row tiles below that block (PanelItem)
   Gemm = 3,          // TileItem list (in-panel or external update)
 };
 struct Step {
@@ -70,6 +70,15 @@ struct PanelItem {
   int32_t c0;
   int32_t nb;
   int32_t row0;   // first panel row of the row tile (>= c0+nb); -1 for the diagonal block
+};
+
+// One task of the persistent triangular solves (64-row / 64-column units).
+//   idx >= 0: diagonal column block idx of supernode s
+//   idx <  0: off-diagonal row tile (-idx - 1), rows w + 64 * (-idx - 1) ...
+// Task lists are topological: every task a task waits on comes earlier.
+struct SolveTask {
+  int32_t s;
+  int32_t idx;
 };
 
 struct Plan {
@@ -89,10 +98,16 @@ struct Plan {
   std::vector<PanelItem> panel_items;
   std::vector<TileItem> tile_items;
   std::vector<Step> steps;
+  std::vector<double> step_flops;  // useful (algorithmic) flops of each step
   // executed flop count of the sequence (w^3/3 + m w^2 + m^2 w per supernode)
   double exec_flops = 0.0;
-  // solve: supernodes of each level (shared with level_sn); big ones flagged
   std::vector<uint8_t> is_big;
+  // persistent solves: forward tasks (postorder), backward tasks (reverse),
+  // and per supernode the number of forward off-diagonal tiles writing its rows
+  std::vector<SolveTask> fwd_tasks, bwd_tasks;
+  std::vector<int32_t> fwd_pending;
+  // algorithmic bytes of one sweep: every panel element read once
+  double solve_sweep_bytes = 0.0;
 };
 
 // Tunables of the plan.
@@ -100,7 +115,7 @@ struct PlanParams {
   int small_max_w = 32;          // widest panel handled by the fused small-panel kernel
   int small_max_bytes = 96 * 1024;
   int nb = 64;                   // column block of the blocked panel factorization
-  int tile_ext_small = 64;       // tile edge for external updates
+  int big_tile_rows = 128;       // products with at least this many rows use 128 x 128 tensor-core tiles
 };
 
 Plan build_plan(const Symbolic& s, const PlanParams& p = PlanParams());

@@ -1,0 +1,300 @@
+// Persistent supernodal triangular solves (sm_100a).
+//
+// Numerics of symPACK's solve tasks (symPACKMatrix2D.hpp):
+//   FUC(J,J): Y_J <- L_JJ^-1 Y_J               (forward_update_contrib, 1519-1527)
+//   FUC(K,J): Y_K[rows] -= L_KJ Y_J            (1589-1592)
+//   BUC(J,I): X_I -= L_JI^T X_J[rows]           (back_update_contrib, 1741-1744)
+//   BUC(I,I): X_I <- L_II^-T X_I                (_tri_solve, 1659-1721)
+// The reference's FUC/BUC task graph (5167-5251, 5728-6322) becomes one
+// persistent launch per sweep: CTAs take tasks from an atomic counter in a
+// topological order (every dependency of a task was handed out earlier, so a
+// waiting CTA only ever waits on CTAs that are already running) and
+// synchronise through per-supernode counters in global memory.  Every wait is
+// bounded; on expiry the kernel records SPB timeout status and all CTAs leave.
+#include "kernels.cuh"
+
+namespace spb {
+namespace dev {
+
+namespace {
+
+constexpr int kT = 64;         // rows / columns per task unit
+constexpr int kPld = 65;       // padded leading dimension of the staged L block
+constexpr int kThreads = 256;
+constexpr size_t kSmemBytes = (size_t)(kT * kPld + 2 * kT * kT) * sizeof(double);
+
+__device__ __forceinline__ void report_status(Status* st, int code, int s, int col) {
+  if (atomicCAS(&st->code, 0, code) == 0) {
+    st->supernode = s;
+    st->column = col;
+  }
+}
+
+__device__ __forceinline__ int ld_acquire(const int32_t* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ int status_code(const Status* st) { return *(volatile const int32_t*)&st->code; }
+
+// Block-wide: wait until *flag >= target (thread 0 spins).  False on timeout or
+// if another CTA has already recorded a failure.
+__device__ bool wait_geq(const int32_t* flag, int target, Status* st, int s, int* sh_ok, long long limit) {
+  if (threadIdx.x == 0) {
+    int good = 1;
+    if (ld_acquire(flag) < target) {
+      good = 0;
+      for (long long it = 0; it < limit; ++it) {
+        __nanosleep(128);
+        if (ld_acquire(flag) >= target) {
+          good = 1;
+          break;
+        }
+        if (status_code(st) != 0) break;
+      }
+      if (!good && status_code(st) == 0) report_status(st, 3, s, target);
+    }
+    __threadfence();
+    *sh_ok = good;
+  }
+  __syncthreads();
+  int r = *sh_ok;
+  __syncthreads();
+  return r != 0;
+}
+
+// acc[i + c*kT] (+/-)= sum_k A[i + k*kPld] * B[k + c*kT]   for i < m, c < nr, k < kk
+template <bool kSub>
+__device__ __forceinline__ void block_gemv(double* acc, const double* A, const double* B, int m, int kk, int nr) {
+  for (int idx = threadIdx.x; idx < m * nr; idx += kThreads) {
+    int c = idx / m, i = idx - c * m;
+    double s = 0.0;
+    for (int k = 0; k < kk; ++k) s = fma(A[i + k * kPld], B[k + c * kT], s);
+    if (kSub) acc[i + c * kT] -= s;
+    else acc[i + c * kT] += s;
+  }
+}
+
+// acc[k + c*kT] -= sum_r A[r + k*kPld] * B[r + c*kT]   (transposed block), k < kk, r < m
+__device__ __forceinline__ void block_gemv_t(double* acc, const double* A, const double* B, int m, int kk, int nr) {
+  for (int idx = threadIdx.x; idx < kk * nr; idx += kThreads) {
+    int c = idx / kk, k = idx - c * kk;
+    double s = 0.0;
+    for (int r = 0; r < m; ++r) s = fma(A[r + k * kPld], B[r + c * kT], s);
+    acc[k + c * kT] -= s;
+  }
+}
+
+// Stage L rows [r0, r0+m) x columns [c0, c0+kk) of a panel into A (ld kPld).
+__device__ __forceinline__ void stage_block(double* A, const double* P, int64_t ld, int r0, int m, int c0, int kk) {
+  for (int idx = threadIdx.x; idx < m * kk; idx += kThreads) {
+    int k = idx / m, r = idx - k * m;
+    A[r + k * kPld] = P[(r0 + r) + (int64_t)(c0 + k) * ld];
+  }
+}
+
+// Stage X rows x0.. (contiguous) or rows rl[0..] (gathered) into B (ld kT), through L2.
+__device__ __forceinline__ void stage_x(double* B, const double* X, int64_t ldx, int x0, const int32_t* rl, int m,
+                                        int nr) {
+  for (int idx = threadIdx.x; idx < m * nr; idx += kThreads) {
+    int c = idx / m, r = idx - c * m;
+    int row = rl ? rl[r] : x0 + r;
+    B[r + c * kT] = __ldcg(X + row + c * ldx);
+  }
+}
+
+}  // namespace
+
+namespace {
+
+// Lower-triangular solves of a kk x kk block held in A (ld kPld) against the
+// right-hand sides acc (ld kT), one warp per right-hand side column.
+// forward: acc <- D^-1 acc ; backward: acc <- D^-T acc.
+template <bool kForward>
+__device__ void block_trsv(double* acc, const double* A, int kk, int nr) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = kThreads / 32;
+  for (int c = warp; c < nr; c += nw) {
+    double v0 = lane < kk ? acc[lane + c * kT] : 0.0;
+    double v1 = lane + 32 < kk ? acc[lane + 32 + c * kT] : 0.0;
+    for (int step = 0; step < kk; ++step) {
+      const int k = kForward ? step : kk - 1 - step;
+      const int owner = k & 31;
+      const bool hi = k >= 32;
+      double xk = __shfl_sync(0xffffffffu, hi ? v1 : v0, owner) / A[k + k * kPld];
+      if (lane == owner) {
+        if (hi) v1 = xk;
+        else v0 = xk;
+      }
+      if (kForward) {
+        // rows j > k: acc_j -= D[j][k] x_k
+        if (lane > k && lane < kk) v0 = fma(-A[lane + k * kPld], xk, v0);
+        if (lane + 32 > k && lane + 32 < kk) v1 = fma(-A[lane + 32 + k * kPld], xk, v1);
+      } else {
+        // rows j < k: acc_j -= D[k][j] x_k
+        if (lane < k) v0 = fma(-A[k + lane * kPld], xk, v0);
+        if (lane + 32 < k) v1 = fma(-A[k + (lane + 32) * kPld], xk, v1);
+      }
+    }
+    if (lane < kk) acc[lane + c * kT] = v0;
+    if (lane + 32 < kk) acc[lane + 32 + c * kT] = v1;
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_solve_forward(PSolveArgs a) {
+  extern __shared__ __align__(16) double sm[];
+  double* Ab = sm;                  // staged L block, ld kPld
+  double* Bx = sm + kT * kPld;      // staged X rows, ld kT
+  double* acc = Bx + kT * kT;       // accumulator, ld kT
+  __shared__ int sh_task, sh_ok;
+  const int nr = a.nrhs;
+  for (;;) {
+    if (threadIdx.x == 0) sh_task = atomicAdd(a.counter, 1);
+    __syncthreads();
+    const int tk = sh_task;
+    __syncthreads();
+    if (tk >= a.ntasks || status_code(a.status) != 0) return;
+    const SolveTask task = a.tasks[tk];
+    const int s = task.s;
+    const SnMeta m = a.meta[s];
+    const double* P = a.L + m.off;
+    const int32_t* rl = a.rows + m.lidx;
+    const int64_t ld = m.ld;
+    if (task.idx >= 0) {
+      // diagonal block t: all descendant updates into these rows, then blocks 0..t-1
+      const int t = task.idx, r0 = t * kT, bt = min(kT, m.w - r0);
+      if (!wait_geq(a.arrived + s, a.expected[s], a.status, s, &sh_ok, a.spin_limit)) return;
+      stage_x(acc, a.X, a.ldx, m.fc + r0, nullptr, bt, nr);
+      for (int i = 0; i < t; ++i) {
+        if (!wait_geq(a.blkdone + s, i + 1, a.status, s, &sh_ok, a.spin_limit)) return;
+        stage_x(Bx, a.X, a.ldx, m.fc + i * kT, nullptr, kT, nr);
+        stage_block(Ab, P, ld, r0, bt, i * kT, kT);
+        __syncthreads();
+        block_gemv<true>(acc, Ab, Bx, bt, kT, nr);
+        __syncthreads();
+      }
+      stage_block(Ab, P, ld, r0, bt, r0, bt);
+      __syncthreads();
+      block_trsv<true>(acc, Ab, bt, nr);
+      __syncthreads();
+      for (int idx = threadIdx.x; idx < bt * nr; idx += kThreads) {
+        int c = idx / bt, r = idx - c * bt;
+        a.X[m.fc + r0 + r + c * a.ldx] = acc[r + c * kT];
+      }
+      __threadfence();
+      __syncthreads();
+      if (threadIdx.x == 0) atomicAdd(a.blkdone + s, 1);
+    } else {
+      // off-diagonal rows: Y_K[rows] -= L_KJ Y_J, accumulated over the column blocks
+      const int u = -task.idx - 1, r0 = m.w + u * kT, bu = min(kT, m.h - r0);
+      const int nblk = (m.w + kT - 1) / kT;
+      for (int idx = threadIdx.x; idx < kT * nr; idx += kThreads) acc[idx % kT + (idx / kT) * kT] = 0.0;
+      for (int i = 0; i < nblk; ++i) {
+        const int bi = min(kT, m.w - i * kT);
+        if (!wait_geq(a.blkdone + s, i + 1, a.status, s, &sh_ok, a.spin_limit)) return;
+        stage_x(Bx, a.X, a.ldx, m.fc + i * kT, nullptr, bi, nr);
+        stage_block(Ab, P, ld, r0, bu, i * kT, bi);
+        __syncthreads();
+        block_gemv<false>(acc, Ab, Bx, bu, bi, nr);
+        __syncthreads();
+      }
+      for (int idx = threadIdx.x; idx < bu * nr; idx += kThreads) {
+        int c = idx / bu, r = idx - c * bu;
+        atomicAdd(a.X + rl[r0 + r] + c * a.ldx, -acc[r + c * kT]);
+      }
+      __threadfence();
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        int last = -1;
+        for (int r = 0; r < bu; ++r) {
+          int tgt = a.supmember[rl[r0 + r]];
+          if (tgt != last) atomicAdd(a.arrived + tgt, 1);
+          last = tgt;
+        }
+      }
+      __syncthreads();
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_solve_backward(PSolveArgs a) {
+  extern __shared__ __align__(16) double sm[];
+  double* Ab = sm;
+  double* Bx = sm + kT * kPld;
+  double* acc = Bx + kT * kT;
+  __shared__ int sh_task, sh_ok;
+  const int nr = a.nrhs;
+  for (;;) {
+    if (threadIdx.x == 0) sh_task = atomicAdd(a.counter, 1);
+    __syncthreads();
+    const int tk = sh_task;
+    __syncthreads();
+    if (tk >= a.ntasks || status_code(a.status) != 0) return;
+    const SolveTask task = a.tasks[tk];
+    const int s = task.s;
+    const SnMeta m = a.meta[s];
+    const double* P = a.L + m.off;
+    const int32_t* rl = a.rows + m.lidx;
+    const int64_t ld = m.ld;
+    const int nblk = (m.w + kT - 1) / kT;
+    const int t = task.idx, c0 = t * kT, bt = min(kT, m.w - c0);
+    const int par = a.sparent[s];
+    if (par >= 0 && !wait_geq(a.blkdone + par, (a.meta[par].w + kT - 1) / kT, a.status, s, &sh_ok, a.spin_limit)) return;
+    stage_x(acc, a.X, a.ldx, m.fc + c0, nullptr, bt, nr);
+    // rows owned by ancestors (final once the parent is done)
+    for (int rr = m.w; rr < m.h; rr += kT) {
+      const int br = min(kT, m.h - rr);
+      stage_x(Bx, a.X, a.ldx, 0, rl + rr, br, nr);
+      stage_block(Ab, P, ld, rr, br, c0, bt);
+      __syncthreads();
+      block_gemv_t(acc, Ab, Bx, br, bt, nr);
+      __syncthreads();
+    }
+    // later diagonal blocks of this supernode, newest first
+    for (int u = nblk - 1; u > t; --u) {
+      if (!wait_geq(a.blkdone + s, nblk - u, a.status, s, &sh_ok, a.spin_limit)) return;
+      const int rr = u * kT, br = min(kT, m.w - rr);
+      stage_x(Bx, a.X, a.ldx, m.fc + rr, nullptr, br, nr);
+      stage_block(Ab, P, ld, rr, br, c0, bt);
+      __syncthreads();
+      block_gemv_t(acc, Ab, Bx, br, bt, nr);
+      __syncthreads();
+    }
+    stage_block(Ab, P, ld, c0, bt, c0, bt);
+    __syncthreads();
+    block_trsv<false>(acc, Ab, bt, nr);
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < bt * nr; idx += kThreads) {
+      int c = idx / bt, r = idx - c * bt;
+      a.X[m.fc + c0 + r + c * a.ldx] = acc[r + c * kT];
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) atomicAdd(a.blkdone + s, 1);
+  }
+}
+
+int g_solve_grid = 0;
+
+}  // namespace
+
+void init_solve_attributes() {
+  cudaFuncSetAttribute(k_solve_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes);
+  cudaFuncSetAttribute(k_solve_backward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes);
+  int dev = 0, sms = 0, per = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_solve_forward, kThreads, kSmemBytes);
+  g_solve_grid = sms * (per > 0 ? per : 1);
+  if (g_solve_grid <= 0) g_solve_grid = 148;
+}
+
+void launch_solve_persistent(cudaStream_t st, const PSolveArgs& a, bool forward) {
+  if (a.ntasks <= 0) return;
+  int grid = g_solve_grid < a.ntasks ? g_solve_grid : a.ntasks;
+  if (forward) k_solve_forward<<<grid, kThreads, kSmemBytes, st>>>(a);
+  else k_solve_backward<<<grid, kThreads, kSmemBytes, st>>>(a);
+}
+
+}  // namespace dev
+}  // namespace spb

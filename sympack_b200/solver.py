@@ -44,6 +44,10 @@ class StateError(SymPACKError):
     """Methods called out of order (e.g. Solve before Factorize)."""
 
 
+class DeviceTimeoutError(SymPACKError):
+    """A bounded device-side wait expired; the handle remains usable."""
+
+
 def _raise(code: int, where: str, handle=None):
     if code == N.SPB_OK:
         return
@@ -54,6 +58,8 @@ def _raise(code: int, where: str, handle=None):
         raise NotSPDError(code, text)
     if code == N.SPB_ERR_STATE:
         raise StateError(code, text)
+    if code == N.SPB_ERR_TIMEOUT:
+        raise DeviceTimeoutError(code, text)
     if code == N.SPB_ERR_INVALID:
         raise ValueError(text)
     raise SymPACKError(code, text)
@@ -245,6 +251,27 @@ class symPACKMatrix2D:
         h = self._need()
         _raise(self._lib.spb_solve_device(h, C.c_void_p(d_rhs_ptr), C.c_void_p(d_x_ptr), nrhs, ld),
                "SolveDevice", h)
+
+    def SetStream(self, stream_handle: int | None) -> None:
+        """Run later calls on a caller-owned CUDA stream (e.g. torch.cuda.current_stream().cuda_stream)."""
+        _raise(self._lib.spb_set_stream(self._need(), C.c_void_p(stream_handle or 0)), "SetStream", self._h)
+
+    def SetWaitLimit(self, polls: int) -> None:
+        """Bound of every device-side wait in the solve kernels (polls ~128 ns apart)."""
+        _raise(self._lib.spb_set_wait_limit(self._need(), int(polls)), "SetWaitLimit", self._h)
+
+    def DebugStall(self, supernode: int) -> None:
+        """Failure-detection test hook: the forward solve waits for an update nobody sends."""
+        _raise(self._lib.spb_debug_stall(self._need(), int(supernode)), "DebugStall", self._h)
+
+    def SetProfiling(self, on: bool = True) -> None:
+        _raise(self._lib.spb_set_profiling(self._need(), 1 if on else 0), "SetProfiling", self._h)
+
+    def GetProfile(self) -> dict:
+        p = N.spb_profile()
+        _raise(self._lib.spb_get_profile(self._need(), C.byref(p)), "GetProfile", self._h)
+        return {name: dict(ms=p.ms[i], flops=p.flops[i], bytes=p.bytes[i], launches=p.launches[i])
+                for i, name in enumerate(N.KIND_NAMES)}
 
     # -- accessors (symPACKMatrixBase.hpp:96-103) ------------------------------
     def info(self) -> N.spb_info:

@@ -1,0 +1,197 @@
+"""GPU factor / solve parity with the CPU oracle (restatement of the reference's
+2D cell algorithm), all through the C ABI.  Tolerance: 1e-12 relative (max-norm)
+for both the factor and the solution, the north-star bound for the FP64 path."""
+import ctypes as C
+import os
+
+import numpy as np
+import pytest
+
+from oracle import numeric
+from sympack_b200 import (DeviceTimeoutError, DistSparseMatrix, NotSPDError, StateError, generators as G,
+                          symPACKMatrix2D, symPACKOptions)
+from sympack_b200 import _native as N
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-12
+
+
+def setup(A, **opt):
+    M = symPACKMatrix2D()
+    M.Init(symPACKOptions(device=0, **opt))
+    M.SymbolicFactorization(A)
+    M.DistributeMatrix(A)
+    M.Factorize()
+    return M
+
+
+def oracle_for(M, A):
+    perm, invp = M.GetOrdering()
+    xl, li = M.GetStructure()
+    sym = dict(xsuper=M.GetSupernodalPartition(), xlindx=xl, lindx=li, supmember=M.GetSupMembership(), invp=invp)
+    f = numeric.OracleFactor(A.size, sym, threads=os.cpu_count())
+    f.distribute(A.colptr, A.rowind, A.nzvalLocal)
+    f.factorize()
+    return f
+
+
+def relerr(a, b):
+    return float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
+
+
+CASES = [
+    ("lap3d_20", lambda: G.laplacian_3d(20, 20, 20, 1e-3)),
+    ("st27_14", lambda: G.stencil27(14, 14, 14, 1e-2, seed=1)),
+    ("st27_12_d1e-5", lambda: G.stencil27(12, 12, 12, 1e-5, seed=2)),
+    ("lap3d_31x17x9", lambda: G.laplacian_3d(31, 17, 9, 1e-3)),
+    ("rand_3000", lambda: G.random_graph_spd(3000, 10, 1.05, seed=9)),
+    ("rand_500_forest", lambda: G.random_graph_spd(500, 1.2, 1.05, seed=5)),
+]
+
+
+@pytest.mark.parametrize("name,gen", CASES)
+def test_factor_and_solution_match_oracle(name, gen):
+    n, cp, ri, v = gen()
+    A = DistSparseMatrix.from_lower_csc(n, cp, ri, v)
+    M = setup(A)
+    f = oracle_for(M, A)
+    assert relerr(M.GetFactor(), f.factor()) <= TOL
+    rng = np.random.default_rng(3)
+    for nrhs in (1, 16, 70):
+        b = rng.standard_normal((n, nrhs))
+        M.Solve(b)
+        x = M.GetSolution(nrhs=nrhs)
+        assert relerr(x, f.solve(b)) <= TOL, nrhs
+
+
+def test_cfg1_through_rutherford_boeing(tmp_path):
+    """2D 5-point Laplacian 64x64 written to RB and read back, as the reference driver does."""
+    n, cp, ri, v = G.laplacian_2d(64, 64)
+    p = str(tmp_path / "lap2d_64.rb")
+    DistSparseMatrix.from_lower_csc(n, cp, ri, v).write_rb(p)
+    A = DistSparseMatrix.from_rb(p)
+    M = setup(A)
+    f = oracle_for(M, A)
+    assert relerr(M.GetFactor(), f.factor()) <= TOL
+    b = np.random.default_rng(0).uniform(-1.0, 1.0, size=(n, 1))
+    M.Solve(b)
+    x = M.GetSolution(nrhs=1)
+    assert relerr(x, f.solve(b)) <= TOL
+    # reference residual metric ||AX - B||_F / ||B||_F (driver/utils.hpp:136-140)
+    assert np.linalg.norm(A.matvec(x) - b) / np.linalg.norm(b) < 1e-13
+
+
+def test_full_size_cfg2_solution_matches_oracle():
+    n, cp, ri, v = G.laplacian_3d(60, 60, 60, 1e-3)
+    A = DistSparseMatrix.from_lower_csc(n, cp, ri, v)
+    M = setup(A)
+    f = oracle_for(M, A)
+    b = np.random.default_rng(0).standard_normal((n, 16))
+    M.Solve(b)
+    x = M.GetSolution(nrhs=16)
+    assert relerr(x, f.solve(b)) <= TOL
+    assert np.linalg.norm(A.matvec(x) - b) / np.linalg.norm(b) < 1e-14
+
+
+def test_device_solve_with_leading_dimension():
+    import torch
+    n, cp, ri, v = G.stencil27(9, 9, 9, 1e-2)
+    A = DistSparseMatrix.from_lower_csc(n, cp, ri, v)
+    M = setup(A)
+    ld = n + 7
+    B = np.zeros((3, ld))
+    B[:, :n] = np.random.default_rng(1).standard_normal((3, n))
+    dB = torch.from_numpy(B).cuda()
+    dX = torch.full_like(dB, 7.0)
+    M.SolveDevice(dB.data_ptr(), dX.data_ptr(), 3, ld)
+    X = dX.cpu().numpy()
+    assert np.all(X[:, n:] == 7.0)  # padding untouched
+    M.Solve(B[:, :n].T.copy())
+    assert relerr(X[:, :n].T, M.GetSolution(nrhs=3)) == 0.0
+
+
+def test_refactorization_with_new_values_reuses_structure():
+    n, cp, ri, v = G.stencil27(11, 11, 11, 1e-2, seed=4)
+    A = DistSparseMatrix.from_lower_csc(n, cp, ri, v)
+    M = setup(A)
+    _, cp2, ri2, v2 = G.stencil27(11, 11, 11, 1e-2, seed=7)  # same pattern, new values
+    assert np.array_equal(cp2, cp) and np.array_equal(ri2, ri)
+    A2 = DistSparseMatrix.from_lower_csc(n, cp, ri, v2)
+    with pytest.raises(StateError):
+        M.Factorize()  # already factored: distribute first
+    M.DistributeMatrix(A2)
+    M.Factorize()
+    f = oracle_for(M, A2)
+    assert relerr(M.GetFactor(), f.factor()) <= TOL
+
+
+def test_not_spd_is_reported_and_handle_recovers():
+    n, cp, ri, v = G.laplacian_3d(12, 12, 12, 1e-3)
+    bad = v.copy()
+    bad[cp[700] - 1] = -1.0  # diagonal entry of column 701
+    A = DistSparseMatrix.from_lower_csc(n, cp, ri, v)
+    Abad = DistSparseMatrix.from_lower_csc(n, cp, ri, bad)
+    M = symPACKMatrix2D()
+    M.Init(symPACKOptions(device=0))
+    M.SymbolicFactorization(A)
+    M.DistributeMatrix(Abad)
+    with pytest.raises(NotSPDError):
+        M.Factorize()
+    code, sn, col = M.GetStatus()
+    assert code == 1 and sn >= 0 and col >= 0
+    M.DistributeMatrix(A)
+    M.Factorize()
+    assert M.GetStatus()[0] == 0
+    f = oracle_for(M, A)
+    assert relerr(M.GetFactor(), f.factor()) <= TOL
+
+
+def test_calls_out_of_order_on_device():
+    n, cp, ri, v = G.laplacian_2d(10, 10)
+    A = DistSparseMatrix.from_lower_csc(n, cp, ri, v)
+    M = symPACKMatrix2D()
+    M.Init(symPACKOptions(device=0))
+    M.SymbolicFactorization(A)
+    with pytest.raises(StateError):
+        M.Factorize()
+    M.DistributeMatrix(A)
+    with pytest.raises(StateError):
+        M.Solve(np.ones(n))
+    M.Factorize()
+    with pytest.raises(StateError):
+        M.GetSolution(nrhs=1)
+
+
+def test_profiled_run_matches_graph_run():
+    n, cp, ri, v = G.stencil27(13, 13, 13, 1e-2, seed=3)
+    A = DistSparseMatrix.from_lower_csc(n, cp, ri, v)
+    M = setup(A)
+    L1 = M.GetFactor()
+    M.SetProfiling(True)
+    M.DistributeMatrix(A)
+    M.Factorize()
+    L2 = M.GetFactor()
+    prof = M.GetProfile()
+    assert relerr(L2, L1) <= TOL
+    assert sum(p["launches"] for k, p in prof.items() if k not in ("solve_forward", "solve_backward")) >= 1
+    assert all(p["ms"] >= 0 for p in prof.values())
+
+
+def test_solve_wait_timeout_is_reported_and_recovers():
+    """A forward wait on an update nobody sends runs out; the call reports a
+    timeout and the next solve on the same handle succeeds."""
+    n, cp, ri, v = G.laplacian_3d(10, 10, 10, 1e-3)
+    A = DistSparseMatrix.from_lower_csc(n, cp, ri, v)
+    M = setup(A)
+    b = np.random.default_rng(0).standard_normal((n, 1))
+    M.Solve(b)
+    x_ok = M.GetSolution(nrhs=1)
+    root = M.info().nsuper - 1
+    M.SetWaitLimit(2000)
+    M.DebugStall(root)
+    with pytest.raises(DeviceTimeoutError):
+        M.Solve(b)
+    M.DebugStall(-1)
+    M.SetWaitLimit(1 << 24)
+    M.Solve(b)
+    assert relerr(M.GetSolution(nrhs=1), x_ok) == 0.0
