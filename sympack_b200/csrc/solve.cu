@@ -146,14 +146,20 @@ __global__ void __launch_bounds__(kThreads) k_solve_forward(PSolveArgs a) {
   double* Ab = sm;                  // staged L block, ld kPld
   double* Bx = sm + kT * kPld;      // staged X rows, ld kT
   double* acc = Bx + kT * kT;       // accumulator, ld kT
-  __shared__ int sh_task, sh_ok;
+  __shared__ int sh_task, sh_stop, sh_ok;
   const int nr = a.nrhs;
   for (;;) {
-    if (threadIdx.x == 0) sh_task = atomicAdd(a.counter, 1);
+    // thread 0 alone reads the counter and the status word, so the whole block
+    // takes the same branch (a barrier reached by only part of a block hangs)
+    if (threadIdx.x == 0) {
+      sh_task = atomicAdd(a.counter, 1);
+      sh_stop = status_code(a.status) != 0;
+    }
     __syncthreads();
     const int tk = sh_task;
+    const bool stop = sh_stop != 0;
     __syncthreads();
-    if (tk >= a.ntasks || status_code(a.status) != 0) return;
+    if (tk >= a.ntasks || stop) return;
     const SolveTask task = a.tasks[tk];
     const int s = task.s;
     const SnMeta m = a.meta[s];
@@ -222,14 +228,20 @@ __global__ void __launch_bounds__(kThreads) k_solve_backward(PSolveArgs a) {
   double* Ab = sm;
   double* Bx = sm + kT * kPld;
   double* acc = Bx + kT * kT;
-  __shared__ int sh_task, sh_ok;
+  __shared__ int sh_task, sh_stop, sh_ok;
   const int nr = a.nrhs;
   for (;;) {
-    if (threadIdx.x == 0) sh_task = atomicAdd(a.counter, 1);
+    // thread 0 alone reads the counter and the status word, so the whole block
+    // takes the same branch (a barrier reached by only part of a block hangs)
+    if (threadIdx.x == 0) {
+      sh_task = atomicAdd(a.counter, 1);
+      sh_stop = status_code(a.status) != 0;
+    }
     __syncthreads();
     const int tk = sh_task;
+    const bool stop = sh_stop != 0;
     __syncthreads();
-    if (tk >= a.ntasks || status_code(a.status) != 0) return;
+    if (tk >= a.ntasks || stop) return;
     const SolveTask task = a.tasks[tk];
     const int s = task.s;
     const SnMeta m = a.meta[s];

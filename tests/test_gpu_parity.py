@@ -107,7 +107,8 @@ def test_device_solve_with_leading_dimension():
     X = dX.cpu().numpy()
     assert np.all(X[:, n:] == 7.0)  # padding untouched
     M.Solve(B[:, :n].T.copy())
-    assert relerr(X[:, :n].T, M.GetSolution(nrhs=3)) == 0.0
+    # scatter-adds use atomics: summation order, hence the last bits, may differ run to run
+    assert relerr(X[:, :n].T, M.GetSolution(nrhs=3)) <= 1e-14
 
 
 def test_refactorization_with_new_values_reuses_structure():
@@ -177,21 +178,45 @@ def test_profiled_run_matches_graph_run():
     assert all(p["ms"] >= 0 for p in prof.values())
 
 
+TIMEOUT_CHILD = r"""
+import sys
+sys.path.insert(0, sys.argv[1])
+import numpy as np
+from sympack_b200 import DeviceTimeoutError, DistSparseMatrix, generators as G, symPACKMatrix2D, symPACKOptions
+n, cp, ri, v = G.laplacian_3d(10, 10, 10, 1e-3)
+A = DistSparseMatrix.from_lower_csc(n, cp, ri, v)
+M = symPACKMatrix2D()
+M.Init(symPACKOptions(device=0))
+M.SymbolicFactorization(A)
+M.DistributeMatrix(A)
+M.Factorize()
+b = np.random.default_rng(0).standard_normal((n, 1))
+M.Solve(b)
+x_ok = M.GetSolution(nrhs=1)
+M.SetWaitLimit(2000)
+M.DebugStall(M.info().nsuper - 1)
+try:
+    M.Solve(b)
+    print("NO_TIMEOUT")
+    sys.exit(1)
+except DeviceTimeoutError:
+    pass
+M.DebugStall(-1)
+M.SetWaitLimit(1 << 24)
+M.Solve(b)
+err = np.max(np.abs(M.GetSolution(nrhs=1) - x_ok)) / np.max(np.abs(x_ok))
+print("RECOVERED", err)
+sys.exit(0 if err <= 1e-14 else 2)
+"""
+
+
 def test_solve_wait_timeout_is_reported_and_recovers():
-    """A forward wait on an update nobody sends runs out; the call reports a
-    timeout and the next solve on the same handle succeeds."""
-    n, cp, ri, v = G.laplacian_3d(10, 10, 10, 1e-3)
-    A = DistSparseMatrix.from_lower_csc(n, cp, ri, v)
-    M = setup(A)
-    b = np.random.default_rng(0).standard_normal((n, 1))
-    M.Solve(b)
-    x_ok = M.GetSolution(nrhs=1)
-    root = M.info().nsuper - 1
-    M.SetWaitLimit(2000)
-    M.DebugStall(root)
-    with pytest.raises(DeviceTimeoutError):
-        M.Solve(b)
-    M.DebugStall(-1)
-    M.SetWaitLimit(1 << 24)
-    M.Solve(b)
-    assert relerr(M.GetSolution(nrhs=1), x_ok) == 0.0
+    """A forward wait on an update nobody sends runs out (bounded device wait);
+    the call reports a timeout and the next solve on the same handle succeeds.
+    Runs in a child process with its own time limit."""
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    r = subprocess.run([sys.executable, "-c", TIMEOUT_CHILD, root], capture_output=True, text=True, timeout=180)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "RECOVERED" in r.stdout
