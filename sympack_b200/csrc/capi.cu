@@ -235,7 +235,7 @@ void enqueue_solve(spb_handle* h, int nrhs) {
   const int ns = P.nsuper;
   for (int c0 = 0; c0 < nrhs; c0 += 64) {
     cudaMemsetAsync(h->dsync, 0, sizeof(int32_t) * (2 + 3 * (size_t)ns), h->stream);
-    spb::dev::PSolveArgs a;
+    spb::dev::PSolveArgs a{};
     a.L = h->dL;
     a.meta = h->dmeta;
     a.rows = h->drows;
@@ -247,6 +247,7 @@ void enqueue_solve(spb_handle* h, int nrhs) {
     a.expected = h->dexpected;
     a.arrived = h->dsync + 2;
     a.status = h->dstatus;
+    a.spin_limit = h->wait_limit;
     const size_t e0 = 4 * (size_t)(c0 / 64);
     a.tasks = h->dfwd;
     a.ntasks = (int)P.fwd_tasks.size();

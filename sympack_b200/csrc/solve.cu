@@ -302,7 +302,7 @@ void init_solve_attributes() {
 }
 
 void launch_solve_persistent(cudaStream_t st, const PSolveArgs& a, bool forward) {
-  if (a.ntasks <= 0) return;
+  if (a.ntasks <= 0 || a.spin_limit <= 0) return;
   int grid = g_solve_grid < a.ntasks ? g_solve_grid : a.ntasks;
   if (forward) k_solve_forward<<<grid, kThreads, kSmemBytes, st>>>(a);
   else k_solve_backward<<<grid, kThreads, kSmemBytes, st>>>(a);
