@@ -113,6 +113,25 @@ int spb_get_solution(spb_handle* h, double* B, int32_t nrhs, int64_t ldb);
 /* Solve with device-resident right-hand sides and solution (both n x nrhs, leading dimension ld). */
 int spb_solve_device(spb_handle* h, const double* d_rhs, double* d_x, int32_t nrhs, int64_t ld);
 
+/* Allocation-free variant of spb_solve_device.  No counterpart in the
+ * reference (which has no device-side solve entry point at all).
+ * For callers that cannot allocate device memory at solve time — code running
+ * while a CUDA graph is captured in global mode, where cudaMalloc is an illegal
+ * call, or services that fix their device-memory budget up front — whereas
+ * spb_solve_device may grow its workspace with cudaMalloc on a call with more
+ * right-hand sides than before.  This entry point calls no cudaMalloc, cudaFree
+ * or allocating library routine: its scratch (the permuted right-hand sides and
+ * the dependency counters) lives in one static __device__ array of 33 MiB that
+ * every GPU which loads the library holds until the process exits.
+ * Limits: n * nrhs <= 4,194,304 and at most 87,380 supernodes; larger requests
+ * return SPB_ERR_INVALID with a message saying so.
+ * The first call on a device resolves the array's device address
+ * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * Every call on a device shares the array: calls whose work overlaps on the GPU
+ * (other handles or streams) race, so serialize them.  The counters are cleared
+ * on every call; nothing else is kept between calls. */
+int spb_solve_device_noalloc(spb_handle* h, const double* d_rhs, double* d_x, int32_t nrhs, int64_t ld);
+
 /* Introspection for parity checks (arrays sized from spb_get_info). */
 int spb_get_info(spb_handle* h, spb_info* info);
 int spb_get_ordering(spb_handle* h, int32_t* perm, int32_t* invp);           /* n each, 1-based */

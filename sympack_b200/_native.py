@@ -97,6 +97,7 @@ SIGNATURES = [
     ("spb_solve", C.c_int, [_P, _DP, C.c_int32, C.c_int64]),
     ("spb_get_solution", C.c_int, [_P, _DP, C.c_int32, C.c_int64]),
     ("spb_solve_device", C.c_int, [_P, _P, _P, C.c_int32, C.c_int64]),
+    ("spb_solve_device_noalloc", C.c_int, [_P, _P, _P, C.c_int32, C.c_int64]),
     ("spb_get_info", C.c_int, [_P, C.POINTER(spb_info)]),
     ("spb_get_ordering", C.c_int, [_P, _I32P, _I32P]),
     ("spb_get_mmd_invp", C.c_int, [_P, _I32P]),

@@ -8,6 +8,7 @@
 #include <cstdio>
 #include <cstring>
 #include <exception>
+#include <mutex>
 #include <new>
 #include <stdexcept>
 #include <string>
@@ -774,3 +775,101 @@ int spb_get_status(spb_handle* h, int32_t* code, int32_t* supernode, int32_t* co
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free solve.
+//
+// spb_solve_device lazily grows the handle's right-hand-side workspace with
+// cudaMalloc when a call asks for more right-hand sides than before.  Some
+// callers cannot let that happen: code that runs while a CUDA graph is being
+// captured in global mode (where cudaMalloc is an illegal call), and services
+// that pin their device-memory budget up front.  spb_solve_device_noalloc
+// gives them the same solve with its scratch (permuted right-hand sides and
+// the dependency counters of the persistent sweeps) in one file-scope
+// __device__ array, so no call allocates or frees anything.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr size_t kNoAllocXBytes = (size_t)32 << 20;   // permuted right-hand sides: 4 Mi doubles
+constexpr size_t kNoAllocSyncBytes = (size_t)1 << 20; // counters of the sweeps: 256 Ki int32
+constexpr int kNoAllocMaxDevices = 64;
+
+// Held by every GPU that loads this library until the process exits (33 MiB).
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocXBytes + kNoAllocSyncBytes];
+
+std::mutex g_noalloc_mutex;
+void* g_noalloc_addr[kNoAllocMaxDevices] = {};  // device address of g_noalloc_scratch, per device
+
+// Host code must not use g_noalloc_scratch's name as a device address: on the
+// host it is a stand-in.  Resolve the real address once per device, with that
+// device current.
+int noalloc_scratch(spb_handle* h, unsigned char** out) {
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_addr[h->device]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) return cuda_fail(h, e == cudaSuccess ? cudaErrorInvalidSymbol : e,
+                                                 "solve_noalloc: cudaGetSymbolAddress");
+    g_noalloc_addr[h->device] = p;
+  }
+  *out = static_cast<unsigned char*>(g_noalloc_addr[h->device]);
+  return SPB_OK;
+}
+
+}  // namespace
+
+extern "C" int spb_solve_device_noalloc(spb_handle* h, const double* d_rhs, double* d_x, int32_t nrhs, int64_t ld) {
+  if (check_handle(h)) return SPB_ERR_INVALID;
+  if (h->device < 0) return fail(h, SPB_ERR_STATE, "host-only handle (device < 0) has no numeric phase");
+  if (!h->factored) return fail(h, SPB_ERR_STATE, "solve: call spb_factorize first");
+  const int n = h->sym.n;
+  const int ns = h->plan.nsuper;
+  if (nrhs <= 0 || ld < n || !d_rhs || !d_x) return fail(h, SPB_ERR_INVALID, "solve: bad right-hand side");
+  if (h->device >= kNoAllocMaxDevices) return fail(h, SPB_ERR_INVALID, "solve_noalloc: device ordinal >= 64");
+  if ((size_t)n * (size_t)nrhs * sizeof(double) > kNoAllocXBytes) {
+    char msg[160];
+    snprintf(msg, sizeof msg, "solve_noalloc: n * nrhs = %lld exceeds the %zu right-hand-side entries of the "
+             "static scratch (32 MiB)", (long long)n * nrhs, kNoAllocXBytes / sizeof(double));
+    return fail(h, SPB_ERR_INVALID, msg);
+  }
+  if ((2 + 3 * (size_t)ns) * sizeof(int32_t) > kNoAllocSyncBytes)
+    return fail(h, SPB_ERR_INVALID, "solve_noalloc: more supernodes than the static scratch counters hold (87,380)");
+  SPB_CK(h, cudaSetDevice(h->device));
+  unsigned char* base = nullptr;
+  int rc = noalloc_scratch(h, &base);
+  if (rc) return rc;
+  double* X = reinterpret_cast<double*>(base);
+  int32_t* sync = reinterpret_cast<int32_t*>(base + kNoAllocXBytes);
+  const spb::Plan& P = h->plan;
+  spb::dev::launch_permute_in(h->stream, X, n, d_rhs, ld, h->dinvp0, n, nrhs);
+  for (int c0 = 0; c0 < nrhs; c0 += 64) {
+    // counters must start at zero; the array keeps whatever the last call left
+    SPB_CK(h, cudaMemsetAsync(sync, 0, sizeof(int32_t) * (2 + 3 * (size_t)ns), h->stream));
+    spb::dev::PSolveArgs a{};
+    a.L = h->dL;
+    a.meta = h->dmeta;
+    a.rows = h->drows;
+    a.supmember = h->dsupm;
+    a.sparent = h->dsparent;
+    a.X = X + (int64_t)c0 * n;
+    a.ldx = n;
+    a.nrhs = std::min(64, nrhs - c0);
+    a.expected = h->dexpected;
+    a.arrived = sync + 2;
+    a.status = h->dstatus;
+    a.spin_limit = h->wait_limit;
+    a.tasks = h->dfwd;
+    a.ntasks = (int)P.fwd_tasks.size();
+    a.counter = sync;
+    a.blkdone = sync + 2 + ns;
+    spb::dev::launch_solve_persistent(h->stream, a, true);
+    a.tasks = h->dbwd;
+    a.ntasks = (int)P.bwd_tasks.size();
+    a.counter = sync + 1;
+    a.blkdone = sync + 2 + 2 * ns;
+    spb::dev::launch_solve_persistent(h->stream, a, false);
+  }
+  spb::dev::launch_permute_out(h->stream, d_x, ld, X, n, h->dinvp0, n, nrhs);
+  SPB_CK(h, cudaGetLastError());
+  return check_solve_status(h);
+}
