@@ -45,6 +45,7 @@ struct spb_handle {
   double* dA = nullptr;
   int32_t* dsmall = nullptr;
   spb::PanelItem* dpanel = nullptr;
+  double* dwinv = nullptr;  // L11^-1 of the diagonal blocks of one step
   spb::TileItem* dtiles = nullptr;
   int32_t* dinvp0 = nullptr;
   int32_t* dlevel_sn = nullptr;
@@ -133,10 +134,10 @@ void enqueue_factor(spb_handle* h) {
         spb::dev::launch_factor_small(h->stream, a, h->dsmall + st.begin, st.count, st.arg);
         break;
       case spb::StepKind::PotrfDiag:
-        spb::dev::launch_potrf_diag(h->stream, a, h->dpanel + st.begin, st.count);
+        spb::dev::launch_potrf_diag(h->stream, a, h->dpanel + st.begin, st.count, h->dwinv);
         break;
       case spb::StepKind::TrsmRows:
-        spb::dev::launch_trsm_rows(h->stream, a, h->dpanel + st.begin, st.count);
+        spb::dev::launch_trsm_rows(h->stream, a, h->dpanel + st.begin, st.count, h->dwinv);
         break;
       case spb::StepKind::Gemm:
         spb::dev::launch_gemm(h->stream, a, h->dtiles + st.begin, st.count, st.tile);
@@ -186,10 +187,10 @@ int factor_profiled(spb_handle* h) {
         spb::dev::launch_factor_small(h->stream, a, h->dsmall + st.begin, st.count, st.arg);
         break;
       case spb::StepKind::PotrfDiag:
-        spb::dev::launch_potrf_diag(h->stream, a, h->dpanel + st.begin, st.count);
+        spb::dev::launch_potrf_diag(h->stream, a, h->dpanel + st.begin, st.count, h->dwinv);
         break;
       case spb::StepKind::TrsmRows:
-        spb::dev::launch_trsm_rows(h->stream, a, h->dpanel + st.begin, st.count);
+        spb::dev::launch_trsm_rows(h->stream, a, h->dpanel + st.begin, st.count, h->dwinv);
         break;
       case spb::StepKind::Gemm:
         spb::dev::launch_gemm(h->stream, a, h->dtiles + st.begin, st.count, st.tile);
@@ -435,6 +436,7 @@ int spb_symbolic(spb_handle* h, int32_t n, const int64_t* colptr, const int32_t*
   SPB_CK(h, dalloc(h, &h->dA, (size_t)h->nnz_a));
   SPB_CK(h, dalloc(h, &h->dsmall, P.small_items.size()));
   SPB_CK(h, dalloc(h, &h->dpanel, P.panel_items.size()));
+  SPB_CK(h, dalloc(h, &h->dwinv, (size_t)std::max(1, P.max_diag_slots) * 64 * 64));
   SPB_CK(h, dalloc(h, &h->dtiles, P.tile_items.size()));
   SPB_CK(h, dalloc(h, &h->dinvp0, invp0.size()));
   SPB_CK(h, dalloc(h, &h->dlevel_sn, lsn.size()));

@@ -78,70 +78,164 @@ __global__ void __launch_bounds__(128) k_factor_small(FactorArgs a, const int32_
 
 constexpr int kNB = 64;
 
-// POTRF of one diagonal block [c0, c0+nb) of a wide panel (one CTA per item).
-__global__ void __launch_bounds__(256) k_potrf_diag(FactorArgs a, const PanelItem* __restrict__ items) {
-  __shared__ double D[kNB * kNB];
+// POTRF of one 64-column diagonal block [c0, c0+nb) of a wide panel (one CTA
+// per item), blocked by 16: warp 0 factors each 16 x 16 diagonal piece, then
+// the rows below are solved against it and the trailing block is updated.  The
+// CTA also writes W = L11^-1 (64 x 64, column-major) to its scratch slot, so the
+// TRSM of the rows below becomes the product R W^T.  A block narrower than 64
+// is padded with the identity.
+constexpr int kDL = kNB + 1;  // padded leading dimension in shared memory
+
+__global__ void __launch_bounds__(256) k_potrf_diag(FactorArgs a, const PanelItem* __restrict__ items,
+                                                    double* __restrict__ winv) {
+  __shared__ double D[kNB * kDL];
   const PanelItem it = items[blockIdx.x];
   const SnMeta m = a.meta[it.s];
   double* g = a.L + m.off;
   const int nb = it.nb, c0 = it.c0;
   const int64_t ld = m.ld;
-  for (int idx = threadIdx.x; idx < nb * nb; idx += blockDim.x) {
-    int c = idx / nb, r = idx - c * nb;
-    D[r + c * kNB] = (r >= c) ? g[(c0 + r) + (int64_t)(c0 + c) * ld] : 0.0;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int idx = tid; idx < kNB * kNB; idx += blockDim.x) {
+    int c = idx / kNB, r = idx - c * kNB;
+    double v = 0.0;
+    if (r < nb && c < nb) {
+      if (r >= c) v = g[(c0 + r) + (int64_t)(c0 + c) * ld];
+    } else if (r == c) {
+      v = 1.0;
+    }
+    D[r + c * kDL] = v;
   }
   __syncthreads();
-  panel_cholesky_smem(D, nb, nb, kNB, a.status, it.s, m.fc + c0);
-  for (int idx = threadIdx.x; idx < nb * nb; idx += blockDim.x) {
+  for (int kb = 0; kb < kNB; kb += 16) {
+    if (warp == 0) {
+      for (int k = kb; k < kb + 16; ++k) {
+        if (lane == 0) {
+          double d = D[k + k * kDL];
+          if (!(d > 0.0)) {
+            if (k < nb) report(a.status, 1, it.s, m.fc + c0 + k);
+            d = 1.0;
+          }
+          D[k + k * kDL] = sqrt(d);
+        }
+        __syncwarp();
+        const double inv = 1.0 / D[k + k * kDL];
+        const int i = k + 1 + lane;
+        if (i < kb + 16) D[i + k * kDL] *= inv;
+        __syncwarp();
+        // columns k+1 .. kb+15 of the 16 x 16 piece: at most 120 entries
+        const int w = kb + 15 - k;
+        for (int idx = lane; idx < w * w; idx += 32) {
+          int jj = k + 1 + idx / w, ii = k + 1 + idx % w;
+          if (ii >= jj) D[ii + jj * kDL] -= D[ii + k * kDL] * D[jj + k * kDL];
+        }
+        __syncwarp();
+      }
+    }
+    __syncthreads();
+    const int below = kNB - kb - 16;
+    if (tid < below) {  // one row per thread: solve against the 16 x 16 piece
+      const int i = kb + 16 + tid;
+      double x[16];
+#pragma unroll
+      for (int j = 0; j < 16; ++j) x[j] = D[i + (kb + j) * kDL];
+#pragma unroll
+      for (int k = 0; k < 16; ++k) {
+        double t = x[k];
+#pragma unroll
+        for (int j = 0; j < k; ++j) t = fma(-x[j], D[kb + k + (kb + j) * kDL], t);
+        x[k] = t / D[kb + k + (kb + k) * kDL];
+      }
+#pragma unroll
+      for (int j = 0; j < 16; ++j) D[i + (kb + j) * kDL] = x[j];
+    }
+    __syncthreads();
+    for (int idx = tid; idx < below * below; idx += blockDim.x) {
+      int j = kb + 16 + idx / below, i = kb + 16 + idx % below;
+      if (i >= j) {
+        double t = D[i + j * kDL];
+#pragma unroll
+        for (int k = 0; k < 16; ++k) t = fma(-D[i + (kb + k) * kDL], D[j + (kb + k) * kDL], t);
+        D[i + j * kDL] = t;
+      }
+    }
+    __syncthreads();
+  }
+  for (int idx = tid; idx < nb * nb; idx += blockDim.x) {
     int c = idx / nb, r = idx - c * nb;
-    if (r >= c) g[(c0 + r) + (int64_t)(c0 + c) * ld] = D[r + c * kNB];
+    if (r >= c) g[(c0 + r) + (int64_t)(c0 + c) * ld] = D[r + c * kDL];
+  }
+  // W = L^-1, column j solved by thread j: W[i][j] = -(sum_{k=j}^{i-1} L[i][k] W[k][j]) / L[i][i]
+  if (winv && tid < kNB) {
+    double* W = winv + (size_t)it.slot * kNB * kNB;
+    const int j = tid;
+    double w[kNB];
+#pragma unroll
+    for (int i = 0; i < kNB; ++i) {
+      double t = (i == j) ? 1.0 : 0.0;
+      if (i > j) {
+        double t0 = 0.0, t1 = 0.0;
+#pragma unroll
+        for (int k = 0; k < i; k += 2) {
+          if (k >= j) t0 = fma(D[i + k * kDL], w[k], t0);
+          if (k + 1 < i && k + 1 >= j) t1 = fma(D[i + (k + 1) * kDL], w[k + 1], t1);
+        }
+        t = -(t0 + t1);
+      }
+      w[i] = (i >= j) ? t / D[i + i * kDL] : 0.0;
+    }
+    double* q = W + (size_t)j * kNB;
+    asm volatile("" : "+l"(q));
+#pragma unroll
+    for (int i = 0; i < kNB; ++i) q[i] = w[i];
   }
 }
 
-// TRSM of one 128-row tile below a factored 64-column diagonal block:
-// R <- R D^-T.  One thread per row; the row lives in registers and is solved
-// by forward substitution against D broadcast from shared memory.
-__global__ void __launch_bounds__(128) k_trsm_rows(FactorArgs a, const PanelItem* __restrict__ items) {
-  __shared__ double D[kNB * kNB];  // row-major: D[k * kNB + j], zero above the diagonal and past nb
-  __shared__ double Dinv[kNB];
+// TRSM of one 64-row tile below a factored diagonal block: R <- R W^T with
+// W = L11^-1 from the scratch slot (64 x 64 FMA tile, 4 x 4 outputs per thread).
+__global__ void __launch_bounds__(256) k_trsm_rows(FactorArgs a, const PanelItem* __restrict__ items,
+                                                   const double* __restrict__ winv) {
+  extern __shared__ double smem_tr[];
+  double* R = smem_tr;              // R[r + k*kDL]
+  double* Wt = smem_tr + kNB * kDL; // Wt[k + j*kDL] = W[j][k]
   const PanelItem it = items[blockIdx.x];
   const SnMeta m = a.meta[it.s];
   double* g = a.L + m.off;
   const int nb = it.nb, c0 = it.c0;
   const int64_t ld = m.ld;
-  for (int idx = threadIdx.x; idx < kNB * kNB; idx += blockDim.x) {
-    int k = idx / kNB, j = idx - k * kNB;
-    D[idx] = (k < nb && j <= k) ? g[(c0 + k) + (int64_t)(c0 + j) * ld] : 0.0;
+  const int rows = min(kNB, m.h - it.row0);
+  const double* W = winv + (size_t)it.slot * kNB * kNB;
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  for (int idx = tid; idx < kNB * kNB; idx += blockDim.x) {
+    int k = idx / kNB, r = idx - k * kNB;
+    R[r + k * kDL] = (r < rows && k < nb) ? g[(it.row0 + r) + (int64_t)(c0 + k) * ld] : 0.0;
+    // W column-major: W[i][jcol] at i + jcol*64; Wt[k + j*kDL] = W[j][k] = W[j + k*64]
+    Wt[k + r * kDL] = W[r + k * kNB];
   }
   __syncthreads();
-  for (int k = threadIdx.x; k < kNB; k += blockDim.x) Dinv[k] = k < nb ? 1.0 / D[k * kNB + k] : 0.0;
-  __syncthreads();
-  const int r = threadIdx.x;
-  if (it.row0 + r >= m.h) return;
-  double x[kNB];
-  {
-    const double* p = g + it.row0 + r + (int64_t)c0 * ld;
+  double acc[4][4];
 #pragma unroll
-    for (int j = 0; j < kNB; ++j, p += ld) x[j] = j < nb ? *p : 0.0;
-  }
+  for (int i = 0; i < 4; ++i)
 #pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+#pragma unroll 4
   for (int k = 0; k < kNB; ++k) {
-    double s0 = x[k], s1 = 0.0;
+    double rv[4], wv[4];
 #pragma unroll
-    for (int j = 0; j + 1 < k; j += 2) {
-      s0 = fma(-x[j], D[k * kNB + j], s0);
-      s1 = fma(-x[j + 1], D[k * kNB + j + 1], s1);
-    }
-    if (k & 1) s0 = fma(-x[k - 1], D[k * kNB + k - 1], s0);
-    x[k] = (s0 + s1) * Dinv[k];
+    for (int i = 0; i < 4; ++i) rv[i] = R[(ty + 16 * i) + k * kDL];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) wv[j] = Wt[k + (tx + 16 * j) * kDL];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) acc[i][j] = fma(rv[i], wv[j], acc[i][j]);
   }
-  // a fresh pointer walk for the stores (keeps 64 addresses from living across the solve)
-  double* q = g + it.row0 + r;
-  asm volatile("" : "+l"(q));
-  q += (int64_t)c0 * ld;
 #pragma unroll
-  for (int j = 0; j < kNB; ++j, q += ld)
-    if (j < nb) *q = x[j];
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      int r = ty + 16 * i, c = tx + 16 * j;
+      if (r < rows && c < nb) g[(it.row0 + r) + (int64_t)(c0 + c) * ld] = acc[i][j];
+    }
 }
 
 __global__ void k_permute_in(double* X, int64_t ldx, const double* B, int64_t ldb, const int32_t* invp0, int n,
@@ -176,6 +270,7 @@ void launch_assemble(cudaStream_t st, double* L, const int64_t* dst, const doubl
 }
 
 void init_kernel_attributes() {
+  cudaFuncSetAttribute(k_trsm_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * kNB * kDL * (int)sizeof(double));
   init_gemm_attributes();
   init_solve_attributes();
   cudaFuncSetAttribute(k_factor_small, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
@@ -185,12 +280,12 @@ void launch_factor_small(cudaStream_t st, const FactorArgs& a, const int32_t* it
   k_factor_small<<<count, 128, smem_bytes, st>>>(a, items);
 }
 
-void launch_potrf_diag(cudaStream_t st, const FactorArgs& a, const PanelItem* items, int count) {
-  k_potrf_diag<<<count, 256, 0, st>>>(a, items);
+void launch_potrf_diag(cudaStream_t st, const FactorArgs& a, const PanelItem* items, int count, double* winv) {
+  k_potrf_diag<<<count, 256, 0, st>>>(a, items, winv);
 }
 
-void launch_trsm_rows(cudaStream_t st, const FactorArgs& a, const PanelItem* items, int count) {
-  k_trsm_rows<<<count, 128, 0, st>>>(a, items);
+void launch_trsm_rows(cudaStream_t st, const FactorArgs& a, const PanelItem* items, int count, const double* winv) {
+  k_trsm_rows<<<count, 256, 2 * kNB * kDL * sizeof(double), st>>>(a, items, winv);
 }
 
 void launch_permute_in(cudaStream_t st, double* X, int64_t ldx, const double* B, int64_t ldb,

@@ -30,8 +30,9 @@ void init_kernel_attributes();
 void init_gemm_attributes();
 void launch_assemble(cudaStream_t st, double* L, const int64_t* dst, const double* vals, int64_t nnz);
 void launch_factor_small(cudaStream_t st, const FactorArgs& a, const int32_t* items, int count, int smem_bytes);
-void launch_potrf_diag(cudaStream_t st, const FactorArgs& a, const PanelItem* items, int count);
-void launch_trsm_rows(cudaStream_t st, const FactorArgs& a, const PanelItem* items, int count);
+// winv: scratch of (diagonal blocks per step) x 64 x 64 doubles; slot per PanelItem
+void launch_potrf_diag(cudaStream_t st, const FactorArgs& a, const PanelItem* items, int count, double* winv);
+void launch_trsm_rows(cudaStream_t st, const FactorArgs& a, const PanelItem* items, int count, const double* winv);
 void launch_gemm(cudaStream_t st, const FactorArgs& a, const TileItem* items, int count, int tile);
 
 // Solves work on the permuted right-hand sides X (n x nrhs, column-major, leading dimension ldx).

@@ -111,19 +111,23 @@ Plan build_plan(const Symbolic& sym, const PlanParams& prm) {
       if (P.is_big[s]) maxw = std::max(maxw, P.meta[s].w);
     for (int c0 = 0; c0 < maxw; c0 += prm.nb) {
       Step pd{StepKind::PotrfDiag, (int32_t)P.panel_items.size(), 0, c0, 0};
+      int nslots = 0;
       for (int s : sns) {
         if (!P.is_big[s] || c0 >= P.meta[s].w) continue;
-        P.panel_items.push_back(PanelItem{s, c0, std::min(prm.nb, P.meta[s].w - c0), -1});
+        P.panel_items.push_back(PanelItem{s, c0, std::min(prm.nb, P.meta[s].w - c0), -1, nslots++});
       }
+      P.max_diag_slots = std::max(P.max_diag_slots, nslots);
       pd.count = (int32_t)P.panel_items.size() - pd.begin;
       if (pd.count) P.steps.push_back(pd);
       Step pt{StepKind::TrsmRows, (int32_t)P.panel_items.size(), 0, c0, 0};
+      int slot = 0;
       for (int s : sns) {
         if (!P.is_big[s]) continue;
         const SnMeta& m = P.meta[s];
         if (c0 >= m.w) continue;
         int nbk = std::min(prm.nb, m.w - c0);
-        for (int r = c0 + nbk; r < m.h; r += 128) P.panel_items.push_back(PanelItem{s, c0, nbk, r});
+        for (int r = c0 + nbk; r < m.h; r += 64) P.panel_items.push_back(PanelItem{s, c0, nbk, r, slot});
+        ++slot;
       }
       pt.count = (int32_t)P.panel_items.size() - pt.begin;
       if (pt.count) P.steps.push_back(pt);
@@ -162,7 +166,7 @@ Plan build_plan(const Symbolic& sym, const PlanParams& prm) {
         f += nb * nb * nb / 3.0;
       } else if (st.kind == StepKind::TrsmRows) {
         const PanelItem& it = P.panel_items[i];
-        double rows = std::min(128, P.meta[it.s].h - it.row0);
+        double rows = std::min(64, P.meta[it.s].h - it.row0);
         f += rows * it.nb * it.nb;
       } else {
         const TileItem& t = P.tile_items[i];
@@ -179,26 +183,31 @@ Plan build_plan(const Symbolic& sym, const PlanParams& prm) {
   }
   for (const SnMeta& m : P.meta) P.solve_sweep_bytes += 8.0 * m.h * m.w;
 
-  // persistent solve task lists
+  // Persistent solve task lists.  Both are ordered by elimination-tree height
+  // level (forward: leaves first; backward: root level first) so that tasks
+  // handed out together are independent; within a supernode, blocks go in
+  // dependency order.  Every task a task waits on is listed earlier.
   P.fwd_pending.assign(ns, 0);
-  for (int s = 0; s < ns; ++s) {
-    const SnMeta& m = P.meta[s];
-    const int nblk = (m.w + 63) / 64, noff = (m.h - m.w + 63) / 64;
-    for (int t = 0; t < nblk; ++t) P.fwd_tasks.push_back(SolveTask{s, t});
-    for (int u = 0; u < noff; ++u) {
-      P.fwd_tasks.push_back(SolveTask{s, -u - 1});
-      int r0 = m.w + 64 * u, r1 = std::min(m.h, r0 + 64), last = -1;
-      for (int r = r0; r < r1; ++r) {
-        int t = P.supmember0[P.rows[m.lidx + r]];
-        if (t != last) P.fwd_pending[t]++;
-        last = t;
+  for (int L = 0; L < H; ++L)
+    for (int s : P.level_sn[L]) {
+      const SnMeta& m = P.meta[s];
+      const int nblk = (m.w + 63) / 64, noff = (m.h - m.w + 63) / 64;
+      for (int t = 0; t < nblk; ++t) P.fwd_tasks.push_back(SolveTask{s, t});
+      for (int u = 0; u < noff; ++u) {
+        P.fwd_tasks.push_back(SolveTask{s, -u - 1});
+        int r0 = m.w + 64 * u, r1 = std::min(m.h, r0 + 64), last = -1;
+        for (int r = r0; r < r1; ++r) {
+          int t = P.supmember0[P.rows[m.lidx + r]];
+          if (t != last) P.fwd_pending[t]++;
+          last = t;
+        }
       }
     }
-  }
-  for (int s = ns - 1; s >= 0; --s) {
-    const int nblk = (P.meta[s].w + 63) / 64;
-    for (int t = nblk - 1; t >= 0; --t) P.bwd_tasks.push_back(SolveTask{s, t});
-  }
+  for (int L = H - 1; L >= 0; --L)
+    for (int s : P.level_sn[L]) {
+      const int nblk = (P.meta[s].w + 63) / 64;
+      for (int t = nblk - 1; t >= 0; --t) P.bwd_tasks.push_back(SolveTask{s, t});
+    }
   return P;
 }
 

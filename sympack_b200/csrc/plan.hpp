@@ -53,7 +53,7 @@ struct TileItem {
 enum class StepKind : int32_t {
   FactorSmall = 0,   // fused POTRF + TRSM of whole panels in shared memory (items = supernode ids)
   PotrfDiag = 1,     // POTRF of one 64-column diagonal block of a wide panel (PanelItem, row0 = -1)
-  TrsmRows = 2,      // TRSM of 128-row tiles below that block (PanelItem)
+  TrsmRows = 2,      // TRSM of 64-row tiles below that block (PanelItem)
   Gemm = 3,          // TileItem list (in-panel or external update)
 };
 struct Step {
@@ -70,6 +70,7 @@ struct PanelItem {
   int32_t c0;
   int32_t nb;
   int32_t row0;   // first panel row of the row tile (>= c0+nb); -1 for the diagonal block
+  int32_t slot;   // scratch slot holding this step's L11^-1 for the supernode
 };
 
 // One task of the persistent triangular solves (64-row / 64-column units).
@@ -98,6 +99,7 @@ struct Plan {
   std::vector<PanelItem> panel_items;
   std::vector<TileItem> tile_items;
   std::vector<Step> steps;
+  int32_t max_diag_slots = 0;      // most diagonal blocks factored in one step (scratch slots)
   std::vector<double> step_flops;  // useful (algorithmic) flops of each step
   // executed flop count of the sequence (w^3/3 + m w^2 + m^2 w per supernode)
   double exec_flops = 0.0;
