@@ -86,7 +86,7 @@ constexpr int kNB = 64;
 // is padded with the identity.
 constexpr int kDL = kNB + 1;  // padded leading dimension in shared memory
 
-__global__ void __launch_bounds__(256) k_potrf_diag(FactorArgs a, const PanelItem* __restrict__ items,
+__global__ void __launch_bounds__(256, 1) k_potrf_diag(FactorArgs a, const PanelItem* __restrict__ items,
                                                     double* __restrict__ winv) {
   __shared__ double D[kNB * kDL];
   const PanelItem it = items[blockIdx.x];
@@ -106,29 +106,34 @@ __global__ void __launch_bounds__(256) k_potrf_diag(FactorArgs a, const PanelIte
     D[r + c * kDL] = v;
   }
   __syncthreads();
+  __shared__ double Rinv[kNB];  // 1 / L_kk
   for (int kb = 0; kb < kNB; kb += 16) {
     if (warp == 0) {
-      for (int k = kb; k < kb + 16; ++k) {
-        if (lane == 0) {
-          double d = D[k + k * kDL];
-          if (!(d > 0.0)) {
-            if (k < nb) report(a.status, 1, it.s, m.fc + c0 + k);
-            d = 1.0;
-          }
-          D[k + k * kDL] = sqrt(d);
+      // 16 x 16 diagonal piece in registers: lane i < 16 holds row i
+      double r[16];
+#pragma unroll
+      for (int j = 0; j < 16; ++j) r[j] = (lane < 16 && j <= lane) ? D[kb + lane + (kb + j) * kDL] : 0.0;
+#pragma unroll
+      for (int k = 0; k < 16; ++k) {
+        double dkk = __shfl_sync(0xffffffffu, r[k], k);
+        if (!(dkk > 0.0)) {
+          if (lane == 0 && kb + k < nb) report(a.status, 1, it.s, m.fc + c0 + kb + k);
+          dkk = 1.0;
         }
-        __syncwarp();
-        const double inv = 1.0 / D[k + k * kDL];
-        const int i = k + 1 + lane;
-        if (i < kb + 16) D[i + k * kDL] *= inv;
-        __syncwarp();
-        // columns k+1 .. kb+15 of the 16 x 16 piece: at most 120 entries
-        const int w = kb + 15 - k;
-        for (int idx = lane; idx < w * w; idx += 32) {
-          int jj = k + 1 + idx / w, ii = k + 1 + idx % w;
-          if (ii >= jj) D[ii + jj * kDL] -= D[ii + k * kDL] * D[jj + k * kDL];
+        const double rs = rsqrt(dkk);  // 1 / L_kk
+        if (lane == k) r[k] = dkk * rs;
+        else if (lane > k && lane < 16) r[k] *= rs;
+        if (lane == 0) Rinv[kb + k] = rs;
+#pragma unroll
+        for (int j = k + 1; j < 16; ++j) {
+          const double ljk = __shfl_sync(0xffffffffu, r[k], j);
+          if (lane >= j && lane < 16) r[j] = fma(-r[k], ljk, r[j]);
         }
-        __syncwarp();
+      }
+      if (lane < 16) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j)
+          if (j <= lane) D[kb + lane + (kb + j) * kDL] = r[j];
       }
     }
     __syncthreads();
@@ -143,7 +148,7 @@ __global__ void __launch_bounds__(256) k_potrf_diag(FactorArgs a, const PanelIte
         double t = x[k];
 #pragma unroll
         for (int j = 0; j < k; ++j) t = fma(-x[j], D[kb + k + (kb + j) * kDL], t);
-        x[k] = t / D[kb + k + (kb + k) * kDL];
+        x[k] = t * Rinv[kb + k];
       }
 #pragma unroll
       for (int j = 0; j < 16; ++j) D[i + (kb + j) * kDL] = x[j];
@@ -164,24 +169,20 @@ __global__ void __launch_bounds__(256) k_potrf_diag(FactorArgs a, const PanelIte
     int c = idx / nb, r = idx - c * nb;
     if (r >= c) g[(c0 + r) + (int64_t)(c0 + c) * ld] = D[r + c * kDL];
   }
-  // W = L^-1, column j solved by thread j: W[i][j] = -(sum_{k=j}^{i-1} L[i][k] W[k][j]) / L[i][i]
+  // W = L^-1, column j by thread j: W[j][j] = 1/L_jj, W[i][j] = -(sum_{k=j}^{i-1} L[i][k] W[k][j]) / L_ii
   if (winv && tid < kNB) {
     double* W = winv + (size_t)it.slot * kNB * kNB;
     const int j = tid;
     double w[kNB];
 #pragma unroll
     for (int i = 0; i < kNB; ++i) {
-      double t = (i == j) ? 1.0 : 0.0;
-      if (i > j) {
-        double t0 = 0.0, t1 = 0.0;
+      double t0 = 0.0, t1 = 0.0;
 #pragma unroll
-        for (int k = 0; k < i; k += 2) {
-          if (k >= j) t0 = fma(D[i + k * kDL], w[k], t0);
-          if (k + 1 < i && k + 1 >= j) t1 = fma(D[i + (k + 1) * kDL], w[k + 1], t1);
-        }
-        t = -(t0 + t1);
+      for (int k = 0; k < i; k += 2) {
+        if (k >= j) t0 = fma(D[i + k * kDL], w[k], t0);
+        if (k + 1 < i && k + 1 >= j) t1 = fma(D[i + (k + 1) * kDL], w[k + 1], t1);
       }
-      w[i] = (i >= j) ? t / D[i + i * kDL] : 0.0;
+      w[i] = (i > j) ? -(t0 + t1) * Rinv[i] : (i == j ? Rinv[i] : 0.0);
     }
     double* q = W + (size_t)j * kNB;
     asm volatile("" : "+l"(q));
