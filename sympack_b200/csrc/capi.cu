@@ -37,7 +37,9 @@ struct spb_handle {
   std::vector<int32_t> rowind;
   std::vector<int32_t> level_off;  // level l covers dlevel_sn[level_off[l] .. level_off[l+1])
   // device buffers
-  double* dL = nullptr;
+  bool fp32 = false;        // precision form: FP32 factor + FP64 refinement
+  size_t elem = 8;          // bytes per factor entry
+  void* dL = nullptr;
   spb::SnMeta* dmeta = nullptr;
   int32_t* drows = nullptr;
   int32_t* dsupm = nullptr;
@@ -45,7 +47,7 @@ struct spb_handle {
   double* dA = nullptr;
   int32_t* dsmall = nullptr;
   spb::PanelItem* dpanel = nullptr;
-  double* dwinv = nullptr;  // L11^-1 of the diagonal blocks of one step
+  double* dwinv = nullptr;  // factored diagonal blocks (FP64) and 1/L_kk of one step
   spb::TileItem* dtiles = nullptr;
   int32_t* dinvp0 = nullptr;
   int32_t* dlevel_sn = nullptr;
@@ -55,6 +57,21 @@ struct spb_handle {
   int32_t* dsparent = nullptr;
   int32_t* dsync = nullptr;  // [fwd counter, bwd counter, arrived[ns], fwd blkdone[ns], bwd blkdone[ns]]
   Status* dstatus = nullptr;
+  // precision form: original matrix as full CSR (FP64) and refinement buffers
+  std::vector<int64_t> csr_rowptr;
+  std::vector<int32_t> csr_col;
+  std::vector<int64_t> csr_src;
+  int64_t* d_rowptr = nullptr;
+  int32_t* d_col = nullptr;
+  int64_t* d_csrsrc = nullptr;
+  double* d_val = nullptr;
+  double* d_norms = nullptr;  // [anorm, bmax[64], xmax[64], rmax[64]]
+  double anorm = 0.0;
+  double* dR = nullptr;       // residual / correction right-hand side (original order)
+  double* dD = nullptr;       // correction (original order)
+  double* dXo = nullptr;      // refined solution (original order)
+  int ir_iterations = 0;
+  double backward_error = -1.0;
   double* dX = nullptr;
   double* dB = nullptr;
   int64_t x_cap = 0;  // doubles available in dX and dB
@@ -110,7 +127,7 @@ void release_device(spb_handle* h) {
   h->allocs.clear();
   h->device_bytes = 0;
   h->dL = nullptr;
-  h->dX = h->dB = nullptr;
+  h->dX = h->dB = h->dR = h->dD = h->dXo = nullptr;
   h->x_cap = 0;
 }
 
@@ -121,6 +138,7 @@ spb::dev::FactorArgs factor_args(spb_handle* h) {
   a.rows = h->drows;
   a.supmember = h->dsupm;
   a.status = h->dstatus;
+  a.fp32 = h->fp32;
   return a;
 }
 
@@ -214,7 +232,7 @@ int factor_profiled(spb_handle* h) {
 int ensure_rhs_capacity(spb_handle* h, int nrhs) {
   int64_t need = (int64_t)h->sym.n * nrhs;
   if (need <= h->x_cap) return SPB_OK;
-  for (double** p : {&h->dX, &h->dB}) {
+  for (double** p : {&h->dX, &h->dB, &h->dR, &h->dD, &h->dXo}) {
     if (*p) {
       auto it = std::find(h->allocs.begin(), h->allocs.end(), (void*)*p);
       if (it != h->allocs.end()) h->allocs.erase(it);
@@ -226,6 +244,11 @@ int ensure_rhs_capacity(spb_handle* h, int nrhs) {
   h->x_cap = 0;
   SPB_CK(h, dalloc(h, &h->dX, need));
   SPB_CK(h, dalloc(h, &h->dB, need));
+  if (h->fp32) {
+    SPB_CK(h, dalloc(h, &h->dR, need));
+    SPB_CK(h, dalloc(h, &h->dD, need));
+    SPB_CK(h, dalloc(h, &h->dXo, need));
+  }
   h->x_cap = need;
   return SPB_OK;
 }
@@ -239,6 +262,7 @@ void enqueue_solve(spb_handle* h, int nrhs) {
     cudaMemsetAsync(h->dsync, 0, sizeof(int32_t) * (2 + 3 * (size_t)ns), h->stream);
     spb::dev::PSolveArgs a{};
     a.L = h->dL;
+    a.fp32 = h->fp32;
     a.meta = h->dmeta;
     a.rows = h->drows;
     a.supmember = h->dsupm;
@@ -302,6 +326,69 @@ int check_solve_status(spb_handle* h) {
     return fail(h, SPB_ERR_TIMEOUT, msg);
   }
   if (st.code != 0 && st.code != 1) return fail(h, SPB_ERR_STRUCTURE, "solve: device status error");
+  return SPB_OK;
+}
+
+// Solve with the factor as it is: b (ld ldb) -> x (ld ldx), through the permuted workspace.
+void plain_solve(spb_handle* h, const double* b, int64_t ldb, double* x, int64_t ldx, int nrhs) {
+  const int n = h->sym.n;
+  spb::dev::launch_permute_in(h->stream, h->dX, n, b, ldb, h->dinvp0, n, nrhs);
+  enqueue_solve(h, nrhs);
+  spb::dev::launch_permute_out(h->stream, x, ldx, h->dX, n, h->dinvp0, n, nrhs);
+}
+
+// Precision form: solve with the FP32 factor, then refine in FP64 until the
+// backward error ||b - A x||_inf / (||A||_inf ||x||_inf + ||b||_inf) of every
+// right-hand side is at most ir_tolerance.  b and x are in the original order.
+int ir_solve(spb_handle* h, const double* d_b, int64_t ldb, double* d_x, int64_t ldx, int nrhs) {
+  const int n = h->sym.n;
+  const double tol = h->opt.ir_tolerance > 0 ? h->opt.ir_tolerance : 1e-12;
+  const int maxit = h->opt.ir_max_iter > 0 ? h->opt.ir_max_iter : 30;
+  int iters_all = 0;
+  double eta_all = 0.0;
+  for (int c0 = 0; c0 < nrhs; c0 += 64) {
+    const int nr = std::min(64, nrhs - c0);
+    const double* b = d_b + (int64_t)c0 * ldb;
+    double* x = d_x + (int64_t)c0 * ldx;
+    plain_solve(h, b, ldb, x, ldx, nr);
+    SPB_CK(h, cudaMemsetAsync(h->d_norms + 1, 0, sizeof(double) * 64, h->stream));
+    spb::dev::launch_colmax(h->stream, b, n, nr, ldb, h->d_norms + 1);
+    double eta = 0.0, eta_prev = 1e300;
+    int it = 0;
+    for (;;) {
+      spb::dev::launch_residual(h->stream, h->d_rowptr, h->d_col, h->d_val, x, b, h->dR, n, nr, ldx);
+      SPB_CK(h, cudaMemsetAsync(h->d_norms + 65, 0, sizeof(double) * 128, h->stream));
+      spb::dev::launch_colmax(h->stream, x, n, nr, ldx, h->d_norms + 65);
+      spb::dev::launch_colmax(h->stream, h->dR, n, nr, ldx, h->d_norms + 129);
+      double nm[1 + 3 * 64];
+      SPB_CK(h, cudaMemcpyAsync(nm, h->d_norms, sizeof(nm), cudaMemcpyDeviceToHost, h->stream));
+      int rc = check_solve_status(h);  // synchronizes
+      if (rc) return rc;
+      eta = 0.0;
+      for (int c = 0; c < nr; ++c) {
+        double den = h->anorm * nm[65 + c] + nm[1 + c];
+        double e = den > 0 ? nm[129 + c] / den : (nm[129 + c] > 0 ? 1e300 : 0.0);
+        eta = std::max(eta, e);
+      }
+      if (eta <= tol) break;
+      if (it >= maxit || (it >= 4 && eta > 0.9 * eta_prev)) {
+        h->ir_iterations = std::max(iters_all, it);
+        h->backward_error = std::max(eta_all, eta);
+        char msg[128];
+        snprintf(msg, sizeof msg, "refinement stopped at backward error %.3e after %d steps (target %.1e)", eta, it,
+                 tol);
+        return fail(h, SPB_ERR_NOT_CONVERGED, msg);
+      }
+      eta_prev = eta;
+      plain_solve(h, h->dR, ldx, h->dD, ldx, nr);
+      spb::dev::launch_axpy(h->stream, x, h->dD, n, nr, ldx);
+      ++it;
+    }
+    iters_all = std::max(iters_all, it);
+    eta_all = std::max(eta_all, eta);
+  }
+  h->ir_iterations = iters_all;
+  h->backward_error = eta_all;
   return SPB_OK;
 }
 
@@ -428,7 +515,13 @@ int spb_symbolic(spb_handle* h, int32_t n, const int64_t* colptr, const int32_t*
   h->level_off[P.nlevels] = (int32_t)lsn.size();
   for (int i = 0; i < n; ++i) invp0[i] = h->sym.invp[i] - 1;
 
-  SPB_CK(h, dalloc(h, &h->dL, P.arena_elems));
+  h->fp32 = h->opt.precision == SPB_PRECISION_FP32_IR;
+  h->elem = h->fp32 ? sizeof(float) : sizeof(double);
+  {
+    unsigned char* arena = nullptr;
+    SPB_CK(h, dalloc(h, &arena, (size_t)P.arena_elems * h->elem));
+    h->dL = arena;
+  }
   SPB_CK(h, dalloc(h, &h->dmeta, P.meta.size()));
   SPB_CK(h, dalloc(h, &h->drows, P.rows.size()));
   SPB_CK(h, dalloc(h, &h->dsupm, P.supmember0.size()));
@@ -436,7 +529,7 @@ int spb_symbolic(spb_handle* h, int32_t n, const int64_t* colptr, const int32_t*
   SPB_CK(h, dalloc(h, &h->dA, (size_t)h->nnz_a));
   SPB_CK(h, dalloc(h, &h->dsmall, P.small_items.size()));
   SPB_CK(h, dalloc(h, &h->dpanel, P.panel_items.size()));
-  SPB_CK(h, dalloc(h, &h->dwinv, (size_t)std::max(1, P.max_diag_slots) * 64 * 64));
+  SPB_CK(h, dalloc(h, &h->dwinv, (size_t)std::max(1, P.max_diag_slots) * (64 * 64 + 64)));
   SPB_CK(h, dalloc(h, &h->dtiles, P.tile_items.size()));
   SPB_CK(h, dalloc(h, &h->dinvp0, invp0.size()));
   SPB_CK(h, dalloc(h, &h->dlevel_sn, lsn.size()));
@@ -463,6 +556,41 @@ int spb_symbolic(spb_handle* h, int32_t n, const int64_t* colptr, const int32_t*
   SPB_CK(h, up(h->dexpected, P.fwd_pending.data(), P.fwd_pending.size() * 4));
   SPB_CK(h, up(h->dsparent, P.sparent.data(), P.sparent.size() * 4));
   SPB_CK(h, cudaMemsetAsync(h->dstatus, 0, sizeof(Status), h->stream));
+  if (h->fp32) {
+    // full symmetric CSR of A in the original ordering; csr_src maps each entry to its input value
+    std::vector<int64_t>& rp = h->csr_rowptr;
+    rp.assign(n + 1, 0);
+    for (int c = 1; c <= n; ++c)
+      for (int64_t p = colptr[c - 1]; p < colptr[c]; ++p) {
+        int r = rowind[p - 1];
+        rp[r]++;
+        if (r != c) rp[c]++;
+      }
+    for (int i = 0; i < n; ++i) rp[i + 1] += rp[i];
+    h->csr_col.assign(rp[n], 0);
+    h->csr_src.assign(rp[n], 0);
+    std::vector<int64_t> fill(rp.begin(), rp.end() - 1);
+    for (int c = 1; c <= n; ++c)
+      for (int64_t p = colptr[c - 1]; p < colptr[c]; ++p) {
+        int r = rowind[p - 1];
+        int64_t k = fill[r - 1]++;
+        h->csr_col[k] = c - 1;
+        h->csr_src[k] = p - 1;
+        if (r != c) {
+          k = fill[c - 1]++;
+          h->csr_col[k] = r - 1;
+          h->csr_src[k] = p - 1;
+        }
+      }
+    SPB_CK(h, dalloc(h, &h->d_rowptr, rp.size()));
+    SPB_CK(h, dalloc(h, &h->d_col, h->csr_col.size()));
+    SPB_CK(h, dalloc(h, &h->d_csrsrc, h->csr_src.size()));
+    SPB_CK(h, dalloc(h, &h->d_val, h->csr_col.size()));
+    SPB_CK(h, dalloc(h, &h->d_norms, 1 + 3 * 64));
+    SPB_CK(h, up(h->d_rowptr, rp.data(), rp.size() * 8));
+    SPB_CK(h, up(h->d_col, h->csr_col.data(), h->csr_col.size() * 4));
+    SPB_CK(h, up(h->d_csrsrc, h->csr_src.data(), h->csr_src.size() * 8));
+  }
   SPB_CK(h, cudaStreamSynchronize(h->stream));
   h->have_symbolic = true;
   return SPB_OK;
@@ -470,13 +598,19 @@ int spb_symbolic(spb_handle* h, int32_t n, const int64_t* colptr, const int32_t*
 
 static int distribute_common(spb_handle* h) {
   const spb::Plan& P = h->plan;
-  SPB_CK(h, cudaMemsetAsync(h->dL, 0, P.arena_elems * sizeof(double), h->stream));
+  SPB_CK(h, cudaMemsetAsync(h->dL, 0, (size_t)P.arena_elems * h->elem, h->stream));
   SPB_CK(h, cudaMemsetAsync(h->dstatus, 0, sizeof(Status), h->stream));
   if (h->profiling) {
     SPB_CK(h, ensure_events(h, 2));
     SPB_CK(h, cudaEventRecord(h->events[0], h->stream));
   }
-  spb::dev::launch_assemble(h->stream, h->dL, h->damap, h->dA, h->nnz_a);
+  spb::dev::launch_assemble(h->stream, h->dL, h->fp32, h->damap, h->dA, h->nnz_a);
+  if (h->fp32) {  // FP64 copy of A for the refinement residuals, and ||A||_inf
+    spb::dev::launch_gather(h->stream, h->d_val, h->dA, h->d_csrsrc, (int64_t)h->csr_col.size());
+    SPB_CK(h, cudaMemsetAsync(h->d_norms, 0, sizeof(double), h->stream));
+    spb::dev::launch_rowsum_max(h->stream, h->d_rowptr, h->d_val, h->sym.n, h->d_norms);
+    SPB_CK(h, cudaMemcpyAsync(&h->anorm, h->d_norms, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  }
   SPB_CK(h, cudaGetLastError());
   if (h->profiling) SPB_CK(h, cudaEventRecord(h->events[1], h->stream));
   SPB_CK(h, cudaStreamSynchronize(h->stream));
@@ -556,6 +690,7 @@ int spb_solve_device(spb_handle* h, const double* d_rhs, double* d_x, int32_t nr
   SPB_CK(h, cudaSetDevice(h->device));
   int rc = ensure_rhs_capacity(h, nrhs);
   if (rc) return rc;
+  if (h->fp32) return ir_solve(h, d_rhs, ld, d_x, ld, nrhs);
   if (h->profiling) SPB_CK(h, ensure_events(h, 4 * (size_t)((nrhs + 63) / 64)));
   spb::dev::launch_permute_in(h->stream, h->dX, n, d_rhs, ld, h->dinvp0, n, nrhs);
   enqueue_solve(h, nrhs);
@@ -577,6 +712,13 @@ int spb_solve(spb_handle* h, const double* rhs, int32_t nrhs, int64_t ldb) {
   if (rc) return rc;
   SPB_CK(h, cudaMemcpy2DAsync(h->dB, (size_t)n * 8, rhs, (size_t)ldb * 8, (size_t)n * 8, nrhs, cudaMemcpyHostToDevice,
                               h->stream));
+  if (h->fp32) {
+    rc = ir_solve(h, h->dB, n, h->dXo, n, nrhs);
+    if (rc) return rc;
+    h->have_solution = true;
+    h->x_nrhs = nrhs;
+    return SPB_OK;
+  }
   if (h->profiling) SPB_CK(h, ensure_events(h, 4 * (size_t)((nrhs + 63) / 64)));
   spb::dev::launch_permute_in(h->stream, h->dX, n, h->dB, n, h->dinvp0, n, nrhs);
   enqueue_solve(h, nrhs);
@@ -597,8 +739,12 @@ int spb_get_solution(spb_handle* h, double* B, int32_t nrhs, int64_t ldb) {
   const int n = h->sym.n;
   if (!B || nrhs <= 0 || nrhs > h->x_nrhs || ldb < n) return fail(h, SPB_ERR_INVALID, "get_solution: bad output");
   SPB_CK(h, cudaSetDevice(h->device));
-  spb::dev::launch_permute_out(h->stream, h->dB, n, h->dX, n, h->dinvp0, n, nrhs);
-  SPB_CK(h, cudaMemcpy2DAsync(B, (size_t)ldb * 8, h->dB, (size_t)n * 8, (size_t)n * 8, nrhs, cudaMemcpyDeviceToHost,
+  const double* src = h->dXo;  // refined solution, original order
+  if (!h->fp32) {
+    spb::dev::launch_permute_out(h->stream, h->dB, n, h->dX, n, h->dinvp0, n, nrhs);
+    src = h->dB;
+  }
+  SPB_CK(h, cudaMemcpy2DAsync(B, (size_t)ldb * 8, src, (size_t)n * 8, (size_t)n * 8, nrhs, cudaMemcpyDeviceToHost,
                               h->stream));
   SPB_CK(h, cudaStreamSynchronize(h->stream));
   return SPB_OK;
@@ -629,6 +775,8 @@ int spb_get_info(spb_handle* h, spb_info* info) {
   info->ncells = (int32_t)h->cells.cells.size();
   info->nblocks = (int32_t)h->cells.block_first_row.size();
   info->factor_launches = (int32_t)P.steps.size();
+  info->ir_iterations = h->ir_iterations;
+  info->backward_error = h->backward_error;
   return SPB_OK;
 }
 
@@ -706,7 +854,13 @@ int spb_get_factor(spb_handle* h, double* out) {
   SPB_CK(h, cudaSetDevice(h->device));
   const spb::Plan& P = h->plan;
   std::vector<double> arena(P.arena_elems);
-  SPB_CK(h, cudaMemcpy(arena.data(), h->dL, P.arena_elems * 8, cudaMemcpyDeviceToHost));
+  if (h->fp32) {
+    std::vector<float> a32(P.arena_elems);
+    SPB_CK(h, cudaMemcpy(a32.data(), h->dL, P.arena_elems * sizeof(float), cudaMemcpyDeviceToHost));
+    for (int64_t i = 0; i < P.arena_elems; ++i) arena[i] = a32[i];
+  } else {
+    SPB_CK(h, cudaMemcpy(arena.data(), h->dL, P.arena_elems * sizeof(double), cudaMemcpyDeviceToHost));
+  }
   int64_t pos = 0;
   for (const auto& m : P.meta) {
     for (int c = 0; c < m.w; ++c)
@@ -828,6 +982,7 @@ extern "C" int spb_solve_device_noalloc(spb_handle* h, const double* d_rhs, doub
   const int ns = h->plan.nsuper;
   if (nrhs <= 0 || ld < n || !d_rhs || !d_x) return fail(h, SPB_ERR_INVALID, "solve: bad right-hand side");
   if (h->device >= kNoAllocMaxDevices) return fail(h, SPB_ERR_INVALID, "solve_noalloc: device ordinal >= 64");
+  if (h->fp32) return fail(h, SPB_ERR_STATE, "solve_noalloc: refinement (FP32_IR) needs workspace; use spb_solve_device");
   if ((size_t)n * (size_t)nrhs * sizeof(double) > kNoAllocXBytes) {
     char msg[160];
     snprintf(msg, sizeof msg, "solve_noalloc: n * nrhs = %lld exceeds the %zu right-hand-side entries of the "
@@ -849,6 +1004,7 @@ extern "C" int spb_solve_device_noalloc(spb_handle* h, const double* d_rhs, doub
     SPB_CK(h, cudaMemsetAsync(sync, 0, sizeof(int32_t) * (2 + 3 * (size_t)ns), h->stream));
     spb::dev::PSolveArgs a{};
     a.L = h->dL;
+    a.fp32 = h->fp32;
     a.meta = h->dmeta;
     a.rows = h->drows;
     a.supmember = h->dsupm;

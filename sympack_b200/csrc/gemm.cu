@@ -39,18 +39,18 @@ __device__ __forceinline__ int find_row(const int32_t* __restrict__ rl, int h, i
 }
 
 // Apply a BM x BN tile of C held in shared memory (column-major, leading dimension ldc).
-template <int BM, int BN, int NT>
-__device__ void tile_epilogue(const FactorArgs& a, const TileItem& it, const SnMeta& m, const double* Cs,
-                              int ldc, int* Rr, int* Rc, int* Tc, int* Pos) {
+template <int BM, int BN, int NT, class T, class CT>
+__device__ void tile_epilogue(const FactorArgs& a, const TileItem& it, const SnMeta& m, const CT* Cs, int ldc,
+                              int* Rr, int* Rc, int* Tc, int* Pos) {
   const int tid = threadIdx.x;
-  double* g = a.L + m.off;
+  T* g = static_cast<T*>(a.L) + m.off;
   if (it.mode == 0) {
     const int64_t ld = m.ld;
     for (int idx = tid; idx < BM * BN; idx += NT) {
       int c = idx / BM, r = idx - c * BM;
       if (r < it.mrows && c < it.ncols) {
         int gr = it.a_row0 + r, gc = it.b_row0 + c;
-        if (gr >= gc) g[gr + (int64_t)gc * ld] -= Cs[r + c * ldc];
+        if (gr >= gc) g[gr + (int64_t)gc * ld] -= (T)Cs[r + c * ldc];
       }
     }
     return;
@@ -78,12 +78,12 @@ __device__ void tile_epilogue(const FactorArgs& a, const TileItem& it, const SnM
       Pos[i] = pos;
     }
     __syncthreads();
-    double* gt = a.L + mt.off;
+    T* gt = static_cast<T*>(a.L) + mt.off;
     const int ncol = ce - c;
     for (int idx = tid; idx < ncol * BM; idx += NT) {
       int cc = c + idx / BM, r = idx % BM;
       int p = Pos[r];
-      if (p >= 0 && Rr[r] >= Rc[cc]) atomicAdd(gt + (int64_t)(Rc[cc] - mt.fc) * mt.ld + p, -Cs[r + cc * ldc]);
+      if (p >= 0 && Rr[r] >= Rc[cc]) atomicAdd(gt + (int64_t)(Rc[cc] - mt.fc) * mt.ld + p, (T)(-Cs[r + cc * ldc]));
     }
     __syncthreads();
     c = ce;
@@ -128,7 +128,7 @@ __global__ void __launch_bounds__(kDThreads, 1) k_gemm_dmma(FactorArgs a, const 
   int* ints = reinterpret_cast<int*>(smem_raw + kDMainBytes);
   const TileItem it = items[blockIdx.x];
   const SnMeta m = a.meta[it.s];
-  const double* g = a.L + m.off;
+  const double* g = static_cast<const double*>(a.L) + m.off;
   const int64_t ld = m.ld;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int wm = warp & 1, wn = warp >> 1;  // 2 x 4 warps, 64 x 32 each
@@ -204,7 +204,7 @@ __global__ void __launch_bounds__(kDThreads, 1) k_gemm_dmma(FactorArgs a, const 
       Cs[r0 + 8 + (c0 + 1) * kDLdc] = acc[mi][ni][3];
     }
   __syncthreads();
-  tile_epilogue<kDM, kDN, kDThreads>(a, it, m, Cs, kDLdc, ints, ints + 128, ints + 256, ints + 384);
+  tile_epilogue<kDM, kDN, kDThreads, double, double>(a, it, m, Cs, kDLdc, ints, ints + 128, ints + 256, ints + 384);
 }
 
 // ---- 64 x 64 FP64 FMA tile --------------------------------------------------------
@@ -212,34 +212,35 @@ constexpr int kSLdc = 65;
 constexpr size_t kSCBytes = (size_t)64 * kSLdc * sizeof(double);
 constexpr size_t kSSmemBytes = kSCBytes + 4 * 64 * sizeof(int);
 
+template <class T>
 __global__ void __launch_bounds__(256) k_gemm_simt(FactorArgs a, const TileItem* __restrict__ items) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  double(*As)[64] = reinterpret_cast<double(*)[64]>(smem_raw);
-  double(*Bs)[64] = reinterpret_cast<double(*)[64]>(smem_raw + 16 * 64 * sizeof(double));
-  double* Cs = reinterpret_cast<double*>(smem_raw);
+  T(*As)[64] = reinterpret_cast<T(*)[64]>(smem_raw);
+  T(*Bs)[64] = reinterpret_cast<T(*)[64]>(smem_raw + 16 * 64 * sizeof(T));
+  T* Cs = reinterpret_cast<T*>(smem_raw);
   int* ints = reinterpret_cast<int*>(smem_raw + kSCBytes);
   const TileItem it = items[blockIdx.x];
   const SnMeta m = a.meta[it.s];
-  const double* g = a.L + m.off;
+  const T* g = static_cast<const T*>(a.L) + m.off;
   const int64_t ld = m.ld;
   const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
-  double acc[4][4];
+  T acc[4][4];
 #pragma unroll
   for (int i = 0; i < 4; ++i)
 #pragma unroll
-    for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+    for (int j = 0; j < 4; ++j) acc[i][j] = T(0);
   for (int kk = 0; kk < it.kn; kk += 16) {
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
       int e = tid + 256 * q, kq = e >> 6, r = e & 63, k = kk + kq;
       const int64_t col = (int64_t)(it.k0 + k) * ld;
-      As[kq][r] = (r < it.mrows && k < it.kn) ? g[it.a_row0 + r + col] : 0.0;
-      Bs[kq][r] = (r < it.ncols && k < it.kn) ? g[it.b_row0 + r + col] : 0.0;
+      As[kq][r] = (r < it.mrows && k < it.kn) ? g[it.a_row0 + r + col] : T(0);
+      Bs[kq][r] = (r < it.ncols && k < it.kn) ? g[it.b_row0 + r + col] : T(0);
     }
     __syncthreads();
 #pragma unroll
     for (int kq = 0; kq < 16; ++kq) {
-      double av[4], bv[4];
+      T av[4], bv[4];
 #pragma unroll
       for (int i = 0; i < 4; ++i) av[i] = As[kq][ty + 16 * i];
 #pragma unroll
@@ -256,19 +257,158 @@ __global__ void __launch_bounds__(256) k_gemm_simt(FactorArgs a, const TileItem*
 #pragma unroll
     for (int j = 0; j < 4; ++j) Cs[(ty + 16 * i) + (tx + 16 * j) * kSLdc] = acc[i][j];
   __syncthreads();
-  tile_epilogue<64, 64, 256>(a, it, m, Cs, kSLdc, ints, ints + 64, ints + 128, ints + 192);
+  tile_epilogue<64, 64, 256, T, T>(a, it, m, Cs, kSLdc, ints, ints + 64, ints + 128, ints + 192);
+}
+
+// ---- 128 x 128 split-precision 3xTF32 tensor-core tile (FP32 storage) -------------
+// Each FP32 operand x is split into tf32 parts hi = rna(x), lo = rna(x - hi);
+// C += A_lo B_hi + A_hi B_lo + A_hi B_hi with FP32 accumulation, which recovers
+// close to FP32 accuracy from the TF32 tensor pipe.
+constexpr int kTK = 32, kTStages = 3, kTLds = 136, kTLdc = 132;
+constexpr size_t kTPipeBytes = (size_t)kTStages * 2 * kTK * kTLds * sizeof(float);
+constexpr size_t kTCBytes = (size_t)128 * kTLdc * sizeof(float);
+constexpr size_t kTMainBytes = kTPipeBytes > kTCBytes ? kTPipeBytes : kTCBytes;
+constexpr size_t kTSmemBytes = kTMainBytes + 4 * 128 * sizeof(int);
+
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem, int src_bytes) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s), "l"(gmem), "r"(src_bytes));
+}
+
+__device__ __forceinline__ uint32_t to_tf32(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(r) : "f"(x));
+  return r;
+}
+
+__device__ __forceinline__ void split_tf32(float x, uint32_t& hi, uint32_t& lo) {
+  hi = to_tf32(x);
+  lo = to_tf32(x - __uint_as_float(hi));
+}
+
+// D(16x8, f32) += A(16x8, tf32, row) * B(8x8, tf32, col); lane = 4*g + t:
+//   a0 = A[g][t], a1 = A[g+8][t], a2 = A[g][t+4], a3 = A[g+8][t+4], b0 = B[t][g], b1 = B[t+4][g]
+__device__ __forceinline__ void mma_tf32(float* d, const uint32_t* a, const uint32_t* b) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+__global__ void __launch_bounds__(256, 1) k_gemm_tf32x3(FactorArgs a, const TileItem* __restrict__ items) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float* pipe = reinterpret_cast<float*>(smem_raw);
+  float* Cs = reinterpret_cast<float*>(smem_raw);
+  int* ints = reinterpret_cast<int*>(smem_raw + kTMainBytes);
+  const TileItem it = items[blockIdx.x];
+  const SnMeta m = a.meta[it.s];
+  const float* g = static_cast<const float*>(a.L) + m.off;
+  const int64_t ld = m.ld;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wm = warp & 1, wn = warp >> 1;
+  const int gq = lane >> 2, tq = lane & 3;
+
+  auto load_stage = [&](int stage, int kk) {
+    float* As = pipe + (size_t)stage * 2 * kTK * kTLds;
+    float* Bs = As + kTK * kTLds;
+#pragma unroll 4
+    for (int q = 0; q < 16; ++q) {
+      int e = tid + q * 256;  // 0 .. 4095: (column, row) of a 32 x 128 operand slab
+      int col = e >> 7, r = e & 127;
+      int k = kk + col;
+      bool kok = k < it.kn;
+      int64_t coff = (int64_t)(it.k0 + (kok ? k : 0)) * ld;
+      bool aok = kok && r < it.mrows;
+      bool bok = kok && r < it.ncols;
+      cp_async4(As + col * kTLds + r, aok ? g + it.a_row0 + r + coff : g, aok ? 4 : 0);
+      cp_async4(Bs + col * kTLds + r, bok ? g + it.b_row0 + r + coff : g, bok ? 4 : 0);
+    }
+  };
+
+  float acc[4][4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc[i][j][q] = 0.f;
+
+  const int nk = (it.kn + kTK - 1) / kTK;
+#pragma unroll
+  for (int st = 0; st < kTStages - 1; ++st) {
+    if (st < nk) load_stage(st, st * kTK);
+    cp_commit();
+  }
+  for (int kt = 0; kt < nk; ++kt) {
+    cp_wait<kTStages - 2>();
+    __syncthreads();
+    const int nxt = kt + kTStages - 1;
+    if (nxt < nk) load_stage(nxt % kTStages, nxt * kTK);
+    cp_commit();
+    const float* As = pipe + (size_t)(kt % kTStages) * 2 * kTK * kTLds;
+    const float* Bs = As + kTK * kTLds;
+#pragma unroll
+    for (int ks = 0; ks < kTK; ks += 8) {
+      uint32_t ahi[4][4], alo[4][4], bhi[4][2], blo[4][2];
+      const float* A0 = As + (ks + tq) * kTLds + wm * 64 + gq;
+      const float* A4 = A0 + 4 * kTLds;
+      const float* B0 = Bs + (ks + tq) * kTLds + wn * 32 + gq;
+      const float* B4 = B0 + 4 * kTLds;
+#pragma unroll
+      for (int mi = 0; mi < 4; ++mi) {
+        split_tf32(A0[mi * 16], ahi[mi][0], alo[mi][0]);
+        split_tf32(A0[mi * 16 + 8], ahi[mi][1], alo[mi][1]);
+        split_tf32(A4[mi * 16], ahi[mi][2], alo[mi][2]);
+        split_tf32(A4[mi * 16 + 8], ahi[mi][3], alo[mi][3]);
+      }
+#pragma unroll
+      for (int ni = 0; ni < 4; ++ni) {
+        split_tf32(B0[ni * 8], bhi[ni][0], blo[ni][0]);
+        split_tf32(B4[ni * 8], bhi[ni][1], blo[ni][1]);
+      }
+#pragma unroll
+      for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni) {
+          mma_tf32(acc[mi][ni], alo[mi], bhi[ni]);
+          mma_tf32(acc[mi][ni], ahi[mi], blo[ni]);
+          mma_tf32(acc[mi][ni], ahi[mi], bhi[ni]);
+        }
+    }
+  }
+  cp_wait<0>();
+  __syncthreads();
+#pragma unroll
+  for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+    for (int ni = 0; ni < 4; ++ni) {
+      int r0 = wm * 64 + mi * 16 + gq, c0 = wn * 32 + ni * 8 + 2 * tq;
+      Cs[r0 + c0 * kTLdc] = acc[mi][ni][0];
+      Cs[r0 + (c0 + 1) * kTLdc] = acc[mi][ni][1];
+      Cs[r0 + 8 + c0 * kTLdc] = acc[mi][ni][2];
+      Cs[r0 + 8 + (c0 + 1) * kTLdc] = acc[mi][ni][3];
+    }
+  __syncthreads();
+  tile_epilogue<128, 128, 256, float, float>(a, it, m, Cs, kTLdc, ints, ints + 128, ints + 256, ints + 384);
 }
 
 }  // namespace
 
 void init_gemm_attributes() {
+  cudaFuncSetAttribute(k_gemm_tf32x3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTSmemBytes);
   cudaFuncSetAttribute(k_gemm_dmma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDSmemBytes);
 }
 
 void launch_gemm(cudaStream_t st, const FactorArgs& a, const TileItem* items, int count, int tile) {
   if (count <= 0) return;
-  if (tile == 128) k_gemm_dmma<<<count, kDThreads, kDSmemBytes, st>>>(a, items);
-  else k_gemm_simt<<<count, 256, kSSmemBytes, st>>>(a, items);
+  if (a.fp32) {
+    if (tile == 128) k_gemm_tf32x3<<<count, 256, kTSmemBytes, st>>>(a, items);
+    else k_gemm_simt<float><<<count, 256, kSSmemBytes, st>>>(a, items);
+  } else {
+    if (tile == 128) k_gemm_dmma<<<count, kDThreads, kDSmemBytes, st>>>(a, items);
+    else k_gemm_simt<double><<<count, 256, kSSmemBytes, st>>>(a, items);
+  }
 }
 
 }  // namespace dev

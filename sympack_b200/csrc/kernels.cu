@@ -52,27 +52,29 @@ __device__ void panel_cholesky_smem(double* P, int h, int w, int ldp, Status* st
   }
 }
 
-__global__ void k_assemble(double* __restrict__ L, const int64_t* __restrict__ dst,
-                           const double* __restrict__ vals, int64_t nnz) {
+template <class T>
+__global__ void k_assemble(T* __restrict__ L, const int64_t* __restrict__ dst, const double* __restrict__ vals,
+                           int64_t nnz) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nnz; i += (int64_t)gridDim.x * blockDim.x)
-    L[dst[i]] = vals[i];
+    L[dst[i]] = (T)vals[i];
 }
 
+template <class T>
 __global__ void __launch_bounds__(128) k_factor_small(FactorArgs a, const int32_t* __restrict__ items) {
   extern __shared__ double P[];
   const int s = items[blockIdx.x];
   const SnMeta m = a.meta[s];
   const int h = m.h, w = m.w;
-  double* g = a.L + m.off;
+  T* g = static_cast<T*>(a.L) + m.off;
   for (int idx = threadIdx.x; idx < h * w; idx += blockDim.x) {
     int c = idx / h, r = idx - c * h;
-    P[idx] = g[r + (int64_t)c * m.ld];
+    P[idx] = (double)g[r + (int64_t)c * m.ld];
   }
   __syncthreads();
   panel_cholesky_smem(P, h, w, h, a.status, s, m.fc);
   for (int idx = threadIdx.x; idx < h * w; idx += blockDim.x) {
     int c = idx / h, r = idx - c * h;
-    g[r + (int64_t)c * m.ld] = P[idx];
+    g[r + (int64_t)c * m.ld] = (T)P[idx];
   }
 }
 
@@ -81,17 +83,19 @@ constexpr int kNB = 64;
 // POTRF of one 64-column diagonal block [c0, c0+nb) of a wide panel (one CTA
 // per item), blocked by 16: warp 0 factors each 16 x 16 diagonal piece, then
 // the rows below are solved against it and the trailing block is updated.  The
-// CTA also writes W = L11^-1 (64 x 64, column-major) to its scratch slot, so the
-// TRSM of the rows below becomes the product R W^T.  A block narrower than 64
-// is padded with the identity.
+// CTA also copies the factored block (FP64) and 1/L_kk to its scratch slot, from
+// where the TRSM of the rows below reads them.  A block narrower than 64 is
+// padded with the identity.
 constexpr int kDL = kNB + 1;  // padded leading dimension in shared memory
+constexpr size_t kSlot = (size_t)kNB * kNB + kNB;  // scratch slot: factored block (FP64) + 1/L_kk
 
+template <class T>
 __global__ void __launch_bounds__(256, 1) k_potrf_diag(FactorArgs a, const PanelItem* __restrict__ items,
                                                     double* __restrict__ winv) {
   __shared__ double D[kNB * kDL];
   const PanelItem it = items[blockIdx.x];
   const SnMeta m = a.meta[it.s];
-  double* g = a.L + m.off;
+  T* g = static_cast<T*>(a.L) + m.off;
   const int nb = it.nb, c0 = it.c0;
   const int64_t ld = m.ld;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -99,7 +103,7 @@ __global__ void __launch_bounds__(256, 1) k_potrf_diag(FactorArgs a, const Panel
     int c = idx / kNB, r = idx - c * kNB;
     double v = 0.0;
     if (r < nb && c < nb) {
-      if (r >= c) v = g[(c0 + r) + (int64_t)(c0 + c) * ld];
+      if (r >= c) v = (double)g[(c0 + r) + (int64_t)(c0 + c) * ld];
     } else if (r == c) {
       v = 1.0;
     }
@@ -167,76 +171,79 @@ __global__ void __launch_bounds__(256, 1) k_potrf_diag(FactorArgs a, const Panel
   }
   for (int idx = tid; idx < nb * nb; idx += blockDim.x) {
     int c = idx / nb, r = idx - c * nb;
-    if (r >= c) g[(c0 + r) + (int64_t)(c0 + c) * ld] = D[r + c * kDL];
+    if (r >= c) g[(c0 + r) + (int64_t)(c0 + c) * ld] = (T)D[r + c * kDL];
   }
-  // W = L^-1, column j by thread j: W[j][j] = 1/L_jj, W[i][j] = -(sum_{k=j}^{i-1} L[i][k] W[k][j]) / L_ii
-  if (winv && tid < kNB) {
-    double* W = winv + (size_t)it.slot * kNB * kNB;
-    const int j = tid;
-    double w[kNB];
-#pragma unroll
-    for (int i = 0; i < kNB; ++i) {
-      double t0 = 0.0, t1 = 0.0;
-#pragma unroll
-      for (int k = 0; k < i; k += 2) {
-        if (k >= j) t0 = fma(D[i + k * kDL], w[k], t0);
-        if (k + 1 < i && k + 1 >= j) t1 = fma(D[i + (k + 1) * kDL], w[k + 1], t1);
-      }
-      w[i] = (i > j) ? -(t0 + t1) * Rinv[i] : (i == j ? Rinv[i] : 0.0);
+  // FP64 copy of the factored block and 1/L_kk for the TRSM of the rows below
+  if (winv) {
+    double* W = winv + (size_t)it.slot * kSlot;
+    for (int idx = tid; idx < kNB * kNB; idx += blockDim.x) {
+      int c = idx / kNB, r = idx - c * kNB;
+      W[idx] = D[r + c * kDL];
     }
-    double* q = W + (size_t)j * kNB;
-    asm volatile("" : "+l"(q));
-#pragma unroll
-    for (int i = 0; i < kNB; ++i) q[i] = w[i];
+    if (tid < kNB) W[kNB * kNB + tid] = Rinv[tid];
   }
 }
 
-// TRSM of one 64-row tile below a factored diagonal block: R <- R W^T with
-// W = L11^-1 from the scratch slot (64 x 64 FMA tile, 4 x 4 outputs per thread).
+// TRSM of one 64-row tile below a factored diagonal block, R <- R L11^-T, by
+// 16-column pieces: each row solves against the 16 x 16 diagonal piece (one
+// thread per row), then the remaining columns of the tile are updated with the
+// solved piece (all threads).  L11 and 1/L_kk come from the scratch slot.
+template <class T>
 __global__ void __launch_bounds__(256) k_trsm_rows(FactorArgs a, const PanelItem* __restrict__ items,
                                                    const double* __restrict__ winv) {
   extern __shared__ double smem_tr[];
-  double* R = smem_tr;              // R[r + k*kDL]
-  double* Wt = smem_tr + kNB * kDL; // Wt[k + j*kDL] = W[j][k]
+  double* R = smem_tr;               // R[r + k*kDL]
+  double* D = smem_tr + kNB * kDL;   // D[i + j*kDL] = L11[i][j]
+  __shared__ double Rinv[kNB];
   const PanelItem it = items[blockIdx.x];
   const SnMeta m = a.meta[it.s];
-  double* g = a.L + m.off;
+  T* g = static_cast<T*>(a.L) + m.off;
   const int nb = it.nb, c0 = it.c0;
   const int64_t ld = m.ld;
   const int rows = min(kNB, m.h - it.row0);
-  const double* W = winv + (size_t)it.slot * kNB * kNB;
-  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  const double* W = winv + (size_t)it.slot * kSlot;
+  const int tid = threadIdx.x;
   for (int idx = tid; idx < kNB * kNB; idx += blockDim.x) {
     int k = idx / kNB, r = idx - k * kNB;
-    R[r + k * kDL] = (r < rows && k < nb) ? g[(it.row0 + r) + (int64_t)(c0 + k) * ld] : 0.0;
-    // W column-major: W[i][jcol] at i + jcol*64; Wt[k + j*kDL] = W[j][k] = W[j + k*64]
-    Wt[k + r * kDL] = W[r + k * kNB];
+    R[r + k * kDL] = (r < rows && k < nb) ? (double)g[(it.row0 + r) + (int64_t)(c0 + k) * ld] : 0.0;
+    D[r + k * kDL] = W[idx];
   }
+  if (tid < kNB) Rinv[tid] = W[kNB * kNB + tid];
   __syncthreads();
-  double acc[4][4];
+  for (int kb = 0; kb < nb; kb += 16) {
+    if (tid < rows) {
+      double x[16];
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
+      for (int j = 0; j < 16; ++j) x[j] = R[tid + (kb + j) * kDL];
 #pragma unroll
-    for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
-#pragma unroll 4
-  for (int k = 0; k < kNB; ++k) {
-    double rv[4], wv[4];
+      for (int k = 0; k < 16; ++k) {
+        double t0 = x[k], t1 = 0.0;
 #pragma unroll
-    for (int i = 0; i < 4; ++i) rv[i] = R[(ty + 16 * i) + k * kDL];
+        for (int j = 0; j + 1 < k; j += 2) {
+          t0 = fma(-x[j], D[kb + k + (kb + j) * kDL], t0);
+          t1 = fma(-x[j + 1], D[kb + k + (kb + j + 1) * kDL], t1);
+        }
+        if (k & 1) t0 = fma(-x[k - 1], D[kb + k + (kb + k - 1) * kDL], t0);
+        x[k] = (t0 + t1) * Rinv[kb + k];
+      }
 #pragma unroll
-    for (int j = 0; j < 4; ++j) wv[j] = Wt[k + (tx + 16 * j) * kDL];
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-      for (int j = 0; j < 4; ++j) acc[i][j] = fma(rv[i], wv[j], acc[i][j]);
-  }
-#pragma unroll
-  for (int i = 0; i < 4; ++i)
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      int r = ty + 16 * i, c = tx + 16 * j;
-      if (r < rows && c < nb) g[(it.row0 + r) + (int64_t)(c0 + c) * ld] = acc[i][j];
+      for (int j = 0; j < 16; ++j) R[tid + (kb + j) * kDL] = x[j];
     }
+    __syncthreads();
+    const int rest = kNB - kb - 16;
+    for (int idx = tid; idx < rows * rest; idx += blockDim.x) {
+      int j = kb + 16 + idx / rows, r = idx % rows;
+      double t = R[r + j * kDL];
+#pragma unroll
+      for (int k = 0; k < 16; ++k) t = fma(-R[r + (kb + k) * kDL], D[j + (kb + k) * kDL], t);
+      R[r + j * kDL] = t;
+    }
+    __syncthreads();
+  }
+  for (int idx = tid; idx < rows * nb; idx += blockDim.x) {
+    int k = idx / rows, r = idx - k * rows;
+    g[(it.row0 + r) + (int64_t)(c0 + k) * ld] = (T)R[r + k * kDL];
+  }
 }
 
 __global__ void k_permute_in(double* X, int64_t ldx, const double* B, int64_t ldb, const int32_t* invp0, int n,
@@ -271,22 +278,34 @@ void launch_assemble(cudaStream_t st, double* L, const int64_t* dst, const doubl
 }
 
 void init_kernel_attributes() {
-  cudaFuncSetAttribute(k_trsm_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * kNB * kDL * (int)sizeof(double));
+  for (auto f : {k_trsm_rows<double>, k_trsm_rows<float>})
+    cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * kNB * kDL * (int)sizeof(double));
+  for (auto f : {k_factor_small<double>, k_factor_small<float>})
+    cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
   init_gemm_attributes();
   init_solve_attributes();
-  cudaFuncSetAttribute(k_factor_small, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
+}
+
+void launch_assemble(cudaStream_t st, void* L, bool fp32, const int64_t* dst, const double* vals, int64_t nnz) {
+  if (nnz <= 0) return;
+  if (fp32) k_assemble<float><<<grid_for(nnz, 256), 256, 0, st>>>(static_cast<float*>(L), dst, vals, nnz);
+  else k_assemble<double><<<grid_for(nnz, 256), 256, 0, st>>>(static_cast<double*>(L), dst, vals, nnz);
 }
 
 void launch_factor_small(cudaStream_t st, const FactorArgs& a, const int32_t* items, int count, int smem_bytes) {
-  k_factor_small<<<count, 128, smem_bytes, st>>>(a, items);
+  if (a.fp32) k_factor_small<float><<<count, 128, smem_bytes, st>>>(a, items);
+  else k_factor_small<double><<<count, 128, smem_bytes, st>>>(a, items);
 }
 
 void launch_potrf_diag(cudaStream_t st, const FactorArgs& a, const PanelItem* items, int count, double* winv) {
-  k_potrf_diag<<<count, 256, 0, st>>>(a, items, winv);
+  if (a.fp32) k_potrf_diag<float><<<count, 256, 0, st>>>(a, items, winv);
+  else k_potrf_diag<double><<<count, 256, 0, st>>>(a, items, winv);
 }
 
 void launch_trsm_rows(cudaStream_t st, const FactorArgs& a, const PanelItem* items, int count, const double* winv) {
-  k_trsm_rows<<<count, 256, 2 * kNB * kDL * sizeof(double), st>>>(a, items, winv);
+  const size_t smem = 2 * kNB * kDL * sizeof(double);
+  if (a.fp32) k_trsm_rows<float><<<count, 256, smem, st>>>(a, items, winv);
+  else k_trsm_rows<double><<<count, 256, smem, st>>>(a, items, winv);
 }
 
 void launch_permute_in(cudaStream_t st, double* X, int64_t ldx, const double* B, int64_t ldb,

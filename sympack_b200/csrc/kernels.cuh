@@ -18,21 +18,23 @@ struct Status {
 
 // Arguments shared by the factor kernels.
 struct FactorArgs {
-  double* L;                 // factor arena
+  void* L;                   // factor arena: double, or float when fp32
   const SnMeta* meta;        // nsuper
   const int32_t* rows;       // concatenated 0-based row lists
   const int32_t* supmember;  // 0-based supernode of each permuted column
   Status* status;
+  bool fp32;                 // FP32 factor storage (precision form)
 };
 
 // Must run once per process (per device) before the first launch or capture.
 void init_kernel_attributes();
 void init_gemm_attributes();
-void launch_assemble(cudaStream_t st, double* L, const int64_t* dst, const double* vals, int64_t nnz);
+void launch_assemble(cudaStream_t st, void* L, bool fp32, const int64_t* dst, const double* vals, int64_t nnz);
 void launch_factor_small(cudaStream_t st, const FactorArgs& a, const int32_t* items, int count, int smem_bytes);
-// winv: scratch of (diagonal blocks per step) x 64 x 64 doubles; slot per PanelItem
+// winv: scratch of (diagonal blocks per step) x (64 x 64 + 64) doubles: factored block and 1/L_kk
 void launch_potrf_diag(cudaStream_t st, const FactorArgs& a, const PanelItem* items, int count, double* winv);
 void launch_trsm_rows(cudaStream_t st, const FactorArgs& a, const PanelItem* items, int count, const double* winv);
+// tile 64: FMA tiles (FP64 or FP32); tile 128: tensor-core tiles (FP64 DMMA, or 3xTF32 for FP32)
 void launch_gemm(cudaStream_t st, const FactorArgs& a, const TileItem* items, int count, int tile);
 
 // Solves work on the permuted right-hand sides X (n x nrhs, column-major, leading dimension ldx).
@@ -41,7 +43,8 @@ void launch_gemm(cudaStream_t st, const FactorArgs& a, const TileItem* items, in
 // zero at launch; expected[s] is the number of forward off-diagonal tiles that
 // write rows of supernode s.
 struct PSolveArgs {
-  const double* L;
+  const void* L;     // factor arena (double, or float when fp32)
+  bool fp32;
   const SnMeta* meta;
   const int32_t* rows;
   const int32_t* supmember;
@@ -60,6 +63,15 @@ struct PSolveArgs {
 };
 void init_solve_attributes();
 void launch_solve_persistent(cudaStream_t st, const PSolveArgs& a, bool forward);
+
+// Precision form (FP64 refinement): gather CSR values, residual r = b - A x,
+// per-column max |v| (out zeroed by the caller), max row sum of |A|, x += d.
+void launch_gather(cudaStream_t st, double* dst, const double* src, const int64_t* idx, int64_t n);
+void launch_residual(cudaStream_t st, const int64_t* rowptr, const int32_t* col, const double* val, const double* x,
+                     const double* b, double* r, int n, int nrhs, int64_t ld);
+void launch_colmax(cudaStream_t st, const double* v, int n, int nrhs, int64_t ld, double* out);
+void launch_rowsum_max(cudaStream_t st, const int64_t* rowptr, const double* val, int n, double* out);
+void launch_axpy(cudaStream_t st, double* x, const double* d, int n, int nrhs, int64_t ld);
 
 // X[invp[i], c] = B[i, c]   and   B[i, c] = X[invp[i], c]
 void launch_permute_in(cudaStream_t st, double* X, int64_t ldx, const double* B, int64_t ldb,

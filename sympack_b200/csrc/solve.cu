@@ -86,11 +86,12 @@ __device__ __forceinline__ void block_gemv_t(double* acc, const double* A, const
   }
 }
 
-// Stage L rows [r0, r0+m) x columns [c0, c0+kk) of a panel into A (ld kPld).
-__device__ __forceinline__ void stage_block(double* A, const double* P, int64_t ld, int r0, int m, int c0, int kk) {
+// Stage L rows [r0, r0+m) x columns [c0, c0+kk) of a panel into A (ld kPld), widened to FP64.
+template <class T>
+__device__ __forceinline__ void stage_block(double* A, const T* P, int64_t ld, int r0, int m, int c0, int kk) {
   for (int idx = threadIdx.x; idx < m * kk; idx += kThreads) {
     int k = idx / m, r = idx - k * m;
-    A[r + k * kPld] = P[(r0 + r) + (int64_t)(c0 + k) * ld];
+    A[r + k * kPld] = (double)P[(r0 + r) + (int64_t)(c0 + k) * ld];
   }
 }
 
@@ -141,6 +142,7 @@ __device__ void block_trsv(double* acc, const double* A, int kk, int nr) {
   }
 }
 
+template <class T>
 __global__ void __launch_bounds__(kThreads) k_solve_forward(PSolveArgs a) {
   extern __shared__ __align__(16) double sm[];
   double* Ab = sm;                  // staged L block, ld kPld
@@ -163,7 +165,7 @@ __global__ void __launch_bounds__(kThreads) k_solve_forward(PSolveArgs a) {
     const SolveTask task = a.tasks[tk];
     const int s = task.s;
     const SnMeta m = a.meta[s];
-    const double* P = a.L + m.off;
+    const T* P = static_cast<const T*>(a.L) + m.off;
     const int32_t* rl = a.rows + m.lidx;
     const int64_t ld = m.ld;
     if (task.idx >= 0) {
@@ -223,6 +225,7 @@ __global__ void __launch_bounds__(kThreads) k_solve_forward(PSolveArgs a) {
   }
 }
 
+template <class T>
 __global__ void __launch_bounds__(kThreads) k_solve_backward(PSolveArgs a) {
   extern __shared__ __align__(16) double sm[];
   double* Ab = sm;
@@ -245,7 +248,7 @@ __global__ void __launch_bounds__(kThreads) k_solve_backward(PSolveArgs a) {
     const SolveTask task = a.tasks[tk];
     const int s = task.s;
     const SnMeta m = a.meta[s];
-    const double* P = a.L + m.off;
+    const T* P = static_cast<const T*>(a.L) + m.off;
     const int32_t* rl = a.rows + m.lidx;
     const int64_t ld = m.ld;
     const int nblk = (m.w + kT - 1) / kT;
@@ -291,12 +294,12 @@ int g_solve_grid = 0;
 }  // namespace
 
 void init_solve_attributes() {
-  cudaFuncSetAttribute(k_solve_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes);
-  cudaFuncSetAttribute(k_solve_backward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes);
+  for (auto f : {k_solve_forward<double>, k_solve_backward<double>, k_solve_forward<float>, k_solve_backward<float>})
+    cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes);
   int dev = 0, sms = 0, per = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_solve_forward, kThreads, kSmemBytes);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_solve_forward<double>, kThreads, kSmemBytes);
   g_solve_grid = sms * (per > 0 ? per : 1);
   if (g_solve_grid <= 0) g_solve_grid = 148;
 }
@@ -304,8 +307,13 @@ void init_solve_attributes() {
 void launch_solve_persistent(cudaStream_t st, const PSolveArgs& a, bool forward) {
   if (a.ntasks <= 0 || a.spin_limit <= 0) return;
   int grid = g_solve_grid < a.ntasks ? g_solve_grid : a.ntasks;
-  if (forward) k_solve_forward<<<grid, kThreads, kSmemBytes, st>>>(a);
-  else k_solve_backward<<<grid, kThreads, kSmemBytes, st>>>(a);
+  if (a.fp32) {
+    if (forward) k_solve_forward<float><<<grid, kThreads, kSmemBytes, st>>>(a);
+    else k_solve_backward<float><<<grid, kThreads, kSmemBytes, st>>>(a);
+  } else {
+    if (forward) k_solve_forward<double><<<grid, kThreads, kSmemBytes, st>>>(a);
+    else k_solve_backward<double><<<grid, kThreads, kSmemBytes, st>>>(a);
+  }
 }
 
 }  // namespace dev

@@ -1,0 +1,78 @@
+"""Precision form: FP32 factor (3xTF32 tensor-core updates, FP64 diagonal pivots)
+plus FP64 iterative refinement.  Every solution must reach backward error
+eta = ||b - A x||_inf / (||A||_inf ||x||_inf + ||b||_inf) <= 1e-12, measured here
+against the FP64 matrix, and agree with the FP64 oracle solution to the forward
+error that backward error allows (kappa * 1e-12)."""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import numeric
+from sympack_b200 import DistSparseMatrix, SymPACKError, generators as G, symPACKMatrix2D, symPACKOptions
+
+pytestmark = pytest.mark.gpu
+
+
+def backward_error(A, x, b):
+    n = A.size
+    r = (b - A.matvec(x)).reshape(n, -1)
+    cols = np.repeat(np.arange(n), np.diff(A.colptr))
+    rows = A.rowind - 1
+    rs = np.zeros(n)
+    np.add.at(rs, rows, np.abs(A.nzvalLocal))
+    off = rows != cols
+    np.add.at(rs, cols[off], np.abs(A.nzvalLocal[off]))
+    x2, b2 = x.reshape(n, -1), b.reshape(n, -1)
+    return float((np.abs(r).max(0) / (rs.max() * np.abs(x2).max(0) + np.abs(b2).max(0))).max())
+
+
+def factor(A, precision, **kw):
+    M = symPACKMatrix2D()
+    M.Init(symPACKOptions(device=0, precision=precision, **kw))
+    M.SymbolicFactorization(A)
+    M.DistributeMatrix(A)
+    M.Factorize()
+    return M
+
+
+@pytest.mark.parametrize("delta,fwd_tol", [(1e-2, 1e-9), (1e-5, 1e-6)])
+@pytest.mark.parametrize("k", [12, 18])
+def test_fp32_ir_reaches_fp64_backward_error(delta, fwd_tol, k):
+    n, cp, ri, v = G.stencil27(k, k, k, delta, seed=2)
+    A = DistSparseMatrix.from_lower_csc(n, cp, ri, v)
+    M = factor(A, "FP32_IR")
+    rng = np.random.default_rng(4)
+    for nrhs in (1, 16):
+        b = rng.standard_normal((n, nrhs))
+        M.Solve(b)
+        x = M.GetSolution(nrhs=nrhs)
+        inf = M.info()
+        assert inf.backward_error <= 1e-12
+        assert backward_error(A, x, b) <= 1e-12
+        # FP64 oracle solution on the same ordering
+        perm, invp = M.GetOrdering()
+        xl, li = M.GetStructure()
+        sym = dict(xsuper=M.GetSupernodalPartition(), xlindx=xl, lindx=li, supmember=M.GetSupMembership(), invp=invp)
+        f = numeric.OracleFactor(n, sym, threads=os.cpu_count())
+        f.distribute(cp, ri, v)
+        f.factorize()
+        xo = f.solve(b)
+        assert np.max(np.abs(x - xo)) / np.max(np.abs(xo)) <= fwd_tol
+
+
+def test_fp32_factor_close_to_fp64_factor():
+    n, cp, ri, v = G.stencil27(14, 14, 14, 1e-2, seed=3)
+    A = DistSparseMatrix.from_lower_csc(n, cp, ri, v)
+    L32 = factor(A, "FP32_IR").GetFactor()
+    L64 = factor(A, "FP64").GetFactor()
+    assert np.max(np.abs(L32 - L64)) / np.max(np.abs(L64)) <= 1e-5
+
+
+def test_refinement_cap_reports_not_converged():
+    n, cp, ri, v = G.stencil27(12, 12, 12, 1e-5, seed=2)
+    A = DistSparseMatrix.from_lower_csc(n, cp, ri, v)
+    M = factor(A, "FP32_IR", ir_max_iter=1, ir_tolerance=1e-16)
+    with pytest.raises(SymPACKError) as e:
+        M.Solve(np.ones(n))
+    assert e.value.code == -8  # SPB_ERR_NOT_CONVERGED
