@@ -47,6 +47,7 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--grid", type=int, default=60, help="grid edge of the 3D Laplacian (60 = the named workload)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-precision", action="store_true", help="skip the FP64 vs FP32+IR comparison")
     return ap.parse_args()
 
 
@@ -56,17 +57,14 @@ def build_matrix(k):
 
 
 def backward_error(A, x, b):
-    """||b - A x||_inf / (||A||_inf ||x||_inf + ||b||_inf), per right-hand side (max)."""
-    r = b - A.matvec(x)
+    """||b - A x||_inf / (||A||_inf ||x||_inf + ||b||_inf), per right-hand side (max), in FP64."""
+    import scipy.sparse as sp
     n = A.size
-    cols = np.repeat(np.arange(n), np.diff(A.colptr))
-    rows = A.rowind - 1
-    rowsum = np.zeros(n)
-    np.add.at(rowsum, rows, np.abs(A.nzvalLocal))
-    off = rows != cols
-    np.add.at(rowsum, cols[off], np.abs(A.nzvalLocal[off]))
-    anorm = rowsum.max()
-    r2, x2, b2 = r.reshape(n, -1), x.reshape(n, -1), b.reshape(n, -1)
+    L = sp.csc_matrix((A.nzvalLocal, A.rowind - 1, A.colptr - 1), shape=(n, n))
+    full = L + sp.tril(L, -1).T
+    r = b.reshape(n, -1) - full @ x.reshape(n, -1)
+    anorm = abs(full).sum(axis=1).max()
+    r2, x2, b2 = r, x.reshape(n, -1), b.reshape(n, -1)
     eta = np.abs(r2).max(0) / (anorm * np.abs(x2).max(0) + np.abs(b2).max(0))
     return float(eta.max())
 
@@ -213,6 +211,58 @@ def run_reference(args):
     return 0
 
 
+def precision_comparison(torch, dev, stream, grid=80, reps=2):
+    """Time-to-solution (DistributeMatrix + Factorize + Solve(nrhs=1)) of the plain FP64
+    path and of the FP32 factor + FP64 refinement on the 27-point stencil, for the two
+    diagonal shifts of the precision workload.  Same matrices, same ordering."""
+    from sympack_b200 import DistSparseMatrix, generators as G, symPACKMatrix2D, symPACKOptions
+    n, cp, ri, v = G.stencil27(grid, grid, grid, 1e-2, seed=0)
+    A = DistSparseMatrix.from_lower_csc(n, cp, ri, v)
+    handles = {}
+    for prec in ("FP64", "FP32_IR"):
+        M = symPACKMatrix2D()
+        M.Init(symPACKOptions(device=dev.index, precision=prec))
+        M.SymbolicFactorization(A)
+        M.SetStream(stream.cuda_stream)
+        handles[prec] = M
+    flops = handles["FP64"].info().flops_stat
+    b = torch.from_numpy(np.random.default_rng(0).standard_normal(n)).to(dev)
+    x = torch.empty_like(b)
+    out = {"workload": f"3D 27-point stencil {grid}^3 (n={n}), off-diagonals U[-1,0), seed 0, nrhs 1",
+           "flops_stat": flops}
+    for delta in (1e-2, 1e-5):
+        _, _, _, vd = G.stencil27(grid, grid, grid, delta, seed=0)
+        dv = torch.from_numpy(vd).to(dev)
+        res = {}
+        for prec, M in handles.items():
+            times = []
+            for r in range(reps + 1):
+                e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+                e0.record(stream)
+                M.DistributeMatrixDevice(dv.data_ptr())
+                M.Factorize()
+                e1.record(stream)
+                M.SolveDevice(b.data_ptr(), x.data_ptr(), 1, n)
+                e2.record(stream)
+                torch.cuda.synchronize()
+                if r:
+                    times.append((e0.elapsed_time(e1), e1.elapsed_time(e2)))
+            fac = min(t[0] for t in times)
+            sol = min(t[1] for t in times)
+            inf = M.info()
+            Ad = DistSparseMatrix.from_lower_csc(n, cp, ri, vd)
+            eta = backward_error(Ad, x.cpu().numpy(), b.cpu().numpy())
+            res[prec] = {"factor_ms": fac, "solve_ms": sol, "time_to_solution_ms": fac + sol,
+                         "factor_tflops": flops / (fac * 1e-3) / 1e12, "backward_error": eta,
+                         "ir_iterations": inf.ir_iterations if prec == "FP32_IR" else 0}
+        res["speedup_time_to_solution"] = res["FP64"]["time_to_solution_ms"] / res["FP32_IR"]["time_to_solution_ms"]
+        out[f"delta={delta:g}"] = res
+    for M in handles.values():
+        M.close()
+    torch.cuda.empty_cache()
+    return out
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -344,6 +394,10 @@ def run_ours(args):
     roofline_solve["frac"] = roofline_solve["achieved"] / roofline_solve["peak"]
     kernels = {k: {"ms": round(p["ms"], 4), "launches": p["launches"]} for k, p in prof.items() if p["launches"]}
 
+    precision = None
+    if not args.no_precision:
+        precision = precision_comparison(torch, dev, stream)
+
     cpu = None
     if world == 1 and rank == 0 and not args.no_cpu_baseline:
         sym = dict(xsuper=M.GetSupernodalPartition(), xlindx=M.GetStructure()[0], lindx=M.GetStructure()[1],
@@ -372,6 +426,7 @@ def run_ours(args):
             "backward_error": {"nrhs1": bwd1, "nrhs16": bwd16, "e2e_nrhs16": bwd_e2e},
             "latency_ms": {"p50": float(np.percentile(tot, 50)), "p99": float(np.percentile(tot, 99))},
             "roofline": roofline, "roofline_solve": roofline_solve, "kernels_profiled_step": kernels,
+            "precision_form": precision,
             "cpu_baseline": cpu,
             "e2e": {"value": world * flops * K / (e2e_ms * 1e-3) / 1e12, "unit": "TFLOP/s",
                     "h2d_bytes_per_step": int(A.nnz * 8 + n * 16 * 8), "d2h_bytes_per_step": int(n * 16 * 8),
