@@ -73,6 +73,8 @@ typedef struct spb_options {
   double ir_tolerance;     /* backward-error target of refinement (1e-12) */
   int ir_max_iter;         /* refinement iteration cap */
   int verbose;
+  int plan_small_max_w;    /* widest supernode factored whole in shared memory (0 = default 32) */
+  int plan_big_tile_rows;  /* products with this many rows use 128 x 128 tensor-core tiles (0 = default 128) */
 } spb_options;
 
 typedef struct spb_info {
@@ -101,6 +103,23 @@ const char* spb_last_error(const spb_handle* h);
 
 /* SymbolicFactorization: structure only (values not needed). */
 int spb_symbolic(spb_handle* h, int32_t n, const int64_t* colptr, const int32_t* rowind);
+/* Batching (no counterpart in the reference, which factors one matrix per
+ * symPACKMatrix2D object): nsys independent SPD systems given as one
+ * block-diagonal lower CSC; system k owns rows and columns
+ * sys_offsets[k] .. sys_offsets[k+1]-1 (0-based, sys_offsets[0] = 0,
+ * sys_offsets[nsys] = n).  Each system gets its own symbolic analysis, exactly
+ * as spb_symbolic would compute it (run in parallel host threads); the analyses
+ * are merged into one forest, so distribute / factorize / solve then handle
+ * every system of an elimination-tree level in the same launches.  Right-hand
+ * sides are the systems' right-hand sides stacked in the same order. */
+int spb_symbolic_batch(spb_handle* h, int32_t nsys, const int32_t* sys_offsets, int32_t n, const int64_t* colptr,
+                       const int32_t* rowind);
+/* Rebuild the device plan of the current analysis with other tile shapes
+ * (0 = default): supernodes up to small_max_w columns (<= 64) are factored
+ * whole in shared memory; update products with at least big_tile_rows rows use
+ * 128 x 128 tensor-core tiles.  The symbolic analysis is kept; values must be
+ * distributed again.  Used by the tile-shape autotuner. */
+int spb_replan(spb_handle* h, int32_t small_max_w, int32_t big_tile_rows);
 /* DistributeMatrix: values in the same order as rowind (host or device pointer). */
 int spb_distribute(spb_handle* h, const double* nzval);
 int spb_distribute_device(spb_handle* h, const double* d_nzval);

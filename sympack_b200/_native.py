@@ -43,6 +43,8 @@ class spb_options(C.Structure):
         ("ir_tolerance", C.c_double),
         ("ir_max_iter", C.c_int),
         ("verbose", C.c_int),
+        ("plan_small_max_w", C.c_int),
+        ("plan_big_tile_rows", C.c_int),
     ]
 
 
@@ -91,6 +93,8 @@ SIGNATURES = [
     ("spb_destroy", None, [_P]),
     ("spb_last_error", C.c_char_p, [_P]),
     ("spb_symbolic", C.c_int, [_P, C.c_int32, _I64P, _I32P]),
+    ("spb_symbolic_batch", C.c_int, [_P, C.c_int32, _I32P, C.c_int32, _I64P, _I32P]),
+    ("spb_replan", C.c_int, [_P, C.c_int32, C.c_int32]),
     ("spb_distribute", C.c_int, [_P, _DP]),
     ("spb_distribute_device", C.c_int, [_P, _P]),
     ("spb_factorize", C.c_int, [_P]),

@@ -8,7 +8,9 @@
 #include <cstdio>
 #include <cstring>
 #include <exception>
+#include <atomic>
 #include <mutex>
+#include <thread>
 #include <new>
 #include <stdexcept>
 #include <string>
@@ -460,7 +462,35 @@ void spb_destroy(spb_handle* h) {
 
 const char* spb_last_error(const spb_handle* h) { return h ? h->err.c_str() : "null handle"; }
 
-int spb_symbolic(spb_handle* h, int32_t n, const int64_t* colptr, const int32_t* rowind) {
+}  // extern "C"
+
+namespace {
+
+spb::RelaxParams relax_of(const spb_options& o) {
+  spb::RelaxParams rp;
+  rp.nrelax0 = o.nrelax0;
+  rp.nrelax1 = o.nrelax1;
+  rp.nrelax2 = o.nrelax2;
+  rp.maxSize = o.max_snode;
+  rp.zrelax0 = o.zrelax0;
+  rp.zrelax1 = o.zrelax1;
+  rp.zrelax2 = o.zrelax2;
+  if (rp.maxSize > 0) {  // RelaxationParameters::SetMaxSize (Types.hpp:63-70)
+    rp.nrelax0 = std::min(rp.nrelax0, rp.maxSize);
+    rp.nrelax1 = std::min(rp.nrelax1, rp.maxSize);
+    rp.nrelax2 = std::min(rp.nrelax2, rp.maxSize);
+  }
+  return rp;
+}
+
+spb::PlanParams plan_params_of(const spb_options& o) {
+  spb::PlanParams pp;
+  if (o.plan_small_max_w > 0) pp.small_max_w = o.plan_small_max_w;
+  if (o.plan_big_tile_rows > 0) pp.big_tile_rows = o.plan_big_tile_rows;
+  return pp;
+}
+
+int begin_symbolic(spb_handle* h, int32_t n, const int64_t* colptr, const int32_t* rowind) {
   if (check_handle(h)) return SPB_ERR_INVALID;
   if (n <= 0 || !colptr || !rowind) return fail(h, SPB_ERR_INVALID, "symbolic: empty matrix or null pointer");
   if (h->device >= 0) {
@@ -469,27 +499,17 @@ int spb_symbolic(spb_handle* h, int32_t n, const int64_t* colptr, const int32_t*
   }
   h->have_symbolic = h->have_values = h->factored = h->have_solution = false;
   h->cells_built = false;
+  h->nnz_a = colptr[n] - 1;
+  h->colptr.assign(colptr, colptr + n + 1);
+  h->rowind.assign(rowind, rowind + h->nnz_a);
+  return SPB_OK;
+}
+
+// Everything after the symbolic analysis: device plan, assembly map and the
+// handle's device buffers.  h->sym must hold the (possibly merged) analysis.
+int install_symbolic(spb_handle* h, int32_t n, const int64_t* colptr, const int32_t* rowind) {
   try {
-    h->nnz_a = colptr[n] - 1;
-    h->colptr.assign(colptr, colptr + n + 1);
-    h->rowind.assign(rowind, rowind + h->nnz_a);
-    spb::RelaxParams rp;
-    rp.nrelax0 = h->opt.nrelax0;
-    rp.nrelax1 = h->opt.nrelax1;
-    rp.nrelax2 = h->opt.nrelax2;
-    rp.maxSize = h->opt.max_snode;
-    rp.zrelax0 = h->opt.zrelax0;
-    rp.zrelax1 = h->opt.zrelax1;
-    rp.zrelax2 = h->opt.zrelax2;
-    if (rp.maxSize > 0) {  // RelaxationParameters::SetMaxSize (Types.hpp:63-70)
-      rp.nrelax0 = std::min(rp.nrelax0, rp.maxSize);
-      rp.nrelax1 = std::min(rp.nrelax1, rp.maxSize);
-      rp.nrelax2 = std::min(rp.nrelax2, rp.maxSize);
-    }
-    h->sym = spb::symbolic_factorization(n, colptr, rowind, (spb::OrderingKind)h->opt.ordering, rp, h->opt.user_perm);
-    h->plan = spb::build_plan(h->sym);
-  } catch (const std::invalid_argument& e) {
-    return fail(h, SPB_ERR_INVALID, e.what());
+    h->plan = spb::build_plan(h->sym, plan_params_of(h->opt));
   } catch (const std::bad_alloc&) {
     return fail(h, SPB_ERR_OOM, "symbolic: host allocation failed");
   } catch (const std::exception& e) {
@@ -594,6 +614,96 @@ int spb_symbolic(spb_handle* h, int32_t n, const int64_t* colptr, const int32_t*
   SPB_CK(h, cudaStreamSynchronize(h->stream));
   h->have_symbolic = true;
   return SPB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int spb_symbolic(spb_handle* h, int32_t n, const int64_t* colptr, const int32_t* rowind) {
+  int rc = begin_symbolic(h, n, colptr, rowind);
+  if (rc) return rc;
+  try {
+    h->sym = spb::symbolic_factorization(n, colptr, rowind, (spb::OrderingKind)h->opt.ordering, relax_of(h->opt),
+                                         h->opt.user_perm);
+  } catch (const std::invalid_argument& e) {
+    return fail(h, SPB_ERR_INVALID, e.what());
+  } catch (const std::bad_alloc&) {
+    return fail(h, SPB_ERR_OOM, "symbolic: host allocation failed");
+  } catch (const std::exception& e) {
+    return fail(h, SPB_ERR_STRUCTURE, e.what());
+  }
+  return install_symbolic(h, n, colptr, rowind);
+}
+
+int spb_replan(spb_handle* h, int32_t small_max_w, int32_t big_tile_rows) {
+  if (check_handle(h)) return SPB_ERR_INVALID;
+  if (!h->have_symbolic) return fail(h, SPB_ERR_STATE, "replan: no symbolic analysis");
+  if (small_max_w < 0 || small_max_w > 64 || big_tile_rows < 0)
+    return fail(h, SPB_ERR_INVALID, "replan: small_max_w must be in [0, 64], big_tile_rows >= 0");
+  h->opt.plan_small_max_w = small_max_w;
+  h->opt.plan_big_tile_rows = big_tile_rows;
+  if (h->device >= 0) {
+    SPB_CK(h, cudaSetDevice(h->device));
+    release_device(h);
+  }
+  h->have_symbolic = h->have_values = h->factored = h->have_solution = false;
+  return install_symbolic(h, h->sym.n, h->colptr.data(), h->rowind.data());
+}
+
+int spb_symbolic_batch(spb_handle* h, int32_t nsys, const int32_t* sys_offsets, int32_t n, const int64_t* colptr,
+                       const int32_t* rowind) {
+  if (check_handle(h)) return SPB_ERR_INVALID;
+  if (nsys <= 0 || !sys_offsets) return fail(h, SPB_ERR_INVALID, "symbolic_batch: no systems");
+  if (h->opt.ordering == SPB_ORDERING_USER)
+    return fail(h, SPB_ERR_INVALID, "symbolic_batch: USER ordering is per matrix; use MMD or NATURAL");
+  int rc = begin_symbolic(h, n, colptr, rowind);
+  if (rc) return rc;
+  if (sys_offsets[0] != 0 || sys_offsets[nsys] != n) return fail(h, SPB_ERR_INVALID, "symbolic_batch: bad offsets");
+  for (int k = 0; k < nsys; ++k)
+    if (sys_offsets[k + 1] <= sys_offsets[k]) return fail(h, SPB_ERR_INVALID, "symbolic_batch: empty system");
+  // each system's columns may only hold rows of the same system (block-diagonal matrix)
+  for (int k = 0; k < nsys; ++k)
+    for (int c = sys_offsets[k] + 1; c <= sys_offsets[k + 1]; ++c)
+      for (int64_t p = colptr[c - 1]; p < colptr[c]; ++p)
+        if (rowind[p - 1] > sys_offsets[k + 1])
+          return fail(h, SPB_ERR_INVALID, "symbolic_batch: entry couples two systems");
+  std::vector<spb::Symbolic> parts(nsys);
+  std::vector<std::string> errors(nsys);
+  const spb::RelaxParams rp = relax_of(h->opt);
+  const spb::OrderingKind ord = (spb::OrderingKind)h->opt.ordering;
+  std::atomic<int> next{0};
+  auto worker = [&]() {
+    std::vector<int64_t> cp;
+    std::vector<int32_t> ri;
+    for (int k = next++; k < nsys; k = next++) {
+      const int o = sys_offsets[k], nk = sys_offsets[k + 1] - o;
+      const int64_t p0 = colptr[o];
+      cp.assign(nk + 1, 0);
+      for (int c = 0; c <= nk; ++c) cp[c] = colptr[o + c] - p0 + 1;
+      ri.resize(cp[nk] - 1);
+      for (int64_t p = 0; p < cp[nk] - 1; ++p) ri[p] = rowind[p0 - 1 + p] - o;
+      try {
+        parts[k] = spb::symbolic_factorization(nk, cp.data(), ri.data(), ord, rp);
+      } catch (const std::exception& e) {
+        errors[k] = e.what();
+      }
+    }
+  };
+  unsigned nthreads = std::max(1u, std::min<unsigned>(std::thread::hardware_concurrency(), (unsigned)nsys));
+  std::vector<std::thread> pool;
+  for (unsigned t = 0; t + 1 < nthreads; ++t) pool.emplace_back(worker);
+  worker();
+  for (std::thread& t : pool) t.join();
+  for (int k = 0; k < nsys; ++k)
+    if (!errors[k].empty())
+      return fail(h, SPB_ERR_INVALID, "symbolic_batch: system " + std::to_string(k) + ": " + errors[k]);
+  try {
+    h->sym = spb::merge_symbolic(parts);
+  } catch (const std::exception& e) {
+    return fail(h, SPB_ERR_INVALID, e.what());
+  }
+  return install_symbolic(h, n, colptr, rowind);
 }
 
 static int distribute_common(spb_handle* h) {

@@ -1049,4 +1049,52 @@ Symbolic symbolic_factorization(int n, const int64_t* colptr, const int32_t* row
   return s;
 }
 
+Symbolic merge_symbolic(const std::vector<Symbolic>& parts) {
+  Symbolic m;
+  int64_t n = 0, nsup = 0, nl = 0;
+  for (const Symbolic& p : parts) {
+    n += p.n;
+    nsup += p.nsuper();
+    nl += (int64_t)p.lindx.size();
+  }
+  if (n > 2000000000LL) throw std::invalid_argument("batch too large for 32-bit indices");
+  m.n = (int)n;
+  m.perm.reserve(n);
+  m.invp.reserve(n);
+  m.mmd_invp.reserve(n);
+  m.parent.reserve(n);
+  m.cc_fund.reserve(n);
+  m.cc.reserve(n);
+  m.supmember.reserve(n);
+  m.xsuper.reserve(nsup + 1);
+  m.xlindx.reserve(nsup + 1);
+  m.lindx.reserve(nl);
+  int32_t off = 0, soff = 0;
+  int64_t loff = 0;
+  for (const Symbolic& p : parts) {
+    for (int i = 0; i < p.n; ++i) {
+      m.perm.push_back(p.perm[i] + off);
+      m.invp.push_back(p.invp[i] + off);
+      m.mmd_invp.push_back(p.mmd_invp[i] + off);
+      m.parent.push_back(p.parent[i] ? p.parent[i] + off : 0);
+      m.cc_fund.push_back(p.cc_fund[i]);
+      m.cc.push_back(p.cc[i]);
+      m.supmember.push_back(p.supmember[i] + soff);
+    }
+    for (int s = 0; s < p.nsuper(); ++s) {
+      m.xsuper.push_back(p.xsuper[s] + off);
+      m.xlindx.push_back(p.xlindx[s] + loff);
+    }
+    for (int32_t r : p.lindx) m.lindx.push_back(r + off);
+    m.flops_stat += p.flops_stat;
+    m.nnzL_stat += p.nnzL_stat;
+    off += p.n;
+    soff += p.nsuper();
+    loff += (int64_t)p.lindx.size();
+  }
+  m.xsuper.push_back(off + 1);
+  m.xlindx.push_back(loff + 1);
+  return m;
+}
+
 }  // namespace spb

@@ -123,4 +123,9 @@ Symbolic symbolic_factorization(int n, const int64_t* colptr, const int32_t* row
                                 OrderingKind ordering, const RelaxParams& relax,
                                 const int32_t* user_perm = nullptr);
 
+// Batching: the symbolic results of independent systems, merged into the
+// symbolic result of their block-diagonal matrix (a forest whose trees are the
+// systems' elimination trees, each system's ordering kept as it is).
+Symbolic merge_symbolic(const std::vector<Symbolic>& parts);
+
 }  // namespace spb

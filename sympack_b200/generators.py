@@ -136,3 +136,51 @@ def config_matrix(name: str, **kw):
         k = int(name.split("_")[1])
         return stencil27(k, k, k, delta=kw.get("delta", 1e-2), seed=kw.get("seed", 0))
     raise ValueError(name)
+
+
+def batch_systems(count: int, n_min: int = 500, n_max: int = 20000, seed: int = 0):
+    """Independent SPD systems of uneven size, n log-uniform in [n_min, n_max].
+
+    Even-numbered systems are Laplacians on random grids (2D 5-point or 3D
+    7-point, shift 1e-3), odd-numbered ones random sparse graphs of average
+    degree 10 with off-diagonals U[-1, 0) and diagonal dominance 1.05.  The
+    grid systems get the grid size closest to the drawn n.  Returns a list of
+    (n, colptr, rowind, nzval)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(count):
+        target = int(round(np.exp(rng.uniform(np.log(n_min), np.log(n_max)))))
+        if k % 2 == 0:
+            if rng.uniform() < 0.5:
+                ar = rng.uniform(0.5, 2.0)
+                nx = max(2, int(round(np.sqrt(target * ar))))
+                ny = max(2, int(round(target / nx)))
+                out.append(laplacian_2d(nx, ny, 1e-3))
+            else:
+                a1, a2 = rng.uniform(0.7, 1.4, size=2)
+                base = (target / (a1 * a2)) ** (1.0 / 3.0)
+                nx = max(2, int(round(base * a1)))
+                ny = max(2, int(round(base * a2)))
+                nz = max(2, int(round(target / (nx * ny))))
+                out.append(laplacian_3d(nx, ny, nz, 1e-3))
+        else:
+            out.append(random_graph_spd(target, 10.0, 1.05, seed=int(rng.integers(1 << 31))))
+    return out
+
+
+def block_diagonal(systems):
+    """Stack systems [(n, colptr, rowind, nzval), ...] into one block-diagonal
+    lower CSC.  Returns (n, colptr, rowind, nzval, sys_offsets) with 0-based
+    system offsets (sys_offsets[k] = first row of system k, last = n)."""
+    offs = np.zeros(len(systems) + 1, np.int32)
+    for k, s in enumerate(systems):
+        offs[k + 1] = offs[k] + s[0]
+    n = int(offs[-1])
+    cps, ris, vals = [np.ones(1, np.int64)], [], []
+    base = 0
+    for k, (nk, cp, ri, v) in enumerate(systems):
+        cps.append(np.asarray(cp[1:], np.int64) - 1 + base + 1)
+        ris.append(np.asarray(ri, np.int32) + offs[k])
+        vals.append(np.asarray(v, np.float64))
+        base += len(ri)
+    return (n, np.concatenate(cps), np.concatenate(ris).astype(np.int32), np.concatenate(vals), offs)

@@ -88,6 +88,8 @@ class symPACKOptions:
     ir_max_iter: int = 30
     device: int = 0
     verbose: int = 0
+    plan_small_max_w: int = 0      # 0 = library default
+    plan_big_tile_rows: int = 0    # 0 = library default
 
     def to_c(self) -> N.spb_options:
         if self.orderingStr not in N.ORDERINGS:
@@ -107,6 +109,8 @@ class symPACKOptions:
         o.ir_tolerance = self.ir_tolerance
         o.ir_max_iter = self.ir_max_iter
         o.verbose = self.verbose
+        o.plan_small_max_w = self.plan_small_max_w
+        o.plan_big_tile_rows = self.plan_big_tile_rows
         return o
 
 
@@ -219,6 +223,19 @@ class symPACKMatrix2D:
         h = self._need()
         self._n = A.size
         _raise(self._lib.spb_symbolic(h, A.size, _i64(A.colptr), _i32(A.rowind)), "SymbolicFactorization", h)
+
+    def SymbolicFactorizationBatch(self, A: DistSparseMatrix, sys_offsets) -> None:
+        """Batching: A is block-diagonal; system k spans rows sys_offsets[k]..sys_offsets[k+1]-1."""
+        h = self._need()
+        self._n = A.size
+        offs = np.ascontiguousarray(sys_offsets, dtype=np.int32)
+        _raise(self._lib.spb_symbolic_batch(h, len(offs) - 1, _i32(offs), A.size, _i64(A.colptr), _i32(A.rowind)),
+               "SymbolicFactorizationBatch", h)
+
+    def Replan(self, small_max_w: int = 0, big_tile_rows: int = 0) -> None:
+        """Rebuild the device plan with other tile shapes; values must be distributed again."""
+        h = self._need()
+        _raise(self._lib.spb_replan(h, int(small_max_w), int(big_tile_rows)), "Replan", h)
 
     def DistributeMatrix(self, A: DistSparseMatrix) -> None:
         h = self._need()
