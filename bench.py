@@ -48,6 +48,13 @@ def parse():
     ap.add_argument("--grid", type=int, default=60, help="grid edge of the 3D Laplacian (60 = the named workload)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-precision", action="store_true", help="skip the FP64 vs FP32+IR comparison")
+    ap.add_argument("--batch-systems", type=int, default=300,
+                    help="systems of the batching workload (2000 = the named workload; host MMD of its random "
+                         "graphs takes minutes)")
+    ap.add_argument("--serve-requests", type=int, default=2000,
+                    help="requests of the serving workload (10000 = the named workload)")
+    ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--no-serve", action="store_true")
     return ap.parse_args()
 
 
@@ -263,6 +270,173 @@ def precision_comparison(torch, dev, stream, grid=80, reps=2):
     return out
 
 
+def per_system_backward_error(systems, offs, x, b):
+    from sympack_b200 import DistSparseMatrix
+    eta = 0.0
+    for k, s in enumerate(systems):
+        lo, hi = int(offs[k]), int(offs[k + 1])
+        eta = max(eta, backward_error(DistSparseMatrix.from_lower_csc(*s), x[lo:hi], b[lo:hi]))
+    return eta
+
+
+def batching_comparison(torch, dev, stream, count, seed=0, subset=64):
+    """Batching form: `count` uneven systems factored together (each etree level
+    of every system in the same launches), plans picked by the autotuner, in
+    FP64 and FP32 + refinement; beside it the first `subset` systems factored
+    one by one versus as one batch."""
+    from sympack_b200 import DistSparseMatrix, autotune, generators as G, symPACKMatrix2D, symPACKOptions
+    systems = G.batch_systems(count, 500, 20000, seed=seed)
+    n, cp, ri, v, offs = G.block_diagonal(systems)
+    A = DistSparseMatrix.from_lower_csc(n, cp, ri, v)
+    b = np.random.default_rng(seed).standard_normal((n, 1))
+    db = torch.from_numpy(b).to(dev)
+    dx = torch.empty_like(db)
+    out = {"workload": f"{count} SPD systems, n log-uniform [500, 20000]; even: 2D/3D Laplacians on random grids, "
+                       f"odd: random graphs avg degree 10, off-diagonals U[-1,0), dominance 1.05 (seed {seed})",
+           "systems": count, "n_total": n}
+    T = symPACKMatrix2D()
+    T.Init(symPACKOptions(device=-1))
+    t0 = time.perf_counter()
+    T.SymbolicFactorizationBatch(A, offs)
+    out["symbolic_s"] = time.perf_counter() - t0
+    inf = T.info()
+    flops = inf.flops_stat
+    out.update(flops_stat=flops, nnz_L=inf.nnz_l, nsuper=inf.nsuper, etree_levels=inf.nlevels,
+               max_width=inf.max_width)
+    for prec in ("FP64", "FP32_IR"):
+        M = symPACKMatrix2D()
+        M.Init(symPACKOptions(device=dev.index, precision=prec))
+        M.SymbolicFactorizationFrom(T)
+        tune = autotune.tune(M, A, offs, reps=1, use_cache=False)
+        M.SetStream(stream.cuda_stream)
+        times = []
+        for r in range(3):
+            M.DistributeMatrix(A)
+            e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+            e0.record(stream)
+            M.Factorize()
+            e1.record(stream)
+            M.SolveDevice(db.data_ptr(), dx.data_ptr(), 1, n)
+            e2.record(stream)
+            torch.cuda.synchronize()
+            if r:
+                times.append((e0.elapsed_time(e1), e1.elapsed_time(e2)))
+        fac = min(t[0] for t in times)
+        sol = min(t[1] for t in times)
+        mi = M.info()
+        out[prec] = {"factor_ms": fac, "solve_ms": sol, "factor_tflops": flops / (fac * 1e-3) / 1e12,
+                     "systems_per_s": count / ((fac + sol) * 1e-3),
+                     "backward_error_max_over_systems": per_system_backward_error(systems, offs, dx.cpu().numpy(), b),
+                     "ir_iterations": mi.ir_iterations if prec == "FP32_IR" else 0,
+                     "factor_launches": mi.factor_launches, "device_bytes": mi.device_bytes,
+                     "autotuned_plan": {"small_max_w": tune["small_max_w"], "big_tile_rows": tune["big_tile_rows"],
+                                        "candidates_ms": {k: round(v * 1e3, 3) for k, v in tune["times"].items()}}}
+        M.close()
+    T.close()
+    # one by one versus batched, on the first `subset` systems (FP64, default plan)
+    sub = systems[:subset]
+    sn, scp, sri, sv, soffs = G.block_diagonal(sub)
+    seq_ms = 0.0
+    for s in sub:
+        As = DistSparseMatrix.from_lower_csc(*s)
+        M = symPACKMatrix2D()
+        M.Init(symPACKOptions(device=dev.index))
+        M.SymbolicFactorization(As)
+        M.SetStream(stream.cuda_stream)
+        M.DistributeMatrix(As)
+        M.Factorize()  # graph capture outside the timing
+        M.DistributeMatrix(As)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        M.Factorize()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        seq_ms += e0.elapsed_time(e1)
+        M.close()
+    As = DistSparseMatrix.from_lower_csc(sn, scp, sri, sv)
+    M = symPACKMatrix2D()
+    M.Init(symPACKOptions(device=dev.index))
+    M.SymbolicFactorizationBatch(As, soffs)
+    M.SetStream(stream.cuda_stream)
+    M.DistributeMatrix(As)
+    M.Factorize()
+    M.DistributeMatrix(As)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    M.Factorize()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    out["one_by_one_vs_batched"] = {"systems": subset, "one_by_one_factor_ms": seq_ms,
+                                    "batched_factor_ms": e0.elapsed_time(e1),
+                                    "speedup": seq_ms / e0.elapsed_time(e1)}
+    M.close()
+    torch.cuda.empty_cache()
+    return out
+
+
+def serving_comparison(torch, dev, count, seed=0, load=2.0):
+    """Serving form: the request stream replayed through the continuous-batching
+    loop (FP32 + refinement, 8 slots, right-hand sides merged per factor) at
+    `load` times the request rate that back-to-back plain FP64 processing of the
+    same stream sustains; that back-to-back run is measured first."""
+    from sympack_b200 import serving as S
+    mk = lambda: S.request_stream(count, 1.0, seed=seed)
+    base_stream = mk()
+    patterns = {}
+    for _, r in base_stream:
+        if r.spec[0] is not None:
+            patterns[(r.spec[0].kind, r.spec[0].k)] = r.spec[0]
+    t0 = time.perf_counter()
+
+    def preload(svc):  # symbolic analyses of the stream's patterns, outside the timed region
+        from sympack_b200 import DistSparseMatrix
+        for P in patterns.values():
+            svc._ensure_pattern(DistSparseMatrix.from_lower_csc(P.n, P.colptr, P.rowind, P.base))
+        for f in list(svc._patterns.values()):
+            f.result()
+
+    base = S.SolverService(device=dev.index, precision="FP64", max_inflight=1, max_batch_rhs=1)
+    preload(base)
+    analyse_s = time.perf_counter() - t0
+    for _, r in base_stream:
+        r.keep = False
+    t0 = time.perf_counter()
+    for _, r in base_stream:  # back to back: each request starts when the previous one ends
+        base.submit(S.materialise(r)).result()
+    base_s = time.perf_counter() - t0
+    base.close()
+    base_rate = count / base_s
+    svc_stream = [(t / (load * base_rate), r) for t, r in mk()]
+    for _, r in svc_stream:
+        r.keep = False
+    svc = S.SolverService(device=dev.index, precision="FP32_IR", max_inflight=8, max_batch_rhs=64)
+    preload(svc)
+    wall = S.replay(svc, svc_stream, timeout=1800)
+    res = [r.future.result() for _, r in svc_stream]
+    svc.close()
+    lat = S.latency_summary([r for _, r in svc_stream])
+    svc_time = [r.t_done - r.t_start for _, r in base_stream]
+    torch.cuda.empty_cache()
+    return {
+        "workload": f"{count} requests, Poisson arrivals, 30% factor+solve on fresh 27-point stencil (delta 1e-2) "
+                    f"or 2D Laplacian matrices, n 1k-216k on a grid ladder, 70% solve-only against the 8 latest "
+                    f"factors, nrhs U{{1..64}} (seed {seed})",
+        "requests": count, "pattern_analysis_s": analyse_s,
+        "back_to_back_fp64": {"solves_per_s": base_rate, "wall_s": base_s,
+                              "service_p50_ms": float(np.percentile(svc_time, 50) * 1e3),
+                              "service_p99_ms": float(np.percentile(svc_time, 99) * 1e3)},
+        "continuous_batching_fp32_ir": {"arrival_rate_per_s": load * base_rate, "solves_per_s": count / wall,
+                                        "wall_s": wall, **lat,
+                                        "max_backward_error": max(x.backward_error for x in res),
+                                        "merged_solve_batches": int(svc.stats["solve_batches"]),
+                                        "solves_in_batches": int(svc.stats["solves"]),
+                                        "factorizations": int(svc.stats["factorizations"]),
+                                        "evictions": int(svc.stats["evictions"]),
+                                        "max_inflight": int(svc.stats["max_inflight"])},
+        "speedup_solves_per_s": (count / wall) / base_rate,
+    }
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -398,6 +572,13 @@ def run_ours(args):
     if not args.no_precision:
         precision = precision_comparison(torch, dev, stream)
 
+    batching = None
+    if not args.no_batch:
+        batching = batching_comparison(torch, dev, stream, args.batch_systems)
+    serving = None
+    if not args.no_serve:
+        serving = serving_comparison(torch, dev, args.serve_requests)
+
     cpu = None
     if world == 1 and rank == 0 and not args.no_cpu_baseline:
         sym = dict(xsuper=M.GetSupernodalPartition(), xlindx=M.GetStructure()[0], lindx=M.GetStructure()[1],
@@ -427,6 +608,8 @@ def run_ours(args):
             "latency_ms": {"p50": float(np.percentile(tot, 50)), "p99": float(np.percentile(tot, 99))},
             "roofline": roofline, "roofline_solve": roofline_solve, "kernels_profiled_step": kernels,
             "precision_form": precision,
+            "batching_form": batching,
+            "serving_form": serving,
             "cpu_baseline": cpu,
             "e2e": {"value": world * flops * K / (e2e_ms * 1e-3) / 1e12, "unit": "TFLOP/s",
                     "h2d_bytes_per_step": int(A.nnz * 8 + n * 16 * 8), "d2h_bytes_per_step": int(n * 16 * 8),

@@ -114,6 +114,16 @@ int spb_symbolic(spb_handle* h, int32_t n, const int64_t* colptr, const int32_t*
  * sides are the systems' right-hand sides stacked in the same order. */
 int spb_symbolic_batch(spb_handle* h, int32_t nsys, const int32_t* sys_offsets, int32_t n, const int64_t* colptr,
                        const int32_t* rowind);
+/* Symbolic-analysis reuse (no counterpart in the reference): give h the
+ * analysis of src (same structure; any handle, host-only included) without
+ * running the ordering again, then set up h's device buffers.  Ordering and
+ * relaxation options of the two handles must agree; precision may differ.
+ * The serving loop uses it to factor fresh values on a known pattern. */
+int spb_symbolic_from(spb_handle* h, const spb_handle* src);
+/* HBM footprint a handle with this analysis needs for factor + a solve of nrhs
+ * right-hand sides in the given precision (bytes requested from the device
+ * allocator).  Works on host-only handles after spb_symbolic. */
+int spb_predict_device_bytes(const spb_handle* h, int32_t precision, int32_t nrhs, int64_t* bytes);
 /* Rebuild the device plan of the current analysis with other tile shapes
  * (0 = default): supernodes up to small_max_w columns (<= 64) are factored
  * whole in shared memory; update products with at least big_tile_rows rows use

@@ -94,6 +94,8 @@ SIGNATURES = [
     ("spb_last_error", C.c_char_p, [_P]),
     ("spb_symbolic", C.c_int, [_P, C.c_int32, _I64P, _I32P]),
     ("spb_symbolic_batch", C.c_int, [_P, C.c_int32, _I32P, C.c_int32, _I64P, _I32P]),
+    ("spb_symbolic_from", C.c_int, [_P, _P]),
+    ("spb_predict_device_bytes", C.c_int, [_P, C.c_int32, C.c_int32, C.POINTER(C.c_int64)]),
     ("spb_replan", C.c_int, [_P, C.c_int32, C.c_int32]),
     ("spb_distribute", C.c_int, [_P, _DP]),
     ("spb_distribute_device", C.c_int, [_P, _P]),

@@ -37,6 +37,7 @@ struct spb_handle {
   int64_t nnz_a = 0;
   std::vector<int64_t> colptr;
   std::vector<int32_t> rowind;
+  std::vector<int64_t> amap;       // arena position of each input entry (DistributeMatrix map)
   std::vector<int32_t> level_off;  // level l covers dlevel_sn[level_off[l] .. level_off[l+1])
   // device buffers
   bool fp32 = false;        // precision form: FP32 factor + FP64 refinement
@@ -112,7 +113,9 @@ template <class T>
 cudaError_t dalloc(spb_handle* h, T** p, size_t count) {
   *p = nullptr;
   if (count == 0) count = 1;
-  cudaError_t e = cudaMalloc((void**)p, count * sizeof(T));
+  // stream-ordered allocation: allocating or freeing one handle's buffers does
+  // not synchronise the device, so handles served side by side keep running
+  cudaError_t e = cudaMallocAsync((void**)p, count * sizeof(T), h->own_stream);
   if (e == cudaSuccess) {
     h->allocs.push_back((void*)*p);
     h->device_bytes += (int64_t)(count * sizeof(T));
@@ -125,7 +128,11 @@ void release_device(spb_handle* h) {
     cudaGraphExecDestroy(h->fgraph);
     h->fgraph = nullptr;
   }
-  for (void* p : h->allocs) cudaFree(p);
+  if (!h->allocs.empty()) {
+    cudaStreamSynchronize(h->stream);  // work using the buffers has finished
+    for (void* p : h->allocs) cudaFreeAsync(p, h->own_stream);
+    cudaStreamSynchronize(h->own_stream);
+  }
   h->allocs.clear();
   h->device_bytes = 0;
   h->dL = nullptr;
@@ -238,7 +245,8 @@ int ensure_rhs_capacity(spb_handle* h, int nrhs) {
     if (*p) {
       auto it = std::find(h->allocs.begin(), h->allocs.end(), (void*)*p);
       if (it != h->allocs.end()) h->allocs.erase(it);
-      cudaFree(*p);
+      cudaStreamSynchronize(h->stream);
+      cudaFreeAsync(*p, h->own_stream);
       h->device_bytes -= h->x_cap * (int64_t)sizeof(double);
       *p = nullptr;
     }
@@ -252,6 +260,7 @@ int ensure_rhs_capacity(spb_handle* h, int nrhs) {
     SPB_CK(h, dalloc(h, &h->dXo, need));
   }
   h->x_cap = need;
+  SPB_CK(h, cudaStreamSynchronize(h->own_stream));  // allocations usable from any stream
   return SPB_OK;
 }
 
@@ -441,7 +450,18 @@ int spb_create(const spb_options* opt, spb_handle** out) {
     delete h;
     return e == cudaErrorMemoryAllocation ? SPB_ERR_OOM : SPB_ERR_CUDA;
   }
-  spb::dev::init_kernel_attributes();
+  {
+    // kernel attributes are per device; handles may be created from several threads
+    static std::mutex mu;
+    static bool done[256] = {};
+    std::lock_guard<std::mutex> lock(mu);
+    if (h->device < 256 && !done[h->device]) {
+      spb::dev::init_kernel_attributes();
+      done[h->device] = true;
+    } else if (h->device >= 256) {
+      spb::dev::init_kernel_attributes();
+    }
+  }
   *out = h;
   return SPB_OK;
 }
@@ -507,24 +527,56 @@ int begin_symbolic(spb_handle* h, int32_t n, const int64_t* colptr, const int32_
 
 // Everything after the symbolic analysis: device plan, assembly map and the
 // handle's device buffers.  h->sym must hold the (possibly merged) analysis.
+int install_device(spb_handle* h);
+
+// Device bytes install_device + a solve of nrhs right-hand sides allocate
+// (the same list of buffers, sizes as requested from cudaMalloc).
+int64_t predict_bytes(const spb_handle* h, bool fp32, int nrhs) {
+  const spb::Plan& P = h->plan;
+  const int64_t n = h->sym.n, ns = P.nsuper;
+  auto b = [](int64_t count, size_t size) { return std::max<int64_t>(count, 1) * (int64_t)size; };
+  int64_t t = b(P.arena_elems, fp32 ? sizeof(float) : sizeof(double));
+  t += b(P.meta.size(), sizeof(spb::SnMeta)) + b(P.rows.size(), 4) + b(P.supmember0.size(), 4);
+  t += b(h->amap.size(), 8) + b(h->nnz_a, 8) + b(P.small_items.size(), 4);
+  t += b(P.panel_items.size(), sizeof(spb::PanelItem));
+  t += b((int64_t)std::max(1, P.max_diag_slots) * (64 * 64 + 64), 8);
+  t += b(P.tile_items.size(), sizeof(spb::TileItem)) + b(n, 4) + b(ns, 4);
+  t += b(P.fwd_tasks.size(), sizeof(spb::SolveTask)) + b(P.bwd_tasks.size(), sizeof(spb::SolveTask));
+  t += b(P.fwd_pending.size(), 4) + b(P.sparent.size(), 4) + b(2 + 3 * ns, 4) + b(1, sizeof(Status));
+  if (fp32) {
+    int64_t offdiag = 0;
+    for (int64_t c = 1; c <= n; ++c)
+      for (int64_t p = h->colptr[c - 1]; p < h->colptr[c]; ++p) offdiag += h->rowind[p - 1] != c;
+    const int64_t nnz_full = h->nnz_a + offdiag;
+    t += b(n + 1, 8) + b(nnz_full, 4) + b(nnz_full, 8) + b(nnz_full, 8) + b(1 + 3 * 64, 8);
+  }
+  if (nrhs > 0) t += (fp32 ? 5 : 2) * b(n * nrhs, 8);
+  return t;
+}
+
 int install_symbolic(spb_handle* h, int32_t n, const int64_t* colptr, const int32_t* rowind) {
   try {
     h->plan = spb::build_plan(h->sym, plan_params_of(h->opt));
+    h->amap = spb::build_assembly_map(h->sym, h->plan, colptr, rowind);
   } catch (const std::bad_alloc&) {
     return fail(h, SPB_ERR_OOM, "symbolic: host allocation failed");
   } catch (const std::exception& e) {
     return fail(h, SPB_ERR_STRUCTURE, e.what());
   }
-  std::vector<int64_t> amap;
-  try {
-    amap = spb::build_assembly_map(h->sym, h->plan, colptr, rowind);
-  } catch (const std::exception& e) {
-    return fail(h, SPB_ERR_STRUCTURE, e.what());
-  }
+  return install_device(h);
+}
+
+// Device buffers of an analysed handle (h->sym, h->plan, h->amap, h->colptr and
+// h->rowind set); a host-only handle just records that the analysis is done.
+int install_device(spb_handle* h) {
   if (h->device < 0) {
     h->have_symbolic = true;
     return SPB_OK;
   }
+  const int32_t n = h->sym.n;
+  const int64_t* colptr = h->colptr.data();
+  const int32_t* rowind = h->rowind.data();
+  const std::vector<int64_t>& amap = h->amap;
   const spb::Plan& P = h->plan;
   std::vector<int32_t> lsn, invp0(n);
   h->level_off.assign(P.nlevels + 1, 0);
@@ -559,6 +611,7 @@ int install_symbolic(spb_handle* h, int32_t n, const int64_t* colptr, const int3
   SPB_CK(h, dalloc(h, &h->dsparent, P.sparent.size()));
   SPB_CK(h, dalloc(h, &h->dsync, 2 + 3 * (size_t)P.nsuper));
   SPB_CK(h, dalloc(h, &h->dstatus, 1));
+  SPB_CK(h, cudaStreamSynchronize(h->own_stream));  // allocations ready before h->stream uses them
   auto up = [&](void* d, const void* s, size_t bytes) {
     return bytes ? cudaMemcpyAsync(d, s, bytes, cudaMemcpyHostToDevice, h->stream) : cudaSuccess;
   };
@@ -607,10 +660,12 @@ int install_symbolic(spb_handle* h, int32_t n, const int64_t* colptr, const int3
     SPB_CK(h, dalloc(h, &h->d_csrsrc, h->csr_src.size()));
     SPB_CK(h, dalloc(h, &h->d_val, h->csr_col.size()));
     SPB_CK(h, dalloc(h, &h->d_norms, 1 + 3 * 64));
+    SPB_CK(h, cudaStreamSynchronize(h->own_stream));
     SPB_CK(h, up(h->d_rowptr, rp.data(), rp.size() * 8));
     SPB_CK(h, up(h->d_col, h->csr_col.data(), h->csr_col.size() * 4));
     SPB_CK(h, up(h->d_csrsrc, h->csr_src.data(), h->csr_src.size() * 8));
   }
+  SPB_CK(h, cudaStreamSynchronize(h->own_stream));
   SPB_CK(h, cudaStreamSynchronize(h->stream));
   h->have_symbolic = true;
   return SPB_OK;
@@ -634,6 +689,50 @@ int spb_symbolic(spb_handle* h, int32_t n, const int64_t* colptr, const int32_t*
     return fail(h, SPB_ERR_STRUCTURE, e.what());
   }
   return install_symbolic(h, n, colptr, rowind);
+}
+
+int spb_symbolic_from(spb_handle* h, const spb_handle* src) {
+  if (check_handle(h) || !src) return SPB_ERR_INVALID;
+  if (h == src) return fail(h, SPB_ERR_INVALID, "symbolic_from: source is the handle itself");
+  if (!src->have_symbolic) return fail(h, SPB_ERR_STATE, "symbolic_from: source has no symbolic analysis");
+  if (h->opt.ordering != src->opt.ordering || h->opt.nrelax0 != src->opt.nrelax0 ||
+      h->opt.nrelax1 != src->opt.nrelax1 || h->opt.nrelax2 != src->opt.nrelax2 ||
+      h->opt.max_snode != src->opt.max_snode || h->opt.zrelax0 != src->opt.zrelax0 ||
+      h->opt.zrelax1 != src->opt.zrelax1 || h->opt.zrelax2 != src->opt.zrelax2)
+    return fail(h, SPB_ERR_INVALID, "symbolic_from: ordering / relaxation options differ from the source's");
+  if (h->device >= 0) {
+    SPB_CK(h, cudaSetDevice(h->device));
+    release_device(h);
+  }
+  h->have_symbolic = h->have_values = h->factored = h->have_solution = false;
+  h->cells_built = false;
+  try {
+    h->sym = src->sym;
+    h->nnz_a = src->nnz_a;
+    h->colptr = src->colptr;
+    h->rowind = src->rowind;
+    if (plan_params_of(h->opt).small_max_w == plan_params_of(src->opt).small_max_w &&
+        plan_params_of(h->opt).big_tile_rows == plan_params_of(src->opt).big_tile_rows) {
+      h->plan = src->plan;
+      h->amap = src->amap;
+    } else {
+      h->plan = spb::build_plan(h->sym, plan_params_of(h->opt));
+      h->amap = spb::build_assembly_map(h->sym, h->plan, h->colptr.data(), h->rowind.data());
+    }
+  } catch (const std::bad_alloc&) {
+    return fail(h, SPB_ERR_OOM, "symbolic_from: host allocation failed");
+  } catch (const std::exception& e) {
+    return fail(h, SPB_ERR_STRUCTURE, e.what());
+  }
+  return install_device(h);
+}
+
+int spb_predict_device_bytes(const spb_handle* h, int32_t precision, int32_t nrhs, int64_t* bytes) {
+  if (!h || !bytes || nrhs < 0 || (precision != SPB_PRECISION_FP64 && precision != SPB_PRECISION_FP32_IR))
+    return SPB_ERR_INVALID;
+  if (!h->have_symbolic) return SPB_ERR_STATE;
+  *bytes = predict_bytes(h, precision == SPB_PRECISION_FP32_IR, nrhs);
+  return SPB_OK;
 }
 
 int spb_replan(spb_handle* h, int32_t small_max_w, int32_t big_tile_rows) {

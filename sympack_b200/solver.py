@@ -232,6 +232,20 @@ class symPACKMatrix2D:
         _raise(self._lib.spb_symbolic_batch(h, len(offs) - 1, _i32(offs), A.size, _i64(A.colptr), _i32(A.rowind)),
                "SymbolicFactorizationBatch", h)
 
+    def SymbolicFactorizationFrom(self, other: "symPACKMatrix2D") -> None:
+        """Reuse other's symbolic analysis (same structure) without ordering again."""
+        h = self._need()
+        self._n = other._n
+        _raise(self._lib.spb_symbolic_from(h, other._need()), "SymbolicFactorizationFrom", h)
+
+    def PredictDeviceBytes(self, precision: str | None = None, nrhs: int = 1) -> int:
+        """HBM bytes a factor + solve of nrhs columns needs with this analysis."""
+        h = self._need()
+        prec = N.PRECISIONS[precision or self.options.precision]
+        out = C.c_int64()
+        _raise(self._lib.spb_predict_device_bytes(h, prec, int(nrhs), C.byref(out)), "PredictDeviceBytes", h)
+        return int(out.value)
+
     def Replan(self, small_max_w: int = 0, big_tile_rows: int = 0) -> None:
         """Rebuild the device plan with other tile shapes; values must be distributed again."""
         h = self._need()
