@@ -45,6 +45,7 @@ class spb_options(C.Structure):
         ("verbose", C.c_int),
         ("plan_small_max_w", C.c_int),
         ("plan_big_tile_rows", C.c_int),
+        ("fp32_engine", C.c_int),
     ]
 
 

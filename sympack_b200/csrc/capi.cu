@@ -68,8 +68,10 @@ struct spb_handle {
   int32_t* d_col = nullptr;
   int64_t* d_csrsrc = nullptr;
   double* d_val = nullptr;
-  double* d_norms = nullptr;  // [anorm, bmax[64], xmax[64], rmax[64]]
-  double anorm = 0.0;
+  // refinement norms of every system: [eta, anorm[nseg], bmax[nseg*64], xmax[nseg*64], rmax[nseg*64]]
+  double* d_norms = nullptr;
+  std::vector<int32_t> seg_off{};  // systems of a batch (0-based row offsets); empty = one system
+  int32_t* d_rowseg = nullptr;     // system of each row (batches only)
   double* dR = nullptr;       // residual / correction right-hand side (original order)
   double* dD = nullptr;       // correction (original order)
   double* dXo = nullptr;      // refined solution (original order)
@@ -137,6 +139,7 @@ void release_device(spb_handle* h) {
   h->device_bytes = 0;
   h->dL = nullptr;
   h->dX = h->dB = h->dR = h->dD = h->dXo = nullptr;
+  h->d_rowseg = nullptr;
   h->x_cap = 0;
 }
 
@@ -148,6 +151,7 @@ spb::dev::FactorArgs factor_args(spb_handle* h) {
   a.supmember = h->dsupm;
   a.status = h->dstatus;
   a.fp32 = h->fp32;
+  a.tc32 = h->opt.fp32_engine == 0;
   return a;
 }
 
@@ -174,6 +178,8 @@ void enqueue_factor(spb_handle* h) {
 }
 
 int check_handle(spb_handle* h) { return h ? SPB_OK : SPB_ERR_INVALID; }
+
+int num_segments(const spb_handle* h) { return h->seg_off.empty() ? 1 : (int)h->seg_off.size() - 1; }
 
 cudaError_t ensure_events(spb_handle* h, size_t count) {
   while (h->events.size() < count) {
@@ -362,25 +368,25 @@ int ir_solve(spb_handle* h, const double* d_b, int64_t ldb, double* d_x, int64_t
     const double* b = d_b + (int64_t)c0 * ldb;
     double* x = d_x + (int64_t)c0 * ldx;
     plain_solve(h, b, ldb, x, ldx, nr);
-    SPB_CK(h, cudaMemsetAsync(h->d_norms + 1, 0, sizeof(double) * 64, h->stream));
-    spb::dev::launch_colmax(h->stream, b, n, nr, ldb, h->d_norms + 1);
+    const int nseg = num_segments(h);
+    double* anorm = h->d_norms + 1;
+    double* bmax = anorm + nseg;
+    double* xmax = bmax + (size_t)nseg * 64;
+    double* rmax = xmax + (size_t)nseg * 64;
+    SPB_CK(h, cudaMemsetAsync(bmax, 0, sizeof(double) * 64 * (size_t)nseg, h->stream));
+    spb::dev::launch_segmax(h->stream, b, n, nr, ldb, h->d_rowseg, bmax);
     double eta = 0.0, eta_prev = 1e300;
     int it = 0;
     for (;;) {
       spb::dev::launch_residual(h->stream, h->d_rowptr, h->d_col, h->d_val, x, b, h->dR, n, nr, ldx);
-      SPB_CK(h, cudaMemsetAsync(h->d_norms + 65, 0, sizeof(double) * 128, h->stream));
-      spb::dev::launch_colmax(h->stream, x, n, nr, ldx, h->d_norms + 65);
-      spb::dev::launch_colmax(h->stream, h->dR, n, nr, ldx, h->d_norms + 129);
-      double nm[1 + 3 * 64];
-      SPB_CK(h, cudaMemcpyAsync(nm, h->d_norms, sizeof(nm), cudaMemcpyDeviceToHost, h->stream));
+      SPB_CK(h, cudaMemsetAsync(xmax, 0, sizeof(double) * 128 * (size_t)nseg, h->stream));
+      SPB_CK(h, cudaMemsetAsync(h->d_norms, 0, sizeof(double), h->stream));
+      spb::dev::launch_segmax(h->stream, x, n, nr, ldx, h->d_rowseg, xmax);
+      spb::dev::launch_segmax(h->stream, h->dR, n, nr, ldx, h->d_rowseg, rmax);
+      spb::dev::launch_eta(h->stream, anorm, bmax, xmax, rmax, nseg, nr, h->d_norms);
+      SPB_CK(h, cudaMemcpyAsync(&eta, h->d_norms, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
       int rc = check_solve_status(h);  // synchronizes
       if (rc) return rc;
-      eta = 0.0;
-      for (int c = 0; c < nr; ++c) {
-        double den = h->anorm * nm[65 + c] + nm[1 + c];
-        double e = den > 0 ? nm[129 + c] / den : (nm[129 + c] > 0 ? 1e300 : 0.0);
-        eta = std::max(eta, e);
-      }
       if (eta <= tol) break;
       if (it >= maxit || (it >= 4 && eta > 0.9 * eta_prev)) {
         h->ir_iterations = std::max(iters_all, it);
@@ -520,6 +526,7 @@ int begin_symbolic(spb_handle* h, int32_t n, const int64_t* colptr, const int32_
   h->have_symbolic = h->have_values = h->factored = h->have_solution = false;
   h->cells_built = false;
   h->nnz_a = colptr[n] - 1;
+  h->seg_off.clear();
   h->colptr.assign(colptr, colptr + n + 1);
   h->rowind.assign(rowind, rowind + h->nnz_a);
   return SPB_OK;
@@ -548,7 +555,9 @@ int64_t predict_bytes(const spb_handle* h, bool fp32, int nrhs) {
     for (int64_t c = 1; c <= n; ++c)
       for (int64_t p = h->colptr[c - 1]; p < h->colptr[c]; ++p) offdiag += h->rowind[p - 1] != c;
     const int64_t nnz_full = h->nnz_a + offdiag;
-    t += b(n + 1, 8) + b(nnz_full, 4) + b(nnz_full, 8) + b(nnz_full, 8) + b(1 + 3 * 64, 8);
+    t += b(n + 1, 8) + b(nnz_full, 4) + b(nnz_full, 8) + b(nnz_full, 8);
+    t += b(1 + (int64_t)num_segments(h) * (1 + 3 * 64), 8);
+    if (!h->seg_off.empty()) t += b(n, 4);
   }
   if (nrhs > 0) t += (fp32 ? 5 : 2) * b(n * nrhs, 8);
   return t;
@@ -659,7 +668,15 @@ int install_device(spb_handle* h) {
     SPB_CK(h, dalloc(h, &h->d_col, h->csr_col.size()));
     SPB_CK(h, dalloc(h, &h->d_csrsrc, h->csr_src.size()));
     SPB_CK(h, dalloc(h, &h->d_val, h->csr_col.size()));
-    SPB_CK(h, dalloc(h, &h->d_norms, 1 + 3 * 64));
+    SPB_CK(h, dalloc(h, &h->d_norms, 1 + (size_t)num_segments(h) * (1 + 3 * 64)));
+    if (!h->seg_off.empty()) {
+      std::vector<int32_t> rowseg(n);
+      for (size_t k = 0; k + 1 < h->seg_off.size(); ++k)
+        for (int32_t i = h->seg_off[k]; i < h->seg_off[k + 1]; ++i) rowseg[i] = (int32_t)k;
+      SPB_CK(h, dalloc(h, &h->d_rowseg, rowseg.size()));
+      SPB_CK(h, cudaStreamSynchronize(h->own_stream));
+      SPB_CK(h, cudaMemcpyAsync(h->d_rowseg, rowseg.data(), rowseg.size() * 4, cudaMemcpyHostToDevice, h->stream));
+    }
     SPB_CK(h, cudaStreamSynchronize(h->own_stream));
     SPB_CK(h, up(h->d_rowptr, rp.data(), rp.size() * 8));
     SPB_CK(h, up(h->d_col, h->csr_col.data(), h->csr_col.size() * 4));
@@ -708,6 +725,7 @@ int spb_symbolic_from(spb_handle* h, const spb_handle* src) {
   h->cells_built = false;
   try {
     h->sym = src->sym;
+    h->seg_off = src->seg_off;
     h->nnz_a = src->nnz_a;
     h->colptr = src->colptr;
     h->rowind = src->rowind;
@@ -802,6 +820,7 @@ int spb_symbolic_batch(spb_handle* h, int32_t nsys, const int32_t* sys_offsets, 
   } catch (const std::exception& e) {
     return fail(h, SPB_ERR_INVALID, e.what());
   }
+  if (nsys > 1) h->seg_off.assign(sys_offsets, sys_offsets + nsys + 1);
   return install_symbolic(h, n, colptr, rowind);
 }
 
@@ -816,9 +835,8 @@ static int distribute_common(spb_handle* h) {
   spb::dev::launch_assemble(h->stream, h->dL, h->fp32, h->damap, h->dA, h->nnz_a);
   if (h->fp32) {  // FP64 copy of A for the refinement residuals, and ||A||_inf
     spb::dev::launch_gather(h->stream, h->d_val, h->dA, h->d_csrsrc, (int64_t)h->csr_col.size());
-    SPB_CK(h, cudaMemsetAsync(h->d_norms, 0, sizeof(double), h->stream));
-    spb::dev::launch_rowsum_max(h->stream, h->d_rowptr, h->d_val, h->sym.n, h->d_norms);
-    SPB_CK(h, cudaMemcpyAsync(&h->anorm, h->d_norms, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    SPB_CK(h, cudaMemsetAsync(h->d_norms + 1, 0, sizeof(double) * num_segments(h), h->stream));
+    spb::dev::launch_rowsum_segmax(h->stream, h->d_rowptr, h->d_val, h->sym.n, h->d_rowseg, h->d_norms + 1);
   }
   SPB_CK(h, cudaGetLastError());
   if (h->profiling) SPB_CK(h, cudaEventRecord(h->events[1], h->stream));

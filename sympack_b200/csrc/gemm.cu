@@ -393,17 +393,212 @@ __global__ void __launch_bounds__(256, 1) k_gemm_tf32x3(FactorArgs a, const Tile
   tile_epilogue<128, 128, 256, float, float>(a, it, m, Cs, kTLdc, ints, ints + 128, ints + 256, ints + 384);
 }
 
+// ---- 128 x 128 split-precision 3xTF32 tile on the 5th-generation tensor core -------
+// tcgen05.mma (kind::tf32, cta_group::1, M = 128, N = 128, K = 8) with the FP32
+// accumulator in tensor memory.  Operands are staged by all 256 threads: FP32
+// panel values are read from HBM (coalesced along the panel's rows), split into
+// tf32 hi / lo parts and written in the canonical MN-major 128-byte-swizzled
+// layout (32 consecutive rows of one column fill one 128 B line; 8 columns form
+// a 1 KB swizzle atom).  One elected thread issues the 12 MMAs of a 32-column
+// chunk (4 K steps x {lo*hi, hi*lo, hi*hi}) and commits them to the chunk's
+// mbarrier; the next chunk is staged into the other buffer meanwhile.  The
+// epilogue reads the accumulator with tcgen05.ld (warp w: lanes 32(w%4).., column
+// half w/4), stages it in shared memory and scatters it like the other tiles.
+constexpr int kUM = 128, kUN = 128, kUK = 32;
+constexpr int kUOpBytes = kUM * kUK * 4;           // one operand part: 16 KB
+constexpr int kUStageBytes = 4 * kUOpBytes;        // A hi, A lo, B hi, B lo
+constexpr int kUStages = 2;
+constexpr int kULdc = 132;
+constexpr size_t kUCBytes = (size_t)kUN * kULdc * sizeof(float);
+constexpr size_t kUMainBytes =
+    (size_t)kUStages * kUStageBytes > kUCBytes ? (size_t)kUStages * kUStageBytes : kUCBytes;
+constexpr size_t kUSmemBytes = 1024 + kUMainBytes + 4 * 128 * sizeof(int) + 64;
+constexpr int kUTmemCols = 128;
+constexpr long long kUWaitLimit = 1LL << 24;  // mbarrier polls before a tile gives up (seconds)
+
+// Byte offset of element (row m, column k) of a 128 x 32 operand part:
+// 32-row blocks 4 KB apart (leading byte offset), 8-column swizzle atoms 1 KB
+// apart (stride byte offset), 16 B chunks of a line XOR-ed with the column.
+__device__ __forceinline__ uint32_t umma_mn_offset(int m, int k) {
+  return (uint32_t)((m >> 5) * 4096 + (k >> 3) * 1024 + (k & 7) * 128 + ((((m & 31) >> 2) ^ (k & 7)) << 4) +
+                    (m & 3) * 4);
+}
+
+// Shared-memory matrix descriptor: start >> 4, LBO 4096 >> 4, SBO 1024 >> 4,
+// descriptor version 1, 128-byte swizzle.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)(4096 >> 4) << 16) | ((uint64_t)(1024 >> 4) << 32) |
+         (1ull << 46) | (2ull << 61);
+}
+
+// Instruction descriptor: D f32, A and B tf32, both MN-major, N = 128, M = 128.
+constexpr uint32_t kUIdesc = (1u << 4) | (2u << 7) | (2u << 10) | (1u << 15) | (1u << 16) |
+                             ((uint32_t)(kUN >> 3) << 17) | ((uint32_t)(kUM >> 4) << 24);
+
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, long long limit) {
+  for (long long i = 0; i < limit; ++i) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.b32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+__global__ void __launch_bounds__(256, 1) k_gemm_tc32(FactorArgs a, const TileItem* __restrict__ items) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const uint32_t raw_addr = (uint32_t)__cvta_generic_to_shared(smem_raw);
+  const uint32_t pad = ((raw_addr + 1023u) & ~1023u) - raw_addr;  // swizzle atoms need 1 KB alignment
+  unsigned char* base = smem_raw + pad;
+  const uint32_t base_addr = raw_addr + pad;
+  float* Cs = reinterpret_cast<float*>(base);  // reused once every MMA has completed
+  int* ints = reinterpret_cast<int*>(base + kUMainBytes);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(base + kUMainBytes + 4 * 128 * sizeof(int));
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + kUStages);
+  __shared__ int sh_abort;
+
+  const TileItem it = items[blockIdx.x];
+  const SnMeta m = a.meta[it.s];
+  const float* g = static_cast<const float*>(a.L) + m.off;
+  const int64_t ld = m.ld;
+  const int tid = threadIdx.x, warp = tid >> 5;
+
+  if (tid == 0) {
+    sh_abort = 0;
+    for (int i = 0; i < kUStages; ++i) {
+      const uint32_t b = (uint32_t)__cvta_generic_to_shared(bars + i);
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(b) : "memory");
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  if (warp == 0) {
+    const uint32_t slot = (uint32_t)__cvta_generic_to_shared(tmem_slot);
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(slot),
+                 "r"(kUTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+
+  // this thread's operand elements: row r, columns kq + 2q (q = 0..15)
+  const int r = tid & 127, kq = tid >> 7;
+  const bool arow = r < it.mrows, brow = r < it.ncols;
+  float va[16], vb[16];
+  auto load_chunk = [&](int kk) {
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+      const int k = kk + kq + 2 * q;
+      const bool kok = k < it.kn;
+      const int64_t coff = (int64_t)(it.k0 + k) * ld;
+      va[q] = (kok && arow) ? g[it.a_row0 + r + coff] : 0.f;
+      vb[q] = (kok && brow) ? g[it.b_row0 + r + coff] : 0.f;
+    }
+  };
+  const int nk = (it.kn + kUK - 1) / kUK;
+  load_chunk(0);
+  int committed = -1;  // last chunk whose MMAs were committed
+  for (int kt = 0; kt < nk; ++kt) {
+    const int st = kt & 1;
+    const uint32_t bar = (uint32_t)__cvta_generic_to_shared(bars + st);
+    if (kt >= 2 && !mbar_wait(bar, (uint32_t)(((kt >> 1) - 1) & 1), kUWaitLimit)) sh_abort = 1;
+    unsigned char* sb = base + st * kUStageBytes;
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+      const uint32_t off = umma_mn_offset(r, kq + 2 * q);
+      uint32_t hi, lo;
+      split_tf32(va[q], hi, lo);
+      *reinterpret_cast<uint32_t*>(sb + off) = hi;
+      *reinterpret_cast<uint32_t*>(sb + kUOpBytes + off) = lo;
+      split_tf32(vb[q], hi, lo);
+      *reinterpret_cast<uint32_t*>(sb + 2 * kUOpBytes + off) = hi;
+      *reinterpret_cast<uint32_t*>(sb + 3 * kUOpBytes + off) = lo;
+    }
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    __syncthreads();
+    if (sh_abort) break;
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+      const uint32_t sa = base_addr + st * kUStageBytes;
+#pragma unroll
+      for (int ks = 0; ks < kUK / 8; ++ks) {
+        const uint64_t ahi = umma_desc(sa + ks * 1024), alo = umma_desc(sa + kUOpBytes + ks * 1024);
+        const uint64_t bhi = umma_desc(sa + 2 * kUOpBytes + ks * 1024), blo = umma_desc(sa + 3 * kUOpBytes + ks * 1024);
+        const uint64_t pa[3] = {alo, ahi, ahi}, pb[3] = {bhi, blo, bhi};
+#pragma unroll
+        for (int p = 0; p < 3; ++p) {
+          const uint32_t acc = (kt > 0 || ks > 0 || p > 0) ? 1u : 0u;
+          asm volatile(
+              "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+              " tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
+              "l"(pa[p]), "l"(pb[p]), "r"(kUIdesc), "r"(acc)
+              : "memory");
+        }
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(bar)
+                   : "memory");
+    }
+    committed = kt;
+    if (kt + 1 < nk) load_chunk((kt + 1) * kUK);
+  }
+  bool ok = !sh_abort;
+  if (committed >= 0) {  // every MMA done before the accumulator is read or the stages reused
+    const uint32_t bar = (uint32_t)__cvta_generic_to_shared(bars + (committed & 1));
+    if (!mbar_wait(bar, (uint32_t)((committed >> 1) & 1), kUWaitLimit)) ok = false;
+  }
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  if (!ok) {
+    if (tid == 0) report_status(a.status, 3, it.s, -1);
+  } else {
+    const int quarter = warp & 3, half = warp >> 2;
+    const int row = quarter * 32 + (tid & 31);
+#pragma unroll
+    for (int part = 0; part < 2; ++part) {
+      const int c0 = half * 64 + part * 32;
+      uint32_t v[32];
+      const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)c0;
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+          "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
+          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+            "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+            "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]),
+            "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]),
+            "=r"(v[30]), "=r"(v[31])
+          : "r"(taddr));
+      asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+      for (int j = 0; j < 32; ++j) Cs[row + (c0 + j) * kULdc] = __uint_as_float(v[j]);
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(kUTmemCols) : "memory");
+  }
+  if (!ok) return;
+  tile_epilogue<kUM, kUN, 256, float, float>(a, it, m, Cs, kULdc, ints, ints + 128, ints + 256, ints + 384);
+}
+
 }  // namespace
 
 void init_gemm_attributes() {
   cudaFuncSetAttribute(k_gemm_tf32x3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTSmemBytes);
+  cudaFuncSetAttribute(k_gemm_tc32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kUSmemBytes);
   cudaFuncSetAttribute(k_gemm_dmma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDSmemBytes);
 }
 
 void launch_gemm(cudaStream_t st, const FactorArgs& a, const TileItem* items, int count, int tile) {
   if (count <= 0) return;
   if (a.fp32) {
-    if (tile == 128) k_gemm_tf32x3<<<count, 256, kTSmemBytes, st>>>(a, items);
+    if (tile == 128 && a.tc32) k_gemm_tc32<<<count, 256, kUSmemBytes, st>>>(a, items);
+    else if (tile == 128) k_gemm_tf32x3<<<count, 256, kTSmemBytes, st>>>(a, items);
     else k_gemm_simt<float><<<count, 256, kSSmemBytes, st>>>(a, items);
   } else {
     if (tile == 128) k_gemm_dmma<<<count, kDThreads, kDSmemBytes, st>>>(a, items);

@@ -79,105 +79,127 @@ __global__ void __launch_bounds__(128) k_factor_small(FactorArgs a, const int32_
 }
 
 constexpr int kNB = 64;
+constexpr int kThreads = 256;  // threads of the POTRF and TRSM kernels
 
 // POTRF of one 64-column diagonal block [c0, c0+nb) of a wide panel (one CTA
-// per item), blocked by 16: warp 0 factors each 16 x 16 diagonal piece, then
-// the rows below are solved against it and the trailing block is updated.  The
-// CTA also copies the factored block (FP64) and 1/L_kk to its scratch slot, from
-// where the TRSM of the rows below reads them.  A block narrower than 64 is
-// padded with the identity.
+// per item), right-looking by 8-column pieces in shared memory: warp 0 factors
+// the 8 x 8 diagonal piece in registers (lane i holds row i, columns exchanged
+// by shuffles), one thread per row solves the rows below against it, and the
+// trailing lower triangle is updated with the solved piece (thread (row,
+// group) updates columns group, group+4, ... of its row, so the piece's row
+// values stay in registers and the column values are warp broadcasts).  The
+// CTA also copies the factored block (FP64) and 1/L_kk to its scratch slot,
+// from where the TRSM of the rows below reads them.  A block narrower than 64
+// is padded with the identity.  Loads and stores are unrolled so that a
+// thread's 16 global accesses are in flight together: the kernel sits on the
+// critical path of every wide supernode and is latency-bound.
 constexpr int kDL = kNB + 1;  // padded leading dimension in shared memory
 constexpr size_t kSlot = (size_t)kNB * kNB + kNB;  // scratch slot: factored block (FP64) + 1/L_kk
+constexpr int kPiece = 8;
 
 template <class T>
-__global__ void __launch_bounds__(256, 1) k_potrf_diag(FactorArgs a, const PanelItem* __restrict__ items,
-                                                    double* __restrict__ winv) {
+__global__ void __launch_bounds__(kThreads, 1) k_potrf_diag(FactorArgs a, const PanelItem* __restrict__ items,
+                                                         double* __restrict__ winv) {
   __shared__ double D[kNB * kDL];
+  __shared__ double Rinv[kNB];  // 1 / L_kk
   const PanelItem it = items[blockIdx.x];
   const SnMeta m = a.meta[it.s];
-  T* g = static_cast<T*>(a.L) + m.off;
+  const T* g = static_cast<const T*>(a.L) + m.off;
   const int nb = it.nb, c0 = it.c0;
   const int64_t ld = m.ld;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  for (int idx = tid; idx < kNB * kNB; idx += blockDim.x) {
-    int c = idx / kNB, r = idx - c * kNB;
-    double v = 0.0;
-    if (r < nb && c < nb) {
-      if (r >= c) v = (double)g[(c0 + r) + (int64_t)(c0 + c) * ld];
-    } else if (r == c) {
-      v = 1.0;
+  {
+    double v[kNB * kNB / kThreads];
+#pragma unroll
+    for (int q = 0; q < kNB * kNB / kThreads; ++q) {
+      const int idx = tid + q * kThreads, c = idx / kNB, r = idx - c * kNB;
+      v[q] = (r < nb && c < nb && r >= c) ? (double)g[(c0 + r) + (int64_t)(c0 + c) * ld] : (r == c ? 1.0 : 0.0);
     }
-    D[r + c * kDL] = v;
+#pragma unroll
+    for (int q = 0; q < kNB * kNB / kThreads; ++q) {
+      const int idx = tid + q * kThreads, c = idx / kNB, r = idx - c * kNB;
+      D[r + c * kDL] = v[q];
+    }
   }
   __syncthreads();
-  __shared__ double Rinv[kNB];  // 1 / L_kk
-  for (int kb = 0; kb < kNB; kb += 16) {
+  const int urow = tid & 63, ugrp = tid >> 6;  // update mapping: row kb+8+urow, columns kb+8+ugrp+4t
+#pragma unroll 1
+  for (int kb = 0; kb < kNB; kb += kPiece) {
     if (warp == 0) {
-      // 16 x 16 diagonal piece in registers: lane i < 16 holds row i
-      double r[16];
+      double r[kPiece];
 #pragma unroll
-      for (int j = 0; j < 16; ++j) r[j] = (lane < 16 && j <= lane) ? D[kb + lane + (kb + j) * kDL] : 0.0;
+      for (int j = 0; j < kPiece; ++j) r[j] = (lane < kPiece && j <= lane) ? D[kb + lane + (kb + j) * kDL] : 0.0;
 #pragma unroll
-      for (int k = 0; k < 16; ++k) {
+      for (int k = 0; k < kPiece; ++k) {
         double dkk = __shfl_sync(0xffffffffu, r[k], k);
         if (!(dkk > 0.0)) {
           if (lane == 0 && kb + k < nb) report(a.status, 1, it.s, m.fc + c0 + kb + k);
           dkk = 1.0;
         }
-        const double rs = rsqrt(dkk);  // 1 / L_kk
+        const double rs = rsqrt(dkk);
         if (lane == k) r[k] = dkk * rs;
-        else if (lane > k && lane < 16) r[k] *= rs;
+        else if (lane > k && lane < kPiece) r[k] *= rs;
         if (lane == 0) Rinv[kb + k] = rs;
 #pragma unroll
-        for (int j = k + 1; j < 16; ++j) {
+        for (int j = k + 1; j < kPiece; ++j) {
           const double ljk = __shfl_sync(0xffffffffu, r[k], j);
-          if (lane >= j && lane < 16) r[j] = fma(-r[k], ljk, r[j]);
+          if (lane >= j && lane < kPiece) r[j] = fma(-r[k], ljk, r[j]);
         }
       }
-      if (lane < 16) {
+      if (lane < kPiece) {
 #pragma unroll
-        for (int j = 0; j < 16; ++j)
+        for (int j = 0; j < kPiece; ++j)
           if (j <= lane) D[kb + lane + (kb + j) * kDL] = r[j];
       }
     }
     __syncthreads();
-    const int below = kNB - kb - 16;
-    if (tid < below) {  // one row per thread: solve against the 16 x 16 piece
-      const int i = kb + 16 + tid;
-      double x[16];
+    const int below = kNB - kb - kPiece;
+    if (below == 0) break;
+    if (tid < below) {  // one row per thread: solve against the 8 x 8 piece
+      const int i = kb + kPiece + tid;
+      double x[kPiece];
 #pragma unroll
-      for (int j = 0; j < 16; ++j) x[j] = D[i + (kb + j) * kDL];
+      for (int j = 0; j < kPiece; ++j) x[j] = D[i + (kb + j) * kDL];
 #pragma unroll
-      for (int k = 0; k < 16; ++k) {
+      for (int k = 0; k < kPiece; ++k) {
         double t = x[k];
 #pragma unroll
         for (int j = 0; j < k; ++j) t = fma(-x[j], D[kb + k + (kb + j) * kDL], t);
         x[k] = t * Rinv[kb + k];
       }
 #pragma unroll
-      for (int j = 0; j < 16; ++j) D[i + (kb + j) * kDL] = x[j];
+      for (int j = 0; j < kPiece; ++j) D[i + (kb + j) * kDL] = x[j];
     }
     __syncthreads();
-    for (int idx = tid; idx < below * below; idx += blockDim.x) {
-      int j = kb + 16 + idx / below, i = kb + 16 + idx % below;
-      if (i >= j) {
-        double t = D[i + j * kDL];
+    if (urow < below) {
+      const int i = kb + kPiece + urow;
+      double x[kPiece];
 #pragma unroll
-        for (int k = 0; k < 16; ++k) t = fma(-D[i + (kb + k) * kDL], D[j + (kb + k) * kDL], t);
-        D[i + j * kDL] = t;
+      for (int k = 0; k < kPiece; ++k) x[k] = D[i + (kb + k) * kDL];
+      for (int j = kb + kPiece + ugrp; j <= i; j += 4) {
+        double t0 = D[i + j * kDL], t1 = 0.0;
+#pragma unroll
+        for (int k = 0; k < kPiece; k += 2) {
+          t0 = fma(-x[k], D[j + (kb + k) * kDL], t0);
+          t1 = fma(-x[k + 1], D[j + (kb + k + 1) * kDL], t1);
+        }
+        D[i + j * kDL] = t0 + t1;
       }
     }
     __syncthreads();
   }
-  for (int idx = tid; idx < nb * nb; idx += blockDim.x) {
-    int c = idx / nb, r = idx - c * nb;
-    if (r >= c) g[(c0 + r) + (int64_t)(c0 + c) * ld] = (T)D[r + c * kDL];
+  T* gw = static_cast<T*>(a.L) + m.off;
+#pragma unroll
+  for (int q = 0; q < kNB * kNB / kThreads; ++q) {
+    const int idx = tid + q * kThreads, c = idx / kNB, r = idx - c * kNB;
+    if (r < nb && c < nb && r >= c) gw[(c0 + r) + (int64_t)(c0 + c) * ld] = (T)D[r + c * kDL];
   }
   // FP64 copy of the factored block and 1/L_kk for the TRSM of the rows below
   if (winv) {
     double* W = winv + (size_t)it.slot * kSlot;
-    for (int idx = tid; idx < kNB * kNB; idx += blockDim.x) {
-      int c = idx / kNB, r = idx - c * kNB;
+#pragma unroll
+    for (int q = 0; q < kNB * kNB / kThreads; ++q) {
+      const int idx = tid + q * kThreads, c = idx / kNB, r = idx - c * kNB;
       W[idx] = D[r + c * kDL];
     }
     if (tid < kNB) W[kNB * kNB + tid] = Rinv[tid];
@@ -185,12 +207,14 @@ __global__ void __launch_bounds__(256, 1) k_potrf_diag(FactorArgs a, const Panel
 }
 
 // TRSM of one 64-row tile below a factored diagonal block, R <- R L11^-T, by
-// 16-column pieces: each row solves against the 16 x 16 diagonal piece (one
+// 8-column pieces: each row solves against the 8 x 8 diagonal piece (one
 // thread per row), then the remaining columns of the tile are updated with the
-// solved piece (all threads).  L11 and 1/L_kk come from the scratch slot.
+// solved piece (thread (row, group) takes columns group, group+4, ...).  L11
+// and 1/L_kk come from the scratch slot.  All loads are issued before the first
+// use (32 per thread in flight).
 template <class T>
-__global__ void __launch_bounds__(256) k_trsm_rows(FactorArgs a, const PanelItem* __restrict__ items,
-                                                   const double* __restrict__ winv) {
+__global__ void __launch_bounds__(kThreads, 2) k_trsm_rows(FactorArgs a, const PanelItem* __restrict__ items,
+                                                        const double* __restrict__ winv) {
   extern __shared__ double smem_tr[];
   double* R = smem_tr;               // R[r + k*kDL]
   double* D = smem_tr + kNB * kDL;   // D[i + j*kDL] = L11[i][j]
@@ -203,46 +227,62 @@ __global__ void __launch_bounds__(256) k_trsm_rows(FactorArgs a, const PanelItem
   const int rows = min(kNB, m.h - it.row0);
   const double* W = winv + (size_t)it.slot * kSlot;
   const int tid = threadIdx.x;
-  for (int idx = tid; idx < kNB * kNB; idx += blockDim.x) {
-    int k = idx / kNB, r = idx - k * kNB;
-    R[r + k * kDL] = (r < rows && k < nb) ? (double)g[(it.row0 + r) + (int64_t)(c0 + k) * ld] : 0.0;
-    D[r + k * kDL] = W[idx];
+  {
+    double v[kNB * kNB / kThreads], w[kNB * kNB / kThreads];
+#pragma unroll
+    for (int q = 0; q < kNB * kNB / kThreads; ++q) {
+      const int idx = tid + q * kThreads, k = idx / kNB, r = idx - k * kNB;
+      v[q] = (r < rows && k < nb) ? (double)g[(it.row0 + r) + (int64_t)(c0 + k) * ld] : 0.0;
+      w[q] = W[idx];
+    }
+#pragma unroll
+    for (int q = 0; q < kNB * kNB / kThreads; ++q) {
+      const int idx = tid + q * kThreads, k = idx / kNB, r = idx - k * kNB;
+      R[r + k * kDL] = v[q];
+      D[r + k * kDL] = w[q];
+    }
   }
   if (tid < kNB) Rinv[tid] = W[kNB * kNB + tid];
   __syncthreads();
-  for (int kb = 0; kb < nb; kb += 16) {
+  const int urow = tid & 63, ugrp = tid >> 6;
+#pragma unroll 1
+  for (int kb = 0; kb < nb; kb += kPiece) {
     if (tid < rows) {
-      double x[16];
+      double x[kPiece];
 #pragma unroll
-      for (int j = 0; j < 16; ++j) x[j] = R[tid + (kb + j) * kDL];
+      for (int j = 0; j < kPiece; ++j) x[j] = R[tid + (kb + j) * kDL];
 #pragma unroll
-      for (int k = 0; k < 16; ++k) {
-        double t0 = x[k], t1 = 0.0;
+      for (int k = 0; k < kPiece; ++k) {
+        double t = x[k];
 #pragma unroll
-        for (int j = 0; j + 1 < k; j += 2) {
-          t0 = fma(-x[j], D[kb + k + (kb + j) * kDL], t0);
-          t1 = fma(-x[j + 1], D[kb + k + (kb + j + 1) * kDL], t1);
-        }
-        if (k & 1) t0 = fma(-x[k - 1], D[kb + k + (kb + k - 1) * kDL], t0);
-        x[k] = (t0 + t1) * Rinv[kb + k];
+        for (int j = 0; j < k; ++j) t = fma(-x[j], D[kb + k + (kb + j) * kDL], t);
+        x[k] = t * Rinv[kb + k];
       }
 #pragma unroll
-      for (int j = 0; j < 16; ++j) R[tid + (kb + j) * kDL] = x[j];
+      for (int j = 0; j < kPiece; ++j) R[tid + (kb + j) * kDL] = x[j];
     }
     __syncthreads();
-    const int rest = kNB - kb - 16;
-    for (int idx = tid; idx < rows * rest; idx += blockDim.x) {
-      int j = kb + 16 + idx / rows, r = idx % rows;
-      double t = R[r + j * kDL];
+    if (kb + kPiece >= nb) break;
+    if (urow < rows) {
+      double x[kPiece];
 #pragma unroll
-      for (int k = 0; k < 16; ++k) t = fma(-R[r + (kb + k) * kDL], D[j + (kb + k) * kDL], t);
-      R[r + j * kDL] = t;
+      for (int k = 0; k < kPiece; ++k) x[k] = R[urow + (kb + k) * kDL];
+      for (int j = kb + kPiece + ugrp; j < nb; j += 4) {
+        double t0 = R[urow + j * kDL], t1 = 0.0;
+#pragma unroll
+        for (int k = 0; k < kPiece; k += 2) {
+          t0 = fma(-x[k], D[j + (kb + k) * kDL], t0);
+          t1 = fma(-x[k + 1], D[j + (kb + k + 1) * kDL], t1);
+        }
+        R[urow + j * kDL] = t0 + t1;
+      }
     }
     __syncthreads();
   }
-  for (int idx = tid; idx < rows * nb; idx += blockDim.x) {
-    int k = idx / rows, r = idx - k * rows;
-    g[(it.row0 + r) + (int64_t)(c0 + k) * ld] = (T)R[r + k * kDL];
+#pragma unroll
+  for (int q = 0; q < kNB * kNB / kThreads; ++q) {
+    const int idx = tid + q * kThreads, k = idx / kNB, r = idx - k * kNB;
+    if (r < rows && k < nb) g[(it.row0 + r) + (int64_t)(c0 + k) * ld] = (T)R[r + k * kDL];
   }
 }
 
@@ -298,14 +338,14 @@ void launch_factor_small(cudaStream_t st, const FactorArgs& a, const int32_t* it
 }
 
 void launch_potrf_diag(cudaStream_t st, const FactorArgs& a, const PanelItem* items, int count, double* winv) {
-  if (a.fp32) k_potrf_diag<float><<<count, 256, 0, st>>>(a, items, winv);
-  else k_potrf_diag<double><<<count, 256, 0, st>>>(a, items, winv);
+  if (a.fp32) k_potrf_diag<float><<<count, kThreads, 0, st>>>(a, items, winv);
+  else k_potrf_diag<double><<<count, kThreads, 0, st>>>(a, items, winv);
 }
 
 void launch_trsm_rows(cudaStream_t st, const FactorArgs& a, const PanelItem* items, int count, const double* winv) {
   const size_t smem = 2 * kNB * kDL * sizeof(double);
-  if (a.fp32) k_trsm_rows<float><<<count, 256, smem, st>>>(a, items, winv);
-  else k_trsm_rows<double><<<count, 256, smem, st>>>(a, items, winv);
+  if (a.fp32) k_trsm_rows<float><<<count, kThreads, smem, st>>>(a, items, winv);
+  else k_trsm_rows<double><<<count, kThreads, smem, st>>>(a, items, winv);
 }
 
 void launch_permute_in(cudaStream_t st, double* X, int64_t ldx, const double* B, int64_t ldb,

@@ -24,6 +24,7 @@ struct FactorArgs {
   const int32_t* supmember;  // 0-based supernode of each permuted column
   Status* status;
   bool fp32;                 // FP32 factor storage (precision form)
+  bool tc32;                 // FP32 128 x 128 tiles on tcgen05 (else mma.sync m16n8k8)
 };
 
 // Must run once per process (per device) before the first launch or capture.
@@ -69,8 +70,12 @@ void launch_solve_persistent(cudaStream_t st, const PSolveArgs& a, bool forward)
 void launch_gather(cudaStream_t st, double* dst, const double* src, const int64_t* idx, int64_t n);
 void launch_residual(cudaStream_t st, const int64_t* rowptr, const int32_t* col, const double* val, const double* x,
                      const double* b, double* r, int n, int nrhs, int64_t ld);
-void launch_colmax(cudaStream_t st, const double* v, int n, int nrhs, int64_t ld, double* out);
-void launch_rowsum_max(cudaStream_t st, const int64_t* rowptr, const double* val, int n, double* out);
+void launch_segmax(cudaStream_t st, const double* v, int n, int nrhs, int64_t ld, const int32_t* rowseg,
+                   double* out);
+void launch_rowsum_segmax(cudaStream_t st, const int64_t* rowptr, const double* val, int n, const int32_t* rowseg,
+                          double* anorm);
+void launch_eta(cudaStream_t st, const double* anorm, const double* bmax, const double* xmax, const double* rmax,
+                int nseg, int nrhs, double* eta);
 void launch_axpy(cudaStream_t st, double* x, const double* d, int n, int nrhs, int64_t ld);
 
 // X[invp[i], c] = B[i, c]   and   B[i, c] = X[invp[i], c]

@@ -61,10 +61,19 @@ def test_fp32_ir_reaches_fp64_backward_error(delta, fwd_tol, k):
         assert np.max(np.abs(x - xo)) / np.max(np.abs(xo)) <= fwd_tol
 
 
-def test_fp32_factor_close_to_fp64_factor():
-    n, cp, ri, v = G.stencil27(14, 14, 14, 1e-2, seed=3)
+@pytest.mark.parametrize("engine", ["tcgen05", "mma.sync"])
+@pytest.mark.parametrize("k", [14, 22])
+def test_fp32_factor_close_to_fp64_factor(engine, k):
+    """FP32 factor (3xTF32 updates on either tensor-core engine) against the FP64
+    factor: FP32-level agreement (1e-5 of the largest entry)."""
+    n, cp, ri, v = G.stencil27(k, k, k, 1e-2, seed=3)
     A = DistSparseMatrix.from_lower_csc(n, cp, ri, v)
-    L32 = factor(A, "FP32_IR").GetFactor()
+    M32 = factor(A, "FP32_IR", fp32_engine=engine)
+    M32.SetProfiling(True)
+    M32.DistributeMatrix(A)
+    M32.Factorize()
+    assert M32.GetProfile()["gemm_dmma"]["launches"] > 0  # 128 x 128 tiles ran
+    L32 = M32.GetFactor()
     L64 = factor(A, "FP64").GetFactor()
     assert np.max(np.abs(L32 - L64)) / np.max(np.abs(L64)) <= 1e-5
 
