@@ -264,6 +264,18 @@ def precision_comparison(torch, dev, stream, grid=80, reps=2):
                          "ir_iterations": inf.ir_iterations if prec == "FP32_IR" else 0}
         res["speedup_time_to_solution"] = res["FP64"]["time_to_solution_ms"] / res["FP32_IR"]["time_to_solution_ms"]
         out[f"delta={delta:g}"] = res
+        if delta == 1e-2:  # kernel breakdown of one eager (profiled) factor + solve per precision
+            for prec, M in handles.items():
+                M.SetProfiling(True)
+                M.DistributeMatrixDevice(dv.data_ptr())
+                M.Factorize()
+                M.SolveDevice(b.data_ptr(), x.data_ptr(), 1, n)
+                prof = M.GetProfile()
+                M.SetProfiling(False)
+                out.setdefault("kernels_profiled", {})[prec] = {
+                    k: {"ms": round(p["ms"], 3), "launches": p["launches"],
+                        "tflops": round(p["flops"] / (p["ms"] * 1e-3) / 1e12, 2) if p["ms"] > 0 else 0.0}
+                    for k, p in prof.items() if p["launches"]}
     for M in handles.values():
         M.close()
     torch.cuda.empty_cache()

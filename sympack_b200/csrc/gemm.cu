@@ -397,10 +397,11 @@ __global__ void __launch_bounds__(256, 1) k_gemm_tf32x3(FactorArgs a, const Tile
 // tcgen05.mma (kind::tf32, cta_group::1, M = 128, N = 128, K = 8) with the FP32
 // accumulator in tensor memory.  Operands are staged by all 256 threads: FP32
 // panel values are read from HBM (coalesced along the panel's rows), split into
-// tf32 hi / lo parts and written in the canonical MN-major 128-byte-swizzled
-// layout (32 consecutive rows of one column fill one 128 B line; 8 columns form
-// a 1 KB swizzle atom).  One elected thread issues the 12 MMAs of a 32-column
-// chunk (4 K steps x {lo*hi, hi*lo, hi*hi}) and commits them to the chunk's
+// tf32 hi / lo parts and written in the canonical K-major 128-byte-swizzled
+// layout (one 128 B line holds the 32 columns of a chunk for one row, 8 rows
+// form a 1 KB swizzle atom, 16 B pieces XOR-ed with the row), one 16 B store
+// per 4 columns.  One elected thread issues the 12 MMAs of a 32-column chunk
+// (4 K steps x {lo*hi, hi*lo, hi*hi}) and commits them to the chunk's
 // mbarrier; the next chunk is staged into the other buffer meanwhile.  The
 // epilogue reads the accumulator with tcgen05.ld (warp w: lanes 32(w%4).., column
 // half w/4), stages it in shared memory and scatters it like the other tiles.
@@ -416,24 +417,24 @@ constexpr size_t kUSmemBytes = 1024 + kUMainBytes + 4 * 128 * sizeof(int) + 64;
 constexpr int kUTmemCols = 128;
 constexpr long long kUWaitLimit = 1LL << 24;  // mbarrier polls before a tile gives up (seconds)
 
-// Byte offset of element (row m, column k) of a 128 x 32 operand part:
-// 32-row blocks 4 KB apart (leading byte offset), 8-column swizzle atoms 1 KB
-// apart (stride byte offset), 16 B chunks of a line XOR-ed with the column.
-__device__ __forceinline__ uint32_t umma_mn_offset(int m, int k) {
-  return (uint32_t)((m >> 5) * 4096 + (k >> 3) * 1024 + (k & 7) * 128 + ((((m & 31) >> 2) ^ (k & 7)) << 4) +
-                    (m & 3) * 4);
+// Byte offset of the 16 B piece holding columns 4*kg .. 4*kg+3 of row m in a
+// 128 x 32 operand part (K-major, 128-byte swizzle).
+__device__ __forceinline__ uint32_t umma_k_offset(int m, int kg) {
+  return (uint32_t)((m >> 3) * 1024 + (m & 7) * 128 + ((kg ^ (m & 7)) << 4));
 }
 
-// Shared-memory matrix descriptor: start >> 4, LBO 4096 >> 4, SBO 1024 >> 4,
-// descriptor version 1, 128-byte swizzle.
+// Shared-memory matrix descriptor of a K-major 128-byte-swizzled operand:
+// start >> 4, leading byte offset 16 (unused by this layout), stride byte
+// offset 1024 (8-row atoms), descriptor version 1, 128-byte swizzle.  A K step
+// of 8 tf32 columns inside the 128 B line advances the start by 32 bytes.
 __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr) {
-  return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)(4096 >> 4) << 16) | ((uint64_t)(1024 >> 4) << 32) |
+  return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)(16 >> 4) << 16) | ((uint64_t)(1024 >> 4) << 32) |
          (1ull << 46) | (2ull << 61);
 }
 
-// Instruction descriptor: D f32, A and B tf32, both MN-major, N = 128, M = 128.
-constexpr uint32_t kUIdesc = (1u << 4) | (2u << 7) | (2u << 10) | (1u << 15) | (1u << 16) |
-                             ((uint32_t)(kUN >> 3) << 17) | ((uint32_t)(kUM >> 4) << 24);
+// Instruction descriptor: D f32, A and B tf32, both K-major, N = 128, M = 128.
+constexpr uint32_t kUIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(kUN >> 3) << 17) |
+                             ((uint32_t)(kUM >> 4) << 24);
 
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, long long limit) {
   for (long long i = 0; i < limit; ++i) {
@@ -486,19 +487,21 @@ __global__ void __launch_bounds__(256, 1) k_gemm_tc32(FactorArgs a, const TileIt
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
   const uint32_t tmem = *tmem_slot;
 
-  // this thread's operand elements: row r, columns kq + 2q (q = 0..15)
+  // this thread's operand pieces: row r, column groups kq + 2q (q = 0..3) of 4 columns
   const int r = tid & 127, kq = tid >> 7;
   const bool arow = r < it.mrows, brow = r < it.ncols;
   float va[16], vb[16];
   auto load_chunk = [&](int kk) {
 #pragma unroll
-    for (int q = 0; q < 16; ++q) {
-      const int k = kk + kq + 2 * q;
-      const bool kok = k < it.kn;
-      const int64_t coff = (int64_t)(it.k0 + k) * ld;
-      va[q] = (kok && arow) ? g[it.a_row0 + r + coff] : 0.f;
-      vb[q] = (kok && brow) ? g[it.b_row0 + r + coff] : 0.f;
-    }
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int k = kk + 4 * (kq + 2 * q) + j;
+        const bool kok = k < it.kn;
+        const int64_t coff = (int64_t)(it.k0 + k) * ld;
+        va[4 * q + j] = (kok && arow) ? g[it.a_row0 + r + coff] : 0.f;
+        vb[4 * q + j] = (kok && brow) ? g[it.b_row0 + r + coff] : 0.f;
+      }
   };
   const int nk = (it.kn + kUK - 1) / kUK;
   load_chunk(0);
@@ -509,15 +512,21 @@ __global__ void __launch_bounds__(256, 1) k_gemm_tc32(FactorArgs a, const TileIt
     if (kt >= 2 && !mbar_wait(bar, (uint32_t)(((kt >> 1) - 1) & 1), kUWaitLimit)) sh_abort = 1;
     unsigned char* sb = base + st * kUStageBytes;
 #pragma unroll
-    for (int q = 0; q < 16; ++q) {
-      const uint32_t off = umma_mn_offset(r, kq + 2 * q);
-      uint32_t hi, lo;
-      split_tf32(va[q], hi, lo);
-      *reinterpret_cast<uint32_t*>(sb + off) = hi;
-      *reinterpret_cast<uint32_t*>(sb + kUOpBytes + off) = lo;
-      split_tf32(vb[q], hi, lo);
-      *reinterpret_cast<uint32_t*>(sb + 2 * kUOpBytes + off) = hi;
-      *reinterpret_cast<uint32_t*>(sb + 3 * kUOpBytes + off) = lo;
+    for (int q = 0; q < 4; ++q) {
+      const uint32_t off = umma_k_offset(r, kq + 2 * q);
+      uint4 ah, al, bh, bl;
+      split_tf32(va[4 * q + 0], ah.x, al.x);
+      split_tf32(va[4 * q + 1], ah.y, al.y);
+      split_tf32(va[4 * q + 2], ah.z, al.z);
+      split_tf32(va[4 * q + 3], ah.w, al.w);
+      split_tf32(vb[4 * q + 0], bh.x, bl.x);
+      split_tf32(vb[4 * q + 1], bh.y, bl.y);
+      split_tf32(vb[4 * q + 2], bh.z, bl.z);
+      split_tf32(vb[4 * q + 3], bh.w, bl.w);
+      *reinterpret_cast<uint4*>(sb + off) = ah;
+      *reinterpret_cast<uint4*>(sb + kUOpBytes + off) = al;
+      *reinterpret_cast<uint4*>(sb + 2 * kUOpBytes + off) = bh;
+      *reinterpret_cast<uint4*>(sb + 3 * kUOpBytes + off) = bl;
     }
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
     __syncthreads();
@@ -527,8 +536,8 @@ __global__ void __launch_bounds__(256, 1) k_gemm_tc32(FactorArgs a, const TileIt
       const uint32_t sa = base_addr + st * kUStageBytes;
 #pragma unroll
       for (int ks = 0; ks < kUK / 8; ++ks) {
-        const uint64_t ahi = umma_desc(sa + ks * 1024), alo = umma_desc(sa + kUOpBytes + ks * 1024);
-        const uint64_t bhi = umma_desc(sa + 2 * kUOpBytes + ks * 1024), blo = umma_desc(sa + 3 * kUOpBytes + ks * 1024);
+        const uint64_t ahi = umma_desc(sa + ks * 32), alo = umma_desc(sa + kUOpBytes + ks * 32);
+        const uint64_t bhi = umma_desc(sa + 2 * kUOpBytes + ks * 32), blo = umma_desc(sa + 3 * kUOpBytes + ks * 32);
         const uint64_t pa[3] = {alo, ahi, ahi}, pb[3] = {bhi, blo, bhi};
 #pragma unroll
         for (int p = 0; p < 3; ++p) {
