@@ -153,8 +153,9 @@ int spb_solve_device(spb_handle* h, const double* d_rhs, double* d_x, int32_t nr
  * or allocating library routine: its scratch (the permuted right-hand sides and
  * the dependency counters) lives in one static __device__ array of 33 MiB that
  * every GPU which loads the library holds until the process exits.
- * Limits: n * nrhs <= 4,194,304 and at most 87,380 supernodes; larger requests
- * return SPB_ERR_INVALID with a message saying so.
+ * Limits: n * nrhs <= 4,194,304, and 2 + 3 * nsuper + 2 * (number of
+ * 64-column blocks over all supernodes) <= 262,144 dependency counters;
+ * larger requests return SPB_ERR_INVALID with a message saying so.
  * The first call on a device resolves the array's device address
  * (cudaGetSymbolAddress); make that first call before any stream capture.
  * Every call on a device shares the array: calls whose work overlaps on the GPU

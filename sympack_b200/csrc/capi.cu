@@ -276,7 +276,7 @@ void enqueue_solve(spb_handle* h, int nrhs) {
   const spb::Plan& P = h->plan;
   const int ns = P.nsuper;
   for (int c0 = 0; c0 < nrhs; c0 += 64) {
-    cudaMemsetAsync(h->dsync, 0, sizeof(int32_t) * (2 + 3 * (size_t)ns), h->stream);
+    cudaMemsetAsync(h->dsync, 0, sizeof(int32_t) * spb::solve_sync_ints(P), h->stream);
     spb::dev::PSolveArgs a{};
     a.L = h->dL;
     a.fp32 = h->fp32;
@@ -296,6 +296,7 @@ void enqueue_solve(spb_handle* h, int nrhs) {
     a.ntasks = (int)P.fwd_tasks.size();
     a.counter = h->dsync;
     a.blkdone = h->dsync + 2 + ns;
+    a.upd = h->dsync + 2 + 3 * (size_t)ns;
     if (h->profiling) cudaEventRecord(h->events[e0], h->stream);
     spb::dev::launch_solve_persistent(h->stream, a, true);
     if (h->profiling) cudaEventRecord(h->events[e0 + 1], h->stream);
@@ -303,6 +304,7 @@ void enqueue_solve(spb_handle* h, int nrhs) {
     a.ntasks = (int)P.bwd_tasks.size();
     a.counter = h->dsync + 1;
     a.blkdone = h->dsync + 2 + 2 * ns;
+    a.upd = h->dsync + 2 + 3 * (size_t)ns + P.nblk_total;
     if (h->profiling) cudaEventRecord(h->events[e0 + 2], h->stream);
     spb::dev::launch_solve_persistent(h->stream, a, false);
     if (h->profiling) cudaEventRecord(h->events[e0 + 3], h->stream);
@@ -549,7 +551,8 @@ int64_t predict_bytes(const spb_handle* h, bool fp32, int nrhs) {
   t += b((int64_t)std::max(1, P.max_diag_slots) * (64 * 64 + 64), 8);
   t += b(P.tile_items.size(), sizeof(spb::TileItem)) + b(n, 4) + b(ns, 4);
   t += b(P.fwd_tasks.size(), sizeof(spb::SolveTask)) + b(P.bwd_tasks.size(), sizeof(spb::SolveTask));
-  t += b(P.fwd_pending.size(), 4) + b(P.sparent.size(), 4) + b(2 + 3 * ns, 4) + b(1, sizeof(Status));
+  t += b(P.fwd_pending.size(), 4) + b(P.sparent.size(), 4) + b((int64_t)spb::solve_sync_ints(P), 4);
+  t += b(1, sizeof(Status));
   if (fp32) {
     int64_t offdiag = 0;
     for (int64_t c = 1; c <= n; ++c)
@@ -618,7 +621,7 @@ int install_device(spb_handle* h) {
   SPB_CK(h, dalloc(h, &h->dbwd, P.bwd_tasks.size()));
   SPB_CK(h, dalloc(h, &h->dexpected, P.fwd_pending.size()));
   SPB_CK(h, dalloc(h, &h->dsparent, P.sparent.size()));
-  SPB_CK(h, dalloc(h, &h->dsync, 2 + 3 * (size_t)P.nsuper));
+  SPB_CK(h, dalloc(h, &h->dsync, spb::solve_sync_ints(P)));
   SPB_CK(h, dalloc(h, &h->dstatus, 1));
   SPB_CK(h, cudaStreamSynchronize(h->own_stream));  // allocations ready before h->stream uses them
   auto up = [&](void* d, const void* s, size_t bytes) {
@@ -1216,8 +1219,10 @@ extern "C" int spb_solve_device_noalloc(spb_handle* h, const double* d_rhs, doub
              "static scratch (32 MiB)", (long long)n * nrhs, kNoAllocXBytes / sizeof(double));
     return fail(h, SPB_ERR_INVALID, msg);
   }
-  if ((2 + 3 * (size_t)ns) * sizeof(int32_t) > kNoAllocSyncBytes)
-    return fail(h, SPB_ERR_INVALID, "solve_noalloc: more supernodes than the static scratch counters hold (87,380)");
+  if (spb::solve_sync_ints(h->plan) * sizeof(int32_t) > kNoAllocSyncBytes)
+    return fail(h, SPB_ERR_INVALID,
+                "solve_noalloc: 2 + 3 * supernodes + 2 * (64-column blocks) exceeds the 262,144 counters of the "
+                "static scratch");
   SPB_CK(h, cudaSetDevice(h->device));
   unsigned char* base = nullptr;
   int rc = noalloc_scratch(h, &base);
@@ -1228,7 +1233,7 @@ extern "C" int spb_solve_device_noalloc(spb_handle* h, const double* d_rhs, doub
   spb::dev::launch_permute_in(h->stream, X, n, d_rhs, ld, h->dinvp0, n, nrhs);
   for (int c0 = 0; c0 < nrhs; c0 += 64) {
     // counters must start at zero; the array keeps whatever the last call left
-    SPB_CK(h, cudaMemsetAsync(sync, 0, sizeof(int32_t) * (2 + 3 * (size_t)ns), h->stream));
+    SPB_CK(h, cudaMemsetAsync(sync, 0, sizeof(int32_t) * spb::solve_sync_ints(P), h->stream));
     spb::dev::PSolveArgs a{};
     a.L = h->dL;
     a.fp32 = h->fp32;
@@ -1247,11 +1252,13 @@ extern "C" int spb_solve_device_noalloc(spb_handle* h, const double* d_rhs, doub
     a.ntasks = (int)P.fwd_tasks.size();
     a.counter = sync;
     a.blkdone = sync + 2 + ns;
+    a.upd = sync + 2 + 3 * (size_t)ns;
     spb::dev::launch_solve_persistent(h->stream, a, true);
     a.tasks = h->dbwd;
     a.ntasks = (int)P.bwd_tasks.size();
     a.counter = sync + 1;
     a.blkdone = sync + 2 + 2 * ns;
+    a.upd = sync + 2 + 3 * (size_t)ns + P.nblk_total;
     spb::dev::launch_solve_persistent(h->stream, a, false);
   }
   spb::dev::launch_permute_out(h->stream, d_x, ld, X, n, h->dinvp0, n, nrhs);

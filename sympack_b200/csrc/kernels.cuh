@@ -40,9 +40,9 @@ void launch_gemm(cudaStream_t st, const FactorArgs& a, const TileItem* items, in
 
 // Solves work on the permuted right-hand sides X (n x nrhs, column-major, leading dimension ldx).
 
-// Persistent sweeps (one launch each).  counter, arrived and blkdone must be
-// zero at launch; expected[s] is the number of forward off-diagonal tiles that
-// write rows of supernode s.
+// Persistent sweeps (one launch each).  counter, arrived, blkdone and upd must
+// be zero at launch; expected[s] is the number of forward off-diagonal tiles
+// that write rows of supernode s.
 struct PSolveArgs {
   const void* L;     // factor arena (double, or float when fp32)
   bool fp32;
@@ -59,6 +59,7 @@ struct PSolveArgs {
   const int32_t* expected;
   int32_t* arrived;
   int32_t* blkdone;
+  int32_t* upd;      // per 64-column block: updates landed (meta.boff + block)
   Status* status;
   long long spin_limit;  // polls (about 128 ns apart) before a wait gives up
 };

@@ -28,6 +28,9 @@ Plan build_plan(const Symbolic& sym, const PlanParams& prm) {
     m.ld = (int32_t)round_up(m.h, 4);
     m.off = off;
     m.lidx = sym.xlindx[s] - 1;
+    m.boff = P.nblk_total;
+    m.pad = 0;
+    P.nblk_total += (m.w + 63) / 64;
     off += round_up((int64_t)m.ld * m.w, 32);
   }
   P.arena_elems = off;
@@ -183,18 +186,23 @@ Plan build_plan(const Symbolic& sym, const PlanParams& prm) {
   }
   for (const SnMeta& m : P.meta) P.solve_sweep_bytes += 8.0 * m.h * m.w;
 
-  // Persistent solve task lists.  Both are ordered by elimination-tree height
-  // level (forward: leaves first; backward: root level first) so that tasks
-  // handed out together are independent; within a supernode, blocks go in
-  // dependency order.  Every task a task waits on is listed earlier.
+  // Persistent solve task lists, ordered by elimination-tree height level
+  // (forward: leaves first; backward: root level first) so that tasks handed
+  // out together are independent.  Within a supernode the sweep is
+  // right-looking by 64-column blocks: a finished diagonal block releases its
+  // updates of every later block at once, so the per-supernode critical path
+  // is one block solve plus one block update per block.
   P.fwd_pending.assign(ns, 0);
   for (int L = 0; L < H; ++L)
     for (int s : P.level_sn[L]) {
       const SnMeta& m = P.meta[s];
       const int nblk = (m.w + 63) / 64, noff = (m.h - m.w + 63) / 64;
-      for (int t = 0; t < nblk; ++t) P.fwd_tasks.push_back(SolveTask{s, t});
+      for (int i = 0; i < nblk; ++i) {
+        P.fwd_tasks.push_back(SolveTask{s, 0, i, i});
+        for (int t = i + 1; t < nblk; ++t) P.fwd_tasks.push_back(SolveTask{s, 1, i, t});
+      }
       for (int u = 0; u < noff; ++u) {
-        P.fwd_tasks.push_back(SolveTask{s, -u - 1});
+        P.fwd_tasks.push_back(SolveTask{s, 2, 0, u});
         int r0 = m.w + 64 * u, r1 = std::min(m.h, r0 + 64), last = -1;
         for (int r = r0; r < r1; ++r) {
           int t = P.supmember0[P.rows[m.lidx + r]];
@@ -206,7 +214,10 @@ Plan build_plan(const Symbolic& sym, const PlanParams& prm) {
   for (int L = H - 1; L >= 0; --L)
     for (int s : P.level_sn[L]) {
       const int nblk = (P.meta[s].w + 63) / 64;
-      for (int t = nblk - 1; t >= 0; --t) P.bwd_tasks.push_back(SolveTask{s, t});
+      for (int t = nblk - 1; t >= 0; --t) {
+        P.bwd_tasks.push_back(SolveTask{s, 0, t, t});
+        for (int u = 0; u < t; ++u) P.bwd_tasks.push_back(SolveTask{s, 1, t, u});
+      }
     }
   return P;
 }

@@ -31,6 +31,8 @@ struct SnMeta {
   int32_t ld;    // leading dimension of the panel
   int64_t off;   // element offset of the panel in the factor arena
   int64_t lidx;  // offset of this supernode's row list in the device row array
+  int32_t boff;  // first of this supernode's 64-column blocks in the per-block solve counters
+  int32_t pad;
 };
 
 // One tile of a Schur-complement product  C = A * B^T  over panel columns
@@ -73,13 +75,19 @@ struct PanelItem {
   int32_t slot;   // scratch slot holding this step's L11^-1 for the supernode
 };
 
-// One task of the persistent triangular solves (64-row / 64-column units).
-//   idx >= 0: diagonal column block idx of supernode s
-//   idx <  0: off-diagonal row tile (-idx - 1), rows w + 64 * (-idx - 1) ...
+// One task of the persistent triangular solves, in 64-row / 64-column units
+// (i, t: column blocks of supernode s; u: 64-row tile below the diagonal block).
+//   forward  kind 0  D(t):    X_t <- L_tt^-1 X_t once every update into block t has landed
+//            kind 1  U(i, t): X_t -= L_ti X_i                          (i < t, after D(i))
+//            kind 2  O(u):    X[rows of tile u] -= sum_i L_ui X_i, scattered to the ancestors
+//   backward kind 0  B(t):    X_t <- L_tt^-T (X_t - sum over ancestor rows r of L_rt^T X_r)
+//            kind 1  V(t, u): X_u -= L_tu^T X_t                        (u < t, after B(t))
 // Task lists are topological: every task a task waits on comes earlier.
 struct SolveTask {
   int32_t s;
-  int32_t idx;
+  int32_t kind;
+  int32_t i;
+  int32_t t;
 };
 
 struct Plan {
@@ -108,6 +116,7 @@ struct Plan {
   // and per supernode the number of forward off-diagonal tiles writing its rows
   std::vector<SolveTask> fwd_tasks, bwd_tasks;
   std::vector<int32_t> fwd_pending;
+  int32_t nblk_total = 0;  // 64-column blocks over all supernodes (per-block solve counters)
   // algorithmic bytes of one sweep: every panel element read once
   double solve_sweep_bytes = 0.0;
 };
@@ -121,6 +130,11 @@ struct PlanParams {
 };
 
 Plan build_plan(const Symbolic& s, const PlanParams& p = PlanParams());
+
+// int32 counters one persistent solve pass uses: two task counters, then per
+// supernode arrivals and forward / backward done-blocks, then per 64-column
+// block forward / backward update counts.
+inline size_t solve_sync_ints(const Plan& P) { return 2 + 3 * (size_t)P.nsuper + 2 * (size_t)P.nblk_total; }
 
 // Destination of each entry of A's lower triangle (input order) in the arena,
 // DistributeMatrix (symPACKMatrix2D.hpp:6336-6576) done once per structure.

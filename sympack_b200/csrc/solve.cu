@@ -87,8 +87,23 @@ __device__ __forceinline__ void block_gemv_t(double* acc, const double* A, const
 }
 
 // Stage L rows [r0, r0+m) x columns [c0, c0+kk) of a panel into A (ld kPld), widened to FP64.
+// A full 64 x 64 block is loaded with all 16 loads of a thread in flight.
 template <class T>
 __device__ __forceinline__ void stage_block(double* A, const T* P, int64_t ld, int r0, int m, int c0, int kk) {
+  if (m == kT && kk == kT) {
+    T v[kT * kT / kThreads];
+#pragma unroll
+    for (int q = 0; q < kT * kT / kThreads; ++q) {
+      const int idx = threadIdx.x + q * kThreads, k = idx / kT, r = idx - k * kT;
+      v[q] = P[(r0 + r) + (int64_t)(c0 + k) * ld];
+    }
+#pragma unroll
+    for (int q = 0; q < kT * kT / kThreads; ++q) {
+      const int idx = threadIdx.x + q * kThreads, k = idx / kT, r = idx - k * kT;
+      A[r + k * kPld] = (double)v[q];
+    }
+    return;
+  }
   for (int idx = threadIdx.x; idx < m * kk; idx += kThreads) {
     int k = idx / m, r = idx - k * m;
     A[r + k * kPld] = (double)P[(r0 + r) + (int64_t)(c0 + k) * ld];
@@ -142,6 +157,28 @@ __device__ void block_trsv(double* acc, const double* A, int kk, int nr) {
   }
 }
 
+// Next task of a persistent sweep; the whole block takes the same branch
+// (thread 0 alone reads the counter and the status word, a barrier reached by
+// only part of a block would hang).  -1 = no task left or a failure recorded.
+__device__ __forceinline__ int next_task(const PSolveArgs& a, int* sh_task, int* sh_stop) {
+  if (threadIdx.x == 0) {
+    *sh_task = atomicAdd(a.counter, 1);
+    *sh_stop = status_code(a.status) != 0;
+  }
+  __syncthreads();
+  const int tk = *sh_task;
+  const bool stop = *sh_stop != 0;
+  __syncthreads();
+  return (tk >= a.ntasks || stop) ? -1 : tk;
+}
+
+// Publish a block's writes, then bump a counter (thread 0).
+__device__ __forceinline__ void signal(int32_t* counter) {
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) atomicAdd(counter, 1);
+}
+
 template <class T>
 __global__ void __launch_bounds__(kThreads) k_solve_forward(PSolveArgs a) {
   extern __shared__ __align__(16) double sm[];
@@ -151,37 +188,21 @@ __global__ void __launch_bounds__(kThreads) k_solve_forward(PSolveArgs a) {
   __shared__ int sh_task, sh_stop, sh_ok;
   const int nr = a.nrhs;
   for (;;) {
-    // thread 0 alone reads the counter and the status word, so the whole block
-    // takes the same branch (a barrier reached by only part of a block hangs)
-    if (threadIdx.x == 0) {
-      sh_task = atomicAdd(a.counter, 1);
-      sh_stop = status_code(a.status) != 0;
-    }
-    __syncthreads();
-    const int tk = sh_task;
-    const bool stop = sh_stop != 0;
-    __syncthreads();
-    if (tk >= a.ntasks || stop) return;
+    const int tk = next_task(a, &sh_task, &sh_stop);
+    if (tk < 0) return;
     const SolveTask task = a.tasks[tk];
     const int s = task.s;
     const SnMeta m = a.meta[s];
     const T* P = static_cast<const T*>(a.L) + m.off;
     const int32_t* rl = a.rows + m.lidx;
     const int64_t ld = m.ld;
-    if (task.idx >= 0) {
-      // diagonal block t: all descendant updates into these rows, then blocks 0..t-1
-      const int t = task.idx, r0 = t * kT, bt = min(kT, m.w - r0);
+    if (task.kind == 0) {
+      // D(t): descendants' and earlier blocks' updates have landed in X_t; X_t <- L_tt^-1 X_t
+      const int t = task.t, r0 = t * kT, bt = min(kT, m.w - r0);
       if (!wait_geq(a.arrived + s, a.expected[s], a.status, s, &sh_ok, a.spin_limit)) return;
-      stage_x(acc, a.X, a.ldx, m.fc + r0, nullptr, bt, nr);
-      for (int i = 0; i < t; ++i) {
-        if (!wait_geq(a.blkdone + s, i + 1, a.status, s, &sh_ok, a.spin_limit)) return;
-        stage_x(Bx, a.X, a.ldx, m.fc + i * kT, nullptr, kT, nr);
-        stage_block(Ab, P, ld, r0, bt, i * kT, kT);
-        __syncthreads();
-        block_gemv<true>(acc, Ab, Bx, bt, kT, nr);
-        __syncthreads();
-      }
+      if (!wait_geq(a.upd + m.boff + t, t, a.status, s, &sh_ok, a.spin_limit)) return;
       stage_block(Ab, P, ld, r0, bt, r0, bt);
+      stage_x(acc, a.X, a.ldx, m.fc + r0, nullptr, bt, nr);
       __syncthreads();
       block_trsv<true>(acc, Ab, bt, nr);
       __syncthreads();
@@ -189,19 +210,32 @@ __global__ void __launch_bounds__(kThreads) k_solve_forward(PSolveArgs a) {
         int c = idx / bt, r = idx - c * bt;
         a.X[m.fc + r0 + r + c * a.ldx] = acc[r + c * kT];
       }
-      __threadfence();
+      signal(a.blkdone + s);
+    } else if (task.kind == 1) {
+      // U(i, t): X_t -= L_ti X_i
+      const int i = task.i, t = task.t, bi = min(kT, m.w - i * kT), r0 = t * kT, bt = min(kT, m.w - r0);
+      stage_block(Ab, P, ld, r0, bt, i * kT, bi);  // L is final: load before waiting
+      if (!wait_geq(a.blkdone + s, i + 1, a.status, s, &sh_ok, a.spin_limit)) return;
+      stage_x(Bx, a.X, a.ldx, m.fc + i * kT, nullptr, bi, nr);
+      for (int idx = threadIdx.x; idx < kT * nr; idx += kThreads) acc[idx] = 0.0;
       __syncthreads();
-      if (threadIdx.x == 0) atomicAdd(a.blkdone + s, 1);
+      block_gemv<false>(acc, Ab, Bx, bt, bi, nr);
+      __syncthreads();
+      for (int idx = threadIdx.x; idx < bt * nr; idx += kThreads) {
+        int c = idx / bt, r = idx - c * bt;
+        atomicAdd(a.X + m.fc + r0 + r + c * a.ldx, -acc[r + c * kT]);
+      }
+      signal(a.upd + m.boff + t);
     } else {
-      // off-diagonal rows: Y_K[rows] -= L_KJ Y_J, accumulated over the column blocks
-      const int u = -task.idx - 1, r0 = m.w + u * kT, bu = min(kT, m.h - r0);
+      // O(u): off-diagonal rows, Y_K[rows] -= L_KJ Y_J accumulated over the column blocks
+      const int u = task.t, r0 = m.w + u * kT, bu = min(kT, m.h - r0);
       const int nblk = (m.w + kT - 1) / kT;
-      for (int idx = threadIdx.x; idx < kT * nr; idx += kThreads) acc[idx % kT + (idx / kT) * kT] = 0.0;
+      for (int idx = threadIdx.x; idx < kT * nr; idx += kThreads) acc[idx] = 0.0;
       for (int i = 0; i < nblk; ++i) {
         const int bi = min(kT, m.w - i * kT);
+        stage_block(Ab, P, ld, r0, bu, i * kT, bi);
         if (!wait_geq(a.blkdone + s, i + 1, a.status, s, &sh_ok, a.spin_limit)) return;
         stage_x(Bx, a.X, a.ldx, m.fc + i * kT, nullptr, bi, nr);
-        stage_block(Ab, P, ld, r0, bu, i * kT, bi);
         __syncthreads();
         block_gemv<false>(acc, Ab, Bx, bu, bi, nr);
         __syncthreads();
@@ -234,17 +268,8 @@ __global__ void __launch_bounds__(kThreads) k_solve_backward(PSolveArgs a) {
   __shared__ int sh_task, sh_stop, sh_ok;
   const int nr = a.nrhs;
   for (;;) {
-    // thread 0 alone reads the counter and the status word, so the whole block
-    // takes the same branch (a barrier reached by only part of a block hangs)
-    if (threadIdx.x == 0) {
-      sh_task = atomicAdd(a.counter, 1);
-      sh_stop = status_code(a.status) != 0;
-    }
-    __syncthreads();
-    const int tk = sh_task;
-    const bool stop = sh_stop != 0;
-    __syncthreads();
-    if (tk >= a.ntasks || stop) return;
+    const int tk = next_task(a, &sh_task, &sh_stop);
+    if (tk < 0) return;
     const SolveTask task = a.tasks[tk];
     const int s = task.s;
     const SnMeta m = a.meta[s];
@@ -252,40 +277,53 @@ __global__ void __launch_bounds__(kThreads) k_solve_backward(PSolveArgs a) {
     const int32_t* rl = a.rows + m.lidx;
     const int64_t ld = m.ld;
     const int nblk = (m.w + kT - 1) / kT;
-    const int t = task.idx, c0 = t * kT, bt = min(kT, m.w - c0);
-    const int par = a.sparent[s];
-    if (par >= 0 && !wait_geq(a.blkdone + par, (a.meta[par].w + kT - 1) / kT, a.status, s, &sh_ok, a.spin_limit)) return;
-    stage_x(acc, a.X, a.ldx, m.fc + c0, nullptr, bt, nr);
-    // rows owned by ancestors (final once the parent is done)
-    for (int rr = m.w; rr < m.h; rr += kT) {
-      const int br = min(kT, m.h - rr);
-      stage_x(Bx, a.X, a.ldx, 0, rl + rr, br, nr);
-      stage_block(Ab, P, ld, rr, br, c0, bt);
+    if (task.kind == 0) {
+      // B(t): X_t <- L_tt^-T (X_t - sum over ancestor rows of L_rt^T X_r - later blocks' updates)
+      const int t = task.t, c0 = t * kT, bt = min(kT, m.w - c0);
+      const int par = a.sparent[s];
+      for (int idx = threadIdx.x; idx < kT * nr; idx += kThreads) acc[idx] = 0.0;
+      if (par >= 0 && !wait_geq(a.blkdone + par, (a.meta[par].w + kT - 1) / kT, a.status, s, &sh_ok, a.spin_limit))
+        return;
+      for (int rr = m.w; rr < m.h; rr += kT) {  // ancestors' rows are final once the parent is done
+        const int br = min(kT, m.h - rr);
+        stage_x(Bx, a.X, a.ldx, 0, rl + rr, br, nr);
+        stage_block(Ab, P, ld, rr, br, c0, bt);
+        __syncthreads();
+        block_gemv_t(acc, Ab, Bx, br, bt, nr);
+        __syncthreads();
+      }
+      stage_block(Ab, P, ld, c0, bt, c0, bt);
+      if (!wait_geq(a.upd + m.boff + t, nblk - 1 - t, a.status, s, &sh_ok, a.spin_limit)) return;
+      stage_x(Bx, a.X, a.ldx, m.fc + c0, nullptr, bt, nr);
       __syncthreads();
-      block_gemv_t(acc, Ab, Bx, br, bt, nr);
+      for (int idx = threadIdx.x; idx < bt * nr; idx += kThreads) {
+        int c = idx / bt, r = idx - c * bt;
+        acc[r + c * kT] += Bx[r + c * kT];
+      }
       __syncthreads();
-    }
-    // later diagonal blocks of this supernode, newest first
-    for (int u = nblk - 1; u > t; --u) {
-      if (!wait_geq(a.blkdone + s, nblk - u, a.status, s, &sh_ok, a.spin_limit)) return;
-      const int rr = u * kT, br = min(kT, m.w - rr);
+      block_trsv<false>(acc, Ab, bt, nr);
+      __syncthreads();
+      for (int idx = threadIdx.x; idx < bt * nr; idx += kThreads) {
+        int c = idx / bt, r = idx - c * bt;
+        a.X[m.fc + c0 + r + c * a.ldx] = acc[r + c * kT];
+      }
+      signal(a.blkdone + s);
+    } else {
+      // V(t, u): X_u -= L_tu^T X_t
+      const int t = task.i, u = task.t, rr = t * kT, br = min(kT, m.w - rr), c0 = u * kT, bu = min(kT, m.w - c0);
+      stage_block(Ab, P, ld, rr, br, c0, bu);
+      if (!wait_geq(a.blkdone + s, nblk - t, a.status, s, &sh_ok, a.spin_limit)) return;
       stage_x(Bx, a.X, a.ldx, m.fc + rr, nullptr, br, nr);
-      stage_block(Ab, P, ld, rr, br, c0, bt);
+      for (int idx = threadIdx.x; idx < kT * nr; idx += kThreads) acc[idx] = 0.0;
       __syncthreads();
-      block_gemv_t(acc, Ab, Bx, br, bt, nr);
+      block_gemv_t(acc, Ab, Bx, br, bu, nr);
       __syncthreads();
+      for (int idx = threadIdx.x; idx < bu * nr; idx += kThreads) {
+        int c = idx / bu, k = idx - c * bu;
+        atomicAdd(a.X + m.fc + c0 + k + c * a.ldx, acc[k + c * kT]);
+      }
+      signal(a.upd + m.boff + u);
     }
-    stage_block(Ab, P, ld, c0, bt, c0, bt);
-    __syncthreads();
-    block_trsv<false>(acc, Ab, bt, nr);
-    __syncthreads();
-    for (int idx = threadIdx.x; idx < bt * nr; idx += kThreads) {
-      int c = idx / bt, r = idx - c * bt;
-      a.X[m.fc + c0 + r + c * a.ldx] = acc[r + c * kT];
-    }
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) atomicAdd(a.blkdone + s, 1);
   }
 }
 
