@@ -48,6 +48,8 @@ def parse():
     ap.add_argument("--grid", type=int, default=60, help="grid edge of the 3D Laplacian (60 = the named workload)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-precision", action="store_true", help="skip the FP64 vs FP32+IR comparison")
+    ap.add_argument("--precision-grid", type=int, default=80,
+                    help="grid edge of the 27-point stencil of the precision comparison (80 = the named workload)")
     ap.add_argument("--batch-systems", type=int, default=300,
                     help="systems of the batching workload (2000 = the named workload; host MMD of its random "
                          "graphs takes minutes)")
@@ -582,7 +584,7 @@ def run_ours(args):
 
     precision = None
     if not args.no_precision:
-        precision = precision_comparison(torch, dev, stream)
+        precision = precision_comparison(torch, dev, stream, grid=args.precision_grid)
 
     batching = None
     if not args.no_batch:
