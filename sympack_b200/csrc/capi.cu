@@ -46,6 +46,9 @@ struct spb_handle {
   spb::SnMeta* dmeta = nullptr;
   int32_t* drows = nullptr;
   int32_t* dsupm = nullptr;
+  int32_t* drowgrp = nullptr;      // relative-index group of each row-list entry
+  spb::RelGroup* dgroups = nullptr;
+  int32_t* drel = nullptr;
   int64_t* damap = nullptr;
   double* dA = nullptr;
   int32_t* dsmall = nullptr;
@@ -150,6 +153,9 @@ spb::dev::FactorArgs factor_args(spb_handle* h) {
   a.rows = h->drows;
   a.supmember = h->dsupm;
   a.status = h->dstatus;
+  a.row_group = h->drowgrp;
+  a.groups = h->dgroups;
+  a.rel = h->drel;
   a.fp32 = h->fp32;
   a.tc32 = h->opt.fp32_engine == 0;
   return a;
@@ -546,6 +552,7 @@ int64_t predict_bytes(const spb_handle* h, bool fp32, int nrhs) {
   auto b = [](int64_t count, size_t size) { return std::max<int64_t>(count, 1) * (int64_t)size; };
   int64_t t = b(P.arena_elems, fp32 ? sizeof(float) : sizeof(double));
   t += b(P.meta.size(), sizeof(spb::SnMeta)) + b(P.rows.size(), 4) + b(P.supmember0.size(), 4);
+  t += b(P.row_group.size(), 4) + b(P.groups.size(), sizeof(spb::RelGroup)) + b(P.rel.size(), 4);
   t += b(h->amap.size(), 8) + b(h->nnz_a, 8) + b(P.small_items.size(), 4);
   t += b(P.panel_items.size(), sizeof(spb::PanelItem));
   t += b((int64_t)std::max(1, P.max_diag_slots) * (64 * 64 + 64), 8);
@@ -609,6 +616,9 @@ int install_device(spb_handle* h) {
   SPB_CK(h, dalloc(h, &h->dmeta, P.meta.size()));
   SPB_CK(h, dalloc(h, &h->drows, P.rows.size()));
   SPB_CK(h, dalloc(h, &h->dsupm, P.supmember0.size()));
+  SPB_CK(h, dalloc(h, &h->drowgrp, P.row_group.size()));
+  SPB_CK(h, dalloc(h, &h->dgroups, P.groups.size()));
+  SPB_CK(h, dalloc(h, &h->drel, P.rel.size()));
   SPB_CK(h, dalloc(h, &h->damap, amap.size()));
   SPB_CK(h, dalloc(h, &h->dA, (size_t)h->nnz_a));
   SPB_CK(h, dalloc(h, &h->dsmall, P.small_items.size()));
@@ -630,6 +640,9 @@ int install_device(spb_handle* h) {
   SPB_CK(h, up(h->dmeta, P.meta.data(), P.meta.size() * sizeof(spb::SnMeta)));
   SPB_CK(h, up(h->drows, P.rows.data(), P.rows.size() * 4));
   SPB_CK(h, up(h->dsupm, P.supmember0.data(), P.supmember0.size() * 4));
+  SPB_CK(h, up(h->drowgrp, P.row_group.data(), P.row_group.size() * 4));
+  SPB_CK(h, up(h->dgroups, P.groups.data(), P.groups.size() * sizeof(spb::RelGroup)));
+  SPB_CK(h, up(h->drel, P.rel.data(), P.rel.size() * 4));
   SPB_CK(h, up(h->damap, amap.data(), amap.size() * 8));
   SPB_CK(h, up(h->dsmall, P.small_items.data(), P.small_items.size() * 4));
   SPB_CK(h, up(h->dpanel, P.panel_items.data(), P.panel_items.size() * sizeof(spb::PanelItem)));

@@ -28,23 +28,18 @@ __device__ __forceinline__ void report_status(Status* st, int code, int s, int c
   }
 }
 
-__device__ __forceinline__ int find_row(const int32_t* __restrict__ rl, int h, int row) {
-  int lo = 0, hi = h;
-  while (lo < hi) {
-    int mid = (lo + hi) >> 1;
-    if (rl[mid] < row) lo = mid + 1;
-    else hi = mid;
-  }
-  return (lo < h && rl[lo] == row) ? lo : -1;
-}
-
 // Apply a BM x BN tile of C held in shared memory (column-major, leading dimension ldc).
+// Mode 1 targets come from the relative indices computed with the plan: per tile
+// column its target column base and group offset (staged in shared memory),
+// then one coalesced position load and one atomic per element.  Consecutive
+// threads take consecutive rows of a column, so both are coalesced.
 template <int BM, int BN, int NT, class T, class CT>
 __device__ void tile_epilogue(const FactorArgs& a, const TileItem& it, const SnMeta& m, const CT* Cs, int ldc,
-                              int* Rr, int* Rc, int* Tc, int* Pos) {
+                              int64_t* Cbase, int64_t* Crel) {
   const int tid = threadIdx.x;
-  T* g = static_cast<T*>(a.L) + m.off;
+  T* L = static_cast<T*>(a.L);
   if (it.mode == 0) {
+    T* g = L + m.off;
     const int64_t ld = m.ld;
     for (int idx = tid; idx < BM * BN; idx += NT) {
       int c = idx / BM, r = idx - c * BM;
@@ -56,37 +51,20 @@ __device__ void tile_epilogue(const FactorArgs& a, const TileItem& it, const SnM
     return;
   }
   const int32_t* rl = a.rows + m.lidx;
-  for (int i = tid; i < BM; i += NT) Rr[i] = i < it.mrows ? rl[it.a_row0 + i] : INT_MAX;
-  for (int i = tid; i < BN; i += NT) {
-    int rc = i < it.ncols ? rl[it.b_row0 + i] : INT_MAX;
-    Rc[i] = rc;
-    Tc[i] = i < it.ncols ? a.supmember[rc] : -1;
+  for (int c = tid; c < BN; c += NT) {
+    if (c < it.ncols) {
+      const int jc = it.b_row0 + c;
+      const RelGroup g = a.groups[a.row_group[m.lidx + jc]];
+      const SnMeta mt = a.meta[g.t];
+      Cbase[c] = mt.off + (int64_t)(rl[jc] - mt.fc) * mt.ld;
+      Crel[c] = g.rel_off - g.j0;
+    }
   }
   __syncthreads();
-  int c = 0;
-  while (c < it.ncols) {
-    const int t = Tc[c];
-    int ce = c + 1;
-    while (ce < it.ncols && Tc[ce] == t) ++ce;
-    const SnMeta mt = a.meta[t];
-    for (int i = tid; i < BM; i += NT) {
-      int pos = -1;
-      if (i < it.mrows && Rr[i] >= Rc[c]) {
-        pos = find_row(a.rows + mt.lidx, mt.h, Rr[i]);
-        if (pos < 0) report_status(a.status, 2, it.s, Rr[i]);
-      }
-      Pos[i] = pos;
-    }
-    __syncthreads();
-    T* gt = static_cast<T*>(a.L) + mt.off;
-    const int ncol = ce - c;
-    for (int idx = tid; idx < ncol * BM; idx += NT) {
-      int cc = c + idx / BM, r = idx % BM;
-      int p = Pos[r];
-      if (p >= 0 && Rr[r] >= Rc[cc]) atomicAdd(gt + (int64_t)(Rc[cc] - mt.fc) * mt.ld + p, (T)(-Cs[r + cc * ldc]));
-    }
-    __syncthreads();
-    c = ce;
+  for (int idx = tid; idx < BM * it.ncols; idx += NT) {
+    const int c = idx / BM, i = idx - c * BM;
+    const int jr = it.a_row0 + i;
+    if (i < it.mrows && jr >= it.b_row0 + c) atomicAdd(L + Cbase[c] + a.rel[Crel[c] + jr], (T)(-Cs[i + c * ldc]));
   }
 }
 
@@ -204,7 +182,7 @@ __global__ void __launch_bounds__(kDThreads, 1) k_gemm_dmma(FactorArgs a, const 
       Cs[r0 + 8 + (c0 + 1) * kDLdc] = acc[mi][ni][3];
     }
   __syncthreads();
-  tile_epilogue<kDM, kDN, kDThreads, double, double>(a, it, m, Cs, kDLdc, ints, ints + 128, ints + 256, ints + 384);
+  tile_epilogue<kDM, kDN, kDThreads, double, double>(a, it, m, Cs, kDLdc, (int64_t*)ints, (int64_t*)ints + 128);
 }
 
 // ---- 64 x 64 FP64 FMA tile --------------------------------------------------------
@@ -257,7 +235,7 @@ __global__ void __launch_bounds__(256) k_gemm_simt(FactorArgs a, const TileItem*
 #pragma unroll
     for (int j = 0; j < 4; ++j) Cs[(ty + 16 * i) + (tx + 16 * j) * kSLdc] = acc[i][j];
   __syncthreads();
-  tile_epilogue<64, 64, 256, T, T>(a, it, m, Cs, kSLdc, ints, ints + 64, ints + 128, ints + 192);
+  tile_epilogue<64, 64, 256, T, T>(a, it, m, Cs, kSLdc, (int64_t*)ints, (int64_t*)ints + 64);
 }
 
 // ---- 128 x 128 split-precision 3xTF32 tensor-core tile (FP32 storage) -------------
@@ -390,7 +368,7 @@ __global__ void __launch_bounds__(256, 1) k_gemm_tf32x3(FactorArgs a, const Tile
       Cs[r0 + 8 + (c0 + 1) * kTLdc] = acc[mi][ni][3];
     }
   __syncthreads();
-  tile_epilogue<128, 128, 256, float, float>(a, it, m, Cs, kTLdc, ints, ints + 128, ints + 256, ints + 384);
+  tile_epilogue<128, 128, 256, float, float>(a, it, m, Cs, kTLdc, (int64_t*)ints, (int64_t*)ints + 128);
 }
 
 // ---- 128 x 128 split-precision 3xTF32 tile on the 5th-generation tensor core -------
@@ -592,7 +570,7 @@ __global__ void __launch_bounds__(256, 1) k_gemm_tc32(FactorArgs a, const TileIt
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(kUTmemCols) : "memory");
   }
   if (!ok) return;
-  tile_epilogue<kUM, kUN, 256, float, float>(a, it, m, Cs, kULdc, ints, ints + 128, ints + 256, ints + 384);
+  tile_epilogue<kUM, kUN, 256, float, float>(a, it, m, Cs, kULdc, (int64_t*)ints, (int64_t*)ints + 128);
 }
 
 }  // namespace

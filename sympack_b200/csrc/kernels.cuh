@@ -23,6 +23,9 @@ struct FactorArgs {
   const int32_t* rows;       // concatenated 0-based row lists
   const int32_t* supmember;  // 0-based supernode of each permuted column
   Status* status;
+  const int32_t* row_group;  // relative-index group of each row-list entry
+  const RelGroup* groups;
+  const int32_t* rel;        // positions of update rows in their targets' row lists
   bool fp32;                 // FP32 factor storage (precision form)
   bool tc32;                 // FP32 128 x 128 tiles on tcgen05 (else mma.sync m16n8k8)
 };

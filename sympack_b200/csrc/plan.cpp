@@ -154,6 +154,32 @@ Plan build_plan(const Symbolic& sym, const PlanParams& prm) {
     }
     flush_gemm();
   }
+  // relative indices of the external updates: groups of off-diagonal rows by
+  // target, positions found by merging the sorted row lists
+  P.row_group.assign(P.rows.size(), -1);
+  for (int s = 0; s < ns; ++s) {
+    const SnMeta& m = P.meta[s];
+    const int32_t* rl = P.rows.data() + m.lidx;
+    int r = m.w;
+    while (r < m.h) {
+      const int t = P.supmember0[rl[r]];
+      const SnMeta& mt = P.meta[t];
+      const int32_t* tl = P.rows.data() + mt.lidx;
+      RelGroup g{t, r, (int64_t)P.rel.size()};
+      const int gid = (int)P.groups.size();
+      P.groups.push_back(g);
+      int q = 0;
+      for (int i = r; i < m.h; ++i) {
+        while (q < mt.h && tl[q] < rl[i]) ++q;
+        if (q == mt.h || tl[q] != rl[i]) throw std::runtime_error("plan: update row missing from its target's structure");
+        P.rel.push_back(q);
+      }
+      int e = r;
+      while (e < m.h && P.supmember0[rl[e]] == t) P.row_group[m.lidx + e++] = gid;
+      r = e;
+    }
+  }
+
   // algorithmic flops per step
   P.step_flops.assign(P.steps.size(), 0.0);
   for (size_t k = 0; k < P.steps.size(); ++k) {

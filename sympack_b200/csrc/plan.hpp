@@ -90,6 +90,17 @@ struct SolveTask {
   int32_t t;
 };
 
+// Relative indices of the external updates (the src_to_tgt_offset maps of
+// symPACKMatrix2D.hpp:1395-1466, computed once per structure instead of per
+// update).  The off-diagonal rows of supernode s that fall in ancestor t form
+// one group; for every off-diagonal row r of s at or after the group's first
+// row j0, rel[rel_off + (r - j0)] is the position of that row in t's row list.
+struct RelGroup {
+  int32_t t;        // target supernode (0-based)
+  int32_t j0;       // panel row of s where the group starts (>= w)
+  int64_t rel_off;  // offset of the group's positions in the rel array
+};
+
 struct Plan {
   int n = 0;
   int nsuper = 0;
@@ -98,6 +109,9 @@ struct Plan {
   int64_t lindx_total = 0;
   std::vector<SnMeta> meta;     // nsuper
   std::vector<int32_t> rows;    // concatenated 0-based row lists (device copy)
+  std::vector<int32_t> row_group;   // per row-list entry: its RelGroup (off-diagonal rows), else -1
+  std::vector<RelGroup> groups;
+  std::vector<int32_t> rel;         // positions in the target row lists
   std::vector<int32_t> supmember0;  // 0-based supernode of each (permuted) column
   std::vector<int32_t> sparent;     // supernodal etree parent (0-based, -1 root)
   std::vector<int32_t> level;       // height level of each supernode
