@@ -28,25 +28,28 @@ __device__ __forceinline__ void report_status(Status* st, int code, int s, int c
   }
 }
 
-// Apply a BM x BN tile of C held in shared memory (column-major, leading dimension ldc).
-// Mode 1 targets come from the relative indices computed with the plan: per tile
-// column its target column base and group offset (staged in shared memory),
-// then one coalesced position load and one atomic per element.  Consecutive
-// threads take consecutive rows of a column, so both are coalesced.
+// Apply a BM x BN tile of C held in shared memory (column-major, leading dimension ldc),
+// subtracting it with fire-and-forget atomic reductions (no load on the thread's
+// critical path).  Each thread keeps one tile row (consecutive threads take
+// consecutive rows, so the reductions of a warp are coalesced) and walks the
+// columns.  Mode 1 targets come from the relative indices computed with the plan:
+// per tile column its target column base and group offset (staged in shared
+// memory); the row's position in a target is loaded once per target group, since
+// the columns of one group share it.
 template <int BM, int BN, int NT, class T, class CT>
 __device__ void tile_epilogue(const FactorArgs& a, const TileItem& it, const SnMeta& m, const CT* Cs, int ldc,
                               int64_t* Cbase, int64_t* Crel) {
-  const int tid = threadIdx.x;
+  static_assert(NT % BM == 0, "one row per thread");
+  const int tid = threadIdx.x, i = tid % BM, c0 = tid / BM;
+  constexpr int kStep = NT / BM;
   T* L = static_cast<T*>(a.L);
+  const int jr = it.a_row0 + i;
   if (it.mode == 0) {
-    T* g = L + m.off;
-    const int64_t ld = m.ld;
-    for (int idx = tid; idx < BM * BN; idx += NT) {
-      int c = idx / BM, r = idx - c * BM;
-      if (r < it.mrows && c < it.ncols) {
-        int gr = it.a_row0 + r, gc = it.b_row0 + c;
-        if (gr >= gc) g[gr + (int64_t)gc * ld] -= (T)Cs[r + c * ldc];
-      }
+    if (i >= it.mrows) return;
+    T* g = L + m.off + jr;
+    for (int c = c0; c < it.ncols; c += kStep) {
+      const int gc = it.b_row0 + c;
+      if (jr >= gc) atomicAdd(g + (int64_t)gc * m.ld, (T)(-Cs[i + c * ldc]));
     }
     return;
   }
@@ -61,10 +64,17 @@ __device__ void tile_epilogue(const FactorArgs& a, const TileItem& it, const SnM
     }
   }
   __syncthreads();
-  for (int idx = tid; idx < BM * it.ncols; idx += NT) {
-    const int c = idx / BM, i = idx - c * BM;
-    const int jr = it.a_row0 + i;
-    if (i < it.mrows && jr >= it.b_row0 + c) atomicAdd(L + Cbase[c] + a.rel[Crel[c] + jr], (T)(-Cs[i + c * ldc]));
+  if (i >= it.mrows) return;
+  int64_t last = INT64_MIN;  // group offsets (rel_off - j0) can be negative
+  int pos = 0;
+  for (int c = c0; c < it.ncols; c += kStep) {
+    if (jr < it.b_row0 + c) break;  // rows are sorted: later columns are above this row
+    const int64_t cr = Crel[c];
+    if (cr != last) {
+      pos = a.rel[cr + jr];
+      last = cr;
+    }
+    atomicAdd(L + Cbase[c] + pos, (T)(-Cs[i + c * ldc]));
   }
 }
 
@@ -386,12 +396,16 @@ __global__ void __launch_bounds__(256, 1) k_gemm_tf32x3(FactorArgs a, const Tile
 constexpr int kUM = 128, kUN = 128, kUK = 32;
 constexpr int kUOpBytes = kUM * kUK * 4;           // one operand part: 16 KB
 constexpr int kUStageBytes = 4 * kUOpBytes;        // A hi, A lo, B hi, B lo
-constexpr int kUStages = 2;
+constexpr int kUStages = 2;                         // split operand buffers (MMA double buffer)
+constexpr int kURaw = 3;                            // raw FP32 chunks in flight (cp.async)
+constexpr int kURawBytes = 2 * kUK * kUM * 4;       // A and B columns of one chunk: 32 KB
 constexpr int kULdc = 132;
 constexpr size_t kUCBytes = (size_t)kUN * kULdc * sizeof(float);
-constexpr size_t kUMainBytes =
-    (size_t)kUStages * kUStageBytes > kUCBytes ? (size_t)kUStages * kUStageBytes : kUCBytes;
-constexpr size_t kUSmemBytes = 1024 + kUMainBytes + 4 * 128 * sizeof(int) + 64;
+constexpr size_t kUOpAll = (size_t)kUStages * kUStageBytes;   // 128 KB; C staging reuses it
+constexpr size_t kUMainBytes = kUOpAll + (size_t)kURaw * kURawBytes;
+constexpr size_t kUSmemBytes = 1024 + kUMainBytes + 64;
+static_assert(kUCBytes <= kUOpAll, "C staging must fit in the operand buffers");
+static_assert(kUSmemBytes <= 232448, "shared memory of the tcgen05 tile");
 constexpr int kUTmemCols = 128;
 constexpr long long kUWaitLimit = 1LL << 24;  // mbarrier polls before a tile gives up (seconds)
 
@@ -434,8 +448,9 @@ __global__ void __launch_bounds__(256, 1) k_gemm_tc32(FactorArgs a, const TileIt
   unsigned char* base = smem_raw + pad;
   const uint32_t base_addr = raw_addr + pad;
   float* Cs = reinterpret_cast<float*>(base);  // reused once every MMA has completed
-  int* ints = reinterpret_cast<int*>(base + kUMainBytes);
-  uint64_t* bars = reinterpret_cast<uint64_t*>(base + kUMainBytes + 4 * 128 * sizeof(int));
+  float* raw = reinterpret_cast<float*>(base + kUOpAll);  // kURaw x {A, B} x [32 columns][128 rows]
+  int* ints = reinterpret_cast<int*>(raw);                  // epilogue maps reuse the raw stages
+  uint64_t* bars = reinterpret_cast<uint64_t*>(base + kUMainBytes);
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + kUStages);
   __shared__ int sh_abort;
 
@@ -465,42 +480,54 @@ __global__ void __launch_bounds__(256, 1) k_gemm_tc32(FactorArgs a, const TileIt
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
   const uint32_t tmem = *tmem_slot;
 
-  // this thread's operand pieces: row r, column groups kq + 2q (q = 0..3) of 4 columns
-  const int r = tid & 127, kq = tid >> 7;
-  const bool arow = r < it.mrows, brow = r < it.ncols;
-  float va[16], vb[16];
-  auto load_chunk = [&](int kk) {
-#pragma unroll
-    for (int q = 0; q < 4; ++q)
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const int k = kk + 4 * (kq + 2 * q) + j;
-        const bool kok = k < it.kn;
-        const int64_t coff = (int64_t)(it.k0 + k) * ld;
-        va[4 * q + j] = (kok && arow) ? g[it.a_row0 + r + coff] : 0.f;
-        vb[4 * q + j] = (kok && brow) ? g[it.b_row0 + r + coff] : 0.f;
-      }
+  // raw chunk kk of A and B: column k of the chunk, row r at raw[stage][op][k][r]
+  auto load_raw = [&](int stage, int kk) {
+    float* ra = raw + (size_t)stage * (kURawBytes / 4);
+    float* rb = ra + kUK * kUM;
+#pragma unroll 4
+    for (int q = 0; q < kUK * kUM / 256; ++q) {
+      const int e = tid + q * 256, col = e >> 7, r = e & 127, k = kk + col;
+      const bool kok = k < it.kn;
+      const int64_t coff = (int64_t)(it.k0 + (kok ? k : 0)) * ld;
+      const bool aok = kok && r < it.mrows, bok = kok && r < it.ncols;
+      cp_async4(ra + col * kUM + r, aok ? g + it.a_row0 + r + coff : g, aok ? 4 : 0);
+      cp_async4(rb + col * kUM + r, bok ? g + it.b_row0 + r + coff : g, bok ? 4 : 0);
+    }
   };
+  // this thread's split pieces: row r, column groups kq + 2q (q = 0..3) of 4 columns
+  const int r = tid & 127, kq = tid >> 7;
   const int nk = (it.kn + kUK - 1) / kUK;
-  load_chunk(0);
+#pragma unroll
+  for (int c = 0; c < kURaw - 1; ++c) {
+    if (c < nk) load_raw(c, c * kUK);
+    cp_commit();
+  }
   int committed = -1;  // last chunk whose MMAs were committed
   for (int kt = 0; kt < nk; ++kt) {
+    const int nxt = kt + kURaw - 1;  // its raw stage was split at kt - 1, before that iteration's barrier
+    if (nxt < nk) load_raw(nxt % kURaw, nxt * kUK);
+    cp_commit();
+    cp_wait<kURaw - 1>();
     const int st = kt & 1;
     const uint32_t bar = (uint32_t)__cvta_generic_to_shared(bars + st);
     if (kt >= 2 && !mbar_wait(bar, (uint32_t)(((kt >> 1) - 1) & 1), kUWaitLimit)) sh_abort = 1;
+    __syncthreads();  // every thread's raw copies of chunk kt have landed
+    const float* ra = raw + (size_t)(kt % kURaw) * (kURawBytes / 4);
+    const float* rb = ra + kUK * kUM;
     unsigned char* sb = base + st * kUStageBytes;
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
+      const int k4 = 4 * (kq + 2 * q);
       const uint32_t off = umma_k_offset(r, kq + 2 * q);
       uint4 ah, al, bh, bl;
-      split_tf32(va[4 * q + 0], ah.x, al.x);
-      split_tf32(va[4 * q + 1], ah.y, al.y);
-      split_tf32(va[4 * q + 2], ah.z, al.z);
-      split_tf32(va[4 * q + 3], ah.w, al.w);
-      split_tf32(vb[4 * q + 0], bh.x, bl.x);
-      split_tf32(vb[4 * q + 1], bh.y, bl.y);
-      split_tf32(vb[4 * q + 2], bh.z, bl.z);
-      split_tf32(vb[4 * q + 3], bh.w, bl.w);
+      split_tf32(ra[(k4 + 0) * kUM + r], ah.x, al.x);
+      split_tf32(ra[(k4 + 1) * kUM + r], ah.y, al.y);
+      split_tf32(ra[(k4 + 2) * kUM + r], ah.z, al.z);
+      split_tf32(ra[(k4 + 3) * kUM + r], ah.w, al.w);
+      split_tf32(rb[(k4 + 0) * kUM + r], bh.x, bl.x);
+      split_tf32(rb[(k4 + 1) * kUM + r], bh.y, bl.y);
+      split_tf32(rb[(k4 + 2) * kUM + r], bh.z, bl.z);
+      split_tf32(rb[(k4 + 3) * kUM + r], bh.w, bl.w);
       *reinterpret_cast<uint4*>(sb + off) = ah;
       *reinterpret_cast<uint4*>(sb + kUOpBytes + off) = al;
       *reinterpret_cast<uint4*>(sb + 2 * kUOpBytes + off) = bh;
@@ -531,8 +558,8 @@ __global__ void __launch_bounds__(256, 1) k_gemm_tc32(FactorArgs a, const TileIt
                    : "memory");
     }
     committed = kt;
-    if (kt + 1 < nk) load_chunk((kt + 1) * kUK);
   }
+  cp_wait<0>();
   bool ok = !sh_abort;
   if (committed >= 0) {  // every MMA done before the accumulator is read or the stages reused
     const uint32_t bar = (uint32_t)__cvta_generic_to_shared(bars + (committed & 1));
