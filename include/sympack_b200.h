@@ -218,6 +218,11 @@ typedef struct spb_profile {
   int32_t launches[SPB_KIND_COUNT];
 } spb_profile;
 int spb_set_profiling(spb_handle* h, int on);
+/* Timeline of the last profiled solve's sweep (0 forward, 1 backward), in task
+ * order: per task {grabbed, dependencies met, done} in device nanoseconds and
+ * (supernode << 8 | task kind).  Copies min(cap, ntasks) tasks; *ntasks gets
+ * the sweep's task count (out may be null to query it). */
+int spb_get_solve_trace(spb_handle* h, int32_t sweep, uint64_t* out, int64_t cap, int64_t* ntasks);
 int spb_get_profile(spb_handle* h, spb_profile* out);
 
 /* Rutherford-Boeing input boundary, replacing ReadMatrix / ReadHB_PARA

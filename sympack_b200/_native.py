@@ -98,6 +98,7 @@ SIGNATURES = [
     ("spb_symbolic_from", C.c_int, [_P, _P]),
     ("spb_predict_device_bytes", C.c_int, [_P, C.c_int32, C.c_int32, C.POINTER(C.c_int64)]),
     ("spb_replan", C.c_int, [_P, C.c_int32, C.c_int32]),
+    ("spb_get_solve_trace", C.c_int, [_P, C.c_int32, C.POINTER(C.c_uint64), C.c_int64, C.POINTER(C.c_int64)]),
     ("spb_distribute", C.c_int, [_P, _DP]),
     ("spb_distribute_device", C.c_int, [_P, _P]),
     ("spb_factorize", C.c_int, [_P]),

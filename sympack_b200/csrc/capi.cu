@@ -91,6 +91,7 @@ struct spb_handle {
   long long wait_limit = 1LL << 24;  // ~2 s of polling per device wait
   int stall_supernode = -1;          // test hook: extra expected arrival nobody delivers
   bool profiling = false;
+  unsigned long long* dtrace = nullptr;  // profiled solves: 4 per task of each sweep (forward, backward)
   spb_profile prof{};
   std::vector<cudaEvent_t> events;
 };
@@ -143,6 +144,7 @@ void release_device(spb_handle* h) {
   h->dL = nullptr;
   h->dX = h->dB = h->dR = h->dD = h->dXo = nullptr;
   h->d_rowseg = nullptr;
+  h->dtrace = nullptr;
   h->x_cap = 0;
 }
 
@@ -251,6 +253,10 @@ int factor_profiled(spb_handle* h) {
 }
 
 int ensure_rhs_capacity(spb_handle* h, int nrhs) {
+  if (h->profiling && !h->dtrace) {  // task timeline of profiled solves
+    SPB_CK(h, dalloc(h, &h->dtrace, 4 * (h->plan.fwd_tasks.size() + h->plan.bwd_tasks.size())));
+    SPB_CK(h, cudaStreamSynchronize(h->own_stream));
+  }
   int64_t need = (int64_t)h->sym.n * nrhs;
   if (need <= h->x_cap) return SPB_OK;
   for (double** p : {&h->dX, &h->dB, &h->dR, &h->dD, &h->dXo}) {
@@ -303,6 +309,7 @@ void enqueue_solve(spb_handle* h, int nrhs) {
     a.counter = h->dsync;
     a.blkdone = h->dsync + 2 + ns;
     a.upd = h->dsync + 2 + 3 * (size_t)ns;
+    a.trace = h->profiling ? h->dtrace : nullptr;
     if (h->profiling) cudaEventRecord(h->events[e0], h->stream);
     spb::dev::launch_solve_persistent(h->stream, a, true);
     if (h->profiling) cudaEventRecord(h->events[e0 + 1], h->stream);
@@ -311,6 +318,7 @@ void enqueue_solve(spb_handle* h, int nrhs) {
     a.counter = h->dsync + 1;
     a.blkdone = h->dsync + 2 + 2 * ns;
     a.upd = h->dsync + 2 + 3 * (size_t)ns + P.nblk_total;
+    a.trace = h->profiling && h->dtrace ? h->dtrace + 4 * P.fwd_tasks.size() : nullptr;
     if (h->profiling) cudaEventRecord(h->events[e0 + 2], h->stream);
     spb::dev::launch_solve_persistent(h->stream, a, false);
     if (h->profiling) cudaEventRecord(h->events[e0 + 3], h->stream);
@@ -1145,6 +1153,21 @@ int spb_set_stream(spb_handle* h, void* stream) {
   if (h->device < 0) return fail(h, SPB_ERR_STATE, "host-only handle (device < 0) has no stream");
   SPB_CK(h, cudaStreamSynchronize(h->stream));
   h->stream = stream ? (cudaStream_t)stream : h->own_stream;
+  return SPB_OK;
+}
+
+int spb_get_solve_trace(spb_handle* h, int32_t sweep, uint64_t* out, int64_t cap, int64_t* ntasks) {
+  if (check_handle(h) || !ntasks || (sweep != 0 && sweep != 1)) return SPB_ERR_INVALID;
+  const spb::Plan& P = h->plan;
+  const size_t nt = sweep == 0 ? P.fwd_tasks.size() : P.bwd_tasks.size();
+  *ntasks = (int64_t)nt;
+  if (!h->dtrace) return fail(h, SPB_ERR_STATE, "solve_trace: no profiled solve yet");
+  if (!out) return SPB_OK;
+  const size_t n = std::min(nt, (size_t)std::max<int64_t>(cap, 0));
+  SPB_CK(h, cudaSetDevice(h->device));
+  SPB_CK(h, cudaStreamSynchronize(h->stream));
+  SPB_CK(h, cudaMemcpy(out, h->dtrace + (sweep ? 4 * P.fwd_tasks.size() : 0), 4 * n * sizeof(uint64_t),
+                       cudaMemcpyDeviceToHost));
   return SPB_OK;
 }
 

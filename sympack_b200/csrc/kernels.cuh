@@ -65,6 +65,7 @@ struct PSolveArgs {
   int32_t* upd;      // per 64-column block: updates landed (meta.boff + block)
   Status* status;
   long long spin_limit;  // polls (about 128 ns apart) before a wait gives up
+  unsigned long long* trace;  // optional, 4 per task: grabbed, dependencies met, done (ns), s << 8 | kind
 };
 void init_solve_attributes();
 void launch_solve_persistent(cudaStream_t st, const PSolveArgs& a, bool forward);

@@ -225,7 +225,7 @@ Plan build_plan(const Symbolic& sym, const PlanParams& prm) {
       const int nblk = (m.w + 63) / 64, noff = (m.h - m.w + 63) / 64;
       for (int i = 0; i < nblk; ++i) {
         P.fwd_tasks.push_back(SolveTask{s, 0, i, i});
-        for (int t = i + 1; t < nblk; ++t) P.fwd_tasks.push_back(SolveTask{s, 1, i, t});
+        for (int t = i + 2; t < nblk; ++t) P.fwd_tasks.push_back(SolveTask{s, 1, i, t});
       }
       for (int u = 0; u < noff; ++u) {
         P.fwd_tasks.push_back(SolveTask{s, 2, 0, u});
@@ -239,10 +239,12 @@ Plan build_plan(const Symbolic& sym, const PlanParams& prm) {
     }
   for (int L = H - 1; L >= 0; --L)
     for (int s : P.level_sn[L]) {
-      const int nblk = (P.meta[s].w + 63) / 64;
+      const SnMeta& m = P.meta[s];
+      const int nblk = (m.w + 63) / 64, noff = (m.h - m.w + 63) / 64;
+      for (int u = 0; u < noff; ++u) P.bwd_tasks.push_back(SolveTask{s, 3, 0, u});
       for (int t = nblk - 1; t >= 0; --t) {
         P.bwd_tasks.push_back(SolveTask{s, 0, t, t});
-        for (int u = 0; u < t; ++u) P.bwd_tasks.push_back(SolveTask{s, 1, t, u});
+        for (int u = 0; u + 2 <= t; ++u) P.bwd_tasks.push_back(SolveTask{s, 1, t, u});
       }
     }
   return P;

@@ -77,11 +77,15 @@ struct PanelItem {
 
 // One task of the persistent triangular solves, in 64-row / 64-column units
 // (i, t: column blocks of supernode s; u: 64-row tile below the diagonal block).
-//   forward  kind 0  D(t):    X_t <- L_tt^-1 X_t once every update into block t has landed
-//            kind 1  U(i, t): X_t -= L_ti X_i                          (i < t, after D(i))
+//   forward  kind 0  D(t):    X_t <- L_tt^-1 X_t once every update into block t
+//                             has landed, then X_{t+1} -= L_{t+1,t} X_t
+//            kind 1  U(i, t): X_t -= L_ti X_i                 (t >= i + 2, after D(i))
 //            kind 2  O(u):    X[rows of tile u] -= sum_i L_ui X_i, scattered to the ancestors
-//   backward kind 0  B(t):    X_t <- L_tt^-T (X_t - sum over ancestor rows r of L_rt^T X_r)
-//            kind 1  V(t, u): X_u -= L_tu^T X_t                        (u < t, after B(t))
+//   backward kind 3  W(u):    X_t -= L_ut^T X[rows of tile u] for every block t
+//                             (ancestor rows, final once the parent is done)
+//            kind 0  B(t):    X_t <- L_tt^-T X_t once every update into block t
+//                             has landed, then X_{t-1} -= L_{t,t-1}^T X_t
+//            kind 1  V(t, u): X_u -= L_tu^T X_t                 (u <= t - 2, after B(t))
 // Task lists are topological: every task a task waits on comes earlier.
 struct SolveTask {
   int32_t s;

@@ -88,7 +88,7 @@ __device__ __forceinline__ void block_gemv_t(double* acc, const double* A, const
 
 // Stage L rows [r0, r0+m) x columns [c0, c0+kk) of a panel into A (ld kPld), widened to FP64.
 // A full 64 x 64 block is loaded with all 16 loads of a thread in flight.
-template <class T>
+template <class T, int kLd = kPld>
 __device__ __forceinline__ void stage_block(double* A, const T* P, int64_t ld, int r0, int m, int c0, int kk) {
   if (m == kT && kk == kT) {
     T v[kT * kT / kThreads];
@@ -100,13 +100,13 @@ __device__ __forceinline__ void stage_block(double* A, const T* P, int64_t ld, i
 #pragma unroll
     for (int q = 0; q < kT * kT / kThreads; ++q) {
       const int idx = threadIdx.x + q * kThreads, k = idx / kT, r = idx - k * kT;
-      A[r + k * kPld] = (double)v[q];
+      A[r + k * kLd] = (double)v[q];
     }
     return;
   }
   for (int idx = threadIdx.x; idx < m * kk; idx += kThreads) {
     int k = idx / m, r = idx - k * m;
-    A[r + k * kPld] = (double)P[(r0 + r) + (int64_t)(c0 + k) * ld];
+    A[r + k * kLd] = (double)P[(r0 + r) + (int64_t)(c0 + k) * ld];
   }
 }
 
@@ -123,6 +123,22 @@ __device__ __forceinline__ void stage_x(double* B, const double* X, int64_t ldx,
 }  // namespace
 
 namespace {
+
+// X[x0 + i, c] (+/-)= sum_k A[i + k*lda] * B[k + c*kT] straight into global X with
+// atomics (i < m, c < nr, k < kk); A column-major with leading dimension lda.
+template <bool kTrans>
+__device__ __forceinline__ void block_gemv_atomic(double* X, int64_t ldx, int x0, const double* A, int lda,
+                                                  const double* B, int m, int kk, int nr, double sign) {
+  for (int idx = threadIdx.x; idx < m * nr; idx += kThreads) {
+    int c = idx / m, i = idx - c * m;
+    double s = 0.0;
+    if (kTrans)
+      for (int k = 0; k < kk; ++k) s = fma(A[k + i * lda], B[k + c * kT], s);
+    else
+      for (int k = 0; k < kk; ++k) s = fma(A[i + k * lda], B[k + c * kT], s);
+    atomicAdd(X + x0 + i + c * ldx, sign * s);
+  }
+}
 
 // Lower-triangular solves of a kk x kk block held in A (ld kPld) against the
 // right-hand sides acc (ld kT), one warp per right-hand side column.
@@ -172,6 +188,17 @@ __device__ __forceinline__ int next_task(const PSolveArgs& a, int* sh_task, int*
   return (tk >= a.ntasks || stop) ? -1 : tk;
 }
 
+__device__ __forceinline__ unsigned long long now_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Task timeline for analysis (thread 0; trace may be null).
+__device__ __forceinline__ void trace_mark(const PSolveArgs& a, int tk, int slot, unsigned long long v) {
+  if (a.trace && threadIdx.x == 0) a.trace[4 * (size_t)tk + slot] = v;
+}
+
 // Publish a block's writes, then bump a counter (thread 0).
 __device__ __forceinline__ void signal(int32_t* counter) {
   __threadfence();
@@ -192,16 +219,22 @@ __global__ void __launch_bounds__(kThreads) k_solve_forward(PSolveArgs a) {
     if (tk < 0) return;
     const SolveTask task = a.tasks[tk];
     const int s = task.s;
+    trace_mark(a, tk, 0, now_ns());
+    trace_mark(a, tk, 3, ((unsigned long long)s << 8) | (unsigned)task.kind);
     const SnMeta m = a.meta[s];
     const T* P = static_cast<const T*>(a.L) + m.off;
     const int32_t* rl = a.rows + m.lidx;
     const int64_t ld = m.ld;
     if (task.kind == 0) {
-      // D(t): descendants' and earlier blocks' updates have landed in X_t; X_t <- L_tt^-1 X_t
+      // D(t): descendants' and earlier blocks' updates have landed in X_t; X_t <- L_tt^-1 X_t,
+      // then the update of the next block, X_{t+1} -= L_{t+1,t} X_t
       const int t = task.t, r0 = t * kT, bt = min(kT, m.w - r0);
+      const int r1 = r0 + kT, b1 = r1 < m.w ? min(kT, m.w - r1) : 0;
+      stage_block(Ab, P, ld, r0, bt, r0, bt);  // L is final: load before waiting
+      if (b1) stage_block<T, kT>(Bx, P, ld, r1, b1, r0, bt);
       if (!wait_geq(a.arrived + s, a.expected[s], a.status, s, &sh_ok, a.spin_limit)) return;
       if (!wait_geq(a.upd + m.boff + t, t, a.status, s, &sh_ok, a.spin_limit)) return;
-      stage_block(Ab, P, ld, r0, bt, r0, bt);
+      trace_mark(a, tk, 1, now_ns());
       stage_x(acc, a.X, a.ldx, m.fc + r0, nullptr, bt, nr);
       __syncthreads();
       block_trsv<true>(acc, Ab, bt, nr);
@@ -210,12 +243,19 @@ __global__ void __launch_bounds__(kThreads) k_solve_forward(PSolveArgs a) {
         int c = idx / bt, r = idx - c * bt;
         a.X[m.fc + r0 + r + c * a.ldx] = acc[r + c * kT];
       }
-      signal(a.blkdone + s);
+      if (b1) block_gemv_atomic<false>(a.X, a.ldx, m.fc + r1, Bx, kT, acc, b1, bt, nr, -1.0);
+      __threadfence();
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        atomicAdd(a.blkdone + s, 1);
+        if (b1) atomicAdd(a.upd + m.boff + t + 1, 1);
+      }
     } else if (task.kind == 1) {
       // U(i, t): X_t -= L_ti X_i
       const int i = task.i, t = task.t, bi = min(kT, m.w - i * kT), r0 = t * kT, bt = min(kT, m.w - r0);
       stage_block(Ab, P, ld, r0, bt, i * kT, bi);  // L is final: load before waiting
       if (!wait_geq(a.blkdone + s, i + 1, a.status, s, &sh_ok, a.spin_limit)) return;
+      trace_mark(a, tk, 1, now_ns());
       stage_x(Bx, a.X, a.ldx, m.fc + i * kT, nullptr, bi, nr);
       for (int idx = threadIdx.x; idx < kT * nr; idx += kThreads) acc[idx] = 0.0;
       __syncthreads();
@@ -240,6 +280,7 @@ __global__ void __launch_bounds__(kThreads) k_solve_forward(PSolveArgs a) {
         block_gemv<false>(acc, Ab, Bx, bu, bi, nr);
         __syncthreads();
       }
+      trace_mark(a, tk, 1, now_ns());
       for (int idx = threadIdx.x; idx < bu * nr; idx += kThreads) {
         int c = idx / bu, r = idx - c * bu;
         atomicAdd(a.X + rl[r0 + r] + c * a.ldx, -acc[r + c * kT]);
@@ -256,6 +297,7 @@ __global__ void __launch_bounds__(kThreads) k_solve_forward(PSolveArgs a) {
       }
       __syncthreads();
     }
+    trace_mark(a, tk, 2, now_ns());
   }
 }
 
@@ -272,34 +314,41 @@ __global__ void __launch_bounds__(kThreads) k_solve_backward(PSolveArgs a) {
     if (tk < 0) return;
     const SolveTask task = a.tasks[tk];
     const int s = task.s;
+    trace_mark(a, tk, 0, now_ns());
+    trace_mark(a, tk, 3, ((unsigned long long)s << 8) | (unsigned)task.kind);
     const SnMeta m = a.meta[s];
     const T* P = static_cast<const T*>(a.L) + m.off;
     const int32_t* rl = a.rows + m.lidx;
     const int64_t ld = m.ld;
     const int nblk = (m.w + kT - 1) / kT;
-    if (task.kind == 0) {
-      // B(t): X_t <- L_tt^-T (X_t - sum over ancestor rows of L_rt^T X_r - later blocks' updates)
-      const int t = task.t, c0 = t * kT, bt = min(kT, m.w - c0);
+    if (task.kind == 3) {
+      // W(u): ancestor rows of tile u, final once the parent is done: X_t -= L_ut^T X_u for
+      // every column block t, newest first (the order the diagonal chain needs them)
+      const int u = task.t, rr = m.w + u * kT, br = min(kT, m.h - rr);
       const int par = a.sparent[s];
-      for (int idx = threadIdx.x; idx < kT * nr; idx += kThreads) acc[idx] = 0.0;
+      stage_block(Ab, P, ld, rr, br, (nblk - 1) * kT, m.w - (nblk - 1) * kT);
       if (par >= 0 && !wait_geq(a.blkdone + par, (a.meta[par].w + kT - 1) / kT, a.status, s, &sh_ok, a.spin_limit))
         return;
-      for (int rr = m.w; rr < m.h; rr += kT) {  // ancestors' rows are final once the parent is done
-        const int br = min(kT, m.h - rr);
-        stage_x(Bx, a.X, a.ldx, 0, rl + rr, br, nr);
-        stage_block(Ab, P, ld, rr, br, c0, bt);
+      trace_mark(a, tk, 1, now_ns());
+      stage_x(Bx, a.X, a.ldx, 0, rl + rr, br, nr);
+      for (int t = nblk - 1; t >= 0; --t) {
+        const int c0 = t * kT, bt = min(kT, m.w - c0);
+        if (t < nblk - 1) stage_block(Ab, P, ld, rr, br, c0, bt);
         __syncthreads();
-        block_gemv_t(acc, Ab, Bx, br, bt, nr);
+        block_gemv_atomic<true>(a.X, a.ldx, m.fc + c0, Ab, kPld, Bx, bt, br, nr, -1.0);
+        __threadfence();
         __syncthreads();
+        if (threadIdx.x == 0) atomicAdd(a.upd + m.boff + t, 1);
       }
-      stage_block(Ab, P, ld, c0, bt, c0, bt);
-      if (!wait_geq(a.upd + m.boff + t, nblk - 1 - t, a.status, s, &sh_ok, a.spin_limit)) return;
-      stage_x(Bx, a.X, a.ldx, m.fc + c0, nullptr, bt, nr);
-      __syncthreads();
-      for (int idx = threadIdx.x; idx < bt * nr; idx += kThreads) {
-        int c = idx / bt, r = idx - c * bt;
-        acc[r + c * kT] += Bx[r + c * kT];
-      }
+    } else if (task.kind == 0) {
+      // B(t): every update into X_t has landed; X_t <- L_tt^-T X_t, then X_{t-1} -= L_{t,t-1}^T X_t
+      const int t = task.t, c0 = t * kT, bt = min(kT, m.w - c0);
+      const int noff = (m.h - m.w + kT - 1) / kT;
+      stage_block(Ab, P, ld, c0, bt, c0, bt);  // L is final: load before waiting
+      if (t > 0) stage_block<T, kT>(Bx, P, ld, c0, bt, c0 - kT, kT);
+      if (!wait_geq(a.upd + m.boff + t, noff + nblk - 1 - t, a.status, s, &sh_ok, a.spin_limit)) return;
+      trace_mark(a, tk, 1, now_ns());
+      stage_x(acc, a.X, a.ldx, m.fc + c0, nullptr, bt, nr);
       __syncthreads();
       block_trsv<false>(acc, Ab, bt, nr);
       __syncthreads();
@@ -307,23 +356,26 @@ __global__ void __launch_bounds__(kThreads) k_solve_backward(PSolveArgs a) {
         int c = idx / bt, r = idx - c * bt;
         a.X[m.fc + c0 + r + c * a.ldx] = acc[r + c * kT];
       }
-      signal(a.blkdone + s);
+      // X_{t-1} -= L_{t,t-1}^T X_t: Bx holds rows c0.. (bt) x columns c0-64.. (64), ld kT
+      if (t > 0) block_gemv_atomic<true>(a.X, a.ldx, m.fc + c0 - kT, Bx, kT, acc, kT, bt, nr, -1.0);
+      __threadfence();
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        atomicAdd(a.blkdone + s, 1);
+        if (t > 0) atomicAdd(a.upd + m.boff + t - 1, 1);
+      }
     } else {
       // V(t, u): X_u -= L_tu^T X_t
       const int t = task.i, u = task.t, rr = t * kT, br = min(kT, m.w - rr), c0 = u * kT, bu = min(kT, m.w - c0);
       stage_block(Ab, P, ld, rr, br, c0, bu);
       if (!wait_geq(a.blkdone + s, nblk - t, a.status, s, &sh_ok, a.spin_limit)) return;
+      trace_mark(a, tk, 1, now_ns());
       stage_x(Bx, a.X, a.ldx, m.fc + rr, nullptr, br, nr);
-      for (int idx = threadIdx.x; idx < kT * nr; idx += kThreads) acc[idx] = 0.0;
       __syncthreads();
-      block_gemv_t(acc, Ab, Bx, br, bu, nr);
-      __syncthreads();
-      for (int idx = threadIdx.x; idx < bu * nr; idx += kThreads) {
-        int c = idx / bu, k = idx - c * bu;
-        atomicAdd(a.X + m.fc + c0 + k + c * a.ldx, acc[k + c * kT]);
-      }
+      block_gemv_atomic<true>(a.X, a.ldx, m.fc + c0, Ab, kPld, Bx, bu, br, nr, -1.0);
       signal(a.upd + m.boff + u);
     }
+    trace_mark(a, tk, 2, now_ns());
   }
 }
 

@@ -302,6 +302,17 @@ class symPACKMatrix2D:
     def SetProfiling(self, on: bool = True) -> None:
         _raise(self._lib.spb_set_profiling(self._need(), 1 if on else 0), "SetProfiling", self._h)
 
+    def GetSolveTrace(self, sweep: int = 0) -> np.ndarray:
+        """Task timeline of the last profiled solve: (ntasks, 4) uint64 rows
+        {grabbed_ns, ready_ns, done_ns, supernode << 8 | kind} (sweep 0 forward, 1 backward)."""
+        h = self._need()
+        nt = C.c_int64()
+        _raise(self._lib.spb_get_solve_trace(h, sweep, None, 0, C.byref(nt)), "GetSolveTrace", h)
+        out = np.zeros((nt.value, 4), np.uint64)
+        _raise(self._lib.spb_get_solve_trace(h, sweep, out.ctypes.data_as(C.POINTER(C.c_uint64)), nt.value,
+                                             C.byref(nt)), "GetSolveTrace", h)
+        return out
+
     def GetProfile(self) -> dict:
         p = N.spb_profile()
         _raise(self._lib.spb_get_profile(self._need(), C.byref(p)), "GetProfile", self._h)
