@@ -28,6 +28,8 @@ struct spb_handle {
   int device = 0;
   cudaStream_t stream = nullptr;      // stream every call runs on
   cudaStream_t own_stream = nullptr;  // created by spb_create
+  cudaStream_t side_stream = nullptr; // look-ahead updates of the captured factorization
+  std::vector<cudaEvent_t> lane_events;
   std::string err;
   bool have_symbolic = false, have_values = false, factored = false, have_solution = false;
   spb::Symbolic sym;
@@ -163,23 +165,87 @@ spb::dev::FactorArgs factor_args(spb_handle* h) {
   return a;
 }
 
-// Issue the factorization steps on the handle's stream (captured into a graph).
-void enqueue_factor(spb_handle* h) {
+void launch_step(spb_handle* h, const spb::dev::FactorArgs& a, const spb::Step& st, cudaStream_t stream);
+
+cudaEvent_t lane_event(spb_handle* h, size_t i) {
+  while (h->lane_events.size() <= i) {
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return nullptr;
+    h->lane_events.push_back(e);
+  }
+  return h->lane_events[i];
+}
+
+// Issue the factorization steps (captured into a graph).  Chain and join steps
+// go to the handle's stream in order; side steps (the update of a block's
+// remaining columns) go to the side stream after the chain has produced their
+// operands, and the POTRF of block k waits for the side update of block k - 2,
+// the last one that writes block k's columns.  Updates are atomic additions,
+// so a chain update and a side update of the same columns may overlap.
+cudaError_t enqueue_factor(spb_handle* h) {
   const spb::Plan& P = h->plan;
   spb::dev::FactorArgs a = factor_args(h);
+  size_t nev = 0;
+  std::vector<std::pair<int, cudaEvent_t>> side;  // (block, event) of this level's side updates
+  size_t waited = 0;                               // side events the chain already waits for
+  bool pending = false;                            // side work not yet joined
+  auto next_event = [&]() { return lane_event(h, nev++); };
   for (const spb::Step& st : P.steps) {
+    if (st.lane == spb::Lane::Join) {
+      if (pending) {
+        cudaEvent_t e = next_event();
+        if (!e) return cudaErrorMemoryAllocation;
+        cudaEventRecord(e, h->side_stream);
+        cudaStreamWaitEvent(h->stream, e, 0);
+        pending = false;
+      }
+      side.clear();
+      waited = 0;
+      launch_step(h, a, st, h->stream);
+    } else if (st.lane == spb::Lane::Chain) {
+      if (st.kind == spb::StepKind::PotrfDiag) {
+        size_t need = waited;
+        while (need < side.size() && side[need].first <= st.blk - 2) ++need;
+        if (need > waited) {
+          cudaStreamWaitEvent(h->stream, side[need - 1].second, 0);
+          waited = need;
+        }
+      }
+      launch_step(h, a, st, h->stream);
+    } else {
+      cudaEvent_t fork = next_event(), done = next_event();
+      if (!fork || !done) return cudaErrorMemoryAllocation;
+      cudaEventRecord(fork, h->stream);
+      cudaStreamWaitEvent(h->side_stream, fork, 0);
+      launch_step(h, a, st, h->side_stream);
+      cudaEventRecord(done, h->side_stream);
+      side.emplace_back(st.blk, done);
+      pending = true;
+    }
+  }
+  if (pending) {
+    cudaEvent_t e = next_event();
+    if (!e) return cudaErrorMemoryAllocation;
+    cudaEventRecord(e, h->side_stream);
+    cudaStreamWaitEvent(h->stream, e, 0);
+  }
+  return cudaGetLastError();
+}
+
+void launch_step(spb_handle* h, const spb::dev::FactorArgs& a, const spb::Step& st, cudaStream_t stream) {
+  {
     switch (st.kind) {
       case spb::StepKind::FactorSmall:
-        spb::dev::launch_factor_small(h->stream, a, h->dsmall + st.begin, st.count, st.arg);
+        spb::dev::launch_factor_small(stream, a, h->dsmall + st.begin, st.count, st.arg);
         break;
       case spb::StepKind::PotrfDiag:
-        spb::dev::launch_potrf_diag(h->stream, a, h->dpanel + st.begin, st.count, h->dwinv);
+        spb::dev::launch_potrf_diag(stream, a, h->dpanel + st.begin, st.count, h->dwinv);
         break;
       case spb::StepKind::TrsmRows:
-        spb::dev::launch_trsm_rows(h->stream, a, h->dpanel + st.begin, st.count, h->dwinv);
+        spb::dev::launch_trsm_rows(stream, a, h->dpanel + st.begin, st.count, h->dwinv);
         break;
       case spb::StepKind::Gemm:
-        spb::dev::launch_gemm(h->stream, a, h->dtiles + st.begin, st.count, st.tile);
+        spb::dev::launch_gemm(stream, a, h->dtiles + st.begin, st.count, st.tile);
         break;
     }
   }
@@ -466,9 +532,11 @@ int spb_create(const spb_options* opt, spb_handle** out) {
   }
   cudaError_t e = cudaSetDevice(h->device);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->side_stream, cudaStreamNonBlocking);
   h->stream = h->own_stream;
   if (e != cudaSuccess) {
     cudaGetLastError();
+    if (h->own_stream) cudaStreamDestroy(h->own_stream);
     delete h;
     return e == cudaErrorMemoryAllocation ? SPB_ERR_OOM : SPB_ERR_CUDA;
   }
@@ -498,6 +566,8 @@ void spb_destroy(spb_handle* h) {
   if (h->stream) cudaStreamSynchronize(h->stream);
   release_device(h);
   for (cudaEvent_t e : h->events) cudaEventDestroy(e);
+  for (cudaEvent_t e : h->lane_events) cudaEventDestroy(e);
+  if (h->side_stream) cudaStreamDestroy(h->side_stream);
   if (h->own_stream) cudaStreamDestroy(h->own_stream);
   delete h;
 }
@@ -910,8 +980,12 @@ int spb_factorize(spb_handle* h) {
   } else if (!h->fgraph && !h->plan.steps.empty()) {
     cudaGraph_t g;
     SPB_CK(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-    enqueue_factor(h);
+    cudaError_t qe = enqueue_factor(h);
     cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+    if (qe != cudaSuccess) {
+      if (e == cudaSuccess) cudaGraphDestroy(g);
+      return cuda_fail(h, qe, "factorize: graph capture");
+    }
     if (e != cudaSuccess) return cuda_fail(h, e, "factorize: graph capture");
     e = cudaGraphInstantiate(&h->fgraph, g, 0);
     cudaGraphDestroy(g);

@@ -66,7 +66,7 @@ Plan build_plan(const Symbolic& sym, const PlanParams& prm) {
                         int k0, int kn) {
     for (int cj = cbeg; cj < cend; cj += T)
       for (int ri = rbeg; ri < rend; ri += T) {
-        if ((ri - rbeg) + T <= (cj - cbeg)) continue;
+        if (ri + T <= cj) continue;  // rows and columns are both panel rows: tile above the diagonal
         TileItem t;
         t.s = s;
         t.mode = mode;
@@ -82,11 +82,11 @@ Plan build_plan(const Symbolic& sym, const PlanParams& prm) {
   // Emit the tiles of one phase as (up to) two launches: 64-wide FMA tiles and
   // 128-wide tensor-core tiles.
   std::vector<TileItem> t64, t128;
-  auto flush_gemm = [&]() {
+  auto flush_gemm = [&](Lane lane, int blk) {
     for (int pass = 0; pass < 2; ++pass) {
       std::vector<TileItem>& v = pass ? t128 : t64;
       if (v.empty()) continue;
-      Step gs{StepKind::Gemm, (int32_t)P.tile_items.size(), (int32_t)v.size(), 0, pass ? 128 : 64};
+      Step gs{StepKind::Gemm, (int32_t)P.tile_items.size(), (int32_t)v.size(), 0, pass ? 128 : 64, lane, blk};
       P.tile_items.insert(P.tile_items.end(), v.begin(), v.end());
       P.steps.push_back(gs);
       v.clear();
@@ -100,6 +100,7 @@ Plan build_plan(const Symbolic& sym, const PlanParams& prm) {
     // 1. fused small panels
     {
       Step st{StepKind::FactorSmall, (int32_t)P.small_items.size(), 0, 0, 0};
+      st.lane = Lane::Join;
       for (int s : sns)
         if (!P.is_big[s]) {
           P.small_items.push_back(s);
@@ -113,7 +114,8 @@ Plan build_plan(const Symbolic& sym, const PlanParams& prm) {
     for (int s : sns)
       if (P.is_big[s]) maxw = std::max(maxw, P.meta[s].w);
     for (int c0 = 0; c0 < maxw; c0 += prm.nb) {
-      Step pd{StepKind::PotrfDiag, (int32_t)P.panel_items.size(), 0, c0, 0};
+      const int blk = c0 / prm.nb;
+      Step pd{StepKind::PotrfDiag, (int32_t)P.panel_items.size(), 0, c0, 0, Lane::Chain, blk};
       int nslots = 0;
       for (int s : sns) {
         if (!P.is_big[s] || c0 >= P.meta[s].w) continue;
@@ -122,7 +124,7 @@ Plan build_plan(const Symbolic& sym, const PlanParams& prm) {
       P.max_diag_slots = std::max(P.max_diag_slots, nslots);
       pd.count = (int32_t)P.panel_items.size() - pd.begin;
       if (pd.count) P.steps.push_back(pd);
-      Step pt{StepKind::TrsmRows, (int32_t)P.panel_items.size(), 0, c0, 0};
+      Step pt{StepKind::TrsmRows, (int32_t)P.panel_items.size(), 0, c0, 0, Lane::Chain, blk};
       int slot = 0;
       for (int s : sns) {
         if (!P.is_big[s]) continue;
@@ -134,17 +136,22 @@ Plan build_plan(const Symbolic& sym, const PlanParams& prm) {
       }
       pt.count = (int32_t)P.panel_items.size() - pt.begin;
       if (pt.count) P.steps.push_back(pt);
-      for (int s : sns) {
-        if (!P.is_big[s]) continue;
-        const SnMeta& m = P.meta[s];
-        if (c0 >= m.w) continue;
-        int nbk = std::min(prm.nb, m.w - c0);
-        int c1 = c0 + nbk;
-        if (c1 >= m.w) continue;
-        int rows = m.h - c1;
-        push_tiles(pick(rows), tile_of(rows), s, 0, c1, m.h, c1, m.w, c0, nbk);
+      // trailing update: the first column tile (it holds the next block) on the chain,
+      // the remaining columns on the side lane
+      for (int pass = 0; pass < 2; ++pass) {
+        for (int s : sns) {
+          if (!P.is_big[s]) continue;
+          const SnMeta& m = P.meta[s];
+          if (c0 >= m.w) continue;
+          int nbk = std::min(prm.nb, m.w - c0);
+          int c1 = c0 + nbk;
+          if (c1 >= m.w) continue;
+          int rows = m.h - c1, T = tile_of(rows);
+          if (pass == 0) push_tiles(pick(rows), T, s, 0, c1, m.h, c1, std::min(m.w, c1 + T), c0, nbk);
+          else if (c1 + T < m.w) push_tiles(pick(rows), T, s, 0, c1, m.h, c1 + T, m.w, c0, nbk);
+        }
+        flush_gemm(pass == 0 ? Lane::Chain : Lane::Side, blk);
       }
-      flush_gemm();
     }
     // 3. external Schur-complement updates of every panel of the level
     for (int s : sns) {
@@ -152,7 +159,7 @@ Plan build_plan(const Symbolic& sym, const PlanParams& prm) {
       int rows = m.h - m.w;
       if (rows > 0) push_tiles(pick(rows), tile_of(rows), s, 1, m.w, m.h, m.w, m.h, 0, m.w);
     }
-    flush_gemm();
+    flush_gemm(Lane::Join, 0);
   }
   // relative indices of the external updates: groups of off-diagonal rows by
   // target, positions found by merging the sorted row lists

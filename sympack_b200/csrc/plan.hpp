@@ -58,12 +58,21 @@ enum class StepKind : int32_t {
   TrsmRows = 2,      // TRSM of 64-row tiles below that block (PanelItem)
   Gemm = 3,          // TileItem list (in-panel or external update)
 };
+// Stream lanes of the captured factorization (look-ahead): the chain of a
+// level's wide panels (POTRF, TRSM and the update of the next column tile) runs
+// in order on the main stream; the update of the remaining columns of block k
+// runs on a side stream beside the chain and must finish before the POTRF of
+// block k + 2; a join step (small panels, external updates) waits for all side work.
+enum class Lane : int32_t { Chain = 0, Side = 1, Join = 2 };
+
 struct Step {
   StepKind kind;
   int32_t begin;  // range into the matching item array
   int32_t count;
   int32_t arg;    // PotrfDiag/TrsmRows: column block start c0; FactorSmall: shared-memory bytes
   int32_t tile;   // Gemm: tile edge (64 or 128)
+  Lane lane = Lane::Join;
+  int32_t blk = 0;  // Chain / Side: column block index k = c0 / 64
 };
 
 // Panel-block work: supernode s, column block [c0, c0+nb), row tile starting at row0.

@@ -76,16 +76,6 @@ __device__ __forceinline__ void block_gemv(double* acc, const double* A, const d
   }
 }
 
-// acc[k + c*kT] -= sum_r A[r + k*kPld] * B[r + c*kT]   (transposed block), k < kk, r < m
-__device__ __forceinline__ void block_gemv_t(double* acc, const double* A, const double* B, int m, int kk, int nr) {
-  for (int idx = threadIdx.x; idx < kk * nr; idx += kThreads) {
-    int c = idx / kk, k = idx - c * kk;
-    double s = 0.0;
-    for (int r = 0; r < m; ++r) s = fma(A[r + k * kPld], B[r + c * kT], s);
-    acc[k + c * kT] -= s;
-  }
-}
-
 // Stage L rows [r0, r0+m) x columns [c0, c0+kk) of a panel into A (ld kPld), widened to FP64.
 // A full 64 x 64 block is loaded with all 16 loads of a thread in flight.
 template <class T, int kLd = kPld>
@@ -129,6 +119,21 @@ namespace {
 template <bool kTrans>
 __device__ __forceinline__ void block_gemv_atomic(double* X, int64_t ldx, int x0, const double* A, int lda,
                                                   const double* B, int m, int kk, int nr, double sign) {
+  if (m * nr * 4 <= kThreads) {  // few outputs (one or two right-hand sides): 4 threads per output
+    const int idx = threadIdx.x >> 2, part = threadIdx.x & 3;
+    const int c = idx / max(m, 1), i = idx - c * m;
+    double s = 0.0;
+    if (idx < m * nr) {
+      if (kTrans)
+        for (int k = part; k < kk; k += 4) s = fma(A[k + i * lda], B[k + c * kT], s);
+      else
+        for (int k = part; k < kk; k += 4) s = fma(A[i + k * lda], B[k + c * kT], s);
+    }
+    s += __shfl_xor_sync(0xffffffffu, s, 1);
+    s += __shfl_xor_sync(0xffffffffu, s, 2);
+    if (idx < m * nr && part == 0) atomicAdd(X + x0 + i + c * ldx, sign * s);
+    return;
+  }
   for (int idx = threadIdx.x; idx < m * nr; idx += kThreads) {
     int c = idx / m, i = idx - c * m;
     double s = 0.0;
@@ -141,10 +146,11 @@ __device__ __forceinline__ void block_gemv_atomic(double* X, int64_t ldx, int x0
 }
 
 // Lower-triangular solves of a kk x kk block held in A (ld kPld) against the
-// right-hand sides acc (ld kT), one warp per right-hand side column.
+// right-hand sides acc (ld kT), one warp per right-hand side column; rinv holds
+// the reciprocals of the diagonal (computed off the dependency chain).
 // forward: acc <- D^-1 acc ; backward: acc <- D^-T acc.
 template <bool kForward>
-__device__ void block_trsv(double* acc, const double* A, int kk, int nr) {
+__device__ void block_trsv(double* acc, const double* A, const double* rinv, int kk, int nr) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = kThreads / 32;
   for (int c = warp; c < nr; c += nw) {
     double v0 = lane < kk ? acc[lane + c * kT] : 0.0;
@@ -153,7 +159,7 @@ __device__ void block_trsv(double* acc, const double* A, int kk, int nr) {
       const int k = kForward ? step : kk - 1 - step;
       const int owner = k & 31;
       const bool hi = k >= 32;
-      double xk = __shfl_sync(0xffffffffu, hi ? v1 : v0, owner) / A[k + k * kPld];
+      double xk = __shfl_sync(0xffffffffu, hi ? v1 : v0, owner) * rinv[k];
       if (lane == owner) {
         if (hi) v1 = xk;
         else v0 = xk;
@@ -213,6 +219,7 @@ __global__ void __launch_bounds__(kThreads) k_solve_forward(PSolveArgs a) {
   double* Bx = sm + kT * kPld;      // staged X rows, ld kT
   double* acc = Bx + kT * kT;       // accumulator, ld kT
   __shared__ int sh_task, sh_stop, sh_ok;
+  __shared__ double sh_rinv[kT];
   const int nr = a.nrhs;
   for (;;) {
     const int tk = next_task(a, &sh_task, &sh_stop);
@@ -232,12 +239,14 @@ __global__ void __launch_bounds__(kThreads) k_solve_forward(PSolveArgs a) {
       const int r1 = r0 + kT, b1 = r1 < m.w ? min(kT, m.w - r1) : 0;
       stage_block(Ab, P, ld, r0, bt, r0, bt);  // L is final: load before waiting
       if (b1) stage_block<T, kT>(Bx, P, ld, r1, b1, r0, bt);
+      __syncthreads();
+      if (threadIdx.x < bt) sh_rinv[threadIdx.x] = 1.0 / Ab[threadIdx.x * (kPld + 1)];
       if (!wait_geq(a.arrived + s, a.expected[s], a.status, s, &sh_ok, a.spin_limit)) return;
       if (!wait_geq(a.upd + m.boff + t, t, a.status, s, &sh_ok, a.spin_limit)) return;
       trace_mark(a, tk, 1, now_ns());
       stage_x(acc, a.X, a.ldx, m.fc + r0, nullptr, bt, nr);
       __syncthreads();
-      block_trsv<true>(acc, Ab, bt, nr);
+      block_trsv<true>(acc, Ab, sh_rinv, bt, nr);
       __syncthreads();
       for (int idx = threadIdx.x; idx < bt * nr; idx += kThreads) {
         int c = idx / bt, r = idx - c * bt;
@@ -308,6 +317,7 @@ __global__ void __launch_bounds__(kThreads) k_solve_backward(PSolveArgs a) {
   double* Bx = sm + kT * kPld;
   double* acc = Bx + kT * kT;
   __shared__ int sh_task, sh_stop, sh_ok;
+  __shared__ double sh_rinv[kT];
   const int nr = a.nrhs;
   for (;;) {
     const int tk = next_task(a, &sh_task, &sh_stop);
@@ -346,11 +356,13 @@ __global__ void __launch_bounds__(kThreads) k_solve_backward(PSolveArgs a) {
       const int noff = (m.h - m.w + kT - 1) / kT;
       stage_block(Ab, P, ld, c0, bt, c0, bt);  // L is final: load before waiting
       if (t > 0) stage_block<T, kT>(Bx, P, ld, c0, bt, c0 - kT, kT);
+      __syncthreads();
+      if (threadIdx.x < bt) sh_rinv[threadIdx.x] = 1.0 / Ab[threadIdx.x * (kPld + 1)];
       if (!wait_geq(a.upd + m.boff + t, noff + nblk - 1 - t, a.status, s, &sh_ok, a.spin_limit)) return;
       trace_mark(a, tk, 1, now_ns());
       stage_x(acc, a.X, a.ldx, m.fc + c0, nullptr, bt, nr);
       __syncthreads();
-      block_trsv<false>(acc, Ab, bt, nr);
+      block_trsv<false>(acc, Ab, sh_rinv, bt, nr);
       __syncthreads();
       for (int idx = threadIdx.x; idx < bt * nr; idx += kThreads) {
         int c = idx / bt, r = idx - c * bt;
