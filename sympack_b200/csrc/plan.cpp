@@ -113,6 +113,7 @@ Plan build_plan(const Symbolic& sym, const PlanParams& prm) {
     int maxw = 0;
     for (int s : sns)
       if (P.is_big[s]) maxw = std::max(maxw, P.meta[s].w);
+    const int outer = std::max(prm.nb, prm.outer_nb / prm.nb * prm.nb);
     for (int c0 = 0; c0 < maxw; c0 += prm.nb) {
       const int blk = c0 / prm.nb;
       Step pd{StepKind::PotrfDiag, (int32_t)P.panel_items.size(), 0, c0, 0, Lane::Chain, blk};
@@ -136,21 +137,36 @@ Plan build_plan(const Symbolic& sym, const PlanParams& prm) {
       }
       pt.count = (int32_t)P.panel_items.size() - pt.begin;
       if (pt.count) P.steps.push_back(pt);
-      // trailing update: the first column tile (it holds the next block) on the chain,
-      // the remaining columns on the side lane
-      for (int pass = 0; pass < 2; ++pass) {
-        for (int s : sns) {
-          if (!P.is_big[s]) continue;
-          const SnMeta& m = P.meta[s];
-          if (c0 >= m.w) continue;
-          int nbk = std::min(prm.nb, m.w - c0);
-          int c1 = c0 + nbk;
-          if (c1 >= m.w) continue;
-          int rows = m.h - c1, T = tile_of(rows);
-          if (pass == 0) push_tiles(pick(rows), T, s, 0, c1, m.h, c1, std::min(m.w, c1 + T), c0, nbk);
-          else if (c1 + T < m.w) push_tiles(pick(rows), T, s, 0, c1, m.h, c1 + T, m.w, c0, nbk);
+      // update inside the outer block (columns up to its end) with this block, on the chain
+      for (int s : sns) {
+        if (!P.is_big[s]) continue;
+        const SnMeta& m = P.meta[s];
+        if (c0 >= m.w) continue;
+        const int nbk = std::min(prm.nb, m.w - c0), c1 = c0 + nbk;
+        const int oend = std::min(m.w, (c0 / outer + 1) * outer);
+        if (c1 >= oend) continue;
+        const int rows = m.h - c1;
+        push_tiles(pick(rows), tile_of(rows), s, 0, c1, m.h, c1, oend, c0, nbk);
+      }
+      flush_gemm(Lane::Chain, blk);
+      // end of an outer block: update every later column with the whole outer block
+      // (K = outer width); the first column tile (it holds the next block) on the
+      // chain, the remaining columns on the side lane
+      if ((c0 + prm.nb) % outer == 0 || c0 + prm.nb >= maxw) {
+        const int ob = c0 / outer * outer;
+        for (int pass = 0; pass < 2; ++pass) {
+          for (int s : sns) {
+            if (!P.is_big[s]) continue;
+            const SnMeta& m = P.meta[s];
+            if (ob >= m.w) continue;
+            const int oe = std::min(m.w, ob + outer);
+            if (oe >= m.w || c0 + prm.nb < oe) continue;  // a narrower panel ended its outer block earlier
+            const int rows = m.h - oe, T = tile_of(rows);
+            if (pass == 0) push_tiles(pick(rows), T, s, 0, oe, m.h, oe, std::min(m.w, oe + T), ob, oe - ob);
+            else if (oe + T < m.w) push_tiles(pick(rows), T, s, 0, oe, m.h, oe + T, m.w, ob, oe - ob);
+          }
+          flush_gemm(pass == 0 ? Lane::Chain : Lane::Side, blk);
         }
-        flush_gemm(pass == 0 ? Lane::Chain : Lane::Side, blk);
       }
     }
     // 3. external Schur-complement updates of every panel of the level

@@ -153,6 +153,7 @@ struct PlanParams {
   int small_max_w = 32;          // widest panel handled by the fused small-panel kernel
   int small_max_bytes = 96 * 1024;
   int nb = 64;                   // column block of the blocked panel factorization
+  int outer_nb = 256;            // outer block: the trailing columns are updated once per outer block
   int big_tile_rows = 128;       // products with at least this many rows use 128 x 128 tensor-core tiles
 };
 
