@@ -36,17 +36,24 @@ __device__ __forceinline__ int ld_acquire(const int32_t* p) {
   return v;
 }
 
+// Counter increment with release semantics: after a barrier, one thread's release
+// publishes the whole block's earlier writes to any thread that acquires the counter.
+__device__ __forceinline__ void red_release(int32_t* p, int v) {
+  asm volatile("red.release.gpu.global.add.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
 __device__ __forceinline__ int status_code(const Status* st) { return *(volatile const int32_t*)&st->code; }
 
-// Block-wide: wait until *flag >= target (thread 0 spins).  False on timeout or
-// if another CTA has already recorded a failure.
+// Block-wide: wait until *flag >= target (thread 0 polls with acquire loads; the
+// barrier then orders every thread's later reads after the acquire).  False on
+// timeout or if another CTA has already recorded a failure.
 __device__ bool wait_geq(const int32_t* flag, int target, Status* st, int s, int* sh_ok, long long limit) {
   if (threadIdx.x == 0) {
     int good = 1;
     if (ld_acquire(flag) < target) {
       good = 0;
       for (long long it = 0; it < limit; ++it) {
-        __nanosleep(128);
+        if (it >= 256) __nanosleep(128);  // short waits poll back to back (each poll is an L2 round trip)
         if (ld_acquire(flag) >= target) {
           good = 1;
           break;
@@ -55,7 +62,6 @@ __device__ bool wait_geq(const int32_t* flag, int target, Status* st, int s, int
       }
       if (!good && status_code(st) == 0) report_status(st, 3, s, target);
     }
-    __threadfence();
     *sh_ok = good;
   }
   __syncthreads();
@@ -207,9 +213,8 @@ __device__ __forceinline__ void trace_mark(const PSolveArgs& a, int tk, int slot
 
 // Publish a block's writes, then bump a counter (thread 0).
 __device__ __forceinline__ void signal(int32_t* counter) {
-  __threadfence();
   __syncthreads();
-  if (threadIdx.x == 0) atomicAdd(counter, 1);
+  if (threadIdx.x == 0) red_release(counter, 1);
 }
 
 template <class T>
@@ -253,11 +258,10 @@ __global__ void __launch_bounds__(kThreads) k_solve_forward(PSolveArgs a) {
         a.X[m.fc + r0 + r + c * a.ldx] = acc[r + c * kT];
       }
       if (b1) block_gemv_atomic<false>(a.X, a.ldx, m.fc + r1, Bx, kT, acc, b1, bt, nr, -1.0);
-      __threadfence();
       __syncthreads();
       if (threadIdx.x == 0) {
-        atomicAdd(a.blkdone + s, 1);
-        if (b1) atomicAdd(a.upd + m.boff + t + 1, 1);
+        if (b1) red_release(a.upd + m.boff + t + 1, 1);  // the next block first: it is on the chain
+        red_release(a.blkdone + s, 1);
       }
     } else if (task.kind == 1) {
       // U(i, t): X_t -= L_ti X_i
@@ -294,9 +298,9 @@ __global__ void __launch_bounds__(kThreads) k_solve_forward(PSolveArgs a) {
         int c = idx / bu, r = idx - c * bu;
         atomicAdd(a.X + rl[r0 + r] + c * a.ldx, -acc[r + c * kT]);
       }
-      __threadfence();
       __syncthreads();
       if (threadIdx.x == 0) {
+        __threadfence();
         int last = -1;
         for (int r = 0; r < bu; ++r) {
           int tgt = a.supmember[rl[r0 + r]];
@@ -346,9 +350,8 @@ __global__ void __launch_bounds__(kThreads) k_solve_backward(PSolveArgs a) {
         if (t < nblk - 1) stage_block(Ab, P, ld, rr, br, c0, bt);
         __syncthreads();
         block_gemv_atomic<true>(a.X, a.ldx, m.fc + c0, Ab, kPld, Bx, bt, br, nr, -1.0);
-        __threadfence();
         __syncthreads();
-        if (threadIdx.x == 0) atomicAdd(a.upd + m.boff + t, 1);
+        if (threadIdx.x == 0) red_release(a.upd + m.boff + t, 1);
       }
     } else if (task.kind == 0) {
       // B(t): every update into X_t has landed; X_t <- L_tt^-T X_t, then X_{t-1} -= L_{t,t-1}^T X_t
@@ -370,11 +373,10 @@ __global__ void __launch_bounds__(kThreads) k_solve_backward(PSolveArgs a) {
       }
       // X_{t-1} -= L_{t,t-1}^T X_t: Bx holds rows c0.. (bt) x columns c0-64.. (64), ld kT
       if (t > 0) block_gemv_atomic<true>(a.X, a.ldx, m.fc + c0 - kT, Bx, kT, acc, kT, bt, nr, -1.0);
-      __threadfence();
       __syncthreads();
       if (threadIdx.x == 0) {
-        atomicAdd(a.blkdone + s, 1);
-        if (t > 0) atomicAdd(a.upd + m.boff + t - 1, 1);
+        if (t > 0) red_release(a.upd + m.boff + t - 1, 1);  // the previous block first: it is on the chain
+        red_release(a.blkdone + s, 1);
       }
     } else {
       // V(t, u): X_u -= L_tu^T X_t
