@@ -75,7 +75,9 @@ typedef struct spb_options {
   int verbose;
   int plan_small_max_w;    /* widest supernode factored whole in shared memory (0 = default 32) */
   int plan_big_tile_rows;  /* products with this many rows use 128 x 128 tensor-core tiles (0 = default 128) */
-  int fp32_engine;         /* FP32_IR 128 x 128 update tiles: 0 = tcgen05 (TMEM accumulator), 1 = mma.sync */
+  int fp32_engine;         /* FP32_IR 128 x 128 update tiles: 0 = tcgen05 one tile per CTA (TMEM
+                              accumulator), 1 = mma.sync, 2 = persistent tcgen05 (two accumulators,
+                              epilogue warps overlapped with the next tile) */
 } spb_options;
 
 typedef struct spb_info {

@@ -161,7 +161,7 @@ spb::dev::FactorArgs factor_args(spb_handle* h) {
   a.groups = h->dgroups;
   a.rel = h->drel;
   a.fp32 = h->fp32;
-  a.tc32 = h->opt.fp32_engine == 0;
+  a.engine = h->opt.fp32_engine;
   return a;
 }
 
@@ -521,7 +521,8 @@ int spb_create(const spb_options* opt, spb_handle** out) {
   if (!h) return SPB_ERR_OOM;
   if (opt) h->opt = *opt;
   else spb_default_options(&h->opt);
-  if (h->opt.ordering < 0 || h->opt.ordering > 2 || h->opt.precision < 0 || h->opt.precision > 1) {
+  if (h->opt.ordering < 0 || h->opt.ordering > 2 || h->opt.precision < 0 || h->opt.precision > 1 ||
+      h->opt.fp32_engine < 0 || h->opt.fp32_engine > 2) {
     delete h;
     return SPB_ERR_INVALID;
   }

@@ -13,6 +13,7 @@
 // The epilogue stages C in shared memory and walks it column by column, so
 // consecutive threads touch consecutive target rows (coalesced atomics).
 #include <climits>
+#include <type_traits>
 
 #include "kernels.cuh"
 
@@ -45,6 +46,28 @@ __device__ void tile_epilogue(const FactorArgs& a, const TileItem& it, const SnM
   T* L = static_cast<T*>(a.L);
   const int jr = it.a_row0 + i;
   if (it.mode == 0) {
+    if constexpr (std::is_same<T, float>::value && std::is_same<CT, float>::value && BM % 128 == 0) {
+      // FP32 panel: 4 consecutive rows per thread and one 16-byte vector reduction per
+      // column; panels start on 32-element boundaries, leading dimensions are multiples
+      // of 4 and in-panel tiles start on 64-row boundaries, so the 4 rows are aligned
+      const int q4 = tid % (BM / 4), cp = tid / (BM / 4), i0 = 4 * q4;
+      constexpr int kCStep = NT / (BM / 4);
+      const int jr0 = it.a_row0 + i0;
+      T* g = L + m.off + jr0;
+      for (int c = cp; c < it.ncols; c += kCStep) {
+        const int gc = it.b_row0 + c;
+        const float4 v = *reinterpret_cast<const float4*>(Cs + i0 + c * ldc);
+        if (i0 + 3 < it.mrows && jr0 >= gc) {
+          atomicAdd(reinterpret_cast<float4*>(g + (int64_t)gc * m.ld), make_float4(-v.x, -v.y, -v.z, -v.w));
+        } else {
+          const float vv[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+          for (int e = 0; e < 4; ++e)
+            if (i0 + e < it.mrows && jr0 + e >= gc) atomicAdd(g + e + (int64_t)gc * m.ld, -vv[e]);
+        }
+      }
+      return;
+    }
     if (i >= it.mrows) return;
     T* g = L + m.off + jr;
     for (int c = c0; c < it.ncols; c += kStep) {
@@ -600,18 +623,260 @@ __global__ void __launch_bounds__(256, 1) k_gemm_tc32(FactorArgs a, const TileIt
   tile_epilogue<kUM, kUN, 256, float, float>(a, it, m, Cs, kULdc, (int64_t*)ints, (int64_t*)ints + 128);
 }
 
+// ---- persistent, warp-specialised variant of the tcgen05 tile ---------------------
+// One CTA per SM loops over the launch's tiles.  Warps 0-7 stage operands and (one
+// thread) issue the MMAs exactly as k_gemm_tc32 does; warps 8-11 are the epilogue:
+// each thread owns one accumulator row, reads it from tensor memory 32 columns at a
+// time and scatters it.  Two accumulators (256 TMEM columns) let the epilogue of
+// tile i run while tile i + 1 is staged and multiplied.  mbarriers: per operand
+// stage (MMAs done, stage reusable), per accumulator "full" (last MMA of a tile
+// done) and "empty" (its 4 epilogue warps have read it).
+constexpr int kPStages = 2, kPRaw = 2, kPThreads = 384;
+constexpr long long kPWaitLimit = 1LL << 22;  // mbarrier polls before a wait gives up
+constexpr size_t kPOpAll = (size_t)kPStages * kUStageBytes;          // 128 KB
+constexpr size_t kPRawAll = (size_t)kPRaw * kURawBytes;              // 64 KB
+constexpr size_t kPMaps = 4 * 128 * sizeof(int64_t);                 // 2 accumulators x {base, rel}
+constexpr size_t kPSmemBytes = 1024 + kPOpAll + kPRawAll + kPMaps + 128;
+static_assert(kPSmemBytes <= 232448, "shared memory of the persistent tcgen05 tile");
+
+__device__ __forceinline__ void named_sync(int id, int count) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
+
+__global__ void __launch_bounds__(kPThreads, 1) k_gemm_tc32p(FactorArgs a, const TileItem* __restrict__ items,
+                                                           int count) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const uint32_t raw_addr = (uint32_t)__cvta_generic_to_shared(smem_raw);
+  const uint32_t pad = ((raw_addr + 1023u) & ~1023u) - raw_addr;  // swizzle atoms need 1 KB alignment
+  unsigned char* base = smem_raw + pad;
+  const uint32_t base_addr = raw_addr + pad;
+  float* raw = reinterpret_cast<float*>(base + kPOpAll);
+  int64_t* maps = reinterpret_cast<int64_t*>(base + kPOpAll + kPRawAll);  // [acc][base 128 | rel 128]
+  uint64_t* bars = reinterpret_cast<uint64_t*>(base + kPOpAll + kPRawAll + kPMaps);
+  uint64_t* stage_bar = bars;      // [kPStages]
+  uint64_t* full_bar = bars + 2;   // [2]
+  uint64_t* empty_bar = bars + 4;  // [2]
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 6);
+  __shared__ int sh_pab, sh_eok[2];  // producer abort (read after producer barriers); epilogue wait results
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  auto sa_of = [](const void* p) { return (uint32_t)__cvta_generic_to_shared(p); };
+
+  if (tid == 0) {
+    sh_pab = 0;
+    sh_eok[0] = sh_eok[1] = 1;
+    for (int i = 0; i < 2; ++i) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(sa_of(stage_bar + i)) : "memory");
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(sa_of(full_bar + i)) : "memory");
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 4;\n" ::"r"(sa_of(empty_bar + i)) : "memory");
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(sa_of(tmem_slot)),
+                 "r"(2 * kUTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp < 8) {
+    // ---- producers: stage operands, one thread issues the MMAs ----
+    const int r = tid & 127, kq = tid >> 7;
+    int gchunk = 0;        // chunks staged by this CTA (operand stage and phase bookkeeping)
+    int last_commit = -1;  // global index of the last committed chunk
+    for (int ti = 0, tile = blockIdx.x; tile < count; tile += gridDim.x, ++ti) {
+      named_sync(1, 256);  // the previous tile's raw stages are consumed; abort flag settled
+      if (sh_pab) break;
+      const TileItem it = items[tile];
+      const SnMeta m = a.meta[it.s];
+      const float* g = static_cast<const float*>(a.L) + m.off;
+      const int64_t ld = m.ld;
+      const int acc = ti & 1;
+      auto load_raw = [&](int stage, int kk) {
+        float* ra = raw + (size_t)stage * (kURawBytes / 4);
+        float* rb = ra + kUK * kUM;
+#pragma unroll 4
+        for (int q = 0; q < kUK * kUM / 256; ++q) {
+          const int e = tid + q * 256, col = e >> 7, rr = e & 127, k = kk + col;
+          const bool kok = k < it.kn;
+          const int64_t coff = (int64_t)(it.k0 + (kok ? k : 0)) * ld;
+          const bool aok = kok && rr < it.mrows, bok = kok && rr < it.ncols;
+          cp_async4(ra + col * kUM + rr, aok ? g + it.a_row0 + rr + coff : g, aok ? 4 : 0);
+          cp_async4(rb + col * kUM + rr, bok ? g + it.b_row0 + rr + coff : g, bok ? 4 : 0);
+        }
+      };
+      const int nk = (it.kn + kUK - 1) / kUK;
+      load_raw(0, 0);
+      cp_commit();
+      for (int kt = 0; kt < nk; ++kt) {
+        if (kt + 1 < nk) load_raw((kt + 1) % kPRaw, (kt + 1) * kUK);
+        cp_commit();
+        cp_wait<kPRaw - 1>();
+        const int G = gchunk + kt, st = G % kPStages;
+        if (G >= kPStages &&
+            !mbar_wait(sa_of(stage_bar + st), (uint32_t)((G / kPStages - 1) & 1), kPWaitLimit))
+          sh_pab = 1;
+        named_sync(1, 256);  // raw chunk kt has landed for every producer
+        const float* ra = raw + (size_t)(kt % kPRaw) * (kURawBytes / 4);
+        const float* rb = ra + kUK * kUM;
+        unsigned char* sb = base + st * kUStageBytes;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const int k4 = 4 * (kq + 2 * q);
+          const uint32_t off = umma_k_offset(r, kq + 2 * q);
+          uint4 ah, al, bh, bl;
+          split_tf32(ra[(k4 + 0) * kUM + r], ah.x, al.x);
+          split_tf32(ra[(k4 + 1) * kUM + r], ah.y, al.y);
+          split_tf32(ra[(k4 + 2) * kUM + r], ah.z, al.z);
+          split_tf32(ra[(k4 + 3) * kUM + r], ah.w, al.w);
+          split_tf32(rb[(k4 + 0) * kUM + r], bh.x, bl.x);
+          split_tf32(rb[(k4 + 1) * kUM + r], bh.y, bl.y);
+          split_tf32(rb[(k4 + 2) * kUM + r], bh.z, bl.z);
+          split_tf32(rb[(k4 + 3) * kUM + r], bh.w, bl.w);
+          *reinterpret_cast<uint4*>(sb + off) = ah;
+          *reinterpret_cast<uint4*>(sb + kUOpBytes + off) = al;
+          *reinterpret_cast<uint4*>(sb + 2 * kUOpBytes + off) = bh;
+          *reinterpret_cast<uint4*>(sb + 3 * kUOpBytes + off) = bl;
+        }
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        named_sync(1, 256);
+        if (sh_pab) break;
+        if (tid == 0) {
+          if (kt == 0 && ti >= 2 &&
+              !mbar_wait(sa_of(empty_bar + acc), (uint32_t)(((ti >> 1) - 1) & 1), kPWaitLimit))
+            sh_pab = 1;  // the accumulator's previous tile has not been read out
+          if (!sh_pab) {
+            asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+            const uint32_t sa = base_addr + st * kUStageBytes, dcol = tmem + (uint32_t)(acc * kUTmemCols);
+#pragma unroll
+            for (int ks = 0; ks < kUK / 8; ++ks) {
+              const uint64_t ahi = umma_desc(sa + ks * 32), alo = umma_desc(sa + kUOpBytes + ks * 32);
+              const uint64_t bhi = umma_desc(sa + 2 * kUOpBytes + ks * 32),
+                             blo = umma_desc(sa + 3 * kUOpBytes + ks * 32);
+              const uint64_t pa[3] = {alo, ahi, ahi}, pb[3] = {bhi, blo, bhi};
+#pragma unroll
+              for (int p = 0; p < 3; ++p) {
+                const uint32_t accum = (kt > 0 || ks > 0 || p > 0) ? 1u : 0u;
+                asm volatile(
+                    "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                    " tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n}\n" ::"r"(dcol),
+                    "l"(pa[p]), "l"(pb[p]), "r"(kUIdesc), "r"(accum)
+                    : "memory");
+              }
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                             sa_of(stage_bar + st))
+                         : "memory");
+            if (kt == nk - 1)
+              asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                               sa_of(full_bar + acc))
+                           : "memory");
+          }
+        }
+        if (!sh_pab) last_commit = G;
+      }
+      gchunk += nk;
+    }
+    cp_wait<0>();
+    if (tid == 0 && last_commit >= 0)  // MMAs finished before the stages and TMEM go away
+      if (!mbar_wait(sa_of(stage_bar + last_commit % kPStages), (uint32_t)((last_commit / kPStages) & 1),
+                     kPWaitLimit))
+        sh_pab = 1;
+  } else {
+    // ---- epilogue: one accumulator row per thread ----
+    const int et = tid - 256, quarter = warp & 3, row = quarter * 32 + lane;
+    for (int ti = 0, tile = blockIdx.x; tile < count; tile += gridDim.x, ++ti) {
+      const TileItem it = items[tile];
+      const SnMeta m = a.meta[it.s];
+      const int acc = ti & 1;
+      int64_t* cbase = maps + acc * 256;
+      int64_t* crel = cbase + 128;
+      if (it.mode == 1 && et < it.ncols) {
+        const int jc = it.b_row0 + et;
+        const RelGroup gr = a.groups[a.row_group[m.lidx + jc]];
+        const SnMeta mt = a.meta[gr.t];
+        cbase[et] = mt.off + (int64_t)(a.rows[m.lidx + jc] - mt.fc) * mt.ld;
+        crel[et] = gr.rel_off - gr.j0;
+      }
+      if (et == 0) sh_eok[acc] = mbar_wait(sa_of(full_bar + acc), (uint32_t)((ti >> 1) & 1), kPWaitLimit) ? 1 : 0;
+      named_sync(2, 128);  // maps ready; the accumulator is full (or the wait gave up)
+      if (!sh_eok[acc]) break;
+      asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+      float* L = static_cast<float*>(a.L);
+      const int jr = it.a_row0 + row;
+      int64_t last = INT64_MIN;
+      int pos = 0;
+      for (int c0 = 0; c0 < kUN; c0 += 32) {
+        uint32_t v[32];
+        const uint32_t taddr = tmem + (uint32_t)(acc * kUTmemCols) + ((uint32_t)(quarter * 32) << 16) + (uint32_t)c0;
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+            "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
+            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+              "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
+              "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]),
+              "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]),
+              "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+            : "r"(taddr));
+        asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+        if (row < it.mrows) {
+#pragma unroll
+          for (int j = 0; j < 32; ++j) {
+            const int c = c0 + j, jc = it.b_row0 + c;
+            if (c < it.ncols && jr >= jc) {
+              const float val = -__uint_as_float(v[j]);
+              if (it.mode == 0) {
+                atomicAdd(L + m.off + jr + (int64_t)jc * m.ld, val);
+              } else {
+                const int64_t cr = crel[c];
+                if (cr != last) {
+                  pos = a.rel[cr + jr];
+                  last = cr;
+                }
+                atomicAdd(L + cbase[c] + pos, val);
+              }
+            }
+          }
+        }
+      }
+      asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+      __syncwarp();
+      if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(sa_of(empty_bar + acc)) : "memory");
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  if ((sh_pab || !sh_eok[0] || !sh_eok[1]) && tid == 0) report_status(a.status, 3, -1, -1);
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(2 * kUTmemCols)
+                 : "memory");
+  }
+}
+
 }  // namespace
 
+static int g_sms = 148;  // persistent tile grid: one CTA per SM
+
 void init_gemm_attributes() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, dev);
+  if (g_sms <= 0) g_sms = 148;
   cudaFuncSetAttribute(k_gemm_tf32x3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTSmemBytes);
   cudaFuncSetAttribute(k_gemm_tc32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kUSmemBytes);
+  cudaFuncSetAttribute(k_gemm_tc32p, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPSmemBytes);
   cudaFuncSetAttribute(k_gemm_dmma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDSmemBytes);
 }
 
 void launch_gemm(cudaStream_t st, const FactorArgs& a, const TileItem* items, int count, int tile) {
   if (count <= 0) return;
   if (a.fp32) {
-    if (tile == 128 && a.tc32) k_gemm_tc32<<<count, 256, kUSmemBytes, st>>>(a, items);
+    if (tile == 128 && a.engine == 2)
+      k_gemm_tc32p<<<count < g_sms ? count : g_sms, kPThreads, kPSmemBytes, st>>>(a, items, count);
+    else if (tile == 128 && a.engine == 0) k_gemm_tc32<<<count, 256, kUSmemBytes, st>>>(a, items);
     else if (tile == 128) k_gemm_tf32x3<<<count, 256, kTSmemBytes, st>>>(a, items);
     else k_gemm_simt<float><<<count, 256, kSSmemBytes, st>>>(a, items);
   } else {

@@ -27,7 +27,7 @@ struct FactorArgs {
   const RelGroup* groups;
   const int32_t* rel;        // positions of update rows in their targets' row lists
   bool fp32;                 // FP32 factor storage (precision form)
-  bool tc32;                 // FP32 128 x 128 tiles on tcgen05 (else mma.sync m16n8k8)
+  int engine;                // FP32 128 x 128 tiles: 0 tcgen05 per tile, 1 mma.sync, 2 persistent tcgen05
 };
 
 // Must run once per process (per device) before the first launch or capture.

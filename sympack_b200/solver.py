@@ -90,7 +90,7 @@ class symPACKOptions:
     verbose: int = 0
     plan_small_max_w: int = 0      # 0 = library default
     plan_big_tile_rows: int = 0    # 0 = library default
-    fp32_engine: str = "tcgen05"   # FP32_IR update tiles: "tcgen05" or "mma.sync"
+    fp32_engine: str = "tcgen05"   # FP32_IR update tiles: "tcgen05", "mma.sync", "tcgen05-persistent"
 
     def to_c(self) -> N.spb_options:
         if self.orderingStr not in N.ORDERINGS:
@@ -112,9 +112,10 @@ class symPACKOptions:
         o.verbose = self.verbose
         o.plan_small_max_w = self.plan_small_max_w
         o.plan_big_tile_rows = self.plan_big_tile_rows
-        if self.fp32_engine not in ("tcgen05", "mma.sync"):
+        engines = {"tcgen05": 0, "mma.sync": 1, "tcgen05-persistent": 2}
+        if self.fp32_engine not in engines:
             raise ValueError(f"unknown fp32_engine {self.fp32_engine!r}")
-        o.fp32_engine = 0 if self.fp32_engine == "tcgen05" else 1
+        o.fp32_engine = engines[self.fp32_engine]
         return o
 
 

@@ -61,7 +61,7 @@ def test_fp32_ir_reaches_fp64_backward_error(delta, fwd_tol, k):
         assert np.max(np.abs(x - xo)) / np.max(np.abs(xo)) <= fwd_tol
 
 
-@pytest.mark.parametrize("engine", ["tcgen05", "mma.sync"])
+@pytest.mark.parametrize("engine", ["tcgen05", "mma.sync", "tcgen05-persistent"])
 @pytest.mark.parametrize("k", [14, 22])
 def test_fp32_factor_close_to_fp64_factor(engine, k):
     """FP32 factor (3xTF32 updates on either tensor-core engine) against the FP64
