@@ -53,3 +53,36 @@ def test_bad_options():
         symPACKMatrix2D().Init(symPACKOptions(orderingStr="METIS"))
     with pytest.raises(ValueError):
         symPACKMatrix2D().Init(symPACKOptions(orderingStr="USER"))
+
+
+def test_fp32_engine_option_is_validated():
+    from sympack_b200 import symPACKMatrix2D, symPACKOptions
+    for eng in ("tcgen05", "mma.sync", "tcgen05-persistent"):
+        M = symPACKMatrix2D()
+        M.Init(symPACKOptions(device=-1, fp32_engine=eng))
+        M.close()
+    with pytest.raises(ValueError):
+        symPACKMatrix2D().Init(symPACKOptions(device=-1, fp32_engine="wmma"))
+
+
+def test_host_only_analysis_predicts_footprint_and_is_reusable():
+    import numpy as np
+    from sympack_b200 import DistSparseMatrix, generators as G, symPACKMatrix2D, symPACKOptions
+    n, cp, ri, v = G.laplacian_2d(20, 20)
+    A = DistSparseMatrix.from_lower_csc(n, cp, ri, v)
+    T = symPACKMatrix2D()
+    T.Init(symPACKOptions(device=-1))
+    T.SymbolicFactorization(A)
+    b64, b32 = T.PredictDeviceBytes("FP64", 1), T.PredictDeviceBytes("FP32_IR", 1)
+    assert b64 > T.info().arena_bytes > 0 and b32 > 0
+    assert T.PredictDeviceBytes("FP64", 64) > b64  # right-hand-side buffers grow with nrhs
+    M = symPACKMatrix2D()
+    M.Init(symPACKOptions(device=-1))
+    M.SymbolicFactorizationFrom(T)
+    assert np.array_equal(M.GetSupernodalPartition(), T.GetSupernodalPartition())
+    assert np.array_equal(M.GetOrdering()[0], T.GetOrdering()[0])
+    with pytest.raises(ValueError):  # different relaxation: the analysis is not reusable
+        R = symPACKMatrix2D()
+        from sympack_b200 import RelaxationParameters
+        R.Init(symPACKOptions(device=-1, relax=RelaxationParameters(nrelax0=4)))
+        R.SymbolicFactorizationFrom(T)

@@ -220,3 +220,23 @@ def test_solve_wait_timeout_is_reported_and_recovers():
     r = subprocess.run([sys.executable, "-c", TIMEOUT_CHILD, root], capture_output=True, text=True, timeout=180)
     assert r.returncode == 0, r.stdout + r.stderr
     assert "RECOVERED" in r.stdout
+
+
+def test_solve_trace_of_a_profiled_solve():
+    n, cp, ri, v = G.laplacian_3d(14, 14, 14, 1e-3)
+    A = DistSparseMatrix.from_lower_csc(n, cp, ri, v)
+    M = symPACKMatrix2D()
+    M.Init(symPACKOptions(device=0))
+    M.SymbolicFactorization(A)
+    M.DistributeMatrix(A)
+    M.Factorize()
+    M.SetProfiling(True)
+    M.Solve(np.ones(n))
+    for sweep, kinds in ((0, {0, 1, 2}), (1, {0, 1, 3})):
+        tr = M.GetSolveTrace(sweep).astype(np.int64)
+        assert tr.shape[1] == 4 and len(tr) > 0
+        t0, t1, t2, sk = tr.T
+        assert np.all(t0 > 0) and np.all(t1 >= t0) and np.all(t2 >= t1)
+        assert set(np.unique(sk & 255)) <= kinds
+        assert np.all((sk >> 8) < M.info().nsuper)
+    M.close()
