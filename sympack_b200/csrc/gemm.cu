@@ -286,6 +286,11 @@ __device__ __forceinline__ void cp_async4(void* smem, const void* gmem, int src_
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s), "l"(gmem), "r"(src_bytes));
 }
 
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, int src_bytes) {
+  unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(gmem), "r"(src_bytes));
+}
+
 __device__ __forceinline__ uint32_t to_tf32(float x) {
   uint32_t r;
   asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(r) : "f"(x));
@@ -420,8 +425,9 @@ constexpr int kUM = 128, kUN = 128, kUK = 32;
 constexpr int kUOpBytes = kUM * kUK * 4;           // one operand part: 16 KB
 constexpr int kUStageBytes = 4 * kUOpBytes;        // A hi, A lo, B hi, B lo
 constexpr int kUStages = 2;                         // split operand buffers (MMA double buffer)
-constexpr int kURaw = 3;                            // raw FP32 chunks in flight (cp.async)
-constexpr int kURawBytes = 2 * kUK * kUM * 4;       // A and B columns of one chunk: 32 KB
+constexpr int kURaw = 2;                            // raw FP32 chunks in flight (cp.async)
+constexpr int kURawLd = kUM + 4;                    // raw column: 128 rows from a 4-row boundary
+constexpr int kURawBytes = 2 * kUK * kURawLd * 4;   // A and B columns of one chunk: 33 KB
 constexpr int kULdc = 132;
 constexpr size_t kUCBytes = (size_t)kUN * kULdc * sizeof(float);
 constexpr size_t kUOpAll = (size_t)kUStages * kUStageBytes;   // 128 KB; C staging reuses it
@@ -503,18 +509,28 @@ __global__ void __launch_bounds__(256, 1) k_gemm_tc32(FactorArgs a, const TileIt
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
   const uint32_t tmem = *tmem_slot;
 
-  // raw chunk kk of A and B: column k of the chunk, row r at raw[stage][op][k][r]
+  // raw chunk kk of A and B in 16-byte copies: column k of the chunk holds panel rows
+  // from the 4-row boundary at or below the tile's first row, so tile row r sits at
+  // raw[stage][op][k][r + shift].  Panels start on 32-element boundaries and their
+  // leading dimension is a multiple of 4, so every copy is aligned; a copy is issued
+  // only if it holds a row of the tile, which keeps it inside the panel's padded column.
+  const int a0 = it.a_row0 & ~3, b0 = it.b_row0 & ~3;
+  const int ashift = it.a_row0 - a0, bshift = it.b_row0 - b0;
   auto load_raw = [&](int stage, int kk) {
     float* ra = raw + (size_t)stage * (kURawBytes / 4);
-    float* rb = ra + kUK * kUM;
-#pragma unroll 4
-    for (int q = 0; q < kUK * kUM / 256; ++q) {
-      const int e = tid + q * 256, col = e >> 7, r = e & 127, k = kk + col;
+    float* rb = ra + kUK * kURawLd;
+    constexpr int kVec = kUK * (kURawLd / 4);  // 16-byte copies per operand
+#pragma unroll
+    for (int q = 0; q < (kVec + 255) / 256; ++q) {
+      const int e = tid + q * 256;
+      if (e >= kVec) break;
+      const int col = e / (kURawLd / 4), f = e - col * (kURawLd / 4), k = kk + col;
       const bool kok = k < it.kn;
       const int64_t coff = (int64_t)(it.k0 + (kok ? k : 0)) * ld;
-      const bool aok = kok && r < it.mrows, bok = kok && r < it.ncols;
-      cp_async4(ra + col * kUM + r, aok ? g + it.a_row0 + r + coff : g, aok ? 4 : 0);
-      cp_async4(rb + col * kUM + r, bok ? g + it.b_row0 + r + coff : g, bok ? 4 : 0);
+      const bool aok = kok && a0 + 4 * f < it.a_row0 + it.mrows;
+      const bool bok = kok && b0 + 4 * f < it.b_row0 + it.ncols;
+      cp_async16(ra + col * kURawLd + 4 * f, aok ? g + a0 + 4 * f + coff : g, aok ? 16 : 0);
+      cp_async16(rb + col * kURawLd + 4 * f, bok ? g + b0 + 4 * f + coff : g, bok ? 16 : 0);
     }
   };
   // this thread's split pieces: row r, column groups kq + 2q (q = 0..3) of 4 columns
@@ -535,22 +551,23 @@ __global__ void __launch_bounds__(256, 1) k_gemm_tc32(FactorArgs a, const TileIt
     const uint32_t bar = (uint32_t)__cvta_generic_to_shared(bars + st);
     if (kt >= 2 && !mbar_wait(bar, (uint32_t)(((kt >> 1) - 1) & 1), kUWaitLimit)) sh_abort = 1;
     __syncthreads();  // every thread's raw copies of chunk kt have landed
-    const float* ra = raw + (size_t)(kt % kURaw) * (kURawBytes / 4);
-    const float* rb = ra + kUK * kUM;
+    const float* ra = raw + (size_t)(kt % kURaw) * (kURawBytes / 4) + r + ashift;
+    const float* rb = raw + (size_t)(kt % kURaw) * (kURawBytes / 4) + kUK * kURawLd + r + bshift;
+    const bool arow = r < it.mrows, brow = r < it.ncols;  // rows past the tile hold other panel rows
     unsigned char* sb = base + st * kUStageBytes;
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
       const int k4 = 4 * (kq + 2 * q);
       const uint32_t off = umma_k_offset(r, kq + 2 * q);
       uint4 ah, al, bh, bl;
-      split_tf32(ra[(k4 + 0) * kUM + r], ah.x, al.x);
-      split_tf32(ra[(k4 + 1) * kUM + r], ah.y, al.y);
-      split_tf32(ra[(k4 + 2) * kUM + r], ah.z, al.z);
-      split_tf32(ra[(k4 + 3) * kUM + r], ah.w, al.w);
-      split_tf32(rb[(k4 + 0) * kUM + r], bh.x, bl.x);
-      split_tf32(rb[(k4 + 1) * kUM + r], bh.y, bl.y);
-      split_tf32(rb[(k4 + 2) * kUM + r], bh.z, bl.z);
-      split_tf32(rb[(k4 + 3) * kUM + r], bh.w, bl.w);
+      split_tf32(arow ? ra[(k4 + 0) * kURawLd] : 0.f, ah.x, al.x);
+      split_tf32(arow ? ra[(k4 + 1) * kURawLd] : 0.f, ah.y, al.y);
+      split_tf32(arow ? ra[(k4 + 2) * kURawLd] : 0.f, ah.z, al.z);
+      split_tf32(arow ? ra[(k4 + 3) * kURawLd] : 0.f, ah.w, al.w);
+      split_tf32(brow ? rb[(k4 + 0) * kURawLd] : 0.f, bh.x, bl.x);
+      split_tf32(brow ? rb[(k4 + 1) * kURawLd] : 0.f, bh.y, bl.y);
+      split_tf32(brow ? rb[(k4 + 2) * kURawLd] : 0.f, bh.z, bl.z);
+      split_tf32(brow ? rb[(k4 + 3) * kURawLd] : 0.f, bh.w, bl.w);
       *reinterpret_cast<uint4*>(sb + off) = ah;
       *reinterpret_cast<uint4*>(sb + kUOpBytes + off) = al;
       *reinterpret_cast<uint4*>(sb + 2 * kUOpBytes + off) = bh;
