@@ -605,12 +605,28 @@ __global__ void __launch_bounds__(256, 1) k_gemm_tc32(FactorArgs a, const TileIt
     const uint32_t bar = (uint32_t)__cvta_generic_to_shared(bars + (committed & 1));
     if (!mbar_wait(bar, (uint32_t)((committed >> 1) & 1), kUWaitLimit)) ok = false;
   }
+  ok = __syncthreads_and(ok) != 0;  // one decision for the whole CTA (tcgen05.ld is warp-collective)
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-  if (!ok) {
-    if (tid == 0) report_status(a.status, 3, it.s, -1);
-  } else {
+  int64_t* cbase = reinterpret_cast<int64_t*>(ints);  // mode 1 column maps (reuse the raw stages)
+  int64_t* crel = cbase + 128;
+  if (ok) {
     const int quarter = warp & 3, half = warp >> 2;
     const int row = quarter * 32 + (tid & 31);
+    if (it.mode == 1) {
+      // external update straight from tensor memory: thread = accumulator row, 64 columns
+      if (tid < it.ncols) {
+        const int jc = it.b_row0 + tid;
+        const RelGroup gr = a.groups[a.row_group[m.lidx + jc]];
+        const SnMeta mt = a.meta[gr.t];
+        cbase[tid] = mt.off + (int64_t)(a.rows[m.lidx + jc] - mt.fc) * mt.ld;
+        crel[tid] = gr.rel_off - gr.j0;
+      }
+      __syncthreads();
+    }
+    float* L = static_cast<float*>(a.L);
+    const int jr = it.a_row0 + row;
+    int64_t last = INT64_MIN;
+    int pos = 0;
 #pragma unroll
     for (int part = 0; part < 2; ++part) {
       const int c0 = half * 64 + part * 32;
@@ -626,8 +642,25 @@ __global__ void __launch_bounds__(256, 1) k_gemm_tc32(FactorArgs a, const TileIt
             "=r"(v[30]), "=r"(v[31])
           : "r"(taddr));
       asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+      if (it.mode == 1) {
+        if (row < it.mrows) {
 #pragma unroll
-      for (int j = 0; j < 32; ++j) Cs[row + (c0 + j) * kULdc] = __uint_as_float(v[j]);
+          for (int j = 0; j < 32; ++j) {
+            const int c = c0 + j;
+            if (c < it.ncols && jr >= it.b_row0 + c) {
+              const int64_t cr = crel[c];
+              if (cr != last) {
+                pos = a.rel[cr + jr];
+                last = cr;
+              }
+              atomicAdd(L + cbase[c] + pos, -__uint_as_float(v[j]));
+            }
+          }
+        }
+      } else {
+#pragma unroll
+        for (int j = 0; j < 32; ++j) Cs[row + (c0 + j) * kULdc] = __uint_as_float(v[j]);
+      }
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
@@ -636,8 +669,11 @@ __global__ void __launch_bounds__(256, 1) k_gemm_tc32(FactorArgs a, const TileIt
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(kUTmemCols) : "memory");
   }
-  if (!ok) return;
-  tile_epilogue<kUM, kUN, 256, float, float>(a, it, m, Cs, kULdc, (int64_t*)ints, (int64_t*)ints + 128);
+  if (!ok) {
+    if (tid == 0) report_status(a.status, 3, it.s, -1);
+    return;
+  }
+  if (it.mode == 0) tile_epilogue<kUM, kUN, 256, float, float>(a, it, m, Cs, kULdc, cbase, crel);
 }
 
 // ---- persistent, warp-specialised variant of the tcgen05 tile ---------------------
