@@ -427,7 +427,8 @@ def serving_comparison(torch, dev, count, seed=0, load=0.8):
         out = {"solves_per_s": count / wall, "wall_s": wall, **S.latency_summary([r for _, r in stream]),
                "service_p50_ms": float(np.percentile([(r.t_done - r.t_start) * 1e3 for _, r in stream], 50)),
                "service_p99_ms": float(np.percentile([(r.t_done - r.t_start) * 1e3 for _, r in stream], 99)),
-               "max_backward_error": max(x.backward_error for x in res)}
+               # FP64 solves skip the residual (backward_error -1): reported as None
+               "max_backward_error": max((x.backward_error for x in res if x.backward_error >= 0), default=None)}
         out.update({k: int(v) for k, v in svc.stats.items()})
         return out
 

@@ -2,8 +2,9 @@
 routines to C so that they can be compiled and executed here (no Fortran
 compiler is installed).  Test infrastructure only.
 
-It handles exactly the subset those six files use (src/ordmmd.F, genmmd.F,
-mmdint.F, mmdelm.F, mmdupd.F, mmdnum.F): `#if MMDIDXSIZE` blocks (the 32-bit
+It handles exactly the subset those files use (the MMD routines src/ordmmd.F,
+genmmd.F, mmdint.F, mmdelm.F, mmdupd.F, mmdnum.F and the RCM routines genrcm.F,
+rcm.F, fnroot.F, rootls.F, degree.F): `#if MMDIDXSIZE` / `#if RCMIDXSIZE` blocks (the 32-bit
 branch is kept, as in the reference's default build, src/CMakeLists.txt:144-148),
 INTEGER declarations of scalars and 1-D arrays, assignments, logical IF with a
 single statement, IF (...) THEN / ENDIF, GO TO, labelled CONTINUE, DO loops with a terminal label,
@@ -27,7 +28,7 @@ def preprocess(text: str, mmdidxsize: int = 32) -> list[str]:
     for line in text.splitlines():
         s = line.strip().replace(" ", "")
         if s.startswith("#if"):
-            m = re.match(r"#ifMMDIDXSIZE==(\d+)", s)
+            m = re.match(r"#if(?:MMD|RCM)IDXSIZE==(\d+)", s)
             if not m:
                 raise ValueError(f"unsupported directive: {line}")
             stack.append(int(m.group(1)) == mmdidxsize)
@@ -217,13 +218,22 @@ class Subroutine:
         return head + decl + "\n".join(self.body) + "\n}\n"
 
 
-def translate(paths: list[str]) -> str:
+def translate(paths: list[str], skip: frozenset = frozenset({"perm_inverse"})) -> str:
+    """C for the subroutines of the given files; subroutines named in `skip` (helpers the
+    path does not call, e.g. perm_inverse at the end of genrcm.F) are left out."""
     subs: list[Subroutine] = []
     for p in paths:
         cur = None
+        skipping = False
         for label, s in statements(preprocess(open(p).read())):
+            if skipping:
+                skipping = s != "end"
+                continue
             if s.startswith("subroutine"):
                 m = re.fullmatch(r"subroutine([a-z][a-z0-9_]*)\((.*)\)", s)
+                if m.group(1) in skip:
+                    skipping = True
+                    continue
                 cur = Subroutine(m.group(1), split_top(m.group(2)))
                 subs.append(cur)
             elif re.match(r"integer(\*\d+)?[a-z]", s):
@@ -236,7 +246,8 @@ def translate(paths: list[str]) -> str:
                 cur.add(label, s)
     protos = "".join(f"void {s.name}_({', '.join('int*' for _ in s.args)});\n" for s in subs)
     banner = ("/* Generated from the reference's Fortran sources by oracle/f77_to_c.py.\n"
-              " * Oracle infrastructure: not part of the product. */\n")
+              " * Oracle infrastructure: not part of the product. */\n"
+              "static int iabs(int x) { return x < 0 ? -x : x; }  /* Fortran IABS */\n")
     return banner + protos + "\n" + "\n".join(s.emit() for s in subs)
 
 

@@ -1,6 +1,7 @@
 """ORACLE — the reference's own MMD Fortran (src/ordmmd.F, genmmd.F, mmdint.F,
-mmdelm.F, mmdupd.F, mmdnum.F), translated by oracle/f77_to_c.py and compiled
-into oracle/_ref/libmmd_ref.so.  Building needs the reference sources
+mmdelm.F, mmdupd.F, mmdnum.F) and RCM Fortran (src/genrcm.F, rcm.F, fnroot.F,
+rootls.F, degree.F), translated by oracle/f77_to_c.py and compiled into
+oracle/_ref/libmmd_ref.so and oracle/_ref/librcm_ref.so.  Building needs the reference sources
 (present in the development container only); the built library may travel.
 Called exactly as Ordering::MMD calls it (src/Ordering.cpp:103-218): the
 expanded graph without diagonal, iwsiz = 4n, invp taken as the result."""
@@ -57,4 +58,50 @@ def ordmmd(n: int, xadj, adj) -> np.ndarray:
                  C.byref(nofsub), C.byref(iflag))
     if iflag.value != 0:
         raise RuntimeError(f"ordmmd iflag={iflag.value}")
+    return invp
+
+
+RCM_FILES = ["genrcm.F", "rcm.F", "fnroot.F", "rootls.F", "degree.F"]
+OUT_RCM_C = HERE / "_ref" / "rcm_ref.c"
+OUT_RCM_SO = HERE / "_ref" / "librcm_ref.so"
+_rcm = None
+
+
+def rcm_available() -> bool:
+    return OUT_RCM_SO.exists() or all((REF_SRC / f).exists() for f in RCM_FILES)
+
+
+def build_rcm(force: bool = False) -> Path:
+    if OUT_RCM_SO.exists() and not force:
+        return OUT_RCM_SO
+    if not all((REF_SRC / f).exists() for f in RCM_FILES):
+        raise FileNotFoundError("reference RCM sources not present")
+    OUT_RCM_SO.parent.mkdir(exist_ok=True)
+    from . import f77_to_c
+    OUT_RCM_C.write_text(f77_to_c.translate([str(REF_SRC / f) for f in RCM_FILES]))
+    tmp = OUT_RCM_SO.with_suffix(".tmp.so")
+    subprocess.run(["gcc", "-O2", "-fPIC", "-shared", "-Wno-unused-label", "-Wno-unused-function", "-o", str(tmp),
+                    str(OUT_RCM_C)], check=True)
+    os.replace(tmp, OUT_RCM_SO)
+    return OUT_RCM_SO
+
+
+def genrcm(n: int, xadj, adj) -> np.ndarray:
+    """invp (1-based) of the reference RCM, called as Ordering::RCM calls it
+    (src/Ordering.cpp:221-300): expanded graph without diagonal, mark and xls of
+    size 2n, invp[perm[i]] = i."""
+    global _rcm
+    if _rcm is None:
+        _rcm = C.CDLL(str(build_rcm()))
+    P = C.POINTER(C.c_int32)
+    xadj = np.ascontiguousarray(xadj, np.int32).copy()  # DEGREE flips signs and restores them
+    adj = np.ascontiguousarray(adj, np.int32)
+    perm = np.zeros(n, np.int32)
+    mark = np.zeros(2 * n, np.int32)
+    xls = np.zeros(2 * n, np.int32)
+    N = C.c_int32(n)
+    _rcm.genrcm_(C.byref(N), xadj.ctypes.data_as(P), adj.ctypes.data_as(P), perm.ctypes.data_as(P),
+                 mark.ctypes.data_as(P), xls.ctypes.data_as(P))
+    invp = np.zeros(n, np.int32)
+    invp[perm - 1] = np.arange(1, n + 1, dtype=np.int32)
     return invp

@@ -8,6 +8,8 @@ for bit.  Each function cites the reference routine it follows (symPACK v2.0):
   set_keep_diag      src/DistSparseMatrixGraph.cpp:39-97
   genmmd             src/genmmd.F, mmdint.F, mmdelm.F, mmdupd.F, mmdnum.F
                      (ordmmd.F:70-79: delta = 0, maxint = 2,000,000,000)
+  genrcm             src/genrcm.F, fnroot.F, rootls.F, degree.F, rcm.F
+                     (called from src/Ordering.cpp:221-300, Ordering::RCM)
   construct_etree    src/ETree.cpp:317-397
   postorder_tree     src/ETree.cpp:24-119
   lcol_row_count     include/sympack/impl/symPACKMatrixBase_impl.hpp:310-470
@@ -16,7 +18,7 @@ for bit.  Each function cites the reference routine it follows (symPACK v2.0):
   relax_supernodes   symPACKMatrixBase_impl.hpp:473-609 (+ DisjointSet, ETree.hpp:12-99)
   symbolic_factor    symPACKMatrixBase_impl.hpp:613-935
   build_cells        include/sympack/symPACKMatrix2D.hpp:3317-3396
-  symbolic_chain     symPACKMatrix2D.hpp:2699-3081 (MMD branch)
+  symbolic_chain     symPACKMatrix2D.hpp:2699-3081 (MMD, RCM and NATURAL branches)
 
 Arrays are Python lists, 1-based values; index 0 of the work arrays of the
 MMD routines is a dummy so that the Fortran subscripts carry over.
@@ -418,6 +420,135 @@ def genmmd(neqns, xadj_in, adj_in):
 
 
 # ------------------------------------------------------ etree and counts --
+def _rootls(root, xadj, adj, mask, xls, ls):
+    """ROOTLS (rootls.F): level structure of root's component among mask != 0;
+    fills ls[1..ccsize], xls[1..nlvl+1]; returns nlvl."""
+    mask[root] = 0
+    ls[1] = root
+    nlvl = lvlend = 0
+    ccsize = 1
+    while True:
+        lbegin = lvlend + 1
+        lvlend = ccsize
+        nlvl += 1
+        xls[nlvl] = lbegin
+        for i in range(lbegin, lvlend + 1):
+            node = ls[i]
+            for j in range(xadj[node], xadj[node + 1]):
+                nbr = adj[j]
+                if mask[nbr] != 0:
+                    ccsize += 1
+                    ls[ccsize] = nbr
+                    mask[nbr] = 0
+        if ccsize - lvlend <= 0:
+            break
+    xls[nlvl + 1] = lvlend + 1
+    for i in range(1, ccsize + 1):
+        mask[ls[i]] = 1
+    return nlvl
+
+
+def _fnroot(root, xadj, adj, mask, xls, ls):
+    """FNROOT (fnroot.F): pseudo-peripheral node of root's component."""
+    nlvl = _rootls(root, xadj, adj, mask, xls, ls)
+    ccsize = xls[nlvl + 1] - 1
+    if nlvl == 1 or nlvl == ccsize:
+        return root
+    while True:
+        jstrt = xls[nlvl]
+        mindeg = ccsize
+        root = ls[jstrt]
+        if ccsize != jstrt:
+            for j in range(jstrt, ccsize + 1):
+                node = ls[j]
+                ndeg = sum(1 for k in range(xadj[node], xadj[node + 1]) if mask[adj[k]] > 0)
+                if ndeg < mindeg:
+                    root, mindeg = node, ndeg
+        nunlvl = _rootls(root, xadj, adj, mask, xls, ls)
+        if nunlvl <= nlvl:
+            return root
+        nlvl = nunlvl
+        if nlvl >= ccsize:
+            return root
+
+
+def _rcm_component(root, xadj, adj, mask, perm, off, deg):
+    """DEGREE + RCM (degree.F, rcm.F): reverse Cuthill-McKee numbering of root's
+    component into perm[off .. off+ccsize-1]; returns ccsize."""
+    # DEGREE: breadth first over the component, counting unmasked neighbours
+    seen = {root}
+    order = [root]
+    lvlend = 0
+    while True:
+        lbegin, lvlend = lvlend, len(order)
+        for i in range(lbegin, lvlend):
+            node = order[i]
+            ideg = 0
+            for j in range(xadj[node], xadj[node + 1]):
+                nbr = adj[j]
+                if mask[nbr] == 0:
+                    continue
+                ideg += 1
+                if nbr not in seen:
+                    seen.add(nbr)
+                    order.append(nbr)
+            deg[node] = ideg
+        if len(order) == lvlend:
+            break
+    ccsize = len(order)
+    mask[root] = 0
+    out = [root]
+    if ccsize > 1:
+        lvlend = 0
+        while True:
+            lbegin, lvlend = lvlend, len(out)
+            for i in range(lbegin, lvlend):
+                node = out[i]
+                fnbr = len(out)
+                for j in range(xadj[node], xadj[node + 1]):
+                    nbr = adj[j]
+                    if mask[nbr] != 0:
+                        mask[nbr] = 0
+                        out.append(nbr)
+                # stable insertion sort of the new neighbours by increasing degree
+                for k in range(fnbr + 1, len(out)):
+                    v = out[k]
+                    l = k - 1
+                    while l >= fnbr and deg[out[l]] > deg[v]:
+                        out[l + 1] = out[l]
+                        l -= 1
+                    out[l + 1] = v
+            if len(out) <= lvlend:
+                break
+        out.reverse()
+    perm[off:off + ccsize] = out
+    return ccsize
+
+
+def genrcm(neqns, xadj_in, adj_in):
+    """GENRCM (genrcm.F) on a 1-based expanded graph without diagonal; returns
+    invp (1-based) as Ordering::RCM forms it (Ordering.cpp:283-286)."""
+    xadj = [0] + list(xadj_in)
+    adj = [0] + list(adj_in)
+    mask = [0] + [1] * neqns
+    xls = [0] * (neqns + 2)
+    ls = [0] * (neqns + 2)
+    deg = [0] * (neqns + 1)
+    perm = [0] * neqns
+    num = 0
+    for i in range(1, neqns + 1):
+        if mask[i] == 0:
+            continue
+        root = _fnroot(i, xadj, adj, mask, xls, ls)
+        num += _rcm_component(root, xadj, adj, mask, perm, num, deg)
+        if num >= neqns:
+            break
+    invp = [0] * neqns
+    for k, node in enumerate(perm):
+        invp[node - 1] = k + 1
+    return invp
+
+
 def construct_etree(n, xadj, adj, perm, invp):
     parent = [0] * n
     ancstr = [0] * n
@@ -780,9 +911,9 @@ def symbolic_chain(n, colptr, rowind, ordering="MMD", relax=None):
     """SymbolicFactorization (symPACKMatrix2D.hpp:2699-3081) on a 1-based lower CSC."""
     relax = relax or {}
     xadj, adj = expand_symmetric(n, colptr, rowind)
-    if ordering == "MMD":
+    if ordering in ("MMD", "RCM"):
         sx, sa = set_keep_diag(n, xadj, adj, False)
-        invp = genmmd(n, sx, sa)
+        invp = genmmd(n, sx, sa) if ordering == "MMD" else genrcm(n, sx, sa)
         gx, ga = set_keep_diag(n, sx, sa, True)
     elif ordering == "NATURAL":
         invp = list(range(1, n + 1))

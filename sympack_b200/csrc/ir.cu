@@ -2,7 +2,7 @@
 //
 // Each step computes r = b - A x with the original matrix in FP64, measures the
 // backward error eta = ||r||_inf / (||A||_inf ||x||_inf + ||b||_inf) per
-// right-hand side and per system (a batch of block-diagonal systems is judged
+// right-hand side and per system (a batch of block-diagonal systems is measured
 // system by system, with that system's own norms), solves A d = r with the FP32 factor and updates x += d in FP64.
 // A is held as full symmetric CSR in the original ordering; its values are
 // gathered from the lower-triangle input on every DistributeMatrix.

@@ -447,6 +447,143 @@ class MinDegree {
 
 }  // namespace
 
+namespace {
+
+// Breadth-first level structure of the component of root among unmasked nodes
+// (ROOTLS, rootls.F).  ls receives the nodes level by level, xls[l] the start of
+// level l (0-based positions, xls[nlvl] = component size).  The mask is restored.
+int rcm_levels(int root, const Graph& g, std::vector<int8_t>& mask, std::vector<int32_t>& ls,
+               std::vector<int32_t>& xls) {
+  mask[root] = 0;
+  ls[0] = root;
+  int nlvl = 0, lvlend = 0, ccsize = 1;
+  for (;;) {
+    const int lbegin = lvlend;
+    lvlend = ccsize;
+    xls[nlvl++] = lbegin;
+    for (int i = lbegin; i < lvlend; ++i) {
+      const int node = ls[i];
+      for (int64_t p = g.colptr[node] - 1; p < g.colptr[node + 1] - 1; ++p) {
+        const int nbr = g.rowind[p] - 1;
+        if (mask[nbr]) {
+          ls[ccsize++] = nbr;
+          mask[nbr] = 0;
+        }
+      }
+    }
+    if (ccsize == lvlend) break;
+  }
+  xls[nlvl] = lvlend;
+  for (int i = 0; i < ccsize; ++i) mask[ls[i]] = 1;
+  return nlvl;
+}
+
+// Pseudo-peripheral node of root's component (FNROOT, fnroot.F): repeat the level
+// structure from the minimum-degree node of the last level (first such node in level
+// order) while the number of levels grows.
+int rcm_root(int root, const Graph& g, std::vector<int8_t>& mask, std::vector<int32_t>& ls,
+             std::vector<int32_t>& xls) {
+  int nlvl = rcm_levels(root, g, mask, ls, xls);
+  const int ccsize = xls[nlvl];
+  if (nlvl == 1 || nlvl == ccsize) return root;
+  for (;;) {
+    const int jstrt = xls[nlvl - 1];
+    int mindeg = ccsize;
+    root = ls[jstrt];
+    if (ccsize != jstrt + 1) {
+      for (int j = jstrt; j < ccsize; ++j) {
+        const int node = ls[j];
+        int ndeg = 0;
+        for (int64_t p = g.colptr[node] - 1; p < g.colptr[node + 1] - 1; ++p) ndeg += mask[g.rowind[p] - 1] > 0;
+        if (ndeg < mindeg) {
+          root = node;
+          mindeg = ndeg;
+        }
+      }
+    }
+    const int nunlvl = rcm_levels(root, g, mask, ls, xls);
+    if (nunlvl <= nlvl) return root;
+    nlvl = nunlvl;
+    if (nlvl >= ccsize) return root;
+  }
+}
+
+}  // namespace
+
+std::vector<int32_t> rcm_order(const Graph& g) {
+  const int n = g.n;
+  std::vector<int8_t> mask(n, 1);
+  std::vector<int32_t> perm(n), xls(n + 1), deg(n), ls(n);
+  std::vector<int8_t> seen(n, 0);
+  int num = 0;
+  for (int i = 0; i < n && num < n; ++i) {
+    if (!mask[i]) continue;
+    const int root = rcm_root(i, g, mask, ls, xls);
+    // degrees within the component among unmasked nodes (DEGREE, degree.F); the
+    // breadth-first order it visits leaves perm[num] = root
+    int32_t* pm = perm.data() + num;
+    pm[0] = root;
+    seen[root] = 1;
+    int ccsize = 1, lvlend = 0;
+    for (;;) {
+      const int lbegin = lvlend;
+      lvlend = ccsize;
+      for (int k = lbegin; k < lvlend; ++k) {
+        const int node = pm[k];
+        int ideg = 0;
+        for (int64_t p = g.colptr[node] - 1; p < g.colptr[node + 1] - 1; ++p) {
+          const int nbr = g.rowind[p] - 1;
+          if (!mask[nbr]) continue;
+          ++ideg;
+          if (seen[nbr]) continue;
+          seen[nbr] = 1;
+          pm[ccsize++] = nbr;
+        }
+        deg[node] = ideg;
+      }
+      if (ccsize == lvlend) break;
+    }
+    for (int k = 0; k < ccsize; ++k) seen[pm[k]] = 0;
+    // Cuthill-McKee numbering (RCM, rcm.F): breadth first from the root, the unnumbered
+    // neighbours of each node appended in adjacency order and then sorted by increasing
+    // degree with a stable insertion sort
+    mask[root] = 0;
+    if (ccsize > 1) {
+      int lnbr = 0;
+      lvlend = -1;
+      for (;;) {
+        const int lbegin = lvlend + 1;
+        lvlend = lnbr;
+        for (int k = lbegin; k <= lvlend; ++k) {
+          const int node = pm[k];
+          const int fnbr = lnbr + 1;
+          for (int64_t p = g.colptr[node] - 1; p < g.colptr[node + 1] - 1; ++p) {
+            const int nbr = g.rowind[p] - 1;
+            if (!mask[nbr]) continue;
+            mask[nbr] = 0;
+            pm[++lnbr] = nbr;
+          }
+          for (int kk = fnbr + 1; kk <= lnbr; ++kk) {
+            const int v = pm[kk];
+            int l = kk - 1;
+            while (l >= fnbr && deg[pm[l]] > deg[v]) {
+              pm[l + 1] = pm[l];
+              --l;
+            }
+            pm[l + 1] = v;
+          }
+        }
+        if (lnbr <= lvlend) break;
+      }
+      std::reverse(pm, pm + ccsize);  // reverse Cuthill-McKee
+    }
+    num += ccsize;
+  }
+  std::vector<int32_t> invp(n);
+  for (int k = 0; k < n; ++k) invp[perm[k]] = k + 1;
+  return invp;
+}
+
 std::vector<int32_t> mmd_order(const Graph& g) {
   const int n = g.n;
   if ((int64_t)g.rowind.size() > (int64_t)std::numeric_limits<int32_t>::max() - 2)
@@ -1011,9 +1148,9 @@ Symbolic symbolic_factorization(int n, const int64_t* colptr, const int32_t* row
   s.n = n;
   Graph full = expand_symmetric(n, colptr, rowind);  // keepDiag = 1, sorted flag kept
   Graph sg = full;                                   // GatherStructure at one rank
-  if (ordering == OrderingKind::MMD) {
+  if (ordering == OrderingKind::MMD || ordering == OrderingKind::RCM) {
     set_keep_diag(sg, false);
-    s.invp = mmd_order(sg);
+    s.invp = ordering == OrderingKind::MMD ? mmd_order(sg) : rcm_order(sg);
     set_keep_diag(sg, true);
   } else if (ordering == OrderingKind::NATURAL) {
     s.invp.resize(n);

@@ -6,6 +6,8 @@
 //   set_keep_diag         DistSparseMatrixGraph.cpp:39-97    (SetKeepDiag)
 //   mmd_order             src/ordmmd.F, genmmd.F, mmdint.F, mmdelm.F, mmdupd.F, mmdnum.F
 //                         via Ordering.cpp:103-218 (Ordering::MMD)
+//   rcm_order             src/genrcm.F, rcm.F, fnroot.F, rootls.F, degree.F
+//                         via Ordering.cpp:221-330 (Ordering::RCM)
 //   construct_etree       ETree.cpp:317-397
 //   postorder_tree        ETree.cpp:24-119 (BTreeToPO, PostOrderTree)
 //   column_counts         symPACKMatrixBase_impl.hpp:310-470 (getLColRowCount)
@@ -45,7 +47,7 @@ struct Graph {
 };
 
 // Ordering selection (Types.hpp OrderingType; only the ones this path supports).
-enum class OrderingKind { MMD = 0, NATURAL = 1, USER = 2 };
+enum class OrderingKind { MMD = 0, NATURAL = 1, USER = 2, RCM = 3 };
 
 // Full symbolic result of SymbolicFactorization on one rank.
 struct Symbolic {
@@ -91,6 +93,11 @@ void set_keep_diag(Graph& g, bool keep);
 // Multiple minimum external degree (delta = 0, maxint = 2e9) on an expanded
 // graph without diagonal.  Returns invp (old -> new, 1-based).
 std::vector<int32_t> mmd_order(const Graph& g_nodiag);
+// Reverse Cuthill-McKee (George & Liu's SPARSPAK GENRCM: pseudo-peripheral root per
+// connected component, breadth-first numbering with neighbours by increasing degree,
+// reversed), on the expanded graph without diagonal in its stored entry order.
+// Returns invp (old -> new, 1-based).
+std::vector<int32_t> rcm_order(const Graph& g_nodiag);
 
 // --- elimination tree & counts --------------------------------------------
 std::vector<int32_t> construct_etree(const Graph& g_diag, const std::vector<int32_t>& perm,

@@ -1,12 +1,12 @@
-"""Generate the golden fixtures of tests/golden/ from the reference's own MMD
-Fortran, executed here through oracle/mmd_reference.py (translated from the
+"""Generate the golden fixtures of tests/golden/ from the reference's own MMD and
+RCM Fortran, executed here through oracle/mmd_reference.py (translated from the
 reference sources and compiled with gcc).  Run in the development container:
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [mmd] [rcm]
 
-mmd_golden.npz holds, per case, the input graph (lower CSC of a seeded
-generator) and the invp the reference MMD returns for it; for the full-size
-configurations it holds the SHA-256 of that invp instead.
+mmd_golden.npz / rcm_golden.npz hold, per case, the input graph (lower CSC of a
+seeded generator) and the invp the reference ordering returns for it; for the
+full-size configurations they hold the SHA-256 of that invp instead.
 """
 import hashlib
 import os
@@ -35,28 +35,36 @@ FULL = {
 }
 
 
-def ref_invp(n, cp, ri):
+def ref_invp(n, cp, ri, ordering="mmd"):
     xadj, adj = so.expand_symmetric(n, cp, ri)
     sx, sa = so.set_keep_diag(n, xadj, adj, False)
-    return mr.ordmmd(n, sx, sa)
+    return mr.ordmmd(n, sx, sa) if ordering == "mmd" else mr.genrcm(n, sx, sa)
 
 
-def main():
+RCM_EXTRA = {
+    "rand_400_forest": lambda: G.random_graph_spd(400, 1.2, 1.05, seed=5),  # many components
+    "lap2d_1x50": lambda: G.laplacian_2d(1, 50),
+}
+
+
+def write(ordering):
     out = {}
-    for name, gen in SMALL.items():
+    cases = dict(SMALL, **(RCM_EXTRA if ordering == "rcm" else {}))
+    for name, gen in cases.items():
         n, cp, ri, _ = gen()
         out[f"{name}/colptr"] = cp
         out[f"{name}/rowind"] = ri
-        out[f"{name}/invp"] = ref_invp(n, cp, ri)
+        out[f"{name}/invp"] = ref_invp(n, cp, ri, ordering)
     for name, gen in FULL.items():
         n, cp, ri, _ = gen()
-        inv = ref_invp(n, cp, ri)
+        inv = ref_invp(n, cp, ri, ordering)
         out[f"{name}/invp_sha256"] = np.frombuffer(hashlib.sha256(inv.astype("<i4").tobytes()).digest(), np.uint8)
         out[f"{name}/invp_head"] = inv[:64]
-    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "mmd_golden.npz")
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), f"{ordering}_golden.npz")
     np.savez_compressed(path, **out)
     print(path, os.path.getsize(path))
 
 
 if __name__ == "__main__":
-    main()
+    for ordering in (sys.argv[1:] or ["mmd", "rcm"]):
+        write(ordering)

@@ -64,6 +64,21 @@ def test_factor_and_solution_match_oracle(name, gen):
         assert relerr(x, f.solve(b)) <= TOL, nrhs
 
 
+@pytest.mark.parametrize("name,gen", [CASES[0], CASES[4], CASES[5]])
+@pytest.mark.parametrize("ordering", ["RCM", "NATURAL"])
+def test_other_orderings_match_oracle(name, gen, ordering):
+    """RCM and NATURAL orderings give long chains of supernodes (deep elimination
+    trees, few per level): the same bound as MMD."""
+    n, cp, ri, v = gen()
+    A = DistSparseMatrix.from_lower_csc(n, cp, ri, v)
+    M = setup(A, orderingStr=ordering)
+    f = oracle_for(M, A)
+    assert relerr(M.GetFactor(), f.factor()) <= TOL
+    b = np.random.default_rng(4).standard_normal((n, 3))
+    M.Solve(b)
+    assert relerr(M.GetSolution(nrhs=3), f.solve(b)) <= TOL
+
+
 def test_cfg1_through_rutherford_boeing(tmp_path):
     """2D 5-point Laplacian 64x64 written to RB and read back, as the reference driver does."""
     n, cp, ri, v = G.laplacian_2d(64, 64)

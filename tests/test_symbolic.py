@@ -1,6 +1,7 @@
-"""Symbolic analysis: bit-exact against the reference MMD (golden fixtures made
-by executing the reference's Fortran), against the independent Python oracle,
-and against mathematical definitions (structure of the dense Cholesky factor)."""
+"""Symbolic analysis: bit-exact against the reference MMD and RCM orderings (golden
+fixtures made by executing the reference's Fortran), against the independent
+Python oracle, and against mathematical definitions (structure of the dense
+Cholesky factor)."""
 import hashlib
 import os
 
@@ -11,6 +12,7 @@ from oracle import symbolic_oracle as so
 from sympack_b200 import DistSparseMatrix, RelaxationParameters, generators as G, symPACKMatrix2D, symPACKOptions
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "mmd_golden.npz")
+GOLDEN_RCM = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "rcm_golden.npz")
 
 
 def analyze(n, cp, ri, **opt):
@@ -25,8 +27,8 @@ def analyze(n, cp, ri, **opt):
                 xsuper=M.GetSupernodalPartition(), supmember=M.GetSupMembership(), xlindx=xl, lindx=li)
 
 
-def golden_cases():
-    g = np.load(GOLDEN)
+def golden_cases(path=GOLDEN):
+    g = np.load(path)
     names = sorted({k.split("/")[0] for k in g.files if k.endswith("/invp")})
     return [(nm, g[f"{nm}/colptr"], g[f"{nm}/rowind"], g[f"{nm}/invp"]) for nm in names]
 
@@ -57,6 +59,42 @@ def test_mmd_full_size_matches_reference_hash(name, gen):
     assert hashlib.sha256(inv.astype("<i4").tobytes()).digest() == g[f"{name}/invp_sha256"].tobytes()
 
 
+@pytest.mark.parametrize("case", golden_cases(GOLDEN_RCM), ids=lambda c: c[0])
+def test_rcm_matches_reference_fortran(case):
+    name, cp, ri, invp = case
+    n = len(cp) - 1
+    assert np.array_equal(analyze(n, cp, ri, orderingStr="RCM")["mmd_invp"], invp)
+
+
+@pytest.mark.parametrize("case", golden_cases(GOLDEN_RCM), ids=lambda c: c[0])
+def test_oracle_rcm_matches_reference_fortran(case):
+    name, cp, ri, invp = case
+    n = len(cp) - 1
+    xadj, adj = so.expand_symmetric(n, cp, ri)
+    sx, sa = so.set_keep_diag(n, xadj, adj, False)
+    assert np.array_equal(np.array(so.genrcm(n, sx, sa)), invp)
+
+
+@pytest.mark.parametrize("name,gen", [("lap3d_60", lambda: G.laplacian_3d(60, 60, 60, 1e-3)),
+                                      ("st27_80", lambda: G.stencil27(80, 80, 80, 1e-2))])
+def test_rcm_full_size_matches_reference_hash(name, gen):
+    g = np.load(GOLDEN_RCM)
+    n, cp, ri, _ = gen()
+    inv = analyze(n, cp, ri, orderingStr="RCM")["mmd_invp"]
+    assert np.array_equal(inv[:64], g[f"{name}/invp_head"])
+    assert hashlib.sha256(inv.astype("<i4").tobytes()).digest() == g[f"{name}/invp_sha256"].tobytes()
+
+
+def test_rcm_is_a_bandwidth_ordering():
+    """On a 2D grid RCM numbers by level sets: the permuted bandwidth stays within
+    one grid line (plus one), far below MMD's."""
+    n, cp, ri, _ = G.laplacian_2d(40, 40)
+    inv = analyze(n, cp, ri, orderingStr="RCM")["mmd_invp"]
+    cols = np.repeat(np.arange(n), np.diff(cp))
+    assert np.abs(inv[ri - 1] - inv[cols]).max() <= 41
+    assert sorted(inv) == list(range(1, n + 1))
+
+
 KEYS = ["mmd_invp", "perm", "invp", "parent", "cc_fund", "cc", "xsuper", "supmember", "xlindx", "lindx"]
 GRAPHS = [
     ("lap2d_64", lambda: G.laplacian_2d(64, 64)),
@@ -69,7 +107,7 @@ GRAPHS = [
 
 
 @pytest.mark.parametrize("name,gen", GRAPHS)
-@pytest.mark.parametrize("ordering", ["MMD", "NATURAL"])
+@pytest.mark.parametrize("ordering", ["MMD", "NATURAL", "RCM"])
 def test_symbolic_chain_matches_oracle(name, gen, ordering):
     n, cp, ri, _ = gen()
     p = analyze(n, cp, ri, orderingStr=ordering)
@@ -121,9 +159,10 @@ def dense_factor_structure(n, cp, ri, invp):
 
 
 @pytest.mark.parametrize("name,gen", GRAPHS[:5])
-def test_etree_counts_structure_match_factor_pattern(name, gen):
+@pytest.mark.parametrize("ordering", ["MMD", "RCM"])
+def test_etree_counts_structure_match_factor_pattern(name, gen, ordering):
     n, cp, ri, _ = gen()
-    p = analyze(n, cp, ri)
+    p = analyze(n, cp, ri, orderingStr=ordering)
     S = dense_factor_structure(n, cp, ri, p["invp"])
     # elimination tree: parent(j) = first off-diagonal nonzero row of column j
     for j in range(n):
