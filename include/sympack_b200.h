@@ -56,6 +56,7 @@ extern "C" {
 #define SPB_ORDERING_NATURAL 1
 #define SPB_ORDERING_USER 2
 #define SPB_ORDERING_RCM 3        /* reverse Cuthill-McKee (genrcm.F) */
+#define SPB_ORDERING_AMD 4        /* approximate minimum degree (amdbar.F) */
 
 #define SPB_PRECISION_FP64 0      /* plain FP64 factor and solve (the drop-in path) */
 #define SPB_PRECISION_FP32_IR 1   /* FP32 factor + FP64 iterative refinement */

@@ -1,14 +1,16 @@
-"""ORACLE build recipe — translate the reference's fixed-form Fortran 77 MMD
+"""ORACLE build recipe — translate the reference's fixed-form Fortran 77 ordering
 routines to C so that they can be compiled and executed here (no Fortran
 compiler is installed).  Test infrastructure only.
 
 It handles exactly the subset those files use (the MMD routines src/ordmmd.F,
-genmmd.F, mmdint.F, mmdelm.F, mmdupd.F, mmdnum.F and the RCM routines genrcm.F,
-rcm.F, fnroot.F, rootls.F, degree.F): `#if MMDIDXSIZE` / `#if RCMIDXSIZE` blocks (the 32-bit
-branch is kept, as in the reference's default build, src/CMakeLists.txt:144-148),
-INTEGER declarations of scalars and 1-D arrays, assignments, logical IF with a
-single statement, IF (...) THEN / ENDIF, GO TO, labelled CONTINUE, DO loops with a terminal label,
-CALL, RETURN and END.  Fortran semantics preserved: arguments by reference,
+genmmd.F, mmdint.F, mmdelm.F, mmdupd.F, mmdnum.F, the RCM routines genrcm.F,
+rcm.F, fnroot.F, rootls.F, degree.F and the AMD routine amdbar.F):
+`#if MMDIDXSIZE` / `RCMIDXSIZE` / `AMDIDXSIZE` blocks (the 32-bit branch is kept,
+as in the reference's default build, src/CMakeLists.txt:138-154), INTEGER
+declarations of scalars and 1-D arrays, INTRINSIC, assignments, logical IF with a
+single statement, IF (...) THEN / ELSE IF (...) THEN / ELSE / ENDIF, GO TO,
+labelled CONTINUE, DO loops with a terminal label, the intrinsics MAX, MIN, MOD
+and ABS of two (one) integer arguments, CALL, RETURN and END.  Fortran semantics preserved: arguments by reference,
 1-based arrays, blanks insignificant, DO trip counts fixed at loop entry.
 
     python oracle/f77_to_c.py OUT.c FILE.F [FILE.F ...]
@@ -18,6 +20,7 @@ from __future__ import annotations
 import re
 import sys
 
+INTRINSICS = {"max", "min", "mod", "abs"}
 OPS = [(".lt.", " < "), (".le.", " <= "), (".gt.", " > "), (".ge.", " >= "), (".eq.", " == "),
        (".ne.", " != "), (".and.", " && "), (".or.", " || "), (".not.", " !")]
 
@@ -28,7 +31,7 @@ def preprocess(text: str, mmdidxsize: int = 32) -> list[str]:
     for line in text.splitlines():
         s = line.strip().replace(" ", "")
         if s.startswith("#if"):
-            m = re.match(r"#if(?:MMD|RCM)IDXSIZE==(\d+)", s)
+            m = re.match(r"#if(?:MMD|RCM|AMD)IDXSIZE==(\d+)", s)
             if not m:
                 raise ValueError(f"unsupported directive: {line}")
             stack.append(int(m.group(1)) == mmdidxsize)
@@ -119,6 +122,11 @@ class Subroutine:
                     out += f"{name}[({self.expr(s[j + 1:k])}) - 1]"
                     i = k + 1
                     continue
+                if j < len(s) and s[j] == "(" and name in INTRINSICS:
+                    k = match_paren(s, j)
+                    out += f"f_{name}(" + ", ".join(self.expr(a) for a in split_top(s[j + 1:k])) + ")"
+                    i = k + 1
+                    continue
                 if name in self.args and name not in self.arrays:
                     out += f"(*{name})"
                 else:
@@ -184,6 +192,17 @@ class Subroutine:
                 self.body.append(f"L{label}: ;")
             self.body.append(f"if ({self.expr(s[3:-5])}) {{")
             return
+        m = re.fullmatch(r"elseif(\(.*\))then", s)
+        if m and match_paren(s, 6) == len(s) - 5:
+            if label:
+                raise ValueError(f"labelled ELSE IF: {s}")
+            self.body.append(f"}} else if ({self.expr(s[7:-5])}) {{")
+            return
+        if s == "else":
+            if label:
+                raise ValueError(f"labelled ELSE: {s}")
+            self.body.append("} else {")
+            return
         if s in ("endif", "endif;"):
             if label:
                 self.body.append(f"L{label}: ;")
@@ -238,6 +257,8 @@ def translate(paths: list[str], skip: frozenset = frozenset({"perm_inverse"})) -
                 subs.append(cur)
             elif re.match(r"integer(\*\d+)?[a-z]", s):
                 cur.declare(s)
+            elif s.startswith("intrinsic"):
+                continue
             elif s == "end":
                 if cur.open_do:
                     raise ValueError(f"unterminated DO in {cur.name}")
@@ -247,7 +268,11 @@ def translate(paths: list[str], skip: frozenset = frozenset({"perm_inverse"})) -
     protos = "".join(f"void {s.name}_({', '.join('int*' for _ in s.args)});\n" for s in subs)
     banner = ("/* Generated from the reference's Fortran sources by oracle/f77_to_c.py.\n"
               " * Oracle infrastructure: not part of the product. */\n"
-              "static int iabs(int x) { return x < 0 ? -x : x; }  /* Fortran IABS */\n")
+              "static int iabs(int x) { return x < 0 ? -x : x; }  /* Fortran IABS */\n"
+              "static int f_abs(int x) { return x < 0 ? -x : x; }\n"
+              "static int f_max(int a, int b) { return a > b ? a : b; }\n"
+              "static int f_min(int a, int b) { return a < b ? a : b; }\n"
+              "static int f_mod(int a, int b) { return a % b; }  /* Fortran MOD: sign of a */\n")
     return banner + protos + "\n" + "\n".join(s.emit() for s in subs)
 
 

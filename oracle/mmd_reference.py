@@ -1,7 +1,8 @@
 """ORACLE — the reference's own MMD Fortran (src/ordmmd.F, genmmd.F, mmdint.F,
-mmdelm.F, mmdupd.F, mmdnum.F) and RCM Fortran (src/genrcm.F, rcm.F, fnroot.F,
-rootls.F, degree.F), translated by oracle/f77_to_c.py and compiled into
-oracle/_ref/libmmd_ref.so and oracle/_ref/librcm_ref.so.  Building needs the reference sources
+mmdelm.F, mmdupd.F, mmdnum.F), RCM Fortran (src/genrcm.F, rcm.F, fnroot.F,
+rootls.F, degree.F) and AMD Fortran (src/amdbar.F), translated by
+oracle/f77_to_c.py and compiled into oracle/_ref/libmmd_ref.so,
+oracle/_ref/librcm_ref.so and oracle/_ref/libamd_ref.so.  Building needs the reference sources
 (present in the development container only); the built library may travel.
 Called exactly as Ordering::MMD calls it (src/Ordering.cpp:103-218): the
 expanded graph without diagonal, iwsiz = 4n, invp taken as the result."""
@@ -104,4 +105,54 @@ def genrcm(n: int, xadj, adj) -> np.ndarray:
                  mark.ctypes.data_as(P), xls.ctypes.data_as(P))
     invp = np.zeros(n, np.int32)
     invp[perm - 1] = np.arange(1, n + 1, dtype=np.int32)
+    return invp
+
+
+AMD_FILES = ["amdbar.F"]
+OUT_AMD_C = HERE / "_ref" / "amd_ref.c"
+OUT_AMD_SO = HERE / "_ref" / "libamd_ref.so"
+_amd = None
+
+
+def amd_available() -> bool:
+    return OUT_AMD_SO.exists() or all((REF_SRC / f).exists() for f in AMD_FILES)
+
+
+def build_amd(force: bool = False) -> Path:
+    if OUT_AMD_SO.exists() and not force:
+        return OUT_AMD_SO
+    if not all((REF_SRC / f).exists() for f in AMD_FILES):
+        raise FileNotFoundError("reference AMD sources not present")
+    OUT_AMD_SO.parent.mkdir(exist_ok=True)
+    from . import f77_to_c
+    OUT_AMD_C.write_text(f77_to_c.translate([str(REF_SRC / f) for f in AMD_FILES]))
+    tmp = OUT_AMD_SO.with_suffix(".tmp.so")
+    subprocess.run(["gcc", "-O2", "-fPIC", "-shared", "-Wno-unused-label", "-Wno-unused-function",
+                    "-fwrapv", "-o", str(tmp), str(OUT_AMD_C)], check=True)
+    os.replace(tmp, OUT_AMD_SO)
+    return OUT_AMD_SO
+
+
+def amdbar(n: int, xadj, adj) -> np.ndarray:
+    """invp (1-based) of the reference AMD, called as Ordering::AMD calls it
+    (src/Ordering.cpp:411-520): expanded graph without diagonal, IW of nnz + n
+    entries, IWLEN = nnz + n, PFREE = nnz + 1, IOVFLO = INT32_MAX; ELEN is invp."""
+    global _amd
+    if _amd is None:
+        _amd = C.CDLL(str(build_amd()))
+    P = C.POINTER(C.c_int32)
+    nnz = len(adj)
+    pe = np.ascontiguousarray(xadj, np.int32)[:n + 1].copy()
+    iw = np.zeros(nnz + n, np.int32)
+    iw[:nnz] = adj
+    ln = np.diff(np.ascontiguousarray(xadj, np.int64)).astype(np.int32)
+    ln = np.append(ln, 0).astype(np.int32)
+    qsize, ecforw, perm, marker, vtxdeg, invp = (np.zeros(n, np.int32) for _ in range(6))
+    iwork = np.zeros(4 * n, np.int32)
+    N, iwlen, pfree = C.c_int32(n), C.c_int32(nnz + n), C.c_int32(nnz + 1)
+    ncmpa, iovflo = C.c_int32(0), C.c_int32(2 ** 31 - 1)
+    _amd.amdbar_(C.byref(N), pe.ctypes.data_as(P), iw.ctypes.data_as(P), ln.ctypes.data_as(P), C.byref(iwlen),
+                 C.byref(pfree), qsize.ctypes.data_as(P), ecforw.ctypes.data_as(P), perm.ctypes.data_as(P),
+                 iwork.ctypes.data_as(P), invp.ctypes.data_as(P), vtxdeg.ctypes.data_as(P), C.byref(ncmpa),
+                 marker.ctypes.data_as(P), C.byref(iovflo))
     return invp

@@ -10,6 +10,7 @@ for bit.  Each function cites the reference routine it follows (symPACK v2.0):
                      (ordmmd.F:70-79: delta = 0, maxint = 2,000,000,000)
   genrcm             src/genrcm.F, fnroot.F, rootls.F, degree.F, rcm.F
                      (called from src/Ordering.cpp:221-300, Ordering::RCM)
+  amdbar             src/amdbar.F (called from src/Ordering.cpp:411-520, Ordering::AMD)
   construct_etree    src/ETree.cpp:317-397
   postorder_tree     src/ETree.cpp:24-119
   lcol_row_count     include/sympack/impl/symPACKMatrixBase_impl.hpp:310-470
@@ -18,7 +19,7 @@ for bit.  Each function cites the reference routine it follows (symPACK v2.0):
   relax_supernodes   symPACKMatrixBase_impl.hpp:473-609 (+ DisjointSet, ETree.hpp:12-99)
   symbolic_factor    symPACKMatrixBase_impl.hpp:613-935
   build_cells        include/sympack/symPACKMatrix2D.hpp:3317-3396
-  symbolic_chain     symPACKMatrix2D.hpp:2699-3081 (MMD, RCM and NATURAL branches)
+  symbolic_chain     symPACKMatrix2D.hpp:2699-3081 (MMD, RCM, AMD and NATURAL branches)
 
 Arrays are Python lists, 1-based values; index 0 of the work arrays of the
 MMD routines is a dummy so that the Fortran subscripts carry over.
@@ -549,6 +550,285 @@ def genrcm(neqns, xadj_in, adj_in):
     return invp
 
 
+def amdbar(n, xadj_in, adj_in):
+    """AMDBAR (amdbar.F) as Ordering::AMD calls it (Ordering.cpp:466-490): IW holds
+    the adjacency plus n free entries (IWLEN = nnz + n, PFREE = nnz + 1), IOVFLO =
+    2**31 - 1; returns ELEN, the inverse permutation (1-based).  Index 0 of every
+    array is a dummy so that the Fortran subscripts carry over."""
+    nnz = len(adj_in)
+    iwlen = nnz + n
+    iw = [0] * (iwlen + 1)
+    iw[1:nnz + 1] = list(adj_in)
+    pe = [0] + [int(x) for x in xadj_in[:n]]
+    ln_ = [0] + [int(xadj_in[i + 1] - xadj_in[i]) for i in range(n)]
+    pfree = nnz + 1
+    nv = [0] * (n + 1)
+    nxt = [0] * (n + 1)
+    last = [0] * (n + 1)
+    head = [0] * (n + 1)
+    elen = [0] * (n + 1)
+    degree = [0] * (n + 1)
+    w = [0] * (n + 1)
+    wflg, mindeg, nel, hmod, dmax = 2, 1, 0, max(1, n - 1), 0
+    wbig = 2 ** 31 - 1 - n
+    for i in range(1, n + 1):
+        nv[i], w[i], degree[i] = 1, 1, ln_[i]
+    for i in range(1, n + 1):
+        deg = degree[i]
+        if deg > 0:
+            inext = head[deg]
+            if inext:
+                last[inext] = i
+            nxt[i] = inext
+            head[deg] = i
+        else:
+            nel += 1
+            elen[i], pe[i], w[i] = -nel, 0, 0
+
+    def remove(i):
+        ilast, inext = last[i], nxt[i]
+        if inext:
+            last[inext] = ilast
+        if ilast:
+            nxt[ilast] = inext
+        else:
+            head[degree[i]] = inext
+
+    def reset_w():
+        for x in range(1, n + 1):
+            if w[x]:
+                w[x] = 1
+
+    while nel < n:
+        deg = mindeg
+        while head[deg] <= 0:
+            deg += 1
+        me = head[deg]
+        mindeg = deg
+        inext = nxt[me]
+        if inext:
+            last[inext] = 0
+        head[deg] = inext
+        elenme = elen[me]
+        elen[me] = -(nel + 1)
+        nvpiv = nv[me]
+        nel += nvpiv
+        nv[me] = -nvpiv
+        degme = 0
+        if elenme == 0:
+            pme1 = pe[me]
+            pme2 = pme1 - 1
+            for p in range(pme1, pme1 + ln_[me]):
+                i = iw[p]
+                if nv[i] > 0:
+                    degme += nv[i]
+                    nv[i] = -nv[i]
+                    pme2 += 1
+                    iw[pme2] = i
+                    remove(i)
+            newmem = 0
+        else:
+            p = pe[me]
+            pme1 = pfree
+            slenme = ln_[me] - elenme
+            for knt1 in range(1, elenme + 2):
+                if knt1 > elenme:
+                    e, pj, ln = me, p, slenme
+                else:
+                    e = iw[p]
+                    p += 1
+                    pj, ln = pe[e], ln_[e]
+                for knt2 in range(1, ln + 1):
+                    i = iw[pj]
+                    pj += 1
+                    nvi = nv[i]
+                    if nvi <= 0:
+                        continue
+                    if pfree > iwlen:  # garbage collection
+                        pe[me] = p
+                        ln_[me] -= knt1
+                        if ln_[me] == 0:
+                            pe[me] = 0
+                        pe[e] = pj
+                        ln_[e] = ln - knt2
+                        if ln_[e] == 0:
+                            pe[e] = 0
+                        for j in range(1, n + 1):
+                            pn = pe[j]
+                            if pn > 0:
+                                pe[j] = iw[pn]
+                                iw[pn] = -j
+                        pdst = psrc = 1
+                        pend = pme1 - 1
+                        while psrc <= pend:
+                            j = -iw[psrc]
+                            psrc += 1
+                            if j > 0:
+                                iw[pdst] = pe[j]
+                                pe[j] = pdst
+                                pdst += 1
+                                lenj = ln_[j]
+                                iw[pdst:pdst + lenj - 1] = iw[psrc:psrc + lenj - 1] if lenj > 1 else []
+                                pdst += lenj - 1
+                                psrc += lenj - 1
+                        p1 = pdst
+                        for ps in range(pme1, pfree):
+                            iw[pdst] = iw[ps]
+                            pdst += 1
+                        pme1, pfree = p1, pdst
+                        pj, p = pe[e], pe[me]
+                    degme += nvi
+                    nv[i] = -nvi
+                    iw[pfree] = i
+                    pfree += 1
+                    remove(i)
+                if e != me:
+                    pe[e], w[e] = -me, 0
+            pme2 = pfree - 1
+            newmem = pfree - pme1
+        degree[me] = degme
+        pe[me] = pme1
+        ln_[me] = pme2 - pme1 + 1
+        if wflg >= wbig:
+            reset_w()
+            wflg = 2
+        for pme in range(pme1, pme2 + 1):
+            i = iw[pme]
+            eln = elen[i]
+            if eln > 0:
+                nvi = -nv[i]
+                wnvi = wflg - nvi
+                for p in range(pe[i], pe[i] + eln):
+                    e = iw[p]
+                    we = w[e]
+                    if we >= wflg:
+                        we -= nvi
+                    elif we != 0:
+                        we = degree[e] + wnvi
+                    w[e] = we
+        for pme in range(pme1, pme2 + 1):
+            i = iw[pme]
+            p1 = pe[i]
+            p2 = p1 + elen[i] - 1
+            pn = p1
+            h = deg = 0
+            for p in range(p1, p2 + 1):
+                e = iw[p]
+                if w[e] != 0:
+                    deg += w[e] - wflg
+                    iw[pn] = e
+                    pn += 1
+                    h += e
+            elen[i] = pn - p1 + 1
+            p3 = pn
+            for p in range(p2 + 1, p1 + ln_[i]):
+                j = iw[p]
+                if nv[j] > 0:
+                    deg += nv[j]
+                    iw[pn] = j
+                    pn += 1
+                    h += j
+            if elen[i] == 1 and p3 == pn:  # mass elimination
+                pe[i] = -me
+                nvi = -nv[i]
+                degme -= nvi
+                nvpiv += nvi
+                nel += nvi
+                nv[i] = elen[i] = 0
+            else:
+                degree[i] = min(degree[i], deg)
+                iw[pn] = iw[p3]
+                iw[p3] = iw[p1]
+                iw[p1] = me
+                ln_[i] = pn - p1 + 1
+                h = h % hmod + 1
+                j = head[h]
+                if j <= 0:
+                    nxt[i] = -j
+                    head[h] = -i
+                else:
+                    nxt[i] = last[j]
+                    last[j] = i
+                last[i] = h
+        degree[me] = degme
+        dmax = max(dmax, degme)
+        wflg += dmax
+        if wflg >= wbig:
+            reset_w()
+            wflg = 2
+        for pme in range(pme1, pme2 + 1):
+            i = iw[pme]
+            if nv[i] >= 0:
+                continue
+            h = last[i]
+            j = head[h]
+            if j == 0:
+                continue
+            if j < 0:
+                i = -j
+                head[h] = 0
+            else:
+                i = last[j]
+                last[j] = 0
+            while i != 0 and nxt[i] != 0:
+                ln, eln = ln_[i], elen[i]
+                for p in range(pe[i] + 1, pe[i] + ln):
+                    w[iw[p]] = wflg
+                jlast, j = i, nxt[i]
+                while j != 0:
+                    if ln_[j] == ln and elen[j] == eln and all(w[iw[p]] == wflg for p in range(pe[j] + 1, pe[j] + ln)):
+                        pe[j] = -i
+                        nv[i] += nv[j]
+                        nv[j] = elen[j] = 0
+                        j = nxt[j]
+                        nxt[jlast] = j
+                    else:
+                        jlast, j = j, nxt[j]
+                wflg += 1
+                i = nxt[i]
+        p = pme1
+        nleft = n - nel
+        for pme in range(pme1, pme2 + 1):
+            i = iw[pme]
+            nvi = -nv[i]
+            if nvi > 0:
+                nv[i] = nvi
+                deg = max(1, min(degree[i] + degme - nvi, nleft - nvi))
+                inext = head[deg]
+                if inext:
+                    last[inext] = i
+                nxt[i] = inext
+                last[i] = 0
+                head[deg] = i
+                mindeg = min(mindeg, deg)
+                degree[i] = deg
+                iw[p] = i
+                p += 1
+        nv[me] = nvpiv + degme
+        ln_[me] = p - pme1
+        if ln_[me] == 0:
+            pe[me] = w[me] = 0
+        if newmem:
+            pfree = p
+    for i in range(1, n + 1):
+        if elen[i] == 0:
+            j = -pe[i]
+            while elen[j] >= 0:
+                j = -pe[j]
+            e = j
+            k = -elen[e]
+            j = i
+            while elen[j] >= 0:
+                jnext = -pe[j]
+                pe[j] = -e
+                if elen[j] == 0:
+                    elen[j] = k
+                    k += 1
+                j = jnext
+            elen[e] = -k
+    return [abs(elen[i]) for i in range(1, n + 1)]
+
+
 def construct_etree(n, xadj, adj, perm, invp):
     parent = [0] * n
     ancstr = [0] * n
@@ -911,9 +1191,9 @@ def symbolic_chain(n, colptr, rowind, ordering="MMD", relax=None):
     """SymbolicFactorization (symPACKMatrix2D.hpp:2699-3081) on a 1-based lower CSC."""
     relax = relax or {}
     xadj, adj = expand_symmetric(n, colptr, rowind)
-    if ordering in ("MMD", "RCM"):
+    if ordering in ("MMD", "RCM", "AMD"):
         sx, sa = set_keep_diag(n, xadj, adj, False)
-        invp = genmmd(n, sx, sa) if ordering == "MMD" else genrcm(n, sx, sa)
+        invp = {"MMD": genmmd, "RCM": genrcm, "AMD": amdbar}[ordering](n, sx, sa)
         gx, ga = set_keep_diag(n, sx, sa, True)
     elif ordering == "NATURAL":
         invp = list(range(1, n + 1))

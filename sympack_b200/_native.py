@@ -23,7 +23,7 @@ SPB_ERR_STRUCTURE = -6
 SPB_ERR_TIMEOUT = -7
 SPB_ERR_NOT_CONVERGED = -8
 
-ORDERINGS = {"MMD": 0, "NATURAL": 1, "USER": 2, "RCM": 3}
+ORDERINGS = {"MMD": 0, "NATURAL": 1, "USER": 2, "RCM": 3, "AMD": 4}
 PRECISIONS = {"FP64": 0, "FP32_IR": 1}
 
 

@@ -20,7 +20,7 @@ CSRC = PKG / "csrc"
 LIBDIR = PKG / "_lib"
 LIB = LIBDIR / "libsympack_b200.so"
 
-SOURCES = ["symbolic.cpp", "plan.cpp", "rb_io.cpp", "kernels.cu", "gemm.cu", "solve.cu", "ir.cu", "capi.cu"]
+SOURCES = ["symbolic.cpp", "amd.cpp", "plan.cpp", "rb_io.cpp", "kernels.cu", "gemm.cu", "solve.cu", "ir.cu", "capi.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -521,7 +521,7 @@ int spb_create(const spb_options* opt, spb_handle** out) {
   if (!h) return SPB_ERR_OOM;
   if (opt) h->opt = *opt;
   else spb_default_options(&h->opt);
-  if (h->opt.ordering < 0 || h->opt.ordering > 3 || h->opt.precision < 0 || h->opt.precision > 1 ||
+  if (h->opt.ordering < 0 || h->opt.ordering > 4 || h->opt.precision < 0 || h->opt.precision > 1 ||
       h->opt.fp32_engine < 0 || h->opt.fp32_engine > 2) {
     delete h;
     return SPB_ERR_INVALID;

@@ -1148,9 +1148,11 @@ Symbolic symbolic_factorization(int n, const int64_t* colptr, const int32_t* row
   s.n = n;
   Graph full = expand_symmetric(n, colptr, rowind);  // keepDiag = 1, sorted flag kept
   Graph sg = full;                                   // GatherStructure at one rank
-  if (ordering == OrderingKind::MMD || ordering == OrderingKind::RCM) {
+  if (ordering == OrderingKind::MMD || ordering == OrderingKind::RCM || ordering == OrderingKind::AMD) {
     set_keep_diag(sg, false);
-    s.invp = ordering == OrderingKind::MMD ? mmd_order(sg) : rcm_order(sg);
+    s.invp = ordering == OrderingKind::MMD ? mmd_order(sg)
+             : ordering == OrderingKind::RCM ? rcm_order(sg)
+                                             : amd_order(sg);
     set_keep_diag(sg, true);
   } else if (ordering == OrderingKind::NATURAL) {
     s.invp.resize(n);

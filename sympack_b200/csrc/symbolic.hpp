@@ -8,6 +8,7 @@
 //                         via Ordering.cpp:103-218 (Ordering::MMD)
 //   rcm_order             src/genrcm.F, rcm.F, fnroot.F, rootls.F, degree.F
 //                         via Ordering.cpp:221-330 (Ordering::RCM)
+//   amd_order (amd.cpp)   src/amdbar.F via Ordering.cpp:411-520 (Ordering::AMD)
 //   construct_etree       ETree.cpp:317-397
 //   postorder_tree        ETree.cpp:24-119 (BTreeToPO, PostOrderTree)
 //   column_counts         symPACKMatrixBase_impl.hpp:310-470 (getLColRowCount)
@@ -47,7 +48,7 @@ struct Graph {
 };
 
 // Ordering selection (Types.hpp OrderingType; only the ones this path supports).
-enum class OrderingKind { MMD = 0, NATURAL = 1, USER = 2, RCM = 3 };
+enum class OrderingKind { MMD = 0, NATURAL = 1, USER = 2, RCM = 3, AMD = 4 };
 
 // Full symbolic result of SymbolicFactorization on one rank.
 struct Symbolic {
@@ -98,6 +99,10 @@ std::vector<int32_t> mmd_order(const Graph& g_nodiag);
 // reversed), on the expanded graph without diagonal in its stored entry order.
 // Returns invp (old -> new, 1-based).
 std::vector<int32_t> rcm_order(const Graph& g_nodiag);
+// Approximate minimum degree (Amestoy, Davis & Duff; the AMDBAR variant: no dense-row
+// detection, no aggressive absorption) on the expanded graph without diagonal, with a
+// workspace of nnz + n entries.  Returns invp (old -> new, 1-based).
+std::vector<int32_t> amd_order(const Graph& g_nodiag);
 
 // --- elimination tree & counts --------------------------------------------
 std::vector<int32_t> construct_etree(const Graph& g_diag, const std::vector<int32_t>& perm,

@@ -1,10 +1,10 @@
-"""Generate the golden fixtures of tests/golden/ from the reference's own MMD and
-RCM Fortran, executed here through oracle/mmd_reference.py (translated from the
-reference sources and compiled with gcc).  Run in the development container:
+"""Generate the golden fixtures of tests/golden/ from the reference's own MMD, RCM
+and AMD Fortran, executed here through oracle/mmd_reference.py (translated from
+the reference sources and compiled with gcc).  Run in the development container:
 
-    python tests/golden/make_golden.py [mmd] [rcm]
+    python tests/golden/make_golden.py [mmd] [rcm] [amd]
 
-mmd_golden.npz / rcm_golden.npz hold, per case, the input graph (lower CSC of a
+mmd_golden.npz / rcm_golden.npz / amd_golden.npz hold, per case, the input graph (lower CSC of a
 seeded generator) and the invp the reference ordering returns for it; for the
 full-size configurations they hold the SHA-256 of that invp instead.
 """
@@ -38,7 +38,7 @@ FULL = {
 def ref_invp(n, cp, ri, ordering="mmd"):
     xadj, adj = so.expand_symmetric(n, cp, ri)
     sx, sa = so.set_keep_diag(n, xadj, adj, False)
-    return mr.ordmmd(n, sx, sa) if ordering == "mmd" else mr.genrcm(n, sx, sa)
+    return {"mmd": mr.ordmmd, "rcm": mr.genrcm, "amd": mr.amdbar}[ordering](n, sx, sa)
 
 
 RCM_EXTRA = {
@@ -49,7 +49,7 @@ RCM_EXTRA = {
 
 def write(ordering):
     out = {}
-    cases = dict(SMALL, **(RCM_EXTRA if ordering == "rcm" else {}))
+    cases = dict(SMALL, **(RCM_EXTRA if ordering != "mmd" else {}))
     for name, gen in cases.items():
         n, cp, ri, _ = gen()
         out[f"{name}/colptr"] = cp
@@ -66,5 +66,5 @@ def write(ordering):
 
 
 if __name__ == "__main__":
-    for ordering in (sys.argv[1:] or ["mmd", "rcm"]):
+    for ordering in (sys.argv[1:] or ["mmd", "rcm", "amd"]):
         write(ordering)

@@ -65,10 +65,10 @@ def test_factor_and_solution_match_oracle(name, gen):
 
 
 @pytest.mark.parametrize("name,gen", [CASES[0], CASES[4], CASES[5]])
-@pytest.mark.parametrize("ordering", ["RCM", "NATURAL"])
+@pytest.mark.parametrize("ordering", ["AMD", "RCM", "NATURAL"])
 def test_other_orderings_match_oracle(name, gen, ordering):
-    """RCM and NATURAL orderings give long chains of supernodes (deep elimination
-    trees, few per level): the same bound as MMD."""
+    """AMD, RCM and NATURAL orderings (RCM and NATURAL give long chains of
+    supernodes: deep elimination trees, few per level): the same bound as MMD."""
     n, cp, ri, v = gen()
     A = DistSparseMatrix.from_lower_csc(n, cp, ri, v)
     M = setup(A, orderingStr=ordering)

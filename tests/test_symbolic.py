@@ -1,4 +1,4 @@
-"""Symbolic analysis: bit-exact against the reference MMD and RCM orderings (golden
+"""Symbolic analysis: bit-exact against the reference MMD, RCM and AMD orderings (golden
 fixtures made by executing the reference's Fortran), against the independent
 Python oracle, and against mathematical definitions (structure of the dense
 Cholesky factor)."""
@@ -13,6 +13,7 @@ from sympack_b200 import DistSparseMatrix, RelaxationParameters, generators as G
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "mmd_golden.npz")
 GOLDEN_RCM = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "rcm_golden.npz")
+GOLDEN_AMD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "amd_golden.npz")
 
 
 def analyze(n, cp, ri, **opt):
@@ -85,6 +86,40 @@ def test_rcm_full_size_matches_reference_hash(name, gen):
     assert hashlib.sha256(inv.astype("<i4").tobytes()).digest() == g[f"{name}/invp_sha256"].tobytes()
 
 
+@pytest.mark.parametrize("case", golden_cases(GOLDEN_AMD), ids=lambda c: c[0])
+def test_amd_matches_reference_fortran(case):
+    name, cp, ri, invp = case
+    n = len(cp) - 1
+    assert np.array_equal(analyze(n, cp, ri, orderingStr="AMD")["mmd_invp"], invp)
+
+
+@pytest.mark.parametrize("case", golden_cases(GOLDEN_AMD), ids=lambda c: c[0])
+def test_oracle_amd_matches_reference_fortran(case):
+    name, cp, ri, invp = case
+    n = len(cp) - 1
+    xadj, adj = so.expand_symmetric(n, cp, ri)
+    sx, sa = so.set_keep_diag(n, xadj, adj, False)
+    assert np.array_equal(np.array(so.amdbar(n, sx, sa)), invp)
+
+
+@pytest.mark.parametrize("name,gen", [("lap3d_60", lambda: G.laplacian_3d(60, 60, 60, 1e-3)),
+                                      ("st27_80", lambda: G.stencil27(80, 80, 80, 1e-2))])
+def test_amd_full_size_matches_reference_hash(name, gen):
+    """Full-size graphs: the workspace of nnz + n entries is compacted several times."""
+    g = np.load(GOLDEN_AMD)
+    n, cp, ri, _ = gen()
+    inv = analyze(n, cp, ri, orderingStr="AMD")["mmd_invp"]
+    assert np.array_equal(inv[:64], g[f"{name}/invp_head"])
+    assert hashlib.sha256(inv.astype("<i4").tobytes()).digest() == g[f"{name}/invp_sha256"].tobytes()
+
+
+def test_amd_fill_close_to_mmd():
+    """Both are minimum-degree heuristics: the factor sizes agree within 15% on a 3D grid."""
+    n, cp, ri, _ = G.laplacian_3d(16, 16, 16, 1e-3)
+    nnz = {o: int(analyze(n, cp, ri, orderingStr=o)["cc_fund"].sum()) for o in ("MMD", "AMD")}
+    assert abs(nnz["AMD"] - nnz["MMD"]) <= 0.15 * nnz["MMD"], nnz
+
+
 def test_rcm_is_a_bandwidth_ordering():
     """On a 2D grid RCM numbers by level sets: the permuted bandwidth stays within
     one grid line (plus one), far below MMD's."""
@@ -107,7 +142,7 @@ GRAPHS = [
 
 
 @pytest.mark.parametrize("name,gen", GRAPHS)
-@pytest.mark.parametrize("ordering", ["MMD", "NATURAL", "RCM"])
+@pytest.mark.parametrize("ordering", ["MMD", "NATURAL", "RCM", "AMD"])
 def test_symbolic_chain_matches_oracle(name, gen, ordering):
     n, cp, ri, _ = gen()
     p = analyze(n, cp, ri, orderingStr=ordering)
@@ -159,7 +194,7 @@ def dense_factor_structure(n, cp, ri, invp):
 
 
 @pytest.mark.parametrize("name,gen", GRAPHS[:5])
-@pytest.mark.parametrize("ordering", ["MMD", "RCM"])
+@pytest.mark.parametrize("ordering", ["MMD", "RCM", "AMD"])
 def test_etree_counts_structure_match_factor_pattern(name, gen, ordering):
     n, cp, ri, _ = gen()
     p = analyze(n, cp, ri, orderingStr=ordering)
