@@ -56,6 +56,7 @@ def parse():
     ap.add_argument("--serve-requests", type=int, default=1000,
                     help="requests of the serving workload (10000 = the named workload)")
     ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--no-ldl", action="store_true", help="skip the LDL^T vs Cholesky comparison")
     ap.add_argument("--no-serve", action="store_true")
     return ap.parse_args()
 
@@ -282,6 +283,53 @@ def precision_comparison(torch, dev, stream, grid=80, reps=2):
         M.close()
     torch.cuda.empty_cache()
     return out
+
+
+def ldl_comparison(torch, dev, stream, grid=60, qd_grid=50, reps=2):
+    """LDL^T (the reference's -fact LDL) next to Cholesky on the headline matrix (same
+    analysis, same flop statistic), and LDL^T alone on a quasi-definite indefinite
+    matrix of the same kind of grid, which Cholesky rejects.  Device-resident values,
+    factor and nrhs-1 solve timed with CUDA events (best of reps)."""
+    from sympack_b200 import DistSparseMatrix, generators as G, symPACKMatrix2D, symPACKOptions
+
+    def run(n, cp, ri, v, dec):
+        A = DistSparseMatrix.from_lower_csc(n, cp, ri, v)
+        M = symPACKMatrix2D()
+        M.Init(symPACKOptions(device=dev.index, decomposition=dec))
+        M.SymbolicFactorization(A)
+        M.SetStream(stream.cuda_stream)
+        dv = torch.from_numpy(v).to(dev)
+        b = torch.from_numpy(np.random.default_rng(0).standard_normal(n)).to(dev)
+        x = torch.empty_like(b)
+        fac, sol = [], []
+        for r in range(reps + 1):
+            e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+            e0.record(stream)
+            M.DistributeMatrixDevice(dv.data_ptr())
+            M.Factorize()
+            e1.record(stream)
+            M.SolveDevice(b.data_ptr(), x.data_ptr(), 1, n)
+            e2.record(stream)
+            torch.cuda.synchronize()
+            if r:
+                fac.append(e0.elapsed_time(e1))
+                sol.append(e1.elapsed_time(e2))
+        flops = M.info().flops_stat
+        out = {"factor_ms": min(fac), "solve_ms": min(sol), "factor_tflops": flops / (min(fac) * 1e-3) / 1e12,
+               "backward_error": backward_error(A, x.cpu().numpy(), b.cpu().numpy())}
+        M.close()
+        torch.cuda.empty_cache()
+        return out
+
+    n, cp, ri, v = build_matrix(grid)
+    res = {"workload": f"3D 7-point Laplacian {grid}^3 + 1e-3 I (n={n}), MMD, nrhs 1",
+           "LL": run(n, cp, ri, v, "LL"), "LDL": run(n, cp, ri, v, "LDL")}
+    res["ldl_over_ll_factor_time"] = res["LDL"]["factor_ms"] / res["LL"]["factor_ms"]
+    qn, qcp, qri, qv = G.quasi_definite_3d(qd_grid, qd_grid, qd_grid, 0.3, 1e-2, seed=0)
+    res["indefinite"] = {"workload": f"quasi-definite 27-point {qd_grid}^3 (n={qn}), 30% negative vertices, "
+                                     f"delta 1e-2, seed 0, MMD, nrhs 1",
+                         "LDL": run(qn, qcp, qri, qv, "LDL")}
+    return res
 
 
 def per_system_backward_error(systems, offs, x, b):
@@ -585,6 +633,10 @@ def run_ours(args):
     if not args.no_precision:
         precision = precision_comparison(torch, dev, stream, grid=args.precision_grid)
 
+    ldl = None
+    if not args.no_ldl:
+        ldl = ldl_comparison(torch, dev, stream, grid=args.grid)
+
     batching = None
     if not args.no_batch:
         batching = batching_comparison(torch, dev, stream, args.batch_systems)
@@ -621,6 +673,7 @@ def run_ours(args):
             "latency_ms": {"p50": float(np.percentile(tot, 50)), "p99": float(np.percentile(tot, 99))},
             "roofline": roofline, "roofline_solve": roofline_solve, "kernels_profiled_step": kernels,
             "precision_form": precision,
+            "ldl_form": ldl,
             "batching_form": batching,
             "serving_form": serving,
             "cpu_baseline": cpu,

@@ -58,6 +58,11 @@ extern "C" {
 #define SPB_ORDERING_RCM 3        /* reverse Cuthill-McKee (genrcm.F) */
 #define SPB_ORDERING_AMD 4        /* approximate minimum degree (amdbar.F) */
 
+#define SPB_DECOMPOSITION_LL 0    /* A = L L^T (Cholesky, DecompositionType::LL, "-fact LL") */
+#define SPB_DECOMPOSITION_LDL 1   /* A = L D L^T without pivoting (DecompositionType::LDL, "-fact LDL"):
+                                     symmetric matrices with nonzero pivots in the chosen ordering,
+                                     e.g. quasi-definite ones; FP64 only; spb_get_factor returns L with
+                                     D on the diagonal; a zero pivot gives SPB_ERR_NOT_SPD */
 #define SPB_PRECISION_FP64 0      /* plain FP64 factor and solve (the drop-in path) */
 #define SPB_PRECISION_FP32_IR 1   /* FP32 factor + FP64 iterative refinement */
 
@@ -80,6 +85,9 @@ typedef struct spb_options {
   int fp32_engine;         /* FP32_IR 128 x 128 update tiles: 0 = tcgen05 one tile per CTA (TMEM
                               accumulator), 1 = mma.sync, 2 = persistent tcgen05 (two accumulators,
                               epilogue warps overlapped with the next tile) */
+  int decomposition;       /* SPB_DECOMPOSITION_* (symPACKOptions::decomposition, Types.hpp:97,119) */
+  int plan_outer_nb;       /* columns per outer block of a wide panel: its trailing columns are
+                              updated once per outer block (0 = default 256; multiple of 64, <= 4096) */
 } spb_options;
 
 typedef struct spb_info {
@@ -134,7 +142,7 @@ int spb_predict_device_bytes(const spb_handle* h, int32_t precision, int32_t nrh
  * whole in shared memory; update products with at least big_tile_rows rows use
  * 128 x 128 tensor-core tiles.  The symbolic analysis is kept; values must be
  * distributed again.  Used by the tile-shape autotuner. */
-int spb_replan(spb_handle* h, int32_t small_max_w, int32_t big_tile_rows);
+int spb_replan(spb_handle* h, int32_t small_max_w, int32_t big_tile_rows, int32_t outer_nb);
 /* DistributeMatrix: values in the same order as rowind (host or device pointer). */
 int spb_distribute(spb_handle* h, const double* nzval);
 int spb_distribute_device(spb_handle* h, const double* d_nzval);

@@ -26,6 +26,7 @@ def load():
         lib.orc_get_factor.argtypes = [VP, DP]
         lib.orc_status.argtypes = [VP]
         lib.orc_set_threads.argtypes = [C.c_int]
+        lib.orc_set_ldl.argtypes = [VP, C.c_int]
         _lib = lib
     return _lib
 
@@ -35,9 +36,10 @@ def _p(a, t):
 
 
 class OracleFactor:
-    """One factorization: cells built from a symbolic result (dict of arrays)."""
+    """One factorization: cells built from a symbolic result (dict of arrays);
+    ldl=True runs the reference's LDL^T cells (D on the factor's diagonal)."""
 
-    def __init__(self, n, sym, threads=None):
+    def __init__(self, n, sym, threads=None, ldl=False):
         lib = load()
         if threads:
             lib.orc_set_threads(int(threads))
@@ -50,6 +52,8 @@ class OracleFactor:
         self.h = lib.orc_create(n, self.nsuper, _p(xs, C.c_int32), _p(xl, C.c_int64), _p(li, C.c_int32),
                                 _p(sm, C.c_int32), _p(iv, C.c_int32))
         self.factor_size = int(np.sum((xl[1:] - xl[:-1]) * (xs[1:] - xs[:-1])))
+        if ldl:
+            lib.orc_set_ldl(self.h, 1)
 
     def distribute(self, colptr, rowind, nzval):
         cp = np.ascontiguousarray(colptr, np.int64)
@@ -62,7 +66,7 @@ class OracleFactor:
     def factorize(self):
         rc = load().orc_factorize(self.h)
         if rc == -2:
-            raise ArithmeticError(f"Matrix is not HPD (supernode {load().orc_status(self.h)})")
+            raise ArithmeticError(f"Matrix is not HPD / zero pivot (supernode {load().orc_status(self.h)})")
         if rc:
             raise RuntimeError(f"oracle factorize failed ({rc})")
 

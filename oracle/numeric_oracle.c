@@ -17,6 +17,15 @@
  *                 with Trsm and Gemm on the permuted RHS       2D.hpp:1486-1797, 5728-6322
  *   get_solution  un-permute                                   2D.hpp:6713-6757
  *
+ * LDL^T (DecompositionType::LDL, blockCellLDL_t, 2D.hpp:1802-2465), selected by
+ * orc_set_ldl:
+ *   factorize     Potrf_LDL('U') of the diagonal cell: unit U = L^T strictly
+ *                 above the diagonal, D on it; a zero pivot stops it   lapack.hpp:206-560
+ *   trsm          Trsm('L','U','T','U') then column I scaled by 1/D_I   2D.hpp:2118-2137
+ *   update        Gemm with W = D L_J^T (computeDLT) instead of L_J^T   2D.hpp:2140-2390
+ *   solve         unit forward sweep, scaling by 1/D (scale_contrib), unit
+ *                 backward sweep                                        2D.hpp:2392-2462
+ *
  * Tasks run in supernode order 1..nsuper, a topological order of the
  * reference's FACTOR -> TRSM -> UPDATE2D_COMP DAG (2D.hpp:3893-3997); at one
  * rank without SP_THREADS the reference also runs them one at a time with a
@@ -60,6 +69,9 @@ typedef struct {
   double* tmp;             /* update buffer */
   size_t tmp_size;
   int status;              /* 0, or the 1-based supernode whose Potrf failed */
+  int ldl;                 /* 1: LDL^T (D on the diagonal of the diagonal cells) */
+  double* scaled;          /* LDL^T: D-scaled copy of a cell (computeDLT) */
+  size_t scaled_size;
 } orc_t;
 
 void orc_set_threads(int t) { scipy_openblas_set_num_threads(t); }
@@ -151,6 +163,7 @@ void orc_destroy(orc_t* o) {
   free(o->supmember);
   free(o->invp);
   free(o->tmp);
+  free(o->scaled);
   free(o);
 }
 
@@ -199,13 +212,49 @@ int orc_distribute(orc_t* o, const int64_t* colptr, const int* rowind, const dou
   return 0;
 }
 
+void orc_set_ldl(orc_t* o, int ldl) { o->ldl = ldl; }
+
+/* Potf2_LDL('U', n, A, lda) (lapack.hpp:206-270): A = U^T D U with unit upper U,
+ * column by column; returns the 1-based column of a zero pivot, or 0.  Potrf_LDL
+ * (lapack.hpp:398-560) blocks the same recurrence by 64 columns. */
+static int potf2_ldl_upper(int n, double* A, int lda, double* work) {
+  for (int j = 0; j < n; ++j) {
+    for (int i = 0; i < j; ++i) work[i] = A[i + (size_t)j * lda] * A[i + (size_t)i * lda];
+    double ajj = A[j + (size_t)j * lda];
+    for (int i = 0; i < j; ++i) ajj -= A[i + (size_t)j * lda] * work[i];
+    A[j + (size_t)j * lda] = ajj;
+    if (!(fabs(ajj) > 0)) return j + 1;
+    for (int c = j + 1; c < n; ++c) {
+      double t = A[j + (size_t)c * lda];
+      for (int i = 0; i < j; ++i) t -= A[i + (size_t)c * lda] * work[i];
+      A[j + (size_t)c * lda] = t * (1.0 / ajj);
+    }
+  }
+  return 0;
+}
+
+static double* scaled_buffer(orc_t* o, size_t need) {
+  if (need > o->scaled_size) {
+    free(o->scaled);
+    o->scaled = (double*)malloc(sizeof(double) * need);
+    o->scaled_size = o->scaled ? need : 0;
+  }
+  return o->scaled;
+}
+
 int orc_factorize(orc_t* o) {
   const double one = 1.0, zero = 0.0;
   for (int I = 1; I <= o->nsuper; ++I) {
     int w = width(o, I), info = 0;
     cell_t* diag = &o->cells[I][0];
     /* FACTOR */
-    scipy_dpotrf_("U", &w, diag->nzval, &w, &info, 1);
+    if (o->ldl) {
+      double* work = scaled_buffer(o, (size_t)w);
+      if (!work) return -3;
+      info = potf2_ldl_upper(w, diag->nzval, w, work);
+    } else {
+      scipy_dpotrf_("U", &w, diag->nzval, &w, &info, 1);
+    }
     if (info != 0) {
       o->status = I;
       return -2;
@@ -213,7 +262,11 @@ int orc_factorize(orc_t* o) {
     /* TRSM of every off-diagonal cell */
     for (int k = 1; k < o->ncells[I]; ++k) {
       cell_t* c = &o->cells[I][k];
-      scipy_dtrsm_("L", "U", "T", "N", &w, &c->nrows, &one, diag->nzval, &w, c->nzval, &w, 1, 1, 1, 1);
+      scipy_dtrsm_("L", "U", "T", o->ldl ? "U" : "N", &w, &c->nrows, &one, diag->nzval, &w, c->nzval, &w, 1, 1, 1,
+                   1);
+      if (o->ldl)
+        for (int q = 0; q < c->nrows; ++q)
+          for (int j = 0; j < w; ++j) c->nzval[(size_t)q * w + j] *= 1.0 / diag->nzval[(size_t)j * w + j];
     }
     /* UPDATE2D_COMP: target (K, J) -= L_KI L_JI^T for K >= J */
     for (int jj = 1; jj < o->ncells[I]; ++jj) {
@@ -225,8 +278,16 @@ int orc_factorize(orc_t* o) {
         cell_t* tgt = find_cell(o, J, K);
         if (!tgt) return -6;
         int mJ = cj->nrows, mK = ck->nrows;
-        /* buf (column-major mJ x mK) = LJ^T-view * LK-view */
-        scipy_dgemm_("T", "N", &mJ, &mK, &w, &one, cj->nzval, &w, ck->nzval, &w, &zero, o->tmp, &mJ, 1, 1);
+        /* buf (column-major mJ x mK) = LJ^T-view * LK-view; LDL^T: D LJ^T-view */
+        const double* lj = cj->nzval;
+        if (o->ldl) {
+          double* S = scaled_buffer(o, (size_t)mJ * w);
+          if (!S) return -3;
+          for (int q = 0; q < mJ; ++q)
+            for (int j = 0; j < w; ++j) S[(size_t)q * w + j] = diag->nzval[(size_t)j * w + j] * cj->nzval[(size_t)q * w + j];
+          lj = S;
+        }
+        scipy_dgemm_("T", "N", &mJ, &mK, &w, &one, lj, &w, ck->nzval, &w, &zero, o->tmp, &mJ, 1, 1);
         /* scatter: row k of the K cell -> target row offset, row j of the J cell -> target column */
         int kr = 0;
         for (int b = 0; b < ck->nblocks; ++b)
@@ -262,7 +323,7 @@ int orc_solve(orc_t* o, double* B, int nrhs, int64_t ldb) {
   for (int J = 1; J <= o->nsuper; ++J) {
     int w = width(o, J);
     double* YJ = Y + (o->xsuper[J - 1] - 1);
-    scipy_dtrsm_("L", "U", "T", "N", &w, &nrhs, &one, o->cells[J][0].nzval, &w, YJ, &n, 1, 1, 1, 1);
+    scipy_dtrsm_("L", "U", "T", o->ldl ? "U" : "N", &w, &nrhs, &one, o->cells[J][0].nzval, &w, YJ, &n, 1, 1, 1, 1);
     for (int k = 1; k < o->ncells[J]; ++k) {
       cell_t* c = &o->cells[J][k];
       for (int b = 0; b < c->nblocks; ++b) {
@@ -272,6 +333,14 @@ int orc_solve(orc_t* o, double* B, int nrhs, int64_t ldb) {
       }
     }
   }
+  /* LDL^T: Y <- D^-1 Y (scale_contrib) */
+  if (o->ldl)
+    for (int J = 1; J <= o->nsuper; ++J) {
+      int w = width(o, J);
+      const double* dg = o->cells[J][0].nzval;
+      for (int c = 0; c < nrhs; ++c)
+        for (int j = 0; j < w; ++j) Y[(size_t)(o->xsuper[J - 1] - 1 + j) + (size_t)c * n] /= dg[(size_t)j * w + j];
+    }
   /* backward: X_J -= L_KJ^T X_K[rows] ; X_J <- L_JJ^-T X_J */
   for (int J = o->nsuper; J >= 1; --J) {
     int w = width(o, J);
@@ -284,7 +353,7 @@ int orc_solve(orc_t* o, double* B, int nrhs, int64_t ldb) {
                      Y + (c->blk_first[b] - 1), &n, &one, XJ, &n, 1, 1);
       }
     }
-    scipy_dtrsm_("L", "U", "N", "N", &w, &nrhs, &one, o->cells[J][0].nzval, &w, XJ, &n, 1, 1, 1, 1);
+    scipy_dtrsm_("L", "U", "N", o->ldl ? "U" : "N", &w, &nrhs, &one, o->cells[J][0].nzval, &w, XJ, &n, 1, 1, 1, 1);
   }
   for (int c = 0; c < nrhs; ++c)
     for (int i = 0; i < n; ++i) B[i + c * ldb] = Y[(size_t)(o->invp[i] - 1) + (size_t)c * n];

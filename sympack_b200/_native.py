@@ -25,6 +25,7 @@ SPB_ERR_NOT_CONVERGED = -8
 
 ORDERINGS = {"MMD": 0, "NATURAL": 1, "USER": 2, "RCM": 3, "AMD": 4}
 PRECISIONS = {"FP64": 0, "FP32_IR": 1}
+DECOMPOSITIONS = {"LL": 0, "LDL": 1}
 
 
 class spb_options(C.Structure):
@@ -46,6 +47,8 @@ class spb_options(C.Structure):
         ("plan_small_max_w", C.c_int),
         ("plan_big_tile_rows", C.c_int),
         ("fp32_engine", C.c_int),
+        ("decomposition", C.c_int),
+        ("plan_outer_nb", C.c_int),
     ]
 
 
@@ -97,7 +100,7 @@ SIGNATURES = [
     ("spb_symbolic_batch", C.c_int, [_P, C.c_int32, _I32P, C.c_int32, _I64P, _I32P]),
     ("spb_symbolic_from", C.c_int, [_P, _P]),
     ("spb_predict_device_bytes", C.c_int, [_P, C.c_int32, C.c_int32, C.POINTER(C.c_int64)]),
-    ("spb_replan", C.c_int, [_P, C.c_int32, C.c_int32]),
+    ("spb_replan", C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32]),
     ("spb_get_solve_trace", C.c_int, [_P, C.c_int32, C.POINTER(C.c_uint64), C.c_int64, C.POINTER(C.c_int64)]),
     ("spb_distribute", C.c_int, [_P, _DP]),
     ("spb_distribute_device", C.c_int, [_P, _P]),

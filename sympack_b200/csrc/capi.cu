@@ -43,8 +43,10 @@ struct spb_handle {
   std::vector<int32_t> level_off;  // level l covers dlevel_sn[level_off[l] .. level_off[l+1])
   // device buffers
   bool fp32 = false;        // precision form: FP32 factor + FP64 refinement
+  bool ldl = false;         // LDL^T decomposition (FP64): dL unit L, dW = L D
   size_t elem = 8;          // bytes per factor entry
   void* dL = nullptr;
+  double* dW = nullptr;
   spb::SnMeta* dmeta = nullptr;
   int32_t* drows = nullptr;
   int32_t* dsupm = nullptr;
@@ -144,6 +146,7 @@ void release_device(spb_handle* h) {
   h->allocs.clear();
   h->device_bytes = 0;
   h->dL = nullptr;
+  h->dW = nullptr;
   h->dX = h->dB = h->dR = h->dD = h->dXo = nullptr;
   h->d_rowseg = nullptr;
   h->dtrace = nullptr;
@@ -162,6 +165,8 @@ spb::dev::FactorArgs factor_args(spb_handle* h) {
   a.rel = h->drel;
   a.fp32 = h->fp32;
   a.engine = h->opt.fp32_engine;
+  a.ldl = h->ldl;
+  a.W = h->dW;
   return a;
 }
 
@@ -356,7 +361,8 @@ void enqueue_solve(spb_handle* h, int nrhs) {
   for (int c0 = 0; c0 < nrhs; c0 += 64) {
     cudaMemsetAsync(h->dsync, 0, sizeof(int32_t) * spb::solve_sync_ints(P), h->stream);
     spb::dev::PSolveArgs a{};
-    a.L = h->dL;
+    // LDL^T: the forward sweep solves with L D (diagonal D), the backward one with unit L
+    a.L = h->ldl ? (void*)h->dW : h->dL;
     a.fp32 = h->fp32;
     a.meta = h->dmeta;
     a.rows = h->drows;
@@ -379,6 +385,7 @@ void enqueue_solve(spb_handle* h, int nrhs) {
     if (h->profiling) cudaEventRecord(h->events[e0], h->stream);
     spb::dev::launch_solve_persistent(h->stream, a, true);
     if (h->profiling) cudaEventRecord(h->events[e0 + 1], h->stream);
+    a.L = h->dL;
     a.tasks = h->dbwd;
     a.ntasks = (int)P.bwd_tasks.size();
     a.counter = h->dsync + 1;
@@ -512,6 +519,7 @@ void spb_default_options(spb_options* o) {
   o->ir_tolerance = 1e-12;
   o->ir_max_iter = 30;
   o->verbose = 0;
+  o->decomposition = SPB_DECOMPOSITION_LL;
 }
 
 int spb_create(const spb_options* opt, spb_handle** out) {
@@ -522,7 +530,9 @@ int spb_create(const spb_options* opt, spb_handle** out) {
   if (opt) h->opt = *opt;
   else spb_default_options(&h->opt);
   if (h->opt.ordering < 0 || h->opt.ordering > 4 || h->opt.precision < 0 || h->opt.precision > 1 ||
-      h->opt.fp32_engine < 0 || h->opt.fp32_engine > 2) {
+      h->opt.fp32_engine < 0 || h->opt.fp32_engine > 2 || h->opt.decomposition < 0 || h->opt.decomposition > 1 ||
+      h->opt.plan_outer_nb < 0 || h->opt.plan_outer_nb > 4096 || h->opt.plan_outer_nb % 64 ||
+      (h->opt.decomposition == SPB_DECOMPOSITION_LDL && h->opt.precision != SPB_PRECISION_FP64)) {
     delete h;
     return SPB_ERR_INVALID;
   }
@@ -600,6 +610,7 @@ spb::PlanParams plan_params_of(const spb_options& o) {
   spb::PlanParams pp;
   if (o.plan_small_max_w > 0) pp.small_max_w = o.plan_small_max_w;
   if (o.plan_big_tile_rows > 0) pp.big_tile_rows = o.plan_big_tile_rows;
+  if (o.plan_outer_nb > 0) pp.outer_nb = o.plan_outer_nb;
   return pp;
 }
 
@@ -630,11 +641,12 @@ int64_t predict_bytes(const spb_handle* h, bool fp32, int nrhs) {
   const int64_t n = h->sym.n, ns = P.nsuper;
   auto b = [](int64_t count, size_t size) { return std::max<int64_t>(count, 1) * (int64_t)size; };
   int64_t t = b(P.arena_elems, fp32 ? sizeof(float) : sizeof(double));
+  if (h->opt.decomposition == SPB_DECOMPOSITION_LDL) t += b(P.arena_elems, sizeof(double));
   t += b(P.meta.size(), sizeof(spb::SnMeta)) + b(P.rows.size(), 4) + b(P.supmember0.size(), 4);
   t += b(P.row_group.size(), 4) + b(P.groups.size(), sizeof(spb::RelGroup)) + b(P.rel.size(), 4);
   t += b(h->amap.size(), 8) + b(h->nnz_a, 8) + b(P.small_items.size(), 4);
   t += b(P.panel_items.size(), sizeof(spb::PanelItem));
-  t += b((int64_t)std::max(1, P.max_diag_slots) * (64 * 64 + 64), 8);
+  t += b((int64_t)std::max(1, P.max_diag_slots) * (int64_t)spb::dev::kDiagSlotDoubles, 8);
   t += b(P.tile_items.size(), sizeof(spb::TileItem)) + b(n, 4) + b(ns, 4);
   t += b(P.fwd_tasks.size(), sizeof(spb::SolveTask)) + b(P.bwd_tasks.size(), sizeof(spb::SolveTask));
   t += b(P.fwd_pending.size(), 4) + b(P.sparent.size(), 4) + b((int64_t)spb::solve_sync_ints(P), 4);
@@ -686,12 +698,14 @@ int install_device(spb_handle* h) {
   for (int i = 0; i < n; ++i) invp0[i] = h->sym.invp[i] - 1;
 
   h->fp32 = h->opt.precision == SPB_PRECISION_FP32_IR;
+  h->ldl = h->opt.decomposition == SPB_DECOMPOSITION_LDL;
   h->elem = h->fp32 ? sizeof(float) : sizeof(double);
   {
     unsigned char* arena = nullptr;
     SPB_CK(h, dalloc(h, &arena, (size_t)P.arena_elems * h->elem));
     h->dL = arena;
   }
+  if (h->ldl) SPB_CK(h, dalloc(h, &h->dW, (size_t)P.arena_elems));
   SPB_CK(h, dalloc(h, &h->dmeta, P.meta.size()));
   SPB_CK(h, dalloc(h, &h->drows, P.rows.size()));
   SPB_CK(h, dalloc(h, &h->dsupm, P.supmember0.size()));
@@ -702,7 +716,7 @@ int install_device(spb_handle* h) {
   SPB_CK(h, dalloc(h, &h->dA, (size_t)h->nnz_a));
   SPB_CK(h, dalloc(h, &h->dsmall, P.small_items.size()));
   SPB_CK(h, dalloc(h, &h->dpanel, P.panel_items.size()));
-  SPB_CK(h, dalloc(h, &h->dwinv, (size_t)std::max(1, P.max_diag_slots) * (64 * 64 + 64)));
+  SPB_CK(h, dalloc(h, &h->dwinv, (size_t)std::max(1, P.max_diag_slots) * spb::dev::kDiagSlotDoubles));
   SPB_CK(h, dalloc(h, &h->dtiles, P.tile_items.size()));
   SPB_CK(h, dalloc(h, &h->dinvp0, invp0.size()));
   SPB_CK(h, dalloc(h, &h->dlevel_sn, lsn.size()));
@@ -848,13 +862,15 @@ int spb_predict_device_bytes(const spb_handle* h, int32_t precision, int32_t nrh
   return SPB_OK;
 }
 
-int spb_replan(spb_handle* h, int32_t small_max_w, int32_t big_tile_rows) {
+int spb_replan(spb_handle* h, int32_t small_max_w, int32_t big_tile_rows, int32_t outer_nb) {
   if (check_handle(h)) return SPB_ERR_INVALID;
   if (!h->have_symbolic) return fail(h, SPB_ERR_STATE, "replan: no symbolic analysis");
-  if (small_max_w < 0 || small_max_w > 64 || big_tile_rows < 0)
-    return fail(h, SPB_ERR_INVALID, "replan: small_max_w must be in [0, 64], big_tile_rows >= 0");
+  if (small_max_w < 0 || small_max_w > 64 || big_tile_rows < 0 || outer_nb < 0 || outer_nb > 4096 || outer_nb % 64)
+    return fail(h, SPB_ERR_INVALID,
+                "replan: small_max_w must be in [0, 64], big_tile_rows >= 0, outer_nb a multiple of 64 in [0, 4096]");
   h->opt.plan_small_max_w = small_max_w;
   h->opt.plan_big_tile_rows = big_tile_rows;
+  h->opt.plan_outer_nb = outer_nb;
   if (h->device >= 0) {
     SPB_CK(h, cudaSetDevice(h->device));
     release_device(h);
@@ -868,7 +884,7 @@ int spb_symbolic_batch(spb_handle* h, int32_t nsys, const int32_t* sys_offsets, 
   if (check_handle(h)) return SPB_ERR_INVALID;
   if (nsys <= 0 || !sys_offsets) return fail(h, SPB_ERR_INVALID, "symbolic_batch: no systems");
   if (h->opt.ordering == SPB_ORDERING_USER)
-    return fail(h, SPB_ERR_INVALID, "symbolic_batch: USER ordering is per matrix; use MMD or NATURAL");
+    return fail(h, SPB_ERR_INVALID, "symbolic_batch: USER ordering is per matrix; use MMD, AMD, RCM or NATURAL");
   int rc = begin_symbolic(h, n, colptr, rowind);
   if (rc) return rc;
   if (sys_offsets[0] != 0 || sys_offsets[nsys] != n) return fail(h, SPB_ERR_INVALID, "symbolic_batch: bad offsets");
@@ -922,6 +938,7 @@ int spb_symbolic_batch(spb_handle* h, int32_t nsys, const int32_t* sys_offsets, 
 static int distribute_common(spb_handle* h) {
   const spb::Plan& P = h->plan;
   SPB_CK(h, cudaMemsetAsync(h->dL, 0, (size_t)P.arena_elems * h->elem, h->stream));
+  if (h->ldl) SPB_CK(h, cudaMemsetAsync(h->dW, 0, (size_t)P.arena_elems * sizeof(double), h->stream));
   SPB_CK(h, cudaMemsetAsync(h->dstatus, 0, sizeof(Status), h->stream));
   if (h->profiling) {
     SPB_CK(h, ensure_events(h, 2));
@@ -999,8 +1016,11 @@ int spb_factorize(spb_handle* h) {
   h->factored = true;
   if (st.code == 1) {
     char msg[128];
-    snprintf(msg, sizeof msg, "Matrix is not HPD: non-positive pivot in supernode %d, column %d", st.supernode + 1,
-             st.column + 1);
+    if (h->ldl)
+      snprintf(msg, sizeof msg, "LDL^T: zero pivot in supernode %d, column %d", st.supernode + 1, st.column + 1);
+    else
+      snprintf(msg, sizeof msg, "Matrix is not HPD: non-positive pivot in supernode %d, column %d", st.supernode + 1,
+               st.column + 1);
     return fail(h, SPB_ERR_NOT_SPD, msg);
   }
   if (st.code != 0) return fail(h, SPB_ERR_STRUCTURE, "factorize: update row missing from target structure");
@@ -1187,10 +1207,18 @@ int spb_get_factor(spb_handle* h, double* out) {
   } else {
     SPB_CK(h, cudaMemcpy(arena.data(), h->dL, P.arena_elems * sizeof(double), cudaMemcpyDeviceToHost));
   }
+  std::vector<double> warena;  // LDL^T: D from the diagonal of L D
+  if (h->ldl) {
+    warena.resize(P.arena_elems);
+    SPB_CK(h, cudaMemcpy(warena.data(), h->dW, P.arena_elems * sizeof(double), cudaMemcpyDeviceToHost));
+  }
   int64_t pos = 0;
   for (const auto& m : P.meta) {
     for (int c = 0; c < m.w; ++c)
-      for (int r = 0; r < m.h; ++r) out[pos + r + (int64_t)c * m.h] = (r < c) ? 0.0 : arena[m.off + r + (int64_t)c * m.ld];
+      for (int r = 0; r < m.h; ++r) {
+        const int64_t at = m.off + r + (int64_t)c * m.ld;
+        out[pos + r + (int64_t)c * m.h] = (r < c) ? 0.0 : (r == c && h->ldl) ? warena[at] : arena[at];
+      }
     pos += (int64_t)m.h * m.w;
   }
   return SPB_OK;
@@ -1346,7 +1374,7 @@ extern "C" int spb_solve_device_noalloc(spb_handle* h, const double* d_rhs, doub
     // counters must start at zero; the array keeps whatever the last call left
     SPB_CK(h, cudaMemsetAsync(sync, 0, sizeof(int32_t) * spb::solve_sync_ints(P), h->stream));
     spb::dev::PSolveArgs a{};
-    a.L = h->dL;
+    a.L = h->ldl ? (void*)h->dW : h->dL;  // LDL^T: forward with L D, backward with unit L
     a.fp32 = h->fp32;
     a.meta = h->dmeta;
     a.rows = h->drows;
@@ -1365,6 +1393,7 @@ extern "C" int spb_solve_device_noalloc(spb_handle* h, const double* d_rhs, doub
     a.blkdone = sync + 2 + ns;
     a.upd = sync + 2 + 3 * (size_t)ns;
     spb::dev::launch_solve_persistent(h->stream, a, true);
+    a.L = h->dL;
     a.tasks = h->dbwd;
     a.ntasks = (int)P.bwd_tasks.size();
     a.counter = sync + 1;

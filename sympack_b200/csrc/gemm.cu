@@ -140,6 +140,7 @@ __global__ void __launch_bounds__(kDThreads, 1) k_gemm_dmma(FactorArgs a, const 
   const TileItem it = items[blockIdx.x];
   const SnMeta m = a.meta[it.s];
   const double* g = static_cast<const double*>(a.L) + m.off;
+  const double* gb = a.ldl ? a.W + m.off : g;  // second operand: L, or L D for LDL^T
   const int64_t ld = m.ld;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int wm = warp & 1, wn = warp >> 1;  // 2 x 4 warps, 64 x 32 each
@@ -158,7 +159,7 @@ __global__ void __launch_bounds__(kDThreads, 1) k_gemm_dmma(FactorArgs a, const 
       bool aok = kok && r < it.mrows;
       bool bok = kok && r < it.ncols;
       cp_async8(As + col * kDLds + r, aok ? g + it.a_row0 + r + coff : g, aok ? 8 : 0);
-      cp_async8(Bs + col * kDLds + r, bok ? g + it.b_row0 + r + coff : g, bok ? 8 : 0);
+      cp_async8(Bs + col * kDLds + r, bok ? gb + it.b_row0 + r + coff : gb, bok ? 8 : 0);
     }
   };
 
@@ -233,6 +234,8 @@ __global__ void __launch_bounds__(256) k_gemm_simt(FactorArgs a, const TileItem*
   const TileItem it = items[blockIdx.x];
   const SnMeta m = a.meta[it.s];
   const T* g = static_cast<const T*>(a.L) + m.off;
+  // second operand: L, or L D for LDL^T (FP64 only, so W is read only when T is double)
+  const T* gb = a.ldl ? reinterpret_cast<const T*>(a.W + m.off) : g;
   const int64_t ld = m.ld;
   const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
   T acc[4][4];
@@ -246,7 +249,7 @@ __global__ void __launch_bounds__(256) k_gemm_simt(FactorArgs a, const TileItem*
       int e = tid + 256 * q, kq = e >> 6, r = e & 63, k = kk + kq;
       const int64_t col = (int64_t)(it.k0 + k) * ld;
       As[kq][r] = (r < it.mrows && k < it.kn) ? g[it.a_row0 + r + col] : T(0);
-      Bs[kq][r] = (r < it.ncols && k < it.kn) ? g[it.b_row0 + r + col] : T(0);
+      Bs[kq][r] = (r < it.ncols && k < it.kn) ? gb[it.b_row0 + r + col] : T(0);
     }
     __syncthreads();
 #pragma unroll

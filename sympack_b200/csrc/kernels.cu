@@ -7,6 +7,10 @@
 //   forward_update / forward_update_contrib   1486-1643
 //   back_update / _tri_solve / back_update_contrib   1645-1797
 // on a column-major panel per supernode instead of row-major cells.
+// LDL^T (blockCellLDL_t, 2D.hpp:1802-2465): Potrf_LDL of the diagonal block
+// (lapack.hpp:206-560, no pivoting, a zero pivot is reported), unit TRSM then
+// scaling by 1/D (2D.hpp:2118-2137), updates with L D as the second operand
+// (computeDLT, 2D.hpp:2140-2160).
 #include <cfloat>
 #include <climits>
 #include <cstdio>
@@ -52,6 +56,33 @@ __device__ void panel_cholesky_smem(double* P, int h, int w, int ldp, Status* st
   }
 }
 
+// LDL^T counterpart: the w x w top block becomes unit L_II with D on its diagonal,
+// the rows below L_KI = A_KI L_II^-T D^-1.  Column k's trailing update uses the
+// column before it is scaled (A_ij -= A_ik A_jk / d_k).  A zero pivot is reported
+// (status 1) and replaced by 1 so that the factorization runs to its end.
+__device__ void panel_ldl_smem(double* P, int h, int w, int ldp, Status* status, int s, int fc) {
+  const int tid = threadIdx.x, nthr = blockDim.x;
+  const int warp = tid >> 5, lane = tid & 31, nw = nthr >> 5;
+  for (int k = 0; k < w; ++k) {
+    if (tid == 0) {
+      const double d = P[k + k * ldp];
+      if (!(fabs(d) > 0.0)) {
+        if (status) report(status, 1, s, fc + k);
+        P[k + k * ldp] = 1.0;
+      }
+    }
+    __syncthreads();
+    const double dinv = 1.0 / P[k + k * ldp];
+    for (int j = k + 1 + warp; j < w; j += nw) {
+      const double ljk = P[j + k * ldp] * dinv;
+      for (int i = j + lane; i < h; i += 32) P[i + j * ldp] -= P[i + k * ldp] * ljk;
+    }
+    __syncthreads();
+    for (int i = k + 1 + tid; i < h; i += nthr) P[i + k * ldp] *= dinv;
+    __syncthreads();
+  }
+}
+
 template <class T>
 __global__ void k_assemble(T* __restrict__ L, const int64_t* __restrict__ dst, const double* __restrict__ vals,
                            int64_t nnz) {
@@ -71,6 +102,17 @@ __global__ void __launch_bounds__(128) k_factor_small(FactorArgs a, const int32_
     P[idx] = (double)g[r + (int64_t)c * m.ld];
   }
   __syncthreads();
+  if (a.ldl) {
+    panel_ldl_smem(P, h, w, h, a.status, s, m.fc);
+    double* gw = a.W + m.off;
+    for (int idx = threadIdx.x; idx < h * w; idx += blockDim.x) {
+      const int c = idx / h, r = idx - c * h;
+      const double v = P[idx], d = P[c + c * h];
+      g[r + (int64_t)c * m.ld] = (T)(r == c ? 1.0 : v);
+      gw[r + (int64_t)c * m.ld] = r == c ? d : (r > c ? v * d : 0.0);
+    }
+    return;
+  }
   panel_cholesky_smem(P, h, w, h, a.status, s, m.fc);
   for (int idx = threadIdx.x; idx < h * w; idx += blockDim.x) {
     int c = idx / h, r = idx - c * h;
@@ -94,7 +136,9 @@ constexpr int kThreads = 256;  // threads of the POTRF and TRSM kernels
 // thread's 16 global accesses are in flight together: the kernel sits on the
 // critical path of every wide supernode and is latency-bound.
 constexpr int kDL = kNB + 1;  // padded leading dimension in shared memory
-constexpr size_t kSlot = (size_t)kNB * kNB + kNB;  // scratch slot: factored block (FP64) + 1/L_kk
+// scratch slot: factored block (FP64), 1/L_kk, and (LDL^T) 1/D_kk
+constexpr size_t kSlot = kDiagSlotDoubles;
+static_assert(kSlot >= (size_t)kNB * kNB + 2 * kNB, "slot layout");
 constexpr int kPiece = 8;
 
 template <class T>
@@ -206,6 +250,84 @@ __global__ void __launch_bounds__(kThreads, 1) k_potrf_diag(FactorArgs a, const 
   }
 }
 
+// LDL^T of one 64-column diagonal block [c0, c0+nb) (one CTA per item), right-looking
+// column by column in shared memory (Potf2_LDL, lapack.hpp:206-270, on the lower
+// triangle): for column k, d = A_kk; every A_ij (k < j <= i) loses A_ik A_jk / d;
+// then column k is divided by d.  L takes the unit block, W the block times D (its
+// diagonal is D), the scratch slot the unit block, 1 in place of 1/L_kk (the TRSM of
+// the rows below then computes R L11^-T, which is W's rows) and 1/D_kk.
+template <class T>
+__global__ void __launch_bounds__(kThreads, 1) k_ldl_diag(FactorArgs a, const PanelItem* __restrict__ items,
+                                                       double* __restrict__ winv) {
+  __shared__ double D[kNB * kDL];
+  __shared__ double Dk[kNB];
+  const PanelItem it = items[blockIdx.x];
+  const SnMeta m = a.meta[it.s];
+  T* g = static_cast<T*>(a.L) + m.off;
+  const int nb = it.nb, c0 = it.c0;
+  const int64_t ld = m.ld;
+  const int tid = threadIdx.x;
+  {
+    double v[kNB * kNB / kThreads];
+#pragma unroll
+    for (int q = 0; q < kNB * kNB / kThreads; ++q) {
+      const int idx = tid + q * kThreads, c = idx / kNB, r = idx - c * kNB;
+      v[q] = (r < nb && c < nb && r >= c) ? (double)g[(c0 + r) + (int64_t)(c0 + c) * ld] : (r == c ? 1.0 : 0.0);
+    }
+#pragma unroll
+    for (int q = 0; q < kNB * kNB / kThreads; ++q) {
+      const int idx = tid + q * kThreads, c = idx / kNB, r = idx - c * kNB;
+      D[r + c * kDL] = v[q];
+    }
+  }
+  __syncthreads();
+  const int urow = tid & 63, ugrp = tid >> 6;
+#pragma unroll 1
+  for (int k = 0; k < kNB; ++k) {
+    double d = D[k + k * kDL];
+    if (!(fabs(d) > 0.0)) {
+      if (tid == 0 && k < nb) report(a.status, 1, it.s, m.fc + c0 + k);
+      d = 1.0;
+    }
+    const double dinv = 1.0 / d;
+    if (urow > k) {  // row urow, columns k+1+ugrp, +4, ... up to the diagonal
+      const double aik = D[urow + k * kDL];
+      for (int j = k + 1 + ugrp; j <= urow; j += 4) D[urow + j * kDL] -= aik * (D[j + k * kDL] * dinv);
+    }
+    __syncthreads();
+    if (tid < kNB) {
+      if (tid > k) D[tid + k * kDL] *= dinv;
+      if (tid == k) {
+        D[k + k * kDL] = 1.0;
+        Dk[k] = d;
+      }
+    }
+    __syncthreads();
+  }
+  double* gw = a.W + m.off;
+#pragma unroll
+  for (int q = 0; q < kNB * kNB / kThreads; ++q) {
+    const int idx = tid + q * kThreads, c = idx / kNB, r = idx - c * kNB;
+    if (r < nb && c < nb && r >= c) {
+      const double l = D[r + c * kDL];
+      g[(c0 + r) + (int64_t)(c0 + c) * ld] = (T)l;
+      gw[(c0 + r) + (int64_t)(c0 + c) * ld] = r == c ? Dk[c] : l * Dk[c];
+    }
+  }
+  if (winv) {
+    double* S = winv + (size_t)it.slot * kSlot;
+#pragma unroll
+    for (int q = 0; q < kNB * kNB / kThreads; ++q) {
+      const int idx = tid + q * kThreads, c = idx / kNB, r = idx - c * kNB;
+      S[idx] = D[r + c * kDL];
+    }
+    if (tid < kNB) {
+      S[kNB * kNB + tid] = 1.0;
+      S[kNB * kNB + kNB + tid] = 1.0 / Dk[tid];
+    }
+  }
+}
+
 // TRSM of one 64-row tile below a factored diagonal block, R <- R L11^-T, by
 // 8-column pieces: each row solves against the 8 x 8 diagonal piece (one
 // thread per row), then the remaining columns of the tile are updated with the
@@ -279,6 +401,20 @@ __global__ void __launch_bounds__(kThreads, 2) k_trsm_rows(FactorArgs a, const P
     }
     __syncthreads();
   }
+  if (a.ldl) {  // R is W's rows (R L11^-T with unit L11); L's rows are R D^-1
+    const double* dinv = W + kNB * kNB + kNB;
+    double* gw = a.W + m.off;
+#pragma unroll
+    for (int q = 0; q < kNB * kNB / kThreads; ++q) {
+      const int idx = tid + q * kThreads, k = idx / kNB, r = idx - k * kNB;
+      if (r < rows && k < nb) {
+        const double v = R[r + k * kDL];
+        g[(it.row0 + r) + (int64_t)(c0 + k) * ld] = (T)(v * dinv[k]);
+        gw[(it.row0 + r) + (int64_t)(c0 + k) * ld] = v;
+      }
+    }
+    return;
+  }
 #pragma unroll
   for (int q = 0; q < kNB * kNB / kThreads; ++q) {
     const int idx = tid + q * kThreads, k = idx / kNB, r = idx - k * kNB;
@@ -338,7 +474,8 @@ void launch_factor_small(cudaStream_t st, const FactorArgs& a, const int32_t* it
 }
 
 void launch_potrf_diag(cudaStream_t st, const FactorArgs& a, const PanelItem* items, int count, double* winv) {
-  if (a.fp32) k_potrf_diag<float><<<count, kThreads, 0, st>>>(a, items, winv);
+  if (a.ldl) k_ldl_diag<double><<<count, kThreads, 0, st>>>(a, items, winv);  // LDL^T is FP64 only
+  else if (a.fp32) k_potrf_diag<float><<<count, kThreads, 0, st>>>(a, items, winv);
   else k_potrf_diag<double><<<count, kThreads, 0, st>>>(a, items, winv);
 }
 

@@ -28,14 +28,23 @@ struct FactorArgs {
   const int32_t* rel;        // positions of update rows in their targets' row lists
   bool fp32;                 // FP32 factor storage (precision form)
   int engine;                // FP32 128 x 128 tiles: 0 tcgen05 per tile, 1 mma.sync, 2 persistent tcgen05
+  // LDL^T (FP64 only): L holds the unit factor (1 on the diagonal) and the working
+  // matrix of unfactored columns; W (same layout) holds L D, so that its diagonal
+  // is D.  Updates are C = L_a (L_b D)^T: the second operand is read from W.
+  bool ldl;
+  double* W;
 };
+
+// Doubles per diagonal-block scratch slot (see launch_potrf_diag).
+constexpr size_t kDiagSlotDoubles = 64 * 64 + 128;
 
 // Must run once per process (per device) before the first launch or capture.
 void init_kernel_attributes();
 void init_gemm_attributes();
 void launch_assemble(cudaStream_t st, void* L, bool fp32, const int64_t* dst, const double* vals, int64_t nnz);
 void launch_factor_small(cudaStream_t st, const FactorArgs& a, const int32_t* items, int count, int smem_bytes);
-// winv: scratch of (diagonal blocks per step) x (64 x 64 + 64) doubles: factored block and 1/L_kk
+// winv: scratch of (diagonal blocks per step) x (64 x 64 + 128) doubles: factored block, 1/L_kk
+// and (LDL^T) 1/D_kk
 void launch_potrf_diag(cudaStream_t st, const FactorArgs& a, const PanelItem* items, int count, double* winv);
 void launch_trsm_rows(cudaStream_t st, const FactorArgs& a, const PanelItem* items, int count, const double* winv);
 // tile 64: FMA tiles (FP64 or FP32); tile 128: tensor-core tiles (FP64 DMMA, or 3xTF32 for FP32)

@@ -123,6 +123,33 @@ def random_graph_spd(n: int, avg_degree: float = 10.0, dominance: float = 1.05, 
     return _dominant(n, lo, hi, off, dominance - 1.0)
 
 
+def quasi_definite_3d(nx: int, ny: int, nz: int, frac_negative: float = 0.3, delta: float = 1e-2, seed: int = 0):
+    """Symmetric indefinite, quasi-definite matrix on a 27-point grid graph: a seeded
+    fraction of the vertices is 'negative'.  Couplings between vertices of the same
+    sign are U[-1, 0) (positive block) or U(0, 1] (negative block), couplings across
+    signs U[-1, 1); the diagonal is sign x (1 + delta) x (sum of |same-sign couplings|),
+    or sign x 1 with none.  So the matrix is [H B^T; B -G] with H, G symmetric
+    diagonally dominant: it has an LDL^T factorization without pivoting in every
+    symmetric ordering, with as many negative pivots as negative vertices.
+    Not positive definite (the Cholesky path rejects it)."""
+    n = nx * ny * nz
+    i, j = _grid_edges((nx, ny, nz), _forward_offsets(3, True))
+    rng = np.random.default_rng(seed)
+    sign = np.where(rng.uniform(size=n) < frac_negative, -1.0, 1.0)
+    same = sign[i] == sign[j]
+    mag = rng.uniform(0.0, 1.0, size=len(i))
+    mag[mag == 0.0] = 0.5
+    off = np.where(same, -sign[i] * mag, rng.uniform(-1.0, 1.0, size=len(i)))
+    absum = np.zeros(n)
+    np.add.at(absum, i[same], mag[same])
+    np.add.at(absum, j[same], mag[same])
+    diag = sign * np.where(absum > 0, absum * (1.0 + delta), 1.0)
+    rows = np.concatenate([np.arange(n), j])
+    cols = np.concatenate([np.arange(n), i])
+    vals = np.concatenate([diag, off])
+    return (n, *_coo_to_lower_csc(n, rows, cols, vals))
+
+
 def config_matrix(name: str, **kw):
     """Named workloads: 'lap2d_64' (n=4096), 'lap3d_60' (n=216,000, shift 1e-3),
     'st27_80' (n=512,000, delta from kw), plus scaled-down variants 'lap3d_<k>', 'st27_<k>'."""

@@ -91,6 +91,8 @@ class symPACKOptions:
     plan_small_max_w: int = 0      # 0 = library default
     plan_big_tile_rows: int = 0    # 0 = library default
     fp32_engine: str = "tcgen05"   # FP32_IR update tiles: "tcgen05", "mma.sync", "tcgen05-persistent"
+    decomposition: str = "LL"      # "LL" (Cholesky) or "LDL" (L D L^T, FP64), the driver's -fact
+    plan_outer_nb: int = 0         # columns per outer block of wide panels (0 = library default 256)
 
     def to_c(self) -> N.spb_options:
         if self.orderingStr not in N.ORDERINGS:
@@ -112,10 +114,14 @@ class symPACKOptions:
         o.verbose = self.verbose
         o.plan_small_max_w = self.plan_small_max_w
         o.plan_big_tile_rows = self.plan_big_tile_rows
+        o.plan_outer_nb = self.plan_outer_nb
         engines = {"tcgen05": 0, "mma.sync": 1, "tcgen05-persistent": 2}
         if self.fp32_engine not in engines:
             raise ValueError(f"unknown fp32_engine {self.fp32_engine!r}")
         o.fp32_engine = engines[self.fp32_engine]
+        if self.decomposition not in N.DECOMPOSITIONS:
+            raise ValueError(f"unknown decomposition {self.decomposition!r} (LL or LDL)")
+        o.decomposition = N.DECOMPOSITIONS[self.decomposition]
         return o
 
 
@@ -251,10 +257,11 @@ class symPACKMatrix2D:
         _raise(self._lib.spb_predict_device_bytes(h, prec, int(nrhs), C.byref(out)), "PredictDeviceBytes", h)
         return int(out.value)
 
-    def Replan(self, small_max_w: int = 0, big_tile_rows: int = 0) -> None:
-        """Rebuild the device plan with other tile shapes; values must be distributed again."""
+    def Replan(self, small_max_w: int = 0, big_tile_rows: int = 0, outer_nb: int = 0) -> None:
+        """Rebuild the device plan with other tile shapes (0 = library default); values
+        must be distributed again."""
         h = self._need()
-        _raise(self._lib.spb_replan(h, int(small_max_w), int(big_tile_rows)), "Replan", h)
+        _raise(self._lib.spb_replan(h, int(small_max_w), int(big_tile_rows), int(outer_nb)), "Replan", h)
 
     def DistributeMatrix(self, A: DistSparseMatrix) -> None:
         h = self._need()

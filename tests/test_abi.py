@@ -65,6 +65,33 @@ def test_fp32_engine_option_is_validated():
         symPACKMatrix2D().Init(symPACKOptions(device=-1, fp32_engine="wmma"))
 
 
+def test_decomposition_option_is_validated():
+    from sympack_b200 import symPACKMatrix2D, symPACKOptions
+    for dec in ("LL", "LDL"):
+        M = symPACKMatrix2D()
+        M.Init(symPACKOptions(device=-1, decomposition=dec))
+        M.close()
+    with pytest.raises(ValueError):
+        symPACKMatrix2D().Init(symPACKOptions(device=-1, decomposition="LU"))
+    with pytest.raises(ValueError):  # LDL^T runs in FP64 only
+        symPACKMatrix2D().Init(symPACKOptions(device=-1, decomposition="LDL", precision="FP32_IR"))
+
+
+def test_ldl_footprint_adds_the_scaled_copy():
+    import numpy as np
+    from sympack_b200 import DistSparseMatrix, generators as G, symPACKMatrix2D, symPACKOptions
+    n, cp, ri, v = G.laplacian_3d(10, 10, 10, 1e-3)
+    A = DistSparseMatrix.from_lower_csc(n, cp, ri, v)
+    got = {}
+    for dec in ("LL", "LDL"):
+        M = symPACKMatrix2D()
+        M.Init(symPACKOptions(device=-1, decomposition=dec))
+        M.SymbolicFactorization(A)
+        got[dec] = (M.PredictDeviceBytes(nrhs=1), M.info().arena_bytes)
+        M.close()
+    assert got["LDL"][0] - got["LL"][0] == got["LL"][1]  # one more FP64 arena (L D)
+
+
 def test_host_only_analysis_predicts_footprint_and_is_reusable():
     import numpy as np
     from sympack_b200 import DistSparseMatrix, generators as G, symPACKMatrix2D, symPACKOptions

@@ -57,3 +57,23 @@ def test_noalloc_rejects_requests_beyond_its_scratch():
                                       too_many, n)
     assert rc == N.SPB_ERR_INVALID
     assert "exceeds" in lib.spb_last_error(M._h).decode()
+
+
+def test_noalloc_solve_with_ldl_factor():
+    """LDL^T handles solve forward with L D and backward with unit L, here too."""
+    import torch
+    n, cp, ri, v = G.quasi_definite_3d(12, 12, 12, 0.3, 1e-2, seed=8)
+    A = DistSparseMatrix.from_lower_csc(n, cp, ri, v)
+    M = symPACKMatrix2D()
+    M.Init(symPACKOptions(device=0, decomposition="LDL"))
+    M.SymbolicFactorization(A)
+    M.DistributeMatrix(A)
+    M.Factorize()
+    lib = N.load()
+    B = torch.from_numpy(np.random.default_rng(2).standard_normal((4, n))).cuda()
+    X_ref, X = torch.empty_like(B), torch.full_like(B, float("nan"))
+    assert lib.spb_solve_device(M._h, C.c_void_p(B.data_ptr()), C.c_void_p(X_ref.data_ptr()), 4, n) == 0
+    rc = lib.spb_solve_device_noalloc(M._h, C.c_void_p(B.data_ptr()), C.c_void_p(X.data_ptr()), 4, n)
+    assert rc == 0, lib.spb_last_error(M._h).decode()
+    ref, new = X_ref.cpu().numpy(), X.cpu().numpy()
+    assert np.max(np.abs(new - ref)) <= TOL * np.max(np.abs(ref))
