@@ -88,6 +88,10 @@ typedef struct spb_options {
   int decomposition;       /* SPB_DECOMPOSITION_* (symPACKOptions::decomposition, Types.hpp:97,119) */
   int plan_outer_nb;       /* columns per outer block of a wide panel: its trailing columns are
                               updated once per outer block (0 = default 256; multiple of 64, <= 4096) */
+  int plan_dense_min_w;    /* narrowest root supernode (no off-diagonal rows, alone at the top of the
+                              tree) whose solves of <= 4 right-hand sides run in one thread-block
+                              cluster (0 = default: never, < 0 = never) */
+  int plan_solve_chunk;    /* column blocks per forward off-diagonal solve task (0 = default 16) */
 } spb_options;
 
 typedef struct spb_info {
@@ -107,6 +111,9 @@ typedef struct spb_info {
   int32_t ir_iterations;   /* refinement steps of the last solve */
   int32_t factor_launches; /* kernels in the factorization graph */
   double backward_error;   /* componentwise-free backward error of the last solve, if computed */
+  int32_t dense_root_width; /* columns of the root solved in one thread-block cluster when a solve
+                               has <= 4 right-hand sides (0 = none): one more launch per sweep */
+  int32_t pad_;
 } spb_info;
 
 void spb_default_options(spb_options* opt);

@@ -49,6 +49,8 @@ class spb_options(C.Structure):
         ("fp32_engine", C.c_int),
         ("decomposition", C.c_int),
         ("plan_outer_nb", C.c_int),
+        ("plan_dense_min_w", C.c_int),
+        ("plan_solve_chunk", C.c_int),
     ]
 
 
@@ -70,6 +72,8 @@ class spb_info(C.Structure):
         ("ir_iterations", C.c_int32),
         ("factor_launches", C.c_int32),
         ("backward_error", C.c_double),
+        ("dense_root_width", C.c_int32),
+        ("pad_", C.c_int32),
     ]
 
 

@@ -358,6 +358,8 @@ int ensure_rhs_capacity(spb_handle* h, int nrhs) {
 void enqueue_solve(spb_handle* h, int nrhs) {
   const spb::Plan& P = h->plan;
   const int ns = P.nsuper;
+  // per-pass events of a profiled solve (every caller, the refinement loop included)
+  const bool prof = h->profiling && ensure_events(h, 4 * (size_t)((nrhs + 63) / 64)) == cudaSuccess;
   for (int c0 = 0; c0 < nrhs; c0 += 64) {
     cudaMemsetAsync(h->dsync, 0, sizeof(int32_t) * spb::solve_sync_ints(P), h->stream);
     spb::dev::PSolveArgs a{};
@@ -376,25 +378,32 @@ void enqueue_solve(spb_handle* h, int nrhs) {
     a.status = h->dstatus;
     a.spin_limit = h->wait_limit;
     const size_t e0 = 4 * (size_t)(c0 / 64);
+    // dense root in one cluster: the persistent sweeps skip its tasks (the last forward
+    // ones, the first backward ones)
+    const bool dense = P.dense_root >= 0 && spb::dev::dense_solve_available(a.nrhs);
+    const int dfw = dense ? P.dense_fwd_tasks : 0, dbw = dense ? P.dense_bwd_tasks : 0;
     a.tasks = h->dfwd;
-    a.ntasks = (int)P.fwd_tasks.size();
+    a.ntasks = (int)P.fwd_tasks.size() - dfw;
     a.counter = h->dsync;
     a.blkdone = h->dsync + 2 + ns;
     a.upd = h->dsync + 2 + 3 * (size_t)ns;
-    a.trace = h->profiling ? h->dtrace : nullptr;
-    if (h->profiling) cudaEventRecord(h->events[e0], h->stream);
+    a.chunk = P.solve_chunk;
+    a.trace = prof ? h->dtrace : nullptr;
+    if (prof) cudaEventRecord(h->events[e0], h->stream);
     spb::dev::launch_solve_persistent(h->stream, a, true);
-    if (h->profiling) cudaEventRecord(h->events[e0 + 1], h->stream);
+    if (dense) spb::dev::launch_solve_dense(h->stream, a, P.dense_root, true);
+    if (prof) cudaEventRecord(h->events[e0 + 1], h->stream);
     a.L = h->dL;
-    a.tasks = h->dbwd;
-    a.ntasks = (int)P.bwd_tasks.size();
+    a.tasks = h->dbwd + dbw;
+    a.ntasks = (int)P.bwd_tasks.size() - dbw;
     a.counter = h->dsync + 1;
     a.blkdone = h->dsync + 2 + 2 * ns;
     a.upd = h->dsync + 2 + 3 * (size_t)ns + P.nblk_total;
-    a.trace = h->profiling && h->dtrace ? h->dtrace + 4 * P.fwd_tasks.size() : nullptr;
-    if (h->profiling) cudaEventRecord(h->events[e0 + 2], h->stream);
+    a.trace = prof && h->dtrace ? h->dtrace + 4 * (P.fwd_tasks.size() + dbw) : nullptr;
+    if (prof) cudaEventRecord(h->events[e0 + 2], h->stream);
+    if (dense) spb::dev::launch_solve_dense(h->stream, a, P.dense_root, false);
     spb::dev::launch_solve_persistent(h->stream, a, false);
-    if (h->profiling) cudaEventRecord(h->events[e0 + 3], h->stream);
+    if (prof) cudaEventRecord(h->events[e0 + 3], h->stream);
   }
 }
 
@@ -412,8 +421,9 @@ int collect_solve_profile(spb_handle* h, int nrhs) {
     h->prof.ms[SPB_KIND_SOLVE_BACKWARD] += b;
     h->prof.bytes[SPB_KIND_SOLVE_FORWARD] += h->plan.solve_sweep_bytes + rhs_bytes;
     h->prof.bytes[SPB_KIND_SOLVE_BACKWARD] += h->plan.solve_sweep_bytes + rhs_bytes;
-    h->prof.launches[SPB_KIND_SOLVE_FORWARD] += 1;
-    h->prof.launches[SPB_KIND_SOLVE_BACKWARD] += 1;
+    const int dense = h->plan.dense_root >= 0 && spb::dev::dense_solve_available(std::min(64, nrhs - c0));
+    h->prof.launches[SPB_KIND_SOLVE_FORWARD] += 1 + dense;
+    h->prof.launches[SPB_KIND_SOLVE_BACKWARD] += 1 + dense;
   }
   return SPB_OK;
 }
@@ -611,6 +621,8 @@ spb::PlanParams plan_params_of(const spb_options& o) {
   if (o.plan_small_max_w > 0) pp.small_max_w = o.plan_small_max_w;
   if (o.plan_big_tile_rows > 0) pp.big_tile_rows = o.plan_big_tile_rows;
   if (o.plan_outer_nb > 0) pp.outer_nb = o.plan_outer_nb;
+  if (o.plan_dense_min_w != 0) pp.dense_min_w = o.plan_dense_min_w < 0 ? 0 : o.plan_dense_min_w;
+  if (o.plan_solve_chunk > 0) pp.solve_chunk = o.plan_solve_chunk;
   return pp;
 }
 
@@ -1121,6 +1133,8 @@ int spb_get_info(spb_handle* h, spb_info* info) {
   info->ncells = (int32_t)h->cells.cells.size();
   info->nblocks = (int32_t)h->cells.block_first_row.size();
   info->factor_launches = (int32_t)P.steps.size();
+  info->dense_root_width =
+      P.dense_root >= 0 && h->device >= 0 && spb::dev::dense_solve_available(1) ? P.meta[P.dense_root].w : 0;
   info->ir_iterations = h->ir_iterations;
   info->backward_error = h->backward_error;
   return SPB_OK;
@@ -1387,18 +1401,23 @@ extern "C" int spb_solve_device_noalloc(spb_handle* h, const double* d_rhs, doub
     a.arrived = sync + 2;
     a.status = h->dstatus;
     a.spin_limit = h->wait_limit;
+    const bool dense = P.dense_root >= 0 && spb::dev::dense_solve_available(a.nrhs);
+    const int dfw = dense ? P.dense_fwd_tasks : 0, dbw = dense ? P.dense_bwd_tasks : 0;
     a.tasks = h->dfwd;
-    a.ntasks = (int)P.fwd_tasks.size();
+    a.ntasks = (int)P.fwd_tasks.size() - dfw;
     a.counter = sync;
     a.blkdone = sync + 2 + ns;
     a.upd = sync + 2 + 3 * (size_t)ns;
+    a.chunk = P.solve_chunk;
     spb::dev::launch_solve_persistent(h->stream, a, true);
+    if (dense) spb::dev::launch_solve_dense(h->stream, a, P.dense_root, true);
     a.L = h->dL;
-    a.tasks = h->dbwd;
-    a.ntasks = (int)P.bwd_tasks.size();
+    a.tasks = h->dbwd + dbw;
+    a.ntasks = (int)P.bwd_tasks.size() - dbw;
     a.counter = sync + 1;
     a.blkdone = sync + 2 + 2 * ns;
     a.upd = sync + 2 + 3 * (size_t)ns + P.nblk_total;
+    if (dense) spb::dev::launch_solve_dense(h->stream, a, P.dense_root, false);
     spb::dev::launch_solve_persistent(h->stream, a, false);
   }
   spb::dev::launch_permute_out(h->stream, d_x, ld, X, n, h->dinvp0, n, nrhs);

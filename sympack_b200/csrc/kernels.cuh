@@ -53,8 +53,8 @@ void launch_gemm(cudaStream_t st, const FactorArgs& a, const TileItem* items, in
 // Solves work on the permuted right-hand sides X (n x nrhs, column-major, leading dimension ldx).
 
 // Persistent sweeps (one launch each).  counter, arrived, blkdone and upd must
-// be zero at launch; expected[s] is the number of forward off-diagonal tiles
-// that write rows of supernode s.
+// be zero at launch; expected[s] is the number of forward off-diagonal (tile, column
+// block) tasks that write rows of supernode s.
 struct PSolveArgs {
   const void* L;     // factor arena (double, or float when fp32)
   bool fp32;
@@ -72,12 +72,18 @@ struct PSolveArgs {
   int32_t* arrived;
   int32_t* blkdone;
   int32_t* upd;      // per 64-column block: updates landed (meta.boff + block)
+  int chunk;         // column blocks per forward off-diagonal task (Plan::solve_chunk)
   Status* status;
   long long spin_limit;  // polls (about 128 ns apart) before a wait gives up
   unsigned long long* trace;  // optional, 4 per task: grabbed, dependencies met, done (ns), s << 8 | kind
 };
 void init_solve_attributes();
 void launch_solve_persistent(cudaStream_t st, const PSolveArgs& a, bool forward);
+// Dense root (Plan::dense_root) solved by one thread-block cluster, for nrhs <= 4:
+// forward after the persistent forward sweep (which skips the root's tasks), backward
+// before the persistent backward sweep (it marks the root done in a.blkdone).
+bool dense_solve_available(int nrhs);
+void launch_solve_dense(cudaStream_t st, const PSolveArgs& a, int s, bool forward);
 
 // Precision form (FP64 refinement): gather CSR values, residual r = b - A x,
 // per-column max |v| (out zeroed by the caller), max row sum of |A|, x += d.

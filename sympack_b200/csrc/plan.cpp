@@ -241,35 +241,69 @@ Plan build_plan(const Symbolic& sym, const PlanParams& prm) {
   // right-looking by 64-column blocks: a finished diagonal block releases its
   // updates of every later block at once, so the per-supernode critical path
   // is one block solve plus one block update per block.
+  // The supernodes of a level advance together: tasks are dealt block by block across
+  // the level (block 0 of every supernode, then block 1, ...), so sibling chains run side
+  // by side instead of one supernode's tasks filling every CTA before the next starts.
+  // Forward off-diagonal work is one task per (row tile, chunk of solve_chunk column
+  // blocks), dealt right after the chunk's last diagonal block: it barely waits and never
+  // holds a CTA across a supernode's whole chain, and its atomic scatter into the
+  // ancestors' rows happens once per chunk.
+  const int chunk = std::max(1, prm.solve_chunk);
+  P.solve_chunk = chunk;
   P.fwd_pending.assign(ns, 0);
-  for (int L = 0; L < H; ++L)
-    for (int s : P.level_sn[L]) {
-      const SnMeta& m = P.meta[s];
-      const int nblk = (m.w + 63) / 64, noff = (m.h - m.w + 63) / 64;
-      for (int i = 0; i < nblk; ++i) {
+  for (int L = 0; L < H; ++L) {
+    int maxblk = 0;
+    for (int s : P.level_sn[L]) maxblk = std::max(maxblk, (P.meta[s].w + 63) / 64);
+    for (int i = 0; i < maxblk; ++i)
+      for (int s : P.level_sn[L]) {
+        const SnMeta& m = P.meta[s];
+        const int nblk = (m.w + 63) / 64, noff = (m.h - m.w + 63) / 64;
+        if (i >= nblk) continue;
         P.fwd_tasks.push_back(SolveTask{s, 0, i, i});
         for (int t = i + 2; t < nblk; ++t) P.fwd_tasks.push_back(SolveTask{s, 1, i, t});
+        if ((i + 1) % chunk == 0 || i == nblk - 1)
+          for (int u = 0; u < noff; ++u) P.fwd_tasks.push_back(SolveTask{s, 2, i / chunk * chunk, u});
       }
+    for (int s : P.level_sn[L]) {
+      const SnMeta& m = P.meta[s];
+      const int nblk = (m.w + 63) / 64, noff = (m.h - m.w + 63) / 64, nchunk = (nblk + chunk - 1) / chunk;
       for (int u = 0; u < noff; ++u) {
-        P.fwd_tasks.push_back(SolveTask{s, 2, 0, u});
         int r0 = m.w + 64 * u, r1 = std::min(m.h, r0 + 64), last = -1;
         for (int r = r0; r < r1; ++r) {
           int t = P.supmember0[P.rows[m.lidx + r]];
-          if (t != last) P.fwd_pending[t]++;
+          if (t != last) P.fwd_pending[t] += nchunk;  // one arrival per chunk
           last = t;
         }
       }
     }
-  for (int L = H - 1; L >= 0; --L)
-    for (int s : P.level_sn[L]) {
-      const SnMeta& m = P.meta[s];
-      const int nblk = (m.w + 63) / 64, noff = (m.h - m.w + 63) / 64;
-      for (int u = 0; u < noff; ++u) P.bwd_tasks.push_back(SolveTask{s, 3, 0, u});
-      for (int t = nblk - 1; t >= 0; --t) {
+  }
+  for (int L = H - 1; L >= 0; --L) {
+    int maxblk = 0;
+    for (int s : P.level_sn[L]) maxblk = std::max(maxblk, (P.meta[s].w + 63) / 64);
+    for (int j = 0; j < maxblk; ++j)
+      for (int s : P.level_sn[L]) {
+        const SnMeta& m = P.meta[s];
+        const int nblk = (m.w + 63) / 64, noff = (m.h - m.w + 63) / 64;
+        if (j >= nblk) continue;
+        if (j == 0)
+          for (int u = 0; u < noff; ++u) P.bwd_tasks.push_back(SolveTask{s, 3, 0, u});
+        const int t = nblk - 1 - j;
         P.bwd_tasks.push_back(SolveTask{s, 0, t, t});
         for (int u = 0; u + 2 <= t; ++u) P.bwd_tasks.push_back(SolveTask{s, 1, t, u});
       }
+  }
+  if (prm.dense_min_w > 0 && H > 0 && P.level_sn[H - 1].size() == 1) {
+    const int s = P.level_sn[H - 1][0];
+    const SnMeta& m = P.meta[s];
+    if (m.h == m.w && m.w >= prm.dense_min_w) {
+      int32_t nf = 0, nbw = 0;
+      while (nf < (int32_t)P.fwd_tasks.size() && P.fwd_tasks[P.fwd_tasks.size() - 1 - nf].s == s) ++nf;
+      while (nbw < (int32_t)P.bwd_tasks.size() && P.bwd_tasks[nbw].s == s) ++nbw;
+      P.dense_root = s;
+      P.dense_fwd_tasks = nf;
+      P.dense_bwd_tasks = nbw;
     }
+  }
   return P;
 }
 

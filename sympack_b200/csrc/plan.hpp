@@ -89,7 +89,8 @@ struct PanelItem {
 //   forward  kind 0  D(t):    X_t <- L_tt^-1 X_t once every update into block t
 //                             has landed, then X_{t+1} -= L_{t+1,t} X_t
 //            kind 1  U(i, t): X_t -= L_ti X_i                 (t >= i + 2, after D(i))
-//            kind 2  O(u):    X[rows of tile u] -= sum_i L_ui X_i, scattered to the ancestors
+//            kind 2  O(i0, u): X[rows of tile u] -= sum_i L_ui X_i over a chunk of column blocks
+//                             from i0, scattered to the ancestors (after the chunk's last D)
 //   backward kind 3  W(u):    X_t -= L_ut^T X[rows of tile u] for every block t
 //                             (ancestor rows, final once the parent is done)
 //            kind 0  B(t):    X_t <- L_tt^-T X_t once every update into block t
@@ -144,6 +145,13 @@ struct Plan {
   std::vector<SolveTask> fwd_tasks, bwd_tasks;
   std::vector<int32_t> fwd_pending;
   int32_t nblk_total = 0;  // 64-column blocks over all supernodes (per-block solve counters)
+  // Dense root: the only supernode of the top level, with no off-diagonal rows and at
+  // least PlanParams::dense_min_w columns, is solved by one thread-block cluster
+  // (few right-hand sides); its tasks are the last dense_fwd_tasks forward tasks and the
+  // first dense_bwd_tasks backward tasks, which the persistent sweeps then skip.
+  int32_t dense_root = -1;
+  int32_t dense_fwd_tasks = 0, dense_bwd_tasks = 0;
+  int32_t solve_chunk = 16;  // column blocks per forward off-diagonal task O(i0, u): blocks i0 .. i0 + chunk - 1
   // algorithmic bytes of one sweep: every panel element read once
   double solve_sweep_bytes = 0.0;
 };
@@ -155,6 +163,9 @@ struct PlanParams {
   int nb = 64;                   // column block of the blocked panel factorization
   int outer_nb = 256;            // outer block: the trailing columns are updated once per outer block
   int big_tile_rows = 128;       // products with at least this many rows use 128 x 128 tensor-core tiles
+  int dense_min_w = 0;           // narrowest root solved by the cluster kernel (0 = never; measured
+                                 // slower than the persistent sweep so far, kept as an option)
+  int solve_chunk = 16;          // column blocks per forward off-diagonal solve task
 };
 
 Plan build_plan(const Symbolic& s, const PlanParams& p = PlanParams());

@@ -121,10 +121,12 @@ __device__ __forceinline__ void stage_x(double* B, const double* X, int64_t ldx,
 namespace {
 
 // X[x0 + i, c] (+/-)= sum_k A[i + k*lda] * B[k + c*kT] straight into global X with
-// atomics (i < m, c < nr, k < kk); A column-major with leading dimension lda.
+// atomics (i < m, c < nr, k < kk); A column-major with leading dimension lda.  With
+// rows, output i goes to X row x0 + rows[i] instead.
 template <bool kTrans>
 __device__ __forceinline__ void block_gemv_atomic(double* X, int64_t ldx, int x0, const double* A, int lda,
-                                                  const double* B, int m, int kk, int nr, double sign) {
+                                                  const double* B, int m, int kk, int nr, double sign,
+                                                  const int32_t* rows = nullptr) {
   if (m * nr * 4 <= kThreads) {  // few outputs (one or two right-hand sides): 4 threads per output
     const int idx = threadIdx.x >> 2, part = threadIdx.x & 3;
     const int c = idx / max(m, 1), i = idx - c * m;
@@ -137,7 +139,7 @@ __device__ __forceinline__ void block_gemv_atomic(double* X, int64_t ldx, int x0
     }
     s += __shfl_xor_sync(0xffffffffu, s, 1);
     s += __shfl_xor_sync(0xffffffffu, s, 2);
-    if (idx < m * nr && part == 0) atomicAdd(X + x0 + i + c * ldx, sign * s);
+    if (idx < m * nr && part == 0) atomicAdd(X + x0 + (rows ? rows[i] : i) + c * ldx, sign * s);
     return;
   }
   for (int idx = threadIdx.x; idx < m * nr; idx += kThreads) {
@@ -147,7 +149,7 @@ __device__ __forceinline__ void block_gemv_atomic(double* X, int64_t ldx, int x0
       for (int k = 0; k < kk; ++k) s = fma(A[k + i * lda], B[k + c * kT], s);
     else
       for (int k = 0; k < kk; ++k) s = fma(A[i + k * lda], B[k + c * kT], s);
-    atomicAdd(X + x0 + i + c * ldx, sign * s);
+    atomicAdd(X + x0 + (rows ? rows[i] : i) + c * ldx, sign * s);
   }
 }
 
@@ -280,13 +282,14 @@ __global__ void __launch_bounds__(kThreads) k_solve_forward(PSolveArgs a) {
       }
       signal(a.upd + m.boff + t);
     } else {
-      // O(u): off-diagonal rows, Y_K[rows] -= L_KJ Y_J accumulated over the column blocks
-      const int u = task.t, r0 = m.w + u * kT, bu = min(kT, m.h - r0);
-      const int nblk = (m.w + kT - 1) / kT;
+      // O(i0, u): off-diagonal rows, Y_K[rows] -= L_KJ Y_J over the column blocks of a
+      // chunk, accumulated, then scattered into the ancestors' rows
+      const int i0 = task.i, u = task.t, r0 = m.w + u * kT, bu = min(kT, m.h - r0);
+      const int i1 = min((m.w + kT - 1) / kT, i0 + a.chunk);
       for (int idx = threadIdx.x; idx < kT * nr; idx += kThreads) acc[idx] = 0.0;
-      for (int i = 0; i < nblk; ++i) {
+      for (int i = i0; i < i1; ++i) {
         const int bi = min(kT, m.w - i * kT);
-        stage_block(Ab, P, ld, r0, bu, i * kT, bi);
+        stage_block(Ab, P, ld, r0, bu, i * kT, bi);  // L is final: load before waiting
         if (!wait_geq(a.blkdone + s, i + 1, a.status, s, &sh_ok, a.spin_limit)) return;
         stage_x(Bx, a.X, a.ldx, m.fc + i * kT, nullptr, bi, nr);
         __syncthreads();
@@ -393,7 +396,257 @@ __global__ void __launch_bounds__(kThreads) k_solve_backward(PSolveArgs a) {
   }
 }
 
+// ---- dense root solve: one thread-block cluster ----------------------------------
+// The root supernode of a nested-dissection tree is a dense w x w lower triangle (the
+// 27-point 80^3 stencil's is 21,146 wide), and a sweep over it is a chain of w/64
+// diagonal-block solves.  Through global counters each link costs several us; inside
+// one cluster it is a barrier.cluster round and a distributed-shared-memory read.
+// Block b (64 columns) belongs to cluster rank b % C.  Step t of the forward sweep:
+// every CTA copies x_t from its owner's shared memory; the owner of block t+1 first
+// subtracts L_{t+1,t} x_t from its rows, solves its diagonal block and publishes
+// x_{t+1}; then every CTA subtracts L_it x_t from the other blocks it owns.  The
+// backward sweep mirrors it with L^T.  X rows of a block are only ever touched by its
+// owner (no atomics); L blocks stream through a cp.async ring ahead of use (L is final,
+// so the loads never wait for the chain).  Few right-hand sides only: the updates are
+// FP64 FMA work on C SMs.
+constexpr int kDenseRhs = 4;       // right-hand sides per launch (the persistent path takes more)
+constexpr int kDenseStages = 4;    // L blocks in flight per CTA
+
+__device__ __forceinline__ void cluster_arrive() { asm volatile("barrier.cluster.arrive.release.aligned;\n" ::: "memory"); }
+__device__ __forceinline__ void cluster_wait() { asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory"); }
+__device__ __forceinline__ unsigned cluster_rank() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ unsigned cluster_size() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(r));
+  return r;
+}
+// Generic address of the same shared-memory location in cluster CTA `rank`.
+__device__ __forceinline__ const double* map_rank(const double* p, unsigned rank) {
+  unsigned long long r;
+  asm volatile("mapa.u64 %0, %1, %2;" : "=l"(r) : "l"(p), "r"(rank));
+  return reinterpret_cast<const double*>(r);
+}
+__device__ __forceinline__ void cp_async16_zfill(void* smem, const void* gmem, bool ok) {
+  unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(gmem), "r"(ok ? 16 : 0));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+// 64 x 64 block of T in shared memory, column-major in 16-byte chunks of kC rows; chunk q
+// of column k sits at chunk position q ^ (k & 7), so that a warp reading one row across
+// 32 columns, or 16 bytes of 8 columns, hits distinct banks.
+template <class T>
+struct SwzBlock {
+  static constexpr int kC = 16 / (int)sizeof(T);
+  __device__ static __forceinline__ int at(int r, int k) { return k * kT + (((r / kC) ^ (k & 7)) * kC) + r % kC; }
+};
+
+// Dense-sweep item order of one cluster rank: forward, steps t = 0 .. nblk-2 and the
+// owned blocks i > t ascending; backward, steps t = nblk-1 .. 1 and the owned blocks
+// j < t descending.  (blk = -1 once exhausted.)
+template <bool kFwd>
+struct DenseItems {
+  int nblk, C, rho, t, blk;
+  __device__ void first_of_step() {
+    for (;;) {
+      if (kFwd ? t > nblk - 2 : t < 1) {
+        blk = -1;
+        return;
+      }
+      blk = kFwd ? t + 1 + ((rho - (t + 1)) % C + C) % C : t - 1 - (((t - 1) - rho) % C + C) % C;
+      if (kFwd ? blk < nblk : blk >= 0) return;
+      t += kFwd ? 1 : -1;
+    }
+  }
+  __device__ void start(int n, int c, int r) {
+    nblk = n;
+    C = c;
+    rho = r;
+    t = kFwd ? 0 : n - 1;
+    first_of_step();
+  }
+  __device__ void next() {
+    blk += kFwd ? C : -C;
+    if (kFwd ? blk >= nblk : blk < 0) {
+      t += kFwd ? 1 : -1;
+      first_of_step();
+    }
+  }
+};
+
+template <class T, bool kFwd>
+__global__ void __launch_bounds__(kThreads, 1) k_solve_dense(PSolveArgs a, int s) {
+  extern __shared__ __align__(16) unsigned char dsm[];
+  T* ring = reinterpret_cast<T*>(dsm);
+  double* Ad = reinterpret_cast<double*>(dsm + (size_t)kDenseStages * kT * kT * sizeof(T));
+  double* xs = Ad + kT * kPld;              // x_t of the current step (ld kT)
+  double* xpub = xs + kT * kDenseRhs;       // x of this CTA's last solved block (ld kT)
+  double* red = xpub + kT * kDenseRhs;      // 2 x 4 x 64 x kDenseRhs partial sums
+  double* rinv = red + 2 * 4 * kT * kDenseRhs;
+  const SnMeta m = a.meta[s];
+  const T* P = static_cast<const T*>(a.L) + m.off;
+  const int64_t ld = m.ld;
+  const int nblk = (m.w + kT - 1) / kT, nr = a.nrhs;
+  const int C = (int)cluster_size(), rho = (int)cluster_rank(), tid = threadIdx.x;
+  double* X = a.X + m.fc;
+  const int64_t ldx = a.ldx;
+  auto bw = [&](int b) { return min(kT, m.w - b * kT); };
+
+  // L block of item (t, b): forward L_{b,t} (rows of b, columns of t), backward L_{t,b}
+  auto issue = [&](const DenseItems<kFwd>& it, int slot) {
+    T* dst = ring + (size_t)slot * kT * kT;
+    constexpr int kC = SwzBlock<T>::kC, kChunks = kT * kT / kC;
+    const int rb = kFwd ? it.blk : it.t, cb = kFwd ? it.t : it.blk;
+    const int nrow = bw(rb), ncol = bw(cb);
+    for (int e = tid; e < kChunks; e += kThreads) {
+      const int k = e / (kT / kC), q = e - k * (kT / kC), r = q * kC;
+      const bool ok = k < ncol && r < nrow;
+      const T* src = ok ? P + (int64_t)rb * kT + r + (int64_t)(cb * kT + k) * ld : P;
+      cp_async16_zfill(dst + SwzBlock<T>::at(r, k), src, ok);
+    }
+  };
+  // stage diagonal block b (FP64, ld kPld) and its reciprocal diagonal
+  auto stage_diag = [&](int b) {
+    if (b < 0 || b >= nblk) return;
+    stage_block(Ad, P, ld, b * kT, bw(b), b * kT, bw(b));
+    __syncthreads();
+    if (tid < bw(b)) rinv[tid] = 1.0 / Ad[tid * (kPld + 1)];
+    __syncthreads();
+  };
+  // solve diagonal block b in place: xpub <- L_bb^-1 (or ^-T) X_b; X_b <- xpub
+  auto solve_diag = [&](int b) {
+    const int n = bw(b);
+    for (int idx = tid; idx < kT * nr; idx += kThreads) {
+      const int c = idx / kT, r = idx - c * kT;
+      xpub[idx] = r < n ? X[b * kT + r + c * ldx] : 0.0;
+    }
+    __syncthreads();
+    block_trsv<kFwd>(xpub, Ad, rinv, n, nr);
+    __syncthreads();
+    for (int idx = tid; idx < kT * nr; idx += kThreads) {
+      const int c = idx / kT, r = idx - c * kT;
+      if (r < n) X[b * kT + r + c * ldx] = xpub[idx];
+    }
+  };
+
+  DenseItems<kFwd> prod, cons;
+  prod.start(nblk, C, rho);
+  cons.start(nblk, C, rho);
+#pragma unroll 1
+  for (int q = 0; q < kDenseStages - 1; ++q) {
+    if (prod.blk >= 0) {
+      issue(prod, q);
+      prod.next();
+    }
+    cp_async_commit();
+  }
+  int nq = 0;  // items consumed
+  // consume one item: X_blk -= L x_t (forward) or L^T x_t (backward); xs holds x_t
+  auto consume = [&]() {
+    cp_async_wait<kDenseStages - 2>();
+    __syncthreads();
+    if (prod.blk >= 0) {
+      issue(prod, (nq + kDenseStages - 1) % kDenseStages);
+      prod.next();
+    }
+    cp_async_commit();
+    const T* Lb = ring + (size_t)(nq % kDenseStages) * kT * kT;
+    double* rd = red + (size_t)(nq & 1) * 4 * kT * kDenseRhs;
+    const int lane_i = tid & 63, part = tid >> 6;
+    double acc[kDenseRhs];
+#pragma unroll
+    for (int c = 0; c < kDenseRhs; ++c) acc[c] = 0.0;
+    if (kFwd) {  // row lane_i, columns part*16 ..
+#pragma unroll 4
+      for (int kk = 0; kk < 16; ++kk) {
+        const int k = part * 16 + kk;
+        const double l = (double)Lb[SwzBlock<T>::at(lane_i, k)];
+#pragma unroll
+        for (int c = 0; c < kDenseRhs; ++c)
+          if (c < nr) acc[c] = fma(l, xs[k + c * kT], acc[c]);
+      }
+    } else {  // column lane_i, rows part*16 ..
+#pragma unroll 4
+      for (int rr = 0; rr < 16; ++rr) {
+        const int r = part * 16 + rr;
+        const double l = (double)Lb[SwzBlock<T>::at(r, lane_i)];
+#pragma unroll
+        for (int c = 0; c < kDenseRhs; ++c)
+          if (c < nr) acc[c] = fma(l, xs[r + c * kT], acc[c]);
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < kDenseRhs; ++c) rd[(part * kT + lane_i) * kDenseRhs + c] = acc[c];
+    __syncthreads();
+    const int n = bw(cons.blk);
+    if (tid < kT * nr) {
+      const int c = tid / kT, r = tid - c * kT;
+      if (r < n) {
+        const double y = rd[r * kDenseRhs + c] + rd[(kT + r) * kDenseRhs + c] + rd[(2 * kT + r) * kDenseRhs + c] +
+                         rd[(3 * kT + r) * kDenseRhs + c];
+        X[cons.blk * kT + r + c * ldx] -= y;
+      }
+    }
+    ++nq;
+    cons.next();
+  };
+
+  // first block solved without any update: forward block 0, backward block nblk-1
+  const int b0 = kFwd ? 0 : nblk - 1;
+  int mydiag = kFwd ? rho : nblk - 1 - (((nblk - 1) - rho) % C + C) % C;  // next owned diagonal block
+  stage_diag(mydiag);
+  const bool own_first = b0 % C == rho;
+  if (own_first) {
+    solve_diag(b0);
+    mydiag += kFwd ? C : -C;
+  }
+  cluster_arrive();
+  if (own_first) stage_diag(mydiag);
+#pragma unroll 1
+  for (int step = 0; step + 1 < nblk; ++step) {
+    const int t = kFwd ? step : nblk - 1 - step, tn = kFwd ? t + 1 : t - 1;
+    cluster_wait();  // x_t is published
+    {
+      const double* src = map_rank(xpub, (unsigned)(t % C));
+      const int n = bw(t);
+      for (int idx = tid; idx < kT * nr; idx += kThreads) {
+        const int r = idx % kT;
+        xs[idx] = r < n ? src[idx] : 0.0;
+      }
+    }
+    __syncthreads();
+    const bool own_next = tn % C == rho;
+    if (own_next) {
+      consume();  // item (t, tn) is this rank's first item of the step
+      __syncthreads();
+      solve_diag(tn);
+      mydiag += kFwd ? C : -C;
+    }
+    cluster_arrive();  // own_next: x_tn published; all: done reading x_t
+    while (cons.blk >= 0 && cons.t == t) consume();
+    if (own_next) stage_diag(mydiag);  // next owned diagonal block, off the chain
+  }
+  cluster_wait();
+  cp_async_wait<0>();
+  if (!kFwd && rho == 0 && tid == 0) a.blkdone[s] = nblk;  // the root is done for the persistent sweep
+}
+
 int g_solve_grid = 0;
+int g_dense_cluster = 0;  // CTAs per dense-root cluster (0 = unavailable)
+
+template <class T, bool kFwd>
+constexpr size_t dense_smem() {
+  return (size_t)kDenseStages * kT * kT * sizeof(T) +
+         ((size_t)kT * kPld + 2 * kT * kDenseRhs + 2 * 4 * kT * kDenseRhs + kT) * sizeof(double);
+}
 
 }  // namespace
 
@@ -406,6 +659,61 @@ void init_solve_attributes() {
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_solve_forward<double>, kThreads, kSmemBytes);
   g_solve_grid = sms * (per > 0 ? per : 1);
   if (g_solve_grid <= 0) g_solve_grid = 148;
+  // dense-root cluster: 16 CTAs where the GPU can co-schedule them, else 8, else none
+  auto set_dense = [](auto f, size_t smem) {
+    cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(f, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+  };
+  set_dense(k_solve_dense<double, true>, dense_smem<double, true>());
+  set_dense(k_solve_dense<double, false>, dense_smem<double, false>());
+  set_dense(k_solve_dense<float, true>, dense_smem<float, true>());
+  set_dense(k_solve_dense<float, false>, dense_smem<float, false>());
+  g_dense_cluster = 0;
+  for (int c : {16, 8}) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(c);
+    cfg.blockDim = dim3(kThreads);
+    cfg.dynamicSmemBytes = dense_smem<double, true>();
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = c;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int nclusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&nclusters, k_solve_dense<double, true>, &cfg) == cudaSuccess &&
+        nclusters > 0) {
+      g_dense_cluster = c;
+      break;
+    }
+  }
+  cudaGetLastError();  // a refused cluster size is not an error of the handle
+}
+
+bool dense_solve_available(int nrhs) { return g_dense_cluster > 0 && nrhs >= 1 && nrhs <= kDenseRhs; }
+
+void launch_solve_dense(cudaStream_t st, const PSolveArgs& a, int s, bool forward) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(g_dense_cluster);
+  cfg.blockDim = dim3(kThreads);
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = g_dense_cluster;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  if (a.fp32) {
+    cfg.dynamicSmemBytes = forward ? dense_smem<float, true>() : dense_smem<float, false>();
+    if (forward) cudaLaunchKernelEx(&cfg, k_solve_dense<float, true>, a, s);
+    else cudaLaunchKernelEx(&cfg, k_solve_dense<float, false>, a, s);
+  } else {
+    cfg.dynamicSmemBytes = forward ? dense_smem<double, true>() : dense_smem<double, false>();
+    if (forward) cudaLaunchKernelEx(&cfg, k_solve_dense<double, true>, a, s);
+    else cudaLaunchKernelEx(&cfg, k_solve_dense<double, false>, a, s);
+  }
 }
 
 void launch_solve_persistent(cudaStream_t st, const PSolveArgs& a, bool forward) {

@@ -85,3 +85,20 @@ def test_refinement_cap_reports_not_converged():
     with pytest.raises(SymPACKError) as e:
         M.Solve(np.ones(n))
     assert e.value.code == -8  # SPB_ERR_NOT_CONVERGED
+
+
+def test_profiling_turned_on_between_refined_solves():
+    """Profiling switched on after an unprofiled factorization: the refinement's sweeps
+    create their own timing events (regression: they once indexed an empty list)."""
+    n, cp, ri, v = G.stencil27(10, 10, 10, 1e-2, seed=5)
+    A = DistSparseMatrix.from_lower_csc(n, cp, ri, v)
+    M = factor(A, "FP32_IR")
+    b = np.random.default_rng(3).standard_normal((n, 2))
+    M.Solve(b)
+    x0 = M.GetSolution(nrhs=2)
+    M.SetProfiling(True)
+    M.Solve(b)
+    x1 = M.GetSolution(nrhs=2)
+    M.SetProfiling(False)
+    assert backward_error(A, x1, b) <= 1e-12
+    assert np.max(np.abs(x1 - x0)) <= 1e-10 * np.max(np.abs(x0))
