@@ -380,7 +380,7 @@ void enqueue_solve(spb_handle* h, int nrhs) {
     const size_t e0 = 4 * (size_t)(c0 / 64);
     // dense root in one cluster: the persistent sweeps skip its tasks (the last forward
     // ones, the first backward ones)
-    const bool dense = P.dense_root >= 0 && spb::dev::dense_solve_available(a.nrhs);
+    const bool dense = P.dense_root >= 0 && spb::dev::dense_solve_available(a.nrhs, P.meta[P.dense_root].w);
     const int dfw = dense ? P.dense_fwd_tasks : 0, dbw = dense ? P.dense_bwd_tasks : 0;
     a.tasks = h->dfwd;
     a.ntasks = (int)P.fwd_tasks.size() - dfw;
@@ -391,7 +391,7 @@ void enqueue_solve(spb_handle* h, int nrhs) {
     a.trace = prof ? h->dtrace : nullptr;
     if (prof) cudaEventRecord(h->events[e0], h->stream);
     spb::dev::launch_solve_persistent(h->stream, a, true);
-    if (dense) spb::dev::launch_solve_dense(h->stream, a, P.dense_root, true);
+    if (dense) spb::dev::launch_solve_dense(h->stream, a, P.dense_root, P.meta[P.dense_root].w, true);
     if (prof) cudaEventRecord(h->events[e0 + 1], h->stream);
     a.L = h->dL;
     a.tasks = h->dbwd + dbw;
@@ -401,7 +401,7 @@ void enqueue_solve(spb_handle* h, int nrhs) {
     a.upd = h->dsync + 2 + 3 * (size_t)ns + P.nblk_total;
     a.trace = prof && h->dtrace ? h->dtrace + 4 * (P.fwd_tasks.size() + dbw) : nullptr;
     if (prof) cudaEventRecord(h->events[e0 + 2], h->stream);
-    if (dense) spb::dev::launch_solve_dense(h->stream, a, P.dense_root, false);
+    if (dense) spb::dev::launch_solve_dense(h->stream, a, P.dense_root, P.meta[P.dense_root].w, false);
     spb::dev::launch_solve_persistent(h->stream, a, false);
     if (prof) cudaEventRecord(h->events[e0 + 3], h->stream);
   }
@@ -421,7 +421,8 @@ int collect_solve_profile(spb_handle* h, int nrhs) {
     h->prof.ms[SPB_KIND_SOLVE_BACKWARD] += b;
     h->prof.bytes[SPB_KIND_SOLVE_FORWARD] += h->plan.solve_sweep_bytes + rhs_bytes;
     h->prof.bytes[SPB_KIND_SOLVE_BACKWARD] += h->plan.solve_sweep_bytes + rhs_bytes;
-    const int dense = h->plan.dense_root >= 0 && spb::dev::dense_solve_available(std::min(64, nrhs - c0));
+    const int dense = h->plan.dense_root >= 0 &&
+                      spb::dev::dense_solve_available(std::min(64, nrhs - c0), h->plan.meta[h->plan.dense_root].w);
     h->prof.launches[SPB_KIND_SOLVE_FORWARD] += 1 + dense;
     h->prof.launches[SPB_KIND_SOLVE_BACKWARD] += 1 + dense;
   }
@@ -1134,7 +1135,9 @@ int spb_get_info(spb_handle* h, spb_info* info) {
   info->nblocks = (int32_t)h->cells.block_first_row.size();
   info->factor_launches = (int32_t)P.steps.size();
   info->dense_root_width =
-      P.dense_root >= 0 && h->device >= 0 && spb::dev::dense_solve_available(1) ? P.meta[P.dense_root].w : 0;
+      P.dense_root >= 0 && h->device >= 0 && spb::dev::dense_solve_available(1, P.meta[P.dense_root].w)
+          ? P.meta[P.dense_root].w
+          : 0;
   info->ir_iterations = h->ir_iterations;
   info->backward_error = h->backward_error;
   return SPB_OK;
@@ -1401,7 +1404,7 @@ extern "C" int spb_solve_device_noalloc(spb_handle* h, const double* d_rhs, doub
     a.arrived = sync + 2;
     a.status = h->dstatus;
     a.spin_limit = h->wait_limit;
-    const bool dense = P.dense_root >= 0 && spb::dev::dense_solve_available(a.nrhs);
+    const bool dense = P.dense_root >= 0 && spb::dev::dense_solve_available(a.nrhs, P.meta[P.dense_root].w);
     const int dfw = dense ? P.dense_fwd_tasks : 0, dbw = dense ? P.dense_bwd_tasks : 0;
     a.tasks = h->dfwd;
     a.ntasks = (int)P.fwd_tasks.size() - dfw;
@@ -1410,14 +1413,14 @@ extern "C" int spb_solve_device_noalloc(spb_handle* h, const double* d_rhs, doub
     a.upd = sync + 2 + 3 * (size_t)ns;
     a.chunk = P.solve_chunk;
     spb::dev::launch_solve_persistent(h->stream, a, true);
-    if (dense) spb::dev::launch_solve_dense(h->stream, a, P.dense_root, true);
+    if (dense) spb::dev::launch_solve_dense(h->stream, a, P.dense_root, P.meta[P.dense_root].w, true);
     a.L = h->dL;
     a.tasks = h->dbwd + dbw;
     a.ntasks = (int)P.bwd_tasks.size() - dbw;
     a.counter = sync + 1;
     a.blkdone = sync + 2 + 2 * ns;
     a.upd = sync + 2 + 3 * (size_t)ns + P.nblk_total;
-    if (dense) spb::dev::launch_solve_dense(h->stream, a, P.dense_root, false);
+    if (dense) spb::dev::launch_solve_dense(h->stream, a, P.dense_root, P.meta[P.dense_root].w, false);
     spb::dev::launch_solve_persistent(h->stream, a, false);
   }
   spb::dev::launch_permute_out(h->stream, d_x, ld, X, n, h->dinvp0, n, nrhs);

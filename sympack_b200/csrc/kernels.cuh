@@ -82,8 +82,8 @@ void launch_solve_persistent(cudaStream_t st, const PSolveArgs& a, bool forward)
 // Dense root (Plan::dense_root) solved by one thread-block cluster, for nrhs <= 4:
 // forward after the persistent forward sweep (which skips the root's tasks), backward
 // before the persistent backward sweep (it marks the root done in a.blkdone).
-bool dense_solve_available(int nrhs);
-void launch_solve_dense(cudaStream_t st, const PSolveArgs& a, int s, bool forward);
+bool dense_solve_available(int nrhs, int w);  // w: the root's width (its blocks' accumulators fit?)
+void launch_solve_dense(cudaStream_t st, const PSolveArgs& a, int s, int w, bool forward);
 
 // Precision form (FP64 refinement): gather CSR values, residual r = b - A x,
 // per-column max |v| (out zeroed by the caller), max row sum of |A|, x += d.

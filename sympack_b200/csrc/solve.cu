@@ -21,7 +21,12 @@ namespace {
 constexpr int kT = 64;         // rows / columns per task unit
 constexpr int kPld = 65;       // padded leading dimension of the staged L block
 constexpr int kThreads = 256;
-constexpr size_t kSmemBytes = (size_t)(kT * kPld + 2 * kT * kT) * sizeof(double);
+// staged L block (64 x 65), a second 64 x 64 block (X rows or the next L block), and
+// the accumulator of kR right-hand sides; kR = 16 keeps three CTAs per SM
+template <int kR>
+constexpr size_t solve_smem() { return (size_t)(kT * kPld + kT * kT + kT * kR) * sizeof(double); }
+template <int kR>
+constexpr int solve_min_blocks() { return kR <= 16 ? 3 : 2; }
 
 __device__ __forceinline__ void report_status(Status* st, int code, int s, int col) {
   if (atomicCAS(&st->code, 0, code) == 0) {
@@ -219,8 +224,8 @@ __device__ __forceinline__ void signal(int32_t* counter) {
   if (threadIdx.x == 0) red_release(counter, 1);
 }
 
-template <class T>
-__global__ void __launch_bounds__(kThreads) k_solve_forward(PSolveArgs a) {
+template <class T, int kR>
+__global__ void __launch_bounds__(kThreads, solve_min_blocks<kR>()) k_solve_forward(PSolveArgs a) {
   extern __shared__ __align__(16) double sm[];
   double* Ab = sm;                  // staged L block, ld kPld
   double* Bx = sm + kT * kPld;      // staged X rows, ld kT
@@ -317,8 +322,8 @@ __global__ void __launch_bounds__(kThreads) k_solve_forward(PSolveArgs a) {
   }
 }
 
-template <class T>
-__global__ void __launch_bounds__(kThreads) k_solve_backward(PSolveArgs a) {
+template <class T, int kR>
+__global__ void __launch_bounds__(kThreads, solve_min_blocks<kR>()) k_solve_backward(PSolveArgs a) {
   extern __shared__ __align__(16) double sm[];
   double* Ab = sm;
   double* Bx = sm + kT * kPld;
@@ -411,6 +416,7 @@ __global__ void __launch_bounds__(kThreads) k_solve_backward(PSolveArgs a) {
 // FP64 FMA work on C SMs.
 constexpr int kDenseRhs = 4;       // right-hand sides per launch (the persistent path takes more)
 constexpr int kDenseStages = 4;    // L blocks in flight per CTA
+constexpr size_t kDenseSmemMax = 227 * 1024;  // dynamic shared memory one CTA may use
 
 __device__ __forceinline__ void cluster_arrive() { asm volatile("barrier.cluster.arrive.release.aligned;\n" ::: "memory"); }
 __device__ __forceinline__ void cluster_wait() { asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory"); }
@@ -482,23 +488,55 @@ struct DenseItems {
   }
 };
 
+// Shared-memory layout of k_solve_dense (bytes), for `nown` owned blocks of nr right-hand sides.
+template <class T>
+struct DenseSmem {
+  size_t ring, ad, xs, xpub, red, rinv, acc, total;
+  __host__ __device__ DenseSmem(int nown, int nr) {
+    ring = 0;
+    ad = ring + (size_t)kDenseStages * kT * kT * sizeof(T);
+    xs = ad + (size_t)kT * kPld * sizeof(double);
+    xpub = xs + (size_t)kT * kDenseRhs * sizeof(double);
+    red = xpub + (size_t)kT * kDenseRhs * sizeof(double);
+    rinv = red + (size_t)4 * kT * kDenseRhs * sizeof(double);
+    acc = rinv + (size_t)kT * sizeof(double);
+    total = acc + (size_t)nown * kT * nr * sizeof(double);
+  }
+};
+
 template <class T, bool kFwd>
 __global__ void __launch_bounds__(kThreads, 1) k_solve_dense(PSolveArgs a, int s) {
   extern __shared__ __align__(16) unsigned char dsm[];
-  T* ring = reinterpret_cast<T*>(dsm);
-  double* Ad = reinterpret_cast<double*>(dsm + (size_t)kDenseStages * kT * kT * sizeof(T));
-  double* xs = Ad + kT * kPld;              // x_t of the current step (ld kT)
-  double* xpub = xs + kT * kDenseRhs;       // x of this CTA's last solved block (ld kT)
-  double* red = xpub + kT * kDenseRhs;      // 2 x 4 x 64 x kDenseRhs partial sums
-  double* rinv = red + 2 * 4 * kT * kDenseRhs;
   const SnMeta m = a.meta[s];
   const T* P = static_cast<const T*>(a.L) + m.off;
   const int64_t ld = m.ld;
   const int nblk = (m.w + kT - 1) / kT, nr = a.nrhs;
   const int C = (int)cluster_size(), rho = (int)cluster_rank(), tid = threadIdx.x;
+  const int nown = (nblk + C - 1) / C;
+  const DenseSmem<T> lay(nown, nr);
+  T* ring = reinterpret_cast<T*>(dsm + lay.ring);
+  double* Ad = reinterpret_cast<double*>(dsm + lay.ad);
+  double* xs = reinterpret_cast<double*>(dsm + lay.xs);      // x_t of the current step (ld kT)
+  double* xpub = reinterpret_cast<double*>(dsm + lay.xpub);  // x of this CTA's last solved block (ld kT)
+  double* red = reinterpret_cast<double*>(dsm + lay.red);    // 4 x 64 x kDenseRhs partial sums
+  double* rinv = reinterpret_cast<double*>(dsm + lay.rinv);
+  double* accown = reinterpret_cast<double*>(dsm + lay.acc);  // X of the owned blocks, nr x 64 each
   double* X = a.X + m.fc;
   const int64_t ldx = a.ldx;
   auto bw = [&](int b) { return min(kT, m.w - b * kT); };
+  auto acc_of = [&](int b) { return accown + (size_t)(b / C) * kT * nr; };  // b owned: b % C == rho
+
+  // the owned blocks' rows of X, held here until solved
+  for (int lb = 0; lb < nown; ++lb) {
+    const int b = rho + lb * C;
+    if (b >= nblk) break;
+    const int n = bw(b);
+    double* acc = accown + (size_t)lb * kT * nr;
+    for (int idx = tid; idx < kT * nr; idx += kThreads) {
+      const int c = idx / kT, r = idx - c * kT;
+      acc[idx] = r < n ? X[b * kT + r + c * ldx] : 0.0;
+    }
+  }
 
   // L block of item (t, b): forward L_{b,t} (rows of b, columns of t), backward L_{t,b}
   auto issue = [&](const DenseItems<kFwd>& it, int slot) {
@@ -521,19 +559,17 @@ __global__ void __launch_bounds__(kThreads, 1) k_solve_dense(PSolveArgs a, int s
     if (tid < bw(b)) rinv[tid] = 1.0 / Ad[tid * (kPld + 1)];
     __syncthreads();
   };
-  // solve diagonal block b in place: xpub <- L_bb^-1 (or ^-T) X_b; X_b <- xpub
+  // solve owned diagonal block b in place in its accumulator, publish it and store it in X
   auto solve_diag = [&](int b) {
     const int n = bw(b);
-    for (int idx = tid; idx < kT * nr; idx += kThreads) {
-      const int c = idx / kT, r = idx - c * kT;
-      xpub[idx] = r < n ? X[b * kT + r + c * ldx] : 0.0;
-    }
+    double* acc = acc_of(b);
     __syncthreads();
-    block_trsv<kFwd>(xpub, Ad, rinv, n, nr);
+    block_trsv<kFwd>(acc, Ad, rinv, n, nr);
     __syncthreads();
     for (int idx = tid; idx < kT * nr; idx += kThreads) {
       const int c = idx / kT, r = idx - c * kT;
-      if (r < n) X[b * kT + r + c * ldx] = xpub[idx];
+      xpub[idx] = r < n ? acc[idx] : 0.0;
+      if (r < n) X[b * kT + r + c * ldx] = acc[idx];
     }
   };
 
@@ -549,7 +585,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_solve_dense(PSolveArgs a, int s
     cp_async_commit();
   }
   int nq = 0;  // items consumed
-  // consume one item: X_blk -= L x_t (forward) or L^T x_t (backward); xs holds x_t
+  // consume one item: X_blk -= L x_t (forward) or L^T x_t (backward), in the owned
+  // accumulator; xs holds x_t
   auto consume = [&]() {
     cp_async_wait<kDenseStages - 2>();
     __syncthreads();
@@ -559,11 +596,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_solve_dense(PSolveArgs a, int s
     }
     cp_async_commit();
     const T* Lb = ring + (size_t)(nq % kDenseStages) * kT * kT;
-    double* rd = red + (size_t)(nq & 1) * 4 * kT * kDenseRhs;
     const int lane_i = tid & 63, part = tid >> 6;
-    double acc[kDenseRhs];
+    double part_sum[kDenseRhs];
 #pragma unroll
-    for (int c = 0; c < kDenseRhs; ++c) acc[c] = 0.0;
+    for (int c = 0; c < kDenseRhs; ++c) part_sum[c] = 0.0;
     if (kFwd) {  // row lane_i, columns part*16 ..
 #pragma unroll 4
       for (int kk = 0; kk < 16; ++kk) {
@@ -571,7 +607,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_solve_dense(PSolveArgs a, int s
         const double l = (double)Lb[SwzBlock<T>::at(lane_i, k)];
 #pragma unroll
         for (int c = 0; c < kDenseRhs; ++c)
-          if (c < nr) acc[c] = fma(l, xs[k + c * kT], acc[c]);
+          if (c < nr) part_sum[c] = fma(l, xs[k + c * kT], part_sum[c]);
       }
     } else {  // column lane_i, rows part*16 ..
 #pragma unroll 4
@@ -580,20 +616,16 @@ __global__ void __launch_bounds__(kThreads, 1) k_solve_dense(PSolveArgs a, int s
         const double l = (double)Lb[SwzBlock<T>::at(r, lane_i)];
 #pragma unroll
         for (int c = 0; c < kDenseRhs; ++c)
-          if (c < nr) acc[c] = fma(l, xs[r + c * kT], acc[c]);
+          if (c < nr) part_sum[c] = fma(l, xs[r + c * kT], part_sum[c]);
       }
     }
 #pragma unroll
-    for (int c = 0; c < kDenseRhs; ++c) rd[(part * kT + lane_i) * kDenseRhs + c] = acc[c];
+    for (int c = 0; c < kDenseRhs; ++c) red[(part * kT + lane_i) * kDenseRhs + c] = part_sum[c];
     __syncthreads();
-    const int n = bw(cons.blk);
     if (tid < kT * nr) {
       const int c = tid / kT, r = tid - c * kT;
-      if (r < n) {
-        const double y = rd[r * kDenseRhs + c] + rd[(kT + r) * kDenseRhs + c] + rd[(2 * kT + r) * kDenseRhs + c] +
-                         rd[(3 * kT + r) * kDenseRhs + c];
-        X[cons.blk * kT + r + c * ldx] -= y;
-      }
+      acc_of(cons.blk)[r + c * kT] -= red[r * kDenseRhs + c] + red[(kT + r) * kDenseRhs + c] +
+                                      red[(2 * kT + r) * kDenseRhs + c] + red[(3 * kT + r) * kDenseRhs + c];
     }
     ++nq;
     cons.next();
@@ -616,17 +648,12 @@ __global__ void __launch_bounds__(kThreads, 1) k_solve_dense(PSolveArgs a, int s
     cluster_wait();  // x_t is published
     {
       const double* src = map_rank(xpub, (unsigned)(t % C));
-      const int n = bw(t);
-      for (int idx = tid; idx < kT * nr; idx += kThreads) {
-        const int r = idx % kT;
-        xs[idx] = r < n ? src[idx] : 0.0;
-      }
+      for (int idx = tid; idx < kT * nr; idx += kThreads) xs[idx] = src[idx];  // rows past the block are 0
     }
     __syncthreads();
     const bool own_next = tn % C == rho;
     if (own_next) {
       consume();  // item (t, tn) is this rank's first item of the step
-      __syncthreads();
       solve_diag(tn);
       mydiag += kFwd ? C : -C;
     }
@@ -642,38 +669,42 @@ __global__ void __launch_bounds__(kThreads, 1) k_solve_dense(PSolveArgs a, int s
 int g_solve_grid = 0;
 int g_dense_cluster = 0;  // CTAs per dense-root cluster (0 = unavailable)
 
-template <class T, bool kFwd>
-constexpr size_t dense_smem() {
-  return (size_t)kDenseStages * kT * kT * sizeof(T) +
-         ((size_t)kT * kPld + 2 * kT * kDenseRhs + 2 * 4 * kT * kDenseRhs + kT) * sizeof(double);
-}
 
 }  // namespace
 
+int g_solve_grid16 = 0;  // CTAs of the persistent sweeps for <= 16 right-hand sides
+
 void init_solve_attributes() {
-  for (auto f : {k_solve_forward<double>, k_solve_backward<double>, k_solve_forward<float>, k_solve_backward<float>})
-    cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes);
-  int dev = 0, sms = 0, per = 0;
+  for (auto f : {k_solve_forward<double, 64>, k_solve_backward<double, 64>, k_solve_forward<float, 64>,
+                 k_solve_backward<float, 64>})
+    cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)solve_smem<64>());
+  for (auto f : {k_solve_forward<double, 16>, k_solve_backward<double, 16>, k_solve_forward<float, 16>,
+                 k_solve_backward<float, 16>})
+    cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)solve_smem<16>());
+  int dev = 0, sms = 0, per = 0, per16 = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_solve_forward<double>, kThreads, kSmemBytes);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_solve_forward<double, 64>, kThreads, solve_smem<64>());
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per16, k_solve_forward<double, 16>, kThreads, solve_smem<16>());
   g_solve_grid = sms * (per > 0 ? per : 1);
   if (g_solve_grid <= 0) g_solve_grid = 148;
+  g_solve_grid16 = sms * (per16 > 0 ? per16 : 1);
+  if (g_solve_grid16 <= 0) g_solve_grid16 = g_solve_grid;
   // dense-root cluster: 16 CTAs where the GPU can co-schedule them, else 8, else none
   auto set_dense = [](auto f, size_t smem) {
     cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     cudaFuncSetAttribute(f, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
   };
-  set_dense(k_solve_dense<double, true>, dense_smem<double, true>());
-  set_dense(k_solve_dense<double, false>, dense_smem<double, false>());
-  set_dense(k_solve_dense<float, true>, dense_smem<float, true>());
-  set_dense(k_solve_dense<float, false>, dense_smem<float, false>());
+  set_dense(k_solve_dense<double, true>, kDenseSmemMax);
+  set_dense(k_solve_dense<double, false>, kDenseSmemMax);
+  set_dense(k_solve_dense<float, true>, kDenseSmemMax);
+  set_dense(k_solve_dense<float, false>, kDenseSmemMax);
   g_dense_cluster = 0;
   for (int c : {16, 8}) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(c);
     cfg.blockDim = dim3(kThreads);
-    cfg.dynamicSmemBytes = dense_smem<double, true>();
+    cfg.dynamicSmemBytes = kDenseSmemMax;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
     attr[0].val.clusterDim.x = c;
@@ -691,9 +722,14 @@ void init_solve_attributes() {
   cudaGetLastError();  // a refused cluster size is not an error of the handle
 }
 
-bool dense_solve_available(int nrhs) { return g_dense_cluster > 0 && nrhs >= 1 && nrhs <= kDenseRhs; }
+bool dense_solve_available(int nrhs, int w) {
+  if (g_dense_cluster <= 0 || nrhs < 1 || nrhs > kDenseRhs || w <= 0) return false;
+  const int nown = ((w + kT - 1) / kT + g_dense_cluster - 1) / g_dense_cluster;
+  return DenseSmem<double>(nown, nrhs).total <= kDenseSmemMax;
+}
 
-void launch_solve_dense(cudaStream_t st, const PSolveArgs& a, int s, bool forward) {
+void launch_solve_dense(cudaStream_t st, const PSolveArgs& a, int s, int w, bool forward) {
+  const int nown = ((w + kT - 1) / kT + g_dense_cluster - 1) / g_dense_cluster;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(g_dense_cluster);
   cfg.blockDim = dim3(kThreads);
@@ -706,11 +742,11 @@ void launch_solve_dense(cudaStream_t st, const PSolveArgs& a, int s, bool forwar
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   if (a.fp32) {
-    cfg.dynamicSmemBytes = forward ? dense_smem<float, true>() : dense_smem<float, false>();
+    cfg.dynamicSmemBytes = DenseSmem<float>(nown, a.nrhs).total;
     if (forward) cudaLaunchKernelEx(&cfg, k_solve_dense<float, true>, a, s);
     else cudaLaunchKernelEx(&cfg, k_solve_dense<float, false>, a, s);
   } else {
-    cfg.dynamicSmemBytes = forward ? dense_smem<double, true>() : dense_smem<double, false>();
+    cfg.dynamicSmemBytes = DenseSmem<double>(nown, a.nrhs).total;
     if (forward) cudaLaunchKernelEx(&cfg, k_solve_dense<double, true>, a, s);
     else cudaLaunchKernelEx(&cfg, k_solve_dense<double, false>, a, s);
   }
@@ -718,13 +754,27 @@ void launch_solve_dense(cudaStream_t st, const PSolveArgs& a, int s, bool forwar
 
 void launch_solve_persistent(cudaStream_t st, const PSolveArgs& a, bool forward) {
   if (a.ntasks <= 0 || a.spin_limit <= 0) return;
-  int grid = g_solve_grid < a.ntasks ? g_solve_grid : a.ntasks;
+  const bool small = a.nrhs <= 16;
+  const int cap = small ? g_solve_grid16 : g_solve_grid;
+  const int grid = cap < a.ntasks ? cap : a.ntasks;
+  if (small) {
+    const size_t sm = solve_smem<16>();
+    if (a.fp32) {
+      if (forward) k_solve_forward<float, 16><<<grid, kThreads, sm, st>>>(a);
+      else k_solve_backward<float, 16><<<grid, kThreads, sm, st>>>(a);
+    } else {
+      if (forward) k_solve_forward<double, 16><<<grid, kThreads, sm, st>>>(a);
+      else k_solve_backward<double, 16><<<grid, kThreads, sm, st>>>(a);
+    }
+    return;
+  }
+  const size_t sm = solve_smem<64>();
   if (a.fp32) {
-    if (forward) k_solve_forward<float><<<grid, kThreads, kSmemBytes, st>>>(a);
-    else k_solve_backward<float><<<grid, kThreads, kSmemBytes, st>>>(a);
+    if (forward) k_solve_forward<float, 64><<<grid, kThreads, sm, st>>>(a);
+    else k_solve_backward<float, 64><<<grid, kThreads, sm, st>>>(a);
   } else {
-    if (forward) k_solve_forward<double><<<grid, kThreads, kSmemBytes, st>>>(a);
-    else k_solve_backward<double><<<grid, kThreads, kSmemBytes, st>>>(a);
+    if (forward) k_solve_forward<double, 64><<<grid, kThreads, sm, st>>>(a);
+    else k_solve_backward<double, 64><<<grid, kThreads, sm, st>>>(a);
   }
 }
 
