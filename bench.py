@@ -416,6 +416,7 @@ def batching_comparison(torch, dev, stream, count, seed=0, subset=64):
                      "ir_iterations": mi.ir_iterations if prec == "FP32_IR" else 0,
                      "factor_launches": mi.factor_launches, "device_bytes": mi.device_bytes,
                      "autotuned_plan": {"small_max_w": tune["small_max_w"], "big_tile_rows": tune["big_tile_rows"],
+                                        "outer_nb": tune["outer_nb"],
                                         "candidates_ms": {k: round(v * 1e3, 3) for k, v in tune["times"].items()}}}
         M.close()
     T.close()

@@ -124,34 +124,38 @@ constexpr int kNB = 64;
 constexpr int kThreads = 256;  // threads of the POTRF and TRSM kernels
 
 // POTRF of one 64-column diagonal block [c0, c0+nb) of a wide panel (one CTA
-// per item), right-looking by 8-column pieces in shared memory: warp 0 factors
-// the 8 x 8 diagonal piece in registers (lane i holds row i, columns exchanged
-// by shuffles), one thread per row solves the rows below against it, and the
-// trailing lower triangle is updated with the solved piece (thread (row,
-// group) updates columns group, group+4, ... of its row, so the piece's row
-// values stay in registers and the column values are warp broadcasts).  The
-// CTA also copies the factored block (FP64) and 1/L_kk to its scratch slot,
-// from where the TRSM of the rows below reads them.  A block narrower than 64
-// is padded with the identity.  Loads and stores are unrolled so that a
-// thread's 16 global accesses are in flight together: the kernel sits on the
-// critical path of every wide supernode and is latency-bound.
+// per item), right-looking by 8-column pieces in shared memory.  Every thread factors
+// the 8 x 8 diagonal piece itself, in registers, from the same shared-memory values (the
+// same operations in the same order, so every copy is identical): no shuffles and no
+// barrier between the piece and the solve of the rows below, which each thread then
+// does for its own row against its register copy.  The factored pieces go to a side
+// array (other threads may still be reading the unfactored piece) and into the block at
+// the end.  The trailing lower triangle is updated with the solved columns (thread
+// (row, group) updates columns group, group+4, ... of its row).  Two barriers per
+// piece.  The CTA also copies the factored block (FP64) and 1/L_kk to its scratch
+// slot, from where the TRSM of the rows below reads them.  A block narrower than 64 is
+// padded with the identity.  The kernel sits on the critical path of every wide
+// supernode and is latency-bound.
 constexpr int kDL = kNB + 1;  // padded leading dimension in shared memory
 // scratch slot: factored block (FP64), 1/L_kk, and (LDL^T) 1/D_kk
 constexpr size_t kSlot = kDiagSlotDoubles;
 static_assert(kSlot >= (size_t)kNB * kNB + 2 * kNB, "slot layout");
 constexpr int kPiece = 8;
+constexpr int kTri = kPiece * (kPiece + 1) / 2;  // entries of a lower-triangular piece
+__host__ __device__ constexpr int tri(int i, int j) { return i * (i + 1) / 2 + j; }  // i >= j
 
 template <class T>
 __global__ void __launch_bounds__(kThreads, 1) k_potrf_diag(FactorArgs a, const PanelItem* __restrict__ items,
                                                          double* __restrict__ winv) {
   __shared__ double D[kNB * kDL];
-  __shared__ double Rinv[kNB];  // 1 / L_kk
+  __shared__ double Lp[kNB / kPiece][kTri];  // factored diagonal pieces
+  __shared__ double Rinv[kNB];               // 1 / L_kk
   const PanelItem it = items[blockIdx.x];
   const SnMeta m = a.meta[it.s];
   const T* g = static_cast<const T*>(a.L) + m.off;
   const int nb = it.nb, c0 = it.c0;
   const int64_t ld = m.ld;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int tid = threadIdx.x;
   {
     double v[kNB * kNB / kThreads];
 #pragma unroll
@@ -169,37 +173,45 @@ __global__ void __launch_bounds__(kThreads, 1) k_potrf_diag(FactorArgs a, const 
   const int urow = tid & 63, ugrp = tid >> 6;  // update mapping: row kb+8+urow, columns kb+8+ugrp+4t
 #pragma unroll 1
   for (int kb = 0; kb < kNB; kb += kPiece) {
-    if (warp == 0) {
-      double r[kPiece];
+    // the 8 x 8 piece, factored by every thread
+    double l[kTri], rs[kPiece];
 #pragma unroll
-      for (int j = 0; j < kPiece; ++j) r[j] = (lane < kPiece && j <= lane) ? D[kb + lane + (kb + j) * kDL] : 0.0;
+    for (int i = 0; i < kPiece; ++i)
 #pragma unroll
-      for (int k = 0; k < kPiece; ++k) {
-        double dkk = __shfl_sync(0xffffffffu, r[k], k);
-        if (!(dkk > 0.0)) {
-          if (lane == 0 && kb + k < nb) report(a.status, 1, it.s, m.fc + c0 + kb + k);
-          dkk = 1.0;
-        }
-        const double rs = rsqrt(dkk);
-        if (lane == k) r[k] = dkk * rs;
-        else if (lane > k && lane < kPiece) r[k] *= rs;
-        if (lane == 0) Rinv[kb + k] = rs;
+      for (int j = 0; j <= i; ++j) l[tri(i, j)] = D[kb + i + (kb + j) * kDL];
 #pragma unroll
-        for (int j = k + 1; j < kPiece; ++j) {
-          const double ljk = __shfl_sync(0xffffffffu, r[k], j);
-          if (lane >= j && lane < kPiece) r[j] = fma(-r[k], ljk, r[j]);
-        }
+    for (int k = 0; k < kPiece; ++k) {
+      double dkk = l[tri(k, k)];
+      if (!(dkk > 0.0)) {
+        if (tid == 0 && kb + k < nb) report(a.status, 1, it.s, m.fc + c0 + kb + k);
+        dkk = 1.0;
       }
-      if (lane < kPiece) {
+      rs[k] = rsqrt(dkk);
+      l[tri(k, k)] = dkk * rs[k];
 #pragma unroll
-        for (int j = 0; j < kPiece; ++j)
-          if (j <= lane) D[kb + lane + (kb + j) * kDL] = r[j];
-      }
+      for (int i = k + 1; i < kPiece; ++i) l[tri(i, k)] *= rs[k];
+#pragma unroll
+      for (int j = k + 1; j < kPiece; ++j)
+#pragma unroll
+        for (int i = j; i < kPiece; ++i) l[tri(i, j)] = fma(-l[tri(i, k)], l[tri(j, k)], l[tri(i, j)]);
     }
-    __syncthreads();
+    if (tid < kTri) {
+      double mine = 0.0;
+#pragma unroll
+      for (int e = 0; e < kTri; ++e)
+        if (e == tid) mine = l[e];
+      Lp[kb / kPiece][tid] = mine;
+    }
+    if (tid < kPiece) {
+      double mine = 0.0;
+#pragma unroll
+      for (int e = 0; e < kPiece; ++e)
+        if (e == tid) mine = rs[e];
+      Rinv[kb + tid] = mine;
+    }
     const int below = kNB - kb - kPiece;
     if (below == 0) break;
-    if (tid < below) {  // one row per thread: solve against the 8 x 8 piece
+    if (tid < below) {  // one row per thread: solve against the piece
       const int i = kb + kPiece + tid;
       double x[kPiece];
 #pragma unroll
@@ -208,8 +220,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_potrf_diag(FactorArgs a, const 
       for (int k = 0; k < kPiece; ++k) {
         double t = x[k];
 #pragma unroll
-        for (int j = 0; j < k; ++j) t = fma(-x[j], D[kb + k + (kb + j) * kDL], t);
-        x[k] = t * Rinv[kb + k];
+        for (int j = 0; j < k; ++j) t = fma(-x[j], l[tri(k, j)], t);
+        x[k] = t * rs[k];
       }
 #pragma unroll
       for (int j = 0; j < kPiece; ++j) D[i + (kb + j) * kDL] = x[j];
@@ -232,6 +244,16 @@ __global__ void __launch_bounds__(kThreads, 1) k_potrf_diag(FactorArgs a, const 
     }
     __syncthreads();
   }
+  __syncthreads();
+  // factored pieces into the block
+  for (int e = tid; e < (kNB / kPiece) * kTri; e += kThreads) {
+    const int p = e / kTri, q = e - p * kTri;
+    int i = 0;
+    while (tri(i + 1, 0) <= q) ++i;
+    const int j = q - tri(i, 0);
+    D[p * kPiece + i + (p * kPiece + j) * kDL] = Lp[p][q];
+  }
+  __syncthreads();
   T* gw = static_cast<T*>(a.L) + m.off;
 #pragma unroll
   for (int q = 0; q < kNB * kNB / kThreads; ++q) {

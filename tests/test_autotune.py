@@ -18,9 +18,10 @@ class FakeM:
         self.factorizations = 0
         self.calls = []
 
-    def Replan(self, w, r):
+    def Replan(self, w, r, outer=0):
         self.plan = (w, r)
-        self.calls.append(("replan", w, r))
+        self.outer = outer
+        self.calls.append(("replan", w, r, outer))
 
     def DistributeMatrix(self, A):
         self.calls.append(("distribute",))
@@ -29,7 +30,7 @@ class FakeM:
         self.factorizations += 1
         # fastest plan: (32, 128); the others are slower in proportion to their distance
         w, r = self.plan
-        time.sleep(0.002 + 0.0005 * (abs(w - 32) / 16 + abs(r - 128) / 32))
+        time.sleep(0.002 + 0.0005 * (abs(w - 32) / 16 + abs(r - 128) / 32) - 0.0003 * (self.outer == 512))
 
 
 @pytest.fixture
@@ -44,13 +45,13 @@ def test_tune_picks_fastest_and_caches(env):
     path, A = env
     M = FakeM()
     r = autotune.tune(M, A, reps=1)
-    assert (r["small_max_w"], r["big_tile_rows"]) == (32, 128) and not r["cached"]
-    assert M.plan == (32, 128) and M.calls[-1] == ("distribute",)
+    assert (r["small_max_w"], r["big_tile_rows"], r["outer_nb"]) == (32, 128, 512) and not r["cached"]
+    assert M.plan == (32, 128) and M.outer == 512 and M.calls[-1] == ("distribute",)
     table = json.loads(path.read_text())
-    assert len(table) == 1 and len(next(iter(table.values()))["times"]) == len(autotune.CANDIDATES)
+    assert len(table) == 1 and len(next(iter(table.values()))["times"]) == len(autotune.CANDIDATES) + 1
     M2 = FakeM()
     r2 = autotune.tune(M2, A, reps=1)
-    assert r2["cached"] and M2.plan == (32, 128) and M2.factorizations == 0
+    assert r2["cached"] and M2.plan == (32, 128) and M2.outer == 512 and M2.factorizations == 0
 
 
 def test_key_depends_on_structure_options_and_offsets(env):
