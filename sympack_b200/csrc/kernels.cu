@@ -272,16 +272,21 @@ __global__ void __launch_bounds__(kThreads, 1) k_potrf_diag(FactorArgs a, const 
   }
 }
 
-// LDL^T of one 64-column diagonal block [c0, c0+nb) (one CTA per item), right-looking
-// column by column in shared memory (Potf2_LDL, lapack.hpp:206-270, on the lower
-// triangle): for column k, d = A_kk; every A_ij (k < j <= i) loses A_ik A_jk / d;
-// then column k is divided by d.  L takes the unit block, W the block times D (its
-// diagonal is D), the scratch slot the unit block, 1 in place of 1/L_kk (the TRSM of
-// the rows below then computes R L11^-T, which is W's rows) and 1/D_kk.
+// LDL^T of one 64-column diagonal block [c0, c0+nb) (one CTA per item), right-looking by
+// 8-column pieces like k_potrf_diag: every thread factors the piece itself in registers
+// (Potf2_LDL, lapack.hpp:206-270, on the lower triangle: d_k = A_kk, |d_k| > 0 or the
+// pivot is reported as a zero pivot; column k is divided by d_k; A_ij loses L_ik A_jk),
+// then each row below solves w = r L^-T against the unit piece (w is that row of L D)
+// and stores r's L values w / d; the trailing triangle loses W_ik L_jk.  L takes the
+// unit block, W the block times D (its diagonal is D), the scratch slot the unit block,
+// 1 in place of 1/L_kk (the TRSM of the rows below then computes R L11^-T, which is W's
+// rows) and 1/D_kk.
 template <class T>
 __global__ void __launch_bounds__(kThreads, 1) k_ldl_diag(FactorArgs a, const PanelItem* __restrict__ items,
                                                        double* __restrict__ winv) {
   __shared__ double D[kNB * kDL];
+  __shared__ double Lp[kNB / kPiece][kTri];  // factored pieces: unit L below, d on the diagonal
+  __shared__ double Wr[kNB * kPiece];        // rows below the current piece: W = L D, ld kNB
   __shared__ double Dk[kNB];
   const PanelItem it = items[blockIdx.x];
   const SnMeta m = a.meta[it.s];
@@ -305,27 +310,93 @@ __global__ void __launch_bounds__(kThreads, 1) k_ldl_diag(FactorArgs a, const Pa
   __syncthreads();
   const int urow = tid & 63, ugrp = tid >> 6;
 #pragma unroll 1
-  for (int k = 0; k < kNB; ++k) {
-    double d = D[k + k * kDL];
-    if (!(fabs(d) > 0.0)) {
-      if (tid == 0 && k < nb) report(a.status, 1, it.s, m.fc + c0 + k);
-      d = 1.0;
+  for (int kb = 0; kb < kNB; kb += kPiece) {
+    double l[kTri], dinv[kPiece];
+#pragma unroll
+    for (int i = 0; i < kPiece; ++i)
+#pragma unroll
+      for (int j = 0; j <= i; ++j) l[tri(i, j)] = D[kb + i + (kb + j) * kDL];
+#pragma unroll
+    for (int k = 0; k < kPiece; ++k) {
+      double d = l[tri(k, k)];
+      if (!(fabs(d) > 0.0)) {
+        if (tid == 0 && kb + k < nb) report(a.status, 1, it.s, m.fc + c0 + kb + k);
+        d = 1.0;
+        l[tri(k, k)] = 1.0;
+      }
+      dinv[k] = 1.0 / d;
+      double w[kPiece];
+#pragma unroll
+      for (int i = k + 1; i < kPiece; ++i) {
+        w[i] = l[tri(i, k)];
+        l[tri(i, k)] = w[i] * dinv[k];
+      }
+#pragma unroll
+      for (int j = k + 1; j < kPiece; ++j)
+#pragma unroll
+        for (int i = j; i < kPiece; ++i) l[tri(i, j)] = fma(-l[tri(i, k)], w[j], l[tri(i, j)]);
     }
-    const double dinv = 1.0 / d;
-    if (urow > k) {  // row urow, columns k+1+ugrp, +4, ... up to the diagonal
-      const double aik = D[urow + k * kDL];
-      for (int j = k + 1 + ugrp; j <= urow; j += 4) D[urow + j * kDL] -= aik * (D[j + k * kDL] * dinv);
+    if (tid < kTri) {
+      double mine = 0.0;
+#pragma unroll
+      for (int e = 0; e < kTri; ++e)
+        if (e == tid) mine = l[e];
+      Lp[kb / kPiece][tid] = mine;
+    }
+    if (tid < kPiece) {
+      double mine = 0.0;
+#pragma unroll
+      for (int e = 0; e < kPiece; ++e)
+        if (e == tid) mine = l[tri(e, e)];
+      Dk[kb + tid] = mine;
+    }
+    const int below = kNB - kb - kPiece;
+    if (below == 0) break;
+    if (tid < below) {  // one row per thread: w = r L^-T (unit piece), L row = w / d
+      const int i = kb + kPiece + tid;
+      double x[kPiece];
+#pragma unroll
+      for (int j = 0; j < kPiece; ++j) x[j] = D[i + (kb + j) * kDL];
+#pragma unroll
+      for (int k = 0; k < kPiece; ++k) {
+        double t = x[k];
+#pragma unroll
+        for (int j = 0; j < k; ++j) t = fma(-x[j], l[tri(k, j)], t);
+        x[k] = t;
+      }
+#pragma unroll
+      for (int j = 0; j < kPiece; ++j) {
+        Wr[i + j * kNB] = x[j];
+        D[i + (kb + j) * kDL] = x[j] * dinv[j];
+      }
     }
     __syncthreads();
-    if (tid < kNB) {
-      if (tid > k) D[tid + k * kDL] *= dinv;
-      if (tid == k) {
-        D[k + k * kDL] = 1.0;
-        Dk[k] = d;
+    if (urow < below) {
+      const int i = kb + kPiece + urow;
+      double x[kPiece];
+#pragma unroll
+      for (int k = 0; k < kPiece; ++k) x[k] = Wr[i + k * kNB];
+      for (int j = kb + kPiece + ugrp; j <= i; j += 4) {
+        double t0 = D[i + j * kDL], t1 = 0.0;
+#pragma unroll
+        for (int k = 0; k < kPiece; k += 2) {
+          t0 = fma(-x[k], D[j + (kb + k) * kDL], t0);
+          t1 = fma(-x[k + 1], D[j + (kb + k + 1) * kDL], t1);
+        }
+        D[i + j * kDL] = t0 + t1;
       }
     }
     __syncthreads();
   }
+  __syncthreads();
+  for (int e = tid; e < (kNB / kPiece) * kTri; e += kThreads) {
+    const int p = e / kTri, q = e - p * kTri;
+    int i = 0;
+    while (tri(i + 1, 0) <= q) ++i;
+    const int j = q - tri(i, 0);
+    D[p * kPiece + i + (p * kPiece + j) * kDL] = i == j ? 1.0 : Lp[p][q];
+  }
+  __syncthreads();
   double* gw = a.W + m.off;
 #pragma unroll
   for (int q = 0; q < kNB * kNB / kThreads; ++q) {
