@@ -259,6 +259,10 @@ Plan build_plan(const Symbolic& sym, const PlanParams& prm) {
         const SnMeta& m = P.meta[s];
         const int nblk = (m.w + 63) / 64, noff = (m.h - m.w + 63) / 64;
         if (i >= nblk) continue;
+        if (nblk == 1 && noff <= kSolveFusedTiles) {  // the whole supernode in one task
+          P.fwd_tasks.push_back(SolveTask{s, 4, 0, 0});
+          continue;
+        }
         P.fwd_tasks.push_back(SolveTask{s, 0, i, i});
         for (int t = i + 2; t < nblk; ++t) P.fwd_tasks.push_back(SolveTask{s, 1, i, t});
         if ((i + 1) % chunk == 0 || i == nblk - 1)
@@ -285,6 +289,10 @@ Plan build_plan(const Symbolic& sym, const PlanParams& prm) {
         const SnMeta& m = P.meta[s];
         const int nblk = (m.w + 63) / 64, noff = (m.h - m.w + 63) / 64;
         if (j >= nblk) continue;
+        if (nblk == 1 && noff <= kSolveFusedTiles) {
+          P.bwd_tasks.push_back(SolveTask{s, 4, 0, 0});
+          continue;
+        }
         if (j == 0)
           for (int u = 0; u < noff; ++u) P.bwd_tasks.push_back(SolveTask{s, 3, 0, u});
         const int t = nblk - 1 - j;

@@ -91,6 +91,9 @@ struct PanelItem {
 //            kind 1  U(i, t): X_t -= L_ti X_i                 (t >= i + 2, after D(i))
 //            kind 2  O(i0, u): X[rows of tile u] -= sum_i L_ui X_i over a chunk of column blocks
 //                             from i0, scattered to the ancestors (after the chunk's last D)
+//            kind 4  F:       a supernode of one block and at most kSolveFusedTiles off-diagonal
+//                             tiles whole: D(0), then every tile's scatter
+//   backward kind 4  G:       the same supernode whole: every tile's X_0 -= L_u0^T X_u, then B(0)
 //   backward kind 3  W(u):    X_t -= L_ut^T X[rows of tile u] for every block t
 //                             (ancestor rows, final once the parent is done)
 //            kind 0  B(t):    X_t <- L_tt^-T X_t once every update into block t
@@ -155,6 +158,10 @@ struct Plan {
   // algorithmic bytes of one sweep: every panel element read once
   double solve_sweep_bytes = 0.0;
 };
+
+// Supernodes of one 64-column block with at most this many off-diagonal 64-row tiles
+// are one solve task per sweep.
+constexpr int kSolveFusedTiles = 4;
 
 // Tunables of the plan.
 struct PlanParams {

@@ -286,6 +286,41 @@ __global__ void __launch_bounds__(kThreads, solve_min_blocks<kR>()) k_solve_forw
         atomicAdd(a.X + m.fc + r0 + r + c * a.ldx, -acc[r + c * kT]);
       }
       signal(a.upd + m.boff + t);
+    } else if (task.kind == 4) {
+      // F: a one-block supernode whole: X_0 <- L_00^-1 X_0, then every off-diagonal tile
+      // scattered into the ancestors' rows
+      const int w = m.w, noff = (m.h - m.w + kT - 1) / kT;
+      stage_block(Ab, P, ld, 0, w, 0, w);  // L is final: load before waiting
+      __syncthreads();
+      if (threadIdx.x < w) sh_rinv[threadIdx.x] = 1.0 / Ab[threadIdx.x * (kPld + 1)];
+      if (!wait_geq(a.arrived + s, a.expected[s], a.status, s, &sh_ok, a.spin_limit)) return;
+      trace_mark(a, tk, 1, now_ns());
+      stage_x(acc, a.X, a.ldx, m.fc, nullptr, w, nr);
+      __syncthreads();
+      block_trsv<true>(acc, Ab, sh_rinv, w, nr);
+      __syncthreads();
+      for (int idx = threadIdx.x; idx < w * nr; idx += kThreads) {
+        int c = idx / w, r = idx - c * w;
+        a.X[m.fc + r + c * a.ldx] = acc[r + c * kT];
+      }
+      for (int u = 0; u < noff; ++u) {
+        const int r0 = w + u * kT, bu = min(kT, m.h - r0);
+        stage_block(Ab, P, ld, r0, bu, 0, w);
+        __syncthreads();
+        block_gemv_atomic<false>(a.X, a.ldx, 0, Ab, kPld, acc, bu, w, nr, -1.0, rl + r0);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+          __threadfence();
+          int last = -1;
+          for (int r = 0; r < bu; ++r) {
+            int tgt = a.supmember[rl[r0 + r]];
+            if (tgt != last) atomicAdd(a.arrived + tgt, 1);
+            last = tgt;
+          }
+        }
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) red_release(a.blkdone + s, 1);
     } else {
       // O(i0, u): off-diagonal rows, Y_K[rows] -= L_KJ Y_J over the column blocks of a
       // chunk, accumulated, then scattered into the ancestors' rows
@@ -343,7 +378,42 @@ __global__ void __launch_bounds__(kThreads, solve_min_blocks<kR>()) k_solve_back
     const int32_t* rl = a.rows + m.lidx;
     const int64_t ld = m.ld;
     const int nblk = (m.w + kT - 1) / kT;
-    if (task.kind == 3) {
+    if (task.kind == 4) {
+      // G: a one-block supernode whole: X_0 -= L_u0^T X_u for every off-diagonal tile
+      // (ancestor rows, final once the parent is done), then X_0 <- L_00^-T X_0
+      const int w = m.w, noff = (m.h - m.w + kT - 1) / kT;
+      const int par = a.sparent[s];
+      if (par >= 0 && !wait_geq(a.blkdone + par, (a.meta[par].w + kT - 1) / kT, a.status, s, &sh_ok, a.spin_limit))
+        return;
+      trace_mark(a, tk, 1, now_ns());
+      stage_x(acc, a.X, a.ldx, m.fc, nullptr, w, nr);
+      for (int u = 0; u < noff; ++u) {
+        const int r0 = w + u * kT, bu = min(kT, m.h - r0);
+        __syncthreads();
+        stage_block(Ab, P, ld, r0, bu, 0, w);
+        stage_x(Bx, a.X, a.ldx, 0, rl + r0, bu, nr);
+        __syncthreads();
+        for (int idx = threadIdx.x; idx < w * nr; idx += kThreads) {  // acc_k -= sum_r L_rk x_r
+          const int c = idx / w, k = idx - c * w;
+          double t = 0.0;
+          for (int r = 0; r < bu; ++r) t = fma(Ab[r + k * kPld], Bx[r + c * kT], t);
+          acc[k + c * kT] -= t;
+        }
+      }
+      __syncthreads();
+      stage_block(Ab, P, ld, 0, w, 0, w);
+      __syncthreads();
+      if (threadIdx.x < w) sh_rinv[threadIdx.x] = 1.0 / Ab[threadIdx.x * (kPld + 1)];
+      __syncthreads();
+      block_trsv<false>(acc, Ab, sh_rinv, w, nr);
+      __syncthreads();
+      for (int idx = threadIdx.x; idx < w * nr; idx += kThreads) {
+        int c = idx / w, r = idx - c * w;
+        a.X[m.fc + r + c * a.ldx] = acc[r + c * kT];
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) red_release(a.blkdone + s, 1);
+    } else if (task.kind == 3) {
       // W(u): ancestor rows of tile u, final once the parent is done: X_t -= L_ut^T X_u for
       // every column block t, newest first (the order the diagonal chain needs them)
       const int u = task.t, rr = m.w + u * kT, br = min(kT, m.h - rr);

@@ -247,7 +247,7 @@ def test_solve_trace_of_a_profiled_solve():
     M.Factorize()
     M.SetProfiling(True)
     M.Solve(np.ones(n))
-    for sweep, kinds in ((0, {0, 1, 2}), (1, {0, 1, 3})):
+    for sweep, kinds in ((0, {0, 1, 2, 4}), (1, {0, 1, 3, 4})):  # 4: a small supernode in one task
         tr = M.GetSolveTrace(sweep).astype(np.int64)
         assert tr.shape[1] == 4 and len(tr) > 0
         t0, t1, t2, sk = tr.T
