@@ -163,7 +163,7 @@ __device__ __forceinline__ void block_gemv_atomic(double* X, int64_t ldx, int x0
 // the reciprocals of the diagonal (computed off the dependency chain).
 // forward: acc <- D^-1 acc ; backward: acc <- D^-T acc.
 template <bool kForward>
-__device__ void block_trsv(double* acc, const double* A, const double* rinv, int kk, int nr) {
+__device__ void block_trsv(double* acc, const double* A, const double* rinv, int kk, int nr, int lda = kPld) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = kThreads / 32;
   for (int c = warp; c < nr; c += nw) {
     double v0 = lane < kk ? acc[lane + c * kT] : 0.0;
@@ -179,12 +179,12 @@ __device__ void block_trsv(double* acc, const double* A, const double* rinv, int
       }
       if (kForward) {
         // rows j > k: acc_j -= D[j][k] x_k
-        if (lane > k && lane < kk) v0 = fma(-A[lane + k * kPld], xk, v0);
-        if (lane + 32 > k && lane + 32 < kk) v1 = fma(-A[lane + 32 + k * kPld], xk, v1);
+        if (lane > k && lane < kk) v0 = fma(-A[lane + k * lda], xk, v0);
+        if (lane + 32 > k && lane + 32 < kk) v1 = fma(-A[lane + 32 + k * lda], xk, v1);
       } else {
         // rows j < k: acc_j -= D[k][j] x_k
-        if (lane < k) v0 = fma(-A[k + lane * kPld], xk, v0);
-        if (lane + 32 < k) v1 = fma(-A[k + (lane + 32) * kPld], xk, v1);
+        if (lane < k) v0 = fma(-A[k + lane * lda], xk, v0);
+        if (lane + 32 < k) v1 = fma(-A[k + (lane + 32) * lda], xk, v1);
       }
     }
     if (lane < kk) acc[lane + c * kT] = v0;
@@ -289,15 +289,32 @@ __global__ void __launch_bounds__(kThreads, solve_min_blocks<kR>()) k_solve_forw
     } else if (task.kind == 4) {
       // F: a one-block supernode whole: X_0 <- L_00^-1 X_0, then every off-diagonal tile
       // scattered into the ancestors' rows
-      const int w = m.w, noff = (m.h - m.w + kT - 1) / kT;
-      stage_block(Ab, P, ld, 0, w, 0, w);  // L is final: load before waiting
+      const int w = m.w, h = m.h, noff = (m.h - m.w + kT - 1) / kT;
+      // a panel that fits the two staging buffers is loaded whole (ld h) before waiting
+      const bool whole = h * w <= kT * kPld + kT * kT;
+      if (whole) {  // eight loads of a thread in flight at a time
+        for (int base = threadIdx.x; base < h * w; base += 8 * kThreads) {
+          T v[8];
+#pragma unroll
+          for (int q = 0; q < 8; ++q) {
+            const int idx = base + q * kThreads, c = idx / h, r = idx - c * h;
+            v[q] = idx < h * w ? P[r + (int64_t)c * ld] : T(0);
+          }
+#pragma unroll
+          for (int q = 0; q < 8; ++q)
+            if (base + q * kThreads < h * w) Ab[base + q * kThreads] = (double)v[q];
+        }
+      } else {
+        stage_block(Ab, P, ld, 0, w, 0, w);  // L is final: load before waiting
+      }
+      const int lda = whole ? h : kPld;
       __syncthreads();
-      if (threadIdx.x < w) sh_rinv[threadIdx.x] = 1.0 / Ab[threadIdx.x * (kPld + 1)];
+      if (threadIdx.x < w) sh_rinv[threadIdx.x] = 1.0 / Ab[threadIdx.x * (lda + 1)];
       if (!wait_geq(a.arrived + s, a.expected[s], a.status, s, &sh_ok, a.spin_limit)) return;
       trace_mark(a, tk, 1, now_ns());
       stage_x(acc, a.X, a.ldx, m.fc, nullptr, w, nr);
       __syncthreads();
-      block_trsv<true>(acc, Ab, sh_rinv, w, nr);
+      block_trsv<true>(acc, Ab, sh_rinv, w, nr, lda);
       __syncthreads();
       for (int idx = threadIdx.x; idx < w * nr; idx += kThreads) {
         int c = idx / w, r = idx - c * w;
@@ -305,9 +322,11 @@ __global__ void __launch_bounds__(kThreads, solve_min_blocks<kR>()) k_solve_forw
       }
       for (int u = 0; u < noff; ++u) {
         const int r0 = w + u * kT, bu = min(kT, m.h - r0);
-        stage_block(Ab, P, ld, r0, bu, 0, w);
-        __syncthreads();
-        block_gemv_atomic<false>(a.X, a.ldx, 0, Ab, kPld, acc, bu, w, nr, -1.0, rl + r0);
+        if (!whole) {
+          stage_block(Ab, P, ld, r0, bu, 0, w);
+          __syncthreads();
+        }
+        block_gemv_atomic<false>(a.X, a.ldx, 0, whole ? Ab + r0 : Ab, lda, acc, bu, w, nr, -1.0, rl + r0);
         __syncthreads();
         if (threadIdx.x == 0) {
           __threadfence();
