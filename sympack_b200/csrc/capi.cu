@@ -619,6 +619,10 @@ spb::RelaxParams relax_of(const spb_options& o) {
 
 spb::PlanParams plan_params_of(const spb_options& o) {
   spb::PlanParams pp;
+  if (o.device >= 0) {
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, o.device) == cudaSuccess && sms > 0) pp.sms = sms;
+  }
   if (o.plan_small_max_w > 0) pp.small_max_w = o.plan_small_max_w;
   if (o.plan_big_tile_rows > 0) pp.big_tile_rows = o.plan_big_tile_rows;
   if (o.plan_outer_nb > 0) pp.outer_nb = o.plan_outer_nb;

@@ -79,6 +79,31 @@ Plan build_plan(const Symbolic& sym, const PlanParams& prm) {
         out.push_back(t);
       }
   };
+  // A launch with fewer tiles than the GPU has slots for them splits each tile's K range
+  // into parts of at least 64 columns (split-K): the update epilogue subtracts with
+  // atomic additions, so the partial products of one tile simply add up.
+  auto split_k = [&](std::vector<TileItem>& v, int per_sm) {
+    const int64_t slots = (int64_t)std::max(1, prm.sms) * per_sm;
+    if (v.empty() || (int64_t)v.size() * 2 > slots) return;
+    const int parts = (int)std::min<int64_t>(8, (slots + (int64_t)v.size() - 1) / (int64_t)v.size());
+    std::vector<TileItem> out;
+    out.reserve(v.size() * parts);
+    for (const TileItem& t : v) {
+      const int p = std::min(parts, t.kn / 64);
+      if (p <= 1) {
+        out.push_back(t);
+        continue;
+      }
+      const int step = (t.kn / p + 63) / 64 * 64;
+      for (int k = 0; k < t.kn; k += step) {
+        TileItem u = t;
+        u.k0 = t.k0 + k;
+        u.kn = std::min(step, t.kn - k);
+        out.push_back(u);
+      }
+    }
+    v.swap(out);
+  };
   // Emit the tiles of one phase as (up to) two launches: 64-wide FMA tiles and
   // 128-wide tensor-core tiles.
   std::vector<TileItem> t64, t128;
@@ -86,6 +111,7 @@ Plan build_plan(const Symbolic& sym, const PlanParams& prm) {
     for (int pass = 0; pass < 2; ++pass) {
       std::vector<TileItem>& v = pass ? t128 : t64;
       if (v.empty()) continue;
+      split_k(v, pass ? 1 : 4);
       Step gs{StepKind::Gemm, (int32_t)P.tile_items.size(), (int32_t)v.size(), 0, pass ? 128 : 64, lane, blk};
       P.tile_items.insert(P.tile_items.end(), v.begin(), v.end());
       P.steps.push_back(gs);

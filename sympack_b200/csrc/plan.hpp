@@ -173,6 +173,8 @@ struct PlanParams {
   int dense_min_w = 0;           // narrowest root solved by the cluster kernel (0 = never; measured
                                  // slower than the persistent sweep so far, kept as an option)
   int solve_chunk = 16;          // column blocks per forward off-diagonal solve task
+  int sms = 148;                 // SMs of the device: a launch with too few tiles to fill them
+                                 // splits its tiles' K range (partial products add atomically)
 };
 
 Plan build_plan(const Symbolic& s, const PlanParams& p = PlanParams());

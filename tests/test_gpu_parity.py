@@ -255,3 +255,20 @@ def test_solve_trace_of_a_profiled_solve():
         assert set(np.unique(sk & 255)) <= kinds
         assert np.all((sk >> 8) < M.info().nsuper)
     M.close()
+
+
+@pytest.mark.parametrize("opt", [dict(plan_outer_nb=64), dict(plan_outer_nb=512), dict(plan_solve_chunk=1),
+                                 dict(plan_solve_chunk=3), dict(plan_small_max_w=16, plan_big_tile_rows=96),
+                                 dict(plan_small_max_w=48, plan_big_tile_rows=256)],
+                         ids=["outer64", "outer512", "chunk1", "chunk3", "small16_rows96", "small48_rows256"])
+def test_plan_options_give_the_same_factor_and_solution(opt):
+    """Every plan tunable changes only the schedule: factor and solution stay within the
+    parity bound of the oracle."""
+    n, cp, ri, v = G.stencil27(16, 16, 16, 1e-2, seed=8)
+    A = DistSparseMatrix.from_lower_csc(n, cp, ri, v)
+    M = setup(A, **opt)
+    f = oracle_for(M, A)
+    assert relerr(M.GetFactor(), f.factor()) <= TOL
+    b = np.random.default_rng(6).standard_normal((n, 5))
+    M.Solve(b)
+    assert relerr(M.GetSolution(nrhs=5), f.solve(b)) <= TOL
