@@ -85,7 +85,7 @@ Plan build_plan(const Symbolic& sym, const PlanParams& prm) {
   auto split_k = [&](std::vector<TileItem>& v, int per_sm) {
     const int64_t slots = (int64_t)std::max(1, prm.sms) * per_sm;
     if (v.empty() || (int64_t)v.size() * 2 > slots) return;
-    const int parts = (int)std::min<int64_t>(8, (slots + (int64_t)v.size() - 1) / (int64_t)v.size());
+    const int parts = (int)std::min<int64_t>(8, slots / (int64_t)v.size());  // one wave
     std::vector<TileItem> out;
     out.reserve(v.size() * parts);
     for (const TileItem& t : v) {
