@@ -461,7 +461,7 @@ def batching_comparison(torch, dev, stream, count, seed=0, subset=64):
     return out
 
 
-def serving_comparison(torch, dev, count, seed=0, load=0.8):
+def serving_comparison(torch, dev, count, seed=0, load=0.7):
     """Serving form on the request stream: (1) back-to-back plain FP64, one request
     after the other; (2) the continuous-batching loop (FP32 + refinement, 8 slots,
     right-hand sides merged per factor) with every request submitted at once, which
@@ -528,9 +528,8 @@ def run_ours(args):
     import torch.distributed as dist
     from sympack_b200 import DistSparseMatrix, symPACKMatrix2D, symPACKOptions
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    from sympack_b200 import replicas
+    world, rank, local = replicas.world_info()
     if world > 1:
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
@@ -571,9 +570,7 @@ def run_ours(args):
         return ev
 
     def barrier():
-        if world > 1:
-            dist.barrier()
-        torch.cuda.synchronize()
+        replicas.barrier(dist, torch.cuda.synchronize)
 
     for _ in range(args.warmup):
         step()
@@ -588,10 +585,7 @@ def run_ours(args):
     s1 = [e[1].elapsed_time(e[2]) for e in evs]
     s16 = [e[2].elapsed_time(e[3]) for e in evs]
     tot = [e[0].elapsed_time(e[3]) for e in evs]
-    sums = torch.tensor([sum(fac), sum(s1), sum(s16), sum(tot)], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(sums, op=dist.ReduceOp.MAX)
-    fac_ms, s1_ms, s16_ms, tot_ms = (float(x) for x in sums.cpu())
+    fac_ms, s1_ms, s16_ms, tot_ms = replicas.max_over_ranks([sum(fac), sum(s1), sum(s16), sum(tot)], dev, dist)
 
     x1 = d_x1.cpu().numpy()
     x16 = np.asfortranarray(d_x16.cpu().numpy().T)
@@ -623,10 +617,7 @@ def run_ours(args):
     barrier()
     e2e_ev = [e2e_step() for _ in range(args.steps)]
     barrier()
-    e2e_ms = torch.tensor([sum(s.elapsed_time(e) for s, e in e2e_ev)], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(e2e_ms, op=dist.ReduceOp.MAX)
-    e2e_ms = float(e2e_ms.cpu())
+    e2e_ms = replicas.max_over_ranks([sum(s.elapsed_time(e) for s, e in e2e_ev)], dev, dist)[0]
     bwd_e2e = backward_error(A, np.asfortranarray(h_out.numpy().T), b16)
 
     # one profiled step (eager launches with per-launch CUDA events) for the roofline
@@ -685,7 +676,7 @@ def run_ours(args):
     launches_per_step = 1 + info.factor_launches + 4 + 4 + (2 if info.dense_root_width else 0)
     if rank == 0:
         line = {
-            "metric": METRIC, "value": world * flops * K / (fac_ms * 1e-3) / 1e12, "unit": "TFLOP/s",
+            "metric": METRIC, "value": replicas.job_rate(flops * K, world, fac_ms) / 1e12, "unit": "TFLOP/s",
             "n_gpus": world, "steps": K, "warmup": args.warmup, "ms_per_step": tot_ms / K,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": WORKLOAD, "n": n, "nnz_L": info.nnz_l, "flops_stat": flops,

@@ -89,9 +89,13 @@ class SolverService:
 
     def __init__(self, device: int = 0, precision: str = "FP32_IR", max_inflight: int = 8,
                  memory_budget: int | None = None, max_batch_rhs: int = 64, ir_tolerance: float = 1e-12,
-                 analysis_threads: int = 4, max_evicted_kept: int = 64):
+                 analysis_threads: int = 4, max_evicted_kept: int = 64, max_factor_inflight: int | None = None):
         self.device, self.precision = device, precision
         self.max_inflight, self.max_batch_rhs, self.ir_tolerance = max_inflight, max_batch_rhs, ir_tolerance
+        # factorizations may hold at most this many slots, so that solves against cached
+        # factors (short) always find one
+        self.max_factor_inflight = max(1, max_inflight - 2 if max_factor_inflight is None else max_factor_inflight)
+        self._factor_inflight = 0
         if memory_budget is None:
             import torch  # device memory query only
             free, _ = torch.cuda.mem_get_info(device)
@@ -237,7 +241,18 @@ class SolverService:
         return self._reserved + need <= self.memory_budget
 
     def _admit(self) -> list:
+        """Start what fits: first the solves whose factor is cached (short jobs, right-hand
+        sides merged per factor), then factorizations, each class in arrival order;
+        factorizations are capped at max_factor_inflight slots."""
         jobs = []
+        self._admit_pass(jobs, solves=True)
+        self._admit_pass(jobs, solves=False)
+        self._inflight += len(jobs)
+        self._factor_inflight += sum(1 for j in jobs if j[0] == "factor")
+        self.stats["max_inflight"] = max(self.stats["max_inflight"], self._inflight)
+        return jobs
+
+    def _admit_pass(self, jobs: list, solves: bool) -> None:
         factor_blocked = False  # a factorization waits for memory: later ones may not pass it
         for req in list(self._waiting):
             if self._inflight + len(jobs) >= self.max_inflight:
@@ -245,7 +260,10 @@ class SolverService:
             if req not in self._waiting:  # taken by a merged solve group above
                 continue
             fid = req.factor_id
-            if req.kind == "solve" and fid in self._factors:
+            cached_solve = req.kind == "solve" and fid in self._factors
+            if solves != cached_solve:
+                continue
+            if cached_solve:
                 F = self._factors[fid]
                 if F.busy:
                     continue
@@ -276,6 +294,8 @@ class SolverService:
             # a factorization: fresh matrix, or refactor of an evicted factor
             if factor_blocked or fid in self._pending_ids:
                 continue
+            if self._factor_inflight + sum(1 for j in jobs if j[0] == "factor") >= self.max_factor_inflight:
+                break
             if fid in self._factors:  # same id factored again: drop the old factor once idle
                 F = self._factors[fid]
                 if F.busy:
@@ -304,9 +324,6 @@ class SolverService:
             self._waiting.remove(req)
             self._evicted.pop(fid, None)
             jobs.append(("factor", req, A, key, T, need))
-        self._inflight += len(jobs)
-        self.stats["max_inflight"] = max(self.stats["max_inflight"], self._inflight)
-        return jobs
 
     # -- workers ----------------------------------------------------------------------
     def _options(self) -> symPACKOptions:
@@ -321,6 +338,8 @@ class SolverService:
         finally:
             with self._cv:
                 self._inflight -= 1
+                if job[0] == "factor":
+                    self._factor_inflight -= 1
                 self._cv.notify_all()
 
     def _finish(self, req: Request, x, inf, batched: int):

@@ -120,7 +120,9 @@ def test_admission_respects_budget_and_refactors_after_eviction(fake):
     futs = []
     for fid, A in mats.items():
         futs.append((fid, None, svc.submit(S.Request("factor_solve", fid, rng.standard_normal(A.size), matrix=A))))
-    for fid, A in mats.items():  # the early factors have been evicted by now: refactored on the miss
+    for _, _, f in futs:  # every factorization done: the early factors were evicted to make room
+        f.result(timeout=60)
+    for fid, A in mats.items():  # solves against evicted factors are refactored on the miss
         b = rng.standard_normal(A.size)
         futs.append((fid, b, svc.submit(S.Request("solve", fid, b))))
     out = [(fid, b, f.result(timeout=60)) for fid, b, f in futs]
@@ -162,3 +164,24 @@ def test_stream_is_seeded_and_mixed():
     assert all(1 <= r.spec[3] <= 64 for _, r in a)
     r = S.materialise(next(r for _, r in a if r.kind == "factor_solve"))
     assert r.matrix.size == r.rhs.shape[0]
+
+
+def test_cached_solves_are_admitted_before_waiting_factorizations(fake):
+    """With factorization slots capped, a solve against a cached factor that arrives after
+    several new factorizations does not wait for them."""
+    rng = np.random.default_rng(2)
+    mats = {f"f{i}": lap(9 + i, 0.2) for i in range(5)}
+    A0 = lap(8, 0.5)
+    svc = S.SolverService(memory_budget=1 << 30, max_inflight=3, max_factor_inflight=1)
+    svc.submit(S.Request("factor_solve", "a", rng.standard_normal(A0.size), matrix=A0)).result(timeout=30)
+    order = []
+    futs = [svc.submit(S.Request("factor_solve", fid, rng.standard_normal(A.size), matrix=A)) for fid, A in mats.items()]
+    b = rng.standard_normal(A0.size)
+    fs = svc.submit(S.Request("solve", "a", b))
+    for f in futs + [fs]:
+        f.add_done_callback(lambda f, order=order: order.append(f))
+    assert np.allclose(fs.result(timeout=30).x, dense_solve(A0, b), rtol=1e-12, atol=1e-12)
+    [f.result(timeout=60) for f in futs]
+    svc.close()
+    assert order.index(fs) < len(futs)  # finished before the last factorization
+    assert svc.stats["max_inflight"] <= 3
