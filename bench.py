@@ -645,19 +645,21 @@ def run_ours(args):
     roofline_solve["frac"] = roofline_solve["achieved"] / roofline_solve["peak"]
     kernels = {k: {"ms": round(p["ms"], 4), "launches": p["launches"]} for k, p in prof.items() if p["launches"]}
 
+    # the precision, LDL^T, batching and serving comparisons are one-GPU measurements: with
+    # several replicas only the headline line is measured
     precision = None
-    if not args.no_precision:
+    if not args.no_precision and world == 1:
         precision = precision_comparison(torch, dev, stream, grid=args.precision_grid)
 
     ldl = None
-    if not args.no_ldl:
+    if not args.no_ldl and world == 1:
         ldl = ldl_comparison(torch, dev, stream, grid=args.grid)
 
     batching = None
-    if not args.no_batch:
+    if not args.no_batch and world == 1:
         batching = batching_comparison(torch, dev, stream, args.batch_systems)
     serving = None
-    if not args.no_serve:
+    if not args.no_serve and world == 1:
         serving = serving_comparison(torch, dev, args.serve_requests)
 
     cpu = None
