@@ -1,0 +1,81 @@
+"""The C boundary from C: include/sympack_b200.h compiles as C99 and a C program linked
+against the library runs the host-only analysis (no GPU needed) and reads the same
+results the Python binding reports."""
+import os
+import shutil
+import subprocess
+
+import numpy as np
+import pytest
+
+from sympack_b200 import DistSparseMatrix, generators as G, symPACKMatrix2D, symPACKOptions
+from sympack_b200 import _native as N
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+PROGRAM = r"""
+#include <stdio.h>
+#include <stdlib.h>
+#include "sympack_b200.h"
+
+/* 2D 5-point Laplacian k x k, lower triangle, 1-based CSC */
+int main(int argc, char** argv) {
+  const int k = atoi(argv[1]), n = k * k;
+  int64_t* colptr = malloc(sizeof(int64_t) * (n + 1));
+  int32_t* rowind = malloc(sizeof(int32_t) * 3 * n);
+  int64_t nz = 0;
+  for (int c = 0; c < n; ++c) {
+    colptr[c] = nz + 1;
+    rowind[nz++] = c + 1;
+    if ((c + 1) % k) rowind[nz++] = c + 2;
+    if (c + k < n) rowind[nz++] = c + k + 1;
+  }
+  colptr[n] = nz + 1;
+  spb_options o;
+  spb_default_options(&o);
+  o.device = -1;                 /* host-only: symbolic analysis */
+  o.ordering = SPB_ORDERING_AMD;
+  spb_handle* h = NULL;
+  if (spb_create(&o, &h) != SPB_OK) return 2;
+  int rc = spb_symbolic(h, n, colptr, rowind);
+  if (rc != SPB_OK) { fprintf(stderr, "%s\n", spb_last_error(h)); return 3; }
+  spb_info info;
+  if (spb_get_info(h, &info) != SPB_OK) return 4;
+  int32_t* perm = malloc(sizeof(int32_t) * n);
+  int32_t* invp = malloc(sizeof(int32_t) * n);
+  if (spb_get_ordering(h, perm, invp) != SPB_OK) return 5;
+  long long check = 0;
+  for (int i = 0; i < n; ++i) check += (long long)(i + 1) * invp[i];
+  printf("%d %d %lld %.1f %lld\n", info.n, info.nsuper, (long long)info.nnz_l, info.flops_stat, check);
+  /* a device call on a host-only handle is refused, not crashed */
+  if (spb_factorize(h) == SPB_OK) return 6;
+  spb_destroy(h);
+  free(colptr); free(rowind); free(perm); free(invp);
+  return 0;
+}
+"""
+
+
+@pytest.mark.skipif(shutil.which("gcc") is None, reason="no C compiler")
+def test_c_program_against_the_library(tmp_path):
+    lib = N.load()  # builds the library if needed
+    libdir = os.path.dirname(lib._name)
+    src = tmp_path / "prog.c"
+    src.write_text(PROGRAM)
+    exe = tmp_path / "prog"
+    subprocess.run(["gcc", "-std=c99", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe),
+                    "-L", libdir, "-lsympack_b200", f"-Wl,-rpath,{libdir}"], check=True)
+    env = dict(os.environ)
+    import nvidia.cuda_runtime as cr  # the CUDA runtime the library links against
+    rt = os.path.join(os.path.dirname(cr.__file__), "lib")
+    env["LD_LIBRARY_PATH"] = rt + os.pathsep + env.get("LD_LIBRARY_PATH", "")
+    out = subprocess.run([str(exe), "24"], check=True, capture_output=True, text=True, env=env).stdout.split()
+    n, cp, ri, v = G.laplacian_2d(24, 24)
+    M = symPACKMatrix2D()
+    M.Init(symPACKOptions(device=-1, orderingStr="AMD"))
+    M.SymbolicFactorization(DistSparseMatrix.from_lower_csc(n, cp, ri, v))
+    inf = M.info()
+    _, invp = M.GetOrdering()
+    assert int(out[0]) == n and int(out[1]) == inf.nsuper and int(out[2]) == inf.nnz_l
+    assert float(out[3]) == pytest.approx(inf.flops_stat)
+    assert int(out[4]) == int(np.sum(np.arange(1, n + 1, dtype=np.int64) * invp))
