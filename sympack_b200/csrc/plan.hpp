@@ -161,7 +161,7 @@ struct Plan {
 
 // Supernodes of one 64-column block with at most this many off-diagonal 64-row tiles
 // are one solve task per sweep.
-constexpr int kSolveFusedTiles = 4;
+constexpr int kSolveFusedTiles = 16;
 
 // Tunables of the plan.
 struct PlanParams {
