@@ -258,3 +258,25 @@ def test_statistics_match_reference_formula():
     assert inf.flops_stat == float(np.sum(p["cc_fund"].astype(np.float64) ** 2))
     assert inf.nnz_l == int(p["cc_fund"].sum())
     assert inf.nsuper == len(p["xsuper"]) - 1
+
+
+TINY = {
+    "n1": (1, [1, 2], [1]),
+    "diag5": (5, [1, 2, 3, 4, 5, 6], [1, 2, 3, 4, 5]),
+    "path2": (2, [1, 3, 4], [1, 2, 2]),
+}
+# invp the reference Fortran (ordmmd / amdbar / genrcm) returns for these graphs
+TINY_INVP = {
+    ("n1", "MMD"): [1], ("n1", "AMD"): [1], ("n1", "RCM"): [1],
+    ("diag5", "MMD"): [5, 4, 3, 2, 1], ("diag5", "AMD"): [1, 2, 3, 4, 5], ("diag5", "RCM"): [1, 2, 3, 4, 5],
+    ("path2", "MMD"): [2, 1], ("path2", "AMD"): [1, 2], ("path2", "RCM"): [2, 1],
+}
+
+
+@pytest.mark.parametrize("case,ordering", sorted(TINY_INVP), ids=lambda x: x if isinstance(x, str) else None)
+def test_tiny_and_edgeless_graphs(case, ordering):
+    """One vertex, vertices without edges, a single edge: the orderings' degenerate paths."""
+    n, cp, ri = TINY[case]
+    p = analyze(n, np.array(cp, np.int64), np.array(ri, np.int32), orderingStr=ordering)
+    assert list(p["mmd_invp"]) == TINY_INVP[(case, ordering)]
+    assert sorted(p["perm"]) == list(range(1, n + 1))
