@@ -272,3 +272,31 @@ def test_plan_options_give_the_same_factor_and_solution(opt):
     b = np.random.default_rng(6).standard_normal((n, 5))
     M.Solve(b)
     assert relerr(M.GetSolution(nrhs=5), f.solve(b)) <= TOL
+
+
+@pytest.mark.parametrize("decomposition", ["LL", "LDL"])
+@pytest.mark.parametrize("case", ["n1", "diag7", "path2", "isolated"])
+def test_degenerate_matrices(case, decomposition):
+    """One unknown, a diagonal matrix, a single edge, and a path with an isolated vertex:
+    one-column supernodes through the small-panel kernel and the fused solve tasks."""
+    if case == "n1":
+        n, cp, ri, v = 1, np.array([1, 2], np.int64), np.array([1], np.int32), np.array([4.0])
+    elif case == "diag7":
+        n, cp, ri, v = 7, np.arange(1, 9, dtype=np.int64), np.arange(1, 8, dtype=np.int32), np.arange(1.0, 8.0)
+    elif case == "path2":
+        n, cp, ri, v = 2, np.array([1, 3, 4], np.int64), np.array([1, 2, 2], np.int32), np.array([3.0, -1.0, 2.0])
+    else:  # vertices 1-2-3 on a path, vertex 4 alone
+        n = 4
+        cp = np.array([1, 3, 5, 6, 7], np.int64)
+        ri = np.array([1, 2, 2, 3, 3, 4], np.int32)
+        v = np.array([4.0, -1.0, 4.0, -1.0, 4.0, 2.5])
+    A = DistSparseMatrix.from_lower_csc(n, cp, ri, v)
+    M = setup(A, decomposition=decomposition)
+    D = np.zeros((n, n))
+    cols = np.repeat(np.arange(n), np.diff(cp))
+    D[ri - 1, cols] = v
+    D = D + np.tril(D, -1).T
+    b = np.random.default_rng(0).standard_normal((n, 2))
+    M.Solve(b)
+    x = M.GetSolution(nrhs=2)
+    assert relerr(x, np.linalg.solve(D, b)) <= TOL
