@@ -79,3 +79,69 @@ def test_c_program_against_the_library(tmp_path):
     assert int(out[0]) == n and int(out[1]) == inf.nsuper and int(out[2]) == inf.nnz_l
     assert float(out[3]) == pytest.approx(inf.flops_stat)
     assert int(out[4]) == int(np.sum(np.arange(1, n + 1, dtype=np.int64) * invp))
+
+
+CPP_PROGRAM = r"""
+#include <cstdio>
+#include <vector>
+#include "sympack_b200.hpp"
+
+// the members of symPACK's DistSparseMatrix<double> at one rank that the class reads
+struct Graph { std::vector<long long> colptr; std::vector<int> rowind; };
+struct DistSparseMatrix { int size; Graph Localg_; std::vector<double> nzvalLocal; };
+
+int main() {
+  const int k = 20, n = k * k;
+  DistSparseMatrix A;
+  A.size = n;
+  for (int c = 0; c < n; ++c) {
+    A.Localg_.colptr.push_back((long long)A.Localg_.rowind.size() + 1);
+    A.Localg_.rowind.push_back(c + 1); A.nzvalLocal.push_back(4.0);
+    if ((c + 1) % k) { A.Localg_.rowind.push_back(c + 2); A.nzvalLocal.push_back(-1.0); }
+    if (c + k < n) { A.Localg_.rowind.push_back(c + k + 1); A.nzvalLocal.push_back(-1.0); }
+  }
+  A.Localg_.colptr.push_back((long long)A.Localg_.rowind.size() + 1);
+  spb_options o;
+  spb_default_options(&o);
+  o.device = -1;
+  sympack_b200::symPACKMatrix2D M;
+  M.Init(o);
+  M.SymbolicFactorization(A);
+  std::vector<int> invp;
+  std::vector<int> perm = M.GetOrdering(&invp);
+  std::vector<int> xsuper = M.GetSupernodalPartition();
+  std::vector<int> parent = M.GetETree();
+  long long check = 0;
+  for (int i = 0; i < n; ++i) check += (long long)(i + 1) * invp[i];
+  std::printf("%d %zu %lld %d\n", M.info().nsuper, xsuper.size(), check, parent[n - 1]);
+  bool threw = false;
+  try { M.Factorize(); } catch (const std::runtime_error&) { threw = true; }  // host-only handle
+  std::printf("%d\n", threw ? 1 : 0);
+  return 0;
+}
+"""
+
+
+@pytest.mark.skipif(shutil.which("g++") is None, reason="no C++ compiler")
+def test_cpp_class_over_the_library(tmp_path):
+    lib = N.load()
+    libdir = os.path.dirname(lib._name)
+    src = tmp_path / "prog.cpp"
+    src.write_text(CPP_PROGRAM)
+    exe = tmp_path / "progxx"
+    subprocess.run(["g++", "-std=c++17", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"), str(src), "-o",
+                    str(exe), "-L", libdir, "-lsympack_b200", f"-Wl,-rpath,{libdir}"], check=True)
+    import nvidia.cuda_runtime as cr
+    env = dict(os.environ)
+    env["LD_LIBRARY_PATH"] = os.path.join(os.path.dirname(cr.__file__), "lib") + os.pathsep + env.get(
+        "LD_LIBRARY_PATH", "")
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True, env=env).stdout.split()
+    n, cp, ri, v = G.laplacian_2d(20, 20)
+    M = symPACKMatrix2D()
+    M.Init(symPACKOptions(device=-1))
+    M.SymbolicFactorization(DistSparseMatrix.from_lower_csc(n, cp, ri, v))
+    _, invp = M.GetOrdering()
+    assert int(out[0]) == M.info().nsuper and int(out[1]) == M.info().nsuper + 1
+    assert int(out[2]) == int(np.sum(np.arange(1, n + 1, dtype=np.int64) * invp))
+    assert int(out[3]) == M.GetETree()[-1]
+    assert out[4] == "1"
