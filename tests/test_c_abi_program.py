@@ -145,3 +145,71 @@ def test_cpp_class_over_the_library(tmp_path):
     assert int(out[2]) == int(np.sum(np.arange(1, n + 1, dtype=np.int64) * invp))
     assert int(out[3]) == M.GetETree()[-1]
     assert out[4] == "1"
+
+
+CPP_DEVICE_PROGRAM = r"""
+#include <cmath>
+#include <cstdio>
+#include <vector>
+#include "sympack_b200.hpp"
+
+struct Graph { std::vector<long long> colptr; std::vector<int> rowind; };
+struct DistSparseMatrix { int size; Graph Localg_; std::vector<double> nzvalLocal; };
+
+int main() {
+  const int k = 40, n = k * k, nrhs = 3;
+  DistSparseMatrix A;
+  A.size = n;
+  for (int c = 0; c < n; ++c) {
+    A.Localg_.colptr.push_back((long long)A.Localg_.rowind.size() + 1);
+    A.Localg_.rowind.push_back(c + 1); A.nzvalLocal.push_back(4.01);
+    if ((c + 1) % k) { A.Localg_.rowind.push_back(c + 2); A.nzvalLocal.push_back(-1.0); }
+    if (c + k < n) { A.Localg_.rowind.push_back(c + k + 1); A.nzvalLocal.push_back(-1.0); }
+  }
+  A.Localg_.colptr.push_back((long long)A.Localg_.rowind.size() + 1);
+  std::vector<double> b(n * nrhs), x(n * nrhs, 0.0);
+  for (int i = 0; i < n * nrhs; ++i) b[i] = std::sin(0.37 * i);
+  spb_options o;
+  spb_default_options(&o);
+  o.device = 0;
+  sympack_b200::symPACKMatrix2D M;
+  M.Init(o);
+  M.SymbolicFactorization(A);
+  M.DistributeMatrix(A);
+  M.Factorize();
+  M.Solve(b.data(), nrhs);
+  M.GetSolution(x.data(), nrhs);
+  // residual ||A x - b|| / ||b|| with the symmetric matrix from its lower triangle
+  double rn = 0.0, bn = 0.0;
+  for (int c = 0; c < nrhs; ++c) {
+    std::vector<double> r(b.begin() + c * n, b.begin() + (c + 1) * n);
+    for (int j = 0; j < n; ++j)
+      for (long long p = A.Localg_.colptr[j] - 1; p < A.Localg_.colptr[j + 1] - 1; ++p) {
+        const int i = A.Localg_.rowind[p] - 1;
+        const double v = A.nzvalLocal[p];
+        r[i] -= v * x[c * n + j];
+        if (i != j) r[j] -= v * x[c * n + i];
+      }
+    for (int i = 0; i < n; ++i) { rn += r[i] * r[i]; bn += b[c * n + i] * b[c * n + i]; }
+  }
+  std::printf("%.3e\n", std::sqrt(rn / bn));
+  return 0;
+}
+"""
+
+
+@pytest.mark.gpu
+def test_cpp_class_factor_and_solve_on_the_device(tmp_path):
+    lib = N.load()
+    libdir = os.path.dirname(lib._name)
+    src = tmp_path / "dev.cpp"
+    src.write_text(CPP_DEVICE_PROGRAM)
+    exe = tmp_path / "devxx"
+    subprocess.run(["g++", "-std=c++17", "-O2", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe), "-L",
+                    libdir, "-lsympack_b200", f"-Wl,-rpath,{libdir}"], check=True)
+    import nvidia.cuda_runtime as cr
+    env = dict(os.environ)
+    env["LD_LIBRARY_PATH"] = os.path.join(os.path.dirname(cr.__file__), "lib") + os.pathsep + env.get(
+        "LD_LIBRARY_PATH", "")
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True, env=env, timeout=300).stdout
+    assert float(out.split()[0]) < 1e-13
