@@ -192,6 +192,86 @@ __device__ void block_trsv(double* acc, const double* A, const double* rinv, int
   }
 }
 
+// Inverses of the eight 8 x 8 diagonal blocks of a full 64 x 64 lower block A (ld kPld),
+// written transposed into A's unused upper triangle: Inv_g[i][j] (i > j) at
+// A[(8g + j) + (8g + i) * kPld]; their diagonal is rinv.  Warp g inverts block g, lane j
+// its column j by substitution.  Computed before a chain task waits, off the chain.
+__device__ void invert_diag8(double* A, const double* rinv) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (warp >= 8 || lane >= 8) return;
+  const int b = 8 * warp, j = lane;
+  double z[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    double t = 0.0;
+#pragma unroll
+    for (int k = 0; k < i; ++k)
+      if (k >= j) t = fma(A[(b + i) + (b + k) * kPld], z[k], t);
+    z[i] = i < j ? 0.0 : (i == j ? rinv[b + i] : -t * rinv[b + i]);
+  }
+#pragma unroll
+  for (int i = 1; i < 8; ++i)
+    if (i > j) A[(b + j) + (b + i) * kPld] = z[i];
+}
+
+// block_trsv for a full 64 x 64 block whose 8 x 8 diagonal inverses invert_diag8 stored:
+// eight groups of 8 rows, each solved by a product with its inverse (every lane computes
+// the group's 8 values from 8 shuffled inputs) and applied to the rows not yet solved.
+// forward: acc <- L^-1 acc ; backward: acc <- L^-T acc.  One warp per right-hand side.
+template <bool kForward>
+__device__ void block_trsv64(double* acc, const double* A, const double* rinv, int nr) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = kThreads / 32;
+  for (int c = warp; c < nr; c += nw) {
+    double v0 = acc[lane + c * kT], v1 = acc[lane + 32 + c * kT];
+#pragma unroll
+    for (int step = 0; step < 8; ++step) {
+      const int g = kForward ? step : 7 - step, b = 8 * g;
+      const bool hi = g >= 4;  // the group's rows are held in v1 of lanes b - 32 ..
+      double r[8], x[8];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) r[j] = __shfl_sync(0xffffffffu, hi ? v1 : v0, (b & 31) + j);
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        double t = rinv[b + j] * r[j];
+        if (kForward) {
+#pragma unroll
+          for (int m = 0; m < j; ++m) t = fma(A[(b + m) + (b + j) * kPld], r[m], t);  // Inv[j][m]
+        } else {
+#pragma unroll
+          for (int m = j + 1; m < 8; ++m) t = fma(A[(b + j) + (b + m) * kPld], r[m], t);  // Inv[m][j]
+        }
+        x[j] = t;
+      }
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        if (!hi && lane == b + j) v0 = x[j];
+        if (hi && lane + 32 == b + j) v1 = x[j];
+      }
+      if (kForward) {  // rows below the group: v_r -= sum_j L[r][b + j] x_j
+        if (lane > b + 7) {
+#pragma unroll
+          for (int j = 0; j < 8; ++j) v0 = fma(-A[lane + (b + j) * kPld], x[j], v0);
+        }
+        if (lane + 32 > b + 7) {
+#pragma unroll
+          for (int j = 0; j < 8; ++j) v1 = fma(-A[lane + 32 + (b + j) * kPld], x[j], v1);
+        }
+      } else {  // rows above the group: v_k -= sum_j L[b + j][k] x_j
+        if (lane < b) {
+#pragma unroll
+          for (int j = 0; j < 8; ++j) v0 = fma(-A[(b + j) + lane * kPld], x[j], v0);
+        }
+        if (lane + 32 < b) {
+#pragma unroll
+          for (int j = 0; j < 8; ++j) v1 = fma(-A[(b + j) + (lane + 32) * kPld], x[j], v1);
+        }
+      }
+    }
+    acc[lane + c * kT] = v0;
+    acc[lane + 32 + c * kT] = v1;
+  }
+}
+
 // Next task of a persistent sweep; the whole block takes the same branch
 // (thread 0 alone reads the counter and the status word, a barrier reached by
 // only part of a block would hang).  -1 = no task left or a failure recorded.
@@ -253,12 +333,17 @@ __global__ void __launch_bounds__(kThreads, solve_min_blocks<kR>()) k_solve_forw
       if (b1) stage_block<T, kT>(Bx, P, ld, r1, b1, r0, bt);
       __syncthreads();
       if (threadIdx.x < bt) sh_rinv[threadIdx.x] = 1.0 / Ab[threadIdx.x * (kPld + 1)];
+      if (bt == kT) {  // full block: 8 x 8 diagonal inverses, off the chain
+        __syncthreads();
+        invert_diag8(Ab, sh_rinv);
+      }
       if (!wait_geq(a.arrived + s, a.expected[s], a.status, s, &sh_ok, a.spin_limit)) return;
       if (!wait_geq(a.upd + m.boff + t, t, a.status, s, &sh_ok, a.spin_limit)) return;
       trace_mark(a, tk, 1, now_ns());
       stage_x(acc, a.X, a.ldx, m.fc + r0, nullptr, bt, nr);
       __syncthreads();
-      block_trsv<true>(acc, Ab, sh_rinv, bt, nr);
+      if (bt == kT) block_trsv64<true>(acc, Ab, sh_rinv, nr);
+      else block_trsv<true>(acc, Ab, sh_rinv, bt, nr);
       __syncthreads();
       for (int idx = threadIdx.x; idx < bt * nr; idx += kThreads) {
         int c = idx / bt, r = idx - c * bt;
@@ -458,11 +543,16 @@ __global__ void __launch_bounds__(kThreads, solve_min_blocks<kR>()) k_solve_back
       if (t > 0) stage_block<T, kT>(Bx, P, ld, c0, bt, c0 - kT, kT);
       __syncthreads();
       if (threadIdx.x < bt) sh_rinv[threadIdx.x] = 1.0 / Ab[threadIdx.x * (kPld + 1)];
+      if (bt == kT) {  // full block: 8 x 8 diagonal inverses, off the chain
+        __syncthreads();
+        invert_diag8(Ab, sh_rinv);
+      }
       if (!wait_geq(a.upd + m.boff + t, noff + nblk - 1 - t, a.status, s, &sh_ok, a.spin_limit)) return;
       trace_mark(a, tk, 1, now_ns());
       stage_x(acc, a.X, a.ldx, m.fc + c0, nullptr, bt, nr);
       __syncthreads();
-      block_trsv<false>(acc, Ab, sh_rinv, bt, nr);
+      if (bt == kT) block_trsv64<false>(acc, Ab, sh_rinv, nr);
+      else block_trsv<false>(acc, Ab, sh_rinv, bt, nr);
       __syncthreads();
       for (int idx = threadIdx.x; idx < bt * nr; idx += kThreads) {
         int c = idx / bt, r = idx - c * bt;
