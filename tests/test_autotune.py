@@ -64,3 +64,14 @@ def test_key_depends_on_structure_options_and_offsets(env):
     n, cp, ri, v = G.laplacian_2d(12, 13)
     k4 = autotune.structure_key(FakeM(), DistSparseMatrix.from_lower_csc(n, cp, ri, v))
     assert len({k1, k2, k3, k4}) == 4
+
+
+def test_old_cache_entry_without_outer_block_is_retuned(env):
+    """An entry written before the outer block was tuned is timed again (and replaced)."""
+    path, A = env
+    M = FakeM()
+    key = autotune.structure_key(M, A)
+    path.write_text(json.dumps({key: {"small_max_w": 48, "big_tile_rows": 256, "seconds": 1.0, "times": {}}}))
+    r = autotune.tune(M, A, reps=1)
+    assert not r["cached"] and r["outer_nb"] in autotune.OUTER_CANDIDATES
+    assert "outer_nb" in json.loads(path.read_text())[key]
