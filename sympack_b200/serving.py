@@ -242,8 +242,9 @@ class SolverService:
 
     def _admit(self) -> list:
         """Start what fits: first the solves whose factor is cached (short jobs, right-hand
-        sides merged per factor), then factorizations, each class in arrival order;
-        factorizations are capped at max_factor_inflight slots."""
+        sides merged per factor; they leave one slot free while a factorization waits),
+        then factorizations, each class in arrival order; factorizations are capped at
+        max_factor_inflight slots."""
         jobs = []
         self._admit_pass(jobs, solves=True)
         self._admit_pass(jobs, solves=False)
@@ -254,8 +255,11 @@ class SolverService:
 
     def _admit_pass(self, jobs: list, solves: bool) -> None:
         factor_blocked = False  # a factorization waits for memory: later ones may not pass it
+        limit = self.max_inflight
+        if solves and any(r.kind != "solve" or r.factor_id not in self._factors for r in self._waiting):
+            limit -= 1  # a waiting factorization keeps one slot: a stream of solves cannot starve it
         for req in list(self._waiting):
-            if self._inflight + len(jobs) >= self.max_inflight:
+            if self._inflight + len(jobs) >= limit:
                 break
             if req not in self._waiting:  # taken by a merged solve group above
                 continue
