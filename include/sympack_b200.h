@@ -164,14 +164,17 @@ int spb_solve_device(spb_handle* h, const double* d_rhs, double* d_x, int32_t nr
 
 /* Allocation-free variant of spb_solve_device.  No counterpart in the
  * reference (which has no device-side solve entry point at all).
- * For callers that cannot allocate device memory at solve time — code running
- * while a CUDA graph is captured in global mode, where cudaMalloc is an illegal
- * call, or services that fix their device-memory budget up front — whereas
- * spb_solve_device may grow its workspace with cudaMalloc on a call with more
- * right-hand sides than before.  This entry point calls no cudaMalloc, cudaFree
- * or allocating library routine: its scratch (the permuted right-hand sides and
- * the dependency counters) lives in one static __device__ array of 33 MiB that
- * every GPU which loads the library holds until the process exits.
+ * For callers that cannot allocate device memory at solve time: services that
+ * reserve their whole device-memory budget at start-up (another allocator, such
+ * as a framework's caching allocator, owns the rest of the GPU, so a cudaMalloc
+ * in the middle of a request could fail), and latency-critical callers, for
+ * which cudaMalloc / cudaFree may synchronize the device and stall the work of
+ * other streams.  spb_solve_device may grow its workspace with cudaMalloc on a
+ * call with more right-hand sides than before; this entry point calls no
+ * cudaMalloc, cudaFree or allocating library routine: its scratch (the permuted
+ * right-hand sides and the dependency counters) lives in one static __device__
+ * array of 33 MiB that every GPU which loads the library holds until the
+ * process exits.
  * Limits: n * nrhs <= 4,194,304, and 2 + 3 * nsuper + 2 * (number of
  * 64-column blocks over all supernodes) <= 262,144 dependency counters;
  * larger requests return SPB_ERR_INVALID with a message saying so.
@@ -179,7 +182,9 @@ int spb_solve_device(spb_handle* h, const double* d_rhs, double* d_x, int32_t nr
  * (cudaGetSymbolAddress); make that first call before any stream capture.
  * Every call on a device shares the array: calls whose work overlaps on the GPU
  * (other handles or streams) race, so serialize them.  The counters are cleared
- * on every call; nothing else is kept between calls. */
+ * on every call (and for every 64 right-hand sides); nothing else is kept
+ * between calls.  Like spb_solve_device, the call reads the device status word
+ * back before it returns, so it waits for the handle's stream. */
 int spb_solve_device_noalloc(spb_handle* h, const double* d_rhs, double* d_x, int32_t nrhs, int64_t ld);
 
 /* Introspection for parity checks (arrays sized from spb_get_info). */

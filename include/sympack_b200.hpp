@@ -13,6 +13,7 @@
  */
 #pragma once
 
+#include <algorithm>
 #include <cstdint>
 #include <stdexcept>
 #include <string>
@@ -21,6 +22,76 @@
 #include "sympack_b200.h"
 
 namespace sympack_b200 {
+
+// Supernode relaxation parameters with the reference's field names, constructors and
+// setters (include/sympack/Types.hpp:22-96): a positive maxSize caps every nrelax.
+// The default is run_sympack2D's (driver/utils.hpp:342-348: SetMaxSize(0), no cap).
+struct RelaxationParameters {
+  int nrelax0 = 8, nrelax1 = 32, nrelax2 = 64;
+  int maxSize = 0;
+  double zrelax0 = 0.8, zrelax1 = 0.1, zrelax2 = 0.05;
+  RelaxationParameters() = default;
+  explicit RelaxationParameters(int pmaxSize) { SetMaxSize(pmaxSize); }
+  RelaxationParameters(int p0, int p1, int p2, int pmaxSize) : nrelax0(p0), nrelax1(p1), nrelax2(p2) {
+    SetMaxSize(pmaxSize);
+  }
+  void SetMaxSize(int pmaxSize) {
+    maxSize = pmaxSize;
+    if (maxSize > 0) {
+      nrelax0 = std::min(nrelax0, maxSize);
+      nrelax1 = std::min(nrelax1, maxSize);
+      nrelax2 = std::min(nrelax2, maxSize);
+    }
+  }
+  void SetNrelax0(int p) { nrelax0 = maxSize > 0 ? std::min(p, maxSize) : p; }
+  void SetNrelax1(int p) { nrelax1 = maxSize > 0 ? std::min(p, maxSize) : p; }
+  void SetNrelax2(int p) { nrelax2 = maxSize > 0 ? std::min(p, maxSize) : p; }
+};
+
+enum class DecompositionType { LL, LDL };
+
+// The symPACKOptions fields this path reads, under the reference's names
+// (include/sympack/Types.hpp:106-201): orderingStr ("MMD", "AMD", "RCM", "NATURAL",
+// "USER"), relax, decomposition, perm (USER ordering, 1-based), verbose.  The fields
+// after them have no counterpart in the reference and select the device, the
+// precision form and its refinement target.
+struct symPACKOptions {
+  std::string orderingStr = "MMD";
+  RelaxationParameters relax;
+  DecompositionType decomposition = DecompositionType::LL;
+  int* perm = nullptr;
+  int verbose = 0;
+  int device = 0;                       // CUDA device ordinal; < 0 = host-only (symbolic analysis)
+  int precision = SPB_PRECISION_FP64;   // or SPB_PRECISION_FP32_IR
+  double ir_tolerance = 1e-12;
+
+  spb_options to_c() const {
+    spb_options o;
+    spb_default_options(&o);
+    if (orderingStr == "MMD") o.ordering = SPB_ORDERING_MMD;
+    else if (orderingStr == "NATURAL") o.ordering = SPB_ORDERING_NATURAL;
+    else if (orderingStr == "RCM") o.ordering = SPB_ORDERING_RCM;
+    else if (orderingStr == "AMD") o.ordering = SPB_ORDERING_AMD;
+    else if (orderingStr == "USER") o.ordering = SPB_ORDERING_USER;
+    else
+      throw std::logic_error("This ordering method is not supported by this solver. Valid options are: "
+                             "MMD AMD RCM NATURAL USER");
+    o.nrelax0 = relax.nrelax0;
+    o.nrelax1 = relax.nrelax1;
+    o.nrelax2 = relax.nrelax2;
+    o.max_snode = relax.maxSize;
+    o.zrelax0 = relax.zrelax0;
+    o.zrelax1 = relax.zrelax1;
+    o.zrelax2 = relax.zrelax2;
+    o.user_perm = perm;
+    o.decomposition = decomposition == DecompositionType::LDL ? SPB_DECOMPOSITION_LDL : SPB_DECOMPOSITION_LL;
+    o.verbose = verbose;
+    o.device = device;
+    o.precision = precision;
+    o.ir_tolerance = ir_tolerance;
+    return o;
+  }
+};
 
 class symPACKMatrix2D {
  public:
@@ -31,6 +102,8 @@ class symPACKMatrix2D {
     if (h_) spb_destroy(h_);
   }
 
+  // symPACKMatrix2D::Init(symPACKOptions&) (2D.hpp:2649).
+  void Init(symPACKOptions& options) { Init(options.to_c()); }
   // Options as spb_options (spb_default_options gives the reference's defaults).
   void Init(const spb_options& o) {
     if (h_) spb_destroy(h_);
@@ -63,7 +136,13 @@ class symPACKMatrix2D {
   void Factorize() { check(spb_factorize(need())); }
 
   // RHS column-major n x nrhs with leading dimension rhs_size (>= n), original ordering.
-  void Solve(const double* RHS, int nrhs, int rhs_size) { check(spb_solve(need(), RHS, nrhs, rhs_size)); }
+  // Xptr is accepted for the signature of symPACKMatrixMeta::Solve (symPACKMatrixBase.hpp:62);
+  // the reference's 2D solver does not use it (2D.hpp:6643-6711) and neither does this one:
+  // the solution stays in the object until GetSolution.
+  void Solve(const double* RHS, int nrhs, int rhs_size, double* Xptr = nullptr) {
+    (void)Xptr;
+    check(spb_solve(need(), RHS, nrhs, rhs_size));
+  }
   void Solve(const double* RHS, int nrhs) { Solve(RHS, nrhs, n_); }
   void GetSolution(double* B, int nrhs, int ldb) { check(spb_get_solution(need(), B, nrhs, ldb)); }
   void GetSolution(double* B, int nrhs) { GetSolution(B, nrhs, n_); }

@@ -16,7 +16,9 @@ from pathlib import Path
 import numpy as np
 
 HERE = Path(__file__).resolve().parent
-REF_SRC = Path("/root/reference/src")
+# Reference source tree: $SYMPACK_REFERENCE (the symPACK checkout), default /root/reference.
+REF_ROOT = Path(os.environ.get("SYMPACK_REFERENCE", "/root/reference"))
+REF_SRC = REF_ROOT / "src"
 FILES = ["ordmmd.F", "genmmd.F", "mmdint.F", "mmdelm.F", "mmdupd.F", "mmdnum.F"]
 OUT_C = HERE / "_ref" / "mmd_ref.c"
 OUT_SO = HERE / "_ref" / "libmmd_ref.so"

@@ -1187,13 +1187,17 @@ def build_cells(xsuper, xlindx, lindx, sup):
     return cells
 
 
-def symbolic_chain(n, colptr, rowind, ordering="MMD", relax=None):
-    """SymbolicFactorization (symPACKMatrix2D.hpp:2699-3081) on a 1-based lower CSC."""
+def symbolic_chain(n, colptr, rowind, ordering="MMD", relax=None, order_fn=None):
+    """SymbolicFactorization (symPACKMatrix2D.hpp:2699-3081) on a 1-based lower CSC.
+
+    order_fn(n, xadj, adj) -> invp replaces the ordering routine of `ordering`
+    (used to run the reference's own compiled ordering in place of the Python one)."""
     relax = relax or {}
     xadj, adj = expand_symmetric(n, colptr, rowind)
     if ordering in ("MMD", "RCM", "AMD"):
         sx, sa = set_keep_diag(n, xadj, adj, False)
-        invp = {"MMD": genmmd, "RCM": genrcm, "AMD": amdbar}[ordering](n, sx, sa)
+        fn = order_fn or {"MMD": genmmd, "RCM": genrcm, "AMD": amdbar}[ordering]
+        invp = [int(i) for i in fn(n, sx, sa)]
         gx, ga = set_keep_diag(n, sx, sa, True)
     elif ordering == "NATURAL":
         invp = list(range(1, n + 1))
@@ -1222,3 +1226,18 @@ def symbolic_chain(n, colptr, rowind, ordering="MMD", relax=None):
                 xsuper=np.array(xsuper, np.int32), supmember=np.array(sup, np.int32),
                 xlindx=np.array(xlindx, np.int64), lindx=np.array(lindx, np.int32),
                 flops_stat=float(sum(float(c) * c for c in cc_fund)), nnzL_stat=int(sum(cc_fund)))
+
+
+def reference_symbolic(n, colptr, rowind):
+    """MMD symbolic analysis computed by the oracle alone: the executed reference
+    MMD (oracle/_ref/libmmd_ref.so, built from src/ordmmd.F and friends) when that
+    library exists, else the Python restatement, then the Python chain above.
+    Returns the arrays the numeric oracle takes plus the reference's statistics
+    (flops = sum of squared fundamental column counts, symPACKMatrix2D.hpp:3009-3016)."""
+    from . import mmd_reference
+    order_fn = None
+    if mmd_reference.OUT_SO.exists():
+        order_fn = lambda nn, x, a: mmd_reference.ordmmd(nn, np.asarray(x, np.int32), np.asarray(a, np.int32))
+    d = symbolic_chain(n, colptr, rowind, "MMD", order_fn=order_fn)
+    sym = dict(xsuper=d["xsuper"], xlindx=d["xlindx"], lindx=d["lindx"], supmember=d["supmember"], invp=d["invp"])
+    return sym, d["flops_stat"], d["nnzL_stat"]

@@ -1327,9 +1327,10 @@ int spb_get_status(spb_handle* h, int32_t* code, int32_t* supernode, int32_t* co
 //
 // spb_solve_device lazily grows the handle's right-hand-side workspace with
 // cudaMalloc when a call asks for more right-hand sides than before.  Some
-// callers cannot let that happen: code that runs while a CUDA graph is being
-// captured in global mode (where cudaMalloc is an illegal call), and services
-// that pin their device-memory budget up front.  spb_solve_device_noalloc
+// callers cannot let that happen: services that reserve their device-memory
+// budget up front (another allocator owns the rest of the GPU, so an allocation
+// in mid-request could fail), and latency-critical callers for which cudaMalloc
+// and cudaFree may synchronize the device.  spb_solve_device_noalloc
 // gives them the same solve with its scratch (permuted right-hand sides and
 // the dependency counters of the persistent sweeps) in one file-scope
 // __device__ array, so no call allocates or frees anything.

@@ -55,6 +55,7 @@ class Request:
     t_done: float = 0.0
     batched: int = 1                   # requests in the solve this one ran in
     refactored: bool = False           # solve against an evicted factor: factored again
+    need: int = 0                      # predicted device bytes of its factorization (0 = not yet known)
     future: Future = field(default_factory=Future, repr=False)
 
     @property
@@ -242,7 +243,8 @@ class SolverService:
 
     def _admit(self) -> list:
         """Start what fits: first the solves whose factor is cached (short jobs, right-hand
-        sides merged per factor; they leave one slot free while a factorization waits),
+        sides merged per factor; they leave one slot free while a factorization that could
+        start now waits),
         then factorizations, each class in arrival order; factorizations are capped at
         max_factor_inflight slots."""
         jobs = []
@@ -253,11 +255,35 @@ class SolverService:
         self.stats["max_inflight"] = max(self.stats["max_inflight"], self._inflight)
         return jobs
 
+    def _factor_need(self, req: Request):
+        """(matrix, pattern key, analysed handle, predicted bytes) of a waiting factorization
+        (fresh matrix or refactor of an evicted factor) whose pattern analysis is done, else None."""
+        A, key = (req.matrix, self._pattern_key(req.matrix)) if req.kind == "factor_solve" else self._evicted[req.factor_id]
+        fut = self._patterns.get(key)
+        if fut is None or not fut.done() or fut.exception() is not None:
+            return None
+        T = fut.result()
+        if not req.need:
+            req.need = T.PredictDeviceBytes(self.precision, req.nrhs) + ALLOC_SLACK
+        return A, key, T, req.need
+
+    def _factor_could_start(self, req: Request) -> bool:
+        """A waiting factorization that would start now if a slot were free: its analysis is
+        done, its id is not being factored, the factorization cap has room and its predicted
+        footprint fits the memory budget."""
+        fid = req.factor_id
+        if req.kind == "solve" and (fid in self._factors or fid not in self._evicted):
+            return False
+        if fid in self._pending_ids or self._factor_inflight >= self.max_factor_inflight:
+            return False
+        got = self._factor_need(req)
+        return got is not None and got[3] <= self.memory_budget
+
     def _admit_pass(self, jobs: list, solves: bool) -> None:
         factor_blocked = False  # a factorization waits for memory: later ones may not pass it
         limit = self.max_inflight
-        if solves and any(r.kind != "solve" or r.factor_id not in self._factors for r in self._waiting):
-            limit -= 1  # a waiting factorization keeps one slot: a stream of solves cannot starve it
+        if solves and any(self._factor_could_start(r) for r in self._waiting):
+            limit -= 1  # a factorization ready to start keeps one slot: a stream of solves cannot starve it
         for req in list(self._waiting):
             if self._inflight + len(jobs) >= limit:
                 break
@@ -318,8 +344,12 @@ class SolverService:
                 self._waiting.remove(req)
                 req.future.set_exception(fut.exception())
                 continue
-            T = fut.result()
-            need = T.PredictDeviceBytes(self.precision, req.nrhs) + ALLOC_SLACK
+            _, _, T, need = self._factor_need(req)
+            if need > self.memory_budget:  # could never fit: fail now instead of waiting forever
+                self._waiting.remove(req)
+                req.future.set_exception(MemoryError(
+                    f"factor {fid!r} needs {need} device bytes, above the memory budget of {self.memory_budget}"))
+                continue
             if not self._evict(need):
                 factor_blocked = True
                 continue

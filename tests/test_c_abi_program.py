@@ -101,12 +101,19 @@ int main() {
     if (c + k < n) { A.Localg_.rowind.push_back(c + k + 1); A.nzvalLocal.push_back(-1.0); }
   }
   A.Localg_.colptr.push_back((long long)A.Localg_.rowind.size() + 1);
-  spb_options o;
-  spb_default_options(&o);
-  o.device = -1;
+  // options set the way run_sympack2D sets the reference's symPACKOptions
+  sympack_b200::symPACKOptions optionsFact;
+  optionsFact.orderingStr = "MMD";
+  optionsFact.relax.SetMaxSize(0);
+  optionsFact.decomposition = sympack_b200::DecompositionType::LL;
+  optionsFact.device = -1;
   sympack_b200::symPACKMatrix2D M;
-  M.Init(o);
+  M.Init(optionsFact);
   M.SymbolicFactorization(A);
+  bool bad_ordering = false;
+  sympack_b200::symPACKOptions bad;
+  bad.orderingStr = "SCOTCH";
+  try { sympack_b200::symPACKMatrix2D B; B.Init(bad); } catch (const std::logic_error&) { bad_ordering = true; }
   std::vector<int> invp;
   std::vector<int> perm = M.GetOrdering(&invp);
   std::vector<int> xsuper = M.GetSupernodalPartition();
@@ -116,7 +123,7 @@ int main() {
   std::printf("%d %zu %lld %d\n", M.info().nsuper, xsuper.size(), check, parent[n - 1]);
   bool threw = false;
   try { M.Factorize(); } catch (const std::runtime_error&) { threw = true; }  // host-only handle
-  std::printf("%d\n", threw ? 1 : 0);
+  std::printf("%d %d\n", threw ? 1 : 0, bad_ordering ? 1 : 0);
   return 0;
 }
 """
@@ -145,6 +152,7 @@ def test_cpp_class_over_the_library(tmp_path):
     assert int(out[2]) == int(np.sum(np.arange(1, n + 1, dtype=np.int64) * invp))
     assert int(out[3]) == M.GetETree()[-1]
     assert out[4] == "1"
+    assert out[5] == "1"  # an ordering the solver does not have is a logic_error, as in the reference
 
 
 CPP_DEVICE_PROGRAM = r"""
@@ -169,15 +177,13 @@ int main() {
   A.Localg_.colptr.push_back((long long)A.Localg_.rowind.size() + 1);
   std::vector<double> b(n * nrhs), x(n * nrhs, 0.0);
   for (int i = 0; i < n * nrhs; ++i) b[i] = std::sin(0.37 * i);
-  spb_options o;
-  spb_default_options(&o);
-  o.device = 0;
+  sympack_b200::symPACKOptions optionsFact;  // device 0, FP64, MMD
   sympack_b200::symPACKMatrix2D M;
-  M.Init(o);
+  M.Init(optionsFact);
   M.SymbolicFactorization(A);
   M.DistributeMatrix(A);
   M.Factorize();
-  M.Solve(b.data(), nrhs);
+  M.Solve(b.data(), nrhs, n, nullptr);  // symPACKMatrixMeta::Solve(RHS, nrhs, rhs_size, Xptr)
   M.GetSolution(x.data(), nrhs);
   // residual ||A x - b|| / ||b|| with the symmetric matrix from its lower triangle
   double rn = 0.0, bn = 0.0;

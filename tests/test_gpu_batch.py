@@ -72,6 +72,46 @@ def test_batch_fp64_matches_single_and_oracle(nrhs):
     M.close()
 
 
+def test_batch_of_200_named_systems_each_matches_its_own_oracle():
+    """200 systems of the batching workload's generator (n log-uniform in [500, 20000],
+    Laplacians and random graphs, seed 0) factored as one batch; every system's solution
+    is checked against an oracle factorization of that system alone (its own analysis)
+    within 1e-12, beside the reference's residual metric (driver/utils.hpp:136-140)."""
+    systems = G.batch_systems(200, 500, 20000, seed=0)
+    M, A, offs = batch_factor(systems)
+    b = np.random.default_rng(4).standard_normal((A.size, 2))
+    M.Solve(b)
+    x = M.GetSolution(nrhs=2)
+    M.close()
+
+    def alone(s):  # host-only analysis of one system by itself (the C calls release the GIL)
+        As = DistSparseMatrix.from_lower_csc(*s)
+        T = symPACKMatrix2D()
+        T.Init(symPACKOptions(device=-1))
+        T.SymbolicFactorization(As)
+        xl, li = T.GetStructure()
+        sym = dict(xsuper=T.GetSupernodalPartition(), xlindx=xl, lindx=li, supmember=T.GetSupMembership(),
+                   invp=T.GetOrdering()[1])
+        T.close()
+        return As, sym
+
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(os.cpu_count()) as ex:
+        analyses = list(ex.map(alone, systems))
+    worst = 0.0
+    for k, (As, sym) in enumerate(analyses):
+        lo, hi = int(offs[k]), int(offs[k + 1])
+        f = numeric.OracleFactor(As.size, sym, threads=os.cpu_count())
+        f.distribute(As.colptr, As.rowind, As.nzvalLocal)
+        f.factorize()
+        bk = np.ascontiguousarray(b[lo:hi])
+        err = rel(x[lo:hi], f.solve(bk))
+        worst = max(worst, err)
+        assert err <= 1e-12, (k, As.size, err)
+        assert np.linalg.norm(As.matvec(x[lo:hi]) - bk) / np.linalg.norm(bk) < 1e-12, k
+    assert worst <= 1e-12
+
+
 def test_batch_fp32_ir_reaches_backward_error():
     systems = G.batch_systems(20, 60, 3000, seed=11)
     M, A, offs = batch_factor(systems, precision="FP32_IR")

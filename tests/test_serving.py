@@ -185,3 +185,45 @@ def test_cached_solves_are_admitted_before_waiting_factorizations(fake):
     svc.close()
     assert order.index(fs) < len(futs)  # finished before the last factorization
     assert svc.stats["max_inflight"] <= 3
+
+
+def test_one_slot_serves_cached_solves_and_factorizations(fake):
+    """max_inflight=1 (so one factorization slot at most): cached solves and new
+    factorizations mixed in one queue all finish; neither class starves the other."""
+    rng = np.random.default_rng(4)
+    A0 = lap(8, 0.5)
+    svc = S.SolverService(memory_budget=1 << 30, max_inflight=1)
+    svc.submit(S.Request("factor_solve", "a", rng.standard_normal(A0.size), matrix=A0)).result(timeout=30)
+    mats = {f"g{i}": lap(7 + i, 0.3) for i in range(3)}
+    futs, checks = [], []
+    for i in range(12):
+        b = rng.standard_normal(A0.size)
+        futs.append(svc.submit(S.Request("solve", "a", b)))
+        checks.append((A0, b))
+        if i % 4 == 0:
+            fid = f"g{i // 4}"
+            b2 = rng.standard_normal(mats[fid].size)
+            futs.append(svc.submit(S.Request("factor_solve", fid, b2, matrix=mats[fid])))
+            checks.append((mats[fid], b2))
+    for f, (A, b) in zip(futs, checks):
+        assert np.allclose(f.result(timeout=60).x, dense_solve(A, b), rtol=1e-12, atol=1e-12)
+    svc.close()
+    assert svc.stats["max_inflight"] == 1
+
+
+def test_oversized_factorization_fails_at_once_and_solves_go_on(fake):
+    """A factorization whose predicted footprint exceeds the whole budget is refused
+    with MemoryError instead of holding the queue; cached solves keep running."""
+    rng = np.random.default_rng(5)
+    A0 = lap(6, 0.5)
+    big = lap(30, 0.5)  # 8 n^2 bytes = 6.5 MB, above the budget below
+    svc = S.SolverService(memory_budget=(4 << 20) + 200_000, max_inflight=2)
+    svc.submit(S.Request("factor_solve", "a", rng.standard_normal(A0.size), matrix=A0)).result(timeout=30)
+    fb = svc.submit(S.Request("factor_solve", "big", rng.standard_normal(big.size), matrix=big))
+    bs = [rng.standard_normal(A0.size) for _ in range(6)]
+    fs = [svc.submit(S.Request("solve", "a", b)) for b in bs]
+    with pytest.raises(MemoryError):
+        fb.result(timeout=30)
+    for f, b in zip(fs, bs):
+        assert np.allclose(f.result(timeout=30).x, dense_solve(A0, b), rtol=1e-12, atol=1e-12)
+    svc.close()

@@ -1,12 +1,14 @@
 """Allocation-free solve entry point (spb_solve_device_noalloc).
 
-It exists for callers that cannot allocate device memory when they solve — for
-example code running inside a CUDA graph capture in global mode, where
-cudaMalloc is an illegal call, or a service with a fixed device-memory budget.
-Its scratch lives in a static device array instead of a cudaMalloc'd workspace.
-These tests call it through the C ABI and compare it with spb_solve_device on
-two calls in a row (the shared array keeps the previous call's contents), and
-check that oversize requests are refused.  This file is collected last."""
+It exists for callers that cannot allocate device memory when they solve — a
+service whose device memory is reserved up front and owned by another
+allocator, where a cudaMalloc in mid-request could fail, or a latency-critical
+caller, for which cudaMalloc may synchronize the device.  Its scratch lives in
+a static device array instead of a cudaMalloc'd workspace.  These tests call it
+through the C ABI and compare it with spb_solve_device on two calls in a row
+(the shared array keeps the previous call's contents), with more than 64
+right-hand sides (two passes over the counters) also against the CPU oracle,
+and check that oversize requests are refused.  This file is collected last."""
 import ctypes as C
 
 import numpy as np
@@ -44,6 +46,35 @@ def test_noalloc_solve_matches_solve_device_twice():
         assert rc == 0, lib.spb_last_error(M._h).decode()
         ref, new = X_ref.cpu().numpy(), X_new.cpu().numpy()
         assert np.max(np.abs(new - ref)) <= TOL * np.max(np.abs(ref))
+
+
+def test_noalloc_solve_beyond_64_columns_matches_solve_device_and_oracle():
+    """nrhs = 70 runs the sweeps twice (64 + 6 columns): the counters are cleared
+    between the passes and the second pass works on the array past column 64."""
+    import torch
+    from oracle import numeric
+    n, cp, ri, v = G.stencil27(12, 12, 12, 1e-2, seed=7)
+    M = factored(n, cp, ri, v)
+    lib = N.load()
+    rng = np.random.default_rng(12)
+    perm, invp = M.GetOrdering()
+    xl, li = M.GetStructure()
+    sym = dict(xsuper=M.GetSupernodalPartition(), xlindx=xl, lindx=li, supmember=M.GetSupMembership(), invp=invp)
+    f = numeric.OracleFactor(n, sym, threads=4)
+    f.distribute(cp, ri, v)
+    f.factorize()
+    for nrhs in (70, 130):  # two calls in a row: 2 and 3 passes
+        Bh = rng.standard_normal((n, nrhs))
+        B = torch.from_numpy(np.ascontiguousarray(Bh.T)).cuda()  # column-major n x nrhs
+        X_ref = torch.empty_like(B)
+        X_new = torch.full_like(B, float("nan"))
+        assert lib.spb_solve_device(M._h, C.c_void_p(B.data_ptr()), C.c_void_p(X_ref.data_ptr()), nrhs, n) == 0
+        rc = lib.spb_solve_device_noalloc(M._h, C.c_void_p(B.data_ptr()), C.c_void_p(X_new.data_ptr()), nrhs, n)
+        assert rc == 0, lib.spb_last_error(M._h).decode()
+        ref, new = X_ref.cpu().numpy().T, X_new.cpu().numpy().T
+        assert np.max(np.abs(new - ref)) <= TOL * np.max(np.abs(ref))
+        xo = f.solve(Bh)
+        assert np.max(np.abs(new - xo)) <= TOL * np.max(np.abs(xo))
 
 
 def test_noalloc_rejects_requests_beyond_its_scratch():
