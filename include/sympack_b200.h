@@ -88,10 +88,11 @@ typedef struct spb_options {
   int decomposition;       /* SPB_DECOMPOSITION_* (symPACKOptions::decomposition, Types.hpp:97,119) */
   int plan_outer_nb;       /* columns per outer block of a wide panel: its trailing columns are
                               updated once per outer block (0 = default 256; multiple of 64, <= 4096) */
-  int plan_dense_min_w;    /* narrowest root supernode (no off-diagonal rows, alone at the top of the
-                              tree) whose solves of <= 4 right-hand sides run in one thread-block
-                              cluster (0 = default: never, < 0 = never) */
-  int plan_solve_chunk;    /* column blocks per forward off-diagonal solve task (0 = default 16) */
+  int plan_dense_min_w;    /* no effect (a former cluster solve of the root, replaced by the
+                              super-block solve); kept for layout */
+  int plan_solve_chunk;    /* 64-column blocks per solve super-block: a supernode wider than one block
+                              is solved through the inverses of its diagonal super-blocks (0 = default 8) */
+  int plan_solve_tiles;    /* 64 x 64 tiles per super-block solve task (0 = default 2) */
 } spb_options;
 
 typedef struct spb_info {
@@ -111,9 +112,9 @@ typedef struct spb_info {
   int32_t ir_iterations;   /* refinement steps of the last solve */
   int32_t factor_launches; /* kernels in the factorization graph */
   double backward_error;   /* componentwise-free backward error of the last solve, if computed */
-  int32_t dense_root_width; /* columns of the root solved in one thread-block cluster when a solve
-                               has <= 4 right-hand sides (0 = none): one more launch per sweep */
+  int32_t dense_root_width; /* always 0 (a former cluster solve of the root; kept for layout) */
   int32_t pad_;
+  int64_t inverse_bytes;    /* device bytes of the diagonal super-block inverses of one operand */
 } spb_info;
 
 void spb_default_options(spb_options* opt);
@@ -172,9 +173,9 @@ int spb_solve_device(spb_handle* h, const double* d_rhs, double* d_x, int32_t nr
  * other streams.  spb_solve_device may grow its workspace with cudaMalloc on a
  * call with more right-hand sides than before; this entry point calls no
  * cudaMalloc, cudaFree or allocating library routine: its scratch (the permuted
- * right-hand sides and the dependency counters) lives in one static __device__
- * array of 33 MiB that every GPU which loads the library holds until the
- * process exits.
+ * right-hand sides, the forward solution and the dependency counters) lives in
+ * one static __device__ array of 65 MiB that every GPU which loads the library
+ * holds until the process exits.
  * Limits: n * nrhs <= 4,194,304, and 2 + 3 * nsuper + 2 * (number of
  * 64-column blocks over all supernodes) <= 262,144 dependency counters;
  * larger requests return SPB_ERR_INVALID with a message saying so.
@@ -183,7 +184,9 @@ int spb_solve_device(spb_handle* h, const double* d_rhs, double* d_x, int32_t nr
  * Every call on a device shares the array: calls whose work overlaps on the GPU
  * (other handles or streams) race, so serialize them.  The counters are cleared
  * on every call (and for every 64 right-hand sides); nothing else is kept
- * between calls.  Like spb_solve_device, the call reads the device status word
+ * between calls.  The first call after a factorization also computes the
+ * factor's diagonal super-block inverses, in memory the handle allocated with
+ * its analysis.  Like spb_solve_device, the call reads the device status word
  * back before it returns, so it waits for the handle's stream. */
 int spb_solve_device_noalloc(spb_handle* h, const double* d_rhs, double* d_x, int32_t nrhs, int64_t ld);
 
@@ -234,7 +237,8 @@ int spb_set_stream(spb_handle* h, void* stream);
 #define SPB_KIND_GEMM_DMMA 5
 #define SPB_KIND_SOLVE_FORWARD 6
 #define SPB_KIND_SOLVE_BACKWARD 7
-#define SPB_KIND_COUNT 8
+#define SPB_KIND_SOLVE_INVERSE 8  /* diagonal super-block inverses (first solve after a factorization) */
+#define SPB_KIND_COUNT 9
 typedef struct spb_profile {
   double ms[SPB_KIND_COUNT];
   double flops[SPB_KIND_COUNT];

@@ -51,6 +51,7 @@ class spb_options(C.Structure):
         ("plan_outer_nb", C.c_int),
         ("plan_dense_min_w", C.c_int),
         ("plan_solve_chunk", C.c_int),
+        ("plan_solve_tiles", C.c_int),
     ]
 
 
@@ -74,19 +75,20 @@ class spb_info(C.Structure):
         ("backward_error", C.c_double),
         ("dense_root_width", C.c_int32),
         ("pad_", C.c_int32),
+        ("inverse_bytes", C.c_int64),
     ]
 
 
 KIND_NAMES = ["assemble", "factor_small", "potrf_diag", "trsm_rows", "gemm_simt", "gemm_dmma",
-              "solve_forward", "solve_backward"]
+              "solve_forward", "solve_backward", "solve_inverse"]
 
 
 class spb_profile(C.Structure):
     _fields_ = [
-        ("ms", C.c_double * 8),
-        ("flops", C.c_double * 8),
-        ("bytes", C.c_double * 8),
-        ("launches", C.c_int32 * 8),
+        ("ms", C.c_double * 9),
+        ("flops", C.c_double * 9),
+        ("bytes", C.c_double * 9),
+        ("launches", C.c_int32 * 9),
     ]
 
 

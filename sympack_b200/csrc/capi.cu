@@ -65,7 +65,11 @@ struct spb_handle {
   spb::SolveTask* dbwd = nullptr;
   int32_t* dexpected = nullptr;
   int32_t* dsparent = nullptr;
-  int32_t* dsync = nullptr;  // [fwd counter, bwd counter, arrived[ns], fwd blkdone[ns], bwd blkdone[ns]]
+  int32_t* dsync = nullptr;  // solve counters (spb::solve_sync_ints)
+  void* dInv = nullptr;      // diagonal super-block inverses of the forward operand (L, or L D for LDL^T)
+  void* dInvB = nullptr;     // LDL^T: inverses of the backward operand (unit L); else dInv
+  spb::InvItem* dinvitems = nullptr;
+  bool inv_stale = true;     // inverses not yet computed for the current factor
   Status* dstatus = nullptr;
   // precision form: original matrix as full CSR (FP64) and refinement buffers
   std::vector<int64_t> csr_rowptr;
@@ -85,8 +89,9 @@ struct spb_handle {
   int ir_iterations = 0;
   double backward_error = -1.0;
   double* dX = nullptr;
+  double* dZ = nullptr;  // solve: forward solution / backward right-hand side (permuted)
   double* dB = nullptr;
-  int64_t x_cap = 0;  // doubles available in dX and dB
+  int64_t x_cap = 0;  // doubles available in dX, dZ and dB
   int x_nrhs = 0;
   int64_t device_bytes = 0;
   cudaGraphExec_t fgraph = nullptr;
@@ -95,6 +100,7 @@ struct spb_handle {
   long long wait_limit = 1LL << 24;  // ~2 s of polling per device wait
   int stall_supernode = -1;          // test hook: extra expected arrival nobody delivers
   bool profiling = false;
+  bool prof_inverse = false;  // the last profiled solve computed the super-block inverses
   unsigned long long* dtrace = nullptr;  // profiled solves: 4 per task of each sweep (forward, backward)
   spb_profile prof{};
   std::vector<cudaEvent_t> events;
@@ -147,7 +153,8 @@ void release_device(spb_handle* h) {
   h->device_bytes = 0;
   h->dL = nullptr;
   h->dW = nullptr;
-  h->dX = h->dB = h->dR = h->dD = h->dXo = nullptr;
+  h->dX = h->dZ = h->dB = h->dR = h->dD = h->dXo = nullptr;
+  h->dInv = h->dInvB = nullptr;
   h->d_rowseg = nullptr;
   h->dtrace = nullptr;
   h->x_cap = 0;
@@ -330,7 +337,7 @@ int ensure_rhs_capacity(spb_handle* h, int nrhs) {
   }
   int64_t need = (int64_t)h->sym.n * nrhs;
   if (need <= h->x_cap) return SPB_OK;
-  for (double** p : {&h->dX, &h->dB, &h->dR, &h->dD, &h->dXo}) {
+  for (double** p : {&h->dX, &h->dZ, &h->dB, &h->dR, &h->dD, &h->dXo}) {
     if (*p) {
       auto it = std::find(h->allocs.begin(), h->allocs.end(), (void*)*p);
       if (it != h->allocs.end()) h->allocs.erase(it);
@@ -342,6 +349,7 @@ int ensure_rhs_capacity(spb_handle* h, int nrhs) {
   }
   h->x_cap = 0;
   SPB_CK(h, dalloc(h, &h->dX, need));
+  SPB_CK(h, dalloc(h, &h->dZ, need));
   SPB_CK(h, dalloc(h, &h->dB, need));
   if (h->fp32) {
     SPB_CK(h, dalloc(h, &h->dR, need));
@@ -353,58 +361,86 @@ int ensure_rhs_capacity(spb_handle* h, int nrhs) {
   return SPB_OK;
 }
 
-// Forward and backward persistent sweeps on the permuted X (n x nrhs, ld n),
-// 64 right-hand sides per pass.
-void enqueue_solve(spb_handle* h, int nrhs) {
+// Diagonal super-block inverses of the current factor, computed by the first solve
+// after a factorization.
+void ensure_inverses(spb_handle* h) {
+  if (!h->inv_stale) return;
+  const spb::Plan& P = h->plan;
+  const int count = (int)P.inv_items.size();
+  spb::dev::launch_sb_inverse(h->stream, h->ldl ? (const void*)h->dW : h->dL, h->dInv, h->fp32, h->dmeta,
+                              h->dinvitems, count, P.solve_sb);
+  if (h->ldl) spb::dev::launch_sb_inverse(h->stream, h->dL, h->dInvB, false, h->dmeta, h->dinvitems, count, P.solve_sb);
+  h->inv_stale = false;
+}
+
+// Forward and backward persistent sweeps on the permuted right-hand sides X (n x nrhs,
+// ld n; the solution replaces them), with Z (same shape) between the sweeps and the
+// counters in sync; 64 right-hand sides per pass.  prof: record the per-pass events.
+void enqueue_sweeps(spb_handle* h, double* X, double* Z, int32_t* sync, int nrhs, bool prof) {
   const spb::Plan& P = h->plan;
   const int ns = P.nsuper;
-  // per-pass events of a profiled solve (every caller, the refinement loop included)
-  const bool prof = h->profiling && ensure_events(h, 4 * (size_t)((nrhs + 63) / 64)) == cudaSuccess;
   for (int c0 = 0; c0 < nrhs; c0 += 64) {
-    cudaMemsetAsync(h->dsync, 0, sizeof(int32_t) * spb::solve_sync_ints(P), h->stream);
+    // counters must start at zero
+    cudaMemsetAsync(sync, 0, sizeof(int32_t) * spb::solve_sync_ints(P), h->stream);
     spb::dev::PSolveArgs a{};
     // LDL^T: the forward sweep solves with L D (diagonal D), the backward one with unit L
     a.L = h->ldl ? (void*)h->dW : h->dL;
+    a.Inv = h->dInv;
     a.fp32 = h->fp32;
     a.meta = h->dmeta;
     a.rows = h->drows;
     a.supmember = h->dsupm;
     a.sparent = h->dsparent;
-    a.X = h->dX + (int64_t)c0 * h->sym.n;
+    a.row_group = h->drowgrp;
+    a.groups = h->dgroups;
+    a.X = X + (int64_t)c0 * h->sym.n;
+    a.Z = Z + (int64_t)c0 * h->sym.n;
     a.ldx = h->sym.n;
     a.nrhs = std::min(64, nrhs - c0);
     a.expected = h->dexpected;
-    a.arrived = h->dsync + 2;
+    a.arrived = sync + 2;
     a.status = h->dstatus;
     a.spin_limit = h->wait_limit;
+    a.sb = P.solve_sb;
+    a.tpt = P.solve_tpt;
     const size_t e0 = 4 * (size_t)(c0 / 64);
-    // dense root in one cluster: the persistent sweeps skip its tasks (the last forward
-    // ones, the first backward ones)
-    const bool dense = P.dense_root >= 0 && spb::dev::dense_solve_available(a.nrhs, P.meta[P.dense_root].w);
-    const int dfw = dense ? P.dense_fwd_tasks : 0, dbw = dense ? P.dense_bwd_tasks : 0;
     a.tasks = h->dfwd;
-    a.ntasks = (int)P.fwd_tasks.size() - dfw;
-    a.counter = h->dsync;
-    a.blkdone = h->dsync + 2 + ns;
-    a.upd = h->dsync + 2 + 3 * (size_t)ns;
-    a.chunk = P.solve_chunk;
+    a.ntasks = (int)P.fwd_tasks.size();
+    a.counter = sync;
+    a.blkdone = sync + 2 + ns;
+    a.upd = sync + 2 + 3 * (size_t)ns;
     a.trace = prof ? h->dtrace : nullptr;
+    const size_t pass_bytes = sizeof(double) * (size_t)h->sym.n * a.nrhs;
     if (prof) cudaEventRecord(h->events[e0], h->stream);
+    cudaMemsetAsync(a.Z, 0, pass_bytes, h->stream);  // DI tasks of wide supernodes add into Z
     spb::dev::launch_solve_persistent(h->stream, a, true);
-    if (dense) spb::dev::launch_solve_dense(h->stream, a, P.dense_root, P.meta[P.dense_root].w, true);
     if (prof) cudaEventRecord(h->events[e0 + 1], h->stream);
     a.L = h->dL;
-    a.tasks = h->dbwd + dbw;
-    a.ntasks = (int)P.bwd_tasks.size() - dbw;
-    a.counter = h->dsync + 1;
-    a.blkdone = h->dsync + 2 + 2 * ns;
-    a.upd = h->dsync + 2 + 3 * (size_t)ns + P.nblk_total;
-    a.trace = prof && h->dtrace ? h->dtrace + 4 * (P.fwd_tasks.size() + dbw) : nullptr;
+    a.Inv = h->ldl ? h->dInvB : h->dInv;
+    a.tasks = h->dbwd;
+    a.ntasks = (int)P.bwd_tasks.size();
+    a.counter = sync + 1;
+    a.blkdone = sync + 2 + 2 * ns;
+    a.upd = sync + 2 + 3 * (size_t)ns + P.nsb_total;
+    a.trace = prof && h->dtrace ? h->dtrace + 4 * P.fwd_tasks.size() : nullptr;
     if (prof) cudaEventRecord(h->events[e0 + 2], h->stream);
-    if (dense) spb::dev::launch_solve_dense(h->stream, a, P.dense_root, P.meta[P.dense_root].w, false);
+    cudaMemsetAsync(a.X, 0, pass_bytes, h->stream);  // the backward DI tasks add into X
     spb::dev::launch_solve_persistent(h->stream, a, false);
     if (prof) cudaEventRecord(h->events[e0 + 3], h->stream);
   }
+}
+
+// Both sweeps on the handle's workspace h->dX (n x nrhs, ld n), inverses first if stale.
+void enqueue_solve(spb_handle* h, int nrhs) {
+  // per-pass events of a profiled solve (every caller, the refinement loop included)
+  const bool prof = h->profiling && ensure_events(h, 4 * (size_t)((nrhs + 63) / 64) + 2) == cudaSuccess;
+  const size_t ie = 4 * (size_t)((nrhs + 63) / 64);
+  const bool inv = h->inv_stale;
+  if (prof) cudaEventRecord(h->events[ie], h->stream);
+  ensure_inverses(h);
+  if (prof) cudaEventRecord(h->events[ie + 1], h->stream);
+  h->prof_inverse = prof && inv;
+  enqueue_sweeps(h, h->dX, h->dZ, h->dsync, nrhs, prof);
 }
 
 // Per-sweep device times of the last profiled solve.
@@ -412,6 +448,16 @@ int collect_solve_profile(spb_handle* h, int nrhs) {
   if (!h->profiling) return SPB_OK;
   SPB_CK(h, cudaStreamSynchronize(h->stream));
   clear_kinds(h, SPB_KIND_SOLVE_FORWARD, SPB_KIND_SOLVE_BACKWARD);
+  h->prof.ms[SPB_KIND_SOLVE_INVERSE] = 0.0;
+  h->prof.launches[SPB_KIND_SOLVE_INVERSE] = 0;
+  h->prof.flops[SPB_KIND_SOLVE_INVERSE] = 0.0;
+  if (h->prof_inverse) {  // the first solve after a factorization computed the inverses
+    const size_t ie = 4 * (size_t)((nrhs + 63) / 64);
+    float ms = 0.f;
+    SPB_CK(h, cudaEventElapsedTime(&ms, h->events[ie], h->events[ie + 1]));
+    h->prof.ms[SPB_KIND_SOLVE_INVERSE] = ms;
+    h->prof.launches[SPB_KIND_SOLVE_INVERSE] = h->ldl ? 2 : 1;
+  }
   for (int c0 = 0, i = 0; c0 < nrhs; c0 += 64, ++i) {
     float f = 0.f, b = 0.f;
     SPB_CK(h, cudaEventElapsedTime(&f, h->events[4 * i], h->events[4 * i + 1]));
@@ -421,10 +467,8 @@ int collect_solve_profile(spb_handle* h, int nrhs) {
     h->prof.ms[SPB_KIND_SOLVE_BACKWARD] += b;
     h->prof.bytes[SPB_KIND_SOLVE_FORWARD] += h->plan.solve_sweep_bytes + rhs_bytes;
     h->prof.bytes[SPB_KIND_SOLVE_BACKWARD] += h->plan.solve_sweep_bytes + rhs_bytes;
-    const int dense = h->plan.dense_root >= 0 &&
-                      spb::dev::dense_solve_available(std::min(64, nrhs - c0), h->plan.meta[h->plan.dense_root].w);
-    h->prof.launches[SPB_KIND_SOLVE_FORWARD] += 1 + dense;
-    h->prof.launches[SPB_KIND_SOLVE_BACKWARD] += 1 + dense;
+    h->prof.launches[SPB_KIND_SOLVE_FORWARD] += 1;
+    h->prof.launches[SPB_KIND_SOLVE_BACKWARD] += 1;
   }
   return SPB_OK;
 }
@@ -626,8 +670,8 @@ spb::PlanParams plan_params_of(const spb_options& o) {
   if (o.plan_small_max_w > 0) pp.small_max_w = o.plan_small_max_w;
   if (o.plan_big_tile_rows > 0) pp.big_tile_rows = o.plan_big_tile_rows;
   if (o.plan_outer_nb > 0) pp.outer_nb = o.plan_outer_nb;
-  if (o.plan_dense_min_w != 0) pp.dense_min_w = o.plan_dense_min_w < 0 ? 0 : o.plan_dense_min_w;
-  if (o.plan_solve_chunk > 0) pp.solve_chunk = o.plan_solve_chunk;
+  if (o.plan_solve_chunk > 0) pp.solve_sb = o.plan_solve_chunk;
+  if (o.plan_solve_tiles > 0) pp.solve_tpt = o.plan_solve_tiles;
   return pp;
 }
 
@@ -667,6 +711,8 @@ int64_t predict_bytes(const spb_handle* h, bool fp32, int nrhs) {
   t += b(P.tile_items.size(), sizeof(spb::TileItem)) + b(n, 4) + b(ns, 4);
   t += b(P.fwd_tasks.size(), sizeof(spb::SolveTask)) + b(P.bwd_tasks.size(), sizeof(spb::SolveTask));
   t += b(P.fwd_pending.size(), 4) + b(P.sparent.size(), 4) + b((int64_t)spb::solve_sync_ints(P), 4);
+  t += b(P.inv_elems, fp32 ? sizeof(float) : sizeof(double)) + b(P.inv_items.size(), sizeof(spb::InvItem));
+  if (h->opt.decomposition == SPB_DECOMPOSITION_LDL) t += b(P.inv_elems, sizeof(double));
   t += b(1, sizeof(Status));
   if (fp32) {
     int64_t offdiag = 0;
@@ -677,7 +723,7 @@ int64_t predict_bytes(const spb_handle* h, bool fp32, int nrhs) {
     t += b(1 + (int64_t)num_segments(h) * (1 + 3 * 64), 8);
     if (!h->seg_off.empty()) t += b(n, 4);
   }
-  if (nrhs > 0) t += (fp32 ? 5 : 2) * b(n * nrhs, 8);
+  if (nrhs > 0) t += (fp32 ? 6 : 3) * b(n * nrhs, 8);
   return t;
 }
 
@@ -742,6 +788,20 @@ int install_device(spb_handle* h) {
   SPB_CK(h, dalloc(h, &h->dexpected, P.fwd_pending.size()));
   SPB_CK(h, dalloc(h, &h->dsparent, P.sparent.size()));
   SPB_CK(h, dalloc(h, &h->dsync, spb::solve_sync_ints(P)));
+  {
+    unsigned char* inv = nullptr;
+    SPB_CK(h, dalloc(h, &inv, (size_t)P.inv_elems * h->elem));
+    h->dInv = inv;
+  }
+  SPB_CK(h, dalloc(h, &h->dinvitems, P.inv_items.size()));
+  if (h->ldl) {
+    double* invb = nullptr;
+    SPB_CK(h, dalloc(h, &invb, (size_t)P.inv_elems));
+    h->dInvB = invb;
+  } else {
+    h->dInvB = h->dInv;
+  }
+  h->inv_stale = true;
   SPB_CK(h, dalloc(h, &h->dstatus, 1));
   SPB_CK(h, cudaStreamSynchronize(h->own_stream));  // allocations ready before h->stream uses them
   auto up = [&](void* d, const void* s, size_t bytes) {
@@ -763,6 +823,7 @@ int install_device(spb_handle* h) {
   SPB_CK(h, up(h->dbwd, P.bwd_tasks.data(), P.bwd_tasks.size() * sizeof(spb::SolveTask)));
   SPB_CK(h, up(h->dexpected, P.fwd_pending.data(), P.fwd_pending.size() * 4));
   SPB_CK(h, up(h->dsparent, P.sparent.data(), P.sparent.size() * 4));
+  SPB_CK(h, up(h->dinvitems, P.inv_items.data(), P.inv_items.size() * sizeof(spb::InvItem)));
   SPB_CK(h, cudaMemsetAsync(h->dstatus, 0, sizeof(Status), h->stream));
   if (h->fp32) {
     // full symmetric CSR of A in the original ordering; csr_src maps each entry to its input value
@@ -855,8 +916,7 @@ int spb_symbolic_from(spb_handle* h, const spb_handle* src) {
     h->nnz_a = src->nnz_a;
     h->colptr = src->colptr;
     h->rowind = src->rowind;
-    if (plan_params_of(h->opt).small_max_w == plan_params_of(src->opt).small_max_w &&
-        plan_params_of(h->opt).big_tile_rows == plan_params_of(src->opt).big_tile_rows) {
+    if (plan_params_of(h->opt) == plan_params_of(src->opt)) {  // same tunables: the same plan
       h->plan = src->plan;
       h->amap = src->amap;
     } else {
@@ -1031,6 +1091,7 @@ int spb_factorize(spb_handle* h) {
   SPB_CK(h, cudaMemcpyAsync(&st, h->dstatus, sizeof(st), cudaMemcpyDeviceToHost, h->stream));
   SPB_CK(h, cudaStreamSynchronize(h->stream));
   h->factored = true;
+  h->inv_stale = true;
   if (st.code == 1) {
     char msg[128];
     if (h->ldl)
@@ -1054,7 +1115,7 @@ int spb_solve_device(spb_handle* h, const double* d_rhs, double* d_x, int32_t nr
   int rc = ensure_rhs_capacity(h, nrhs);
   if (rc) return rc;
   if (h->fp32) return ir_solve(h, d_rhs, ld, d_x, ld, nrhs);
-  if (h->profiling) SPB_CK(h, ensure_events(h, 4 * (size_t)((nrhs + 63) / 64)));
+  if (h->profiling) SPB_CK(h, ensure_events(h, 4 * (size_t)((nrhs + 63) / 64) + 2));
   spb::dev::launch_permute_in(h->stream, h->dX, n, d_rhs, ld, h->dinvp0, n, nrhs);
   enqueue_solve(h, nrhs);
   rc = collect_solve_profile(h, nrhs);
@@ -1138,10 +1199,8 @@ int spb_get_info(spb_handle* h, spb_info* info) {
   info->ncells = (int32_t)h->cells.cells.size();
   info->nblocks = (int32_t)h->cells.block_first_row.size();
   info->factor_launches = (int32_t)P.steps.size();
-  info->dense_root_width =
-      P.dense_root >= 0 && h->device >= 0 && spb::dev::dense_solve_available(1, P.meta[P.dense_root].w)
-          ? P.meta[P.dense_root].w
-          : 0;
+  info->dense_root_width = 0;  // the cluster root solve gave way to the super-block solve
+  info->inverse_bytes = P.inv_elems * (int64_t)(h->opt.precision == SPB_PRECISION_FP32_IR ? 4 : 8);
   info->ir_iterations = h->ir_iterations;
   info->backward_error = h->backward_error;
   return SPB_OK;
@@ -1331,8 +1390,8 @@ int spb_get_status(spb_handle* h, int32_t* code, int32_t* supernode, int32_t* co
 // budget up front (another allocator owns the rest of the GPU, so an allocation
 // in mid-request could fail), and latency-critical callers for which cudaMalloc
 // and cudaFree may synchronize the device.  spb_solve_device_noalloc
-// gives them the same solve with its scratch (permuted right-hand sides and
-// the dependency counters of the persistent sweeps) in one file-scope
+// gives them the same solve with its scratch (permuted right-hand sides, the
+// forward solution and the dependency counters of the persistent sweeps) in one file-scope
 // __device__ array, so no call allocates or frees anything.
 // ---------------------------------------------------------------------------
 namespace {
@@ -1341,8 +1400,9 @@ constexpr size_t kNoAllocXBytes = (size_t)32 << 20;   // permuted right-hand sid
 constexpr size_t kNoAllocSyncBytes = (size_t)1 << 20; // counters of the sweeps: 256 Ki int32
 constexpr int kNoAllocMaxDevices = 64;
 
-// Held by every GPU that loads this library until the process exits (33 MiB).
-static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocXBytes + kNoAllocSyncBytes];
+// Held by every GPU that loads this library until the process exits (65 MiB): the
+// permuted right-hand sides X, the forward solution Z (same size) and the counters.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[2 * kNoAllocXBytes + kNoAllocSyncBytes];
 
 std::mutex g_noalloc_mutex;
 void* g_noalloc_addr[kNoAllocMaxDevices] = {};  // device address of g_noalloc_scratch, per device
@@ -1370,14 +1430,13 @@ extern "C" int spb_solve_device_noalloc(spb_handle* h, const double* d_rhs, doub
   if (h->device < 0) return fail(h, SPB_ERR_STATE, "host-only handle (device < 0) has no numeric phase");
   if (!h->factored) return fail(h, SPB_ERR_STATE, "solve: call spb_factorize first");
   const int n = h->sym.n;
-  const int ns = h->plan.nsuper;
   if (nrhs <= 0 || ld < n || !d_rhs || !d_x) return fail(h, SPB_ERR_INVALID, "solve: bad right-hand side");
   if (h->device >= kNoAllocMaxDevices) return fail(h, SPB_ERR_INVALID, "solve_noalloc: device ordinal >= 64");
   if (h->fp32) return fail(h, SPB_ERR_STATE, "solve_noalloc: refinement (FP32_IR) needs workspace; use spb_solve_device");
   if ((size_t)n * (size_t)nrhs * sizeof(double) > kNoAllocXBytes) {
     char msg[160];
     snprintf(msg, sizeof msg, "solve_noalloc: n * nrhs = %lld exceeds the %zu right-hand-side entries of the "
-             "static scratch (32 MiB)", (long long)n * nrhs, kNoAllocXBytes / sizeof(double));
+             "static scratch (2 x 32 MiB)", (long long)n * nrhs, kNoAllocXBytes / sizeof(double));
     return fail(h, SPB_ERR_INVALID, msg);
   }
   if (spb::solve_sync_ints(h->plan) * sizeof(int32_t) > kNoAllocSyncBytes)
@@ -1389,45 +1448,11 @@ extern "C" int spb_solve_device_noalloc(spb_handle* h, const double* d_rhs, doub
   int rc = noalloc_scratch(h, &base);
   if (rc) return rc;
   double* X = reinterpret_cast<double*>(base);
-  int32_t* sync = reinterpret_cast<int32_t*>(base + kNoAllocXBytes);
-  const spb::Plan& P = h->plan;
+  double* Z = reinterpret_cast<double*>(base + kNoAllocXBytes);
+  int32_t* sync = reinterpret_cast<int32_t*>(base + 2 * kNoAllocXBytes);
   spb::dev::launch_permute_in(h->stream, X, n, d_rhs, ld, h->dinvp0, n, nrhs);
-  for (int c0 = 0; c0 < nrhs; c0 += 64) {
-    // counters must start at zero; the array keeps whatever the last call left
-    SPB_CK(h, cudaMemsetAsync(sync, 0, sizeof(int32_t) * spb::solve_sync_ints(P), h->stream));
-    spb::dev::PSolveArgs a{};
-    a.L = h->ldl ? (void*)h->dW : h->dL;  // LDL^T: forward with L D, backward with unit L
-    a.fp32 = h->fp32;
-    a.meta = h->dmeta;
-    a.rows = h->drows;
-    a.supmember = h->dsupm;
-    a.sparent = h->dsparent;
-    a.X = X + (int64_t)c0 * n;
-    a.ldx = n;
-    a.nrhs = std::min(64, nrhs - c0);
-    a.expected = h->dexpected;
-    a.arrived = sync + 2;
-    a.status = h->dstatus;
-    a.spin_limit = h->wait_limit;
-    const bool dense = P.dense_root >= 0 && spb::dev::dense_solve_available(a.nrhs, P.meta[P.dense_root].w);
-    const int dfw = dense ? P.dense_fwd_tasks : 0, dbw = dense ? P.dense_bwd_tasks : 0;
-    a.tasks = h->dfwd;
-    a.ntasks = (int)P.fwd_tasks.size() - dfw;
-    a.counter = sync;
-    a.blkdone = sync + 2 + ns;
-    a.upd = sync + 2 + 3 * (size_t)ns;
-    a.chunk = P.solve_chunk;
-    spb::dev::launch_solve_persistent(h->stream, a, true);
-    if (dense) spb::dev::launch_solve_dense(h->stream, a, P.dense_root, P.meta[P.dense_root].w, true);
-    a.L = h->dL;
-    a.tasks = h->dbwd + dbw;
-    a.ntasks = (int)P.bwd_tasks.size() - dbw;
-    a.counter = sync + 1;
-    a.blkdone = sync + 2 + 2 * ns;
-    a.upd = sync + 2 + 3 * (size_t)ns + P.nblk_total;
-    if (dense) spb::dev::launch_solve_dense(h->stream, a, P.dense_root, P.meta[P.dense_root].w, false);
-    spb::dev::launch_solve_persistent(h->stream, a, false);
-  }
+  ensure_inverses(h);  // the first solve after a factorization computes them (arena of the analysis)
+  enqueue_sweeps(h, X, Z, sync, nrhs, false);
   spb::dev::launch_permute_out(h->stream, d_x, ld, X, n, h->dinvp0, n, nrhs);
   SPB_CK(h, cudaGetLastError());
   return check_solve_status(h);

@@ -53,37 +53,42 @@ void launch_gemm(cudaStream_t st, const FactorArgs& a, const TileItem* items, in
 // Solves work on the permuted right-hand sides X (n x nrhs, column-major, leading dimension ldx).
 
 // Persistent sweeps (one launch each).  counter, arrived, blkdone and upd must
-// be zero at launch; expected[s] is the number of forward off-diagonal (tile, column
-// block) tasks that write rows of supernode s.
+// be zero at launch; expected[s] is the number of forward arrivals (off-diagonal
+// task, target) that write rows of supernode s.  Forward: Y = X (accumulated),
+// solution to Z; backward: Z (accumulated), solution to X.
 struct PSolveArgs {
-  const void* L;     // factor arena (double, or float when fp32)
+  const void* L;     // factor arena (double, or float when fp32): L, or L D for the LDL^T forward sweep
+  const void* Inv;   // diagonal super-block inverses of that operand (same type)
   bool fp32;
   const SnMeta* meta;
   const int32_t* rows;
   const int32_t* supmember;
   const int32_t* sparent;
+  const int32_t* row_group;  // relative-index group of each row-list entry (arrival targets)
+  const RelGroup* groups;
   double* X;
-  int64_t ldx;
+  double* Z;
+  int64_t ldx;       // leading dimension of X and Z
   int nrhs;  // <= 64
   const SolveTask* tasks;
   int ntasks;
   int32_t* counter;
   const int32_t* expected;
   int32_t* arrived;
-  int32_t* blkdone;
-  int32_t* upd;      // per 64-column block: updates landed (meta.boff + block)
-  int chunk;         // column blocks per forward off-diagonal task (Plan::solve_chunk)
+  int32_t* blkdone;  // per supernode: finished diagonal tasks of this sweep
+  int32_t* upd;      // per super-block (meta.sboff + p): updates landed
+  int sb;            // 64-column blocks per super-block (Plan::solve_sb)
+  int tpt;           // tiles per DI / U / V / O / W task (Plan::solve_tpt)
   Status* status;
   long long spin_limit;  // polls (about 128 ns apart) before a wait gives up
   unsigned long long* trace;  // optional, 4 per task: grabbed, dependencies met, done (ns), s << 8 | kind
 };
 void init_solve_attributes();
 void launch_solve_persistent(cudaStream_t st, const PSolveArgs& a, bool forward);
-// Dense root (Plan::dense_root) solved by one thread-block cluster, for nrhs <= 4:
-// forward after the persistent forward sweep (which skips the root's tasks), backward
-// before the persistent backward sweep (it marks the root done in a.blkdone).
-bool dense_solve_available(int nrhs, int w);  // w: the root's width (its blocks' accumulators fit?)
-void launch_solve_dense(cudaStream_t st, const PSolveArgs& a, int s, int w, bool forward);
+// Inverses of the diagonal super-blocks of L (the whole list of items, Plan::inv_items),
+// written to Inv in 64 x 64 tiles at meta.ioff.
+void launch_sb_inverse(cudaStream_t st, const void* L, void* Inv, bool fp32, const SnMeta* meta,
+                       const InvItem* items, int count, int sb);
 
 // Precision form (FP64 refinement): gather CSR values, residual r = b - A x,
 // per-column max |v| (out zeroed by the caller), max row sum of |A|, x += d.

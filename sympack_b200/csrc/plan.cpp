@@ -29,7 +29,8 @@ Plan build_plan(const Symbolic& sym, const PlanParams& prm) {
     m.off = off;
     m.lidx = sym.xlindx[s] - 1;
     m.boff = P.nblk_total;
-    m.pad = 0;
+    m.sboff = 0;
+    m.ioff = -1;
     P.nblk_total += (m.w + 63) / 64;
     off += round_up((int64_t)m.ld * m.w, 32);
   }
@@ -261,82 +262,103 @@ Plan build_plan(const Symbolic& sym, const PlanParams& prm) {
   }
   for (const SnMeta& m : P.meta) P.solve_sweep_bytes += 8.0 * m.h * m.w;
 
+  // Solve super-blocks: per supernode, its first super-block counter and (for
+  // supernodes wider than one block) the offset of its inverse tiles.
+  const int SB = std::max(1, prm.solve_sb);
+  const int TPT = std::max(1, prm.solve_tpt);
+  P.solve_sb = SB;
+  P.solve_tpt = TPT;
+  auto nblk_of = [&](int s) { return (P.meta[s].w + 63) / 64; };
+  auto nsb_of = [&](int s) { return (nblk_of(s) + SB - 1) / SB; };
+  auto nb_in = [&](int s, int p) { return std::min(SB, nblk_of(s) - p * SB); };
+  for (int s = 0; s < ns; ++s) {
+    SnMeta& m = P.meta[s];
+    m.sboff = P.nsb_total;
+    P.nsb_total += nsb_of(s);
+    if (nblk_of(s) > 1) {
+      m.ioff = P.inv_elems;
+      for (int p = 0; p < nsb_of(s); ++p) {
+        P.inv_elems += inv_tiles(nb_in(s, p)) * 4096;
+        for (int j = 0; j < nb_in(s, p); ++j) P.inv_items.push_back(InvItem{s, p, j, 0});
+      }
+    }
+  }
+  // Longest inverse items first (column block 0 of a full super-block has the most tiles).
+  std::stable_sort(P.inv_items.begin(), P.inv_items.end(), [&](const InvItem& x, const InvItem& y) {
+    return nb_in(x.s, x.p) - x.j > nb_in(y.s, y.p) - y.j;
+  });
+
   // Persistent solve task lists, ordered by elimination-tree height level
   // (forward: leaves first; backward: root level first) so that tasks handed
-  // out together are independent.  Within a supernode the sweep is
-  // right-looking by 64-column blocks: a finished diagonal block releases its
-  // updates of every later block at once, so the per-supernode critical path
-  // is one block solve plus one block update per block.
-  // The supernodes of a level advance together: tasks are dealt block by block across
-  // the level (block 0 of every supernode, then block 1, ...), so sibling chains run side
-  // by side instead of one supernode's tasks filling every CTA before the next starts.
-  // Forward off-diagonal work is one task per (row tile, chunk of solve_chunk column
-  // blocks), dealt right after the chunk's last diagonal block: it barely waits and never
-  // holds a CTA across a supernode's whole chain, and its atomic scatter into the
-  // ancestors' rows happens once per chunk.
-  const int chunk = std::max(1, prm.solve_chunk);
-  P.solve_chunk = chunk;
+  // out together are independent.  The supernodes of a level advance together:
+  // tasks are dealt super-block by super-block across the level, so sibling
+  // supernodes run side by side.  Within a super-block the tasks on the critical
+  // path come first: the DI tasks, then the updates of the next super-block, then
+  // the other updates and the off-diagonal tiles.  A task covers up to TPT tiles.
+  auto chunks = [&](std::vector<SolveTask>& out, int s, int kind, int p, int t, int q_begin, int q_end) {
+    for (int q0 = q_begin; q0 < q_end; q0 += TPT) out.push_back(SolveTask{s, kind, pack_task_i(p, q0 - q_begin), t});
+  };
   P.fwd_pending.assign(ns, 0);
   for (int L = 0; L < H; ++L) {
-    int maxblk = 0;
-    for (int s : P.level_sn[L]) maxblk = std::max(maxblk, (P.meta[s].w + 63) / 64);
-    for (int i = 0; i < maxblk; ++i)
+    int maxsb = 0;
+    for (int s : P.level_sn[L]) maxsb = std::max(maxsb, nsb_of(s));
+    for (int p = 0; p < maxsb; ++p)
       for (int s : P.level_sn[L]) {
         const SnMeta& m = P.meta[s];
-        const int nblk = (m.w + 63) / 64, noff = (m.h - m.w + 63) / 64;
-        if (i >= nblk) continue;
-        if (nblk == 1 && noff <= kSolveFusedTiles) {  // the whole supernode in one task
-          P.fwd_tasks.push_back(SolveTask{s, 4, 0, 0});
+        const int nblk = nblk_of(s), noff = (m.h - m.w + 63) / 64;
+        if (p >= nsb_of(s)) continue;
+        if (nblk == 1) {
+          if (noff <= kSolveFusedTiles) {  // the whole supernode in one task
+            P.fwd_tasks.push_back(SolveTask{s, 4, 0, 0});
+          } else {
+            P.fwd_tasks.push_back(SolveTask{s, 0, 0, 0});
+            for (int u = 0; u < noff; ++u) P.fwd_tasks.push_back(SolveTask{s, 2, 0, u});
+          }
           continue;
         }
-        P.fwd_tasks.push_back(SolveTask{s, 0, i, i});
-        for (int t = i + 2; t < nblk; ++t) P.fwd_tasks.push_back(SolveTask{s, 1, i, t});
-        if ((i + 1) % chunk == 0 || i == nblk - 1)
-          for (int u = 0; u < noff; ++u) P.fwd_tasks.push_back(SolveTask{s, 2, i / chunk * chunk, u});
+        const int nb = nb_in(s, p);
+        for (int r = 0; r < nb; ++r) chunks(P.fwd_tasks, s, 5, p, r, 0, r + 1);
+        for (int t = (p + 1) * SB; t < nblk; ++t) chunks(P.fwd_tasks, s, 1, p, t, 0, nb);
+        for (int u = 0; u < noff; ++u) chunks(P.fwd_tasks, s, 2, p, u, 0, nb);
       }
+    // arrivals: one per (off-diagonal task, target supernode of its tile)
     for (int s : P.level_sn[L]) {
       const SnMeta& m = P.meta[s];
-      const int nblk = (m.w + 63) / 64, noff = (m.h - m.w + 63) / 64, nchunk = (nblk + chunk - 1) / chunk;
+      const int noff = (m.h - m.w + 63) / 64;
+      int nsrc = 0;
+      for (int p = 0; p < nsb_of(s); ++p) nsrc += solve_ntask(nb_in(s, p), TPT);
       for (int u = 0; u < noff; ++u) {
         int r0 = m.w + 64 * u, r1 = std::min(m.h, r0 + 64), last = -1;
         for (int r = r0; r < r1; ++r) {
           int t = P.supmember0[P.rows[m.lidx + r]];
-          if (t != last) P.fwd_pending[t] += nchunk;  // one arrival per chunk
+          if (t != last) P.fwd_pending[t] += nsrc;
           last = t;
         }
       }
     }
   }
   for (int L = H - 1; L >= 0; --L) {
-    int maxblk = 0;
-    for (int s : P.level_sn[L]) maxblk = std::max(maxblk, (P.meta[s].w + 63) / 64);
-    for (int j = 0; j < maxblk; ++j)
+    int maxsb = 0;
+    for (int s : P.level_sn[L]) maxsb = std::max(maxsb, nsb_of(s));
+    for (int j = 0; j < maxsb; ++j)
       for (int s : P.level_sn[L]) {
         const SnMeta& m = P.meta[s];
-        const int nblk = (m.w + 63) / 64, noff = (m.h - m.w + 63) / 64;
-        if (j >= nblk) continue;
-        if (nblk == 1 && noff <= kSolveFusedTiles) {
-          P.bwd_tasks.push_back(SolveTask{s, 4, 0, 0});
+        const int nblk = nblk_of(s), noff = (m.h - m.w + 63) / 64, nsb = nsb_of(s);
+        if (j >= nsb) continue;
+        if (nblk == 1) {
+          if (noff <= kSolveFusedTiles) {
+            P.bwd_tasks.push_back(SolveTask{s, 4, 0, 0});
+          } else {
+            for (int u = 0; u < noff; ++u) P.bwd_tasks.push_back(SolveTask{s, 3, 0, u});
+            P.bwd_tasks.push_back(SolveTask{s, 0, 0, 0});
+          }
           continue;
         }
-        if (j == 0)
-          for (int u = 0; u < noff; ++u) P.bwd_tasks.push_back(SolveTask{s, 3, 0, u});
-        const int t = nblk - 1 - j;
-        P.bwd_tasks.push_back(SolveTask{s, 0, t, t});
-        for (int u = 0; u + 2 <= t; ++u) P.bwd_tasks.push_back(SolveTask{s, 1, t, u});
+        const int p = nsb - 1 - j, nb = nb_in(s, p);  // super-blocks from the last one down
+        for (int u = 0; u < noff; ++u) chunks(P.bwd_tasks, s, 3, p, u, 0, nb);
+        for (int r = nb - 1; r >= 0; --r) chunks(P.bwd_tasks, s, 5, p, r, 0, nb - r);
+        for (int t = p * SB - 1; t >= 0; --t) chunks(P.bwd_tasks, s, 1, p, t, 0, nb);
       }
-  }
-  if (prm.dense_min_w > 0 && H > 0 && P.level_sn[H - 1].size() == 1) {
-    const int s = P.level_sn[H - 1][0];
-    const SnMeta& m = P.meta[s];
-    if (m.h == m.w && m.w >= prm.dense_min_w) {
-      int32_t nf = 0, nbw = 0;
-      while (nf < (int32_t)P.fwd_tasks.size() && P.fwd_tasks[P.fwd_tasks.size() - 1 - nf].s == s) ++nf;
-      while (nbw < (int32_t)P.bwd_tasks.size() && P.bwd_tasks[nbw].s == s) ++nbw;
-      P.dense_root = s;
-      P.dense_fwd_tasks = nf;
-      P.dense_bwd_tasks = nbw;
-    }
   }
   return P;
 }

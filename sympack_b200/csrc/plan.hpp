@@ -31,8 +31,9 @@ struct SnMeta {
   int32_t ld;    // leading dimension of the panel
   int64_t off;   // element offset of the panel in the factor arena
   int64_t lidx;  // offset of this supernode's row list in the device row array
-  int32_t boff;  // first of this supernode's 64-column blocks in the per-block solve counters
-  int32_t pad;
+  int32_t boff;  // first of this supernode's 64-column blocks over all supernodes
+  int32_t sboff; // first of this supernode's solve super-blocks in the per-super-block solve counters
+  int64_t ioff;  // element offset of its diagonal super-block inverses in the inverse arena (-1: none)
 };
 
 // One tile of a Schur-complement product  C = A * B^T  over panel columns
@@ -84,28 +85,79 @@ struct PanelItem {
   int32_t slot;   // scratch slot holding this step's L11^-1 for the supernode
 };
 
-// One task of the persistent triangular solves, in 64-row / 64-column units
-// (i, t: column blocks of supernode s; u: 64-row tile below the diagonal block).
-//   forward  kind 0  D(t):    X_t <- L_tt^-1 X_t once every update into block t
-//                             has landed, then X_{t+1} -= L_{t+1,t} X_t
-//            kind 1  U(i, t): X_t -= L_ti X_i                 (t >= i + 2, after D(i))
-//            kind 2  O(i0, u): X[rows of tile u] -= sum_i L_ui X_i over a chunk of column blocks
-//                             from i0, scattered to the ancestors (after the chunk's last D)
-//            kind 4  F:       a supernode of one block and at most kSolveFusedTiles off-diagonal
-//                             tiles whole: D(0), then every tile's scatter
-//   backward kind 4  G:       the same supernode whole: every tile's X_0 -= L_u0^T X_u, then B(0)
-//   backward kind 3  W(u):    X_t -= L_ut^T X[rows of tile u] for every block t
-//                             (ancestor rows, final once the parent is done)
-//            kind 0  B(t):    X_t <- L_tt^-T X_t once every update into block t
-//                             has landed, then X_{t-1} -= L_{t,t-1}^T X_t
-//            kind 1  V(t, u): X_u -= L_tu^T X_t                 (u <= t - 2, after B(t))
+// One task of the persistent triangular solves.  A supernode of one 64-column block
+// is solved by substitution; a wider one is cut into super-blocks of sb 64-column
+// blocks (the last one shorter), and the diagonal triangle of every super-block p is
+// applied through its inverse Inv_p (computed once per factorization, in 64 x 64
+// tiles), so a super-block costs two parallel steps instead of a chain of sb block
+// solves.  Forward (permuted right-hand sides Y in, solution of L y = b in Z):
+//            kind 4  F:        one-block supernode with at most kSolveFusedTiles
+//                              off-diagonal tiles, whole: Z_0 <- L_00^-1 Y_0, then every
+//                              tile's Y[ancestor rows] -= L_u0 Z_0
+//            kind 0  D:        one-block supernode: Z_0 <- L_00^-1 Y_0
+//            kind 5  DI(p, r): Z[block r of p] <- sum_{q <= r} Inv_p(r, q) Y[block q of p]
+//                              once the descendants' and earlier super-blocks' updates landed
+//            kind 1  U(p, t):  Y[block t] -= L(t, super-block p) Z[p]   (t in a later super-block)
+//            kind 2  O(p, u):  Y[rows of off-diagonal tile u] -= L(u, super-block p) Z[p],
+//                              scattered into the ancestors' rows
+// Backward (Z in, solution X):
+//            kind 4  G:        the F supernode whole: Z_0 -= L_u0^T X[ancestor rows of u] for
+//                              every tile, then X_0 <- L_00^-T Z_0
+//            kind 3  W(p, u):  Z[p] -= L(u, super-block p)^T X[ancestor rows of tile u]
+//                              (final once the parent is done)
+//            kind 0  B:        one-block supernode: X_0 <- L_00^-T Z_0
+//            kind 5  DI(p, r): X[block r of p] <- sum_{q >= r} Inv_p(q, r)^T Z[block q of p]
+//            kind 1  V(p, t):  Z[block t] -= L(super-block p, t)^T X[p]   (t in an earlier super-block)
 // Task lists are topological: every task a task waits on comes earlier.
+// DI, U, V, O and W tasks each cover at most tpt of their 64 x 64 tiles (the first one
+// q0), adding their part atomically, so that a step of a wide supernode's chain is
+// spread over many CTAs.
 struct SolveTask {
   int32_t s;
   int32_t kind;
-  int32_t i;
-  int32_t t;
+  int32_t i;  // super-block p (DI, U, V, O, W) | first tile q0 << 24
+  int32_t t;  // block r within p (DI), target block t (U, V) or tile u (O, W)
 };
+inline int32_t pack_task_i(int p, int q0) { return p | (q0 << 24); }
+
+// Task counts of the super-block solve (host and device): tasks of a run of `tiles`
+// tiles, and the DI tasks of a super-block of nb blocks (sum over its rows r of the
+// tasks of r + 1 tiles; the same sum counts the backward rows of nb - r tiles).
+#ifdef __CUDACC__
+#define SPB_HD __host__ __device__
+#else
+#define SPB_HD
+#endif
+SPB_HD inline int solve_ntask(int tiles, int tpt) { return (tiles + tpt - 1) / tpt; }
+SPB_HD inline int solve_di_tasks(int nb, int tpt) {
+  int c = 0;
+  for (int r = 0; r < nb; ++r) c += solve_ntask(r + 1, tpt);
+  return c;
+}
+// DI tasks of super-blocks p0 .. p1 - 1 of a supernode of nblk blocks.
+SPB_HD inline int solve_di_range(int nblk, int sb, int tpt, int p0, int p1) {
+  const int nsb = (nblk + sb - 1) / sb, nlast = nblk - (nsb - 1) * sb;
+  int c = 0;
+  for (int p = p0; p < p1; ++p) c += solve_di_tasks(p == nsb - 1 ? nlast : sb, tpt);
+  return c;
+}
+// Diagonal tasks that mark a supernode done in a sweep (the count its blkdone reaches).
+SPB_HD inline int solve_done_count(int w, int sb, int tpt) {
+  const int nblk = (w + 63) / 64;
+  return nblk == 1 ? 1 : solve_di_range(nblk, sb, tpt, 0, (nblk + sb - 1) / sb);
+}
+
+// One CTA of the super-block inverse kernel: column block j of Inv_p of supernode s
+// (tiles (i, j), i = j .. nb_p - 1).
+struct InvItem {
+  int32_t s;
+  int32_t p;
+  int32_t j;
+  int32_t pad;
+};
+
+// 64 x 64 tiles of the inverse of a super-block of nb blocks (lower triangle of tiles).
+inline int64_t inv_tiles(int nb) { return (int64_t)nb * (nb + 1) / 2; }
 
 // Relative indices of the external updates (the src_to_tgt_offset maps of
 // symPACKMatrix2D.hpp:1395-1466, computed once per structure instead of per
@@ -147,14 +199,13 @@ struct Plan {
   // and per supernode the number of forward off-diagonal tiles writing its rows
   std::vector<SolveTask> fwd_tasks, bwd_tasks;
   std::vector<int32_t> fwd_pending;
-  int32_t nblk_total = 0;  // 64-column blocks over all supernodes (per-block solve counters)
-  // Dense root: the only supernode of the top level, with no off-diagonal rows and at
-  // least PlanParams::dense_min_w columns, is solved by one thread-block cluster
-  // (few right-hand sides); its tasks are the last dense_fwd_tasks forward tasks and the
-  // first dense_bwd_tasks backward tasks, which the persistent sweeps then skip.
-  int32_t dense_root = -1;
-  int32_t dense_fwd_tasks = 0, dense_bwd_tasks = 0;
-  int32_t solve_chunk = 16;  // column blocks per forward off-diagonal task O(i0, u): blocks i0 .. i0 + chunk - 1
+  int32_t nblk_total = 0;  // 64-column blocks over all supernodes
+  int32_t nsb_total = 0;   // solve super-blocks over all supernodes (per-super-block counters)
+  int32_t solve_sb = 8;    // 64-column blocks per solve super-block
+  int32_t solve_tpt = 2;   // 64 x 64 tiles per DI / U / V / O / W task
+  // diagonal super-block inverses: arena size (elements) and one item per (super-block, column block)
+  int64_t inv_elems = 0;
+  std::vector<InvItem> inv_items;
   // algorithmic bytes of one sweep: every panel element read once
   double solve_sweep_bytes = 0.0;
 };
@@ -170,18 +221,23 @@ struct PlanParams {
   int nb = 64;                   // column block of the blocked panel factorization
   int outer_nb = 256;            // outer block: the trailing columns are updated once per outer block
   int big_tile_rows = 128;       // products with at least this many rows use 128 x 128 tensor-core tiles
-  int dense_min_w = 0;           // narrowest root solved by the cluster kernel (0 = never; measured
-                                 // slower than the persistent sweep so far, kept as an option)
-  int solve_chunk = 16;          // column blocks per forward off-diagonal solve task
+  int solve_sb = 8;              // 64-column blocks per solve super-block (>= 1)
+  int solve_tpt = 2;             // 64 x 64 tiles per DI / U / V / O / W solve task (>= 1)
   int sms = 148;                 // SMs of the device: a launch with too few tiles to fill them
                                  // splits its tiles' K range (partial products add atomically)
+  bool operator==(const PlanParams& o) const {
+    return small_max_w == o.small_max_w && small_max_bytes == o.small_max_bytes && nb == o.nb &&
+           outer_nb == o.outer_nb && big_tile_rows == o.big_tile_rows && solve_sb == o.solve_sb &&
+           solve_tpt == o.solve_tpt && sms == o.sms;
+  }
 };
 
 Plan build_plan(const Symbolic& s, const PlanParams& p = PlanParams());
 
 // int32 counters one persistent solve pass uses: two task counters, then per
-// supernode arrivals and forward / backward done-blocks, then per 64-column
-// block forward / backward update counts.
+// supernode arrivals and forward / backward done blocks, then per super-block
+// forward / backward update counts.  Sized by 64-column blocks (at least as many
+// as super-blocks).
 inline size_t solve_sync_ints(const Plan& P) { return 2 + 3 * (size_t)P.nsuper + 2 * (size_t)P.nblk_total; }
 
 // Destination of each entry of A's lower triangle (input order) in the arena,

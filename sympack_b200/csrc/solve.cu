@@ -9,8 +9,18 @@
 // persistent launch per sweep: CTAs take tasks from an atomic counter in a
 // topological order (every dependency of a task was handed out earlier, so a
 // waiting CTA only ever waits on CTAs that are already running) and
-// synchronise through per-supernode counters in global memory.  Every wait is
-// bounded; on expiry the kernel records SPB timeout status and all CTAs leave.
+// synchronise through counters in global memory.  Every wait is bounded; on
+// expiry the kernel records SPB timeout status and all CTAs leave.
+//
+// A supernode wider than one 64-column block is split into super-blocks of sb
+// blocks.  The diagonal triangle of a super-block is applied through its
+// inverse (k_sb_inverse, once per factorization), so the sb dependent block
+// solves of a substitution become sb independent row-block products: the chain
+// of a wide supernode has two steps per super-block (its DI products, then the
+// updates of the next super-block) instead of one per 64 columns.  The forward
+// sweep reads the permuted right-hand sides Y (accumulating the descendants'
+// contributions there) and writes its solution to Z; the backward sweep
+// accumulates into Z and writes the final solution X.
 #include "kernels.cuh"
 
 namespace spb {
@@ -19,10 +29,10 @@ namespace dev {
 namespace {
 
 constexpr int kT = 64;         // rows / columns per task unit
-constexpr int kPld = 65;       // padded leading dimension of the staged L block
+constexpr int kPld = 65;       // padded leading dimension of a staged 64 x 64 tile
 constexpr int kThreads = 256;
-// staged L block (64 x 65), a second 64 x 64 block (X rows or the next L block), and
-// the accumulator of kR right-hand sides; kR = 16 keeps three CTAs per SM
+// staged tile (64 x 65), right-hand-side staging (64 x 64), and the accumulator of kR
+// right-hand sides; kR = 16 keeps three CTAs per SM
 template <int kR>
 constexpr size_t solve_smem() { return (size_t)(kT * kPld + kT * kT + kT * kR) * sizeof(double); }
 template <int kR>
@@ -41,7 +51,7 @@ __device__ __forceinline__ int ld_acquire(const int32_t* p) {
   return v;
 }
 
-// Counter increment with release semantics: after a barrier, one thread's release
+// Counter increment with release semantics: after a barrier, a thread's release
 // publishes the whole block's earlier writes to any thread that acquires the counter.
 __device__ __forceinline__ void red_release(int32_t* p, int v) {
   asm volatile("red.release.gpu.global.add.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
@@ -75,20 +85,38 @@ __device__ bool wait_geq(const int32_t* flag, int target, Status* st, int s, int
   return r != 0;
 }
 
-// acc[i + c*kT] (+/-)= sum_k A[i + k*kPld] * B[k + c*kT]   for i < m, c < nr, k < kk
-template <bool kSub>
-__device__ __forceinline__ void block_gemv(double* acc, const double* A, const double* B, int m, int kk, int nr) {
-  for (int idx = threadIdx.x; idx < m * nr; idx += kThreads) {
-    int c = idx / m, i = idx - c * m;
-    double s = 0.0;
-    for (int k = 0; k < kk; ++k) s = fma(A[i + k * kPld], B[k + c * kT], s);
-    if (kSub) acc[i + c * kT] -= s;
-    else acc[i + c * kT] += s;
+// A 64 x 64 tile of T (column-major, leading dimension ld; rows < m and columns < kk
+// valid, zero elsewhere) held in registers, 16 entries per thread, so that the next
+// tile's loads are in flight while the current one is used.
+template <class T>
+struct TileRegs {
+  static constexpr int kPer = kT * kT / kThreads;
+  T v[kPer];
+  __device__ __forceinline__ void load(const T* P, int64_t ld, int m, int kk) {
+    if (m == kT && kk == kT) {
+#pragma unroll
+      for (int q = 0; q < kPer; ++q) {
+        const int idx = threadIdx.x + q * kThreads, k = idx >> 6, r = idx & 63;
+        v[q] = P[r + (int64_t)k * ld];
+      }
+      return;
+    }
+#pragma unroll
+    for (int q = 0; q < kPer; ++q) {
+      const int idx = threadIdx.x + q * kThreads, k = idx >> 6, r = idx & 63;
+      v[q] = (r < m && k < kk) ? P[r + (int64_t)k * ld] : T(0);
+    }
   }
-}
+  __device__ __forceinline__ void store(double* A) const {
+#pragma unroll
+    for (int q = 0; q < kPer; ++q) {
+      const int idx = threadIdx.x + q * kThreads, k = idx >> 6, r = idx & 63;
+      A[r + k * kPld] = (double)v[q];
+    }
+  }
+};
 
 // Stage L rows [r0, r0+m) x columns [c0, c0+kk) of a panel into A (ld kPld), widened to FP64.
-// A full 64 x 64 block is loaded with all 16 loads of a thread in flight.
 template <class T, int kLd = kPld>
 __device__ __forceinline__ void stage_block(double* A, const T* P, int64_t ld, int r0, int m, int c0, int kk) {
   if (m == kT && kk == kT) {
@@ -111,19 +139,41 @@ __device__ __forceinline__ void stage_block(double* A, const T* P, int64_t ld, i
   }
 }
 
-// Stage X rows x0.. (contiguous) or rows rl[0..] (gathered) into B (ld kT), through L2.
-__device__ __forceinline__ void stage_x(double* B, const double* X, int64_t ldx, int x0, const int32_t* rl, int m,
-                                        int nr) {
+// Stage X rows x0.. (contiguous) or rows rl[0..] (gathered) into B (leading dimension
+// ldb), through L2.
+__device__ __forceinline__ void stage_x(double* B, int ldb, const double* X, int64_t ldx, int x0, const int32_t* rl,
+                                        int m, int nr) {
   for (int idx = threadIdx.x; idx < m * nr; idx += kThreads) {
     int c = idx / m, r = idx - c * m;
     int row = rl ? rl[r] : x0 + r;
-    B[r + c * kT] = __ldcg(X + row + c * ldx);
+    B[r + c * ldb] = __ldcg(X + row + c * ldx);
   }
 }
 
-}  // namespace
-
-namespace {
+// acc[i + c*kT] += sum_{k < kk} A(i, k) B[k + c*ldb]  for i < m, c < nr, with
+// A(i, k) = A[i + k*kPld] (kTrans false) or A[k + i*kPld] (kTrans true).  Few outputs
+// (one right-hand side): four threads per output and a shuffle reduction.
+template <bool kTrans>
+__device__ __forceinline__ void tile_gemv(double* acc, const double* A, const double* B, int ldb, int m, int kk,
+                                          int nr) {
+  if (m * nr * 4 <= kThreads) {
+    const int idx = threadIdx.x >> 2, part = threadIdx.x & 3;
+    const int c = idx / m, i = idx - c * m;
+    double s = 0.0;
+    if (idx < m * nr)
+      for (int k = part; k < kk; k += 4) s = fma(kTrans ? A[k + i * kPld] : A[i + k * kPld], B[k + c * ldb], s);
+    s += __shfl_xor_sync(0xffffffffu, s, 1);
+    s += __shfl_xor_sync(0xffffffffu, s, 2);
+    if (idx < m * nr && part == 0) acc[i + c * kT] += s;
+    return;
+  }
+  for (int idx = threadIdx.x; idx < m * nr; idx += kThreads) {
+    const int c = idx / m, i = idx - c * m;
+    double s = 0.0;
+    for (int k = 0; k < kk; ++k) s = fma(kTrans ? A[k + i * kPld] : A[i + k * kPld], B[k + c * ldb], s);
+    acc[i + c * kT] += s;
+  }
+}
 
 // X[x0 + i, c] (+/-)= sum_k A[i + k*lda] * B[k + c*kT] straight into global X with
 // atomics (i < m, c < nr, k < kk); A column-major with leading dimension lda.  With
@@ -158,7 +208,7 @@ __device__ __forceinline__ void block_gemv_atomic(double* X, int64_t ldx, int x0
   }
 }
 
-// Lower-triangular solves of a kk x kk block held in A (ld kPld) against the
+// Lower-triangular solves of a kk x kk block held in A (ld lda) against the
 // right-hand sides acc (ld kT), one warp per right-hand side column; rinv holds
 // the reciprocals of the diagonal (computed off the dependency chain).
 // forward: acc <- D^-1 acc ; backward: acc <- D^-T acc.
@@ -304,15 +354,73 @@ __device__ __forceinline__ void signal(int32_t* counter) {
   if (threadIdx.x == 0) red_release(counter, 1);
 }
 
+// Forward arrivals of one off-diagonal tile (panel rows r0 .. r1-1 of supernode s):
+// one per target supernode, i.e. per relative-index group the rows span (groups are
+// maximal runs of rows with the same target, numbered in row order), signalled in
+// parallel after the block's scatter.
+__device__ __forceinline__ void signal_arrivals(const PSolveArgs& a, const SnMeta& m, int r0, int r1) {
+  __syncthreads();
+  const int g0 = a.row_group[m.lidx + r0], g1 = a.row_group[m.lidx + r1 - 1];
+  for (int g = g0 + (int)threadIdx.x; g <= g1; g += kThreads) red_release(a.arrived + a.groups[g].t, 1);
+}
+
+// Shape of super-block p of a supernode of nblk 64-column blocks.
+struct SuperBlock {
+  int b0, nb;  // first block, blocks
+  __device__ SuperBlock(int p, int sb, int nblk) : b0(p * sb), nb(min(sb, nblk - p * sb)) {}
+};
+
+// First element of tile (r, q) (r >= q) of the inverse of super-block p.
+template <class T>
+__device__ __forceinline__ const T* inv_tile(const PSolveArgs& a, const SnMeta& m, int p, int r, int q) {
+  const int64_t full = (int64_t)a.sb * (a.sb + 1) / 2;
+  return static_cast<const T*>(a.Inv) + m.ioff + ((int64_t)p * full + (int64_t)r * (r + 1) / 2 + q) * (kT * kT);
+}
+
+// acc (64 x nr, ld kT) = sum_{j0 <= j < j1} tile_j (x) x_j, with the tile loads one
+// ahead in registers (the caller has issued tile j0's).  tile(j, regs) issues the
+// loads of tile j; xrow(j) gives the first X row of x_j, xlen(j) its valid rows;
+// kTrans applies the tiles transposed; m = valid outputs.  The x blocks are staged
+// all at once when they fit Bx.
+template <class T, bool kTrans, class TileFn, class XRow, class XLen>
+__device__ __forceinline__ void slab_product(double* acc, double* Ab, double* Bx, int j0, int j1, TileRegs<T>& regs,
+                                             TileFn tile, const double* X, int64_t ldx, XRow xrow, XLen xlen,
+                                             int m, int nr) {
+  const int nt = j1 - j0;
+  for (int idx = threadIdx.x; idx < kT * nr; idx += kThreads) acc[idx] = 0.0;
+  const bool all = nt * kT * nr <= kT * kT;
+  if (all)
+    for (int j = 0; j < nt; ++j) stage_x(Bx + j * kT, nt * kT, X, ldx, xrow(j0 + j), nullptr, xlen(j0 + j), nr);
+  for (int j = 0; j < nt; ++j) {
+    regs.store(Ab);
+    if (j + 1 < nt) tile(j0 + j + 1, regs);
+    if (!all) stage_x(Bx, kT, X, ldx, xrow(j0 + j), nullptr, xlen(j0 + j), nr);
+    __syncthreads();
+    if (all) tile_gemv<kTrans>(acc, Ab, Bx + j * kT, nt * kT, m, xlen(j0 + j), nr);
+    else tile_gemv<kTrans>(acc, Ab, Bx, kT, m, xlen(j0 + j), nr);
+    __syncthreads();
+  }
+}
+
+// out[x0 + i + c*ldx] += sign * acc[i + c*kT] for i < m, c < nr (atomic).
+__device__ __forceinline__ void add_out(double* out, int64_t ldx, int x0, const double* acc, int m, int nr,
+                                        double sign, const int32_t* rows = nullptr) {
+  for (int idx = threadIdx.x; idx < m * nr; idx += kThreads) {
+    int c = idx / m, i = idx - c * m;
+    atomicAdd(out + x0 + (rows ? rows[i] : i) + c * ldx, sign * acc[i + c * kT]);
+  }
+}
+
 template <class T, int kR>
 __global__ void __launch_bounds__(kThreads, solve_min_blocks<kR>()) k_solve_forward(PSolveArgs a) {
   extern __shared__ __align__(16) double sm[];
-  double* Ab = sm;                  // staged L block, ld kPld
-  double* Bx = sm + kT * kPld;      // staged X rows, ld kT
+  double* Ab = sm;                  // staged tile, ld kPld
+  double* Bx = sm + kT * kPld;      // staged right-hand-side rows
   double* acc = Bx + kT * kT;       // accumulator, ld kT
   __shared__ int sh_task, sh_stop, sh_ok;
   __shared__ double sh_rinv[kT];
   const int nr = a.nrhs;
+  TileRegs<T> regs;
   for (;;) {
     const int tk = next_task(a, &sh_task, &sh_stop);
     if (tk < 0) return;
@@ -324,56 +432,85 @@ __global__ void __launch_bounds__(kThreads, solve_min_blocks<kR>()) k_solve_forw
     const T* P = static_cast<const T*>(a.L) + m.off;
     const int32_t* rl = a.rows + m.lidx;
     const int64_t ld = m.ld;
-    if (task.kind == 0) {
-      // D(t): descendants' and earlier blocks' updates have landed in X_t; X_t <- L_tt^-1 X_t,
-      // then the update of the next block, X_{t+1} -= L_{t+1,t} X_t
-      const int t = task.t, r0 = t * kT, bt = min(kT, m.w - r0);
-      const int r1 = r0 + kT, b1 = r1 < m.w ? min(kT, m.w - r1) : 0;
-      stage_block(Ab, P, ld, r0, bt, r0, bt);  // L is final: load before waiting
-      if (b1) stage_block<T, kT>(Bx, P, ld, r1, b1, r0, bt);
+    const int nblk = (m.w + kT - 1) / kT;
+    if (task.kind == 5) {
+      // DI(p, r): Z[block r of p] += sum_{q <= r, this task's tiles} Inv_p(r, q) Y[block q of p]
+      const int p = task.i & 0xffffff, q0 = task.i >> 24, r = task.t;
+      const SuperBlock B(p, a.sb, nblk);
+      const int t = B.b0 + r, bt = min(kT, m.w - t * kT), q1 = min(r + 1, q0 + a.tpt);
+      auto tile = [&](int q, TileRegs<T>& R) { R.load(inv_tile<T>(a, m, p, r, q), kT, kT, kT); };
+      tile(q0, regs);  // the inverse is final: load before waiting
+      if (!wait_geq(a.arrived + s, a.expected[s], a.status, s, &sh_ok, a.spin_limit)) return;
+      if (!wait_geq(a.upd + m.sboff + p, p * B.nb * solve_ntask(a.sb, a.tpt), a.status, s, &sh_ok, a.spin_limit))
+        return;
+      trace_mark(a, tk, 1, now_ns());
+      slab_product<T, false>(
+          acc, Ab, Bx, q0, q1, regs, tile, a.X, a.ldx, [&](int q) { return m.fc + (B.b0 + q) * kT; },
+          [&](int q) { return min(kT, m.w - (B.b0 + q) * kT); }, bt, nr);
+      add_out(a.Z, a.ldx, m.fc + t * kT, acc, bt, nr, 1.0);
+      signal(a.blkdone + s);
+    } else if (task.kind == 1) {
+      // U(p, t): Y[block t] -= L(t, super-block p) Z[p] over this task's tiles
+      const int p = task.i & 0xffffff, q0 = task.i >> 24, t = task.t;
+      const SuperBlock B(p, a.sb, nblk);
+      const int r0 = t * kT, bt = min(kT, m.w - r0), q1 = min(B.nb, q0 + a.tpt);
+      auto tile = [&](int q, TileRegs<T>& R) {
+        const int c0 = (B.b0 + q) * kT;
+        R.load(P + r0 + (int64_t)c0 * ld, ld, bt, min(kT, m.w - c0));
+      };
+      tile(q0, regs);  // L is final: load before waiting
+      if (!wait_geq(a.blkdone + s, solve_di_range(nblk, a.sb, a.tpt, 0, p + 1), a.status, s, &sh_ok, a.spin_limit))
+        return;
+      trace_mark(a, tk, 1, now_ns());
+      slab_product<T, false>(
+          acc, Ab, Bx, q0, q1, regs, tile, a.Z, a.ldx, [&](int q) { return m.fc + (B.b0 + q) * kT; },
+          [&](int q) { return min(kT, m.w - (B.b0 + q) * kT); }, bt, nr);
+      add_out(a.X, a.ldx, m.fc + r0, acc, bt, nr, -1.0);
+      signal(a.upd + m.sboff + t / a.sb);
+    } else if (task.kind == 2) {
+      // O(p, u): Y[ancestor rows of tile u] -= L(u, super-block p) Z[p] over this task's tiles
+      const int p = task.i & 0xffffff, q0 = task.i >> 24, u = task.t, r0 = m.w + u * kT, bu = min(kT, m.h - r0);
+      const SuperBlock B(p, a.sb, nblk);
+      const int q1 = min(B.nb, q0 + a.tpt);
+      auto tile = [&](int q, TileRegs<T>& R) {
+        const int c0 = (B.b0 + q) * kT;
+        R.load(P + r0 + (int64_t)c0 * ld, ld, bu, min(kT, m.w - c0));
+      };
+      tile(q0, regs);
+      if (!wait_geq(a.blkdone + s, solve_di_range(nblk, a.sb, a.tpt, 0, p + 1), a.status, s, &sh_ok, a.spin_limit))
+        return;
+      trace_mark(a, tk, 1, now_ns());
+      slab_product<T, false>(
+          acc, Ab, Bx, q0, q1, regs, tile, a.Z, a.ldx, [&](int q) { return m.fc + (B.b0 + q) * kT; },
+          [&](int q) { return min(kT, m.w - (B.b0 + q) * kT); }, bu, nr);
+      add_out(a.X, a.ldx, 0, acc, bu, nr, -1.0, rl + r0);
+      signal_arrivals(a, m, r0, r0 + bu);
       __syncthreads();
-      if (threadIdx.x < bt) sh_rinv[threadIdx.x] = 1.0 / Ab[threadIdx.x * (kPld + 1)];
-      if (bt == kT) {  // full block: 8 x 8 diagonal inverses, off the chain
+    } else if (task.kind == 0) {
+      // D: one-block supernode, Z_0 <- L_00^-1 Y_0 (its off-diagonal tiles are O tasks)
+      const int w = m.w;
+      stage_block(Ab, P, ld, 0, w, 0, w);  // L is final: load before waiting
+      __syncthreads();
+      if (threadIdx.x < w) sh_rinv[threadIdx.x] = 1.0 / Ab[threadIdx.x * (kPld + 1)];
+      if (w == kT) {  // full block: 8 x 8 diagonal inverses, off the chain
         __syncthreads();
         invert_diag8(Ab, sh_rinv);
       }
       if (!wait_geq(a.arrived + s, a.expected[s], a.status, s, &sh_ok, a.spin_limit)) return;
-      if (!wait_geq(a.upd + m.boff + t, t, a.status, s, &sh_ok, a.spin_limit)) return;
       trace_mark(a, tk, 1, now_ns());
-      stage_x(acc, a.X, a.ldx, m.fc + r0, nullptr, bt, nr);
+      stage_x(acc, kT, a.X, a.ldx, m.fc, nullptr, w, nr);
       __syncthreads();
-      if (bt == kT) block_trsv64<true>(acc, Ab, sh_rinv, nr);
-      else block_trsv<true>(acc, Ab, sh_rinv, bt, nr);
+      if (w == kT) block_trsv64<true>(acc, Ab, sh_rinv, nr);
+      else block_trsv<true>(acc, Ab, sh_rinv, w, nr);
       __syncthreads();
-      for (int idx = threadIdx.x; idx < bt * nr; idx += kThreads) {
-        int c = idx / bt, r = idx - c * bt;
-        a.X[m.fc + r0 + r + c * a.ldx] = acc[r + c * kT];
+      for (int idx = threadIdx.x; idx < w * nr; idx += kThreads) {
+        int c = idx / w, i = idx - c * w;
+        a.Z[m.fc + i + c * a.ldx] = acc[i + c * kT];
       }
-      if (b1) block_gemv_atomic<false>(a.X, a.ldx, m.fc + r1, Bx, kT, acc, b1, bt, nr, -1.0);
-      __syncthreads();
-      if (threadIdx.x == 0) {
-        if (b1) red_release(a.upd + m.boff + t + 1, 1);  // the next block first: it is on the chain
-        red_release(a.blkdone + s, 1);
-      }
-    } else if (task.kind == 1) {
-      // U(i, t): X_t -= L_ti X_i
-      const int i = task.i, t = task.t, bi = min(kT, m.w - i * kT), r0 = t * kT, bt = min(kT, m.w - r0);
-      stage_block(Ab, P, ld, r0, bt, i * kT, bi);  // L is final: load before waiting
-      if (!wait_geq(a.blkdone + s, i + 1, a.status, s, &sh_ok, a.spin_limit)) return;
-      trace_mark(a, tk, 1, now_ns());
-      stage_x(Bx, a.X, a.ldx, m.fc + i * kT, nullptr, bi, nr);
-      for (int idx = threadIdx.x; idx < kT * nr; idx += kThreads) acc[idx] = 0.0;
-      __syncthreads();
-      block_gemv<false>(acc, Ab, Bx, bt, bi, nr);
-      __syncthreads();
-      for (int idx = threadIdx.x; idx < bt * nr; idx += kThreads) {
-        int c = idx / bt, r = idx - c * bt;
-        atomicAdd(a.X + m.fc + r0 + r + c * a.ldx, -acc[r + c * kT]);
-      }
-      signal(a.upd + m.boff + t);
-    } else if (task.kind == 4) {
-      // F: a one-block supernode whole: X_0 <- L_00^-1 X_0, then every off-diagonal tile
-      // scattered into the ancestors' rows
+      signal(a.blkdone + s);
+    } else {
+      // F: one-block supernode whole: Z_0 <- L_00^-1 Y_0, then every off-diagonal tile's
+      // Y[ancestor rows] -= L_u0 Z_0
       const int w = m.w, h = m.h, noff = (m.h - m.w + kT - 1) / kT;
       // a panel that fits the two staging buffers is loaded whole (ld h) before waiting
       const bool whole = h * w <= kT * kPld + kT * kT;
@@ -397,13 +534,13 @@ __global__ void __launch_bounds__(kThreads, solve_min_blocks<kR>()) k_solve_forw
       if (threadIdx.x < w) sh_rinv[threadIdx.x] = 1.0 / Ab[threadIdx.x * (lda + 1)];
       if (!wait_geq(a.arrived + s, a.expected[s], a.status, s, &sh_ok, a.spin_limit)) return;
       trace_mark(a, tk, 1, now_ns());
-      stage_x(acc, a.X, a.ldx, m.fc, nullptr, w, nr);
+      stage_x(acc, kT, a.X, a.ldx, m.fc, nullptr, w, nr);
       __syncthreads();
       block_trsv<true>(acc, Ab, sh_rinv, w, nr, lda);
       __syncthreads();
       for (int idx = threadIdx.x; idx < w * nr; idx += kThreads) {
-        int c = idx / w, r = idx - c * w;
-        a.X[m.fc + r + c * a.ldx] = acc[r + c * kT];
+        int c = idx / w, i = idx - c * w;
+        a.Z[m.fc + i + c * a.ldx] = acc[i + c * kT];
       }
       for (int u = 0; u < noff; ++u) {
         const int r0 = w + u * kT, bu = min(kT, m.h - r0);
@@ -412,50 +549,10 @@ __global__ void __launch_bounds__(kThreads, solve_min_blocks<kR>()) k_solve_forw
           __syncthreads();
         }
         block_gemv_atomic<false>(a.X, a.ldx, 0, whole ? Ab + r0 : Ab, lda, acc, bu, w, nr, -1.0, rl + r0);
+        signal_arrivals(a, m, r0, r0 + bu);  // one per (tile, target), as the plan counts them
         __syncthreads();
-        if (threadIdx.x == 0) {
-          __threadfence();
-          int last = -1;
-          for (int r = 0; r < bu; ++r) {
-            int tgt = a.supmember[rl[r0 + r]];
-            if (tgt != last) atomicAdd(a.arrived + tgt, 1);
-            last = tgt;
-          }
-        }
       }
-      __syncthreads();
       if (threadIdx.x == 0) red_release(a.blkdone + s, 1);
-    } else {
-      // O(i0, u): off-diagonal rows, Y_K[rows] -= L_KJ Y_J over the column blocks of a
-      // chunk, accumulated, then scattered into the ancestors' rows
-      const int i0 = task.i, u = task.t, r0 = m.w + u * kT, bu = min(kT, m.h - r0);
-      const int i1 = min((m.w + kT - 1) / kT, i0 + a.chunk);
-      for (int idx = threadIdx.x; idx < kT * nr; idx += kThreads) acc[idx] = 0.0;
-      for (int i = i0; i < i1; ++i) {
-        const int bi = min(kT, m.w - i * kT);
-        stage_block(Ab, P, ld, r0, bu, i * kT, bi);  // L is final: load before waiting
-        if (!wait_geq(a.blkdone + s, i + 1, a.status, s, &sh_ok, a.spin_limit)) return;
-        stage_x(Bx, a.X, a.ldx, m.fc + i * kT, nullptr, bi, nr);
-        __syncthreads();
-        block_gemv<false>(acc, Ab, Bx, bu, bi, nr);
-        __syncthreads();
-      }
-      trace_mark(a, tk, 1, now_ns());
-      for (int idx = threadIdx.x; idx < bu * nr; idx += kThreads) {
-        int c = idx / bu, r = idx - c * bu;
-        atomicAdd(a.X + rl[r0 + r] + c * a.ldx, -acc[r + c * kT]);
-      }
-      __syncthreads();
-      if (threadIdx.x == 0) {
-        __threadfence();
-        int last = -1;
-        for (int r = 0; r < bu; ++r) {
-          int tgt = a.supmember[rl[r0 + r]];
-          if (tgt != last) atomicAdd(a.arrived + tgt, 1);
-          last = tgt;
-        }
-      }
-      __syncthreads();
     }
     trace_mark(a, tk, 2, now_ns());
   }
@@ -470,6 +567,7 @@ __global__ void __launch_bounds__(kThreads, solve_min_blocks<kR>()) k_solve_back
   __shared__ int sh_task, sh_stop, sh_ok;
   __shared__ double sh_rinv[kT];
   const int nr = a.nrhs;
+  TileRegs<T> regs;
   for (;;) {
     const int tk = next_task(a, &sh_task, &sh_stop);
     if (tk < 0) return;
@@ -481,21 +579,107 @@ __global__ void __launch_bounds__(kThreads, solve_min_blocks<kR>()) k_solve_back
     const T* P = static_cast<const T*>(a.L) + m.off;
     const int32_t* rl = a.rows + m.lidx;
     const int64_t ld = m.ld;
-    const int nblk = (m.w + kT - 1) / kT;
-    if (task.kind == 4) {
-      // G: a one-block supernode whole: X_0 -= L_u0^T X_u for every off-diagonal tile
-      // (ancestor rows, final once the parent is done), then X_0 <- L_00^-T X_0
-      const int w = m.w, noff = (m.h - m.w + kT - 1) / kT;
-      const int par = a.sparent[s];
-      if (par >= 0 && !wait_geq(a.blkdone + par, (a.meta[par].w + kT - 1) / kT, a.status, s, &sh_ok, a.spin_limit))
+    const int nblk = (m.w + kT - 1) / kT, nsb = (nblk + a.sb - 1) / a.sb;
+    const int noff = (m.h - m.w + kT - 1) / kT;
+    if (task.kind == 5) {
+      // DI(p, r): X[block r of p] += sum_{q >= r, this task's tiles} Inv_p(q, r)^T Z[block q of p]
+      const int p = task.i & 0xffffff, j0 = task.i >> 24, r = task.t;
+      const SuperBlock B(p, a.sb, nblk);
+      const int t = B.b0 + r, bt = min(kT, m.w - t * kT), j1 = min(B.nb - r, j0 + a.tpt);
+      auto tile = [&](int j, TileRegs<T>& R) { R.load(inv_tile<T>(a, m, p, r + j, r), kT, kT, kT); };
+      tile(j0, regs);
+      // W tasks of every off-diagonal tile, V tasks of every later super-block into each block of p
+      const int nlast = nblk - (nsb - 1) * a.sb;
+      const int later = p < nsb - 1 ? (nsb - 2 - p) * solve_ntask(a.sb, a.tpt) + solve_ntask(nlast, a.tpt) : 0;
+      if (!wait_geq(a.upd + m.sboff + p, noff * solve_ntask(B.nb, a.tpt) + B.nb * later, a.status, s, &sh_ok,
+                    a.spin_limit))
         return;
       trace_mark(a, tk, 1, now_ns());
-      stage_x(acc, a.X, a.ldx, m.fc, nullptr, w, nr);
+      slab_product<T, true>(
+          acc, Ab, Bx, j0, j1, regs, tile, a.Z, a.ldx, [&](int j) { return m.fc + (t + j) * kT; },
+          [&](int j) { return min(kT, m.w - (t + j) * kT); }, bt, nr);
+      add_out(a.X, a.ldx, m.fc + t * kT, acc, bt, nr, 1.0);
+      signal(a.blkdone + s);
+    } else if (task.kind == 1) {
+      // V(p, t): Z[block t] -= L(super-block p, t)^T X[p] over this task's tiles
+      const int p = task.i & 0xffffff, q0 = task.i >> 24, t = task.t, c0 = t * kT, bt = min(kT, m.w - c0);
+      const SuperBlock B(p, a.sb, nblk);
+      const int q1 = min(B.nb, q0 + a.tpt);
+      auto tile = [&](int q, TileRegs<T>& R) {
+        const int r0 = (B.b0 + q) * kT;
+        R.load(P + r0 + (int64_t)c0 * ld, ld, min(kT, m.w - r0), bt);
+      };
+      tile(q0, regs);
+      if (!wait_geq(a.blkdone + s, solve_di_range(nblk, a.sb, a.tpt, p, nsb), a.status, s, &sh_ok, a.spin_limit))
+        return;
+      trace_mark(a, tk, 1, now_ns());
+      slab_product<T, true>(
+          acc, Ab, Bx, q0, q1, regs, tile, a.X, a.ldx, [&](int q) { return m.fc + (B.b0 + q) * kT; },
+          [&](int q) { return min(kT, m.w - (B.b0 + q) * kT); }, bt, nr);
+      add_out(a.Z, a.ldx, m.fc + c0, acc, bt, nr, -1.0);
+      signal(a.upd + m.sboff + t / a.sb);
+    } else if (task.kind == 3) {
+      // W(p, u): Z[p] -= L(u, super-block p)^T X[ancestor rows of tile u] over this task's
+      // tiles, final once the parent is done
+      const int p = task.i & 0xffffff, q0 = task.i >> 24, u = task.t, rr = m.w + u * kT, br = min(kT, m.h - rr);
+      const SuperBlock B(p, a.sb, nblk);
+      const int q1 = min(B.nb, q0 + a.tpt);
+      const int par = a.sparent[s];
+      regs.load(P + rr + (int64_t)(B.b0 + q0) * kT * ld, ld, br, min(kT, m.w - (B.b0 + q0) * kT));
+      if (par >= 0 &&
+          !wait_geq(a.blkdone + par, solve_done_count(a.meta[par].w, a.sb, a.tpt), a.status, s, &sh_ok, a.spin_limit))
+        return;
+      trace_mark(a, tk, 1, now_ns());
+      stage_x(Bx, kT, a.X, a.ldx, 0, rl + rr, br, nr);
+      for (int q = q0; q < q1; ++q) {
+        const int c0 = (B.b0 + q) * kT, bq = min(kT, m.w - c0);
+        regs.store(Ab);
+        if (q + 1 < q1) {
+          const int c1 = c0 + kT;
+          regs.load(P + rr + (int64_t)c1 * ld, ld, br, min(kT, m.w - c1));
+        }
+        __syncthreads();
+        block_gemv_atomic<true>(a.Z, a.ldx, m.fc + c0, Ab, kPld, Bx, bq, br, nr, -1.0);
+        __syncthreads();
+      }
+      if (threadIdx.x == 0) red_release(a.upd + m.sboff + p, 1);
+    } else if (task.kind == 0) {
+      // B: one-block supernode, X_0 <- L_00^-T Z_0 once its W updates landed
+      const int w = m.w;
+      stage_block(Ab, P, ld, 0, w, 0, w);  // L is final: load before waiting
+      __syncthreads();
+      if (threadIdx.x < w) sh_rinv[threadIdx.x] = 1.0 / Ab[threadIdx.x * (kPld + 1)];
+      if (w == kT) {  // full block: 8 x 8 diagonal inverses, off the chain
+        __syncthreads();
+        invert_diag8(Ab, sh_rinv);
+      }
+      if (!wait_geq(a.upd + m.sboff, noff, a.status, s, &sh_ok, a.spin_limit)) return;
+      trace_mark(a, tk, 1, now_ns());
+      stage_x(acc, kT, a.Z, a.ldx, m.fc, nullptr, w, nr);
+      __syncthreads();
+      if (w == kT) block_trsv64<false>(acc, Ab, sh_rinv, nr);
+      else block_trsv<false>(acc, Ab, sh_rinv, w, nr);
+      __syncthreads();
+      for (int idx = threadIdx.x; idx < w * nr; idx += kThreads) {
+        int c = idx / w, i = idx - c * w;
+        a.X[m.fc + i + c * a.ldx] = acc[i + c * kT];
+      }
+      signal(a.blkdone + s);
+    } else {
+      // G: one-block supernode whole: Z_0 -= L_u0^T X_u for every off-diagonal tile
+      // (ancestor rows, final once the parent is done), then X_0 <- L_00^-T Z_0
+      const int w = m.w;
+      const int par = a.sparent[s];
+      if (par >= 0 &&
+          !wait_geq(a.blkdone + par, solve_done_count(a.meta[par].w, a.sb, a.tpt), a.status, s, &sh_ok, a.spin_limit))
+        return;
+      trace_mark(a, tk, 1, now_ns());
+      stage_x(acc, kT, a.Z, a.ldx, m.fc, nullptr, w, nr);
       for (int u = 0; u < noff; ++u) {
         const int r0 = w + u * kT, bu = min(kT, m.h - r0);
         __syncthreads();
         stage_block(Ab, P, ld, r0, bu, 0, w);
-        stage_x(Bx, a.X, a.ldx, 0, rl + r0, bu, nr);
+        stage_x(Bx, kT, a.X, a.ldx, 0, rl + r0, bu, nr);
         __syncthreads();
         for (int idx = threadIdx.x; idx < w * nr; idx += kThreads) {  // acc_k -= sum_r L_rk x_r
           const int c = idx / w, k = idx - c * w;
@@ -512,345 +696,131 @@ __global__ void __launch_bounds__(kThreads, solve_min_blocks<kR>()) k_solve_back
       block_trsv<false>(acc, Ab, sh_rinv, w, nr);
       __syncthreads();
       for (int idx = threadIdx.x; idx < w * nr; idx += kThreads) {
-        int c = idx / w, r = idx - c * w;
-        a.X[m.fc + r + c * a.ldx] = acc[r + c * kT];
+        int c = idx / w, i = idx - c * w;
+        a.X[m.fc + i + c * a.ldx] = acc[i + c * kT];
       }
       __syncthreads();
       if (threadIdx.x == 0) red_release(a.blkdone + s, 1);
-    } else if (task.kind == 3) {
-      // W(u): ancestor rows of tile u, final once the parent is done: X_t -= L_ut^T X_u for
-      // every column block t, newest first (the order the diagonal chain needs them)
-      const int u = task.t, rr = m.w + u * kT, br = min(kT, m.h - rr);
-      const int par = a.sparent[s];
-      stage_block(Ab, P, ld, rr, br, (nblk - 1) * kT, m.w - (nblk - 1) * kT);
-      if (par >= 0 && !wait_geq(a.blkdone + par, (a.meta[par].w + kT - 1) / kT, a.status, s, &sh_ok, a.spin_limit))
-        return;
-      trace_mark(a, tk, 1, now_ns());
-      stage_x(Bx, a.X, a.ldx, 0, rl + rr, br, nr);
-      for (int t = nblk - 1; t >= 0; --t) {
-        const int c0 = t * kT, bt = min(kT, m.w - c0);
-        if (t < nblk - 1) stage_block(Ab, P, ld, rr, br, c0, bt);
-        __syncthreads();
-        block_gemv_atomic<true>(a.X, a.ldx, m.fc + c0, Ab, kPld, Bx, bt, br, nr, -1.0);
-        __syncthreads();
-        if (threadIdx.x == 0) red_release(a.upd + m.boff + t, 1);
-      }
-    } else if (task.kind == 0) {
-      // B(t): every update into X_t has landed; X_t <- L_tt^-T X_t, then X_{t-1} -= L_{t,t-1}^T X_t
-      const int t = task.t, c0 = t * kT, bt = min(kT, m.w - c0);
-      const int noff = (m.h - m.w + kT - 1) / kT;
-      stage_block(Ab, P, ld, c0, bt, c0, bt);  // L is final: load before waiting
-      if (t > 0) stage_block<T, kT>(Bx, P, ld, c0, bt, c0 - kT, kT);
-      __syncthreads();
-      if (threadIdx.x < bt) sh_rinv[threadIdx.x] = 1.0 / Ab[threadIdx.x * (kPld + 1)];
-      if (bt == kT) {  // full block: 8 x 8 diagonal inverses, off the chain
-        __syncthreads();
-        invert_diag8(Ab, sh_rinv);
-      }
-      if (!wait_geq(a.upd + m.boff + t, noff + nblk - 1 - t, a.status, s, &sh_ok, a.spin_limit)) return;
-      trace_mark(a, tk, 1, now_ns());
-      stage_x(acc, a.X, a.ldx, m.fc + c0, nullptr, bt, nr);
-      __syncthreads();
-      if (bt == kT) block_trsv64<false>(acc, Ab, sh_rinv, nr);
-      else block_trsv<false>(acc, Ab, sh_rinv, bt, nr);
-      __syncthreads();
-      for (int idx = threadIdx.x; idx < bt * nr; idx += kThreads) {
-        int c = idx / bt, r = idx - c * bt;
-        a.X[m.fc + c0 + r + c * a.ldx] = acc[r + c * kT];
-      }
-      // X_{t-1} -= L_{t,t-1}^T X_t: Bx holds rows c0.. (bt) x columns c0-64.. (64), ld kT
-      if (t > 0) block_gemv_atomic<true>(a.X, a.ldx, m.fc + c0 - kT, Bx, kT, acc, kT, bt, nr, -1.0);
-      __syncthreads();
-      if (threadIdx.x == 0) {
-        if (t > 0) red_release(a.upd + m.boff + t - 1, 1);  // the previous block first: it is on the chain
-        red_release(a.blkdone + s, 1);
-      }
-    } else {
-      // V(t, u): X_u -= L_tu^T X_t
-      const int t = task.i, u = task.t, rr = t * kT, br = min(kT, m.w - rr), c0 = u * kT, bu = min(kT, m.w - c0);
-      stage_block(Ab, P, ld, rr, br, c0, bu);
-      if (!wait_geq(a.blkdone + s, nblk - t, a.status, s, &sh_ok, a.spin_limit)) return;
-      trace_mark(a, tk, 1, now_ns());
-      stage_x(Bx, a.X, a.ldx, m.fc + rr, nullptr, br, nr);
-      __syncthreads();
-      block_gemv_atomic<true>(a.X, a.ldx, m.fc + c0, Ab, kPld, Bx, bu, br, nr, -1.0);
-      signal(a.upd + m.boff + u);
     }
     trace_mark(a, tk, 2, now_ns());
   }
 }
 
-// ---- dense root solve: one thread-block cluster ----------------------------------
-// The root supernode of a nested-dissection tree is a dense w x w lower triangle (the
-// 27-point 80^3 stencil's is 21,146 wide), and a sweep over it is a chain of w/64
-// diagonal-block solves.  Through global counters each link costs several us; inside
-// one cluster it is a barrier.cluster round and a distributed-shared-memory read.
-// Block b (64 columns) belongs to cluster rank b % C.  Step t of the forward sweep:
-// every CTA copies x_t from its owner's shared memory; the owner of block t+1 first
-// subtracts L_{t+1,t} x_t from its rows, solves its diagonal block and publishes
-// x_{t+1}; then every CTA subtracts L_it x_t from the other blocks it owns.  The
-// backward sweep mirrors it with L^T.  X rows of a block are only ever touched by its
-// owner (no atomics); L blocks stream through a cp.async ring ahead of use (L is final,
-// so the loads never wait for the chain).  Few right-hand sides only: the updates are
-// FP64 FMA work on C SMs.
-constexpr int kDenseRhs = 4;       // right-hand sides per launch (the persistent path takes more)
-constexpr int kDenseStages = 4;    // L blocks in flight per CTA
-constexpr size_t kDenseSmemMax = 227 * 1024;  // dynamic shared memory one CTA may use
+// ---- diagonal super-block inverses ---------------------------------------------------
+// One CTA per (super-block p, column block j): the tiles Inv(i, j), i = j .. nb - 1, of
+// Inv_p = L_pp^-1 by block substitution down column j:
+//   Inv(j, j) = L_jj^-1,   Inv(i, j) = -L_ii^-1 sum_{k=j}^{i-1} L_ik Inv(k, j),
+// in FP64 (the panel widened), stored in the arena's type.  The tiles of column j above
+// tile i are this CTA's own earlier writes, read back through L2.
+constexpr int kInvThreads = 256;
+constexpr size_t kInvSmem = (size_t)3 * kT * kPld * sizeof(double);  // two CTAs per SM
 
-__device__ __forceinline__ void cluster_arrive() { asm volatile("barrier.cluster.arrive.release.aligned;\n" ::: "memory"); }
-__device__ __forceinline__ void cluster_wait() { asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory"); }
-__device__ __forceinline__ unsigned cluster_rank() {
-  unsigned r;
-  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
-  return r;
-}
-__device__ __forceinline__ unsigned cluster_size() {
-  unsigned r;
-  asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(r));
-  return r;
-}
-// Generic address of the same shared-memory location in cluster CTA `rank`.
-__device__ __forceinline__ const double* map_rank(const double* p, unsigned rank) {
-  unsigned long long r;
-  asm volatile("mapa.u64 %0, %1, %2;" : "=l"(r) : "l"(p), "r"(rank));
-  return reinterpret_cast<const double*>(r);
-}
-__device__ __forceinline__ void cp_async16_zfill(void* smem, const void* gmem, bool ok) {
-  unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(gmem), "r"(ok ? 16 : 0));
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
-}
-
-// 64 x 64 block of T in shared memory, column-major in 16-byte chunks of kC rows; chunk q
-// of column k sits at chunk position q ^ (k & 7), so that a warp reading one row across
-// 32 columns, or 16 bytes of 8 columns, hits distinct banks.
-template <class T>
-struct SwzBlock {
-  static constexpr int kC = 16 / (int)sizeof(T);
-  __device__ static __forceinline__ int at(int r, int k) { return k * kT + (((r / kC) ^ (k & 7)) * kC) + r % kC; }
-};
-
-// Dense-sweep item order of one cluster rank: forward, steps t = 0 .. nblk-2 and the
-// owned blocks i > t ascending; backward, steps t = nblk-1 .. 1 and the owned blocks
-// j < t descending.  (blk = -1 once exhausted.)
-template <bool kFwd>
-struct DenseItems {
-  int nblk, C, rho, t, blk;
-  __device__ void first_of_step() {
-    for (;;) {
-      if (kFwd ? t > nblk - 2 : t < 1) {
-        blk = -1;
-        return;
-      }
-      blk = kFwd ? t + 1 + ((rho - (t + 1)) % C + C) % C : t - 1 - (((t - 1) - rho) % C + C) % C;
-      if (kFwd ? blk < nblk : blk >= 0) return;
-      t += kFwd ? 1 : -1;
+// C (64 x 64, ld kPld) = A * B or += A * B (both 64 x 64, ld kPld); thread (ty, tx)
+// owns C[ty + 16 ii][tx + 16 jj].
+template <bool kAccumulate>
+__device__ __forceinline__ void gemm64(double* C, const double* A, const double* B, double scale) {
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  double c[4][4] = {};
+  for (int k = 0; k < kT; ++k) {
+    double av[4], bv[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) av[i] = A[ty + 16 * i + k * kPld];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) bv[j] = B[k + (tx + 16 * j) * kPld];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) c[i][j] = fma(av[i], bv[j], c[i][j]);
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      double& d = C[ty + 16 * i + (tx + 16 * j) * kPld];
+      d = kAccumulate ? d + scale * c[i][j] : scale * c[i][j];
     }
-  }
-  __device__ void start(int n, int c, int r) {
-    nblk = n;
-    C = c;
-    rho = r;
-    t = kFwd ? 0 : n - 1;
-    first_of_step();
-  }
-  __device__ void next() {
-    blk += kFwd ? C : -C;
-    if (kFwd ? blk >= nblk : blk < 0) {
-      t += kFwd ? 1 : -1;
-      first_of_step();
+}
+
+// Ti = inverse of the b x b lower triangle of Ls (both ld kPld; zero outside b x b).
+// Four threads per column c: x_i = (delta_ic - sum_{k<i} L_ik x_k) / L_ii down the column.
+__device__ __forceinline__ void tri_inverse64(double* Ti, const double* Ls, int b) {
+  const int c = threadIdx.x >> 2, part = threadIdx.x & 3;
+  for (int i = 0; i < kT; ++i) {
+    double s = 0.0;
+    if (i < b && c < b && i > c)
+      for (int k = c + part; k < i; k += 4) s = fma(Ls[i + k * kPld], Ti[k + c * kPld], s);
+    s += __shfl_xor_sync(0xffffffffu, s, 1);
+    s += __shfl_xor_sync(0xffffffffu, s, 2);
+    if (part == 0) {
+      double x = 0.0;
+      if (i < b && c < b && i >= c) x = (i == c ? 1.0 : -s) / Ls[i + i * kPld];
+      Ti[i + c * kPld] = x;
     }
+    __syncwarp();
   }
-};
+}
 
-// Shared-memory layout of k_solve_dense (bytes), for `nown` owned blocks of nr right-hand sides.
 template <class T>
-struct DenseSmem {
-  size_t ring, ad, xs, xpub, red, rinv, acc, total;
-  __host__ __device__ DenseSmem(int nown, int nr) {
-    ring = 0;
-    ad = ring + (size_t)kDenseStages * kT * kT * sizeof(T);
-    xs = ad + (size_t)kT * kPld * sizeof(double);
-    xpub = xs + (size_t)kT * kDenseRhs * sizeof(double);
-    red = xpub + (size_t)kT * kDenseRhs * sizeof(double);
-    rinv = red + (size_t)4 * kT * kDenseRhs * sizeof(double);
-    acc = rinv + (size_t)kT * sizeof(double);
-    total = acc + (size_t)nown * kT * nr * sizeof(double);
-  }
-};
-
-template <class T, bool kFwd>
-__global__ void __launch_bounds__(kThreads, 1) k_solve_dense(PSolveArgs a, int s) {
-  extern __shared__ __align__(16) unsigned char dsm[];
-  const SnMeta m = a.meta[s];
-  const T* P = static_cast<const T*>(a.L) + m.off;
+__global__ void __launch_bounds__(kInvThreads, 2) k_sb_inverse(const T* __restrict__ L, T* __restrict__ Inv,
+                                                               const SnMeta* __restrict__ meta,
+                                                               const InvItem* __restrict__ items, int sb) {
+  extern __shared__ __align__(16) double smi[];
+  double* Ls = smi;               // L(i, k), then L(i, i), then the output tile
+  double* Ti = Ls + kT * kPld;    // Inv(k, j) while accumulating, then L(i, i)^-1
+  double* Acc = Ti + kT * kPld;
+  const InvItem it = items[blockIdx.x];
+  const SnMeta m = meta[it.s];
+  const int nblk = (m.w + kT - 1) / kT, b0 = it.p * sb, nb = min(sb, nblk - b0), j = it.j;
+  const int64_t full = (int64_t)sb * (sb + 1) / 2;
+  T* base = Inv + m.ioff + (int64_t)it.p * full * (kT * kT);
+  const T* P = L + m.off;
   const int64_t ld = m.ld;
-  const int nblk = (m.w + kT - 1) / kT, nr = a.nrhs;
-  const int C = (int)cluster_size(), rho = (int)cluster_rank(), tid = threadIdx.x;
-  const int nown = (nblk + C - 1) / C;
-  const DenseSmem<T> lay(nown, nr);
-  T* ring = reinterpret_cast<T*>(dsm + lay.ring);
-  double* Ad = reinterpret_cast<double*>(dsm + lay.ad);
-  double* xs = reinterpret_cast<double*>(dsm + lay.xs);      // x_t of the current step (ld kT)
-  double* xpub = reinterpret_cast<double*>(dsm + lay.xpub);  // x of this CTA's last solved block (ld kT)
-  double* red = reinterpret_cast<double*>(dsm + lay.red);    // 4 x 64 x kDenseRhs partial sums
-  double* rinv = reinterpret_cast<double*>(dsm + lay.rinv);
-  double* accown = reinterpret_cast<double*>(dsm + lay.acc);  // X of the owned blocks, nr x 64 each
-  double* X = a.X + m.fc;
-  const int64_t ldx = a.ldx;
-  auto bw = [&](int b) { return min(kT, m.w - b * kT); };
-  auto acc_of = [&](int b) { return accown + (size_t)(b / C) * kT * nr; };  // b owned: b % C == rho
-
-  // the owned blocks' rows of X, held here until solved
-  for (int lb = 0; lb < nown; ++lb) {
-    const int b = rho + lb * C;
-    if (b >= nblk) break;
-    const int n = bw(b);
-    double* acc = accown + (size_t)lb * kT * nr;
-    for (int idx = tid; idx < kT * nr; idx += kThreads) {
-      const int c = idx / kT, r = idx - c * kT;
-      acc[idx] = r < n ? X[b * kT + r + c * ldx] : 0.0;
-    }
-  }
-
-  // L block of item (t, b): forward L_{b,t} (rows of b, columns of t), backward L_{t,b}
-  auto issue = [&](const DenseItems<kFwd>& it, int slot) {
-    T* dst = ring + (size_t)slot * kT * kT;
-    constexpr int kC = SwzBlock<T>::kC, kChunks = kT * kT / kC;
-    const int rb = kFwd ? it.blk : it.t, cb = kFwd ? it.t : it.blk;
-    const int nrow = bw(rb), ncol = bw(cb);
-    for (int e = tid; e < kChunks; e += kThreads) {
-      const int k = e / (kT / kC), q = e - k * (kT / kC), r = q * kC;
-      const bool ok = k < ncol && r < nrow;
-      const T* src = ok ? P + (int64_t)rb * kT + r + (int64_t)(cb * kT + k) * ld : P;
-      cp_async16_zfill(dst + SwzBlock<T>::at(r, k), src, ok);
+  auto tile_ptr = [&](int r, int q) { return base + ((int64_t)r * (r + 1) / 2 + q) * (kT * kT); };
+  auto stage_L = [&](double* dst, int r0, int rb, int c0, int cb) {
+    for (int idx = threadIdx.x; idx < kT * kT; idx += kInvThreads) {
+      const int k = idx >> 6, r = idx & 63;
+      dst[r + k * kPld] = (r < rb && k < cb) ? (double)P[r0 + r + (int64_t)(c0 + k) * ld] : 0.0;
     }
   };
-  // stage diagonal block b (FP64, ld kPld) and its reciprocal diagonal
-  auto stage_diag = [&](int b) {
-    if (b < 0 || b >= nblk) return;
-    stage_block(Ad, P, ld, b * kT, bw(b), b * kT, bw(b));
-    __syncthreads();
-    if (tid < bw(b)) rinv[tid] = 1.0 / Ad[tid * (kPld + 1)];
-    __syncthreads();
-  };
-  // solve owned diagonal block b in place in its accumulator, publish it and store it in X
-  auto solve_diag = [&](int b) {
-    const int n = bw(b);
-    double* acc = acc_of(b);
-    __syncthreads();
-    block_trsv<kFwd>(acc, Ad, rinv, n, nr);
-    __syncthreads();
-    for (int idx = tid; idx < kT * nr; idx += kThreads) {
-      const int c = idx / kT, r = idx - c * kT;
-      xpub[idx] = r < n ? acc[idx] : 0.0;
-      if (r < n) X[b * kT + r + c * ldx] = acc[idx];
-    }
-  };
-
-  DenseItems<kFwd> prod, cons;
-  prod.start(nblk, C, rho);
-  cons.start(nblk, C, rho);
-#pragma unroll 1
-  for (int q = 0; q < kDenseStages - 1; ++q) {
-    if (prod.blk >= 0) {
-      issue(prod, q);
-      prod.next();
-    }
-    cp_async_commit();
-  }
-  int nq = 0;  // items consumed
-  // consume one item: X_blk -= L x_t (forward) or L^T x_t (backward), in the owned
-  // accumulator; xs holds x_t
-  auto consume = [&]() {
-    cp_async_wait<kDenseStages - 2>();
-    __syncthreads();
-    if (prod.blk >= 0) {
-      issue(prod, (nq + kDenseStages - 1) % kDenseStages);
-      prod.next();
-    }
-    cp_async_commit();
-    const T* Lb = ring + (size_t)(nq % kDenseStages) * kT * kT;
-    const int lane_i = tid & 63, part = tid >> 6;
-    double part_sum[kDenseRhs];
-#pragma unroll
-    for (int c = 0; c < kDenseRhs; ++c) part_sum[c] = 0.0;
-    if (kFwd) {  // row lane_i, columns part*16 ..
-#pragma unroll 4
-      for (int kk = 0; kk < 16; ++kk) {
-        const int k = part * 16 + kk;
-        const double l = (double)Lb[SwzBlock<T>::at(lane_i, k)];
-#pragma unroll
-        for (int c = 0; c < kDenseRhs; ++c)
-          if (c < nr) part_sum[c] = fma(l, xs[k + c * kT], part_sum[c]);
-      }
-    } else {  // column lane_i, rows part*16 ..
-#pragma unroll 4
-      for (int rr = 0; rr < 16; ++rr) {
-        const int r = part * 16 + rr;
-        const double l = (double)Lb[SwzBlock<T>::at(r, lane_i)];
-#pragma unroll
-        for (int c = 0; c < kDenseRhs; ++c)
-          if (c < nr) part_sum[c] = fma(l, xs[r + c * kT], part_sum[c]);
+  for (int i = j; i < nb; ++i) {
+    const int ci = (b0 + i) * kT, bi = min(kT, m.w - ci);
+    if (i > j) {  // Acc = sum_{k=j}^{i-1} L_ik Inv(k, j)
+      for (int k = j; k < i; ++k) {
+        const int ck = (b0 + k) * kT, bk = min(kT, m.w - ck);
+        stage_L(Ls, ci, bi, ck, bk);
+        const T* src = tile_ptr(k, j);
+        for (int idx = threadIdx.x; idx < kT * kT; idx += kInvThreads) {
+          const int kk = idx >> 6, r = idx & 63;
+          Ti[r + kk * kPld] = (double)__ldcg(src + idx);
+        }
+        __syncthreads();
+        if (k == j) gemm64<false>(Acc, Ls, Ti, 1.0);
+        else gemm64<true>(Acc, Ls, Ti, 1.0);
+        __syncthreads();
       }
     }
-#pragma unroll
-    for (int c = 0; c < kDenseRhs; ++c) red[(part * kT + lane_i) * kDenseRhs + c] = part_sum[c];
+    stage_L(Ls, ci, bi, ci, bi);
     __syncthreads();
-    if (tid < kT * nr) {
-      const int c = tid / kT, r = tid - c * kT;
-      acc_of(cons.blk)[r + c * kT] -= red[r * kDenseRhs + c] + red[(kT + r) * kDenseRhs + c] +
-                                      red[(2 * kT + r) * kDenseRhs + c] + red[(3 * kT + r) * kDenseRhs + c];
+    tri_inverse64(Ti, Ls, bi);
+    __syncthreads();
+    const double* out = Ti;
+    if (i > j) {  // Inv(i, j) = -L_ii^-1 Acc
+      gemm64<false>(Ls, Ti, Acc, -1.0);
+      __syncthreads();
+      out = Ls;
     }
-    ++nq;
-    cons.next();
-  };
-
-  // first block solved without any update: forward block 0, backward block nblk-1
-  const int b0 = kFwd ? 0 : nblk - 1;
-  int mydiag = kFwd ? rho : nblk - 1 - (((nblk - 1) - rho) % C + C) % C;  // next owned diagonal block
-  stage_diag(mydiag);
-  const bool own_first = b0 % C == rho;
-  if (own_first) {
-    solve_diag(b0);
-    mydiag += kFwd ? C : -C;
-  }
-  cluster_arrive();
-  if (own_first) stage_diag(mydiag);
-#pragma unroll 1
-  for (int step = 0; step + 1 < nblk; ++step) {
-    const int t = kFwd ? step : nblk - 1 - step, tn = kFwd ? t + 1 : t - 1;
-    cluster_wait();  // x_t is published
-    {
-      const double* src = map_rank(xpub, (unsigned)(t % C));
-      for (int idx = tid; idx < kT * nr; idx += kThreads) xs[idx] = src[idx];  // rows past the block are 0
+    T* dst = tile_ptr(i, j);
+    for (int idx = threadIdx.x; idx < kT * kT; idx += kInvThreads) {
+      const int kk = idx >> 6, r = idx & 63;
+      dst[idx] = (T)out[r + kk * kPld];
     }
     __syncthreads();
-    const bool own_next = tn % C == rho;
-    if (own_next) {
-      consume();  // item (t, tn) is this rank's first item of the step
-      solve_diag(tn);
-      mydiag += kFwd ? C : -C;
-    }
-    cluster_arrive();  // own_next: x_tn published; all: done reading x_t
-    while (cons.blk >= 0 && cons.t == t) consume();
-    if (own_next) stage_diag(mydiag);  // next owned diagonal block, off the chain
   }
-  cluster_wait();
-  cp_async_wait<0>();
-  if (!kFwd && rho == 0 && tid == 0) a.blkdone[s] = nblk;  // the root is done for the persistent sweep
 }
-
-int g_solve_grid = 0;
-int g_dense_cluster = 0;  // CTAs per dense-root cluster (0 = unavailable)
-
 
 }  // namespace
 
+int g_solve_grid = 0;    // CTAs of the persistent sweeps (resident CTAs of the device)
 int g_solve_grid16 = 0;  // CTAs of the persistent sweeps for <= 16 right-hand sides
 
 void init_solve_attributes() {
@@ -860,6 +830,8 @@ void init_solve_attributes() {
   for (auto f : {k_solve_forward<double, 16>, k_solve_backward<double, 16>, k_solve_forward<float, 16>,
                  k_solve_backward<float, 16>})
     cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)solve_smem<16>());
+  cudaFuncSetAttribute(k_sb_inverse<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kInvSmem);
+  cudaFuncSetAttribute(k_sb_inverse<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kInvSmem);
   int dev = 0, sms = 0, per = 0, per16 = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -869,66 +841,17 @@ void init_solve_attributes() {
   if (g_solve_grid <= 0) g_solve_grid = 148;
   g_solve_grid16 = sms * (per16 > 0 ? per16 : 1);
   if (g_solve_grid16 <= 0) g_solve_grid16 = g_solve_grid;
-  // dense-root cluster: 16 CTAs where the GPU can co-schedule them, else 8, else none
-  auto set_dense = [](auto f, size_t smem) {
-    cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaFuncSetAttribute(f, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
-  };
-  set_dense(k_solve_dense<double, true>, kDenseSmemMax);
-  set_dense(k_solve_dense<double, false>, kDenseSmemMax);
-  set_dense(k_solve_dense<float, true>, kDenseSmemMax);
-  set_dense(k_solve_dense<float, false>, kDenseSmemMax);
-  g_dense_cluster = 0;
-  for (int c : {16, 8}) {
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(c);
-    cfg.blockDim = dim3(kThreads);
-    cfg.dynamicSmemBytes = kDenseSmemMax;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = c;
-    attr[0].val.clusterDim.y = 1;
-    attr[0].val.clusterDim.z = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    int nclusters = 0;
-    if (cudaOccupancyMaxActiveClusters(&nclusters, k_solve_dense<double, true>, &cfg) == cudaSuccess &&
-        nclusters > 0) {
-      g_dense_cluster = c;
-      break;
-    }
-  }
-  cudaGetLastError();  // a refused cluster size is not an error of the handle
 }
 
-bool dense_solve_available(int nrhs, int w) {
-  if (g_dense_cluster <= 0 || nrhs < 1 || nrhs > kDenseRhs || w <= 0) return false;
-  const int nown = ((w + kT - 1) / kT + g_dense_cluster - 1) / g_dense_cluster;
-  return DenseSmem<double>(nown, nrhs).total <= kDenseSmemMax;
-}
-
-void launch_solve_dense(cudaStream_t st, const PSolveArgs& a, int s, int w, bool forward) {
-  const int nown = ((w + kT - 1) / kT + g_dense_cluster - 1) / g_dense_cluster;
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(g_dense_cluster);
-  cfg.blockDim = dim3(kThreads);
-  cfg.stream = st;
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeClusterDimension;
-  attr[0].val.clusterDim.x = g_dense_cluster;
-  attr[0].val.clusterDim.y = 1;
-  attr[0].val.clusterDim.z = 1;
-  cfg.attrs = attr;
-  cfg.numAttrs = 1;
-  if (a.fp32) {
-    cfg.dynamicSmemBytes = DenseSmem<float>(nown, a.nrhs).total;
-    if (forward) cudaLaunchKernelEx(&cfg, k_solve_dense<float, true>, a, s);
-    else cudaLaunchKernelEx(&cfg, k_solve_dense<float, false>, a, s);
-  } else {
-    cfg.dynamicSmemBytes = DenseSmem<double>(nown, a.nrhs).total;
-    if (forward) cudaLaunchKernelEx(&cfg, k_solve_dense<double, true>, a, s);
-    else cudaLaunchKernelEx(&cfg, k_solve_dense<double, false>, a, s);
-  }
+void launch_sb_inverse(cudaStream_t st, const void* L, void* Inv, bool fp32, const SnMeta* meta,
+                       const InvItem* items, int count, int sb) {
+  if (count <= 0) return;
+  if (fp32)
+    k_sb_inverse<float><<<count, kInvThreads, kInvSmem, st>>>(static_cast<const float*>(L), static_cast<float*>(Inv),
+                                                              meta, items, sb);
+  else
+    k_sb_inverse<double><<<count, kInvThreads, kInvSmem, st>>>(static_cast<const double*>(L),
+                                                               static_cast<double*>(Inv), meta, items, sb);
 }
 
 void launch_solve_persistent(cudaStream_t st, const PSolveArgs& a, bool forward) {

@@ -93,8 +93,9 @@ class symPACKOptions:
     fp32_engine: str = "tcgen05"   # FP32_IR update tiles: "tcgen05", "mma.sync", "tcgen05-persistent"
     decomposition: str = "LL"      # "LL" (Cholesky) or "LDL" (L D L^T, FP64), the driver's -fact
     plan_outer_nb: int = 0         # columns per outer block of wide panels (0 = library default 256)
-    plan_dense_min_w: int = 0      # narrowest dense root solved by one cluster (0 = default: never, -1 = never)
-    plan_solve_chunk: int = 0      # column blocks per forward off-diagonal solve task (0 = default 16)
+    plan_dense_min_w: int = 0      # accepted for compatibility, no effect (the super-block solve replaced it)
+    plan_solve_chunk: int = 0      # 64-column blocks per solve super-block (0 = library default 8)
+    plan_solve_tiles: int = 0      # 64 x 64 tiles per super-block solve task (0 = library default 2)
 
     def to_c(self) -> N.spb_options:
         if self.orderingStr not in N.ORDERINGS:
@@ -119,6 +120,7 @@ class symPACKOptions:
         o.plan_outer_nb = self.plan_outer_nb
         o.plan_dense_min_w = self.plan_dense_min_w
         o.plan_solve_chunk = self.plan_solve_chunk
+        o.plan_solve_tiles = self.plan_solve_tiles
         engines = {"tcgen05": 0, "mma.sync": 1, "tcgen05-persistent": 2}
         if self.fp32_engine not in engines:
             raise ValueError(f"unknown fp32_engine {self.fp32_engine!r}")

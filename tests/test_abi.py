@@ -87,9 +87,10 @@ def test_ldl_footprint_adds_the_scaled_copy():
         M = symPACKMatrix2D()
         M.Init(symPACKOptions(device=-1, decomposition=dec))
         M.SymbolicFactorization(A)
-        got[dec] = (M.PredictDeviceBytes(nrhs=1), M.info().arena_bytes)
+        got[dec] = (M.PredictDeviceBytes(nrhs=1), M.info().arena_bytes, M.info().inverse_bytes)
         M.close()
-    assert got["LDL"][0] - got["LL"][0] == got["LL"][1]  # one more FP64 arena (L D)
+    # one more FP64 arena (L D) and the inverses of its diagonal super-blocks
+    assert got["LDL"][0] - got["LL"][0] == got["LL"][1] + got["LL"][2]
 
 
 def test_host_only_analysis_predicts_footprint_and_is_reusable():

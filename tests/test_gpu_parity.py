@@ -277,7 +277,7 @@ def test_solve_trace_of_a_profiled_solve():
     M.Factorize()
     M.SetProfiling(True)
     M.Solve(np.ones(n))
-    for sweep, kinds in ((0, {0, 1, 2, 4}), (1, {0, 1, 3, 4})):  # 4: a small supernode in one task
+    for sweep, kinds in ((0, {0, 1, 2, 4, 5}), (1, {0, 1, 3, 4, 5})):  # 4: a small supernode in one task
         tr = M.GetSolveTrace(sweep).astype(np.int64)
         assert tr.shape[1] == 4 and len(tr) > 0
         t0, t1, t2, sk = tr.T
@@ -290,7 +290,7 @@ def test_solve_trace_of_a_profiled_solve():
 @pytest.mark.parametrize("opt", [dict(plan_outer_nb=64), dict(plan_outer_nb=512), dict(plan_solve_chunk=1),
                                  dict(plan_solve_chunk=3), dict(plan_small_max_w=16, plan_big_tile_rows=96),
                                  dict(plan_small_max_w=48, plan_big_tile_rows=256)],
-                         ids=["outer64", "outer512", "chunk1", "chunk3", "small16_rows96", "small48_rows256"])
+                         ids=["outer64", "outer512", "superblock1", "superblock3", "small16_rows96", "small48_rows256"])
 def test_plan_options_give_the_same_factor_and_solution(opt):
     """Every plan tunable changes only the schedule: factor and solution stay within the
     parity bound of the oracle."""
