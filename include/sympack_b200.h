@@ -93,7 +93,13 @@ typedef struct spb_options {
   int plan_solve_chunk;    /* 64-column blocks per solve super-block: a supernode wider than one block
                               is solved through the inverses of its diagonal super-blocks (0 = default 8) */
   int plan_solve_tiles;    /* 64 x 64 tiles per super-block solve task (0 = default 2) */
+  int factor_schedule;     /* FP64 factorization: SPB_FACTOR_PERSISTENT (default) runs every task in one
+                              persistent launch ordered by dependency counters; SPB_FACTOR_STEPS runs
+                              the level-ordered launch sequence (the FP32 form always does) */
 } spb_options;
+
+#define SPB_FACTOR_PERSISTENT 0
+#define SPB_FACTOR_STEPS 1
 
 typedef struct spb_info {
   int32_t n;
@@ -110,11 +116,14 @@ typedef struct spb_info {
   int32_t ncells;          /* reference 2D cells (K, I) */
   int32_t nblocks;         /* reference contiguous-row blocks */
   int32_t ir_iterations;   /* refinement steps of the last solve */
-  int32_t factor_launches; /* kernels in the factorization graph */
+  int32_t factor_launches; /* kernels of one factorization (1 for the persistent schedule) */
   double backward_error;   /* componentwise-free backward error of the last solve, if computed */
   int32_t dense_root_width; /* always 0 (a former cluster solve of the root; kept for layout) */
   int32_t pad_;
   int64_t inverse_bytes;    /* device bytes of the diagonal super-block inverses of one operand */
+  double factor_sched_us;   /* makespan the persistent factorization's ordering simulation predicts */
+  int32_t factor_tasks;     /* tasks of the persistent factorization */
+  int32_t pad2_;
 } spb_info;
 
 void spb_default_options(spb_options* opt);
@@ -208,14 +217,25 @@ int spb_get_factor(spb_handle* h, double* out);
 /* Status of the last factorization: code, supernode (0-based), column (0-based, permuted). */
 int spb_get_status(spb_handle* h, int32_t* code, int32_t* supernode, int32_t* column);
 
-/* Bound on every device-side wait of the persistent solve kernels, in polls
- * about 128 ns apart (default 2^24, a couple of seconds).  A wait that runs out
- * records a timeout; the call returns SPB_ERR_TIMEOUT and the context stays usable. */
+/* Bound on every device-side wait of the persistent solve and factorization
+ * kernels, in polls about 128 ns apart (default 2^24, a couple of seconds).  A wait
+ * that runs out records a timeout; the call returns SPB_ERR_TIMEOUT and the context
+ * stays usable. */
 int spb_set_wait_limit(spb_handle* h, int64_t polls);
 /* Test hook for failure detection: make the forward solve expect one more
  * incoming update for `supernode` than any task delivers (its wait then runs
  * out); -1 restores the true counts. */
 int spb_debug_stall(spb_handle* h, int32_t supernode);
+/* Test hook for failure detection: make the persistent factorization wait for one
+ * more external update into `supernode` than any task delivers; -1 restores. */
+int spb_debug_stall_factor(spb_handle* h, int32_t supernode);
+/* Per-task timeline of the persistent factorization (analysis): after
+ * spb_set_factor_trace(h, 1) every factorization records, per task in dispatch
+ * order, {handed out, dependencies met, done} (ns, globaltimer) and the SM;
+ * spb_get_factor_trace copies 4 * ntasks values and the task kinds
+ * (0 small panel, 1 diagonal block, 2 TRSM tile, 3 64 x 64 tile, 4 128 x 128 tile). */
+int spb_set_factor_trace(spb_handle* h, int32_t on);
+int spb_get_factor_trace(spb_handle* h, uint64_t* out, int64_t cap, int64_t* ntasks, int32_t* kinds);
 /* Reset the device status word (after a reported failure). */
 int spb_clear_status(spb_handle* h);
 

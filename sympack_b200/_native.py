@@ -52,6 +52,7 @@ class spb_options(C.Structure):
         ("plan_dense_min_w", C.c_int),
         ("plan_solve_chunk", C.c_int),
         ("plan_solve_tiles", C.c_int),
+        ("factor_schedule", C.c_int),
     ]
 
 
@@ -76,6 +77,9 @@ class spb_info(C.Structure):
         ("dense_root_width", C.c_int32),
         ("pad_", C.c_int32),
         ("inverse_bytes", C.c_int64),
+        ("factor_sched_us", C.c_double),
+        ("factor_tasks", C.c_int32),
+        ("pad2_", C.c_int32),
     ]
 
 
@@ -127,6 +131,9 @@ SIGNATURES = [
     ("spb_get_status", C.c_int, [_P, _I32P, _I32P, _I32P]),
     ("spb_set_wait_limit", C.c_int, [_P, C.c_int64]),
     ("spb_debug_stall", C.c_int, [_P, C.c_int32]),
+    ("spb_debug_stall_factor", C.c_int, [_P, C.c_int32]),
+    ("spb_set_factor_trace", C.c_int, [_P, C.c_int32]),
+    ("spb_get_factor_trace", C.c_int, [_P, C.POINTER(C.c_uint64), C.c_int64, C.POINTER(C.c_int64), _I32P]),
     ("spb_clear_status", C.c_int, [_P]),
     ("spb_set_stream", C.c_int, [_P, _P]),
     ("spb_set_profiling", C.c_int, [_P, C.c_int]),

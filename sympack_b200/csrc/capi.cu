@@ -59,6 +59,12 @@ struct spb_handle {
   spb::PanelItem* dpanel = nullptr;
   double* dwinv = nullptr;  // factored diagonal blocks (FP64) and 1/L_kk of one step
   spb::TileItem* dtiles = nullptr;
+  spb::FTask* dftasks = nullptr;   // persistent factorization: tasks, waits, signals, counters
+  spb::FWait* dfwaits = nullptr;
+  int32_t* dfsigs = nullptr;
+  int32_t* dfctr = nullptr;        // nfctr counters + the task counter
+  unsigned long long* dftrace = nullptr;  // factor trace (spb_set_factor_trace): 4 per task
+  bool factor_trace = false;
   int32_t* dinvp0 = nullptr;
   int32_t* dlevel_sn = nullptr;
   spb::SolveTask* dfwd = nullptr;
@@ -155,9 +161,14 @@ void release_device(spb_handle* h) {
   h->dW = nullptr;
   h->dX = h->dZ = h->dB = h->dR = h->dD = h->dXo = nullptr;
   h->dInv = h->dInvB = nullptr;
+  h->dftrace = nullptr;
   h->d_rowseg = nullptr;
   h->dtrace = nullptr;
   h->x_cap = 0;
+}
+
+bool persistent_factor(const spb_handle* h) {
+  return h->opt.precision == SPB_PRECISION_FP64 && h->opt.factor_schedule == SPB_FACTOR_PERSISTENT;
 }
 
 spb::dev::FactorArgs factor_args(spb_handle* h) {
@@ -197,6 +208,24 @@ cudaEvent_t lane_event(spb_handle* h, size_t i) {
 cudaError_t enqueue_factor(spb_handle* h) {
   const spb::Plan& P = h->plan;
   spb::dev::FactorArgs a = factor_args(h);
+  if (persistent_factor(h)) {  // every task in one launch, ordered by dependency counters
+    spb::dev::FactorSched f{};
+    f.tasks = h->dftasks;
+    f.ntasks = (int)P.ftasks.size();
+    f.waits = h->dfwaits;
+    f.sigs = h->dfsigs;
+    f.ctr = h->dfctr;
+    f.counter = h->dfctr + P.nfctr;
+    f.small_items = h->dsmall;
+    f.panel = h->dpanel;
+    f.tiles = h->dtiles;
+    f.winv = h->dwinv;
+    f.spin_limit = h->wait_limit;
+    f.trace = h->factor_trace ? h->dftrace : nullptr;
+    cudaMemsetAsync(h->dfctr, 0, sizeof(int32_t) * ((size_t)P.nfctr + 1), h->stream);
+    spb::dev::launch_factor_persistent(h->stream, a, f);
+    return cudaGetLastError();
+  }
   size_t nev = 0;
   std::vector<std::pair<int, cudaEvent_t>> side;  // (block, event) of this level's side updates
   size_t waited = 0;                               // side events the chain already waits for
@@ -712,6 +741,8 @@ int64_t predict_bytes(const spb_handle* h, bool fp32, int nrhs) {
   t += b(P.fwd_tasks.size(), sizeof(spb::SolveTask)) + b(P.bwd_tasks.size(), sizeof(spb::SolveTask));
   t += b(P.fwd_pending.size(), 4) + b(P.sparent.size(), 4) + b((int64_t)spb::solve_sync_ints(P), 4);
   t += b(P.inv_elems, fp32 ? sizeof(float) : sizeof(double)) + b(P.inv_items.size(), sizeof(spb::InvItem));
+  t += b(P.ftasks.size(), sizeof(spb::FTask)) + b(P.fwaits.size(), sizeof(spb::FWait)) + b(P.fsigs.size(), 4) +
+       b(P.nfctr + 1, 4);
   if (h->opt.decomposition == SPB_DECOMPOSITION_LDL) t += b(P.inv_elems, sizeof(double));
   t += b(1, sizeof(Status));
   if (fp32) {
@@ -794,6 +825,10 @@ int install_device(spb_handle* h) {
     h->dInv = inv;
   }
   SPB_CK(h, dalloc(h, &h->dinvitems, P.inv_items.size()));
+  SPB_CK(h, dalloc(h, &h->dftasks, P.ftasks.size()));
+  SPB_CK(h, dalloc(h, &h->dfwaits, P.fwaits.size()));
+  SPB_CK(h, dalloc(h, &h->dfsigs, P.fsigs.size()));
+  SPB_CK(h, dalloc(h, &h->dfctr, (size_t)P.nfctr + 1));
   if (h->ldl) {
     double* invb = nullptr;
     SPB_CK(h, dalloc(h, &invb, (size_t)P.inv_elems));
@@ -824,6 +859,9 @@ int install_device(spb_handle* h) {
   SPB_CK(h, up(h->dexpected, P.fwd_pending.data(), P.fwd_pending.size() * 4));
   SPB_CK(h, up(h->dsparent, P.sparent.data(), P.sparent.size() * 4));
   SPB_CK(h, up(h->dinvitems, P.inv_items.data(), P.inv_items.size() * sizeof(spb::InvItem)));
+  SPB_CK(h, up(h->dftasks, P.ftasks.data(), P.ftasks.size() * sizeof(spb::FTask)));
+  SPB_CK(h, up(h->dfwaits, P.fwaits.data(), P.fwaits.size() * sizeof(spb::FWait)));
+  SPB_CK(h, up(h->dfsigs, P.fsigs.data(), P.fsigs.size() * 4));
   SPB_CK(h, cudaMemsetAsync(h->dstatus, 0, sizeof(Status), h->stream));
   if (h->fp32) {
     // full symmetric CSR of A in the original ordering; csr_src maps each entry to its input value
@@ -1101,6 +1139,12 @@ int spb_factorize(spb_handle* h) {
                st.column + 1);
     return fail(h, SPB_ERR_NOT_SPD, msg);
   }
+  if (st.code == 3) {  // a bounded wait of the persistent factorization expired; the context is intact
+    SPB_CK(h, cudaMemsetAsync(h->dstatus, 0, sizeof(Status), h->stream));
+    SPB_CK(h, cudaStreamSynchronize(h->stream));
+    h->factored = false;
+    return fail(h, SPB_ERR_TIMEOUT, "factorize: a device wait expired");
+  }
   if (st.code != 0) return fail(h, SPB_ERR_STRUCTURE, "factorize: update row missing from target structure");
   return SPB_OK;
 }
@@ -1198,8 +1242,10 @@ int spb_get_info(spb_handle* h, spb_info* info) {
   info->flops_exec = P.exec_flops;
   info->ncells = (int32_t)h->cells.cells.size();
   info->nblocks = (int32_t)h->cells.block_first_row.size();
-  info->factor_launches = (int32_t)P.steps.size();
+  info->factor_launches = persistent_factor(h) ? 1 : (int32_t)P.steps.size();
   info->dense_root_width = 0;  // the cluster root solve gave way to the super-block solve
+  info->factor_sched_us = P.fsim_us;
+  info->factor_tasks = (int32_t)P.ftasks.size();
   info->inverse_bytes = P.inv_elems * (int64_t)(h->opt.precision == SPB_PRECISION_FP32_IR ? 4 : 8);
   info->ir_iterations = h->ir_iterations;
   info->backward_error = h->backward_error;
@@ -1320,6 +1366,47 @@ int spb_debug_stall(spb_handle* h, int32_t supernode) {
   SPB_CK(h, cudaMemcpyAsync(h->dexpected, e.data(), e.size() * 4, cudaMemcpyHostToDevice, h->stream));
   SPB_CK(h, cudaStreamSynchronize(h->stream));
   h->stall_supernode = supernode;
+  return SPB_OK;
+}
+
+int spb_set_factor_trace(spb_handle* h, int32_t on) {
+  if (check_handle(h)) return SPB_ERR_INVALID;
+  if (!h->have_symbolic || h->device < 0) return fail(h, SPB_ERR_STATE, "factor_trace: needs a device handle");
+  SPB_CK(h, cudaSetDevice(h->device));
+  if (on && !h->dftrace) {
+    SPB_CK(h, dalloc(h, &h->dftrace, 4 * std::max<size_t>(1, h->plan.ftasks.size())));
+    SPB_CK(h, cudaStreamSynchronize(h->own_stream));
+  }
+  if (h->fgraph) {  // the captured factorization holds the trace pointer: capture again
+    cudaGraphExecDestroy(h->fgraph);
+    h->fgraph = nullptr;
+  }
+  h->factor_trace = on != 0;
+  return SPB_OK;
+}
+
+int spb_get_factor_trace(spb_handle* h, uint64_t* out, int64_t cap, int64_t* ntasks, int32_t* kinds) {
+  if (check_handle(h)) return SPB_ERR_INVALID;
+  if (!h->dftrace) return fail(h, SPB_ERR_STATE, "factor_trace: no traced factorization");
+  const int64_t n = (int64_t)h->plan.ftasks.size();
+  if (ntasks) *ntasks = n;
+  if (!out) return SPB_OK;
+  if (cap < n) return fail(h, SPB_ERR_INVALID, "factor_trace: buffer too small");
+  SPB_CK(h, cudaMemcpy(out, h->dftrace, 4 * n * sizeof(uint64_t), cudaMemcpyDeviceToHost));
+  if (kinds)
+    for (int64_t i = 0; i < n; ++i) kinds[i] = h->plan.ftasks[i].kind;
+  return SPB_OK;
+}
+
+int spb_debug_stall_factor(spb_handle* h, int32_t supernode) {
+  if (check_handle(h)) return SPB_ERR_INVALID;
+  if (!h->have_symbolic || h->device < 0) return fail(h, SPB_ERR_STATE, "debug_stall_factor: needs a device handle");
+  if (supernode >= h->plan.nsuper) return fail(h, SPB_ERR_INVALID, "debug_stall_factor: supernode out of range");
+  std::vector<spb::FWait> w = h->plan.fwaits;
+  for (spb::FWait& x : w)
+    if (supernode >= 0 && x.ctr == supernode) x.target += 1;  // ext counters come first
+  SPB_CK(h, cudaMemcpyAsync(h->dfwaits, w.data(), w.size() * sizeof(spb::FWait), cudaMemcpyHostToDevice, h->stream));
+  SPB_CK(h, cudaStreamSynchronize(h->stream));
   return SPB_OK;
 }
 

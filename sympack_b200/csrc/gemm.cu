@@ -15,7 +15,7 @@
 #include <climits>
 #include <type_traits>
 
-#include "kernels.cuh"
+#include "factor_tasks.cuh"
 
 namespace spb {
 namespace dev {
@@ -132,12 +132,11 @@ __device__ __forceinline__ void dmma_16x8x4(double* d, double a0, double a1, dou
       : "d"(a0), "d"(a1), "d"(b0));
 }
 
-__global__ void __launch_bounds__(kDThreads, 1) k_gemm_dmma(FactorArgs a, const TileItem* __restrict__ items) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+// One 128 x 128 DMMA tile (kDThreads threads, kDSmemBytes of shared memory).
+__device__ void dmma_tile_task(const FactorArgs& a, const TileItem& it, unsigned char* smem_raw) {
   double* pipe = reinterpret_cast<double*>(smem_raw);
   double* Cs = reinterpret_cast<double*>(smem_raw);  // reused once the main loop is done
   int* ints = reinterpret_cast<int*>(smem_raw + kDMainBytes);
-  const TileItem it = items[blockIdx.x];
   const SnMeta m = a.meta[it.s];
   const double* g = static_cast<const double*>(a.L) + m.off;
   const double* gb = a.ldl ? a.W + m.off : g;  // second operand: L, or L D for LDL^T
@@ -219,19 +218,23 @@ __global__ void __launch_bounds__(kDThreads, 1) k_gemm_dmma(FactorArgs a, const 
   tile_epilogue<kDM, kDN, kDThreads, double, double>(a, it, m, Cs, kDLdc, (int64_t*)ints, (int64_t*)ints + 128);
 }
 
+__global__ void __launch_bounds__(kDThreads, 1) k_gemm_dmma(FactorArgs a, const TileItem* __restrict__ items) {
+  extern __shared__ __align__(16) unsigned char smem_dmma[];
+  dmma_tile_task(a, items[blockIdx.x], smem_dmma);
+}
+
 // ---- 64 x 64 FP64 FMA tile --------------------------------------------------------
 constexpr int kSLdc = 65;
 constexpr size_t kSCBytes = (size_t)64 * kSLdc * sizeof(double);
 constexpr size_t kSSmemBytes = kSCBytes + 4 * 64 * sizeof(int);
 
+// One 64 x 64 FMA tile (256 threads, kSSmemBytes of shared memory).
 template <class T>
-__global__ void __launch_bounds__(256) k_gemm_simt(FactorArgs a, const TileItem* __restrict__ items) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+__device__ void simt_tile_task(const FactorArgs& a, const TileItem& it, unsigned char* smem_raw) {
   T(*As)[64] = reinterpret_cast<T(*)[64]>(smem_raw);
   T(*Bs)[64] = reinterpret_cast<T(*)[64]>(smem_raw + 16 * 64 * sizeof(T));
   T* Cs = reinterpret_cast<T*>(smem_raw);
   int* ints = reinterpret_cast<int*>(smem_raw + kSCBytes);
-  const TileItem it = items[blockIdx.x];
   const SnMeta m = a.meta[it.s];
   const T* g = static_cast<const T*>(a.L) + m.off;
   // second operand: L, or L D for LDL^T (FP64 only, so W is read only when T is double)
@@ -272,6 +275,12 @@ __global__ void __launch_bounds__(256) k_gemm_simt(FactorArgs a, const TileItem*
     for (int j = 0; j < 4; ++j) Cs[(ty + 16 * i) + (tx + 16 * j) * kSLdc] = acc[i][j];
   __syncthreads();
   tile_epilogue<64, 64, 256, T, T>(a, it, m, Cs, kSLdc, (int64_t*)ints, (int64_t*)ints + 64);
+}
+
+template <class T>
+__global__ void __launch_bounds__(256) k_gemm_simt(FactorArgs a, const TileItem* __restrict__ items) {
+  extern __shared__ __align__(16) unsigned char smem_simt[];
+  simt_tile_task<T>(a, items[blockIdx.x], smem_simt);
 }
 
 // ---- 128 x 128 split-precision 3xTF32 tensor-core tile (FP32 storage) -------------
@@ -917,6 +926,108 @@ __global__ void __launch_bounds__(kPThreads, 1) k_gemm_tc32p(FactorArgs a, const
 
 static int g_sms = 148;  // persistent tile grid: one CTA per SM
 
+// ---- persistent factorization ------------------------------------------------------
+// One CTA per SM takes the tasks of Plan::ftasks in order from an atomic counter,
+// waits until the counters it depends on reach their targets (thread 0 polls with
+// acquire loads, bounded), runs the task body with the whole block and publishes with
+// release reductions on the counters it bumps.  The order is topological, so every
+// task a CTA waits for was handed out earlier to a running CTA.
+namespace {
+
+__device__ __forceinline__ int ld_acquire_i(const int32_t* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void red_release_i(int32_t* p, int v) {
+  asm volatile("red.release.gpu.global.add.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ int status_of(const Status* st) { return *(volatile const int32_t*)&st->code; }
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ unsigned smid() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%smid;" : "=r"(r));
+  return r;
+}
+
+constexpr size_t kFSmemBytes = kDSmemBytes;  // the largest task body (the DMMA tile)
+
+__global__ void __launch_bounds__(256, 1) k_factor_persistent(FactorArgs a, FactorSched f) {
+  extern __shared__ __align__(16) unsigned char smem_f[];
+  __shared__ int sh_task, sh_go;
+  for (;;) {
+    if (threadIdx.x == 0) {
+      int tk = atomicAdd(f.counter, 1);
+      int go = tk < f.ntasks && status_of(a.status) == 0;
+      if (go && f.trace) f.trace[4 * (size_t)tk] = global_ns();
+      if (go) {
+        const FTask t = f.tasks[tk];
+        for (int w = 0; w < t.nwait && go; ++w) {
+          const FWait fw = f.waits[t.wait0 + w];
+          const int32_t* c = f.ctr + fw.ctr;
+          if (ld_acquire_i(c) >= fw.target) continue;
+          go = 0;
+          for (long long it = 0; it < f.spin_limit; ++it) {
+            if (it >= 256) __nanosleep(128);
+            if (ld_acquire_i(c) >= fw.target) {
+              go = 1;
+              break;
+            }
+            if (status_of(a.status) != 0) break;
+          }
+          if (!go && atomicCAS(&a.status->code, 0, 3) == 0) {  // a wait expired
+            a.status->supernode = -1;
+            a.status->column = fw.ctr;
+          }
+        }
+      }
+      if (go && f.trace) {
+        f.trace[4 * (size_t)tk + 1] = global_ns();
+        f.trace[4 * (size_t)tk + 3] = smid();
+      }
+      sh_task = tk;
+      sh_go = go;
+    }
+    __syncthreads();
+    const int tk = sh_task;
+    if (!sh_go) return;
+    const FTask t = f.tasks[tk];
+    switch (t.kind) {
+      case 0:
+        ftask::factor_small_task<double>(a, f.small_items[t.item], reinterpret_cast<double*>(smem_f));
+        break;
+      case 1:
+        if (a.ldl) ftask::ldl_diag_task<double>(a, f.panel[t.item], f.winv, reinterpret_cast<double*>(smem_f));
+        else ftask::potrf_diag_task<double>(a, f.panel[t.item], f.winv, reinterpret_cast<double*>(smem_f));
+        break;
+      case 2:
+        ftask::trsm_rows_task<double>(a, f.panel[t.item], f.winv, reinterpret_cast<double*>(smem_f));
+        break;
+      case 3:
+        simt_tile_task<double>(a, f.tiles[t.item], smem_f);
+        break;
+      default:
+        dmma_tile_task(a, f.tiles[t.item], smem_f);
+        break;
+    }
+    __syncthreads();
+    if (f.trace && threadIdx.x == 0) f.trace[4 * (size_t)tk + 2] = global_ns();
+    for (int i = threadIdx.x; i < t.nsig; i += blockDim.x) red_release_i(f.ctr + f.sigs[t.sig0 + i], 1);
+  }
+}
+
+}  // namespace
+
+void launch_factor_persistent(cudaStream_t st, const FactorArgs& a, const FactorSched& f) {
+  if (f.ntasks <= 0 || f.spin_limit <= 0) return;
+  const int grid = g_sms < f.ntasks ? g_sms : f.ntasks;
+  k_factor_persistent<<<grid, 256, kFSmemBytes, st>>>(a, f);
+}
+
 void init_gemm_attributes() {
   int dev = 0;
   if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, dev);
@@ -925,6 +1036,7 @@ void init_gemm_attributes() {
   cudaFuncSetAttribute(k_gemm_tc32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kUSmemBytes);
   cudaFuncSetAttribute(k_gemm_tc32p, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPSmemBytes);
   cudaFuncSetAttribute(k_gemm_dmma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDSmemBytes);
+  cudaFuncSetAttribute(k_factor_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFSmemBytes);
 }
 
 void launch_gemm(cudaStream_t st, const FactorArgs& a, const TileItem* items, int count, int tile) {

@@ -15,73 +15,14 @@
 #include <climits>
 #include <cstdio>
 
-#include "kernels.cuh"
+#include "factor_tasks.cuh"
 
 namespace spb {
 namespace dev {
 
 namespace {
 
-__device__ __forceinline__ void report(Status* st, int code, int s, int col) {
-  if (atomicCAS(&st->code, 0, code) == 0) {
-    st->supernode = s;
-    st->column = col;
-  }
-}
-
-// Unblocked right-looking Cholesky of an h x w column-major panel held in
-// shared memory (leading dimension ldp): the w x w top block becomes L_II and
-// the rows below become L_KI = A_KI L_II^-T.  All threads of the block take part.
-__device__ void panel_cholesky_smem(double* P, int h, int w, int ldp, Status* status, int s, int fc) {
-  const int tid = threadIdx.x, nthr = blockDim.x;
-  const int warp = tid >> 5, lane = tid & 31, nw = nthr >> 5;
-  for (int k = 0; k < w; ++k) {
-    if (tid == 0) {
-      double d = P[k + k * ldp];
-      if (!(d > 0.0)) {
-        if (status) report(status, 1, s, fc + k);
-        d = 1.0;
-      }
-      P[k + k * ldp] = sqrt(d);
-    }
-    __syncthreads();
-    const double inv = 1.0 / P[k + k * ldp];
-    for (int i = k + 1 + tid; i < h; i += nthr) P[i + k * ldp] *= inv;
-    __syncthreads();
-    for (int j = k + 1 + warp; j < w; j += nw) {
-      const double ljk = P[j + k * ldp];
-      for (int i = j + lane; i < h; i += 32) P[i + j * ldp] -= P[i + k * ldp] * ljk;
-    }
-    __syncthreads();
-  }
-}
-
-// LDL^T counterpart: the w x w top block becomes unit L_II with D on its diagonal,
-// the rows below L_KI = A_KI L_II^-T D^-1.  Column k's trailing update uses the
-// column before it is scaled (A_ij -= A_ik A_jk / d_k).  A zero pivot is reported
-// (status 1) and replaced by 1 so that the factorization runs to its end.
-__device__ void panel_ldl_smem(double* P, int h, int w, int ldp, Status* status, int s, int fc) {
-  const int tid = threadIdx.x, nthr = blockDim.x;
-  const int warp = tid >> 5, lane = tid & 31, nw = nthr >> 5;
-  for (int k = 0; k < w; ++k) {
-    if (tid == 0) {
-      const double d = P[k + k * ldp];
-      if (!(fabs(d) > 0.0)) {
-        if (status) report(status, 1, s, fc + k);
-        P[k + k * ldp] = 1.0;
-      }
-    }
-    __syncthreads();
-    const double dinv = 1.0 / P[k + k * ldp];
-    for (int j = k + 1 + warp; j < w; j += nw) {
-      const double ljk = P[j + k * ldp] * dinv;
-      for (int i = j + lane; i < h; i += 32) P[i + j * ldp] -= P[i + k * ldp] * ljk;
-    }
-    __syncthreads();
-    for (int i = k + 1 + tid; i < h; i += nthr) P[i + k * ldp] *= dinv;
-    __syncthreads();
-  }
-}
+using namespace ftask;
 
 template <class T>
 __global__ void k_assemble(T* __restrict__ L, const int64_t* __restrict__ dst, const double* __restrict__ vals,
@@ -92,427 +33,29 @@ __global__ void k_assemble(T* __restrict__ L, const int64_t* __restrict__ dst, c
 
 template <class T>
 __global__ void __launch_bounds__(128) k_factor_small(FactorArgs a, const int32_t* __restrict__ items) {
-  extern __shared__ double P[];
-  const int s = items[blockIdx.x];
-  const SnMeta m = a.meta[s];
-  const int h = m.h, w = m.w;
-  T* g = static_cast<T*>(a.L) + m.off;
-  for (int idx = threadIdx.x; idx < h * w; idx += blockDim.x) {
-    int c = idx / h, r = idx - c * h;
-    P[idx] = (double)g[r + (int64_t)c * m.ld];
-  }
-  __syncthreads();
-  if (a.ldl) {
-    panel_ldl_smem(P, h, w, h, a.status, s, m.fc);
-    double* gw = a.W + m.off;
-    for (int idx = threadIdx.x; idx < h * w; idx += blockDim.x) {
-      const int c = idx / h, r = idx - c * h;
-      const double v = P[idx], d = P[c + c * h];
-      g[r + (int64_t)c * m.ld] = (T)(r == c ? 1.0 : v);
-      gw[r + (int64_t)c * m.ld] = r == c ? d : (r > c ? v * d : 0.0);
-    }
-    return;
-  }
-  panel_cholesky_smem(P, h, w, h, a.status, s, m.fc);
-  for (int idx = threadIdx.x; idx < h * w; idx += blockDim.x) {
-    int c = idx / h, r = idx - c * h;
-    g[r + (int64_t)c * m.ld] = (T)P[idx];
-  }
+  extern __shared__ double sm_small[];
+  factor_small_task<T>(a, items[blockIdx.x], sm_small);
 }
-
-constexpr int kNB = 64;
-constexpr int kThreads = 256;  // threads of the POTRF and TRSM kernels
-
-// POTRF of one 64-column diagonal block [c0, c0+nb) of a wide panel (one CTA
-// per item), right-looking by 8-column pieces in shared memory.  Every thread factors
-// the 8 x 8 diagonal piece itself, in registers, from the same shared-memory values (the
-// same operations in the same order, so every copy is identical): no shuffles and no
-// barrier between the piece and the solve of the rows below, which each thread then
-// does for its own row against its register copy.  The factored pieces go to a side
-// array (other threads may still be reading the unfactored piece) and into the block at
-// the end.  The trailing lower triangle is updated with the solved columns (thread
-// (row, group) updates columns group, group+4, ... of its row).  Two barriers per
-// piece.  The CTA also copies the factored block (FP64) and 1/L_kk to its scratch
-// slot, from where the TRSM of the rows below reads them.  A block narrower than 64 is
-// padded with the identity.  The kernel sits on the critical path of every wide
-// supernode and is latency-bound.
-constexpr int kDL = kNB + 1;  // padded leading dimension in shared memory
-// scratch slot: factored block (FP64), 1/L_kk, and (LDL^T) 1/D_kk
-constexpr size_t kSlot = kDiagSlotDoubles;
-static_assert(kSlot >= (size_t)kNB * kNB + 2 * kNB, "slot layout");
-constexpr int kPiece = 8;
-constexpr int kTri = kPiece * (kPiece + 1) / 2;  // entries of a lower-triangular piece
-__host__ __device__ constexpr int tri(int i, int j) { return i * (i + 1) / 2 + j; }  // i >= j
 
 template <class T>
 __global__ void __launch_bounds__(kThreads, 1) k_potrf_diag(FactorArgs a, const PanelItem* __restrict__ items,
                                                          double* __restrict__ winv) {
-  __shared__ double D[kNB * kDL];
-  __shared__ double Lp[kNB / kPiece][kTri];  // factored diagonal pieces
-  __shared__ double Rinv[kNB];               // 1 / L_kk
-  const PanelItem it = items[blockIdx.x];
-  const SnMeta m = a.meta[it.s];
-  const T* g = static_cast<const T*>(a.L) + m.off;
-  const int nb = it.nb, c0 = it.c0;
-  const int64_t ld = m.ld;
-  const int tid = threadIdx.x;
-  {
-    double v[kNB * kNB / kThreads];
-#pragma unroll
-    for (int q = 0; q < kNB * kNB / kThreads; ++q) {
-      const int idx = tid + q * kThreads, c = idx / kNB, r = idx - c * kNB;
-      v[q] = (r < nb && c < nb && r >= c) ? (double)g[(c0 + r) + (int64_t)(c0 + c) * ld] : (r == c ? 1.0 : 0.0);
-    }
-#pragma unroll
-    for (int q = 0; q < kNB * kNB / kThreads; ++q) {
-      const int idx = tid + q * kThreads, c = idx / kNB, r = idx - c * kNB;
-      D[r + c * kDL] = v[q];
-    }
-  }
-  __syncthreads();
-  const int urow = tid & 63, ugrp = tid >> 6;  // update mapping: row kb+8+urow, columns kb+8+ugrp+4t
-#pragma unroll 1
-  for (int kb = 0; kb < kNB; kb += kPiece) {
-    // the 8 x 8 piece, factored by every thread
-    double l[kTri], rs[kPiece];
-#pragma unroll
-    for (int i = 0; i < kPiece; ++i)
-#pragma unroll
-      for (int j = 0; j <= i; ++j) l[tri(i, j)] = D[kb + i + (kb + j) * kDL];
-#pragma unroll
-    for (int k = 0; k < kPiece; ++k) {
-      double dkk = l[tri(k, k)];
-      if (!(dkk > 0.0)) {
-        if (tid == 0 && kb + k < nb) report(a.status, 1, it.s, m.fc + c0 + kb + k);
-        dkk = 1.0;
-      }
-      rs[k] = rsqrt(dkk);
-      l[tri(k, k)] = dkk * rs[k];
-#pragma unroll
-      for (int i = k + 1; i < kPiece; ++i) l[tri(i, k)] *= rs[k];
-#pragma unroll
-      for (int j = k + 1; j < kPiece; ++j)
-#pragma unroll
-        for (int i = j; i < kPiece; ++i) l[tri(i, j)] = fma(-l[tri(i, k)], l[tri(j, k)], l[tri(i, j)]);
-    }
-    if (tid < kTri) {
-      double mine = 0.0;
-#pragma unroll
-      for (int e = 0; e < kTri; ++e)
-        if (e == tid) mine = l[e];
-      Lp[kb / kPiece][tid] = mine;
-    }
-    if (tid < kPiece) {
-      double mine = 0.0;
-#pragma unroll
-      for (int e = 0; e < kPiece; ++e)
-        if (e == tid) mine = rs[e];
-      Rinv[kb + tid] = mine;
-    }
-    const int below = kNB - kb - kPiece;
-    if (below == 0) break;
-    if (tid < below) {  // one row per thread: solve against the piece
-      const int i = kb + kPiece + tid;
-      double x[kPiece];
-#pragma unroll
-      for (int j = 0; j < kPiece; ++j) x[j] = D[i + (kb + j) * kDL];
-#pragma unroll
-      for (int k = 0; k < kPiece; ++k) {
-        double t = x[k];
-#pragma unroll
-        for (int j = 0; j < k; ++j) t = fma(-x[j], l[tri(k, j)], t);
-        x[k] = t * rs[k];
-      }
-#pragma unroll
-      for (int j = 0; j < kPiece; ++j) D[i + (kb + j) * kDL] = x[j];
-    }
-    __syncthreads();
-    if (urow < below) {
-      const int i = kb + kPiece + urow;
-      double x[kPiece];
-#pragma unroll
-      for (int k = 0; k < kPiece; ++k) x[k] = D[i + (kb + k) * kDL];
-      for (int j = kb + kPiece + ugrp; j <= i; j += 4) {
-        double t0 = D[i + j * kDL], t1 = 0.0;
-#pragma unroll
-        for (int k = 0; k < kPiece; k += 2) {
-          t0 = fma(-x[k], D[j + (kb + k) * kDL], t0);
-          t1 = fma(-x[k + 1], D[j + (kb + k + 1) * kDL], t1);
-        }
-        D[i + j * kDL] = t0 + t1;
-      }
-    }
-    __syncthreads();
-  }
-  __syncthreads();
-  // factored pieces into the block
-  for (int e = tid; e < (kNB / kPiece) * kTri; e += kThreads) {
-    const int p = e / kTri, q = e - p * kTri;
-    int i = 0;
-    while (tri(i + 1, 0) <= q) ++i;
-    const int j = q - tri(i, 0);
-    D[p * kPiece + i + (p * kPiece + j) * kDL] = Lp[p][q];
-  }
-  __syncthreads();
-  T* gw = static_cast<T*>(a.L) + m.off;
-#pragma unroll
-  for (int q = 0; q < kNB * kNB / kThreads; ++q) {
-    const int idx = tid + q * kThreads, c = idx / kNB, r = idx - c * kNB;
-    if (r < nb && c < nb && r >= c) gw[(c0 + r) + (int64_t)(c0 + c) * ld] = (T)D[r + c * kDL];
-  }
-  // FP64 copy of the factored block and 1/L_kk for the TRSM of the rows below
-  if (winv) {
-    double* W = winv + (size_t)it.slot * kSlot;
-#pragma unroll
-    for (int q = 0; q < kNB * kNB / kThreads; ++q) {
-      const int idx = tid + q * kThreads, c = idx / kNB, r = idx - c * kNB;
-      W[idx] = D[r + c * kDL];
-    }
-    if (tid < kNB) W[kNB * kNB + tid] = Rinv[tid];
-  }
+  extern __shared__ double sm_diag[];
+  potrf_diag_task<T>(a, items[blockIdx.x], winv, sm_diag);
 }
 
-// LDL^T of one 64-column diagonal block [c0, c0+nb) (one CTA per item), right-looking by
-// 8-column pieces like k_potrf_diag: every thread factors the piece itself in registers
-// (Potf2_LDL, lapack.hpp:206-270, on the lower triangle: d_k = A_kk, |d_k| > 0 or the
-// pivot is reported as a zero pivot; column k is divided by d_k; A_ij loses L_ik A_jk),
-// then each row below solves w = r L^-T against the unit piece (w is that row of L D)
-// and stores r's L values w / d; the trailing triangle loses W_ik L_jk.  L takes the
-// unit block, W the block times D (its diagonal is D), the scratch slot the unit block,
-// 1 in place of 1/L_kk (the TRSM of the rows below then computes R L11^-T, which is W's
-// rows) and 1/D_kk.
 template <class T>
 __global__ void __launch_bounds__(kThreads, 1) k_ldl_diag(FactorArgs a, const PanelItem* __restrict__ items,
                                                        double* __restrict__ winv) {
-  __shared__ double D[kNB * kDL];
-  __shared__ double Lp[kNB / kPiece][kTri];  // factored pieces: unit L below, d on the diagonal
-  __shared__ double Wr[kNB * kPiece];        // rows below the current piece: W = L D, ld kNB
-  __shared__ double Dk[kNB];
-  const PanelItem it = items[blockIdx.x];
-  const SnMeta m = a.meta[it.s];
-  T* g = static_cast<T*>(a.L) + m.off;
-  const int nb = it.nb, c0 = it.c0;
-  const int64_t ld = m.ld;
-  const int tid = threadIdx.x;
-  {
-    double v[kNB * kNB / kThreads];
-#pragma unroll
-    for (int q = 0; q < kNB * kNB / kThreads; ++q) {
-      const int idx = tid + q * kThreads, c = idx / kNB, r = idx - c * kNB;
-      v[q] = (r < nb && c < nb && r >= c) ? (double)g[(c0 + r) + (int64_t)(c0 + c) * ld] : (r == c ? 1.0 : 0.0);
-    }
-#pragma unroll
-    for (int q = 0; q < kNB * kNB / kThreads; ++q) {
-      const int idx = tid + q * kThreads, c = idx / kNB, r = idx - c * kNB;
-      D[r + c * kDL] = v[q];
-    }
-  }
-  __syncthreads();
-  const int urow = tid & 63, ugrp = tid >> 6;
-#pragma unroll 1
-  for (int kb = 0; kb < kNB; kb += kPiece) {
-    double l[kTri], dinv[kPiece];
-#pragma unroll
-    for (int i = 0; i < kPiece; ++i)
-#pragma unroll
-      for (int j = 0; j <= i; ++j) l[tri(i, j)] = D[kb + i + (kb + j) * kDL];
-#pragma unroll
-    for (int k = 0; k < kPiece; ++k) {
-      double d = l[tri(k, k)];
-      if (!(fabs(d) > 0.0)) {
-        if (tid == 0 && kb + k < nb) report(a.status, 1, it.s, m.fc + c0 + kb + k);
-        d = 1.0;
-        l[tri(k, k)] = 1.0;
-      }
-      dinv[k] = 1.0 / d;
-      double w[kPiece];
-#pragma unroll
-      for (int i = k + 1; i < kPiece; ++i) {
-        w[i] = l[tri(i, k)];
-        l[tri(i, k)] = w[i] * dinv[k];
-      }
-#pragma unroll
-      for (int j = k + 1; j < kPiece; ++j)
-#pragma unroll
-        for (int i = j; i < kPiece; ++i) l[tri(i, j)] = fma(-l[tri(i, k)], w[j], l[tri(i, j)]);
-    }
-    if (tid < kTri) {
-      double mine = 0.0;
-#pragma unroll
-      for (int e = 0; e < kTri; ++e)
-        if (e == tid) mine = l[e];
-      Lp[kb / kPiece][tid] = mine;
-    }
-    if (tid < kPiece) {
-      double mine = 0.0;
-#pragma unroll
-      for (int e = 0; e < kPiece; ++e)
-        if (e == tid) mine = l[tri(e, e)];
-      Dk[kb + tid] = mine;
-    }
-    const int below = kNB - kb - kPiece;
-    if (below == 0) break;
-    if (tid < below) {  // one row per thread: w = r L^-T (unit piece), L row = w / d
-      const int i = kb + kPiece + tid;
-      double x[kPiece];
-#pragma unroll
-      for (int j = 0; j < kPiece; ++j) x[j] = D[i + (kb + j) * kDL];
-#pragma unroll
-      for (int k = 0; k < kPiece; ++k) {
-        double t = x[k];
-#pragma unroll
-        for (int j = 0; j < k; ++j) t = fma(-x[j], l[tri(k, j)], t);
-        x[k] = t;
-      }
-#pragma unroll
-      for (int j = 0; j < kPiece; ++j) {
-        Wr[i + j * kNB] = x[j];
-        D[i + (kb + j) * kDL] = x[j] * dinv[j];
-      }
-    }
-    __syncthreads();
-    if (urow < below) {
-      const int i = kb + kPiece + urow;
-      double x[kPiece];
-#pragma unroll
-      for (int k = 0; k < kPiece; ++k) x[k] = Wr[i + k * kNB];
-      for (int j = kb + kPiece + ugrp; j <= i; j += 4) {
-        double t0 = D[i + j * kDL], t1 = 0.0;
-#pragma unroll
-        for (int k = 0; k < kPiece; k += 2) {
-          t0 = fma(-x[k], D[j + (kb + k) * kDL], t0);
-          t1 = fma(-x[k + 1], D[j + (kb + k + 1) * kDL], t1);
-        }
-        D[i + j * kDL] = t0 + t1;
-      }
-    }
-    __syncthreads();
-  }
-  __syncthreads();
-  for (int e = tid; e < (kNB / kPiece) * kTri; e += kThreads) {
-    const int p = e / kTri, q = e - p * kTri;
-    int i = 0;
-    while (tri(i + 1, 0) <= q) ++i;
-    const int j = q - tri(i, 0);
-    D[p * kPiece + i + (p * kPiece + j) * kDL] = i == j ? 1.0 : Lp[p][q];
-  }
-  __syncthreads();
-  double* gw = a.W + m.off;
-#pragma unroll
-  for (int q = 0; q < kNB * kNB / kThreads; ++q) {
-    const int idx = tid + q * kThreads, c = idx / kNB, r = idx - c * kNB;
-    if (r < nb && c < nb && r >= c) {
-      const double l = D[r + c * kDL];
-      g[(c0 + r) + (int64_t)(c0 + c) * ld] = (T)l;
-      gw[(c0 + r) + (int64_t)(c0 + c) * ld] = r == c ? Dk[c] : l * Dk[c];
-    }
-  }
-  if (winv) {
-    double* S = winv + (size_t)it.slot * kSlot;
-#pragma unroll
-    for (int q = 0; q < kNB * kNB / kThreads; ++q) {
-      const int idx = tid + q * kThreads, c = idx / kNB, r = idx - c * kNB;
-      S[idx] = D[r + c * kDL];
-    }
-    if (tid < kNB) {
-      S[kNB * kNB + tid] = 1.0;
-      S[kNB * kNB + kNB + tid] = 1.0 / Dk[tid];
-    }
-  }
+  extern __shared__ double sm_ldl[];
+  ldl_diag_task<T>(a, items[blockIdx.x], winv, sm_ldl);
 }
 
-// TRSM of one 64-row tile below a factored diagonal block, R <- R L11^-T, by
-// 8-column pieces: each row solves against the 8 x 8 diagonal piece (one
-// thread per row), then the remaining columns of the tile are updated with the
-// solved piece (thread (row, group) takes columns group, group+4, ...).  L11
-// and 1/L_kk come from the scratch slot.  All loads are issued before the first
-// use (32 per thread in flight).
 template <class T>
 __global__ void __launch_bounds__(kThreads, 2) k_trsm_rows(FactorArgs a, const PanelItem* __restrict__ items,
                                                         const double* __restrict__ winv) {
-  extern __shared__ double smem_tr[];
-  double* R = smem_tr;               // R[r + k*kDL]
-  double* D = smem_tr + kNB * kDL;   // D[i + j*kDL] = L11[i][j]
-  __shared__ double Rinv[kNB];
-  const PanelItem it = items[blockIdx.x];
-  const SnMeta m = a.meta[it.s];
-  T* g = static_cast<T*>(a.L) + m.off;
-  const int nb = it.nb, c0 = it.c0;
-  const int64_t ld = m.ld;
-  const int rows = min(kNB, m.h - it.row0);
-  const double* W = winv + (size_t)it.slot * kSlot;
-  const int tid = threadIdx.x;
-  {
-    double v[kNB * kNB / kThreads], w[kNB * kNB / kThreads];
-#pragma unroll
-    for (int q = 0; q < kNB * kNB / kThreads; ++q) {
-      const int idx = tid + q * kThreads, k = idx / kNB, r = idx - k * kNB;
-      v[q] = (r < rows && k < nb) ? (double)g[(it.row0 + r) + (int64_t)(c0 + k) * ld] : 0.0;
-      w[q] = W[idx];
-    }
-#pragma unroll
-    for (int q = 0; q < kNB * kNB / kThreads; ++q) {
-      const int idx = tid + q * kThreads, k = idx / kNB, r = idx - k * kNB;
-      R[r + k * kDL] = v[q];
-      D[r + k * kDL] = w[q];
-    }
-  }
-  if (tid < kNB) Rinv[tid] = W[kNB * kNB + tid];
-  __syncthreads();
-  const int urow = tid & 63, ugrp = tid >> 6;
-#pragma unroll 1
-  for (int kb = 0; kb < nb; kb += kPiece) {
-    if (tid < rows) {
-      double x[kPiece];
-#pragma unroll
-      for (int j = 0; j < kPiece; ++j) x[j] = R[tid + (kb + j) * kDL];
-#pragma unroll
-      for (int k = 0; k < kPiece; ++k) {
-        double t = x[k];
-#pragma unroll
-        for (int j = 0; j < k; ++j) t = fma(-x[j], D[kb + k + (kb + j) * kDL], t);
-        x[k] = t * Rinv[kb + k];
-      }
-#pragma unroll
-      for (int j = 0; j < kPiece; ++j) R[tid + (kb + j) * kDL] = x[j];
-    }
-    __syncthreads();
-    if (kb + kPiece >= nb) break;
-    if (urow < rows) {
-      double x[kPiece];
-#pragma unroll
-      for (int k = 0; k < kPiece; ++k) x[k] = R[urow + (kb + k) * kDL];
-      for (int j = kb + kPiece + ugrp; j < nb; j += 4) {
-        double t0 = R[urow + j * kDL], t1 = 0.0;
-#pragma unroll
-        for (int k = 0; k < kPiece; k += 2) {
-          t0 = fma(-x[k], D[j + (kb + k) * kDL], t0);
-          t1 = fma(-x[k + 1], D[j + (kb + k + 1) * kDL], t1);
-        }
-        R[urow + j * kDL] = t0 + t1;
-      }
-    }
-    __syncthreads();
-  }
-  if (a.ldl) {  // R is W's rows (R L11^-T with unit L11); L's rows are R D^-1
-    const double* dinv = W + kNB * kNB + kNB;
-    double* gw = a.W + m.off;
-#pragma unroll
-    for (int q = 0; q < kNB * kNB / kThreads; ++q) {
-      const int idx = tid + q * kThreads, k = idx / kNB, r = idx - k * kNB;
-      if (r < rows && k < nb) {
-        const double v = R[r + k * kDL];
-        g[(it.row0 + r) + (int64_t)(c0 + k) * ld] = (T)(v * dinv[k]);
-        gw[(it.row0 + r) + (int64_t)(c0 + k) * ld] = v;
-      }
-    }
-    return;
-  }
-#pragma unroll
-  for (int q = 0; q < kNB * kNB / kThreads; ++q) {
-    const int idx = tid + q * kThreads, k = idx / kNB, r = idx - k * kNB;
-    if (r < rows && k < nb) g[(it.row0 + r) + (int64_t)(c0 + k) * ld] = (T)R[r + k * kDL];
-  }
+  extern __shared__ double sm_trsm[];
+  trsm_rows_task<T>(a, items[blockIdx.x], winv, sm_trsm);
 }
 
 __global__ void k_permute_in(double* X, int64_t ldx, const double* B, int64_t ldb, const int32_t* invp0, int n,
@@ -548,7 +91,7 @@ void launch_assemble(cudaStream_t st, double* L, const int64_t* dst, const doubl
 
 void init_kernel_attributes() {
   for (auto f : {k_trsm_rows<double>, k_trsm_rows<float>})
-    cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * kNB * kDL * (int)sizeof(double));
+    cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, kTrsmSmemDoubles * (int)sizeof(double));
   for (auto f : {k_factor_small<double>, k_factor_small<float>})
     cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
   init_gemm_attributes();
@@ -567,13 +110,14 @@ void launch_factor_small(cudaStream_t st, const FactorArgs& a, const int32_t* it
 }
 
 void launch_potrf_diag(cudaStream_t st, const FactorArgs& a, const PanelItem* items, int count, double* winv) {
-  if (a.ldl) k_ldl_diag<double><<<count, kThreads, 0, st>>>(a, items, winv);  // LDL^T is FP64 only
-  else if (a.fp32) k_potrf_diag<float><<<count, kThreads, 0, st>>>(a, items, winv);
-  else k_potrf_diag<double><<<count, kThreads, 0, st>>>(a, items, winv);
+  const size_t smem = kDiagSmemDoubles * sizeof(double);
+  if (a.ldl) k_ldl_diag<double><<<count, kThreads, smem, st>>>(a, items, winv);  // LDL^T is FP64 only
+  else if (a.fp32) k_potrf_diag<float><<<count, kThreads, smem, st>>>(a, items, winv);
+  else k_potrf_diag<double><<<count, kThreads, smem, st>>>(a, items, winv);
 }
 
 void launch_trsm_rows(cudaStream_t st, const FactorArgs& a, const PanelItem* items, int count, const double* winv) {
-  const size_t smem = 2 * kNB * kDL * sizeof(double);
+  const size_t smem = kTrsmSmemDoubles * sizeof(double);
   if (a.fp32) k_trsm_rows<float><<<count, kThreads, smem, st>>>(a, items, winv);
   else k_trsm_rows<double><<<count, kThreads, smem, st>>>(a, items, winv);
 }

@@ -50,6 +50,26 @@ void launch_trsm_rows(cudaStream_t st, const FactorArgs& a, const PanelItem* ite
 // tile 64: FMA tiles (FP64 or FP32); tile 128: tensor-core tiles (FP64 DMMA, or 3xTF32 for FP32)
 void launch_gemm(cudaStream_t st, const FactorArgs& a, const TileItem* items, int count, int tile);
 
+// Persistent factorization (FP64, Cholesky or LDL^T): one launch runs every task of
+// Plan::ftasks; ctr (Plan::nfctr) and counter must be zero at launch.  Waits are
+// bounded by spin_limit polls (~128 ns apart); on expiry status 3 is recorded and every
+// CTA leaves.
+struct FactorSched {
+  const FTask* tasks;
+  int ntasks;
+  const FWait* waits;
+  const int32_t* sigs;
+  int32_t* ctr;
+  int32_t* counter;  // next task to hand out
+  const int32_t* small_items;
+  const PanelItem* panel;
+  const TileItem* tiles;
+  double* winv;      // scratch slots of the diagonal blocks
+  long long spin_limit;
+  unsigned long long* trace;  // optional, 4 per task: grabbed, dependencies met, done (ns), SM id
+};
+void launch_factor_persistent(cudaStream_t st, const FactorArgs& a, const FactorSched& f);
+
 // Solves work on the permuted right-hand sides X (n x nrhs, column-major, leading dimension ldx).
 
 // Persistent sweeps (one launch each).  counter, arrived, blkdone and upd must

@@ -1,11 +1,15 @@
 #include "plan.hpp"
 
 #include <algorithm>
+#include <queue>
 #include <stdexcept>
+#include <utility>
 
 namespace spb {
 
 static int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
+
+static void build_factor_dag(Plan& P);
 
 Plan build_plan(const Symbolic& sym, const PlanParams& prm) {
   Plan P;
@@ -144,12 +148,15 @@ Plan build_plan(const Symbolic& sym, const PlanParams& prm) {
     for (int c0 = 0; c0 < maxw; c0 += prm.nb) {
       const int blk = c0 / prm.nb;
       Step pd{StepKind::PotrfDiag, (int32_t)P.panel_items.size(), 0, c0, 0, Lane::Chain, blk};
+      // every diagonal block has its own scratch slot (the persistent factorization keeps
+      // several blocks of one supernode in flight)
+      const int slot0 = P.max_diag_slots;
       int nslots = 0;
       for (int s : sns) {
         if (!P.is_big[s] || c0 >= P.meta[s].w) continue;
-        P.panel_items.push_back(PanelItem{s, c0, std::min(prm.nb, P.meta[s].w - c0), -1, nslots++});
+        P.panel_items.push_back(PanelItem{s, c0, std::min(prm.nb, P.meta[s].w - c0), -1, slot0 + nslots++});
       }
-      P.max_diag_slots = std::max(P.max_diag_slots, nslots);
+      P.max_diag_slots = slot0 + nslots;
       pd.count = (int32_t)P.panel_items.size() - pd.begin;
       if (pd.count) P.steps.push_back(pd);
       Step pt{StepKind::TrsmRows, (int32_t)P.panel_items.size(), 0, c0, 0, Lane::Chain, blk};
@@ -159,7 +166,7 @@ Plan build_plan(const Symbolic& sym, const PlanParams& prm) {
         const SnMeta& m = P.meta[s];
         if (c0 >= m.w) continue;
         int nbk = std::min(prm.nb, m.w - c0);
-        for (int r = c0 + nbk; r < m.h; r += 64) P.panel_items.push_back(PanelItem{s, c0, nbk, r, slot});
+        for (int r = c0 + nbk; r < m.h; r += 64) P.panel_items.push_back(PanelItem{s, c0, nbk, r, slot0 + slot});
         ++slot;
       }
       pt.count = (int32_t)P.panel_items.size() - pt.begin;
@@ -261,6 +268,7 @@ Plan build_plan(const Symbolic& sym, const PlanParams& prm) {
     P.step_flops[k] = f;
   }
   for (const SnMeta& m : P.meta) P.solve_sweep_bytes += 8.0 * m.h * m.w;
+  build_factor_dag(P);
 
   // Solve super-blocks: per supernode, its first super-block counter and (for
   // supernodes wider than one block) the offset of its inverse tiles.
@@ -381,6 +389,208 @@ std::vector<int64_t> build_assembly_map(const Symbolic& sym, const Plan& P, cons
       dst[p - 1] = m.off + (int64_t)(pc - m.fc) * m.ld + (it - rl);
     }
   return dst;
+}
+
+// Persistent factorization: the items of the step sequence as one task graph.
+//   small panel s        waits ext[s] complete                        bumps sdone[s]
+//   POTRF of block b     waits ext[s] complete and col[b] complete    bumps blk[b], sdone[s]
+//   TRSM row tile of b   waits blk[b] >= 1 (its POTRF)                bumps blk[b], sdone[s]
+//   in-panel update      waits blk[b] complete for its K blocks       bumps col[c] of its column blocks
+//   external update      waits sdone[s] complete                      bumps ext[t] of its targets
+// (the reference's FACTOR -> TRSM -> UPDATE dependencies, symPACKMatrix2D.hpp:3893-3997, at
+// block granularity).  The dispatch order comes from a list-scheduling simulation on
+// the SMs with estimated task times, highest bottom level first, and is topological:
+// a CTA only ever waits for tasks handed out before its own.
+static void build_factor_dag(Plan& P) {
+  const int ns = P.nsuper, nb = P.nblk_total;
+  const int EXT = 0, SDONE = ns, BLK = 2 * ns, COL = 2 * ns + nb;
+  P.nfctr = 2 * ns + 2 * nb;
+  std::vector<int32_t> e_ext(ns, 0), e_sdone(ns, 0), e_blk(nb, 0), e_col(nb, 0);
+  struct Raw {
+    int kind, item, s;
+    std::vector<int32_t> sig;
+    double us;
+  };
+  std::vector<Raw> raw;
+  // tasks of each step in step order (already topological), signals first
+  for (const Step& st : P.steps) {
+    for (int i = st.begin; i < st.begin + st.count; ++i) {
+      Raw r;
+      r.item = i;
+      if (st.kind == StepKind::FactorSmall) {
+        const int s = P.small_items[i];
+        const SnMeta& m = P.meta[s];
+        r.kind = 0;
+        r.s = s;
+        r.sig = {SDONE + s};
+        const double w = m.w, mm = m.h - m.w;
+        r.us = 3.0 + 2.0 * (w * w * w / 3.0 + mm * w * w) / 20e3;
+        e_sdone[s] += 1;
+      } else if (st.kind == StepKind::PotrfDiag || st.kind == StepKind::TrsmRows) {
+        const PanelItem& it = P.panel_items[i];
+        const int b = P.meta[it.s].boff + it.c0 / 64;
+        r.kind = st.kind == StepKind::PotrfDiag ? 1 : 2;
+        r.s = it.s;
+        r.sig = {BLK + b, SDONE + it.s};
+        r.us = r.kind == 1 ? 22.0 : 10.0;
+        e_blk[b] += 1;
+        e_sdone[it.s] += 1;
+      } else {
+        const TileItem& t = P.tile_items[i];
+        const SnMeta& m = P.meta[t.s];
+        r.kind = st.tile == 128 ? 4 : 3;
+        r.s = t.s;
+        const double fl = 2.0 * t.mrows * t.ncols * t.kn;
+        r.us = st.tile == 128 ? 3.0 + fl / 130e3 : 2.0 + fl / 30e3;
+        if (t.mode == 0) {
+          for (int c = t.b_row0 / 64; c <= (t.b_row0 + t.ncols - 1) / 64; ++c) {
+            r.sig.push_back(COL + m.boff + c);
+            e_col[m.boff + c] += 1;
+          }
+        } else {
+          int last = -1;
+          for (int c = 0; c < t.ncols; ++c) {
+            const int g = P.row_group[m.lidx + t.b_row0 + c];
+            const int tgt = P.groups[g].t;
+            if (tgt != last) {
+              r.sig.push_back(EXT + tgt);
+              e_ext[tgt] += 1;
+            }
+            last = tgt;
+          }
+        }
+      }
+      raw.push_back(std::move(r));
+    }
+  }
+  // waits of every task
+  std::vector<std::vector<FWait>> waits(raw.size());
+  for (size_t k = 0; k < raw.size(); ++k) {
+    const Raw& r = raw[k];
+    if (r.kind == 0) {
+      waits[k] = {{EXT + r.s, e_ext[r.s]}};
+    } else if (r.kind == 1 || r.kind == 2) {
+      const PanelItem& it = P.panel_items[r.item];
+      const int b = P.meta[it.s].boff + it.c0 / 64;
+      if (r.kind == 1) waits[k] = {{EXT + r.s, e_ext[r.s]}, {COL + b, e_col[b]}};
+      else waits[k] = {{BLK + b, 1}};
+    } else {
+      const TileItem& t = P.tile_items[r.item];
+      const SnMeta& m = P.meta[t.s];
+      if (t.mode == 0) {
+        for (int c = t.k0 / 64; c <= (t.k0 + t.kn - 1) / 64; ++c) waits[k].push_back({BLK + m.boff + c, e_blk[m.boff + c]});
+      } else {
+        waits[k] = {{SDONE + t.s, e_sdone[t.s]}};
+      }
+    }
+  }
+  // dependency graph for the simulation: every counter is a zero-time join node whose
+  // predecessors are its signalling tasks; a task depends on the joins it waits for
+  // (a TRSM tile waits for its block's POTRF only)
+  const int nt = (int)raw.size(), nc = P.nfctr, nn = nt + nc;
+  std::vector<std::vector<int32_t>> succ(nn);
+  std::vector<int32_t> npred(nn, 0);
+  std::vector<int32_t> potrf_of(nb, -1);
+  for (int k = 0; k < nt; ++k)
+    if (raw[k].kind == 1) potrf_of[P.meta[P.panel_items[raw[k].item].s].boff + P.panel_items[raw[k].item].c0 / 64] = k;
+  for (int k = 0; k < nt; ++k) {
+    for (int32_t c : raw[k].sig) {
+      succ[k].push_back(nt + c);
+      npred[nt + c]++;
+    }
+    for (const FWait& w : waits[k]) {
+      if (w.target <= 0) continue;
+      int from = nt + w.ctr;
+      if (raw[k].kind == 2) from = potrf_of[w.ctr - BLK];
+      succ[from].push_back(k);
+      npred[k]++;
+    }
+  }
+  // bottom levels (longest path to the end), in reverse topological order: counters
+  // and tasks are processed after all their successors via a Kahn order
+  std::vector<double> dur(nn, 0.0), blev(nn, 0.0);
+  for (int k = 0; k < nt; ++k) dur[k] = raw[k].us;
+  std::vector<int32_t> order;
+  order.reserve(nn);
+  {
+    std::vector<int32_t> indeg = npred;
+    for (int v = 0; v < nn; ++v)
+      if (!indeg[v]) order.push_back(v);
+    for (size_t q = 0; q < order.size(); ++q)
+      for (int32_t u : succ[order[q]])
+        if (--indeg[u] == 0) order.push_back(u);
+    if ((int)order.size() != nn) throw std::runtime_error("plan: factorization task graph has a cycle");
+  }
+  for (int q = nn - 1; q >= 0; --q) {
+    const int v = order[q];
+    double best = 0.0;
+    for (int32_t u : succ[v]) best = std::max(best, blev[u]);
+    blev[v] = dur[v] + best;
+  }
+  // list scheduling on the SMs (one CTA per SM)
+  const int workers = 148;
+  std::vector<int32_t> pend = npred;
+  auto cmp = [&](int32_t x, int32_t y) { return blev[x] < blev[y] || (blev[x] == blev[y] && x > y); };
+  std::priority_queue<int32_t, std::vector<int32_t>, decltype(cmp)> ready(cmp);
+  using Ev = std::pair<double, int32_t>;
+  std::priority_queue<Ev, std::vector<Ev>, std::greater<Ev>> running;
+  std::vector<int32_t> dispatch;
+  dispatch.reserve(nt);
+  std::vector<int32_t> stack;
+  auto complete = [&](int32_t v) {  // v finished: release successors, joins complete at once
+    stack.push_back(v);
+    while (!stack.empty()) {
+      const int32_t x = stack.back();
+      stack.pop_back();
+      for (int32_t u : succ[x])
+        if (--pend[u] == 0) {
+          if (u >= nt) stack.push_back(u);
+          else ready.push(u);
+        }
+    }
+  };
+  for (int v = nt; v < nn; ++v)
+    if (!pend[v]) complete(v);
+  for (int v = 0; v < nt; ++v)
+    if (!pend[v]) ready.push(v);
+  double now = 0.0;
+  int busy = 0;
+  while ((int)dispatch.size() < nt) {
+    while (busy < workers && !ready.empty()) {
+      const int32_t v = ready.top();
+      ready.pop();
+      dispatch.push_back(v);
+      running.push({now + dur[v], v});
+      ++busy;
+    }
+    if (running.empty()) throw std::runtime_error("plan: factorization schedule stalled");
+    const Ev e = running.top();
+    running.pop();
+    now = e.first;
+    --busy;
+    complete(e.second);
+  }
+  while (!running.empty()) {
+    now = running.top().first;
+    running.pop();
+  }
+  P.fsim_us = now;
+  P.ftasks.clear();
+  P.fwaits.clear();
+  P.fsigs.clear();
+  for (int32_t k : dispatch) {
+    FTask t;
+    t.kind = raw[k].kind;
+    t.item = raw[k].item;
+    t.wait0 = (int32_t)P.fwaits.size();
+    for (const FWait& w : waits[k])
+      if (w.target > 0) P.fwaits.push_back(w);
+    t.nwait = (int32_t)P.fwaits.size() - t.wait0;
+    t.sig0 = (int32_t)P.fsigs.size();
+    P.fsigs.insert(P.fsigs.end(), raw[k].sig.begin(), raw[k].sig.end());
+    t.nsig = (int32_t)raw[k].sig.size();
+    P.ftasks.push_back(t);
+  }
 }
 
 }  // namespace spb

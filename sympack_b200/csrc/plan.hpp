@@ -85,6 +85,25 @@ struct PanelItem {
   int32_t slot;   // scratch slot holding this step's L11^-1 for the supernode
 };
 
+// One task of the persistent factorization: a small panel, a diagonal block, a TRSM
+// row tile or an update tile (the items of the step sequence), with the dependency
+// counters it waits for and the ones it bumps when done.  Counters: per supernode the
+// external update tiles landed (ext) and its finished panel tasks (sdone), per 64-column
+// block its finished POTRF / TRSM tasks (blk) and the in-panel update tiles landed in
+// its columns (col).
+struct FTask {
+  int32_t kind;   // 0 small panel, 1 diagonal block, 2 TRSM row tile, 3 64 x 64 tile, 4 128 x 128 tile
+  int32_t item;   // index into small_items / panel_items / tile_items
+  int32_t wait0;  // fwaits[wait0 .. wait0 + nwait)
+  int32_t nwait;
+  int32_t sig0;   // fsigs[sig0 .. sig0 + nsig)
+  int32_t nsig;
+};
+struct FWait {
+  int32_t ctr;
+  int32_t target;
+};
+
 // One task of the persistent triangular solves.  A supernode of one 64-column block
 // is solved by substitution; a wider one is cut into super-blocks of sb 64-column
 // blocks (the last one shorter), and the diagonal triangle of every super-block p is
@@ -190,7 +209,13 @@ struct Plan {
   std::vector<PanelItem> panel_items;
   std::vector<TileItem> tile_items;
   std::vector<Step> steps;
-  int32_t max_diag_slots = 0;      // most diagonal blocks factored in one step (scratch slots)
+  int32_t max_diag_slots = 0;      // scratch slots of the diagonal blocks (one per diagonal block)
+  // persistent factorization: tasks in dispatch order (topological), their waits and signals
+  std::vector<FTask> ftasks;
+  std::vector<FWait> fwaits;
+  std::vector<int32_t> fsigs;
+  int32_t nfctr = 0;               // counters: ext[ns], sdone[ns], blk[nblk_total], col[nblk_total]
+  double fsim_us = 0.0;            // makespan of the list-scheduling simulation that ordered them
   std::vector<double> step_flops;  // useful (algorithmic) flops of each step
   // executed flop count of the sequence (w^3/3 + m w^2 + m^2 w per supernode)
   double exec_flops = 0.0;

@@ -96,6 +96,7 @@ class symPACKOptions:
     plan_dense_min_w: int = 0      # accepted for compatibility, no effect (the super-block solve replaced it)
     plan_solve_chunk: int = 0      # 64-column blocks per solve super-block (0 = library default 8)
     plan_solve_tiles: int = 0      # 64 x 64 tiles per super-block solve task (0 = library default 2)
+    factor_schedule: str = "persistent"  # FP64 factorization: "persistent" (one launch) or "steps"
 
     def to_c(self) -> N.spb_options:
         if self.orderingStr not in N.ORDERINGS:
@@ -121,6 +122,10 @@ class symPACKOptions:
         o.plan_dense_min_w = self.plan_dense_min_w
         o.plan_solve_chunk = self.plan_solve_chunk
         o.plan_solve_tiles = self.plan_solve_tiles
+        schedules = {"persistent": 0, "steps": 1}
+        if self.factor_schedule not in schedules:
+            raise ValueError(f"unknown factor_schedule {self.factor_schedule!r} (persistent or steps)")
+        o.factor_schedule = schedules[self.factor_schedule]
         engines = {"tcgen05": 0, "mma.sync": 1, "tcgen05-persistent": 2}
         if self.fp32_engine not in engines:
             raise ValueError(f"unknown fp32_engine {self.fp32_engine!r}")
@@ -312,6 +317,26 @@ class symPACKMatrix2D:
     def DebugStall(self, supernode: int) -> None:
         """Failure-detection test hook: the forward solve waits for an update nobody sends."""
         _raise(self._lib.spb_debug_stall(self._need(), int(supernode)), "DebugStall", self._h)
+
+    def SetFactorTrace(self, on: bool = True) -> None:
+        """Record the per-task timeline of later persistent factorizations."""
+        _raise(self._lib.spb_set_factor_trace(self._need(), 1 if on else 0), "SetFactorTrace", self._h)
+
+    def GetFactorTrace(self):
+        """(ntasks, 4) uint64 rows {handed out, dependencies met, done (ns), SM} in dispatch
+        order, and the task kinds (0 small, 1 diagonal block, 2 TRSM, 3 64x64 tile, 4 128x128 tile)."""
+        h = self._need()
+        nt = C.c_int64()
+        _raise(self._lib.spb_get_factor_trace(h, None, 0, C.byref(nt), None), "GetFactorTrace", h)
+        out = np.zeros((nt.value, 4), np.uint64)
+        kinds = np.zeros(nt.value, np.int32)
+        _raise(self._lib.spb_get_factor_trace(h, out.ctypes.data_as(C.POINTER(C.c_uint64)), nt.value, C.byref(nt),
+                                              kinds.ctypes.data_as(C.POINTER(C.c_int32))), "GetFactorTrace", h)
+        return out, kinds
+
+    def DebugStallFactor(self, supernode: int) -> None:
+        """Failure-detection test hook: the persistent factorization waits for an update nobody sends."""
+        _raise(self._lib.spb_debug_stall_factor(self._need(), int(supernode)), "DebugStallFactor", self._h)
 
     def SetProfiling(self, on: bool = True) -> None:
         _raise(self._lib.spb_set_profiling(self._need(), 1 if on else 0), "SetProfiling", self._h)

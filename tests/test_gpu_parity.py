@@ -267,6 +267,74 @@ def test_solve_wait_timeout_is_reported_and_recovers():
     assert "RECOVERED" in r.stdout
 
 
+FACTOR_TIMEOUT_CHILD = r"""
+import sys
+sys.path.insert(0, sys.argv[1])
+import numpy as np
+from sympack_b200 import DeviceTimeoutError, DistSparseMatrix, generators as G, symPACKMatrix2D, symPACKOptions
+n, cp, ri, v = G.laplacian_3d(12, 12, 12, 1e-3)
+A = DistSparseMatrix.from_lower_csc(n, cp, ri, v)
+M = symPACKMatrix2D()
+M.Init(symPACKOptions(device=0))
+M.SymbolicFactorization(A)
+M.DistributeMatrix(A)
+M.Factorize()
+b = np.random.default_rng(0).standard_normal((n, 1))
+M.Solve(b)
+x_ok = M.GetSolution(nrhs=1)
+M.SetWaitLimit(2000)
+M.DebugStallFactor(M.info().nsuper - 1)  # the root waits for one external update too many
+M.DistributeMatrix(A)
+try:
+    M.Factorize()
+    print("NO_TIMEOUT")
+    sys.exit(1)
+except DeviceTimeoutError:
+    pass
+M.DebugStallFactor(-1)
+M.SetWaitLimit(1 << 24)
+M.DistributeMatrix(A)
+M.Factorize()
+M.Solve(b)
+err = np.max(np.abs(M.GetSolution(nrhs=1) - x_ok)) / np.max(np.abs(x_ok))
+print("RECOVERED", err)
+sys.exit(0 if err <= 1e-14 else 2)
+"""
+
+
+def test_factor_wait_timeout_is_reported_and_recovers():
+    """The persistent factorization's bounded waits: a supernode waits for an external
+    update nobody sends, the call reports a timeout, and the same handle factors again
+    afterwards.  Runs in a child process with its own time limit."""
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    r = subprocess.run([sys.executable, "-c", FACTOR_TIMEOUT_CHILD, root], capture_output=True, text=True, timeout=180)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "RECOVERED" in r.stdout
+
+
+@pytest.mark.parametrize("schedule", ["persistent", "steps"])
+def test_factor_schedules_match_oracle(schedule):
+    """The persistent factorization and the level-ordered launch sequence give the
+    oracle's factor within the parity bound (FP64 Cholesky and LDL^T)."""
+    for name, gen, dec in (("st27_16", lambda: G.stencil27(16, 16, 16, 1e-2, seed=8), "LL"),
+                           ("rand_3000", lambda: G.random_graph_spd(3000, 10, 1.05, seed=9), "LL"),
+                           ("qd_14", lambda: G.quasi_definite_3d(14, 14, 14, 0.3, 1e-2, seed=3), "LDL")):
+        n, cp, ri, v = gen()
+        A = DistSparseMatrix.from_lower_csc(n, cp, ri, v)
+        M = setup(A, factor_schedule=schedule, decomposition=dec)
+        perm, invp = M.GetOrdering()
+        xl, li = M.GetStructure()
+        sym = dict(xsuper=M.GetSupernodalPartition(), xlindx=xl, lindx=li, supmember=M.GetSupMembership(), invp=invp)
+        f = numeric.OracleFactor(A.size, sym, threads=os.cpu_count(), ldl=dec == "LDL")
+        f.distribute(A.colptr, A.rowind, A.nzvalLocal)
+        f.factorize()
+        assert relerr(M.GetFactor(), f.factor()) <= TOL, name
+        assert M.info().factor_launches == (1 if schedule == "persistent" else M.info().factor_launches)
+        M.close()
+
+
 def test_solve_trace_of_a_profiled_solve():
     n, cp, ri, v = G.laplacian_3d(14, 14, 14, 1e-3)
     A = DistSparseMatrix.from_lower_csc(n, cp, ri, v)
