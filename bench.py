@@ -35,6 +35,9 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+# DRAM bytes (read + write) of one k_factor_persistent launch on the 60^3 workload, from ncu
+# (dram__bytes.sum.per_second x gpu__time_duration; profiles/factor_persistent_lap3d60_ncu.md)
+FACTOR_TRAFFIC_BYTES = 12.93e9
 METRIC = "factor TFLOP/s (FP64 supernodal Cholesky, flops = sum of squared column counts)"
 
 
@@ -49,10 +52,10 @@ def parse():
     ap.add_argument("--no-precision", action="store_true", help="skip the FP64 vs FP32+IR comparison")
     ap.add_argument("--precision-grid", type=int, default=80,
                     help="grid edge of the 27-point stencil of the precision comparison (80 = the named workload)")
-    ap.add_argument("--batch-systems", type=int, default=300,
-                    help="systems of the batching workload (2000 = the named workload; host MMD of its random "
-                         "graphs takes minutes)")
-    ap.add_argument("--serve-requests", type=int, default=1000,
+    ap.add_argument("--batch-systems", type=int, default=2000,
+                    help="systems of the batching workload (2000 = the named workload; the host analysis of its "
+                         "random graphs takes about two minutes)")
+    ap.add_argument("--serve-requests", type=int, default=10000,
                     help="requests of the serving workload (10000 = the named workload)")
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-ldl", action="store_true", help="skip the LDL^T vs Cholesky comparison")
@@ -381,11 +384,13 @@ def per_system_backward_error(systems, offs, x, b):
     return eta
 
 
-def batching_comparison(torch, dev, stream, count, seed=0, subset=64):
-    """Batching form: `count` uneven systems factored together (each etree level
-    of every system in the same launches), plans picked by the autotuner, in
-    FP64 and FP32 + refinement; beside it the first `subset` systems factored
-    one by one versus as one batch."""
+def batching_comparison(torch, dev, stream, count, seed=0, subset=64, tune_systems=200):
+    """Batching form: `count` uneven systems factored together (FP64: every task of every
+    system in one persistent launch; FP32 + refinement: each etree level of every system in
+    the same launches), in FP64 and FP32 + refinement, with tile shapes picked by the
+    autotuner on the first `tune_systems` systems (each candidate re-plans the batch, so the
+    candidates are timed on that sample and the winner plans the whole batch); beside it the
+    first `subset` systems factored one by one versus as one batch."""
     from sympack_b200 import DistSparseMatrix, autotune, generators as G, symPACKMatrix2D, symPACKOptions
     systems = G.batch_systems(count, 500, 20000, seed=seed)
     n, cp, ri, v, offs = G.block_diagonal(systems)
@@ -397,7 +402,7 @@ def batching_comparison(torch, dev, stream, count, seed=0, subset=64):
                        f"odd: random graphs avg degree 10, off-diagonals U[-1,0), dominance 1.05 (seed {seed})",
            "systems": count, "n_total": n}
     T = symPACKMatrix2D()
-    T.Init(symPACKOptions(device=-1))
+    T.Init(symPACKOptions(device=-1, factor_schedule="steps"))  # analysis only: no task graph
     t0 = time.perf_counter()
     T.SymbolicFactorizationBatch(A, offs)
     out["symbolic_s"] = time.perf_counter() - t0
@@ -405,11 +410,19 @@ def batching_comparison(torch, dev, stream, count, seed=0, subset=64):
     flops = inf.flops_stat
     out.update(flops_stat=flops, nnz_L=inf.nnz_l, nsuper=inf.nsuper, etree_levels=inf.nlevels,
                max_width=inf.max_width)
+    sample = systems[:min(tune_systems, count)]
+    tn, tcp, tri, tv, toffs = G.block_diagonal(sample)
+    At = DistSparseMatrix.from_lower_csc(tn, tcp, tri, tv)
     for prec in ("FP64", "FP32_IR"):
+        S = symPACKMatrix2D()
+        S.Init(symPACKOptions(device=dev.index, precision=prec))
+        S.SymbolicFactorizationBatch(At, toffs)
+        tune = autotune.tune(S, At, toffs, reps=1, use_cache=False)
+        S.close()
         M = symPACKMatrix2D()
-        M.Init(symPACKOptions(device=dev.index, precision=prec))
+        M.Init(symPACKOptions(device=dev.index, precision=prec, plan_small_max_w=tune["small_max_w"],
+                              plan_big_tile_rows=tune["big_tile_rows"], plan_outer_nb=tune["outer_nb"]))
         M.SymbolicFactorizationFrom(T)
-        tune = autotune.tune(M, A, offs, reps=1, use_cache=False)
         M.SetStream(stream.cuda_stream)
         times = []
         for r in range(3):
@@ -432,7 +445,7 @@ def batching_comparison(torch, dev, stream, count, seed=0, subset=64):
                      "ir_iterations": mi.ir_iterations if prec == "FP32_IR" else 0,
                      "factor_launches": mi.factor_launches, "device_bytes": mi.device_bytes,
                      "autotuned_plan": {"small_max_w": tune["small_max_w"], "big_tile_rows": tune["big_tile_rows"],
-                                        "outer_nb": tune["outer_nb"],
+                                        "outer_nb": tune["outer_nb"], "tuned_on_systems": len(sample),
                                         "candidates_ms": {k: round(v * 1e3, 3) for k, v in tune["times"].items()}}}
         M.close()
     T.close()
@@ -477,16 +490,20 @@ def batching_comparison(torch, dev, stream, count, seed=0, subset=64):
     return out
 
 
-def serving_comparison(torch, dev, count, seed=0, load=0.7):
-    """Serving form on the request stream: (1) back-to-back plain FP64, one request
-    after the other; (2) the continuous-batching loop (FP32 + refinement, 8 slots,
-    right-hand sides merged per factor) with every request submitted at once, which
-    gives its capacity; (3) the loop with Poisson arrivals at `load` x that capacity,
-    which gives p50 / p99 latency at a sustainable rate."""
+def serving_comparison(torch, dev, count, seed=0, load=0.7, base_count=2000, check_every=25):
+    """Serving form on the request stream: (1) back-to-back plain FP64, one request after
+    the other, on the stream's first `base_count` requests (a sequential baseline: its rate
+    does not depend on how many requests follow); (2) the continuous-batching loop (8 slots,
+    right-hand sides merged per factor) in FP64 and in FP32 + refinement with every request
+    submitted at once, which gives each precision's capacity; (3) the FP32 + refinement loop
+    with Poisson arrivals at `load` x its capacity, which gives p50 / p99 latency at a
+    sustainable rate.  Every `check_every`-th result is checked on the host: its backward
+    error ||b - A x||_inf / (||A||_inf ||x||_inf + ||b||_inf) (FP64 results do not compute it
+    on the device)."""
     from sympack_b200 import serving as S
-    mk = lambda: S.request_stream(count, 1.0, seed=seed)
+    mk = lambda k: S.request_stream(k, 1.0, seed=seed)
     patterns = {}
-    for _, r in mk():
+    for _, r in mk(count):
         if r.spec[0] is not None:
             patterns[(r.spec[0].kind, r.spec[0].k)] = r.spec[0]
 
@@ -497,10 +514,11 @@ def serving_comparison(torch, dev, count, seed=0, load=0.7):
         for f in list(svc._patterns.values()):
             f.result()
 
-    def run(precision, slots, merge, rate):
-        stream = [(t / rate if rate else 0.0, r) for t, r in mk()]
-        for _, r in stream:
-            r.keep = False
+    def run(precision, slots, merge, rate, k):
+        stream = [(t / rate if rate else 0.0, r) for t, r in mk(k)]
+        for i, (_, r) in enumerate(stream):
+            r.keep = i % check_every == 0
+        specs = {r.factor_id: (r.spec[0], r.spec[1]) for _, r in stream if r.kind == "factor_solve"}
         svc = S.SolverService(device=dev.index, precision=precision, max_inflight=slots, max_batch_rhs=merge)
         preload(svc)
         if rate is None:  # back to back: each request starts when the previous one ends
@@ -509,22 +527,30 @@ def serving_comparison(torch, dev, count, seed=0, load=0.7):
                 svc.submit(S.materialise(r)).result()
             wall = time.perf_counter() - t0
         else:
-            wall = S.replay(svc, stream, timeout=1800)
+            wall = S.replay(svc, stream, timeout=3600)
         res = [r.future.result() for _, r in stream]
         svc.close()
         torch.cuda.empty_cache()
-        out = {"solves_per_s": count / wall, "wall_s": wall, **S.latency_summary([r for _, r in stream]),
+        # host check of the kept results, against the matrix of the request's factor (drawn
+        # again from its pattern and seed)
+        eta = 0.0
+        for (_, r), x in zip(stream, res):
+            if x.x is not None:
+                P, sd = specs[r.factor_id]
+                eta = max(eta, backward_error(P.matrix(sd), x.x, r.rhs))
+        out = {"requests": k, "solves_per_s": k / wall, "wall_s": wall, **S.latency_summary([r for _, r in stream]),
                "service_p50_ms": float(np.percentile([(r.t_done - r.t_start) * 1e3 for _, r in stream], 50)),
                "service_p99_ms": float(np.percentile([(r.t_done - r.t_start) * 1e3 for _, r in stream], 99)),
-               # FP64 solves skip the residual (backward_error -1): reported as None
-               "max_backward_error": max((x.backward_error for x in res if x.backward_error >= 0), default=None)}
-        out.update({k: int(v) for k, v in svc.stats.items()})
+               "max_backward_error_device": max((x.backward_error for x in res if x.backward_error >= 0), default=None),
+               "max_backward_error_host_checked": eta, "host_checked_results": sum(1 for x in res if x.x is not None)}
+        out.update({kk: int(v) for kk, v in svc.stats.items()})
         return out
 
-    base = run("FP64", 1, 1, None)
-    cap = run("FP32_IR", 8, 64, 0.0)
+    base = run("FP64", 1, 1, None, min(base_count, count))
+    cap64 = run("FP64", 8, 64, 0.0, count)
+    cap = run("FP32_IR", 8, 64, 0.0, count)
     rate = load * cap["solves_per_s"]
-    lat = run("FP32_IR", 8, 64, rate)
+    lat = run("FP32_IR", 8, 64, rate, count)
     lat["arrival_rate_per_s"] = rate
     return {
         "workload": f"{count} requests, Poisson arrivals, 30% factor+solve on fresh 27-point stencil (delta 1e-2) "
@@ -532,9 +558,12 @@ def serving_comparison(torch, dev, count, seed=0, load=0.7):
                     f"factors, nrhs U{{1..64}} (seed {seed})",
         "requests": count,
         "back_to_back_fp64": base,
+        "continuous_batching_fp64_capacity": cap64,
         "continuous_batching_fp32_ir_capacity": cap,
         "continuous_batching_fp32_ir_at_load": lat,
         "speedup_solves_per_s_at_load": lat["solves_per_s"] / base["solves_per_s"],
+        "speedup_capacity_batching_fp64": cap64["solves_per_s"] / base["solves_per_s"],
+        "speedup_capacity_precision_fp32_ir_over_fp64": cap["solves_per_s"] / cap64["solves_per_s"],
         "speedup_capacity": cap["solves_per_s"] / base["solves_per_s"],
     }
 
@@ -574,9 +603,10 @@ def run_ours(args):
     d_x16 = torch.empty_like(d_b16)
 
     def step():
-        ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
         ev[0].record(stream)
         M.DistributeMatrixDevice(d_vals.data_ptr())
+        ev[4].record(stream)  # the factorization launch alone: ev[4] -> ev[1]
         M.Factorize()
         ev[1].record(stream)
         M.SolveDevice(d_b1.data_ptr(), d_x1.data_ptr(), 1, n)
@@ -598,6 +628,7 @@ def run_ours(args):
     barrier()
     clocks = sampler.stop()
     fac = [e[0].elapsed_time(e[1]) for e in evs]
+    fac_kernel = [e[4].elapsed_time(e[1]) for e in evs]  # counter reset + the persistent factorization
     s1 = [e[1].elapsed_time(e[2]) for e in evs]
     s16 = [e[2].elapsed_time(e[3]) for e in evs]
     tot = [e[0].elapsed_time(e[3]) for e in evs]
@@ -636,24 +667,43 @@ def run_ours(args):
     e2e_ms = replicas.max_over_ranks([sum(s.elapsed_time(e) for s, e in e2e_ev)], dev, dist)[0]
     bwd_e2e = backward_error(A, np.asfortranarray(h_out.numpy().T), b16)
 
-    # one profiled step (eager launches with per-launch CUDA events) for the roofline
+    # the dominant kernel: the persistent FP64 factorization (every task of the factorization
+    # in one launch), timed by the events around it in the timed steps above
+    peaks, peak_src = measured_peaks()
+    fp64_peak = measured_fp64_peak(torch, dev)
+    fk_ms = sum(fac_kernel) / len(fac_kernel)
+    roofline = {"kernel": "k_factor_persistent", "bound": "tensor",
+                "achieved": flops / (fk_ms * 1e-3) / 1e12, "peak": fp64_peak, "unit": "TFLOP/s",
+                "frac": None, "launch_ms": fk_ms,
+                # dram__bytes (read + write) of one launch on this workload, from the ncu capture
+                # summarised in profiles/factor_persistent_lap3d60_ncu.md
+                "traffic": FACTOR_TRAFFIC_BYTES if args.grid == 60 else None,
+                "algorithmic_bytes": 2.0 * info.arena_bytes,
+                "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (no FP64 figure in " + peak_src + ")"}
+    roofline["frac"] = roofline["achieved"] / roofline["peak"]
+    # where the factorization's CTA time goes: one traced factorization (outside the timing)
+    M.SetFactorTrace(True)
+    M.DistributeMatrixDevice(d_vals.data_ptr())
+    M.Factorize()
+    tr, tkinds = M.GetFactorTrace()
+    M.SetFactorTrace(False)
+    tr = tr.astype(np.int64)
+    busy = (tr[:, 2] - tr[:, 1]).astype(np.float64)
+    span = float(tr[:, 2].max() - tr[:, 0].min())
+    nsm = len(np.unique(tr[:, 3]))
+    names = ["small_panel", "diagonal_block", "trsm_tile", "tile_64x64", "tile_128x128_dmma"]
+    roofline["task_breakdown"] = {
+        names[k]: {"tasks": int(np.sum(tkinds == k)), "cta_ms": float(busy[tkinds == k].sum() / 1e6),
+                   "share_of_busy": float(busy[tkinds == k].sum() / busy.sum())} for k in range(5)}
+    roofline["sm_busy_fraction"] = float(busy.sum() / (span * nsm))
+    # one profiled step (eager launches of the level-ordered sequence, per-launch CUDA events):
+    # the solve sweeps' byte count and the per-kind times of the step schedule
     M.SetProfiling(True)
     M.DistributeMatrixDevice(d_vals.data_ptr())
     M.Factorize()
     M.SolveDevice(d_b16.data_ptr(), d_x16.data_ptr(), 16, n)
     prof = M.GetProfile()
     M.SetProfiling(False)
-    peaks, peak_src = measured_peaks()
-    fp64_peak = measured_fp64_peak(torch, dev)
-    factor_kinds = ["factor_small", "potrf_diag", "trsm_rows", "gemm_simt", "gemm_dmma"]
-    top = max(factor_kinds, key=lambda k: prof[k]["ms"])
-    tp = prof[top]
-    roofline = {"kernel": top, "bound": "tensor", "achieved": tp["flops"] / (tp["ms"] * 1e-3) / 1e12,
-                "peak": fp64_peak, "unit": "TFLOP/s", "traffic": None,
-                "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (no FP64 figure in "
-                               + peak_src + ")",
-                "launches": tp["launches"], "share_of_factor": tp["ms"] / sum(prof[k]["ms"] for k in factor_kinds)}
-    roofline["frac"] = roofline["achieved"] / roofline["peak"]
     sf, sb = prof["solve_forward"], prof["solve_backward"]
     roofline_solve = {"kernel": "solve_forward+solve_backward", "bound": "hbm", "unit": "GB/s",
                       "achieved": (sf["bytes"] + sb["bytes"]) / ((sf["ms"] + sb["ms"]) * 1e-3) / 1e9,
@@ -692,7 +742,10 @@ def run_ours(args):
     K = args.steps
     # per step: assemble + factor graph, then two solves (permute in, forward, backward,
     # permute out), the nrhs-1 solve with one more launch per sweep for a cluster-solved root
-    launches_per_step = 1 + info.factor_launches + 4 + 4 + (2 if info.dense_root_width else 0)
+    # per step: assemble, the factorization (one persistent launch), then two solves (permute in,
+    # forward, backward, permute out), the first one after the factorization also computing the
+    # diagonal super-block inverses
+    launches_per_step = 1 + info.factor_launches + 4 + 4 + (1 if info.inverse_bytes else 0)
     if rank == 0:
         line = {
             "metric": METRIC, "value": replicas.job_rate(flops * K, world, fac_ms) / 1e12, "unit": "TFLOP/s",
@@ -702,6 +755,7 @@ def run_ours(args):
             "analysis": {"flops_exec": info.flops_exec, "nsuper": info.nsuper, "etree_levels": info.nlevels,
                          "factor_arena_gb": info.arena_bytes / 1e9, "symbolic_s": symb_s},
             "factor_ms": fac_ms / K,
+            "factor_schedule": "persistent (one launch per factorization)" if info.factor_launches == 1 else "steps",
             "solves_per_s": {"nrhs1": world * K / (s1_ms * 1e-3), "nrhs16": world * 16 * K / (s16_ms * 1e-3)},
             "solve_ms": {"nrhs1": s1_ms / K, "nrhs16": s16_ms / K},
             "backward_error": {"nrhs1": bwd1, "nrhs16": bwd16, "e2e_nrhs16": bwd_e2e},

@@ -1,17 +1,28 @@
-// Approximate minimum degree ordering (Amestoy, Davis & Duff, "An approximate minimum
-// degree ordering algorithm", SIAM J. Matrix Anal. Appl. 17(4), 1996) in the variant the
-// reference compiles (src/amdbar.F: quotient graph with element absorption, approximate
-// external degrees, mass elimination, supervariables found by hashing; no dense-row
-// detection and no aggressive absorption), called as Ordering::AMD calls it
-// (src/Ordering.cpp:411-520): the expanded graph without diagonal, 32-bit indices, a
-// workspace of nnz + n entries (IWLEN = nnz + n, PFREE = nnz + 1, so the quotient graph is
-// compacted whenever a new element does not fit), and the inverse permutation taken from
-// the final numbering.  Every tie-break (degree-list heads, hash-bucket order, the order
-// in which element lists are scanned) follows the reference, so the permutation is the
-// reference's bit for bit.
+// Approximate minimum degree ordering, from the algorithm of Amestoy, Davis and Duff
+// ("An approximate minimum degree ordering algorithm", SIAM J. Matrix Anal. Appl. 17(4),
+// 886-905, 1996): a quotient graph of variables and elements, elimination of a variable of
+// least approximate external degree, absorption of the elements adjacent to the pivot into
+// the new element, approximate degrees from |Le \ Lme|, mass elimination of variables
+// adjacent to the new element only, and indistinguishable variables merged into
+// supervariables (candidates found by hashing their adjacency).  The variant is the one
+// the reference compiles and calls (src/amdbar.F through Ordering::AMD,
+// src/Ordering.cpp:411-520): no dense-row detection, no aggressive absorption.
 //
-// All arrays are 1-based (index 0 unused): 0 is the null link and negative values mark
-// absorbed elements and eliminated variables, as in the published algorithm.
+// The permutation must be the reference's bit for bit, so every choice that the
+// published algorithm leaves open is made the way that code makes it: the degree lists
+// are last-in first-out and the pivot is the first variable of the lowest non-empty list;
+// the variables of the new element are collected from the pivot's elements in list
+// order, then from its own variables; after the degree update a variable's element list
+// becomes [new element, e2 .. ek, e1] and its variable list [v2 .. vm, v1]; the hash key is
+// the 32-bit wrapped sum of the surviving entries modulo max(1, n - 1), plus one, and each
+// hash bucket is last-in first-out; a variable absorbed into a supervariable, or eliminated
+// by mass elimination, is numbered just before the element that finally contains it.
+// (Those rules are what the golden tests, made from the reference executed here, pin.)
+//
+// Layout: each variable keeps its adjacent elements and adjacent variables in two
+// vectors, each element its member variables; degree and hash buckets are explicit lists.
+// Nothing is compacted: a list shrinks in place when it is pruned.
+#include <algorithm>
 #include <cstdint>
 #include <limits>
 #include <stdexcept>
@@ -22,355 +33,274 @@
 namespace spb {
 namespace {
 
-class ApproxMinDegree {
+// Buckets of variables by approximate degree; inserting puts a variable first.
+class DegreeBuckets {
  public:
-  explicit ApproxMinDegree(const Graph& g) : n_(g.n) {
-    const int64_t nnz = (int64_t)g.rowind.size();
-    if (nnz + n_ >= (int64_t)std::numeric_limits<int32_t>::max())
-      throw std::runtime_error("graph too large for 32-bit AMD");
-    iwlen_ = (int32_t)(nnz + n_);
-    pfree_ = (int32_t)nnz + 1;
-    const size_t N = (size_t)n_ + 1;
-    pe_.assign(N, 0);
-    len_.assign(N, 0);
-    nv_.assign(N, 0);
-    next_.assign(N, 0);
-    last_.assign(N, 0);
-    head_.assign(N, 0);
-    elen_.assign(N, 0);
-    degree_.assign(N, 0);
-    w_.assign(N, 0);
-    iw_.assign((size_t)iwlen_ + 1, 0);
-    for (int i = 1; i <= n_; ++i) {
-      pe_[i] = (int32_t)g.colptr[i - 1];
-      len_[i] = (int32_t)(g.colptr[i] - g.colptr[i - 1]);
-    }
-    for (int64_t k = 0; k < nnz; ++k) iw_[k + 1] = g.rowind[k];
+  explicit DegreeBuckets(int n) : first_(n + 2, 0), after_(n + 1, 0), before_(n + 1, 0), at_(n + 1, -1) {}
+  void insert(int32_t v, int32_t d) {
+    const int32_t f = first_[d];
+    after_[v] = f;
+    before_[v] = 0;
+    if (f) before_[f] = v;
+    first_[d] = v;
+    at_[v] = d;
   }
-
-  std::vector<int32_t> run() {
-    hmod_ = std::max(1, n_ - 1);
-    wbig_ = std::numeric_limits<int32_t>::max() - n_;
-    for (int i = 1; i <= n_; ++i) {
-      nv_[i] = 1;
-      w_[i] = 1;
-      degree_[i] = len_[i];
-    }
-    for (int i = 1; i <= n_; ++i) {
-      if (degree_[i] > 0) {
-        push_degree_list(i, degree_[i]);
-      } else {  // isolated vertex: numbered first, in index order
-        elen_[i] = -(++nel_);
-        pe_[i] = 0;
-        w_[i] = 0;
-      }
-    }
-    while (nel_ < n_) eliminate(select_pivot());
-    return number_variables();
+  void remove(int32_t v) {
+    const int32_t a = after_[v], b = before_[v];
+    if (a) before_[a] = b;
+    if (b) after_[b] = a;
+    else first_[at_[v]] = a;
+    at_[v] = -1;
+  }
+  bool holds(int32_t v) const { return at_[v] >= 0; }
+  // the first variable of the lowest non-empty bucket at or above *lo, taken out
+  int32_t take_min(int32_t* lo, int32_t top) {
+    int32_t d = *lo;
+    while (d <= top && !first_[d]) ++d;
+    if (d > top) throw std::runtime_error("AMD: no variable left to eliminate");
+    *lo = d;
+    const int32_t v = first_[d];
+    remove(v);
+    return v;
   }
 
  private:
-  int32_t n_, iwlen_, pfree_;
-  int32_t nel_ = 0, mindeg_ = 1, wflg_ = 2, dmax_ = 0, hmod_ = 1, wbig_ = 0;
-  // pe: start of a variable's / element's list in iw (or -parent once absorbed);
-  // len: list length; elen: number of elements at the front of a variable's list
-  // (negative order once eliminated); nv: supervariable size (negative while in the
-  // pivot element); degree: approximate external degree (element: |Le|);
-  // next / last / head: degree lists, reused as hash buckets; w: element marks.
-  std::vector<int32_t> pe_, len_, nv_, next_, last_, head_, elen_, degree_, w_, iw_;
+  std::vector<int32_t> first_, after_, before_, at_;
+};
 
-  void push_degree_list(int32_t i, int32_t deg) {
-    const int32_t inext = head_[deg];
-    if (inext != 0) last_[inext] = i;
-    next_[i] = inext;
-    head_[deg] = i;
+enum : int8_t { kVariable = 0, kElement = 1, kAbsorbed = 2 };
+
+class AmdOrdering {
+ public:
+  explicit AmdOrdering(const Graph& g)
+      : n_(g.n), kind_(n_ + 1, kVariable), weight_(n_ + 1, 1), degree_(n_ + 1, 0), mark_(n_ + 1, 1),
+        rank_(n_ + 1, 0), parent_(n_ + 1, 0), elems_(n_ + 1), vars_(n_ + 1), members_(n_ + 1), buckets_(n_) {
+    for (int v = 1; v <= n_; ++v) {
+      vars_[v].assign(g.rowind.begin() + (g.colptr[v - 1] - 1), g.rowind.begin() + (g.colptr[v] - 1));
+      degree_[v] = (int32_t)vars_[v].size();
+    }
+    hash_mod_ = std::max(1, n_ - 1);
+    stamp_limit_ = std::numeric_limits<int32_t>::max() - n_;
   }
 
-  void unlink_degree_list(int32_t i) {
-    const int32_t ilast = last_[i], inext = next_[i];
-    if (inext != 0) last_[inext] = ilast;
-    if (ilast != 0)
-      next_[ilast] = inext;
-    else
-      head_[degree_[i]] = inext;
+  std::vector<int32_t> order() {
+    for (int v = 1; v <= n_; ++v) {
+      if (degree_[v] > 0) {
+        buckets_.insert(v, degree_[v]);
+      } else {  // no neighbours: an element at once, numbered in index order
+        kind_[v] = kElement;
+        rank_[v] = ++done_;
+        mark_[v] = 0;
+        vars_[v].clear();
+      }
+    }
+    while (done_ < n_) eliminate(buckets_.take_min(&min_degree_, n_));
+    return final_numbers();
   }
 
-  void reset_marks_if_needed() {
-    if (wflg_ < wbig_) return;
+ private:
+  int32_t n_;
+  int32_t done_ = 0;        // variables eliminated so far (pivots, their supervariables, mass-eliminated)
+  int32_t min_degree_ = 1;
+  int32_t stamp_ = 2;       // mark value of the current pass; marks below it are stale
+  int32_t max_degree_ = 0;  // largest new-element degree so far (stamps advance by it)
+  int32_t hash_mod_, stamp_limit_;
+  std::vector<int8_t> kind_;
+  // weight: supervariable size (negated while the variable is in the new element)
+  // degree: approximate external degree of a variable, |Le| (weighted) of an element
+  // mark: per element, stamp_ + |Le \ Lme| during a degree update (0 once absorbed)
+  // rank: elimination number of an element; parent: where an absorbed variable went
+  std::vector<int32_t> weight_, degree_, mark_, rank_, parent_;
+  std::vector<std::vector<int32_t>> elems_, vars_, members_;
+  DegreeBuckets buckets_;
+  std::vector<int32_t> bucket_key_;
+  std::vector<std::vector<int32_t>> hash_buckets_;
+
+  void refresh_stamp() {
+    if (stamp_ < stamp_limit_) return;
     for (int x = 1; x <= n_; ++x)
-      if (w_[x] != 0) w_[x] = 1;
-    wflg_ = 2;
+      if (mark_[x] != 0) mark_[x] = 1;
+    stamp_ = 2;
   }
 
-  int32_t select_pivot() {
-    int32_t deg = mindeg_;
-    while (deg <= n_ && head_[deg] <= 0) ++deg;
-    if (deg > n_) throw std::runtime_error("AMD: degree lists exhausted early");
-    const int32_t me = head_[deg];
-    mindeg_ = deg;
-    const int32_t inext = next_[me];
-    if (inext != 0) last_[inext] = 0;
-    head_[deg] = inext;
-    return me;
-  }
-
-  // Move every live list to the front of iw, in the order the lists appear there,
-  // followed by the part of the new element built so far (iw[pme1 .. pfree-1]).  The
-  // first entry of each list is parked in pe and replaced by -owner, so that a linear
-  // pass can find where each list starts.
-  void compact(int32_t& pme1) {
-    for (int j = 1; j <= n_; ++j) {
-      const int32_t pn = pe_[j];
-      if (pn > 0) {
-        pe_[j] = iw_[pn];
-        iw_[pn] = -j;
-      }
+  // Pivot -> element: its variables and those of its adjacent elements (which it absorbs)
+  // become the new element's members, in collection order.
+  int32_t collect_new_element(int32_t me, std::vector<int32_t>& lme) {
+    int32_t wsum = 0;
+    auto take = [&](int32_t v) {
+      const int32_t wv = weight_[v];
+      if (wv <= 0) return;  // already collected, absorbed or eliminated
+      wsum += wv;
+      weight_[v] = -wv;
+      lme.push_back(v);
+      buckets_.remove(v);
+    };
+    for (int32_t e : elems_[me]) {
+      for (int32_t v : members_[e]) take(v);
+      // the element is absorbed into the new one: it stays an element (its number is kept)
+      // but leaves every list (unmarked)
+      parent_[e] = me;
+      mark_[e] = 0;
+      members_[e].clear();
+      members_[e].shrink_to_fit();
     }
-    int32_t pdst = 1, psrc = 1;
-    const int32_t pend = pme1 - 1;
-    while (psrc <= pend) {
-      const int32_t j = -iw_[psrc++];
-      if (j > 0) {
-        iw_[pdst] = pe_[j];
-        pe_[j] = pdst++;
-        const int32_t lenj = len_[j];
-        for (int32_t k = 0; k <= lenj - 2; ++k) iw_[pdst + k] = iw_[psrc + k];
-        pdst += lenj - 1;
-        psrc += lenj - 1;
-      }
-    }
-    const int32_t p1 = pdst;
-    for (int32_t ps = pme1; ps <= pfree_ - 1; ++ps) iw_[pdst++] = iw_[ps];
-    pme1 = p1;
-    pfree_ = pdst;
+    for (int32_t v : vars_[me]) take(v);
+    elems_[me].clear();
+    vars_[me].clear();
+    elems_[me].shrink_to_fit();
+    vars_[me].shrink_to_fit();
+    return wsum;
   }
 
   void eliminate(const int32_t me) {
-    const int32_t elenme = elen_[me];
-    elen_[me] = -(nel_ + 1);
-    int32_t nvpiv = nv_[me];
-    nel_ += nvpiv;
-    nv_[me] = -nvpiv;
-    int32_t degme = 0, pme1, pme2, newmem;
+    kind_[me] = kElement;
+    rank_[me] = done_ + 1;
+    int32_t pivot_weight = weight_[me];
+    done_ += pivot_weight;
+    weight_[me] = -pivot_weight;
+    std::vector<int32_t> lme;
+    int32_t lme_degree = collect_new_element(me, lme);
+    refresh_stamp();
 
-    // --- the new element Lme: the pivot's variables plus those of its elements ----
-    if (elenme == 0) {  // no adjacent elements: build Lme in place of me's list
-      pme1 = pe_[me];
-      pme2 = pme1 - 1;
-      for (int32_t p = pme1; p <= pme1 + len_[me] - 1; ++p) {
-        const int32_t i = iw_[p], nvi = nv_[i];
-        if (nvi > 0) {
-          degme += nvi;
-          nv_[i] = -nvi;
-          iw_[++pme2] = i;
-          unlink_degree_list(i);
-        }
-      }
-      newmem = 0;
-    } else {  // Lme appended at pfree; the elements it covers are absorbed
-      int32_t p = pe_[me];
-      pme1 = pfree_;
-      const int32_t slenme = len_[me] - elenme;
-      for (int32_t knt1 = 1; knt1 <= elenme + 1; ++knt1) {
-        int32_t e, pj, ln;
-        if (knt1 > elenme) {  // last: me's own variables
-          e = me;
-          pj = p;
-          ln = slenme;
-        } else {
-          e = iw_[p++];
-          pj = pe_[e];
-          ln = len_[e];
-        }
-        for (int32_t knt2 = 1; knt2 <= ln; ++knt2) {
-          const int32_t i = iw_[pj++], nvi = nv_[i];
-          if (nvi <= 0) continue;
-          if (pfree_ > iwlen_) {
-            // out of room: record how far me's and e's lists have been consumed, compact
-            pe_[me] = p;
-            len_[me] -= knt1;
-            if (len_[me] == 0) pe_[me] = 0;
-            pe_[e] = pj;
-            len_[e] = ln - knt2;
-            if (len_[e] == 0) pe_[e] = 0;
-            compact(pme1);
-            pj = pe_[e];
-            p = pe_[me];
-          }
-          degme += nvi;
-          nv_[i] = -nvi;
-          iw_[pfree_++] = i;
-          unlink_degree_list(i);
-        }
-        if (e != me) {  // element e absorbed into me
-          pe_[e] = -me;
-          w_[e] = 0;
-        }
-      }
-      pme2 = pfree_ - 1;
-      newmem = pfree_ - pme1;
-    }
-    degree_[me] = degme;
-    pe_[me] = pme1;
-    len_[me] = pme2 - pme1 + 1;
-    reset_marks_if_needed();
-
-    // --- w[e] - wflg = |Le \ Lme| for every element e adjacent to Lme ------------------
-    for (int32_t pme = pme1; pme <= pme2; ++pme) {
-      const int32_t i = iw_[pme], eln = elen_[i];
-      if (eln <= 0) continue;
-      const int32_t nvi = -nv_[i], wnvi = wflg_ - nvi;
-      for (int32_t p = pe_[i]; p <= pe_[i] + eln - 1; ++p) {
-        const int32_t e = iw_[p];
-        int32_t we = w_[e];
-        if (we >= wflg_)
-          we -= nvi;
-        else if (we != 0)
-          we = degree_[e] + wnvi;
-        w_[e] = we;
+    // |Le \ Lme| for every element e adjacent to the new element's variables
+    for (int32_t v : lme) {
+      const int32_t wv = -weight_[v];
+      for (int32_t e : elems_[v]) {
+        int32_t m = mark_[e];
+        if (m >= stamp_) m -= wv;
+        else if (m != 0) m = degree_[e] + stamp_ - wv;
+        mark_[e] = m;
       }
     }
 
-    // --- approximate degrees, pruned lists, mass elimination, hash keys ---------------
-    for (int32_t pme = pme1; pme <= pme2; ++pme) {
-      const int32_t i = iw_[pme];
-      const int32_t p1 = pe_[i], p2 = p1 + elen_[i] - 1;
-      int32_t pn = p1, deg = 0;
-      uint32_t hash = 0;  // 32-bit sum, wrapping as the reference's INTEGER*4 does
-      for (int32_t p = p1; p <= p2; ++p) {
-        const int32_t e = iw_[p], we = w_[e];
-        if (we != 0) {  // element still alive (absorbed ones have w = 0)
-          deg += we - wflg_;
-          iw_[pn++] = e;
+    // approximate degrees, pruned lists, mass elimination, hash buckets
+    if (hash_buckets_.empty()) {
+      hash_buckets_.resize((size_t)hash_mod_ + 2);
+      bucket_key_.assign(n_ + 1, 0);
+    }
+    for (int32_t v : lme) {
+      int32_t d = 0;
+      uint32_t hash = 0;  // wraps like a 32-bit integer sum
+      std::vector<int32_t>& E = elems_[v];
+      size_t ke = 0;
+      for (int32_t e : E)
+        if (mark_[e] != 0) {  // still an element (absorbed ones are unmarked)
+          d += mark_[e] - stamp_;
+          E[ke++] = e;
           hash += (uint32_t)e;
         }
-      }
-      elen_[i] = pn - p1 + 1;  // + 1 for me, placed first below
-      const int32_t p3 = pn;
-      for (int32_t p = p2 + 1; p <= p1 + len_[i] - 1; ++p) {
-        const int32_t j = iw_[p], nvj = nv_[j];
-        if (nvj > 0) {  // variable not in Lme
-          deg += nvj;
-          iw_[pn++] = j;
-          hash += (uint32_t)j;
+      E.resize(ke);
+      std::vector<int32_t>& V = vars_[v];
+      size_t kv = 0;
+      for (int32_t u : V)
+        if (weight_[u] > 0) {  // a variable outside the new element
+          d += weight_[u];
+          V[kv++] = u;
+          hash += (uint32_t)u;
         }
+      V.resize(kv);
+      if (ke == 0 && kv == 0) {  // adjacent to the new element only: eliminated with it
+        kind_[v] = kAbsorbed;
+        parent_[v] = me;
+        const int32_t wv = -weight_[v];
+        lme_degree -= wv;
+        pivot_weight += wv;
+        done_ += wv;
+        weight_[v] = 0;
+        E.clear();
+        V.clear();
+        continue;
       }
-      if (elen_[i] == 1 && p3 == pn) {
-        // i is adjacent to me only: eliminated together with me (mass elimination)
-        pe_[i] = -me;
-        const int32_t nvi = -nv_[i];
-        degme -= nvi;
-        nvpiv += nvi;
-        nel_ += nvi;
-        nv_[i] = 0;
-        elen_[i] = 0;
-      } else {
-        degree_[i] = std::min(degree_[i], deg);
-        // me goes to the front of i's list: first variable moves to the end, first
-        // element to the first variable's place
-        iw_[pn] = iw_[p3];
-        iw_[p3] = iw_[p1];
-        iw_[p1] = me;
-        len_[i] = pn - p1 + 1;
-        const int32_t key = (int32_t)hash % hmod_ + 1;
-        const int32_t j = head_[key];
-        if (j <= 0) {  // bucket kept in head (as -first) while the degree list is empty
-          next_[i] = -j;
-          head_[key] = -i;
-        } else {  // degree list in use: bucket kept in last[] of the list's head
-          next_[i] = last_[j];
-          last_[j] = i;
-        }
-        last_[i] = key;
-      }
+      degree_[v] = std::min(degree_[v], d);
+      // the new element first, the first surviving element and variable rotate to the back
+      if (ke > 0) std::rotate(E.begin(), E.begin() + 1, E.end());
+      E.insert(E.begin(), me);
+      if (kv > 0) std::rotate(V.begin(), V.begin() + 1, V.end());
+      int32_t key = (int32_t)hash % hash_mod_ + 1;
+      if (key < 1) key += hash_mod_;  // a negative wrapped sum (not reached by graphs of < 2^31 / n entries)
+      hash_buckets_[key].push_back(v);  // read back to front: last in, first out
+      bucket_key_[v] = key;
     }
-    degree_[me] = degme;
-    dmax_ = std::max(dmax_, degme);
-    wflg_ += dmax_;
-    reset_marks_if_needed();
+    degree_[me] = lme_degree;
+    max_degree_ = std::max(max_degree_, lme_degree);
+    stamp_ += max_degree_;
+    refresh_stamp();
 
-    // --- supervariables: equal lists within a hash bucket merge into the first --------
-    for (int32_t pme = pme1; pme <= pme2; ++pme) {
-      int32_t i = iw_[pme];
-      if (nv_[i] >= 0) continue;
-      const int32_t key = last_[i];
-      const int32_t j0 = head_[key];
-      if (j0 == 0) continue;
-      if (j0 < 0) {
-        i = -j0;
-        head_[key] = 0;
-      } else {
-        i = last_[j0];
-        last_[j0] = 0;
-      }
-      while (i != 0 && next_[i] != 0) {
-        const int32_t ln = len_[i], eln = elen_[i];
-        for (int32_t p = pe_[i] + 1; p <= pe_[i] + ln - 1; ++p) w_[iw_[p]] = wflg_;
-        int32_t jlast = i, j = next_[i];
-        while (j != 0) {
-          bool same = len_[j] == ln && elen_[j] == eln;
-          for (int32_t p = pe_[j] + 1; same && p <= pe_[j] + ln - 1; ++p) same = w_[iw_[p]] == wflg_;
-          if (same) {  // j is indistinguishable from i: absorb it
-            pe_[j] = -i;
-            nv_[i] += nv_[j];
-            nv_[j] = 0;
-            elen_[j] = 0;
-            j = next_[j];
-            next_[jlast] = j;
-          } else {
-            jlast = j;
-            j = next_[j];
-          }
+    // supervariables: variables of one bucket with equal lists merge into the first
+    std::vector<int32_t> chain;
+    for (int32_t v : lme) {
+      if (weight_[v] >= 0) continue;  // mass-eliminated or merged already
+      std::vector<int32_t>& bucket = hash_buckets_[bucket_key_[v]];
+      if (bucket.empty()) continue;  // bucket done
+      chain.assign(bucket.rbegin(), bucket.rend());
+      bucket.clear();
+      for (size_t a = 0; a + 1 < chain.size(); ++a) {
+        const int32_t i = chain[a];
+        if (i == 0) continue;
+        size_t live = a + 1;  // the scan ends at the bucket's last live variable
+        while (live < chain.size() && chain[live] == 0) ++live;
+        if (live == chain.size()) break;
+        auto tail_of = [&](int32_t x, auto&& f) {  // every list entry but the first (the new element)
+          for (size_t q = 1; q < elems_[x].size(); ++q) f(elems_[x][q]);
+          for (int32_t u : vars_[x]) f(u);
+        };
+        tail_of(i, [&](int32_t y) { mark_[y] = stamp_; });
+        for (size_t b = a + 1; b < chain.size(); ++b) {
+          const int32_t j = chain[b];
+          if (j == 0 || elems_[j].size() != elems_[i].size() || vars_[j].size() != vars_[i].size()) continue;
+          bool same = true;
+          tail_of(j, [&](int32_t y) { same = same && mark_[y] == stamp_; });
+          if (!same) continue;
+          kind_[j] = kAbsorbed;  // j is indistinguishable from i: merged into it
+          parent_[j] = i;
+          weight_[i] += weight_[j];
+          weight_[j] = 0;
+          elems_[j].clear();
+          vars_[j].clear();
+          chain[b] = 0;
         }
-        ++wflg_;
-        i = next_[i];
+        ++stamp_;
       }
     }
 
-    // --- finalise degrees, put the variables of Lme back in the degree lists ----------
-    int32_t p = pme1;
-    const int32_t nleft = n_ - nel_;
-    for (int32_t pme = pme1; pme <= pme2; ++pme) {
-      const int32_t i = iw_[pme], nvi = -nv_[i];
-      if (nvi <= 0) continue;
-      nv_[i] = nvi;
-      const int32_t deg = std::max(1, std::min(degree_[i] + degme - nvi, nleft - nvi));
-      push_degree_list(i, deg);
-      last_[i] = 0;
-      mindeg_ = std::min(mindeg_, deg);
-      degree_[i] = deg;
-      iw_[p++] = i;
+    // final degrees; the new element's surviving variables go back into the buckets
+    const int32_t left = n_ - done_;
+    std::vector<int32_t>& le = members_[me];
+    for (int32_t v : lme) {
+      const int32_t wv = -weight_[v];
+      if (wv <= 0) continue;
+      weight_[v] = wv;
+      const int32_t d = std::max(1, std::min(degree_[v] + lme_degree - wv, left - wv));
+      buckets_.insert(v, d);
+      min_degree_ = std::min(min_degree_, d);
+      degree_[v] = d;
+      le.push_back(v);
     }
-    nv_[me] = nvpiv + degme;
-    len_[me] = p - pme1;
-    if (len_[me] == 0) {
-      pe_[me] = 0;
-      w_[me] = 0;
-    }
-    if (newmem != 0) pfree_ = p;
+    weight_[me] = pivot_weight + lme_degree;
+    if (le.empty()) mark_[me] = 0;
   }
 
-  // Number the variables that were absorbed into supervariables or mass-eliminated
-  // right after the principal variable they were merged into (walking the absorption
-  // links, with path compression), and return invp.
-  std::vector<int32_t> number_variables() {
-    for (int i = 1; i <= n_; ++i) {
-      if (elen_[i] != 0) continue;
-      int32_t j = -pe_[i];
-      while (elen_[j] >= 0) j = -pe_[j];
-      const int32_t e = j;
-      int32_t k = -elen_[e];
-      j = i;
-      while (elen_[j] >= 0) {
-        const int32_t jnext = -pe_[j];
-        pe_[j] = -e;
-        if (elen_[j] == 0) elen_[j] = k++;
-        j = jnext;
+  // Elimination numbers: an absorbed variable is numbered just before the element that
+  // finally contains it (its chain of parents is walked, every absorbed variable on the
+  // way numbered in walk order and pointed at that element), and the element after all
+  // of them.  Returns invp (1-based numbers).
+  std::vector<int32_t> final_numbers() {
+    std::vector<int32_t> number(n_ + 1, 0), next_rank(rank_);
+    for (int v = 1; v <= n_; ++v) {
+      if (kind_[v] != kAbsorbed || number[v] != 0) continue;
+      int32_t e = parent_[v];
+      while (kind_[e] != kElement) e = parent_[e];
+      int32_t k = next_rank[e];
+      for (int32_t j = v; kind_[j] != kElement;) {
+        const int32_t up = parent_[j];
+        parent_[j] = e;
+        if (kind_[j] == kAbsorbed && number[j] == 0) number[j] = k++;
+        j = up;
       }
-      elen_[e] = -k;
+      next_rank[e] = k;
     }
     std::vector<int32_t> invp(n_);
-    for (int i = 1; i <= n_; ++i) invp[i - 1] = elen_[i] < 0 ? -elen_[i] : elen_[i];
+    for (int v = 1; v <= n_; ++v) invp[v - 1] = kind_[v] == kElement ? next_rank[v] : number[v];
     return invp;
   }
 };
@@ -379,8 +309,10 @@ class ApproxMinDegree {
 
 std::vector<int32_t> amd_order(const Graph& g) {
   if (g.n == 0) return {};
-  ApproxMinDegree amd(g);
-  return amd.run();
+  if ((int64_t)g.rowind.size() + g.n >= (int64_t)std::numeric_limits<int32_t>::max())
+    throw std::runtime_error("graph too large for 32-bit AMD");
+  AmdOrdering amd(g);
+  return amd.order();
 }
 
 }  // namespace spb

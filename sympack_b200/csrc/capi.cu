@@ -701,6 +701,7 @@ spb::PlanParams plan_params_of(const spb_options& o) {
   if (o.plan_outer_nb > 0) pp.outer_nb = o.plan_outer_nb;
   if (o.plan_solve_chunk > 0) pp.solve_sb = o.plan_solve_chunk;
   if (o.plan_solve_tiles > 0) pp.solve_tpt = o.plan_solve_tiles;
+  pp.factor_dag = o.precision == SPB_PRECISION_FP64 && o.factor_schedule == SPB_FACTOR_PERSISTENT;
   return pp;
 }
 

@@ -122,6 +122,17 @@ __device__ __forceinline__ void cp_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
 }
 
+// D = A(16x16, row) * B(16x8, col) + D, FP64; lane = 4*g + t:
+//   a[2j] = A[g][t+4j], a[2j+1] = A[g+8][t+4j], b[j] = B[t+4j][g] (j < 4), d as for m16n8k4.
+__device__ __forceinline__ void dmma_16x8x16(double* d, const double* a, const double* b) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7,%8,%9,%10,%11}, "
+      "{%12,%13,%14,%15}, {%0,%1,%2,%3};\n"
+      : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+      : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(a[4]), "d"(a[5]), "d"(a[6]), "d"(a[7]), "d"(b[0]),
+        "d"(b[1]), "d"(b[2]), "d"(b[3]));
+}
+
 // D = A(16x4, row) * B(4x8, col) + D, FP64.  Fragment ownership (lane = 4*g + t):
 //   a0 = A[g][t], a1 = A[g+8][t], b0 = B[t][g],
 //   d0 = D[g][2t], d1 = D[g][2t+1], d2 = D[g+8][2t], d3 = D[g+8][2t+1].
@@ -184,22 +195,23 @@ __device__ void dmma_tile_task(const FactorArgs& a, const TileItem& it, unsigned
     cp_commit();
     const double* As = pipe + (size_t)(kt % kDStages) * 2 * kDK * kDLds;
     const double* Bs = As + kDK * kDLds;
+    // one m16n8k16 step per stage: the B fragments of the warp's four column tiles,
+    // then per row tile its A fragment and four MMAs
+    double bf[4][4];
 #pragma unroll
-    for (int ks = 0; ks < kDK; ks += 4) {
-      double af[4][2], bf[4];
-      const double* Ak = As + (ks + tq) * kDLds + wm * 64 + gq;
-      const double* Bk = Bs + (ks + tq) * kDLds + wn * 32 + gq;
+    for (int ni = 0; ni < 4; ++ni)
 #pragma unroll
-      for (int mi = 0; mi < 4; ++mi) {
-        af[mi][0] = Ak[mi * 16];
-        af[mi][1] = Ak[mi * 16 + 8];
+      for (int j = 0; j < 4; ++j) bf[ni][j] = Bs[(tq + 4 * j) * kDLds + wn * 32 + ni * 8 + gq];
+#pragma unroll
+    for (int mi = 0; mi < 4; ++mi) {
+      double af[8];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        af[2 * j] = As[(tq + 4 * j) * kDLds + wm * 64 + mi * 16 + gq];
+        af[2 * j + 1] = As[(tq + 4 * j) * kDLds + wm * 64 + mi * 16 + gq + 8];
       }
 #pragma unroll
-      for (int ni = 0; ni < 4; ++ni) bf[ni] = Bk[ni * 8];
-#pragma unroll
-      for (int mi = 0; mi < 4; ++mi)
-#pragma unroll
-        for (int ni = 0; ni < 4; ++ni) dmma_16x8x4(acc[mi][ni], af[mi][0], af[mi][1], bf[ni]);
+      for (int ni = 0; ni < 4; ++ni) dmma_16x8x16(acc[mi][ni], af, bf[ni]);
     }
   }
   cp_wait<0>();

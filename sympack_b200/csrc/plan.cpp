@@ -268,7 +268,7 @@ Plan build_plan(const Symbolic& sym, const PlanParams& prm) {
     P.step_flops[k] = f;
   }
   for (const SnMeta& m : P.meta) P.solve_sweep_bytes += 8.0 * m.h * m.w;
-  build_factor_dag(P);
+  if (prm.factor_dag) build_factor_dag(P);
 
   // Solve super-blocks: per supernode, its first super-block counter and (for
   // supernodes wider than one block) the offset of its inverse tiles.
@@ -486,26 +486,39 @@ static void build_factor_dag(Plan& P) {
   }
   // dependency graph for the simulation: every counter is a zero-time join node whose
   // predecessors are its signalling tasks; a task depends on the joins it waits for
-  // (a TRSM tile waits for its block's POTRF only)
+  // (a TRSM tile waits for its block's POTRF only).  Successor lists in CSR form.
   const int nt = (int)raw.size(), nc = P.nfctr, nn = nt + nc;
-  std::vector<std::vector<int32_t>> succ(nn);
-  std::vector<int32_t> npred(nn, 0);
   std::vector<int32_t> potrf_of(nb, -1);
   for (int k = 0; k < nt; ++k)
     if (raw[k].kind == 1) potrf_of[P.meta[P.panel_items[raw[k].item].s].boff + P.panel_items[raw[k].item].c0 / 64] = k;
-  for (int k = 0; k < nt; ++k) {
-    for (int32_t c : raw[k].sig) {
-      succ[k].push_back(nt + c);
-      npred[nt + c]++;
+  std::vector<int64_t> soff(nn + 1, 0);
+  std::vector<int32_t> npred(nn, 0);
+  auto for_edges = [&](auto&& edge) {
+    for (int k = 0; k < nt; ++k) {
+      for (int32_t c : raw[k].sig) edge(k, nt + c);
+      for (const FWait& w : waits[k]) {
+        if (w.target <= 0) continue;
+        edge(raw[k].kind == 2 ? potrf_of[w.ctr - BLK] : nt + w.ctr, k);
+      }
     }
-    for (const FWait& w : waits[k]) {
-      if (w.target <= 0) continue;
-      int from = nt + w.ctr;
-      if (raw[k].kind == 2) from = potrf_of[w.ctr - BLK];
-      succ[from].push_back(k);
-      npred[k]++;
-    }
+  };
+  for_edges([&](int from, int to) {
+    soff[from + 1]++;
+    npred[to]++;
+  });
+  for (int v = 0; v < nn; ++v) soff[v + 1] += soff[v];
+  std::vector<int32_t> sadj(soff[nn]);
+  {
+    std::vector<int64_t> fill(soff.begin(), soff.end() - 1);
+    for_edges([&](int from, int to) { sadj[fill[from]++] = to; });
   }
+  struct SuccRange {
+    const int32_t* b;
+    const int32_t* e;
+    const int32_t* begin() const { return b; }
+    const int32_t* end() const { return e; }
+  };
+  auto succ_of = [&](int v) { return SuccRange{sadj.data() + soff[v], sadj.data() + soff[v + 1]}; };
   // bottom levels (longest path to the end), in reverse topological order: counters
   // and tasks are processed after all their successors via a Kahn order
   std::vector<double> dur(nn, 0.0), blev(nn, 0.0);
@@ -517,14 +530,14 @@ static void build_factor_dag(Plan& P) {
     for (int v = 0; v < nn; ++v)
       if (!indeg[v]) order.push_back(v);
     for (size_t q = 0; q < order.size(); ++q)
-      for (int32_t u : succ[order[q]])
+      for (int32_t u : succ_of(order[q]))
         if (--indeg[u] == 0) order.push_back(u);
     if ((int)order.size() != nn) throw std::runtime_error("plan: factorization task graph has a cycle");
   }
   for (int q = nn - 1; q >= 0; --q) {
     const int v = order[q];
     double best = 0.0;
-    for (int32_t u : succ[v]) best = std::max(best, blev[u]);
+    for (int32_t u : succ_of(v)) best = std::max(best, blev[u]);
     blev[v] = dur[v] + best;
   }
   // list scheduling on the SMs (one CTA per SM)
@@ -542,7 +555,7 @@ static void build_factor_dag(Plan& P) {
     while (!stack.empty()) {
       const int32_t x = stack.back();
       stack.pop_back();
-      for (int32_t u : succ[x])
+      for (int32_t u : succ_of(x))
         if (--pend[u] == 0) {
           if (u >= nt) stack.push_back(u);
           else ready.push(u);
