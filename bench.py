@@ -56,7 +56,13 @@ def parse():
                     help="systems of the batching workload (2000 = the named workload; the host analysis of its "
                          "random graphs takes about two minutes)")
     ap.add_argument("--serve-requests", type=int, default=10000,
-                    help="requests of the serving workload (10000 = the named workload)")
+                    help="requests of the serving workload (10000 = the named workload), run whole by the "
+                         "continuous-batching loop at capacity")
+    ap.add_argument("--serve-sample", type=int, default=2000,
+                    help="requests of the stream's start run back to back (FP64 baseline) and with Poisson "
+                         "arrivals at 0.7x capacity (a rate: it does not depend on how many follow)")
+    ap.add_argument("--serve-fp64-batching", action="store_true",
+                    help="also run the continuous-batching loop in FP64 at capacity")
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-ldl", action="store_true", help="skip the LDL^T vs Cholesky comparison")
     ap.add_argument("--no-serve", action="store_true")
@@ -247,42 +253,54 @@ def precision_comparison(torch, dev, stream, grid=80, reps=2):
     from sympack_b200 import DistSparseMatrix, generators as G, symPACKMatrix2D, symPACKOptions
     n, cp, ri, v = G.stencil27(grid, grid, grid, 1e-2, seed=0)
     A = DistSparseMatrix.from_lower_csc(n, cp, ri, v)
-    handles = {}
-    for prec in ("FP64", "FP32_IR"):
-        M = symPACKMatrix2D()
-        M.Init(symPACKOptions(device=dev.index, precision=prec))
-        M.SymbolicFactorization(A)
-        M.SetStream(stream.cuda_stream)
-        handles[prec] = M
-    flops = handles["FP64"].info().flops_stat
+    T = symPACKMatrix2D()
+    T.Init(symPACKOptions(device=-1))
+    T.SymbolicFactorization(A)
+    flops = T.info().flops_stat
     b = torch.from_numpy(np.random.default_rng(0).standard_normal(n)).to(dev)
     x = torch.empty_like(b)
     out = {"workload": f"3D 27-point stencil {grid}^3 (n={n}), off-diagonals U[-1,0), seed 0, nrhs 1",
            "flops_stat": flops}
-    # outer block of the blocked panel factorization: each precision keeps the faster of
-    # 256 and 512 columns on this matrix (timed once, outside the comparison)
+    # plan of each precision: the fastest factorization schedule (one persistent launch, or
+    # the level-ordered launch sequence) and outer block (256 or 512 columns) on this matrix,
+    # timed once, outside the comparison
     _, _, _, v0 = G.stencil27(grid, grid, grid, 1e-2, seed=0)
     dv0 = torch.from_numpy(v0).to(dev)
-    outer = {}
-    for prec, M in handles.items():
+    handles, plans = {}, {}
+    for prec in ("FP64", "FP32_IR"):
         best = None
-        for onb in (256, 512):
-            M.Replan(0, 0, onb)
-            ts = []
-            for r in range(3):
-                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                e0.record(stream)
-                M.DistributeMatrixDevice(dv0.data_ptr())
-                M.Factorize()
-                e1.record(stream)
-                torch.cuda.synchronize()
-                if r:
-                    ts.append(e0.elapsed_time(e1))
-            if best is None or min(ts) < best[1]:
-                best = (onb, min(ts))
-        M.Replan(0, 0, best[0])
-        outer[prec] = {"outer_nb": best[0], "factor_ms": best[1]}
-    out["outer_block"] = outer
+        for sched in ("persistent", "steps"):
+            M = symPACKMatrix2D()
+            M.Init(symPACKOptions(device=dev.index, precision=prec, factor_schedule=sched))
+            M.SymbolicFactorizationFrom(T)
+            M.SetStream(stream.cuda_stream)
+            mine = None
+            for onb in (256, 512):
+                M.Replan(0, 0, onb)
+                ts = []
+                for r in range(3):
+                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    e0.record(stream)
+                    M.DistributeMatrixDevice(dv0.data_ptr())
+                    M.Factorize()
+                    e1.record(stream)
+                    torch.cuda.synchronize()
+                    if r:
+                        ts.append(e0.elapsed_time(e1))
+                plans.setdefault(prec, {})[f"{sched},{onb}"] = round(min(ts), 2)
+                if mine is None or min(ts) < mine[1]:
+                    mine = (onb, min(ts))
+            if best is None or mine[1] < best[2]:
+                if best is not None:
+                    best[3].close()
+                M.Replan(0, 0, mine[0])
+                best = (sched, mine[0], mine[1], M)
+            else:
+                M.close()
+        handles[prec] = best[3]
+        plans[prec]["chosen"] = {"factor_schedule": best[0], "outer_nb": best[1], "factor_ms": best[2]}
+    T.close()
+    out["plans_factor_ms"] = plans
     for delta in (1e-2, 1e-5):
         _, _, _, vd = G.stencil27(grid, grid, grid, delta, seed=0)
         dv = torch.from_numpy(vd).to(dev)
@@ -391,7 +409,9 @@ def batching_comparison(torch, dev, stream, count, seed=0, subset=64, tune_syste
     autotuner on the first `tune_systems` systems (each candidate re-plans the batch, so the
     candidates are timed on that sample and the winner plans the whole batch); beside it the
     first `subset` systems factored one by one versus as one batch."""
-    from sympack_b200 import DistSparseMatrix, autotune, generators as G, symPACKMatrix2D, symPACKOptions
+    from sympack_b200 import (DistSparseMatrix, SymPACKError, autotune, generators as G, symPACKMatrix2D,
+                              symPACKOptions)
+    SPB_ERR_OOM = -3  # include/sympack_b200.h
     systems = G.batch_systems(count, 500, 20000, seed=seed)
     n, cp, ri, v, offs = G.block_diagonal(systems)
     A = DistSparseMatrix.from_lower_csc(n, cp, ri, v)
@@ -419,10 +439,21 @@ def batching_comparison(torch, dev, stream, count, seed=0, subset=64, tune_syste
         S.SymbolicFactorizationBatch(At, toffs)
         tune = autotune.tune(S, At, toffs, reps=1, use_cache=False)
         S.close()
-        M = symPACKMatrix2D()
-        M.Init(symPACKOptions(device=dev.index, precision=prec, plan_small_max_w=tune["small_max_w"],
-                              plan_big_tile_rows=tune["big_tile_rows"], plan_outer_nb=tune["outer_nb"]))
-        M.SymbolicFactorizationFrom(T)
+        # the FP32 tiles read TMA-fed split copies of the panels when they fit the device
+        # (they double the FP32 arena), else stage and split their operands per tile
+        engines = [{}] if prec == "FP64" else [{"fp32_engine": "tcgen05-tma"}, {"fp32_engine": "tcgen05"}]
+        for eng in engines:
+            M = symPACKMatrix2D()
+            M.Init(symPACKOptions(device=dev.index, precision=prec, plan_small_max_w=tune["small_max_w"],
+                                  plan_big_tile_rows=tune["big_tile_rows"], plan_outer_nb=tune["outer_nb"], **eng))
+            try:
+                M.SymbolicFactorizationFrom(T)
+                break
+            except SymPACKError as e:
+                M.close()
+                torch.cuda.empty_cache()
+                if e.code != SPB_ERR_OOM or eng is engines[-1]:
+                    raise
         M.SetStream(stream.cuda_stream)
         times = []
         for r in range(3):
@@ -444,6 +475,7 @@ def batching_comparison(torch, dev, stream, count, seed=0, subset=64, tune_syste
                      "backward_error_max_over_systems": per_system_backward_error(systems, offs, dx.cpu().numpy(), b),
                      "ir_iterations": mi.ir_iterations if prec == "FP32_IR" else 0,
                      "factor_launches": mi.factor_launches, "device_bytes": mi.device_bytes,
+                     "fp32_engine": eng.get("fp32_engine"),
                      "autotuned_plan": {"small_max_w": tune["small_max_w"], "big_tile_rows": tune["big_tile_rows"],
                                         "outer_nb": tune["outer_nb"], "tuned_on_systems": len(sample),
                                         "candidates_ms": {k: round(v * 1e3, 3) for k, v in tune["times"].items()}}}
@@ -490,16 +522,17 @@ def batching_comparison(torch, dev, stream, count, seed=0, subset=64, tune_syste
     return out
 
 
-def serving_comparison(torch, dev, count, seed=0, load=0.7, base_count=2000, check_every=25):
+def serving_comparison(torch, dev, count, seed=0, load=0.7, sample=2000, fp64_batching=False, check_every=25):
     """Serving form on the request stream: (1) back-to-back plain FP64, one request after
-    the other, on the stream's first `base_count` requests (a sequential baseline: its rate
+    the other, on the stream's first `sample` requests (a sequential baseline: its rate
     does not depend on how many requests follow); (2) the continuous-batching loop (8 slots,
-    right-hand sides merged per factor) in FP64 and in FP32 + refinement with every request
-    submitted at once, which gives each precision's capacity; (3) the FP32 + refinement loop
-    with Poisson arrivals at `load` x its capacity, which gives p50 / p99 latency at a
-    sustainable rate.  Every `check_every`-th result is checked on the host: its backward
-    error ||b - A x||_inf / (||A||_inf ||x||_inf + ||b||_inf) (FP64 results do not compute it
-    on the device)."""
+    right-hand sides merged per factor) in FP32 + refinement with all `count` requests
+    submitted at once, which gives its capacity (and, with `fp64_batching`, the same loop in
+    FP64); (3) the FP32 + refinement loop on the first `sample` requests with Poisson
+    arrivals at `load` x its capacity, which gives p50 / p99 latency at a sustainable rate.
+    Every `check_every`-th result is checked on the host: its backward error
+    ||b - A x||_inf / (||A||_inf ||x||_inf + ||b||_inf) (FP64 results do not compute it on
+    the device)."""
     from sympack_b200 import serving as S
     mk = lambda k: S.request_stream(k, 1.0, seed=seed)
     patterns = {}
@@ -546,26 +579,29 @@ def serving_comparison(torch, dev, count, seed=0, load=0.7, base_count=2000, che
         out.update({kk: int(v) for kk, v in svc.stats.items()})
         return out
 
-    base = run("FP64", 1, 1, None, min(base_count, count))
-    cap64 = run("FP64", 8, 64, 0.0, count)
+    sample = min(sample, count)
+    base = run("FP64", 1, 1, None, sample)
     cap = run("FP32_IR", 8, 64, 0.0, count)
     rate = load * cap["solves_per_s"]
-    lat = run("FP32_IR", 8, 64, rate, count)
+    lat = run("FP32_IR", 8, 64, rate, sample)
     lat["arrival_rate_per_s"] = rate
-    return {
+    out = {
         "workload": f"{count} requests, Poisson arrivals, 30% factor+solve on fresh 27-point stencil (delta 1e-2) "
                     f"or 2D Laplacian matrices, n 1k-216k on a grid ladder, 70% solve-only against the 8 latest "
                     f"factors, nrhs U{{1..64}} (seed {seed})",
         "requests": count,
         "back_to_back_fp64": base,
-        "continuous_batching_fp64_capacity": cap64,
         "continuous_batching_fp32_ir_capacity": cap,
         "continuous_batching_fp32_ir_at_load": lat,
         "speedup_solves_per_s_at_load": lat["solves_per_s"] / base["solves_per_s"],
-        "speedup_capacity_batching_fp64": cap64["solves_per_s"] / base["solves_per_s"],
-        "speedup_capacity_precision_fp32_ir_over_fp64": cap["solves_per_s"] / cap64["solves_per_s"],
         "speedup_capacity": cap["solves_per_s"] / base["solves_per_s"],
     }
+    if fp64_batching:
+        cap64 = run("FP64", 8, 64, 0.0, count)
+        out["continuous_batching_fp64_capacity"] = cap64
+        out["speedup_capacity_batching_fp64"] = cap64["solves_per_s"] / base["solves_per_s"]
+        out["speedup_capacity_precision_fp32_ir_over_fp64"] = cap["solves_per_s"] / cap64["solves_per_s"]
+    return out
 
 
 def run_ours(args):
@@ -726,7 +762,8 @@ def run_ours(args):
     precision = section(not args.no_precision, precision_comparison, torch, dev, stream, grid=args.precision_grid)
     ldl = section(not args.no_ldl, ldl_comparison, torch, dev, stream, grid=args.grid)
     batching = section(not args.no_batch, batching_comparison, torch, dev, stream, args.batch_systems)
-    serving = section(not args.no_serve, serving_comparison, torch, dev, args.serve_requests)
+    serving = section(not args.no_serve, serving_comparison, torch, dev, args.serve_requests,
+                      sample=args.serve_sample, fp64_batching=args.serve_fp64_batching)
 
     cpu = None
     if world == 1 and rank == 0 and not args.no_cpu_baseline:

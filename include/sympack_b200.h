@@ -82,9 +82,12 @@ typedef struct spb_options {
   int verbose;
   int plan_small_max_w;    /* widest supernode factored whole in shared memory (0 = default 32) */
   int plan_big_tile_rows;  /* products with this many rows use 128 x 128 tensor-core tiles (0 = default 128) */
-  int fp32_engine;         /* FP32_IR 128 x 128 update tiles: 0 = tcgen05 one tile per CTA (TMEM
-                              accumulator), 1 = mma.sync, 2 = persistent tcgen05 (two accumulators,
-                              epilogue warps overlapped with the next tile) */
+  int fp32_engine;         /* FP32_IR 128 x 128 update tiles: 3 = tcgen05 with its operands loaded by
+                              TMA from split (hi / lo) copies of the panels, one tensor map per panel
+                              with such tiles (spb_default_options; the copies double the FP32 arena's
+                              footprint); 0 = tcgen05 with operands staged by cp.async and split per
+                              tile (no copies); 1 = mma.sync; 2 = a persistent tcgen05 variant (two
+                              accumulators, epilogue warps overlapped with the next tile) */
   int decomposition;       /* SPB_DECOMPOSITION_* (symPACKOptions::decomposition, Types.hpp:97,119) */
   int plan_outer_nb;       /* columns per outer block of a wide panel: its trailing columns are
                               updated once per outer block (0 = default 256; multiple of 64, <= 4096) */
@@ -93,13 +96,17 @@ typedef struct spb_options {
   int plan_solve_chunk;    /* 64-column blocks per solve super-block: a supernode wider than one block
                               is solved through the inverses of its diagonal super-blocks (0 = default 8) */
   int plan_solve_tiles;    /* 64 x 64 tiles per super-block solve task (0 = default 2) */
-  int factor_schedule;     /* FP64 factorization: SPB_FACTOR_PERSISTENT (default) runs every task in one
-                              persistent launch ordered by dependency counters; SPB_FACTOR_STEPS runs
-                              the level-ordered launch sequence (the FP32 form always does) */
+  int factor_schedule;     /* SPB_FACTOR_PERSISTENT runs every task of the factorization in one
+                              persistent launch ordered by dependency counters (FP64, and the FP32
+                              form with fp32_engine 3); SPB_FACTOR_STEPS runs the level-ordered launch
+                              sequence replayed from a CUDA graph (the FP32 form with engines 0-2
+                              always does); SPB_FACTOR_AUTO (0, the default) is persistent for FP64
+                              and steps for the FP32 form */
 } spb_options;
 
-#define SPB_FACTOR_PERSISTENT 0
+#define SPB_FACTOR_AUTO 0
 #define SPB_FACTOR_STEPS 1
+#define SPB_FACTOR_PERSISTENT 2
 
 typedef struct spb_info {
   int32_t n;

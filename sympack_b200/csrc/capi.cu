@@ -2,12 +2,15 @@
 // include/sympack_b200.h).  A handle plays the role of one symPACKMatrix2D
 // object at one rank: it owns the symbolic analysis (host), the device plan,
 // the factor arena in HBM, and a CUDA graph replaying the factorization.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <exception>
+#include <memory>
 #include <atomic>
 #include <mutex>
 #include <thread>
@@ -59,6 +62,10 @@ struct spb_handle {
   spb::PanelItem* dpanel = nullptr;
   double* dwinv = nullptr;  // factored diagonal blocks (FP64) and 1/L_kk of one step
   spb::TileItem* dtiles = nullptr;
+  float* dsplit = nullptr;         // FP32 engine 3: split copies of the panels with 128 x 128 tiles
+  int64_t* dsplit_off = nullptr;   // offset of each supernode's copy (-1: none)
+  CUtensorMap* dtmaps = nullptr;   // their tiled tensor maps
+  int32_t* dtmap_of = nullptr;     // map of each supernode (-1: none)
   spb::FTask* dftasks = nullptr;   // persistent factorization: tasks, waits, signals, counters
   spb::FWait* dfwaits = nullptr;
   int32_t* dfsigs = nullptr;
@@ -110,6 +117,10 @@ struct spb_handle {
   unsigned long long* dtrace = nullptr;  // profiled solves: 4 per task of each sweep (forward, backward)
   spb_profile prof{};
   std::vector<cudaEvent_t> events;
+  // footprint predictions for the other precision: its plan, built on first use
+  mutable std::mutex pred_mu;
+  mutable std::unique_ptr<spb::Plan> pred_plan[2];
+  mutable spb::PlanParams pred_prm[2];
 };
 
 namespace {
@@ -161,15 +172,24 @@ void release_device(spb_handle* h) {
   h->dW = nullptr;
   h->dX = h->dZ = h->dB = h->dR = h->dD = h->dXo = nullptr;
   h->dInv = h->dInvB = nullptr;
+  h->dsplit = nullptr;
+  h->dsplit_off = nullptr;
+  h->dtmaps = nullptr;
+  h->dtmap_of = nullptr;
   h->dftrace = nullptr;
   h->d_rowseg = nullptr;
   h->dtrace = nullptr;
   h->x_cap = 0;
 }
 
-bool persistent_factor(const spb_handle* h) {
-  return h->opt.precision == SPB_PRECISION_FP64 && h->opt.factor_schedule == SPB_FACTOR_PERSISTENT;
+// The persistent factorization runs FP64 handles (unless the steps are asked for) and
+// FP32 handles that ask for it and whose 128 x 128 tiles use the TMA-fed tcgen05 engine
+// (the one with a task body for the persistent kernel).
+bool persistent_schedule(const spb_options& o) {
+  if (o.precision == SPB_PRECISION_FP64) return o.factor_schedule != SPB_FACTOR_STEPS;
+  return o.factor_schedule == SPB_FACTOR_PERSISTENT && o.fp32_engine == 3;
 }
+bool persistent_factor(const spb_handle* h) { return persistent_schedule(h->opt); }
 
 spb::dev::FactorArgs factor_args(spb_handle* h) {
   spb::dev::FactorArgs a;
@@ -183,6 +203,10 @@ spb::dev::FactorArgs factor_args(spb_handle* h) {
   a.rel = h->drel;
   a.fp32 = h->fp32;
   a.engine = h->opt.fp32_engine;
+  a.split = h->dsplit;
+  a.split_off = h->dsplit_off;
+  a.tmaps = h->dtmaps;
+  a.tmap_of = h->dtmap_of;
   a.ldl = h->ldl;
   a.W = h->dW;
   return a;
@@ -604,6 +628,8 @@ void spb_default_options(spb_options* o) {
   o->ir_max_iter = 30;
   o->verbose = 0;
   o->decomposition = SPB_DECOMPOSITION_LL;
+  o->fp32_engine = 3;
+  o->factor_schedule = SPB_FACTOR_AUTO;
 }
 
 int spb_create(const spb_options* opt, spb_handle** out) {
@@ -614,8 +640,9 @@ int spb_create(const spb_options* opt, spb_handle** out) {
   if (opt) h->opt = *opt;
   else spb_default_options(&h->opt);
   if (h->opt.ordering < 0 || h->opt.ordering > 4 || h->opt.precision < 0 || h->opt.precision > 1 ||
-      h->opt.fp32_engine < 0 || h->opt.fp32_engine > 2 || h->opt.decomposition < 0 || h->opt.decomposition > 1 ||
+      h->opt.fp32_engine < 0 || h->opt.fp32_engine > 3 || h->opt.decomposition < 0 || h->opt.decomposition > 1 ||
       h->opt.plan_outer_nb < 0 || h->opt.plan_outer_nb > 4096 || h->opt.plan_outer_nb % 64 ||
+      h->opt.factor_schedule < SPB_FACTOR_AUTO || h->opt.factor_schedule > SPB_FACTOR_PERSISTENT ||
       (h->opt.decomposition == SPB_DECOMPOSITION_LDL && h->opt.precision != SPB_PRECISION_FP64)) {
     delete h;
     return SPB_ERR_INVALID;
@@ -701,8 +728,92 @@ spb::PlanParams plan_params_of(const spb_options& o) {
   if (o.plan_outer_nb > 0) pp.outer_nb = o.plan_outer_nb;
   if (o.plan_solve_chunk > 0) pp.solve_sb = o.plan_solve_chunk;
   if (o.plan_solve_tiles > 0) pp.solve_tpt = o.plan_solve_tiles;
-  pp.factor_dag = o.precision == SPB_PRECISION_FP64 && o.factor_schedule == SPB_FACTOR_PERSISTENT;
+  pp.factor_dag = persistent_schedule(o);
+  pp.fp32 = o.precision == SPB_PRECISION_FP32_IR;
   return pp;
+}
+
+// Map index of every supernode that owns 128 x 128 tiles (-1 for the others); returns the count.
+int tile_map_index(const spb::Plan& P, std::vector<int32_t>& of) {
+  of.assign(P.nsuper, -1);
+  int n = 0;
+  for (const spb::Step& st : P.steps) {
+    if (st.kind != spb::StepKind::Gemm || st.tile != 128) continue;
+    for (int i = st.begin; i < st.begin + st.count; ++i) {
+      const int s = P.tile_items[i].s;
+      if (of[s] < 0) of[s] = n++;
+    }
+  }
+  return n;
+}
+
+// Floats of the split copies (hi and lo rows of every panel with 128 x 128 tiles), the
+// offset of each supernode's copy (-1: none) in `off`.
+int64_t split_layout(const spb::Plan& P, const std::vector<int32_t>& of, std::vector<int64_t>& off) {
+  off.assign(P.nsuper, -1);
+  int64_t t = 0;
+  for (int s = 0; s < P.nsuper; ++s) {
+    if (of[s] < 0) continue;
+    const spb::SnMeta& m = P.meta[s];
+    off[s] = t;
+    t += (2 * (int64_t)m.h * ((m.w + 3) & ~3) + 31) / 32 * 32;  // 128-byte aligned copies
+  }
+  return t;
+}
+
+// Split copies of the FP32 panels read by the TMA-fed tcgen05 tiles, and their 3-D tiled
+// tensor maps: columns inner (extent w, pitch round_up(w, 4)), rows (extent h), then
+// {hi, lo}; 32 x 128 x 2 boxes, 128-byte swizzle, zero outside the panel.  Checks the
+// tile shape that engine relies on (a K range of whole 32-column chunks, or one ending at
+// the panel's last column).
+int build_tile_maps(spb_handle* h) {
+  const spb::Plan& P = h->plan;
+  std::vector<int32_t> of;
+  const int nmaps = tile_map_index(P, of);
+  for (const spb::Step& st : P.steps) {
+    if (st.kind != spb::StepKind::Gemm || st.tile != 128) continue;
+    for (int i = st.begin; i < st.begin + st.count; ++i) {
+      const spb::TileItem& t = P.tile_items[i];
+      if (!(t.kn % 32 == 0 || t.k0 + t.kn == P.meta[t.s].w) || t.k0 % 4)
+        return fail(h, SPB_ERR_STRUCTURE, "plan: a 128 x 128 tile does not fit the TMA-fed engine");
+    }
+  }
+  static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+  if (!encode) {
+    cudaDriverEntryPointQueryResult q;
+    void* fn = nullptr;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &fn, 12000, cudaEnableDefault, &q) !=
+            cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !fn)
+      return fail(h, SPB_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+    encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  }
+  std::vector<int64_t> off;
+  const int64_t floats = split_layout(P, of, off);
+  SPB_CK(h, dalloc(h, &h->dsplit, (size_t)floats));
+  SPB_CK(h, dalloc(h, &h->dsplit_off, off.size()));
+  SPB_CK(h, dalloc(h, &h->dtmaps, (size_t)std::max(nmaps, 1)));
+  SPB_CK(h, dalloc(h, &h->dtmap_of, of.size()));
+  std::vector<CUtensorMap> maps(std::max(nmaps, 1));
+  for (int s = 0; s < P.nsuper; ++s) {
+    if (of[s] < 0) continue;
+    const spb::SnMeta& m = P.meta[s];
+    const cuuint64_t pitch = (cuuint64_t)((m.w + 3) & ~3);
+    cuuint64_t dims[3] = {(cuuint64_t)m.w, (cuuint64_t)m.h, 2};
+    cuuint64_t strides[2] = {pitch * sizeof(float), pitch * (cuuint64_t)m.h * sizeof(float)};
+    cuuint32_t box[3] = {32, 128, 2}, es[3] = {1, 1, 1};
+    const CUresult r = encode(&maps[of[s]], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, h->dsplit + off[s], dims, strides,
+                              box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(h, SPB_ERR_CUDA, "cuTensorMapEncodeTiled failed for a panel");
+  }
+  SPB_CK(h, cudaStreamSynchronize(h->own_stream));
+  SPB_CK(h, cudaMemcpyAsync(h->dtmaps, maps.data(), maps.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice,
+                            h->stream));
+  SPB_CK(h, cudaMemcpyAsync(h->dtmap_of, of.data(), of.size() * 4, cudaMemcpyHostToDevice, h->stream));
+  SPB_CK(h, cudaMemcpyAsync(h->dsplit_off, off.data(), off.size() * 8, cudaMemcpyHostToDevice, h->stream));
+  SPB_CK(h, cudaStreamSynchronize(h->stream));  // the host copies go out of scope
+  return SPB_OK;
 }
 
 int begin_symbolic(spb_handle* h, int32_t n, const int64_t* colptr, const int32_t* rowind) {
@@ -726,13 +837,28 @@ int begin_symbolic(spb_handle* h, int32_t n, const int64_t* colptr, const int32_
 int install_device(spb_handle* h);
 
 // Device bytes install_device + a solve of nrhs right-hand sides allocate
-// (the same list of buffers, sizes as requested from cudaMalloc).
+// (the same list of buffers, sizes as requested from cudaMalloc).  The plan depends on
+// the precision (tile shapes, task graph), so a prediction for the other precision plans
+// the analysis for it (once per handle and precision).
 int64_t predict_bytes(const spb_handle* h, bool fp32, int nrhs) {
-  const spb::Plan& P = h->plan;
+  spb_options o = h->opt;
+  o.precision = fp32 ? SPB_PRECISION_FP32_IR : SPB_PRECISION_FP64;
+  const spb::PlanParams want = plan_params_of(o);
+  const spb::Plan* plan = &h->plan;
+  if (!(want == plan_params_of(h->opt))) {
+    std::lock_guard<std::mutex> lock(h->pred_mu);
+    std::unique_ptr<spb::Plan>& c = h->pred_plan[fp32 ? 1 : 0];
+    if (!c || !(h->pred_prm[fp32 ? 1 : 0] == want)) {
+      c = std::make_unique<spb::Plan>(spb::build_plan(h->sym, want));
+      h->pred_prm[fp32 ? 1 : 0] = want;
+    }
+    plan = c.get();
+  }
+  const spb::Plan& P = *plan;
   const int64_t n = h->sym.n, ns = P.nsuper;
   auto b = [](int64_t count, size_t size) { return std::max<int64_t>(count, 1) * (int64_t)size; };
   int64_t t = b(P.arena_elems, fp32 ? sizeof(float) : sizeof(double));
-  if (h->opt.decomposition == SPB_DECOMPOSITION_LDL) t += b(P.arena_elems, sizeof(double));
+  if (o.decomposition == SPB_DECOMPOSITION_LDL) t += b(P.arena_elems, sizeof(double));
   t += b(P.meta.size(), sizeof(spb::SnMeta)) + b(P.rows.size(), 4) + b(P.supmember0.size(), 4);
   t += b(P.row_group.size(), 4) + b(P.groups.size(), sizeof(spb::RelGroup)) + b(P.rel.size(), 4);
   t += b(h->amap.size(), 8) + b(h->nnz_a, 8) + b(P.small_items.size(), 4);
@@ -744,7 +870,7 @@ int64_t predict_bytes(const spb_handle* h, bool fp32, int nrhs) {
   t += b(P.inv_elems, fp32 ? sizeof(float) : sizeof(double)) + b(P.inv_items.size(), sizeof(spb::InvItem));
   t += b(P.ftasks.size(), sizeof(spb::FTask)) + b(P.fwaits.size(), sizeof(spb::FWait)) + b(P.fsigs.size(), 4) +
        b(P.nfctr + 1, 4);
-  if (h->opt.decomposition == SPB_DECOMPOSITION_LDL) t += b(P.inv_elems, sizeof(double));
+  if (o.decomposition == SPB_DECOMPOSITION_LDL) t += b(P.inv_elems, sizeof(double));
   t += b(1, sizeof(Status));
   if (fp32) {
     int64_t offdiag = 0;
@@ -754,6 +880,12 @@ int64_t predict_bytes(const spb_handle* h, bool fp32, int nrhs) {
     t += b(n + 1, 8) + b(nnz_full, 4) + b(nnz_full, 8) + b(nnz_full, 8);
     t += b(1 + (int64_t)num_segments(h) * (1 + 3 * 64), 8);
     if (!h->seg_off.empty()) t += b(n, 4);
+  }
+  if (fp32 && o.fp32_engine == 3) {
+    std::vector<int32_t> of;
+    std::vector<int64_t> off;
+    const int nmaps = tile_map_index(P, of);
+    t += b(split_layout(P, of, off), sizeof(float)) + b(ns, 8) + b(nmaps, sizeof(CUtensorMap)) + b(ns, 4);
   }
   if (nrhs > 0) t += (fp32 ? 6 : 3) * b(n * nrhs, 8);
   return t;
@@ -774,6 +906,11 @@ int install_symbolic(spb_handle* h, int32_t n, const int64_t* colptr, const int3
 // Device buffers of an analysed handle (h->sym, h->plan, h->amap, h->colptr and
 // h->rowind set); a host-only handle just records that the analysis is done.
 int install_device(spb_handle* h) {
+  {  // a new analysis: earlier predictions' plans are stale
+    std::lock_guard<std::mutex> lock(h->pred_mu);
+    h->pred_plan[0].reset();
+    h->pred_plan[1].reset();
+  }
   if (h->device < 0) {
     h->have_symbolic = true;
     return SPB_OK;
@@ -864,6 +1001,10 @@ int install_device(spb_handle* h) {
   SPB_CK(h, up(h->dfwaits, P.fwaits.data(), P.fwaits.size() * sizeof(spb::FWait)));
   SPB_CK(h, up(h->dfsigs, P.fsigs.data(), P.fsigs.size() * 4));
   SPB_CK(h, cudaMemsetAsync(h->dstatus, 0, sizeof(Status), h->stream));
+  if (h->fp32 && h->opt.fp32_engine == 3) {
+    const int rc = build_tile_maps(h);
+    if (rc != SPB_OK) return rc;
+  }
   if (h->fp32) {
     // full symmetric CSR of A in the original ordering; csr_src maps each entry to its input value
     std::vector<int64_t>& rp = h->csr_rowptr;

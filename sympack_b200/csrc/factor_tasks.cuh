@@ -11,6 +11,7 @@
 // (lapack.hpp:206-560, no pivoting, a zero pivot is reported), unit TRSM then
 // scaling by 1/D (2D.hpp:2118-2137).
 #pragma once
+#include <type_traits>
 #include "kernels.cuh"
 
 namespace spb {
@@ -79,6 +80,21 @@ __device__ void panel_ldl_smem(double* P, int h, int w, int ldp, Status* status,
   }
 }
 
+// Split copy of final FP32 panel rows (TMA-fed tcgen05 tiles): tf32 hi part (round to
+// nearest, ties away) and the rounded remainder, row-major, hi block then lo block.
+__device__ __forceinline__ void split_store(const FactorArgs& a, const SnMeta& m, int64_t off, int r, int c, float x) {
+  uint32_t hi, lo;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(hi) : "f"(x));
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(lo) : "f"(x - __uint_as_float(hi)));
+  const int64_t pitch = (m.w + 3) & ~3;
+  float* p = a.split + off + (int64_t)r * pitch + c;
+  p[0] = __uint_as_float(hi);
+  p[(int64_t)m.h * pitch] = __uint_as_float(lo);
+}
+// The copy's writes come before the TMA loads (async proxy) of the tasks that wait for
+// this one's counters.
+__device__ __forceinline__ void split_fence() { asm volatile("fence.proxy.async.global;" ::: "memory"); }
+
 // Small panel s factored whole in shared memory P (h * w doubles).
 template <class T>
 __device__ void factor_small_task(const FactorArgs& a, int s, double* P) {
@@ -105,6 +121,16 @@ __device__ void factor_small_task(const FactorArgs& a, int s, double* P) {
   for (int idx = threadIdx.x; idx < h * w; idx += blockDim.x) {
     int c = idx / h, r = idx - c * h;
     g[r + (int64_t)c * m.ld] = (T)P[idx];
+  }
+  if constexpr (std::is_same<T, float>::value) {
+    const int64_t off = a.split ? a.split_off[s] : -1;
+    if (off >= 0) {  // off-diagonal rows, row by row (consecutive threads take consecutive columns)
+      for (int idx = threadIdx.x; idx < (h - w) * w; idx += blockDim.x) {
+        const int r = w + idx / w, c = idx % w;
+        split_store(a, m, off, r, c, (float)P[r + c * h]);
+      }
+      split_fence();
+    }
   }
 }
 
@@ -500,6 +526,17 @@ __device__ void trsm_rows_task(const FactorArgs& a, const PanelItem& it, const d
   for (int q = 0; q < kNB * kNB / kThreads; ++q) {
     const int idx = tid + q * kThreads, k = idx / kNB, r = idx - k * kNB;
     if (r < rows && k < nb) g[(it.row0 + r) + (int64_t)(c0 + k) * ld] = (T)R[r + k * kDL];
+  }
+  if constexpr (std::is_same<T, float>::value) {
+    const int64_t off = a.split ? a.split_off[it.s] : -1;
+    if (off >= 0) {  // the tile's rows, row by row (consecutive threads take consecutive columns)
+#pragma unroll
+      for (int q = 0; q < kNB * kNB / kThreads; ++q) {
+        const int idx = tid + q * kThreads, r = idx / kNB, k = idx - r * kNB;
+        if (r < rows && k < nb) split_store(a, m, off, it.row0 + r, c0 + k, (float)R[r + k * kDL]);
+      }
+      split_fence();
+    }
   }
 }
 

@@ -6,10 +6,14 @@
 //   then the src_to_tgt_offset / colindx scatter of 2D.hpp:1395-1466), fused so
 //   that C never leaves the SM.
 //
-// Two tile engines share one epilogue:
-//   k_gemm_dmma  128 x 128 tiles on the FP64 tensor pipe (mma.sync m16n8k4 .f64),
-//                3-stage cp.async pipeline, 8 warps of 64 x 32
-//   k_gemm_simt   64 x 64 tiles with FP64 FMA, for narrow updates
+// Tile engines (one shared epilogue for the tiles staged in shared memory):
+//   k_gemm_dmma   128 x 64 FP64 tiles on the FP64 tensor pipe (mma.sync m16n8k4 .f64),
+//                 3-stage cp.async pipeline, 8 warps of 32 x 32, two CTAs per SM
+//   k_gemm_simt   64 x 64 tiles with FMA, for narrow updates
+//   k_gemm_tc32   128 x 128 FP32 tiles, 3xTF32 on tcgen05, operands staged by cp.async
+//   k_gemm_tc32t  the same on TMA-fed MN-major operands (also a task of the persistent
+//                 FP32 factorization)
+//   k_gemm_tc32p, k_gemm_tf32x3   a persistent tcgen05 variant and an mma.sync one
 // The epilogue stages C in shared memory and walks it column by column, so
 // consecutive threads touch consecutive target rows (coalesced atomics).
 #include <climits>
@@ -105,12 +109,23 @@ __device__ void tile_epilogue(const FactorArgs& a, const TileItem& it, const SnM
 
 namespace {
 
-// ---- 128 x 128 FP64 tensor-core tile ------------------------------------------
-constexpr int kDM = 128, kDN = 128, kDK = 16, kDStages = 3, kDLds = 132, kDLdc = 130, kDThreads = 256;
-constexpr size_t kDPipeBytes = (size_t)kDStages * 2 * kDK * kDLds * sizeof(double);
-constexpr size_t kDCBytes = (size_t)kDN * kDLdc * sizeof(double);
-constexpr size_t kDMainBytes = kDPipeBytes > kDCBytes ? kDPipeBytes : kDCBytes;
-constexpr size_t kDSmemBytes = kDMainBytes + 4 * 128 * sizeof(int);
+// ---- 128 x BN FP64 tensor-core tile ------------------------------------------------
+// BN = 64: 8 warps of 32 x 32 (4 x 2), two CTAs per SM (128 registers a thread, 79 KB of
+// shared memory each), so that one CTA's prologue and atomic epilogue overlap the other's
+// MMAs; BN = 128: 8 warps of 64 x 32 (2 x 4), one CTA per SM.
+constexpr int kDM = 128, kDK = 16, kDStages = 3, kDLds = 132, kDLdc = 130, kDThreads = 256;
+constexpr int kDTileN = 64;  // FP64 update tiles are 128 x 64 (Plan: big_tile_cols)
+template <int BN>
+struct DTile {
+  static constexpr int kLdb = BN + 4;
+  static constexpr int kWarpsN = BN / 32, kWarpsM = 8 / kWarpsN;
+  static constexpr int kMI = kDM / kWarpsM / 16;  // 16-row MMA tiles per warp
+  static constexpr size_t kPipeBytes = (size_t)kDStages * kDK * (kDLds + kLdb) * sizeof(double);
+  static constexpr size_t kCBytes = (size_t)BN * kDLdc * sizeof(double);
+  static constexpr size_t kMainBytes = kPipeBytes > kCBytes ? kPipeBytes : kCBytes;
+  static constexpr size_t kSmemBytes = kMainBytes + 4 * 128 * sizeof(int);
+};
+constexpr size_t kDSmemBytes = DTile<kDTileN>::kSmemBytes;
 
 __device__ __forceinline__ void cp_async8(void* smem, const void* gmem, int src_bytes) {
   unsigned s = (unsigned)__cvta_generic_to_shared(smem);
@@ -120,17 +135,6 @@ __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_grou
 template <int N>
 __device__ __forceinline__ void cp_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
-}
-
-// D = A(16x16, row) * B(16x8, col) + D, FP64; lane = 4*g + t:
-//   a[2j] = A[g][t+4j], a[2j+1] = A[g+8][t+4j], b[j] = B[t+4j][g] (j < 4), d as for m16n8k4.
-__device__ __forceinline__ void dmma_16x8x16(double* d, const double* a, const double* b) {
-  asm volatile(
-      "mma.sync.aligned.m16n8k16.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7,%8,%9,%10,%11}, "
-      "{%12,%13,%14,%15}, {%0,%1,%2,%3};\n"
-      : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
-      : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(a[4]), "d"(a[5]), "d"(a[6]), "d"(a[7]), "d"(b[0]),
-        "d"(b[1]), "d"(b[2]), "d"(b[3]));
 }
 
 // D = A(16x4, row) * B(4x8, col) + D, FP64.  Fragment ownership (lane = 4*g + t):
@@ -143,21 +147,24 @@ __device__ __forceinline__ void dmma_16x8x4(double* d, double a0, double a1, dou
       : "d"(a0), "d"(a1), "d"(b0));
 }
 
-// One 128 x 128 DMMA tile (kDThreads threads, kDSmemBytes of shared memory).
+// One 128 x BN DMMA tile (kDThreads threads, DTile<BN>::kSmemBytes of shared memory).
+template <int BN>
 __device__ void dmma_tile_task(const FactorArgs& a, const TileItem& it, unsigned char* smem_raw) {
+  using D = DTile<BN>;
   double* pipe = reinterpret_cast<double*>(smem_raw);
   double* Cs = reinterpret_cast<double*>(smem_raw);  // reused once the main loop is done
-  int* ints = reinterpret_cast<int*>(smem_raw + kDMainBytes);
+  int* ints = reinterpret_cast<int*>(smem_raw + D::kMainBytes);
   const SnMeta m = a.meta[it.s];
   const double* g = static_cast<const double*>(a.L) + m.off;
   const double* gb = a.ldl ? a.W + m.off : g;  // second operand: L, or L D for LDL^T
   const int64_t ld = m.ld;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int wm = warp & 1, wn = warp >> 1;  // 2 x 4 warps, 64 x 32 each
+  const int wm = warp % D::kWarpsM, wn = warp / D::kWarpsM;
   const int gq = lane >> 2, tq = lane & 3;
+  constexpr int kStageElems = kDK * (kDLds + D::kLdb);
 
   auto load_stage = [&](int stage, int kk) {
-    double* As = pipe + (size_t)stage * 2 * kDK * kDLds;
+    double* As = pipe + (size_t)stage * kStageElems;
     double* Bs = As + kDK * kDLds;
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
@@ -167,15 +174,23 @@ __device__ void dmma_tile_task(const FactorArgs& a, const TileItem& it, unsigned
       bool kok = k < it.kn;
       int64_t coff = (int64_t)(it.k0 + (kok ? k : 0)) * ld;
       bool aok = kok && r < it.mrows;
-      bool bok = kok && r < it.ncols;
       cp_async8(As + col * kDLds + r, aok ? g + it.a_row0 + r + coff : g, aok ? 8 : 0);
-      cp_async8(Bs + col * kDLds + r, bok ? gb + it.b_row0 + r + coff : gb, bok ? 8 : 0);
+    }
+#pragma unroll
+    for (int q = 0; q < 16 * BN / kDThreads; ++q) {
+      int e = tid + q * kDThreads;  // (column, row) of a 16 x BN operand slab
+      int col = e / BN, r = e % BN;
+      int k = kk + col;
+      bool kok = k < it.kn;
+      int64_t coff = (int64_t)(it.k0 + (kok ? k : 0)) * ld;
+      bool bok = kok && r < it.ncols;
+      cp_async8(Bs + col * D::kLdb + r, bok ? gb + it.b_row0 + r + coff : gb, bok ? 8 : 0);
     }
   };
 
-  double acc[4][4][4];
+  double acc[D::kMI][4][4];
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
+  for (int i = 0; i < D::kMI; ++i)
 #pragma unroll
     for (int j = 0; j < 4; ++j)
 #pragma unroll
@@ -193,46 +208,43 @@ __device__ void dmma_tile_task(const FactorArgs& a, const TileItem& it, unsigned
     const int nxt = kt + kDStages - 1;
     if (nxt < nk) load_stage(nxt % kDStages, nxt * kDK);
     cp_commit();
-    const double* As = pipe + (size_t)(kt % kDStages) * 2 * kDK * kDLds;
+    const double* As = pipe + (size_t)(kt % kDStages) * kStageElems;
     const double* Bs = As + kDK * kDLds;
-    // one m16n8k16 step per stage: the B fragments of the warp's four column tiles,
+    // four m16n8k4 steps per stage: the B fragments of the warp's four column tiles,
     // then per row tile its A fragment and four MMAs
-    double bf[4][4];
 #pragma unroll
-    for (int ni = 0; ni < 4; ++ni)
+    for (int kk = 0; kk < kDK; kk += 4) {
+      double bf[4];
 #pragma unroll
-      for (int j = 0; j < 4; ++j) bf[ni][j] = Bs[(tq + 4 * j) * kDLds + wn * 32 + ni * 8 + gq];
+      for (int ni = 0; ni < 4; ++ni) bf[ni] = Bs[(kk + tq) * D::kLdb + wn * 32 + ni * 8 + gq];
 #pragma unroll
-    for (int mi = 0; mi < 4; ++mi) {
-      double af[8];
+      for (int mi = 0; mi < D::kMI; ++mi) {
+        const int r0 = wm * (16 * D::kMI) + mi * 16 + gq;
+        const double a0 = As[(kk + tq) * kDLds + r0], a1 = As[(kk + tq) * kDLds + r0 + 8];
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        af[2 * j] = As[(tq + 4 * j) * kDLds + wm * 64 + mi * 16 + gq];
-        af[2 * j + 1] = As[(tq + 4 * j) * kDLds + wm * 64 + mi * 16 + gq + 8];
+        for (int ni = 0; ni < 4; ++ni) dmma_16x8x4(acc[mi][ni], a0, a1, bf[ni]);
       }
-#pragma unroll
-      for (int ni = 0; ni < 4; ++ni) dmma_16x8x16(acc[mi][ni], af, bf[ni]);
     }
   }
   cp_wait<0>();
   __syncthreads();
 #pragma unroll
-  for (int mi = 0; mi < 4; ++mi)
+  for (int mi = 0; mi < D::kMI; ++mi)
 #pragma unroll
     for (int ni = 0; ni < 4; ++ni) {
-      int r0 = wm * 64 + mi * 16 + gq, c0 = wn * 32 + ni * 8 + 2 * tq;
+      int r0 = wm * (16 * D::kMI) + mi * 16 + gq, c0 = wn * 32 + ni * 8 + 2 * tq;
       Cs[r0 + c0 * kDLdc] = acc[mi][ni][0];
       Cs[r0 + (c0 + 1) * kDLdc] = acc[mi][ni][1];
       Cs[r0 + 8 + c0 * kDLdc] = acc[mi][ni][2];
       Cs[r0 + 8 + (c0 + 1) * kDLdc] = acc[mi][ni][3];
     }
   __syncthreads();
-  tile_epilogue<kDM, kDN, kDThreads, double, double>(a, it, m, Cs, kDLdc, (int64_t*)ints, (int64_t*)ints + 128);
+  tile_epilogue<kDM, BN, kDThreads, double, double>(a, it, m, Cs, kDLdc, (int64_t*)ints, (int64_t*)ints + 128);
 }
 
-__global__ void __launch_bounds__(kDThreads, 1) k_gemm_dmma(FactorArgs a, const TileItem* __restrict__ items) {
+__global__ void __launch_bounds__(kDThreads, 2) k_gemm_dmma(FactorArgs a, const TileItem* __restrict__ items) {
   extern __shared__ __align__(16) unsigned char smem_dmma[];
-  dmma_tile_task(a, items[blockIdx.x], smem_dmma);
+  dmma_tile_task<kDTileN>(a, items[blockIdx.x], smem_dmma);
 }
 
 // ---- 64 x 64 FP64 FMA tile --------------------------------------------------------
@@ -700,6 +712,265 @@ __global__ void __launch_bounds__(256, 1) k_gemm_tc32(FactorArgs a, const TileIt
   if (it.mode == 0) tile_epilogue<kUM, kUN, 256, float, float>(a, it, m, Cs, kULdc, cbase, crel);
 }
 
+// ---- 128 x 128 3xTF32 tile with TMA-fed operands -------------------------------------
+// The FP32 panels of supernodes with these tiles have a split copy: once a row of a
+// panel is final (TRSM tile, or small panel), its tf32 hi part (cvt.rna) and lo part
+// (the rounded remainder) are written row-major, hi block then lo block (row pitch
+// round_up(w, 4)).  A 3-D tiled tensor map per panel (columns inner, rows, hi / lo; 128-byte
+// swizzle, zero outside the panel) lets one TMA load bring a 128-row x 32-column chunk of
+// both parts straight into the K-major 128-byte-swizzled layout the MMAs read (8-row atoms
+// of 1 KB; hi at +0, lo at +16 KB), so a tile is TMA -> tcgen05 -> TMEM with no thread
+// touching its operands.  Thread 0 issues the loads and the chunk's 12 MMAs (4 K steps x
+// {lo*hi, hi*lo, hi*hi}, the order of k_gemm_tc32) and commits them to the stage's mbarrier;
+// it refills a stage once the MMAs that read it are done.  Three stages of 64 KB (A hi,
+// A lo, B hi, B lo); a tile whose two operands are the same rows loads one.  Accumulator row
+// i is panel row a_row0 + i and column j panel row b_row0 + j.
+constexpr int kVStages = 3;
+constexpr int kVOpBytes = 128 * 32 * 4;              // one operand part: 16 KB
+constexpr int kVStageBytes = 4 * kVOpBytes;          // A hi, A lo, B hi, B lo
+constexpr size_t kVMainBytes = (size_t)kVStages * kVStageBytes;
+constexpr size_t kVSmemBytes = 1024 + kVMainBytes + 2 * kVStages * sizeof(uint64_t) + 16;
+static_assert(kUCBytes + 2 * 128 * sizeof(int64_t) <= kVMainBytes, "C staging and column maps fit the stages");
+static_assert(kVSmemBytes <= 232448, "shared memory of the TMA-fed tcgen05 tile");
+
+// 32 columns x 128 rows x {hi, lo} of a panel's split copy (tensor map, coordinates
+// column, row, part) into dst, completing on bar.
+__device__ __forceinline__ void tma_load_3d(uint32_t dst, const void* map, int x, int y, uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];\n" ::"r"(dst),
+      "l"(map), "r"(x), "r"(y), "r"(0), "r"(bar)
+      : "memory");
+}
+
+// Per-CTA state of the TMA-fed tile: stage buffers (1 KB aligned), the per-stage
+// mbarriers and the tensor-memory accumulator, kept across the tiles a persistent CTA
+// runs; g counts the chunks this CTA has run, so chunk q of its life uses stage q % 3
+// and waits for phase (q / 3) & 1 of that stage's barriers.
+struct TcTile {
+  unsigned char* base;
+  uint32_t base_addr;
+  uint64_t* full;  // chunk landed (TMA transaction bytes)
+  uint64_t* done;  // chunk's MMAs finished (tcgen05.commit)
+  uint32_t tmem;
+  uint32_t g;
+};
+
+// All threads: barriers, 128 tensor-memory columns (kVSmemBytes of dynamic shared memory).
+__device__ __forceinline__ void tc_setup(TcTile& S, unsigned char* smem_raw) {
+  const uint32_t raw_addr = (uint32_t)__cvta_generic_to_shared(smem_raw);
+  const uint32_t pad = ((raw_addr + 1023u) & ~1023u) - raw_addr;  // swizzle atoms need 1 KB alignment
+  S.base = smem_raw + pad;
+  S.base_addr = raw_addr + pad;
+  S.full = reinterpret_cast<uint64_t*>(S.base + kVMainBytes);
+  S.done = S.full + kVStages;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(S.done + kVStages);
+  S.g = 0;
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < 2 * kVStages; ++i) {
+      const uint32_t b = (uint32_t)__cvta_generic_to_shared(S.full + i);
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(b) : "memory");
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  if ((threadIdx.x >> 5) == 0) {
+    const uint32_t slot = (uint32_t)__cvta_generic_to_shared(tmem_slot);
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(slot),
+                 "r"(kUTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  S.tmem = *tmem_slot;
+}
+
+__device__ __forceinline__ void tc_teardown(const TcTile& S) {
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  if ((threadIdx.x >> 5) == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(S.tmem), "r"(kUTmemCols)
+                 : "memory");
+  }
+}
+
+// One TMA-fed tile (all 256 threads).  Returns false, after recording status 3, when a
+// barrier wait gave up; the CTA's copies and MMAs in flight have then been waited for
+// (bounded).  The stages' shared memory may hold anything written by earlier work.
+__device__ bool tc32t_tile_task(const FactorArgs& a, const TileItem& it, TcTile& S) {
+  __shared__ int sh_abort, sh_last;
+  unsigned char* base = S.base;
+  const uint32_t base_addr = S.base_addr;
+  float* Cs = reinterpret_cast<float*>(base);  // mode 0 staging, once every MMA has completed
+  int64_t* cbase = reinterpret_cast<int64_t*>(base + kUCBytes);
+  int64_t* crel = cbase + 128;
+  const SnMeta m = a.meta[it.s];
+  const void* map = static_cast<const unsigned char*>(a.tmaps) + 128 * (size_t)a.tmap_of[it.s];
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const bool same = it.a_row0 == it.b_row0;  // both operands are the same panel rows
+  const int nops = same ? 1 : 2;
+  const int nk = (it.kn + 31) / 32;
+  const uint32_t g0 = S.g;
+
+  // earlier generic-proxy accesses of the stages come before this tile's TMA writes
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+  if (tid == 0) sh_abort = 0;
+  __syncthreads();
+
+  if (tid == 0) {
+    // the split copy was written by other CTAs (generic proxy) before the counters
+    // this task waited for were released
+    asm volatile("fence.proxy.async.global;\n" ::: "memory");
+    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;\n" ::"l"(map) : "memory");
+    // chunk kt into stage (g0 + kt) % kVStages: one box of 32 columns x 128 rows x {hi, lo} per operand
+    auto issue = [&](int kt) {
+      const int st = (g0 + kt) % kVStages;
+      const uint32_t sa = base_addr + st * kVStageBytes;
+      const uint32_t bar = (uint32_t)__cvta_generic_to_shared(S.full + st);
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(nops * 2 * kVOpBytes)
+                   : "memory");
+      const int x = it.k0 + kt * 32;
+      tma_load_3d(sa, map, x, it.a_row0, bar);
+      if (!same) tma_load_3d(sa + 2 * kVOpBytes, map, x, it.b_row0, bar);
+    };
+    int issued = 0;
+    for (; issued < nk && issued < kVStages; ++issued) issue(issued);
+    int committed = -1;
+    for (int kt = 0; kt < nk; ++kt) {
+      const uint32_t q = g0 + kt;
+      const int st = q % kVStages;
+      if (!mbar_wait((uint32_t)__cvta_generic_to_shared(S.full + st), (q / kVStages) & 1, kUWaitLimit)) {
+        sh_abort = 1;
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+      const uint32_t sa = base_addr + st * kVStageBytes;
+      const uint32_t sbb = same ? sa : sa + 2 * kVOpBytes;
+#pragma unroll
+      for (int ks = 0; ks < 4; ++ks) {  // K step of 8 columns = 32 bytes of each 128-byte line
+        const uint64_t ahi = umma_desc(sa + ks * 32), alo = umma_desc(sa + kVOpBytes + ks * 32);
+        const uint64_t bhi = umma_desc(sbb + ks * 32), blo = umma_desc(sbb + kVOpBytes + ks * 32);
+        const uint64_t pa[3] = {alo, ahi, ahi}, pb[3] = {bhi, blo, bhi};
+#pragma unroll
+        for (int p = 0; p < 3; ++p) {
+          const uint32_t acc = (kt > 0 || ks > 0 || p > 0) ? 1u : 0u;
+          asm volatile(
+              "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+              " tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n}\n" ::"r"(S.tmem),
+              "l"(pa[p]), "l"(pb[p]), "r"(kUIdesc), "r"(acc)
+              : "memory");
+        }
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                       (uint32_t)__cvta_generic_to_shared(S.done + st))
+                   : "memory");
+      committed = kt;
+      // refill the stage of the previous chunk once its MMAs are done (this chunk's queue behind them)
+      const int pk = kt - 1;
+      if (pk >= 0 && issued < nk) {
+        const uint32_t pq = g0 + pk;
+        if (!mbar_wait((uint32_t)__cvta_generic_to_shared(S.done + pq % kVStages), (pq / kVStages) & 1,
+                       kUWaitLimit)) {
+          sh_abort = 1;
+          break;
+        }
+        issue(issued++);
+      }
+    }
+    if (sh_abort) {  // let this CTA's copies in flight land before the stages are reused (bounded)
+      for (int kt = committed + 1; kt < issued; ++kt) {
+        const uint32_t q = g0 + kt;
+        mbar_wait((uint32_t)__cvta_generic_to_shared(S.full + q % kVStages), (q / kVStages) & 1, kUWaitLimit);
+      }
+    }
+    sh_last = committed;
+  }
+  __syncthreads();
+  const int committed = sh_last;
+  bool ok = !sh_abort;
+  if (committed >= 0) {  // every thread: the last commit covers every earlier MMA
+    const uint32_t q = g0 + committed;
+    if (!mbar_wait((uint32_t)__cvta_generic_to_shared(S.done + q % kVStages), (q / kVStages) & 1, kUWaitLimit))
+      ok = false;
+  }
+  S.g = g0 + nk;  // every chunk's barrier phases were consumed (the loop ran to nk unless aborted)
+  ok = __syncthreads_and(ok) != 0;  // one decision for the whole CTA (tcgen05.ld is warp-collective)
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  if (ok) {
+    const int quarter = warp & 3, half = warp >> 2;
+    const int row = quarter * 32 + (tid & 31);
+    if (it.mode == 1) {
+      if (tid < it.ncols) {
+        const int jc = it.b_row0 + tid;
+        const RelGroup gr = a.groups[a.row_group[m.lidx + jc]];
+        const SnMeta mt = a.meta[gr.t];
+        cbase[tid] = mt.off + (int64_t)(a.rows[m.lidx + jc] - mt.fc) * mt.ld;
+        crel[tid] = gr.rel_off - gr.j0;
+      }
+      __syncthreads();
+    }
+    float* L = static_cast<float*>(a.L);
+    const int jr = it.a_row0 + row;
+    int64_t last = INT64_MIN;
+    int pos = 0;
+#pragma unroll
+    for (int part = 0; part < 2; ++part) {
+      const int c0 = half * 64 + part * 32;
+      uint32_t v[32];
+      const uint32_t taddr = S.tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)c0;
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+          "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
+          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+            "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+            "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]),
+            "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]),
+            "=r"(v[30]), "=r"(v[31])
+          : "r"(taddr));
+      asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+      if (it.mode == 1) {
+        if (row < it.mrows) {
+#pragma unroll
+          for (int j = 0; j < 32; ++j) {
+            const int c = c0 + j;
+            if (c < it.ncols && jr >= it.b_row0 + c) {
+              const int64_t cr = crel[c];
+              if (cr != last) {
+                pos = a.rel[cr + jr];
+                last = cr;
+              }
+              atomicAdd(L + cbase[c] + pos, -__uint_as_float(v[j]));
+            }
+          }
+        }
+      } else {
+#pragma unroll
+        for (int j = 0; j < 32; ++j) Cs[row + (c0 + j) * kULdc] = __uint_as_float(v[j]);
+      }
+    }
+  }
+  // the accumulator has been read before the next tile's MMAs overwrite it
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  if (!ok) {
+    if (tid == 0) report_status(a.status, 3, it.s, -1);
+    return false;
+  }
+  if (it.mode == 0) tile_epilogue<kUM, kUN, 256, float, float>(a, it, m, Cs, kULdc, cbase, crel);
+  return true;
+}
+
+__global__ void __launch_bounds__(256, 1) k_gemm_tc32t(FactorArgs a, const TileItem* __restrict__ items) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  TcTile S;
+  tc_setup(S, smem_raw);
+  tc32t_tile_task(a, items[blockIdx.x], S);
+  tc_teardown(S);
+}
+
 // ---- persistent, warp-specialised variant of the tcgen05 tile ---------------------
 // One CTA per SM loops over the launch's tiles.  Warps 0-7 stage operands and (one
 // thread) issue the MMAs exactly as k_gemm_tc32 does; warps 8-11 are the epilogue:
@@ -937,6 +1208,7 @@ __global__ void __launch_bounds__(kPThreads, 1) k_gemm_tc32p(FactorArgs a, const
 }  // namespace
 
 static int g_sms = 148;  // persistent tile grid: one CTA per SM
+static int g_fper64 = 1, g_fper32 = 1;  // resident CTAs per SM of the persistent factorization
 
 // ---- persistent factorization ------------------------------------------------------
 // One CTA per SM takes the tasks of Plan::ftasks in order from an atomic counter,
@@ -966,11 +1238,21 @@ __device__ __forceinline__ unsigned smid() {
   return r;
 }
 
-constexpr size_t kFSmemBytes = kDSmemBytes;  // the largest task body (the DMMA tile)
+// The largest task body: the DMMA tile (FP64), the TMA-fed tcgen05 tile (FP32), whose
+// stages and barriers sit above every other body's shared memory (at most 96 KB).
+constexpr size_t kFSmemBytes = kDSmemBytes > 96 * 1024 ? kDSmemBytes : 96 * 1024;  // small panels: 96 KB
+constexpr size_t kFSmemBytes32 = kVSmemBytes;
+static_assert(kFSmemBytes32 >= 96 * 1024 + 1024, "FP32 persistent shared memory");
 
-__global__ void __launch_bounds__(256, 1) k_factor_persistent(FactorArgs a, FactorSched f) {
+// FP64: two CTAs per SM (128 x 64 DMMA tiles); FP32: one (the TMA-fed tile's 193 KB).
+template <class T>
+__global__ void __launch_bounds__(256, std::is_same<T, float>::value ? 1 : 2)
+    k_factor_persistent(FactorArgs a, FactorSched f) {
+  constexpr bool kF32 = std::is_same<T, float>::value;
   extern __shared__ __align__(16) unsigned char smem_f[];
   __shared__ int sh_task, sh_go;
+  TcTile tc;
+  if constexpr (kF32) tc_setup(tc, smem_f);  // tensor memory and stage barriers for the whole launch
   for (;;) {
     if (threadIdx.x == 0) {
       int tk = atomicAdd(f.counter, 1);
@@ -1006,38 +1288,44 @@ __global__ void __launch_bounds__(256, 1) k_factor_persistent(FactorArgs a, Fact
     }
     __syncthreads();
     const int tk = sh_task;
-    if (!sh_go) return;
+    if (!sh_go) break;
     const FTask t = f.tasks[tk];
     switch (t.kind) {
       case 0:
-        ftask::factor_small_task<double>(a, f.small_items[t.item], reinterpret_cast<double*>(smem_f));
+        ftask::factor_small_task<T>(a, f.small_items[t.item], reinterpret_cast<double*>(smem_f));
         break;
       case 1:
-        if (a.ldl) ftask::ldl_diag_task<double>(a, f.panel[t.item], f.winv, reinterpret_cast<double*>(smem_f));
-        else ftask::potrf_diag_task<double>(a, f.panel[t.item], f.winv, reinterpret_cast<double*>(smem_f));
+        if (!kF32 && a.ldl) ftask::ldl_diag_task<T>(a, f.panel[t.item], f.winv, reinterpret_cast<double*>(smem_f));
+        else ftask::potrf_diag_task<T>(a, f.panel[t.item], f.winv, reinterpret_cast<double*>(smem_f));
         break;
       case 2:
-        ftask::trsm_rows_task<double>(a, f.panel[t.item], f.winv, reinterpret_cast<double*>(smem_f));
+        ftask::trsm_rows_task<T>(a, f.panel[t.item], f.winv, reinterpret_cast<double*>(smem_f));
         break;
       case 3:
-        simt_tile_task<double>(a, f.tiles[t.item], smem_f);
+        simt_tile_task<T>(a, f.tiles[t.item], smem_f);
         break;
       default:
-        dmma_tile_task(a, f.tiles[t.item], smem_f);
+        if constexpr (kF32) tc32t_tile_task(a, f.tiles[t.item], tc);  // a failure records status 3
+        else dmma_tile_task<kDTileN>(a, f.tiles[t.item], smem_f);
         break;
     }
     __syncthreads();
     if (f.trace && threadIdx.x == 0) f.trace[4 * (size_t)tk + 2] = global_ns();
     for (int i = threadIdx.x; i < t.nsig; i += blockDim.x) red_release_i(f.ctr + f.sigs[t.sig0 + i], 1);
   }
+  if constexpr (kF32) tc_teardown(tc);
 }
 
 }  // namespace
 
 void launch_factor_persistent(cudaStream_t st, const FactorArgs& a, const FactorSched& f) {
   if (f.ntasks <= 0 || f.spin_limit <= 0) return;
-  const int grid = g_sms < f.ntasks ? g_sms : f.ntasks;
-  k_factor_persistent<<<grid, 256, kFSmemBytes, st>>>(a, f);
+  // as many CTAs as fit at once (a CTA only waits for tasks handed out before its own,
+  // so the grid size is a matter of speed, not of progress)
+  const int fit = (a.fp32 ? g_fper32 : g_fper64) * g_sms;
+  const int grid = fit < f.ntasks ? fit : f.ntasks;
+  if (a.fp32) k_factor_persistent<float><<<grid, 256, kFSmemBytes32, st>>>(a, f);
+  else k_factor_persistent<double><<<grid, 256, kFSmemBytes, st>>>(a, f);
 }
 
 void init_gemm_attributes() {
@@ -1046,9 +1334,21 @@ void init_gemm_attributes() {
   if (g_sms <= 0) g_sms = 148;
   cudaFuncSetAttribute(k_gemm_tf32x3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTSmemBytes);
   cudaFuncSetAttribute(k_gemm_tc32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kUSmemBytes);
+  cudaFuncSetAttribute(k_gemm_tc32t, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kVSmemBytes);
   cudaFuncSetAttribute(k_gemm_tc32p, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPSmemBytes);
   cudaFuncSetAttribute(k_gemm_dmma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDSmemBytes);
-  cudaFuncSetAttribute(k_factor_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFSmemBytes);
+  cudaFuncSetAttribute(k_factor_persistent<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFSmemBytes);
+  cudaFuncSetAttribute(k_factor_persistent<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFSmemBytes32);
+  int nb = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_factor_persistent<double>, 256, kFSmemBytes) ==
+          cudaSuccess &&
+      nb > 0)
+    g_fper64 = nb;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_factor_persistent<float>, 256, kFSmemBytes32) ==
+          cudaSuccess &&
+      nb > 0)
+    g_fper32 = nb;
+  cudaGetLastError();
 }
 
 void launch_gemm(cudaStream_t st, const FactorArgs& a, const TileItem* items, int count, int tile) {
@@ -1057,6 +1357,7 @@ void launch_gemm(cudaStream_t st, const FactorArgs& a, const TileItem* items, in
     if (tile == 128 && a.engine == 2)
       k_gemm_tc32p<<<count < g_sms ? count : g_sms, kPThreads, kPSmemBytes, st>>>(a, items, count);
     else if (tile == 128 && a.engine == 0) k_gemm_tc32<<<count, 256, kUSmemBytes, st>>>(a, items);
+    else if (tile == 128 && a.engine == 3) k_gemm_tc32t<<<count, 256, kVSmemBytes, st>>>(a, items);
     else if (tile == 128) k_gemm_tf32x3<<<count, 256, kTSmemBytes, st>>>(a, items);
     else k_gemm_simt<float><<<count, 256, kSSmemBytes, st>>>(a, items);
   } else {

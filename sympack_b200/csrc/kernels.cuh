@@ -27,7 +27,16 @@ struct FactorArgs {
   const RelGroup* groups;
   const int32_t* rel;        // positions of update rows in their targets' row lists
   bool fp32;                 // FP32 factor storage (precision form)
-  int engine;                // FP32 128 x 128 tiles: 0 tcgen05 per tile, 1 mma.sync, 2 persistent tcgen05
+  int engine;                // FP32 128 x 128 tiles: 0 tcgen05 per tile, 1 mma.sync, 2 persistent tcgen05,
+                             // 3 tcgen05 fed by TMA
+  // engine 3: split copies of the FP32 panels that have 128 x 128 tiles (per supernode
+  // its offset in floats, -1 for none: hi rows then lo rows, row pitch round_up(w, 4)),
+  // written by the tasks that finish panel rows, and their tiled tensor maps
+  // (CUtensorMap, 128 B each, 64-byte aligned; map index per supernode)
+  float* split = nullptr;
+  const int64_t* split_off = nullptr;
+  const void* tmaps = nullptr;
+  const int32_t* tmap_of = nullptr;
   // LDL^T (FP64 only): L holds the unit factor (1 on the diagonal) and the working
   // matrix of unfactored columns; W (same layout) holds L D, so that its diagonal
   // is D.  Updates are C = L_a (L_b D)^T: the second operand is read from W.

@@ -9,7 +9,7 @@ namespace spb {
 
 static int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
 
-static void build_factor_dag(Plan& P);
+static void build_factor_dag(Plan& P, const PlanParams& prm);
 
 Plan build_plan(const Symbolic& sym, const PlanParams& prm) {
   Plan P;
@@ -69,7 +69,8 @@ Plan build_plan(const Symbolic& sym, const PlanParams& prm) {
   // tiles entirely above the diagonal of a symmetric product are skipped.
   auto push_tiles = [&](std::vector<TileItem>& out, int T, int s, int mode, int rbeg, int rend, int cbeg, int cend,
                         int k0, int kn) {
-    for (int cj = cbeg; cj < cend; cj += T)
+    const int TN = T == 128 && !prm.fp32 ? 64 : T;  // FP64 tensor-core tiles are 128 x 64
+    for (int cj = cbeg; cj < cend; cj += TN)
       for (int ri = rbeg; ri < rend; ri += T) {
         if (ri + T <= cj) continue;  // rows and columns are both panel rows: tile above the diagonal
         TileItem t;
@@ -80,7 +81,7 @@ Plan build_plan(const Symbolic& sym, const PlanParams& prm) {
         t.k0 = k0;
         t.kn = kn;
         t.mrows = std::min(T, rend - ri);
-        t.ncols = std::min(T, cend - cj);
+        t.ncols = std::min(TN, cend - cj);
         out.push_back(t);
       }
   };
@@ -116,7 +117,7 @@ Plan build_plan(const Symbolic& sym, const PlanParams& prm) {
     for (int pass = 0; pass < 2; ++pass) {
       std::vector<TileItem>& v = pass ? t128 : t64;
       if (v.empty()) continue;
-      split_k(v, pass ? 1 : 4);
+      split_k(v, pass ? (prm.fp32 ? 1 : 2) : 4);  // CTAs per SM of the tile engines
       Step gs{StepKind::Gemm, (int32_t)P.tile_items.size(), (int32_t)v.size(), 0, pass ? 128 : 64, lane, blk};
       P.tile_items.insert(P.tile_items.end(), v.begin(), v.end());
       P.steps.push_back(gs);
@@ -268,7 +269,7 @@ Plan build_plan(const Symbolic& sym, const PlanParams& prm) {
     P.step_flops[k] = f;
   }
   for (const SnMeta& m : P.meta) P.solve_sweep_bytes += 8.0 * m.h * m.w;
-  if (prm.factor_dag) build_factor_dag(P);
+  if (prm.factor_dag) build_factor_dag(P, prm);
 
   // Solve super-blocks: per supernode, its first super-block counter and (for
   // supernodes wider than one block) the offset of its inverse tiles.
@@ -401,7 +402,7 @@ std::vector<int64_t> build_assembly_map(const Symbolic& sym, const Plan& P, cons
 // block granularity).  The dispatch order comes from a list-scheduling simulation on
 // the SMs with estimated task times, highest bottom level first, and is topological:
 // a CTA only ever waits for tasks handed out before its own.
-static void build_factor_dag(Plan& P) {
+static void build_factor_dag(Plan& P, const PlanParams& prm) {
   const int ns = P.nsuper, nb = P.nblk_total;
   const int EXT = 0, SDONE = ns, BLK = 2 * ns, COL = 2 * ns + nb;
   P.nfctr = 2 * ns + 2 * nb;
@@ -441,7 +442,8 @@ static void build_factor_dag(Plan& P) {
         r.kind = st.tile == 128 ? 4 : 3;
         r.s = t.s;
         const double fl = 2.0 * t.mrows * t.ncols * t.kn;
-        r.us = st.tile == 128 ? 3.0 + fl / 130e3 : 2.0 + fl / 30e3;
+        // per-CTA rates: FP64 128 x 64 tiles at two CTAs per SM, FP32 3xTF32 tiles at one
+        r.us = st.tile == 128 ? 3.0 + fl / (prm.fp32 ? 600e3 : 65e3) : 2.0 + fl / 30e3;
         if (t.mode == 0) {
           for (int c = t.b_row0 / 64; c <= (t.b_row0 + t.ncols - 1) / 64; ++c) {
             r.sig.push_back(COL + m.boff + c);
@@ -540,8 +542,8 @@ static void build_factor_dag(Plan& P) {
     for (int32_t u : succ_of(v)) best = std::max(best, blev[u]);
     blev[v] = dur[v] + best;
   }
-  // list scheduling on the SMs (one CTA per SM)
-  const int workers = 148;
+  // list scheduling on the SMs' CTA slots (two per SM for FP64, one for FP32)
+  const int workers = std::max(1, prm.sms) * (prm.fp32 ? 1 : 2);
   std::vector<int32_t> pend = npred;
   auto cmp = [&](int32_t x, int32_t y) { return blev[x] < blev[y] || (blev[x] == blev[y] && x > y); };
   std::priority_queue<int32_t, std::vector<int32_t>, decltype(cmp)> ready(cmp);

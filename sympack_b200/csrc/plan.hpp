@@ -251,10 +251,12 @@ struct PlanParams {
   int sms = 148;                 // SMs of the device: a launch with too few tiles to fill them
                                  // splits its tiles' K range (partial products add atomically)
   bool factor_dag = true;        // build the persistent factorization's task graph (FP64 handles)
+  bool fp32 = false;             // FP32 factor (precision form): 128 x 128 tensor-core tiles, one CTA
+                                 // per SM; FP64: 128 x 64 tiles at two CTAs per SM
   bool operator==(const PlanParams& o) const {
     return small_max_w == o.small_max_w && small_max_bytes == o.small_max_bytes && nb == o.nb &&
            outer_nb == o.outer_nb && big_tile_rows == o.big_tile_rows && solve_sb == o.solve_sb &&
-           solve_tpt == o.solve_tpt && sms == o.sms && factor_dag == o.factor_dag;
+           solve_tpt == o.solve_tpt && sms == o.sms && factor_dag == o.factor_dag && fp32 == o.fp32;
   }
 };
 

@@ -190,10 +190,10 @@ class SolverService:
                 self._patterns[key].add_done_callback(lambda _f: self._notify())
         return key
 
-    @staticmethod
-    def _analyse(A: DistSparseMatrix) -> symPACKMatrix2D:
+    def _analyse(self, A: DistSparseMatrix) -> symPACKMatrix2D:
+        # analysed with the service's precision: its plan is the one the factor handles use
         T = symPACKMatrix2D()
-        T.Init(symPACKOptions(device=-1))
+        T.Init(symPACKOptions(device=-1, precision=self.precision))
         T.SymbolicFactorization(A)
         return T
 

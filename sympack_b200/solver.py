@@ -90,13 +90,15 @@ class symPACKOptions:
     verbose: int = 0
     plan_small_max_w: int = 0      # 0 = library default
     plan_big_tile_rows: int = 0    # 0 = library default
-    fp32_engine: str = "tcgen05"   # FP32_IR update tiles: "tcgen05", "mma.sync", "tcgen05-persistent"
+    fp32_engine: str = "tcgen05-tma"  # FP32_IR update tiles: "tcgen05-tma", "tcgen05", "mma.sync",
+                                      # "tcgen05-persistent"
     decomposition: str = "LL"      # "LL" (Cholesky) or "LDL" (L D L^T, FP64), the driver's -fact
     plan_outer_nb: int = 0         # columns per outer block of wide panels (0 = library default 256)
     plan_dense_min_w: int = 0      # accepted for compatibility, no effect (the super-block solve replaced it)
     plan_solve_chunk: int = 0      # 64-column blocks per solve super-block (0 = library default 8)
     plan_solve_tiles: int = 0      # 64 x 64 tiles per super-block solve task (0 = library default 2)
-    factor_schedule: str = "persistent"  # FP64 factorization: "persistent" (one launch) or "steps"
+    factor_schedule: str = "auto"  # "persistent" (one launch; FP64, or FP32_IR with tcgen05-tma), "steps",
+                                   # or "auto" (persistent for FP64, steps for FP32_IR)
 
     def to_c(self) -> N.spb_options:
         if self.orderingStr not in N.ORDERINGS:
@@ -122,11 +124,11 @@ class symPACKOptions:
         o.plan_dense_min_w = self.plan_dense_min_w
         o.plan_solve_chunk = self.plan_solve_chunk
         o.plan_solve_tiles = self.plan_solve_tiles
-        schedules = {"persistent": 0, "steps": 1}
+        schedules = {"auto": 0, "steps": 1, "persistent": 2}
         if self.factor_schedule not in schedules:
-            raise ValueError(f"unknown factor_schedule {self.factor_schedule!r} (persistent or steps)")
+            raise ValueError(f"unknown factor_schedule {self.factor_schedule!r} (auto, persistent or steps)")
         o.factor_schedule = schedules[self.factor_schedule]
-        engines = {"tcgen05": 0, "mma.sync": 1, "tcgen05-persistent": 2}
+        engines = {"tcgen05": 0, "mma.sync": 1, "tcgen05-persistent": 2, "tcgen05-tma": 3}
         if self.fp32_engine not in engines:
             raise ValueError(f"unknown fp32_engine {self.fp32_engine!r}")
         o.fp32_engine = engines[self.fp32_engine]

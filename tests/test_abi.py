@@ -1,5 +1,6 @@
 """The C-ABI library loads and exports every entry point include/*.h declares;
 host-only handles give the documented status codes (no GPU needed)."""
+import ctypes as C
 import glob
 import os
 import re
@@ -57,12 +58,28 @@ def test_bad_options():
 
 def test_fp32_engine_option_is_validated():
     from sympack_b200 import symPACKMatrix2D, symPACKOptions
-    for eng in ("tcgen05", "mma.sync", "tcgen05-persistent"):
+    for eng in ("tcgen05", "mma.sync", "tcgen05-persistent", "tcgen05-tma"):
         M = symPACKMatrix2D()
         M.Init(symPACKOptions(device=-1, fp32_engine=eng))
         M.close()
     with pytest.raises(ValueError):
         symPACKMatrix2D().Init(symPACKOptions(device=-1, fp32_engine="wmma"))
+
+
+def test_factor_schedule_option_is_validated():
+    for sched in ("auto", "persistent", "steps"):
+        for prec in ("FP64", "FP32_IR"):
+            M = symPACKMatrix2D()
+            M.Init(symPACKOptions(device=-1, factor_schedule=sched, precision=prec))
+            M.close()
+    with pytest.raises(ValueError):
+        symPACKMatrix2D().Init(symPACKOptions(device=-1, factor_schedule="eager"))
+    o = N.spb_options()
+    N.load().spb_default_options(C.byref(o))
+    assert o.factor_schedule == 0 and o.fp32_engine == 3  # auto schedule, TMA-fed FP32 tiles
+    o.factor_schedule = 3
+    h = C.c_void_p()
+    assert N.load().spb_create(C.byref(o), C.byref(h)) == -1  # SPB_ERR_INVALID
 
 
 def test_decomposition_option_is_validated():

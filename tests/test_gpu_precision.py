@@ -61,7 +61,7 @@ def test_fp32_ir_reaches_fp64_backward_error(delta, fwd_tol, k):
         assert np.max(np.abs(x - xo)) / np.max(np.abs(xo)) <= fwd_tol
 
 
-@pytest.mark.parametrize("engine", ["tcgen05", "mma.sync", "tcgen05-persistent"])
+@pytest.mark.parametrize("engine", ["tcgen05", "mma.sync", "tcgen05-persistent", "tcgen05-tma"])
 @pytest.mark.parametrize("k", [14, 22])
 def test_fp32_factor_close_to_fp64_factor(engine, k):
     """FP32 factor (3xTF32 updates on either tensor-core engine) against the FP64
@@ -76,6 +76,32 @@ def test_fp32_factor_close_to_fp64_factor(engine, k):
     L32 = M32.GetFactor()
     L64 = factor(A, "FP64").GetFactor()
     assert np.max(np.abs(L32 - L64)) / np.max(np.abs(L64)) <= 1e-5
+
+
+@pytest.mark.parametrize("k,delta", [(22, 1e-2), (26, 1e-5)])
+def test_fp32_persistent_factorization_matches_step_sequence(k, delta):
+    """The TMA-fed tcgen05 engine in the persistent factorization (one launch) against the
+    same engine in the level-ordered launch sequence: the same tiles and operations in
+    another order, so FP32-level agreement (1e-6 of the largest entry), and refined
+    solutions at backward error <= 1e-12 twice in a row (the second factorization reuses
+    the launch with its counters cleared)."""
+    n, cp, ri, v = G.stencil27(k, k, k, delta, seed=5)
+    A = DistSparseMatrix.from_lower_csc(n, cp, ri, v)
+    got = {}
+    for sched in ("persistent", "steps"):
+        M = factor(A, "FP32_IR", fp32_engine="tcgen05-tma", factor_schedule=sched)
+        assert (M.info().factor_launches == 1) == (sched == "persistent")
+        got[sched] = M.GetFactor()
+        b = np.random.default_rng(7).standard_normal((n, 3))
+        for rep in range(2):
+            if rep:
+                M.DistributeMatrix(A)
+                M.Factorize()
+            M.Solve(b)
+            x = M.GetSolution(nrhs=3)
+            assert backward_error(A, x, b) <= 1e-12
+        M.close()
+    assert np.max(np.abs(got["persistent"] - got["steps"])) / np.max(np.abs(got["steps"])) <= 1e-6
 
 
 def test_refinement_cap_reports_not_converged():
