@@ -58,7 +58,7 @@ def parse():
     ap.add_argument("--serve-requests", type=int, default=10000,
                     help="requests of the serving workload (10000 = the named workload), run whole by the "
                          "continuous-batching loop at capacity")
-    ap.add_argument("--serve-sample", type=int, default=2000,
+    ap.add_argument("--serve-sample", type=int, default=1000,
                     help="requests of the stream's start run back to back (FP64 baseline) and with Poisson "
                          "arrivals at 0.7x capacity (a rate: it does not depend on how many follow)")
     ap.add_argument("--serve-fp64-batching", action="store_true",
@@ -522,7 +522,7 @@ def batching_comparison(torch, dev, stream, count, seed=0, subset=64, tune_syste
     return out
 
 
-def serving_comparison(torch, dev, count, seed=0, load=0.7, sample=2000, fp64_batching=False, check_every=25):
+def serving_comparison(torch, dev, count, seed=0, load=0.7, sample=1000, fp64_batching=False, check_every=25):
     """Serving form on the request stream: (1) back-to-back plain FP64, one request after
     the other, on the stream's first `sample` requests (a sequential baseline: its rate
     does not depend on how many requests follow); (2) the continuous-batching loop (8 slots,
@@ -727,11 +727,12 @@ def run_ours(args):
     busy = (tr[:, 2] - tr[:, 1]).astype(np.float64)
     span = float(tr[:, 2].max() - tr[:, 0].min())
     nsm = len(np.unique(tr[:, 3]))
-    names = ["small_panel", "diagonal_block", "trsm_tile", "tile_64x64", "tile_128x128_dmma"]
+    names = ["small_panel", "diagonal_block", "trsm_tile", "tile_64x64_fma", "tile_128x64_dmma"]
     roofline["task_breakdown"] = {
         names[k]: {"tasks": int(np.sum(tkinds == k)), "cta_ms": float(busy[tkinds == k].sum() / 1e6),
                    "share_of_busy": float(busy[tkinds == k].sum() / busy.sum())} for k in range(5)}
-    roofline["sm_busy_fraction"] = float(busy.sum() / (span * nsm))
+    # CTAs running a task, averaged over the launch and the SMs (two CTAs fit on an SM)
+    roofline["mean_busy_ctas_per_sm"] = float(busy.sum() / (span * nsm))
     # one profiled step (eager launches of the level-ordered sequence, per-launch CUDA events):
     # the solve sweeps' byte count and the per-kind times of the step schedule
     M.SetProfiling(True)
