@@ -97,7 +97,7 @@ __device__ __forceinline__ void split_fence() { asm volatile("fence.proxy.async.
 
 // Small panel s factored whole in shared memory P (h * w doubles).
 template <class T>
-__device__ void factor_small_task(const FactorArgs& a, int s, double* P) {
+__device__ __noinline__ void factor_small_task(const FactorArgs& a, int s, double* P) {
   const SnMeta m = a.meta[s];
   const int h = m.h, w = m.w;
   T* g = static_cast<T*>(a.L) + m.off;
@@ -162,7 +162,7 @@ __host__ __device__ constexpr int tri(int i, int j) { return i * (i + 1) / 2 + j
 constexpr int kDiagSmemDoubles = kNB * kDL + (kNB / kPiece) * kTri + kNB * kPiece + kNB;
 
 template <class T>
-__device__ void potrf_diag_task(const FactorArgs& a, const PanelItem& it, double* __restrict__ winv, double* sm) {
+__device__ __noinline__ void potrf_diag_task(const FactorArgs& a, const PanelItem& it, double* __restrict__ winv, double* sm) {
   double* D = sm;
   double(*Lp)[kTri] = reinterpret_cast<double(*)[kTri]>(sm + kNB * kDL);  // factored diagonal pieces
   double* Rinv = sm + kNB * kDL + (kNB / kPiece) * kTri;                  // 1 / L_kk
@@ -297,7 +297,7 @@ __device__ void potrf_diag_task(const FactorArgs& a, const PanelItem& it, double
 // 1 in place of 1/L_kk (the TRSM of the rows below then computes R L11^-T, which is W's
 // rows) and 1/D_kk.
 template <class T>
-__device__ void ldl_diag_task(const FactorArgs& a, const PanelItem& it, double* __restrict__ winv, double* sm) {
+__device__ __noinline__ void ldl_diag_task(const FactorArgs& a, const PanelItem& it, double* __restrict__ winv, double* sm) {
   double* D = sm;
   double(*Lp)[kTri] = reinterpret_cast<double(*)[kTri]>(sm + kNB * kDL);  // unit L below, d on the diagonal
   double* Wr = sm + kNB * kDL + (kNB / kPiece) * kTri;                    // rows below the piece: W = L D, ld kNB
@@ -444,7 +444,7 @@ __device__ void ldl_diag_task(const FactorArgs& a, const PanelItem& it, double* 
 constexpr int kTrsmSmemDoubles = 2 * kNB * kDL + kNB;
 
 template <class T>
-__device__ void trsm_rows_task(const FactorArgs& a, const PanelItem& it, const double* __restrict__ winv,
+__device__ __noinline__ void trsm_rows_task(const FactorArgs& a, const PanelItem& it, const double* __restrict__ winv,
                                double* sm) {
   double* R = sm;                // R[r + k*kDL]
   double* D = sm + kNB * kDL;    // D[i + j*kDL] = L11[i][j]

@@ -109,33 +109,48 @@ __device__ void tile_epilogue(const FactorArgs& a, const TileItem& it, const SnM
 
 namespace {
 
+// Bounded wait for the phase of an mbarrier with the given parity to complete.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, long long limit) {
+  for (long long i = 0; i < limit; ++i) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.b32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
 // ---- 128 x BN FP64 tensor-core tile ------------------------------------------------
-// BN = 64: 8 warps of 32 x 32 (4 x 2), two CTAs per SM (128 registers a thread, 79 KB of
-// shared memory each), so that one CTA's prologue and atomic epilogue overlap the other's
-// MMAs; BN = 128: 8 warps of 64 x 32 (2 x 4), one CTA per SM.
-constexpr int kDM = 128, kDK = 16, kDStages = 3, kDLds = 132, kDLdc = 130, kDThreads = 256;
-constexpr int kDTileN = 64;  // FP64 update tiles are 128 x 64 (Plan: big_tile_cols)
+// BN = 64: 8 warps of 32 x 32 (4 x 2), two CTAs per SM (126 registers, 102 KB of shared
+// memory each), so that one CTA's prologue and atomic epilogue overlap the other's MMAs.
+// Operands arrive by bulk asynchronous copies (cp.async.bulk, the TMA engine's untiled
+// form): per 16-column stage one copy per panel column and operand (128 or BN rows, 1 KB /
+// 512 B) into a padded column-major layout whose fragment reads are bank-conflict free,
+// issued by the lanes of warp 0 and completed on the stage's mbarrier (transaction bytes);
+// every warp releases a stage on a second mbarrier once it has read it, and warp 0
+// refills it.  No block-wide barrier in the K loop.  Copies start on 16-byte boundaries,
+// so an operand's rows are counted from the even row at or below its first row: accumulator
+// row i is panel row (a_row0 & ~1) + i (the plan cuts these tiles so that they fit).
+constexpr int kDM = 128, kDK = 16, kDStages = 4, kDLds = 132, kDLdc = 130, kDThreads = 256;
+constexpr int kDTileN = 64;  // FP64 update tiles are 128 x 64
 template <int BN>
 struct DTile {
   static constexpr int kLdb = BN + 4;
   static constexpr int kWarpsN = BN / 32, kWarpsM = 8 / kWarpsN;
   static constexpr int kMI = kDM / kWarpsM / 16;  // 16-row MMA tiles per warp
-  static constexpr size_t kPipeBytes = (size_t)kDStages * kDK * (kDLds + kLdb) * sizeof(double);
+  static constexpr int kStageElems = kDK * (kDLds + kLdb);
+  static constexpr size_t kPipeBytes = (size_t)kDStages * kStageElems * sizeof(double);
   static constexpr size_t kCBytes = (size_t)BN * kDLdc * sizeof(double);
   static constexpr size_t kMainBytes = kPipeBytes > kCBytes ? kPipeBytes : kCBytes;
-  static constexpr size_t kSmemBytes = kMainBytes + 4 * 128 * sizeof(int);
+  static constexpr size_t kIntsBytes = 4 * 128 * sizeof(int);
+  static constexpr size_t kSmemBytes = kMainBytes + kIntsBytes + 2 * kDStages * sizeof(uint64_t);
+  static_assert((kDLds * 8) % 16 == 0 && (kLdb * 8) % 16 == 0 && (kStageElems * 8) % 16 == 0,
+                "bulk copy destinations on 16-byte boundaries");
 };
 constexpr size_t kDSmemBytes = DTile<kDTileN>::kSmemBytes;
-
-__device__ __forceinline__ void cp_async8(void* smem, const void* gmem, int src_bytes) {
-  unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(src_bytes));
-}
-__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-template <int N>
-__device__ __forceinline__ void cp_wait() {
-  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
-}
 
 // D = A(16x4, row) * B(4x8, col) + D, FP64.  Fragment ownership (lane = 4*g + t):
 //   a0 = A[g][t], a1 = A[g+8][t], b0 = B[t][g],
@@ -147,10 +162,53 @@ __device__ __forceinline__ void dmma_16x8x4(double* d, double a0, double a1, dou
       : "d"(a0), "d"(a1), "d"(b0));
 }
 
-// One 128 x BN DMMA tile (kDThreads threads, DTile<BN>::kSmemBytes of shared memory).
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+constexpr long long kDWaitLimit = 1LL << 24;  // mbarrier polls before a DMMA tile gives up (seconds)
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(bar)
+               : "memory");
+}
+
+// Stage barriers of the DMMA tile, kept across the tiles a persistent CTA runs: g counts the
+// stages this CTA has consumed, so stage q of its life uses buffer q % kDStages and phase
+// (q / kDStages) & 1 of that buffer's barriers.
+struct DmPipe {
+  uint64_t* full;   // copies landed: one arrival (with the byte count) + transaction bytes
+  uint64_t* empty;  // read by all 8 warps
+  uint32_t g;
+};
+
 template <int BN>
-__device__ void dmma_tile_task(const FactorArgs& a, const TileItem& it, unsigned char* smem_raw) {
+__device__ __forceinline__ void dm_setup(DmPipe& P, unsigned char* smem_raw) {
   using D = DTile<BN>;
+  P.full = reinterpret_cast<uint64_t*>(smem_raw + D::kMainBytes + D::kIntsBytes);
+  P.empty = P.full + kDStages;
+  P.g = 0;
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < kDStages; ++i) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(P.full + i)) : "memory");
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(P.empty + i)), "r"(kDThreads / 32)
+                   : "memory");
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncthreads();
+}
+
+// One 128 x BN DMMA tile (kDThreads threads, DTile<BN>::kSmemBytes of shared memory).
+// Returns false, after recording status 3, when a barrier wait gave up (the copies in
+// flight have then been waited for, bounded).
+template <int BN>
+__device__ bool dmma_tile_task(const FactorArgs& a, const TileItem& it, unsigned char* smem_raw, DmPipe& P) {
+  using D = DTile<BN>;
+  __shared__ int sh_abort;
   double* pipe = reinterpret_cast<double*>(smem_raw);
   double* Cs = reinterpret_cast<double*>(smem_raw);  // reused once the main loop is done
   int* ints = reinterpret_cast<int*>(smem_raw + D::kMainBytes);
@@ -161,32 +219,48 @@ __device__ void dmma_tile_task(const FactorArgs& a, const TileItem& it, unsigned
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int wm = warp % D::kWarpsM, wn = warp / D::kWarpsM;
   const int gq = lane >> 2, tq = lane & 3;
-  constexpr int kStageElems = kDK * (kDLds + D::kLdb);
+  const int a0 = it.a_row0 & ~1, b0 = it.b_row0 & ~1;
+  const int ashift = it.a_row0 - a0, bshift = it.b_row0 - b0;
+  // rows copied per column: the tile's rows, within the column's padded storage (ld, a
+  // multiple of 4, so the count is even and the copy a multiple of 16 bytes)
+  const int nra = (int)min((int64_t)kDM, ld - a0), nrb = (int)min((int64_t)BN, ld - b0);
+  const int nk = (it.kn + kDK - 1) / kDK;
+  const uint32_t g0 = P.g;
 
-  auto load_stage = [&](int stage, int kk) {
-    double* As = pipe + (size_t)stage * kStageElems;
+  // earlier generic-proxy accesses of the stages (other tasks, the last epilogue) come
+  // before this tile's copies
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+  if (tid == 0) sh_abort = 0;
+  __syncthreads();
+
+  // stage kt (all lanes of warp 0): zero the K lines past kn up to the next multiple of 4,
+  // then one column copy per lane (A: lanes 0-15, B: lanes 16-31)
+  int issued = 0;
+  auto issue = [&](int kt) {
+    const uint32_t q = g0 + kt;
+    double* As = pipe + (size_t)(q % kDStages) * D::kStageElems;
     double* Bs = As + kDK * kDLds;
-#pragma unroll
-    for (int q = 0; q < 8; ++q) {
-      int e = tid + q * kDThreads;  // 0 .. 2047: (column, row) of a 16 x 128 operand slab
-      int col = e >> 7, r = e & 127;
-      int k = kk + col;
-      bool kok = k < it.kn;
-      int64_t coff = (int64_t)(it.k0 + (kok ? k : 0)) * ld;
-      bool aok = kok && r < it.mrows;
-      cp_async8(As + col * kDLds + r, aok ? g + it.a_row0 + r + coff : g, aok ? 8 : 0);
+    const int kv = min(kDK, it.kn - kt * kDK), kz = min(kDK, (kv + 3) & ~3);
+    for (int e = lane; e < (kz - kv) * (kDLds + D::kLdb); e += 32) {
+      const int l = kv + e / (kDLds + D::kLdb), o = e % (kDLds + D::kLdb);
+      if (o < kDLds) As[l * kDLds + o] = 0.0;
+      else Bs[l * D::kLdb + o - kDLds] = 0.0;
     }
-#pragma unroll
-    for (int q = 0; q < 16 * BN / kDThreads; ++q) {
-      int e = tid + q * kDThreads;  // (column, row) of a 16 x BN operand slab
-      int col = e / BN, r = e % BN;
-      int k = kk + col;
-      bool kok = k < it.kn;
-      int64_t coff = (int64_t)(it.k0 + (kok ? k : 0)) * ld;
-      bool bok = kok && r < it.ncols;
-      cp_async8(Bs + col * D::kLdb + r, bok ? gb + it.b_row0 + r + coff : gb, bok ? 8 : 0);
-    }
+    const uint32_t bar = smem_u32(P.full + q % kDStages);
+    __syncwarp();
+    if (lane == 0)
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar),
+                   "r"((uint32_t)(kv * (nra + nrb) * 8))
+                   : "memory");
+    __syncwarp();
+    const int64_t k = it.k0 + (int64_t)kt * kDK;
+    if (lane < kv) bulk_g2s(smem_u32(As + lane * kDLds), g + a0 + (k + lane) * ld, (uint32_t)nra * 8, bar);
+    else if (lane >= 16 && lane - 16 < kv)
+      bulk_g2s(smem_u32(Bs + (lane - 16) * D::kLdb), gb + b0 + (k + lane - 16) * ld, (uint32_t)nrb * 8, bar);
+    ++issued;
   };
+  if (warp == 0)
+    for (int kt = 0; kt < nk && kt < kDStages; ++kt) issue(kt);
 
   double acc[D::kMI][4][4];
 #pragma unroll
@@ -196,55 +270,83 @@ __device__ void dmma_tile_task(const FactorArgs& a, const TileItem& it, unsigned
 #pragma unroll
       for (int q = 0; q < 4; ++q) acc[i][j][q] = 0.0;
 
-  const int nk = (it.kn + kDK - 1) / kDK;
-#pragma unroll
-  for (int s = 0; s < kDStages - 1; ++s) {
-    if (s < nk) load_stage(s, s * kDK);
-    cp_commit();
-  }
+  bool ok = true;
   for (int kt = 0; kt < nk; ++kt) {
-    cp_wait<kDStages - 2>();
-    __syncthreads();
-    const int nxt = kt + kDStages - 1;
-    if (nxt < nk) load_stage(nxt % kDStages, nxt * kDK);
-    cp_commit();
-    const double* As = pipe + (size_t)(kt % kDStages) * kStageElems;
+    const uint32_t q = g0 + kt;
+    const int st = q % kDStages;
+    if (!mbar_wait(smem_u32(P.full + st), (q / kDStages) & 1, kDWaitLimit)) {
+      ok = false;
+      break;
+    }
+    const double* As = pipe + (size_t)st * D::kStageElems;
     const double* Bs = As + kDK * kDLds;
-    // four m16n8k4 steps per stage: the B fragments of the warp's four column tiles,
-    // then per row tile its A fragment and four MMAs
+    const int kz = min(kDK, ((it.kn - kt * kDK) + 3) & ~3);
+    // m16n8k4 steps: the B fragments of the warp's four column tiles, then per row tile
+    // its A fragment and four MMAs
 #pragma unroll
     for (int kk = 0; kk < kDK; kk += 4) {
+      if (kk >= kz) break;
       double bf[4];
 #pragma unroll
       for (int ni = 0; ni < 4; ++ni) bf[ni] = Bs[(kk + tq) * D::kLdb + wn * 32 + ni * 8 + gq];
 #pragma unroll
       for (int mi = 0; mi < D::kMI; ++mi) {
         const int r0 = wm * (16 * D::kMI) + mi * 16 + gq;
-        const double a0 = As[(kk + tq) * kDLds + r0], a1 = As[(kk + tq) * kDLds + r0 + 8];
+        const double x0 = As[(kk + tq) * kDLds + r0], x1 = As[(kk + tq) * kDLds + r0 + 8];
 #pragma unroll
-        for (int ni = 0; ni < 4; ++ni) dmma_16x8x4(acc[mi][ni], a0, a1, bf[ni]);
+        for (int ni = 0; ni < 4; ++ni) dmma_16x8x4(acc[mi][ni], x0, x1, bf[ni]);
       }
     }
+    __syncwarp();
+    if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(P.empty + st)) : "memory");
+    // warp 0 refills the buffer of the previous stage once every warp has read it
+    const int pk = kt - 1;
+    if (warp == 0 && pk >= 0 && pk + kDStages < nk) {
+      const uint32_t pq = g0 + pk;
+      if (!mbar_wait(smem_u32(P.empty + pq % kDStages), (pq / kDStages) & 1, kDWaitLimit)) {
+        ok = false;
+        break;
+      }
+      issue(pk + kDStages);
+    }
   }
-  cp_wait<0>();
-  __syncthreads();
+  if (!ok) sh_abort = 1;
+  ok = __syncthreads_and(ok) != 0;
+  if (!ok) {
+    if (warp == 0 && lane == 0) {  // let this CTA's copies in flight land (bounded)
+      for (int kt = 0; kt < issued; ++kt) {
+        const uint32_t q = g0 + kt;
+        mbar_wait(smem_u32(P.full + q % kDStages), (q / kDStages) & 1, kDWaitLimit);
+      }
+      report_status(a.status, 3, it.s, -1);
+    }
+    __syncthreads();
+    P.g = g0 + nk;
+    return false;
+  }
+  P.g = g0 + nk;
+  // accumulator row r / column c are panel rows a0 + r / b0 + c; Cs holds the tile from
+  // a_row0 / b_row0
 #pragma unroll
   for (int mi = 0; mi < D::kMI; ++mi)
 #pragma unroll
     for (int ni = 0; ni < 4; ++ni) {
-      int r0 = wm * (16 * D::kMI) + mi * 16 + gq, c0 = wn * 32 + ni * 8 + 2 * tq;
-      Cs[r0 + c0 * kDLdc] = acc[mi][ni][0];
-      Cs[r0 + (c0 + 1) * kDLdc] = acc[mi][ni][1];
-      Cs[r0 + 8 + c0 * kDLdc] = acc[mi][ni][2];
-      Cs[r0 + 8 + (c0 + 1) * kDLdc] = acc[mi][ni][3];
+      const int r0 = wm * (16 * D::kMI) + mi * 16 + gq - ashift, c0 = wn * 32 + ni * 8 + 2 * tq - bshift;
+      if (r0 >= 0 && c0 >= 0) Cs[r0 + c0 * kDLdc] = acc[mi][ni][0];
+      if (r0 >= 0 && c0 + 1 >= 0) Cs[r0 + (c0 + 1) * kDLdc] = acc[mi][ni][1];
+      if (c0 >= 0) Cs[r0 + 8 + c0 * kDLdc] = acc[mi][ni][2];
+      if (c0 + 1 >= 0) Cs[r0 + 8 + (c0 + 1) * kDLdc] = acc[mi][ni][3];
     }
   __syncthreads();
   tile_epilogue<kDM, BN, kDThreads, double, double>(a, it, m, Cs, kDLdc, (int64_t*)ints, (int64_t*)ints + 128);
+  return true;
 }
 
 __global__ void __launch_bounds__(kDThreads, 2) k_gemm_dmma(FactorArgs a, const TileItem* __restrict__ items) {
   extern __shared__ __align__(16) unsigned char smem_dmma[];
-  dmma_tile_task<kDTileN>(a, items[blockIdx.x], smem_dmma);
+  DmPipe P;
+  dm_setup<kDTileN>(P, smem_dmma);
+  dmma_tile_task<kDTileN>(a, items[blockIdx.x], smem_dmma, P);
 }
 
 // ---- 64 x 64 FP64 FMA tile --------------------------------------------------------
@@ -254,7 +356,7 @@ constexpr size_t kSSmemBytes = kSCBytes + 4 * 64 * sizeof(int);
 
 // One 64 x 64 FMA tile (256 threads, kSSmemBytes of shared memory).
 template <class T>
-__device__ void simt_tile_task(const FactorArgs& a, const TileItem& it, unsigned char* smem_raw) {
+__device__ __noinline__ void simt_tile_task(const FactorArgs& a, const TileItem& it, unsigned char* smem_raw) {
   T(*As)[64] = reinterpret_cast<T(*)[64]>(smem_raw);
   T(*Bs)[64] = reinterpret_cast<T(*)[64]>(smem_raw + 16 * 64 * sizeof(T));
   T* Cs = reinterpret_cast<T*>(smem_raw);
@@ -493,18 +595,6 @@ __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr) {
 constexpr uint32_t kUIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(kUN >> 3) << 17) |
                              ((uint32_t)(kUM >> 4) << 24);
 
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, long long limit) {
-  for (long long i = 0; i < limit; ++i) {
-    uint32_t done;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.b32 %0, 1, 0, p;\n}\n"
-        : "=r"(done)
-        : "r"(bar), "r"(parity)
-        : "memory");
-    if (done) return true;
-  }
-  return false;
-}
 
 __global__ void __launch_bounds__(256, 1) k_gemm_tc32(FactorArgs a, const TileItem* __restrict__ items) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -1240,7 +1330,9 @@ __device__ __forceinline__ unsigned smid() {
 
 // The largest task body: the DMMA tile (FP64), the TMA-fed tcgen05 tile (FP32), whose
 // stages and barriers sit above every other body's shared memory (at most 96 KB).
-constexpr size_t kFSmemBytes = kDSmemBytes > 96 * 1024 ? kDSmemBytes : 96 * 1024;  // small panels: 96 KB
+constexpr size_t kFSmemBytes = kDSmemBytes;  // the DMMA pipe and its barriers (above every other body's)
+static_assert(kFSmemBytes >= 96 * 1024 + DTile<kDTileN>::kIntsBytes + 2 * kDStages * sizeof(uint64_t),
+              "small panels (96 KB) stay below the DMMA stage barriers");
 constexpr size_t kFSmemBytes32 = kVSmemBytes;
 static_assert(kFSmemBytes32 >= 96 * 1024 + 1024, "FP32 persistent shared memory");
 
@@ -1252,7 +1344,9 @@ __global__ void __launch_bounds__(256, std::is_same<T, float>::value ? 1 : 2)
   extern __shared__ __align__(16) unsigned char smem_f[];
   __shared__ int sh_task, sh_go;
   TcTile tc;
+  DmPipe dp;
   if constexpr (kF32) tc_setup(tc, smem_f);  // tensor memory and stage barriers for the whole launch
+  else dm_setup<kDTileN>(dp, smem_f);
   for (;;) {
     if (threadIdx.x == 0) {
       int tk = atomicAdd(f.counter, 1);
@@ -1306,7 +1400,7 @@ __global__ void __launch_bounds__(256, std::is_same<T, float>::value ? 1 : 2)
         break;
       default:
         if constexpr (kF32) tc32t_tile_task(a, f.tiles[t.item], tc);  // a failure records status 3
-        else dmma_tile_task<kDTileN>(a, f.tiles[t.item], smem_f);
+        else dmma_tile_task<kDTileN>(a, f.tiles[t.item], smem_f, dp);
         break;
     }
     __syncthreads();

@@ -67,21 +67,26 @@ Plan build_plan(const Symbolic& sym, const PlanParams& prm) {
 
   // Tiles of a (rend-rbeg) x (cend-cbeg) product, rows/cols counted from rbeg/cbeg;
   // tiles entirely above the diagonal of a symmetric product are skipped.
+  // FP64 tensor-core tiles are 128 x 64 and copy their operands' columns from the even row
+  // at or below their first row, so they are cut from even rows (the first tile of a range
+  // that starts on an odd row has one row fewer).
   auto push_tiles = [&](std::vector<TileItem>& out, int T, int s, int mode, int rbeg, int rend, int cbeg, int cend,
                         int k0, int kn) {
-    const int TN = T == 128 && !prm.fp32 ? 64 : T;  // FP64 tensor-core tiles are 128 x 64
-    for (int cj = cbeg; cj < cend; cj += TN)
-      for (int ri = rbeg; ri < rend; ri += T) {
+    const bool dmma = T == 128 && !prm.fp32;
+    const int TN = dmma ? 64 : T;
+    const int r00 = dmma ? (rbeg & ~1) : rbeg, c00 = dmma ? (cbeg & ~1) : cbeg;
+    for (int cj = c00; cj < cend; cj += TN)
+      for (int ri = r00; ri < rend; ri += T) {
         if (ri + T <= cj) continue;  // rows and columns are both panel rows: tile above the diagonal
         TileItem t;
         t.s = s;
         t.mode = mode;
-        t.a_row0 = ri;
-        t.b_row0 = cj;
+        t.a_row0 = std::max(ri, rbeg);
+        t.b_row0 = std::max(cj, cbeg);
         t.k0 = k0;
         t.kn = kn;
-        t.mrows = std::min(T, rend - ri);
-        t.ncols = std::min(TN, cend - cj);
+        t.mrows = std::min(ri + T, rend) - t.a_row0;
+        t.ncols = std::min(cj + TN, cend) - t.b_row0;
         out.push_back(t);
       }
   };
