@@ -37,7 +37,7 @@ sys.path.insert(0, ROOT)
 
 # DRAM bytes (read + write) of one k_factor_persistent launch on the 60^3 workload, from ncu
 # (dram__bytes.sum.per_second x gpu__time_duration; profiles/factor_persistent_lap3d60_ncu.md)
-FACTOR_TRAFFIC_BYTES = 12.93e9
+FACTOR_TRAFFIC_BYTES = 15.57e9
 METRIC = "factor TFLOP/s (FP64 supernodal Cholesky, flops = sum of squared column counts)"
 
 

@@ -77,6 +77,7 @@ struct spb_handle {
   spb::SolveTask* dfwd = nullptr;
   spb::SolveTask* dbwd = nullptr;
   int32_t* dexpected = nullptr;
+  int32_t* dtiny = nullptr;        // leaf supernodes of the forward sweep's T tasks
   int32_t* dsparent = nullptr;
   int32_t* dsync = nullptr;  // solve counters (spb::solve_sync_ints)
   void* dInv = nullptr;      // diagonal super-block inverses of the forward operand (L, or L D for LDL^T)
@@ -451,6 +452,7 @@ void enqueue_sweeps(spb_handle* h, double* X, double* Z, int32_t* sync, int nrhs
     a.ldx = h->sym.n;
     a.nrhs = std::min(64, nrhs - c0);
     a.expected = h->dexpected;
+    a.tiny = h->dtiny;
     a.arrived = sync + 2;
     a.status = h->dstatus;
     a.spin_limit = h->wait_limit;
@@ -866,7 +868,8 @@ int64_t predict_bytes(const spb_handle* h, bool fp32, int nrhs) {
   t += b((int64_t)std::max(1, P.max_diag_slots) * (int64_t)spb::dev::kDiagSlotDoubles, 8);
   t += b(P.tile_items.size(), sizeof(spb::TileItem)) + b(n, 4) + b(ns, 4);
   t += b(P.fwd_tasks.size(), sizeof(spb::SolveTask)) + b(P.bwd_tasks.size(), sizeof(spb::SolveTask));
-  t += b(P.fwd_pending.size(), 4) + b(P.sparent.size(), 4) + b((int64_t)spb::solve_sync_ints(P), 4);
+  t += b(P.fwd_pending.size(), 4) + b(P.tiny.size(), 4) + b(P.sparent.size(), 4) +
+       b((int64_t)spb::solve_sync_ints(P), 4);
   t += b(P.inv_elems, fp32 ? sizeof(float) : sizeof(double)) + b(P.inv_items.size(), sizeof(spb::InvItem));
   t += b(P.ftasks.size(), sizeof(spb::FTask)) + b(P.fwaits.size(), sizeof(spb::FWait)) + b(P.fsigs.size(), 4) +
        b(P.nfctr + 1, 4);
@@ -955,6 +958,7 @@ int install_device(spb_handle* h) {
   SPB_CK(h, dalloc(h, &h->dfwd, P.fwd_tasks.size()));
   SPB_CK(h, dalloc(h, &h->dbwd, P.bwd_tasks.size()));
   SPB_CK(h, dalloc(h, &h->dexpected, P.fwd_pending.size()));
+  SPB_CK(h, dalloc(h, &h->dtiny, P.tiny.size()));
   SPB_CK(h, dalloc(h, &h->dsparent, P.sparent.size()));
   SPB_CK(h, dalloc(h, &h->dsync, spb::solve_sync_ints(P)));
   {
@@ -995,6 +999,7 @@ int install_device(spb_handle* h) {
   SPB_CK(h, up(h->dfwd, P.fwd_tasks.data(), P.fwd_tasks.size() * sizeof(spb::SolveTask)));
   SPB_CK(h, up(h->dbwd, P.bwd_tasks.data(), P.bwd_tasks.size() * sizeof(spb::SolveTask)));
   SPB_CK(h, up(h->dexpected, P.fwd_pending.data(), P.fwd_pending.size() * 4));
+  SPB_CK(h, up(h->dtiny, P.tiny.data(), P.tiny.size() * 4));
   SPB_CK(h, up(h->dsparent, P.sparent.data(), P.sparent.size() * 4));
   SPB_CK(h, up(h->dinvitems, P.inv_items.data(), P.inv_items.size() * sizeof(spb::InvItem)));
   SPB_CK(h, up(h->dftasks, P.ftasks.data(), P.ftasks.size() * sizeof(spb::FTask)));

@@ -1081,6 +1081,250 @@ __device__ __forceinline__ void named_sync(int id, int count) {
   asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
 }
 
+// ---- persistent, warp-specialised TMA-fed tcgen05 tile ----------------------------------
+// One CTA per SM loops over the launch's tiles (tile blockIdx.x + i * gridDim.x).  Warp 0
+// (one lane) issues the TMA loads of every chunk into a ring of three 64 KB stages, warp 1
+// (one lane) the MMAs into one of two tensor-memory accumulators (256 columns), and warps
+// 2-5 read an accumulator out and subtract it while the next tile is loaded and multiplied.
+// mbarriers: per stage "full" (TMA bytes landed) and "done" (its MMAs finished), per
+// accumulator "ready" (last MMA of a tile done) and "free" (its 4 epilogue warps have read
+// it).  The in-panel tiles go through a 32-column staging buffer so that each thread
+// subtracts 4 consecutive rows at a time (16-byte reductions); external updates are
+// scattered straight from the registers.
+constexpr int kWThreads = 192;
+constexpr int kWCsLd = 132;                                          // staging: 32 columns x 128 rows
+constexpr size_t kWCsBytes = (size_t)32 * kWCsLd * sizeof(float);    // 16.5 KB
+constexpr size_t kWMapBytes = 2 * 256 * sizeof(int64_t);             // per accumulator {base, rel}
+constexpr size_t kWSmemBytes = 1024 + kVMainBytes + kWCsBytes + kWMapBytes + 16 * sizeof(uint64_t) + 16;
+static_assert(kWSmemBytes <= 232448, "shared memory of the warp-specialised tcgen05 tile");
+
+__global__ void __launch_bounds__(kWThreads, 1) k_gemm_tc32w(FactorArgs a, const TileItem* __restrict__ items,
+                                                             int count) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const uint32_t raw_addr = (uint32_t)__cvta_generic_to_shared(smem_raw);
+  const uint32_t pad = ((raw_addr + 1023u) & ~1023u) - raw_addr;  // swizzle atoms need 1 KB alignment
+  unsigned char* base = smem_raw + pad;
+  const uint32_t base_addr = raw_addr + pad;
+  float* Cs = reinterpret_cast<float*>(base + kVMainBytes);
+  int64_t* maps = reinterpret_cast<int64_t*>(base + kVMainBytes + kWCsBytes);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(base + kVMainBytes + kWCsBytes + kWMapBytes);
+  uint64_t* full = bars;           // [kVStages]
+  uint64_t* done = bars + 3;       // [kVStages]
+  uint64_t* ready = bars + 6;      // [2]
+  uint64_t* freed = bars + 8;      // [2]
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 10);
+  __shared__ int sh_abort, sh_eab;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  auto sa = [](const void* p) { return (uint32_t)__cvta_generic_to_shared(p); };
+  static_assert(kVStages == 3, "barrier layout");
+
+  if (tid == 0) {
+    sh_abort = 0;
+    sh_eab = 0;
+    for (int i = 0; i < 3; ++i) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(sa(full + i)) : "memory");
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(sa(done + i)) : "memory");
+    }
+    for (int i = 0; i < 2; ++i) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(sa(ready + i)) : "memory");
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 4;\n" ::"r"(sa(freed + i)) : "memory");
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(sa(tmem_slot)),
+                 "r"(2 * kUTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0) {
+    // ---- TMA producer ----
+    if (lane == 0) {
+      uint32_t G = 0;  // chunks issued by this CTA
+      for (int tile = blockIdx.x; tile < count && !sh_abort; tile += gridDim.x) {
+        const TileItem it = items[tile];
+        const void* map = static_cast<const unsigned char*>(a.tmaps) + 128 * (size_t)a.tmap_of[it.s];
+        asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;\n" ::"l"(map) : "memory");
+        const bool same = it.a_row0 == it.b_row0;
+        const int nk = (it.kn + 31) / 32;
+        for (int kt = 0; kt < nk; ++kt, ++G) {
+          const int st = G % kVStages;
+          if (G >= kVStages &&
+              !mbar_wait(sa(done + st), (G / kVStages - 1) & 1, kUWaitLimit)) {  // the stage's MMAs finished
+            sh_abort = 1;
+            break;
+          }
+          const uint32_t s0 = base_addr + st * kVStageBytes;
+          asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(sa(full + st)),
+                       "r"((same ? 1 : 2) * 2 * kVOpBytes)
+                       : "memory");
+          tma_load_3d(s0, map, it.k0 + kt * 32, it.a_row0, sa(full + st));
+          if (!same) tma_load_3d(s0 + 2 * kVOpBytes, map, it.k0 + kt * 32, it.b_row0, sa(full + st));
+        }
+      }
+      // the last stages' copies have landed before the CTA leaves (bounded)
+      for (uint32_t q = G > kVStages ? G - kVStages : 0; q < G; ++q)
+        mbar_wait(sa(full + q % kVStages), (q / kVStages) & 1, kUWaitLimit);
+    }
+  } else if (warp == 1) {
+    // ---- MMA issuer ----
+    if (lane == 0) {
+      uint32_t G = 0;
+      int last = -1;  // stage of the last committed chunk, and its phase
+      uint32_t lastq = 0;
+      int ti = 0;
+      for (int tile = blockIdx.x; tile < count && !sh_abort; tile += gridDim.x, ++ti) {
+        const TileItem it = items[tile];
+        const bool same = it.a_row0 == it.b_row0;
+        const int nk = (it.kn + 31) / 32, acc = ti & 1;
+        if (ti >= 2 && !mbar_wait(sa(freed + acc), ((ti >> 1) - 1) & 1, kUWaitLimit)) {
+          sh_abort = 1;
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        const uint32_t dcol = tmem + (uint32_t)(acc * kUTmemCols);
+        for (int kt = 0; kt < nk; ++kt, ++G) {
+          const int st = G % kVStages;
+          if (!mbar_wait(sa(full + st), (G / kVStages) & 1, kUWaitLimit)) {
+            sh_abort = 1;
+            break;
+          }
+          asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+          const uint32_t s0 = base_addr + st * kVStageBytes;
+          const uint32_t sb = same ? s0 : s0 + 2 * kVOpBytes;
+#pragma unroll
+          for (int ks = 0; ks < 4; ++ks) {
+            const uint64_t ahi = umma_desc(s0 + ks * 32), alo = umma_desc(s0 + kVOpBytes + ks * 32);
+            const uint64_t bhi = umma_desc(sb + ks * 32), blo = umma_desc(sb + kVOpBytes + ks * 32);
+            const uint64_t pa[3] = {alo, ahi, ahi}, pb[3] = {bhi, blo, bhi};
+#pragma unroll
+            for (int p = 0; p < 3; ++p) {
+              const uint32_t accum = (kt > 0 || ks > 0 || p > 0) ? 1u : 0u;
+              asm volatile(
+                  "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                  " tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n}\n" ::"r"(dcol),
+                  "l"(pa[p]), "l"(pb[p]), "r"(kUIdesc), "r"(accum)
+                  : "memory");
+            }
+          }
+          asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                           sa(done + st))
+                       : "memory");
+          last = st;
+          lastq = G;
+        }
+        if (sh_abort) break;
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                         sa(ready + acc))
+                     : "memory");
+      }
+      if (last >= 0)  // every MMA finished before the stages and the tensor memory go away (bounded)
+        mbar_wait(sa(done + last), (lastq / kVStages) & 1, kUWaitLimit);
+    }
+  } else {
+    // ---- epilogue: warps 2-5, one accumulator row per thread ----
+    const int et = tid - 64, quarter = warp & 3, row = quarter * 32 + lane;
+    float* L = static_cast<float*>(a.L);
+    int ti = 0;
+    for (int tile = blockIdx.x; tile < count; tile += gridDim.x, ++ti) {
+      const TileItem it = items[tile];
+      const SnMeta m = a.meta[it.s];
+      const int acc = ti & 1;
+      int64_t* cbase = maps + acc * 256;
+      int64_t* crel = cbase + 128;
+      if (it.mode == 1 && et < it.ncols) {
+        const int jc = it.b_row0 + et;
+        const RelGroup gr = a.groups[a.row_group[m.lidx + jc]];
+        const SnMeta mt = a.meta[gr.t];
+        cbase[et] = mt.off + (int64_t)(a.rows[m.lidx + jc] - mt.fc) * mt.ld;
+        crel[et] = gr.rel_off - gr.j0;
+      }
+      const bool ok = mbar_wait(sa(ready + acc), (ti >> 1) & 1, kUWaitLimit);
+      if (!ok) sh_eab = 1;  // written by epilogue threads only, so all of them read the same value
+      named_sync(1, 128);   // maps ready; every epilogue thread has seen the accumulator ready (or not)
+      if (sh_eab) {
+        if (et == 0) sh_abort = 1;
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+      const int jr = it.a_row0 + row;
+      int64_t last = INT64_MIN;
+      int pos = 0;
+      for (int c0 = 0; c0 < kUN; c0 += 32) {
+        uint32_t v[32];
+        const uint32_t taddr = tmem + (uint32_t)(acc * kUTmemCols) + ((uint32_t)(quarter * 32) << 16) + (uint32_t)c0;
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+            "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
+            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+              "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
+              "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]),
+              "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]),
+              "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+            : "r"(taddr));
+        asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+        if (it.mode == 1) {
+          if (row < it.mrows) {
+#pragma unroll
+            for (int j = 0; j < 32; ++j) {
+              const int c = c0 + j;
+              if (c < it.ncols && jr >= it.b_row0 + c) {
+                const int64_t cr = crel[c];
+                if (cr != last) {
+                  pos = a.rel[cr + jr];
+                  last = cr;
+                }
+                atomicAdd(L + cbase[c] + pos, -__uint_as_float(v[j]));
+              }
+            }
+          }
+        } else {
+          // in-panel: stage 32 columns, then 4 consecutive rows per reduction (the panel starts
+          // on 32 elements, ld is a multiple of 4 and in-panel tiles start on 64-row boundaries)
+#pragma unroll
+          for (int j = 0; j < 32; ++j) Cs[row + j * kWCsLd] = __uint_as_float(v[j]);
+          named_sync(1, 128);
+          float* g = L + m.off + it.a_row0;
+#pragma unroll
+          for (int q = 0; q < 8; ++q) {
+            const int idx = et + q * 128, q4 = idx & 31, j = idx >> 5, i0 = 4 * q4, c = c0 + j;
+            if (c >= it.ncols) continue;
+            const int gc = it.b_row0 + c, jr0 = it.a_row0 + i0;
+            const float4 val = *reinterpret_cast<const float4*>(Cs + i0 + j * kWCsLd);
+            float* dst = g + i0 + (int64_t)gc * m.ld;
+            if (i0 + 3 < it.mrows && jr0 >= gc) {
+              atomicAdd(reinterpret_cast<float4*>(dst), make_float4(-val.x, -val.y, -val.z, -val.w));
+            } else {
+              const float vv[4] = {val.x, val.y, val.z, val.w};
+#pragma unroll
+              for (int e = 0; e < 4; ++e)
+                if (i0 + e < it.mrows && jr0 + e >= gc) atomicAdd(dst + e, -vv[e]);
+            }
+          }
+          named_sync(1, 128);  // the staging buffer is free for the next 32 columns
+        }
+      }
+      asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+      __syncwarp();
+      if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(sa(freed + acc)) : "memory");
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  if (sh_abort && tid == 0) report_status(a.status, 3, -1, -1);
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(2 * kUTmemCols)
+                 : "memory");
+  }
+}
+
+
 __global__ void __launch_bounds__(kPThreads, 1) k_gemm_tc32p(FactorArgs a, const TileItem* __restrict__ items,
                                                            int count) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -1429,6 +1673,7 @@ void init_gemm_attributes() {
   cudaFuncSetAttribute(k_gemm_tf32x3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTSmemBytes);
   cudaFuncSetAttribute(k_gemm_tc32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kUSmemBytes);
   cudaFuncSetAttribute(k_gemm_tc32t, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kVSmemBytes);
+  cudaFuncSetAttribute(k_gemm_tc32w, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWSmemBytes);
   cudaFuncSetAttribute(k_gemm_tc32p, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPSmemBytes);
   cudaFuncSetAttribute(k_gemm_dmma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDSmemBytes);
   cudaFuncSetAttribute(k_factor_persistent<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFSmemBytes);
@@ -1451,7 +1696,8 @@ void launch_gemm(cudaStream_t st, const FactorArgs& a, const TileItem* items, in
     if (tile == 128 && a.engine == 2)
       k_gemm_tc32p<<<count < g_sms ? count : g_sms, kPThreads, kPSmemBytes, st>>>(a, items, count);
     else if (tile == 128 && a.engine == 0) k_gemm_tc32<<<count, 256, kUSmemBytes, st>>>(a, items);
-    else if (tile == 128 && a.engine == 3) k_gemm_tc32t<<<count, 256, kVSmemBytes, st>>>(a, items);
+    else if (tile == 128 && a.engine == 3)
+      k_gemm_tc32w<<<count < g_sms ? count : g_sms, kWThreads, kWSmemBytes, st>>>(a, items, count);
     else if (tile == 128) k_gemm_tf32x3<<<count, 256, kTSmemBytes, st>>>(a, items);
     else k_gemm_simt<float><<<count, 256, kSSmemBytes, st>>>(a, items);
   } else {

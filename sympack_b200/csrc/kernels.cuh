@@ -101,6 +101,7 @@ struct PSolveArgs {
   int nrhs;  // <= 64
   const SolveTask* tasks;
   int ntasks;
+  const int32_t* tiny;  // leaf supernodes of the forward T tasks (Plan::tiny)
   int32_t* counter;
   const int32_t* expected;
   int32_t* arrived;

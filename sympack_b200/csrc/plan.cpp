@@ -313,6 +313,18 @@ Plan build_plan(const Symbolic& sym, const PlanParams& prm) {
     for (int q0 = q_begin; q0 < q_end; q0 += TPT) out.push_back(SolveTask{s, kind, pack_task_i(p, q0 - q_begin), t});
   };
   P.fwd_pending.assign(ns, 0);
+  // tiny leaves first: a thread each, no waits
+  auto tiny_leaf = [&](int s) {
+    const SnMeta& m = P.meta[s];
+    return P.level[s] == 0 && m.w <= kTinyMaxW && (int64_t)m.w * m.h <= kTinyMaxElems;
+  };
+  P.tiny.clear();
+  if (H > 0)
+    for (int s : P.level_sn[0])
+      if (tiny_leaf(s)) P.tiny.push_back(s);
+  for (size_t i = 0; i < P.tiny.size(); i += kTinyBatch)
+    P.fwd_tasks.push_back(SolveTask{P.tiny[i], 6, (int32_t)i,
+                                    (int32_t)std::min<size_t>(kTinyBatch, P.tiny.size() - i)});
   for (int L = 0; L < H; ++L) {
     int maxsb = 0;
     for (int s : P.level_sn[L]) maxsb = std::max(maxsb, nsb_of(s));
@@ -321,6 +333,7 @@ Plan build_plan(const Symbolic& sym, const PlanParams& prm) {
         const SnMeta& m = P.meta[s];
         const int nblk = nblk_of(s), noff = (m.h - m.w + 63) / 64;
         if (p >= nsb_of(s)) continue;
+        if (tiny_leaf(s)) continue;
         if (nblk == 1) {
           if (noff <= kSolveFusedTiles) {  // the whole supernode in one task
             P.fwd_tasks.push_back(SolveTask{s, 4, 0, 0});
@@ -359,6 +372,7 @@ Plan build_plan(const Symbolic& sym, const PlanParams& prm) {
         const SnMeta& m = P.meta[s];
         const int nblk = nblk_of(s), noff = (m.h - m.w + 63) / 64, nsb = nsb_of(s);
         if (j >= nsb) continue;
+        if (tiny_leaf(s)) continue;
         if (nblk == 1) {
           if (noff <= kSolveFusedTiles) {
             P.bwd_tasks.push_back(SolveTask{s, 4, 0, 0});
@@ -374,6 +388,9 @@ Plan build_plan(const Symbolic& sym, const PlanParams& prm) {
         for (int t = p * SB - 1; t >= 0; --t) chunks(P.bwd_tasks, s, 1, p, t, 0, nb);
       }
   }
+  for (size_t i = 0; i < P.tiny.size(); i += kTinyBatch)  // the tiny leaves last
+    P.bwd_tasks.push_back(SolveTask{P.tiny[i], 6, (int32_t)i,
+                                    (int32_t)std::min<size_t>(kTinyBatch, P.tiny.size() - i)});
   return P;
 }
 

@@ -110,6 +110,8 @@ struct FWait {
 // applied through its inverse Inv_p (computed once per factorization, in 64 x 64
 // tiles), so a super-block costs two parallel steps instead of a chain of sb block
 // solves.  Forward (permuted right-hand sides Y in, solution of L y = b in Z):
+//            kind 6  T(i, t):  t tiny leaf supernodes tiny[i .. i + t), one per thread, whole
+//                              (no arrivals to wait for; solve, scatter, signal)
 //            kind 4  F:        one-block supernode with at most kSolveFusedTiles
 //                              off-diagonal tiles, whole: Z_0 <- L_00^-1 Y_0, then every
 //                              tile's Y[ancestor rows] -= L_u0 Z_0
@@ -120,6 +122,7 @@ struct FWait {
 //            kind 2  O(p, u):  Y[rows of off-diagonal tile u] -= L(u, super-block p) Z[p],
 //                              scattered into the ancestors' rows
 // Backward (Z in, solution X):
+//            kind 6  T(i, t):  the tiny leaves, one per thread, each once its parent is done
 //            kind 4  G:        the F supernode whole: Z_0 -= L_u0^T X[ancestor rows of u] for
 //                              every tile, then X_0 <- L_00^-T Z_0
 //            kind 3  W(p, u):  Z[p] -= L(u, super-block p)^T X[ancestor rows of tile u]
@@ -224,6 +227,7 @@ struct Plan {
   // and per supernode the number of forward off-diagonal tiles writing its rows
   std::vector<SolveTask> fwd_tasks, bwd_tasks;
   std::vector<int32_t> fwd_pending;
+  std::vector<int32_t> tiny;  // leaf supernodes of the forward T tasks
   int32_t nblk_total = 0;  // 64-column blocks over all supernodes
   int32_t nsb_total = 0;   // solve super-blocks over all supernodes (per-super-block counters)
   int32_t solve_sb = 8;    // 64-column blocks per solve super-block
@@ -238,6 +242,9 @@ struct Plan {
 // Supernodes of one 64-column block with at most this many off-diagonal 64-row tiles
 // are one solve task per sweep.
 constexpr int kSolveFusedTiles = 16;
+// Tiny leaf supernodes (at most kTinyMaxW columns and kTinyMaxElems panel entries) are
+// solved forward one per thread, kTinyBatch to a task.
+constexpr int kTinyMaxW = 4, kTinyMaxElems = 64, kTinyBatch = 128;
 
 // Tunables of the plan.
 struct PlanParams {

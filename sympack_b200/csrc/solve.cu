@@ -411,6 +411,106 @@ __device__ __forceinline__ void add_out(double* out, int64_t ldx, int x0, const 
   }
 }
 
+// Forward sweep of one tiny leaf supernode s (w <= kTinyMaxW columns, no arrivals to wait
+// for) by one thread: Z_0 <- L_00^-1 Y_0 by substitution (multiplying by the pivots'
+// reciprocals), then Y[ancestor rows] -= L_u0 Z_0 with atomic additions, then one arrival
+// per target group of its rows (the release orders the thread's own writes) and its
+// diagonal-done count.
+template <class T>
+__device__ void tiny_forward(const PSolveArgs& a, int s, int nr) {
+  const SnMeta m = a.meta[s];
+  const T* P = static_cast<const T*>(a.L) + m.off;
+  const int32_t* rl = a.rows + m.lidx;
+  const int w = m.w, h = m.h;
+  const int64_t ld = m.ld;
+  double rinv[kTinyMaxW];
+#pragma unroll
+  for (int j = 0; j < kTinyMaxW; ++j) rinv[j] = j < w ? 1.0 / (double)P[j + j * ld] : 0.0;
+  for (int c = 0; c < nr; ++c) {
+    const int64_t xo = (int64_t)c * a.ldx;
+    double y[kTinyMaxW];
+#pragma unroll
+    for (int j = 0; j < kTinyMaxW; ++j) {
+      if (j >= w) break;
+      double t = a.X[m.fc + j + xo];
+#pragma unroll
+      for (int k = 0; k < j; ++k) t = fma(-(double)P[j + k * ld], y[k], t);
+      y[j] = t * rinv[j];
+      a.Z[m.fc + j + xo] = y[j];
+    }
+    for (int r = w; r < h; ++r) {
+      double t = 0.0;
+#pragma unroll
+      for (int j = 0; j < kTinyMaxW; ++j)
+        if (j < w) t = fma((double)P[r + j * ld], y[j], t);
+      atomicAdd(a.X + rl[r] + xo, -t);
+    }
+  }
+  if (h > w) {
+    const int g0 = a.row_group[m.lidx + w], g1 = a.row_group[m.lidx + h - 1];
+    for (int g = g0; g <= g1; ++g) red_release(a.arrived + a.groups[g].t, 1);
+  }
+  red_release(a.blkdone + s, 1);
+}
+
+// Backward sweep of one tiny leaf supernode s by one thread, once its parent is done
+// (bounded wait, like wait_geq but per thread): Z_0 -= L_u0^T X[ancestor rows], then
+// X_0 <- L_00^-T Z_0 by substitution; then its diagonal-done count.
+template <class T>
+__device__ void tiny_backward(const PSolveArgs& a, int s, int nr) {
+  const SnMeta m = a.meta[s];
+  const int par = a.sparent[s];
+  if (par >= 0) {
+    const int target = solve_done_count(a.meta[par].w, a.sb, a.tpt);
+    const int32_t* flag = a.blkdone + par;
+    if (ld_acquire(flag) < target) {
+      bool good = false;
+      for (long long it = 0; it < a.spin_limit; ++it) {
+        if (it >= 256) __nanosleep(128);
+        if (ld_acquire(flag) >= target) {
+          good = true;
+          break;
+        }
+        if (status_code(a.status) != 0) return;
+      }
+      if (!good) {
+        report_status(a.status, 3, s, target);
+        return;
+      }
+    }
+  }
+  const T* P = static_cast<const T*>(a.L) + m.off;
+  const int32_t* rl = a.rows + m.lidx;
+  const int w = m.w, h = m.h;
+  const int64_t ld = m.ld;
+  double rinv[kTinyMaxW];
+#pragma unroll
+  for (int j = 0; j < kTinyMaxW; ++j) rinv[j] = j < w ? 1.0 / (double)P[j + j * ld] : 0.0;
+  for (int c = 0; c < nr; ++c) {
+    const int64_t xo = (int64_t)c * a.ldx;
+    double z[kTinyMaxW];
+#pragma unroll
+    for (int j = 0; j < kTinyMaxW; ++j) z[j] = j < w ? a.Z[m.fc + j + xo] : 0.0;
+    for (int r = w; r < h; ++r) {
+      const double xr = a.X[rl[r] + xo];
+#pragma unroll
+      for (int j = 0; j < kTinyMaxW; ++j)
+        if (j < w) z[j] = fma(-(double)P[r + j * ld], xr, z[j]);
+    }
+#pragma unroll
+    for (int j = kTinyMaxW - 1; j >= 0; --j) {
+      if (j >= w) continue;
+      double t = z[j];
+#pragma unroll
+      for (int k = j + 1; k < kTinyMaxW; ++k)
+        if (k < w) t = fma(-(double)P[k + j * ld], z[k], t);
+      z[j] = t * rinv[j];
+      a.X[m.fc + j + xo] = z[j];
+    }
+  }
+  red_release(a.blkdone + s, 1);
+}
+
 template <class T, int kR>
 __global__ void __launch_bounds__(kThreads, solve_min_blocks<kR>()) k_solve_forward(PSolveArgs a) {
   extern __shared__ __align__(16) double sm[];
@@ -433,7 +533,12 @@ __global__ void __launch_bounds__(kThreads, solve_min_blocks<kR>()) k_solve_forw
     const int32_t* rl = a.rows + m.lidx;
     const int64_t ld = m.ld;
     const int nblk = (m.w + kT - 1) / kT;
-    if (task.kind == 5) {
+    if (task.kind == 6) {
+      // T: tiny leaf supernodes, one per thread (nothing to wait for)
+      trace_mark(a, tk, 1, now_ns());
+      if ((int)threadIdx.x < task.t) tiny_forward<T>(a, a.tiny[task.i + threadIdx.x], nr);
+      __syncthreads();
+    } else if (task.kind == 5) {
       // DI(p, r): Z[block r of p] += sum_{q <= r, this task's tiles} Inv_p(r, q) Y[block q of p]
       const int p = task.i & 0xffffff, q0 = task.i >> 24, r = task.t;
       const SuperBlock B(p, a.sb, nblk);
@@ -581,7 +686,13 @@ __global__ void __launch_bounds__(kThreads, solve_min_blocks<kR>()) k_solve_back
     const int64_t ld = m.ld;
     const int nblk = (m.w + kT - 1) / kT, nsb = (nblk + a.sb - 1) / a.sb;
     const int noff = (m.h - m.w + kT - 1) / kT;
-    if (task.kind == 5) {
+    if (task.kind == 6) {
+      // T: tiny leaf supernodes, one per thread (each waits for its parent)
+      trace_mark(a, tk, 1, now_ns());
+      if ((int)threadIdx.x < task.t) tiny_backward<T>(a, a.tiny[task.i + threadIdx.x], nr);
+      __syncthreads();
+      if (status_code(a.status) != 0) return;
+    } else if (task.kind == 5) {
       // DI(p, r): X[block r of p] += sum_{q >= r, this task's tiles} Inv_p(q, r)^T Z[block q of p]
       const int p = task.i & 0xffffff, j0 = task.i >> 24, r = task.t;
       const SuperBlock B(p, a.sb, nblk);

@@ -345,7 +345,8 @@ def test_solve_trace_of_a_profiled_solve():
     M.Factorize()
     M.SetProfiling(True)
     M.Solve(np.ones(n))
-    for sweep, kinds in ((0, {0, 1, 2, 4, 5}), (1, {0, 1, 3, 4, 5})):  # 4: a small supernode in one task
+    # 4: a small supernode in one task, 6: a batch of tiny leaves (one per thread)
+    for sweep, kinds in ((0, {0, 1, 2, 4, 5, 6}), (1, {0, 1, 3, 4, 5, 6})):
         tr = M.GetSolveTrace(sweep).astype(np.int64)
         assert tr.shape[1] == 4 and len(tr) > 0
         t0, t1, t2, sk = tr.T
