@@ -761,6 +761,18 @@ def run_ours(args):
             return {"error": repr(e)[:400]}
 
     precision = section(not args.no_precision, precision_comparison, torch, dev, stream, grid=args.precision_grid)
+    # roofline of the FP32 update tiles: 3xTF32 issues three MMAs per useful product; tcgen05
+    # runs kind::tf32 at half the dense kind::f16 rate, so the TF32 peak is half the measured bf16
+    try:
+        tiles = precision["kernels_profiled"]["FP32_IR"]["gemm_dmma"]
+        tf32_peak = peaks["bf16_tflops"] / 2
+        precision["fp32_tile_roofline"] = {
+            "kernel": "k_gemm_tc32w", "bound": "tensor", "unit": "TFLOP/s",
+            "useful": tiles["tflops"], "mma_work": 3 * tiles["tflops"], "peak": tf32_peak,
+            "frac": 3 * tiles["tflops"] / tf32_peak,
+            "peak_source": "half the dense bf16 rate of " + peak_src + " (tcgen05 kind::tf32 runs at half kind::f16)"}
+    except (KeyError, TypeError):
+        pass
     ldl = section(not args.no_ldl, ldl_comparison, torch, dev, stream, grid=args.grid)
     batching = section(not args.no_batch, batching_comparison, torch, dev, stream, args.batch_systems)
     serving = section(not args.no_serve, serving_comparison, torch, dev, args.serve_requests,
