@@ -11,8 +11,8 @@
 //                 3-stage cp.async pipeline, 8 warps of 32 x 32, two CTAs per SM
 //   k_gemm_simt   64 x 64 tiles with FMA, for narrow updates
 //   k_gemm_tc32   128 x 128 FP32 tiles, 3xTF32 on tcgen05, operands staged by cp.async
-//   k_gemm_tc32t  the same on TMA-fed MN-major operands (also a task of the persistent
-//                 FP32 factorization)
+//   k_gemm_tc32w  the same on TMA-loaded split copies, persistent and warp-specialised
+//                 (tc32t_tile_task: one such tile, a task of the persistent FP32 factorization)
 //   k_gemm_tc32p, k_gemm_tf32x3   a persistent tcgen05 variant and an mma.sync one
 // The epilogue stages C in shared memory and walks it column by column, so
 // consecutive threads touch consecutive target rows (coalesced atomics).
@@ -1053,13 +1053,6 @@ __device__ bool tc32t_tile_task(const FactorArgs& a, const TileItem& it, TcTile&
   return true;
 }
 
-__global__ void __launch_bounds__(256, 1) k_gemm_tc32t(FactorArgs a, const TileItem* __restrict__ items) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  TcTile S;
-  tc_setup(S, smem_raw);
-  tc32t_tile_task(a, items[blockIdx.x], S);
-  tc_teardown(S);
-}
 
 // ---- persistent, warp-specialised variant of the tcgen05 tile ---------------------
 // One CTA per SM loops over the launch's tiles.  Warps 0-7 stage operands and (one
@@ -1672,7 +1665,6 @@ void init_gemm_attributes() {
   if (g_sms <= 0) g_sms = 148;
   cudaFuncSetAttribute(k_gemm_tf32x3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTSmemBytes);
   cudaFuncSetAttribute(k_gemm_tc32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kUSmemBytes);
-  cudaFuncSetAttribute(k_gemm_tc32t, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kVSmemBytes);
   cudaFuncSetAttribute(k_gemm_tc32w, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWSmemBytes);
   cudaFuncSetAttribute(k_gemm_tc32p, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPSmemBytes);
   cudaFuncSetAttribute(k_gemm_dmma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDSmemBytes);
