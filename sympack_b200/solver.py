@@ -326,7 +326,8 @@ class symPACKMatrix2D:
 
     def GetFactorTrace(self):
         """(ntasks, 4) uint64 rows {handed out, dependencies met, done (ns), SM} in dispatch
-        order, and the task kinds (0 small, 1 diagonal block, 2 TRSM, 3 64x64 tile, 4 128x128 tile)."""
+        order, and the task kinds (0 small, 1 diagonal block, 2 TRSM, 3 64 x 64 tile, 4 tensor-core tile:
+        128 x 64 in FP64, 128 x 128 in FP32)."""
         h = self._need()
         nt = C.c_int64()
         _raise(self._lib.spb_get_factor_trace(h, None, 0, C.byref(nt), None), "GetFactorTrace", h)
