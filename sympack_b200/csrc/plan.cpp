@@ -455,7 +455,7 @@ static void build_factor_dag(Plan& P, const PlanParams& prm) {
         r.kind = st.kind == StepKind::PotrfDiag ? 1 : 2;
         r.s = it.s;
         r.sig = {BLK + b, SDONE + it.s};
-        r.us = r.kind == 1 ? 22.0 : 10.0;
+        r.us = r.kind == 1 ? 24.0 : 12.0;
         e_blk[b] += 1;
         e_sdone[it.s] += 1;
       } else {
@@ -464,8 +464,10 @@ static void build_factor_dag(Plan& P, const PlanParams& prm) {
         r.kind = st.tile == 128 ? 4 : 3;
         r.s = t.s;
         const double fl = 2.0 * t.mrows * t.ncols * t.kn;
-        // per-CTA rates: FP64 128 x 64 tiles at two CTAs per SM, FP32 3xTF32 tiles at one
-        r.us = st.tile == 128 ? 3.0 + fl / (prm.fp32 ? 600e3 : 65e3) : 2.0 + fl / 30e3;
+        // per-CTA rates (FP64 128 x 64 tiles at two CTAs per SM, FP32 3xTF32 tiles at one),
+        // like the diagonal-block and TRSM times above, from the task timeline of a traced
+        // factorization (spb_get_factor_trace)
+        r.us = st.tile == 128 ? 3.0 + fl / (prm.fp32 ? 600e3 : 90e3) : 2.0 + fl / 30e3;
         if (t.mode == 0) {
           for (int c = t.b_row0 / 64; c <= (t.b_row0 + t.ncols - 1) / 64; ++c) {
             r.sig.push_back(COL + m.boff + c);
