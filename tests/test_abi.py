@@ -131,3 +131,26 @@ def test_host_only_analysis_predicts_footprint_and_is_reusable():
         from sympack_b200 import RelaxationParameters
         R.Init(symPACKOptions(device=-1, relax=RelaxationParameters(nrelax0=4)))
         R.SymbolicFactorizationFrom(T)
+
+
+def test_footprint_prediction_follows_the_target_precision_and_engine():
+    """The plan depends on the precision (tile shapes, task graph), so a host-only analysis
+    predicts the same footprint for a precision whatever precision it was made in; the
+    TMA-fed FP32 tiles add split copies of the panels (at most two more FP32 arenas)."""
+    n, cp, ri, v = G.stencil27(14, 14, 14, 1e-2)
+    A = DistSparseMatrix.from_lower_csc(n, cp, ri, v)
+    got = {}
+    for prec in ("FP64", "FP32_IR"):
+        for eng in ("tcgen05-tma", "tcgen05"):
+            T = symPACKMatrix2D()
+            T.Init(symPACKOptions(device=-1, precision=prec, fp32_engine=eng))
+            T.SymbolicFactorization(A)
+            got[(prec, eng)] = (T.PredictDeviceBytes("FP64", 1), T.PredictDeviceBytes("FP32_IR", 1),
+                                T.info().arena_bytes, T.info().nsuper)
+            T.close()
+    for eng in ("tcgen05-tma", "tcgen05"):
+        assert got[("FP64", eng)][:2] == got[("FP32_IR", eng)][:2]
+    fp64_tma, fp32_tma, arena, ns = got[("FP64", "tcgen05-tma")]
+    assert got[("FP64", "tcgen05")][0] == fp64_tma  # the FP32 engine does not change an FP64 footprint
+    extra = fp32_tma - got[("FP64", "tcgen05")][1]
+    assert 0 < extra <= arena + 256 * ns  # two FP32 copies = one FP64 arena, plus maps and alignment
