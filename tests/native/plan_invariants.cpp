@@ -1,0 +1,171 @@
+// Host-side invariants of the device plan (plan.cpp), checked on grid matrices without a
+// GPU: tile shapes the tile engines rely on, the dispatch order of the persistent
+// factorization (every task's dependencies are signalled by tasks handed out before it),
+// and the tiny-leaf solve tasks.  Prints "ok" or the first violation and exits non-zero.
+#include <cstdio>
+#include <cstdlib>
+#include <set>
+#include <vector>
+
+#include "plan.hpp"
+
+using namespace spb;
+
+static int fails = 0;
+static long long n_tiles = 0, n_ftasks = 0, n_tiny = 0, n_big_tiles = 0;
+#define CHECK(cond, ...)                  \
+  do {                                    \
+    if (!(cond)) {                        \
+      if (fails++ < 10) {                 \
+        std::fprintf(stderr, __VA_ARGS__); \
+        std::fprintf(stderr, "\n");       \
+      }                                   \
+    }                                     \
+  } while (0)
+
+// Lower CSC (1-based, diagonal first) of a k x k x k grid with 7- or 27-point couplings.
+static void grid_matrix(int k, bool full, std::vector<int64_t>& cp, std::vector<int32_t>& ri) {
+  const int n = k * k * k;
+  cp.assign(1, 1);
+  ri.clear();
+  for (int z = 0; z < k; ++z)
+    for (int y = 0; y < k; ++y)
+      for (int x = 0; x < k; ++x) {
+        const int c = x + k * (y + k * z);
+        std::set<int> rows{c};
+        for (int dz = -1; dz <= 1; ++dz)
+          for (int dy = -1; dy <= 1; ++dy)
+            for (int dx = -1; dx <= 1; ++dx) {
+              const int nn = (dx != 0) + (dy != 0) + (dz != 0);
+              if (nn == 0 || (!full && nn != 1)) continue;
+              const int X = x + dx, Y = y + dy, Z = z + dz;
+              if (X < 0 || Y < 0 || Z < 0 || X >= k || Y >= k || Z >= k) continue;
+              const int r = X + k * (Y + k * Z);
+              if (r > c) rows.insert(r);
+            }
+        for (int r : rows) ri.push_back(r + 1);
+        cp.push_back((int64_t)ri.size() + 1);
+      }
+  (void)n;
+}
+
+static void check_plan(const Symbolic& sym, const PlanParams& prm, const char* what) {
+  const Plan P = build_plan(sym, prm);
+  // tiles
+  for (const Step& st : P.steps) {
+    if (st.kind != StepKind::Gemm) continue;
+    for (int i = st.begin; i < st.begin + st.count; ++i) {
+      const TileItem& t = P.tile_items[i];
+      const SnMeta& m = P.meta[t.s];
+      ++n_tiles;
+      n_big_tiles += st.tile == 128;
+      CHECK(t.mrows >= 1 && t.ncols >= 1 && t.kn >= 1, "%s: empty tile", what);
+      CHECK(t.a_row0 >= 0 && t.a_row0 + t.mrows <= m.h && t.b_row0 >= 0 && t.b_row0 + t.ncols <= m.h,
+            "%s: tile outside the panel rows", what);
+      CHECK(t.k0 >= 0 && t.k0 + t.kn <= m.w, "%s: K range outside the panel", what);
+      if (t.mode == 1) CHECK(t.a_row0 >= m.w && t.b_row0 >= m.w, "%s: external tile in the diagonal block", what);
+      else CHECK(t.b_row0 >= t.k0 + t.kn && t.a_row0 >= t.k0 + t.kn, "%s: in-panel tile overlaps its K columns", what);
+      if (st.tile == 128 && !prm.fp32)  // bulk copies start on the even row below
+        CHECK((t.a_row0 & 1) + t.mrows <= 128 && (t.b_row0 & 1) + t.ncols <= 64, "%s: FP64 tile shape", what);
+      if (st.tile == 128 && prm.fp32)   // 32-column TMA chunks that never read past the K range inside the panel
+        CHECK(t.mrows <= 128 && t.ncols <= 128 && t.k0 % 4 == 0 && (t.kn % 32 == 0 || t.k0 + t.kn == m.w),
+              "%s: FP32 tile shape", what);
+      if (st.tile == 64) CHECK(t.mrows <= 64 && t.ncols <= 64, "%s: 64 x 64 tile shape", what);
+    }
+  }
+  // persistent factorization: executing the tasks one by one in dispatch order never waits
+  if (prm.factor_dag) {
+    CHECK(!P.ftasks.empty(), "%s: no factor tasks", what);
+    n_ftasks += (long long)P.ftasks.size();
+    std::vector<int64_t> ctr(P.nfctr, 0);
+    for (size_t i = 0; i < P.ftasks.size(); ++i) {
+      const FTask& t = P.ftasks[i];
+      for (int w = 0; w < t.nwait; ++w) {
+        const FWait& fw = P.fwaits[t.wait0 + w];
+        CHECK(fw.ctr >= 0 && fw.ctr < P.nfctr, "%s: wait on a counter out of range", what);
+        CHECK(ctr[fw.ctr] >= fw.target, "%s: task %zu waits for a task handed out after it", what, i);
+      }
+      for (int q = 0; q < t.nsig; ++q) {
+        const int c = P.fsigs[t.sig0 + q];
+        CHECK(c >= 0 && c < P.nfctr, "%s: signal out of range", what);
+        ++ctr[c];
+      }
+    }
+  }
+  // solve: tiny leaves first (forward) and last (backward), each in exactly one batch
+  std::vector<int> seen(P.nsuper, 0);
+  bool tiny_phase = true;
+  for (const SolveTask& t : P.fwd_tasks) {
+    if (t.kind == 6) {
+      CHECK(tiny_phase, "%s: a tiny batch after other forward tasks", what);
+      CHECK(t.t >= 1 && t.t <= kTinyBatch && t.i + t.t <= (int)P.tiny.size(), "%s: tiny batch range", what);
+      for (int j = t.i; j < t.i + t.t; ++j) seen[P.tiny[j]]++;
+    } else {
+      tiny_phase = false;
+      seen[t.s] += 0;
+    }
+  }
+  n_tiny += (long long)P.tiny.size();
+  for (int s : P.tiny) {
+    const SnMeta& m = P.meta[s];
+    CHECK(seen[s] == 1, "%s: tiny supernode %d in %d batches", what, s, seen[s]);
+    CHECK(P.level[s] == 0 && m.w <= kTinyMaxW && (int64_t)m.w * m.h <= kTinyMaxElems, "%s: tiny criteria", what);
+  }
+  std::vector<int> fwd_tasks_of(P.nsuper, 0), bwd_tasks_of(P.nsuper, 0);
+  for (const SolveTask& t : P.fwd_tasks)
+    if (t.kind != 6) fwd_tasks_of[t.s]++;
+  bool after = false;
+  int bwd_tiny = 0;
+  for (const SolveTask& t : P.bwd_tasks) {
+    if (t.kind == 6) {
+      after = true;
+      bwd_tiny += t.t;
+    } else {
+      CHECK(!after, "%s: a backward task after the tiny batches", what);
+      bwd_tasks_of[t.s]++;
+    }
+  }
+  CHECK(bwd_tiny == (int)P.tiny.size(), "%s: backward tiny count", what);
+  for (int s = 0; s < P.nsuper; ++s) {
+    const bool tiny = seen[s] > 0;
+    CHECK(tiny == (fwd_tasks_of[s] == 0), "%s: supernode %d forward tasks %d tiny %d", what, s, fwd_tasks_of[s], tiny);
+    CHECK(tiny == (bwd_tasks_of[s] == 0), "%s: supernode %d backward tasks %d tiny %d", what, s, bwd_tasks_of[s], tiny);
+    if (tiny) CHECK(P.fwd_pending[s] == 0, "%s: tiny supernode %d expects arrivals", what, s);
+  }
+}
+
+int main() {
+  for (int full = 0; full < 2; ++full)
+    for (int k : {6, 12, 20, 28}) {
+      std::vector<int64_t> cp;
+      std::vector<int32_t> ri;
+      grid_matrix(k, full, cp, ri);
+      const int n = k * k * k;
+      const Symbolic sym = symbolic_factorization(n, cp.data(), ri.data(), OrderingKind::MMD, RelaxParams());
+      char what[64];
+      PlanParams p64;
+      p64.factor_dag = true;
+      std::snprintf(what, sizeof what, "%s %d^3 FP64", full ? "27-point" : "7-point", k);
+      check_plan(sym, p64, what);
+      PlanParams p32;
+      p32.fp32 = true;
+      p32.factor_dag = true;
+      std::snprintf(what, sizeof what, "%s %d^3 FP32", full ? "27-point" : "7-point", k);
+      check_plan(sym, p32, what);
+      PlanParams small;
+      small.outer_nb = 64;
+      small.big_tile_rows = 96;
+      small.small_max_w = 16;
+      small.solve_sb = 3;
+      small.solve_tpt = 1;
+      std::snprintf(what, sizeof what, "%s %d^3 FP64 small blocks", full ? "27-point" : "7-point", k);
+      check_plan(sym, small, what);
+    }
+  if (fails) {
+    std::fprintf(stderr, "%d violations\n", fails);
+    return 1;
+  }
+  std::printf("ok: %lld tiles (%lld tensor-core), %lld factor tasks, %lld tiny leaves\n", n_tiles, n_big_tiles,
+              n_ftasks, n_tiny);
+  return 0;
+}

@@ -1,0 +1,26 @@
+"""Host-side invariants of the device plan, compiled from the library's own plan and
+symbolic sources with g++ (no GPU): the tile shapes the tensor-core engines rely on (FP64
+tiles cut from even rows for the 16-byte bulk copies, FP32 tiles in whole 32-column TMA
+chunks), the persistent factorization's dispatch order (run one task at a time in that
+order, no task ever waits), and the tiny-leaf solve batches (first forward, last
+backward, every tiny leaf in exactly one)."""
+import os
+import shutil
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+CSRC = os.path.join(ROOT, "sympack_b200", "csrc")
+
+
+@pytest.mark.skipif(shutil.which("g++") is None, reason="needs g++")
+def test_plan_invariants_on_grid_matrices(tmp_path):
+    exe = tmp_path / "plan_invariants"
+    srcs = [os.path.join(ROOT, "tests", "native", "plan_invariants.cpp")]
+    srcs += [os.path.join(CSRC, f) for f in ("plan.cpp", "symbolic.cpp", "amd.cpp")]
+    subprocess.run(["g++", "-O2", "-std=c++17", "-I", CSRC, *srcs, "-o", str(exe)], check=True,
+                   capture_output=True, text=True)
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    assert r.stdout.startswith("ok")
