@@ -3,6 +3,7 @@
 // factorization (every task's dependencies are signalled by tasks handed out before it),
 // and the tiny-leaf solve tasks.  Prints "ok" or the first violation and exits non-zero.
 #include <cstdio>
+#include <algorithm>
 #include <cstdlib>
 #include <set>
 #include <vector>
@@ -126,6 +127,33 @@ static void check_plan(const Symbolic& sym, const PlanParams& prm, const char* w
     }
   }
   CHECK(bwd_tiny == (int)P.tiny.size(), "%s: backward tiny count", what);
+  // forward arrivals: what the tasks signal (one per relative-index group of the rows of
+  // each 64-row off-diagonal tile they scatter: O tasks per tile, F and tiny supernodes
+  // per tile of all their rows) equals what each target waits for
+  std::vector<int64_t> arrivals(P.nsuper, 0);
+  auto signal_rows = [&](int s, int r0, int r1) {
+    const SnMeta& m = P.meta[s];
+    const int g0 = P.row_group[m.lidx + r0], g1 = P.row_group[m.lidx + r1 - 1];
+    for (int g = g0; g <= g1; ++g) arrivals[P.groups[g].t]++;
+  };
+  auto signal_all_tiles = [&](int s) {
+    const SnMeta& m = P.meta[s];
+    for (int r0 = m.w; r0 < m.h; r0 += 64) signal_rows(s, r0, std::min(m.h, r0 + 64));
+  };
+  for (const SolveTask& t : P.fwd_tasks) {
+    if (t.kind == 6) {
+      for (int j = t.i; j < t.i + t.t; ++j) signal_all_tiles(P.tiny[j]);
+    } else if (t.kind == 4) {
+      signal_all_tiles(t.s);
+    } else if (t.kind == 2) {
+      const SnMeta& m = P.meta[t.s];
+      const int r0 = m.w + 64 * t.t;
+      signal_rows(t.s, r0, std::min(m.h, r0 + 64));
+    }
+  }
+  for (int s = 0; s < P.nsuper; ++s)
+    CHECK(arrivals[s] == P.fwd_pending[s], "%s: supernode %d gets %lld forward arrivals, waits for %d", what, s,
+          (long long)arrivals[s], P.fwd_pending[s]);
   for (int s = 0; s < P.nsuper; ++s) {
     const bool tiny = seen[s] > 0;
     CHECK(tiny == (fwd_tasks_of[s] == 0), "%s: supernode %d forward tasks %d tiny %d", what, s, fwd_tasks_of[s], tiny);

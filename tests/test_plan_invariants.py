@@ -2,8 +2,10 @@
 symbolic sources with g++ (no GPU): the tile shapes the tensor-core engines rely on (FP64
 tiles cut from even rows for the 16-byte bulk copies, FP32 tiles in whole 32-column TMA
 chunks), the persistent factorization's dispatch order (run one task at a time in that
-order, no task ever waits), and the tiny-leaf solve batches (first forward, last
-backward, every tiny leaf in exactly one)."""
+order, no task ever waits), the tiny-leaf solve batches (first forward, last backward,
+every tiny leaf in exactly one), and the forward solve's arrival counts (what the tasks
+signal equals what each supernode waits for, so no sweep waits for an arrival nobody
+sends)."""
 import os
 import shutil
 import subprocess
