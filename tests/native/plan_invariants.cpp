@@ -154,6 +154,114 @@ static void check_plan(const Symbolic& sym, const PlanParams& prm, const char* w
   for (int s = 0; s < P.nsuper; ++s)
     CHECK(arrivals[s] == P.fwd_pending[s], "%s: supernode %d gets %lld forward arrivals, waits for %d", what, s,
           (long long)arrivals[s], P.fwd_pending[s]);
+
+  // both sweeps run one task at a time in dispatch order with the kernels' wait targets and
+  // signals (solve.cu): no task ever waits, and every supernode ends done
+  const int SB = P.solve_sb, TPT = P.solve_tpt;
+  auto nblk_of = [&](int s) { return (P.meta[s].w + 63) / 64; };
+  auto nsb_of = [&](int s) { return (nblk_of(s) + SB - 1) / SB; };
+  auto nb_in = [&](int s, int p) { return std::min(SB, nblk_of(s) - p * SB); };
+  for (int sweep = 0; sweep < 2; ++sweep) {
+    std::vector<int64_t> arrived(P.nsuper, 0), done(P.nsuper, 0), upd(std::max(1, P.nsb_total), 0);
+    const std::vector<SolveTask>& tasks = sweep == 0 ? P.fwd_tasks : P.bwd_tasks;
+    auto need = [&](bool ok, size_t i, const char* which) {
+      CHECK(ok, "%s: %s task %zu (%s) would wait for a task handed out after it", what,
+            sweep ? "backward" : "forward", i, which);
+    };
+    auto parent_done = [&](int s) {
+      const int par = P.sparent[s];
+      return par < 0 || done[par] >= solve_done_count(P.meta[par].w, SB, TPT);
+    };
+    for (size_t i = 0; i < tasks.size(); ++i) {
+      const SolveTask& t = tasks[i];
+      const int s = t.s;
+      const SnMeta& m = P.meta[s];
+      const int p = t.i & 0xffffff, nblk = nblk_of(s), nsb = nsb_of(s), noff = (m.h - m.w + 63) / 64;
+      if (sweep == 0) {
+        switch (t.kind) {
+          case 6:
+            for (int j = t.i; j < t.i + t.t; ++j) {
+              const int q = P.tiny[j];
+              for (int r0 = P.meta[q].w; r0 < P.meta[q].h; r0 += 64) {
+                const int g0 = P.row_group[P.meta[q].lidx + r0];
+                const int g1 = P.row_group[P.meta[q].lidx + std::min(P.meta[q].h, r0 + 64) - 1];
+                for (int g = g0; g <= g1; ++g) arrived[P.groups[g].t]++;
+              }
+              done[q]++;
+            }
+            break;
+          case 5:
+            need(arrived[s] >= P.fwd_pending[s] && upd[m.sboff + p] >= (int64_t)p * nb_in(s, p) * solve_ntask(SB, TPT),
+                 i, "DI");
+            done[s]++;
+            break;
+          case 1:
+            need(done[s] >= solve_di_range(nblk, SB, TPT, 0, p + 1), i, "U");
+            upd[m.sboff + t.t / SB]++;
+            break;
+          case 2: {
+            need(nblk == 1 ? done[s] >= 1 : done[s] >= solve_di_range(nblk, SB, TPT, 0, p + 1), i, "O");
+            const int r0 = m.w + 64 * t.t, g0 = P.row_group[m.lidx + r0];
+            const int g1 = P.row_group[m.lidx + std::min(m.h, r0 + 64) - 1];
+            for (int g = g0; g <= g1; ++g) arrived[P.groups[g].t]++;
+            break;
+          }
+          case 0:
+            need(arrived[s] >= P.fwd_pending[s], i, "D");
+            done[s]++;
+            break;
+          case 4:
+            need(arrived[s] >= P.fwd_pending[s], i, "F");
+            for (int r0 = m.w; r0 < m.h; r0 += 64) {
+              const int g0 = P.row_group[m.lidx + r0], g1 = P.row_group[m.lidx + std::min(m.h, r0 + 64) - 1];
+              for (int g = g0; g <= g1; ++g) arrived[P.groups[g].t]++;
+            }
+            done[s]++;
+            break;
+          default:
+            CHECK(false, "%s: unknown forward task kind %d", what, t.kind);
+        }
+      } else {
+        switch (t.kind) {
+          case 6:
+            for (int j = t.i; j < t.i + t.t; ++j) {
+              need(parent_done(P.tiny[j]), i, "T");
+              done[P.tiny[j]]++;
+            }
+            break;
+          case 5: {
+            const int nlast = nblk - (nsb - 1) * SB;
+            const int later = p < nsb - 1 ? (nsb - 2 - p) * solve_ntask(SB, TPT) + solve_ntask(nlast, TPT) : 0;
+            need(upd[m.sboff + p] >= (int64_t)noff * solve_ntask(nb_in(s, p), TPT) + (int64_t)nb_in(s, p) * later, i,
+                 "DI");
+            done[s]++;
+            break;
+          }
+          case 1:
+            need(done[s] >= solve_di_range(nblk, SB, TPT, p, nsb), i, "V");
+            upd[m.sboff + t.t / SB]++;
+            break;
+          case 3:
+            need(parent_done(s), i, "W");
+            upd[m.sboff + p]++;
+            break;
+          case 0:
+            need(upd[m.sboff] >= noff, i, "B");
+            done[s]++;
+            break;
+          case 4:
+            need(parent_done(s), i, "G");
+            done[s]++;
+            break;
+          default:
+            CHECK(false, "%s: unknown backward task kind %d", what, t.kind);
+        }
+      }
+    }
+    for (int s = 0; s < P.nsuper; ++s)
+      CHECK(done[s] == solve_done_count(P.meta[s].w, SB, TPT), "%s: %s sweep leaves supernode %d at %lld of %d",
+            what, sweep ? "backward" : "forward", s, (long long)done[s], solve_done_count(P.meta[s].w, SB, TPT));
+  }
   for (int s = 0; s < P.nsuper; ++s) {
     const bool tiny = seen[s] > 0;
     CHECK(tiny == (fwd_tasks_of[s] == 0), "%s: supernode %d forward tasks %d tiny %d", what, s, fwd_tasks_of[s], tiny);

@@ -3,9 +3,10 @@ symbolic sources with g++ (no GPU): the tile shapes the tensor-core engines rely
 tiles cut from even rows for the 16-byte bulk copies, FP32 tiles in whole 32-column TMA
 chunks), the persistent factorization's dispatch order (run one task at a time in that
 order, no task ever waits), the tiny-leaf solve batches (first forward, last backward,
-every tiny leaf in exactly one), and the forward solve's arrival counts (what the tasks
-signal equals what each supernode waits for, so no sweep waits for an arrival nobody
-sends)."""
+every tiny leaf in exactly one), the forward solve's arrival counts (what the tasks
+signal equals what each supernode waits for), and both solve sweeps run one task at a time
+in dispatch order with the kernels' wait targets and signals (no task waits for one handed
+out after it, and every supernode ends done)."""
 import os
 import shutil
 import subprocess
