@@ -1162,11 +1162,20 @@ int spb_symbolic_batch(spb_handle* h, int32_t nsys, const int32_t* sys_offsets, 
   std::vector<std::string> errors(nsys);
   const spb::RelaxParams rp = relax_of(h->opt);
   const spb::OrderingKind ord = (spb::OrderingKind)h->opt.ordering;
+  // largest systems first, so that no large analysis starts last and runs alone
+  std::vector<int> order(nsys);
+  for (int k = 0; k < nsys; ++k) order[k] = k;
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+    const int64_t ex = colptr[sys_offsets[x + 1]] - colptr[sys_offsets[x]];
+    const int64_t ey = colptr[sys_offsets[y + 1]] - colptr[sys_offsets[y]];
+    return ex > ey;
+  });
   std::atomic<int> next{0};
   auto worker = [&]() {
     std::vector<int64_t> cp;
     std::vector<int32_t> ri;
-    for (int k = next++; k < nsys; k = next++) {
+    for (int slot = next++; slot < nsys; slot = next++) {
+      const int k = order[slot];
       const int o = sys_offsets[k], nk = sys_offsets[k + 1] - o;
       const int64_t p0 = colptr[o];
       cp.assign(nk + 1, 0);
