@@ -1,5 +1,5 @@
-// Host-side invariants of the device plan (plan.cpp), checked on grid matrices without a
-// GPU: tile shapes the tile engines rely on, the dispatch order of the persistent
+// Host-side invariants of the device plan (plan.cpp), checked on grid matrices and a
+// block-diagonal batch without a GPU: tile shapes the tile engines rely on, the dispatch order of the persistent
 // factorization (every task's dependencies are signalled by tasks handed out before it),
 // and the tiny-leaf solve tasks.  Prints "ok" or the first violation and exits non-zero.
 #include <cstdio>
@@ -48,6 +48,27 @@ static void grid_matrix(int k, bool full, std::vector<int64_t>& cp, std::vector<
         cp.push_back((int64_t)ri.size() + 1);
       }
   (void)n;
+}
+
+// Lower CSC (1-based) of a dense n x n matrix: one supernode of n columns.
+static void dense_matrix(int n, std::vector<int64_t>& cp, std::vector<int32_t>& ri) {
+  cp.assign(1, 1);
+  ri.clear();
+  for (int c = 0; c < n; ++c) {
+    for (int r = c; r < n; ++r) ri.push_back(r + 1);
+    cp.push_back((int64_t)ri.size() + 1);
+  }
+}
+
+// Lower CSC (1-based) of a path graph (tridiagonal): a chain of narrow supernodes.
+static void path_matrix(int n, std::vector<int64_t>& cp, std::vector<int32_t>& ri) {
+  cp.assign(1, 1);
+  ri.clear();
+  for (int c = 0; c < n; ++c) {
+    ri.push_back(c + 1);
+    if (c + 1 < n) ri.push_back(c + 2);
+    cp.push_back((int64_t)ri.size() + 1);
+  }
 }
 
 static void check_plan(const Symbolic& sym, const PlanParams& prm, const char* what) {
@@ -289,6 +310,7 @@ int main() {
       std::snprintf(what, sizeof what, "%s %d^3 FP32", full ? "27-point" : "7-point", k);
       check_plan(sym, p32, what);
       PlanParams small;
+      small.factor_dag = true;
       small.outer_nb = 64;
       small.big_tile_rows = 96;
       small.small_max_w = 16;
@@ -297,6 +319,47 @@ int main() {
       std::snprintf(what, sizeof what, "%s %d^3 FP64 small blocks", full ? "27-point" : "7-point", k);
       check_plan(sym, small, what);
     }
+  // a block-diagonal batch (a forest of elimination trees, merged as the batch analysis
+  // merges its systems): grids, a dense block wider than one outer block, a path, and
+  // many one-column systems
+  {
+    std::vector<Symbolic> parts;
+    std::vector<int64_t> cp;
+    std::vector<int32_t> ri;
+    auto add = [&](int n) {
+      parts.push_back(symbolic_factorization(n, cp.data(), ri.data(), OrderingKind::MMD, RelaxParams()));
+    };
+    grid_matrix(9, true, cp, ri);
+    add(9 * 9 * 9);
+    dense_matrix(300, cp, ri);
+    add(300);
+    for (int k : {3, 5, 7}) {
+      grid_matrix(k, false, cp, ri);
+      add(k * k * k);
+    }
+    path_matrix(500, cp, ri);
+    add(500);
+    dense_matrix(1, cp, ri);
+    for (int j = 0; j < 40; ++j) add(1);
+    grid_matrix(14, false, cp, ri);
+    add(14 * 14 * 14);
+    const Symbolic forest = merge_symbolic(parts);
+    PlanParams p64;
+    p64.factor_dag = true;
+    check_plan(forest, p64, "batch FP64");
+    PlanParams p32;
+    p32.fp32 = true;
+    p32.factor_dag = true;
+    check_plan(forest, p32, "batch FP32");
+    PlanParams small;
+    small.factor_dag = true;
+    small.outer_nb = 64;
+    small.big_tile_rows = 96;
+    small.small_max_w = 16;
+    small.solve_sb = 3;
+    small.solve_tpt = 1;
+    check_plan(forest, small, "batch FP64 small blocks");
+  }
   if (fails) {
     std::fprintf(stderr, "%d violations\n", fails);
     return 1;

@@ -6,7 +6,9 @@ order, no task ever waits), the tiny-leaf solve batches (first forward, last bac
 every tiny leaf in exactly one), the forward solve's arrival counts (what the tasks
 signal equals what each supernode waits for), and both solve sweeps run one task at a time
 in dispatch order with the kernels' wait targets and signals (no task waits for one handed
-out after it, and every supernode ends done)."""
+out after it, and every supernode ends done).  The matrices: 7- and 27-point grids, and a
+block-diagonal batch merged as the batch analysis merges its systems (grids, a dense block,
+a path, one-column systems), each planned in FP64, FP32 and with small blocks."""
 import os
 import shutil
 import subprocess
@@ -18,7 +20,7 @@ CSRC = os.path.join(ROOT, "sympack_b200", "csrc")
 
 
 @pytest.mark.skipif(shutil.which("g++") is None, reason="needs g++")
-def test_plan_invariants_on_grid_matrices(tmp_path):
+def test_plan_invariants_on_grid_matrices_and_a_batch(tmp_path):
     exe = tmp_path / "plan_invariants"
     srcs = [os.path.join(ROOT, "tests", "native", "plan_invariants.cpp")]
     srcs += [os.path.join(CSRC, f) for f in ("plan.cpp", "symbolic.cpp", "amd.cpp")]
