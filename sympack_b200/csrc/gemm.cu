@@ -1053,23 +1053,6 @@ __device__ bool tc32t_tile_task(const FactorArgs& a, const TileItem& it, TcTile&
   return true;
 }
 
-
-// ---- persistent, warp-specialised variant of the tcgen05 tile ---------------------
-// One CTA per SM loops over the launch's tiles.  Warps 0-7 stage operands and (one
-// thread) issue the MMAs exactly as k_gemm_tc32 does; warps 8-11 are the epilogue:
-// each thread owns one accumulator row, reads it from tensor memory 32 columns at a
-// time and scatters it.  Two accumulators (256 TMEM columns) let the epilogue of
-// tile i run while tile i + 1 is staged and multiplied.  mbarriers: per operand
-// stage (MMAs done, stage reusable), per accumulator "full" (last MMA of a tile
-// done) and "empty" (its 4 epilogue warps have read it).
-constexpr int kPStages = 2, kPRaw = 2, kPThreads = 384;
-constexpr long long kPWaitLimit = 1LL << 22;  // mbarrier polls before a wait gives up
-constexpr size_t kPOpAll = (size_t)kPStages * kUStageBytes;          // 128 KB
-constexpr size_t kPRawAll = (size_t)kPRaw * kURawBytes;              // 64 KB
-constexpr size_t kPMaps = 4 * 128 * sizeof(int64_t);                 // 2 accumulators x {base, rel}
-constexpr size_t kPSmemBytes = 1024 + kPOpAll + kPRawAll + kPMaps + 128;
-static_assert(kPSmemBytes <= 232448, "shared memory of the persistent tcgen05 tile");
-
 __device__ __forceinline__ void named_sync(int id, int count) {
   asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
 }
@@ -1317,6 +1300,21 @@ __global__ void __launch_bounds__(kWThreads, 1) k_gemm_tc32w(FactorArgs a, const
   }
 }
 
+// ---- persistent, warp-specialised variant of the tcgen05 tile ---------------------
+// One CTA per SM loops over the launch's tiles.  Warps 0-7 stage operands and (one
+// thread) issue the MMAs exactly as k_gemm_tc32 does; warps 8-11 are the epilogue:
+// each thread owns one accumulator row, reads it from tensor memory 32 columns at a
+// time and scatters it.  Two accumulators (256 TMEM columns) let the epilogue of
+// tile i run while tile i + 1 is staged and multiplied.  mbarriers: per operand
+// stage (MMAs done, stage reusable), per accumulator "full" (last MMA of a tile
+// done) and "empty" (its 4 epilogue warps have read it).
+constexpr int kPStages = 2, kPRaw = 2, kPThreads = 384;
+constexpr long long kPWaitLimit = 1LL << 22;  // mbarrier polls before a wait gives up
+constexpr size_t kPOpAll = (size_t)kPStages * kUStageBytes;          // 128 KB
+constexpr size_t kPRawAll = (size_t)kPRaw * kURawBytes;              // 64 KB
+constexpr size_t kPMaps = 4 * 128 * sizeof(int64_t);                 // 2 accumulators x {base, rel}
+constexpr size_t kPSmemBytes = 1024 + kPOpAll + kPRawAll + kPMaps + 128;
+static_assert(kPSmemBytes <= 232448, "shared memory of the persistent tcgen05 tile");
 
 __global__ void __launch_bounds__(kPThreads, 1) k_gemm_tc32p(FactorArgs a, const TileItem* __restrict__ items,
                                                            int count) {
