@@ -25,7 +25,9 @@ namespace sympack_b200 {
 
 // Supernode relaxation parameters with the reference's field names, constructors and
 // setters (include/sympack/Types.hpp:22-96): a positive maxSize caps every nrelax.
-// The default is run_sympack2D's (driver/utils.hpp:342-348: SetMaxSize(0), no cap).
+// A default-constructed object has no cap (maxSize 0; the reference leaves maxSize
+// unset there), which is also what run_sympack2D sets without -b
+// (driver/utils.hpp:341-348: SetMaxSize(0)).
 struct RelaxationParameters {
   int nrelax0 = 8, nrelax1 = 32, nrelax2 = 64;
   int maxSize = 0;
@@ -54,10 +56,13 @@ enum class DecompositionType { LL, LDL };
 // (include/sympack/Types.hpp:106-201): orderingStr ("MMD", "AMD", "RCM", "NATURAL",
 // "USER"), relax, decomposition, perm (USER ordering, 1-based), verbose.  The fields
 // after them have no counterpart in the reference and select the device, the
-// precision form and its refinement target.
+// precision form and its refinement target.  The defaults are the reference
+// constructor's (Types.hpp:158-188), relax included: supernodes of at most 150 columns
+// (RelaxationParameters(150) and SetMaxSize(150), Types.hpp:173-174) until the caller
+// sets another cap, as run_sympack2D does with relax.SetMaxSize.
 struct symPACKOptions {
   std::string orderingStr = "MMD";
-  RelaxationParameters relax;
+  RelaxationParameters relax = RelaxationParameters(150);
   DecompositionType decomposition = DecompositionType::LL;
   int* perm = nullptr;
   int verbose = 0;

@@ -124,6 +124,28 @@ int main() {
   bool threw = false;
   try { M.Factorize(); } catch (const std::runtime_error&) { threw = true; }  // host-only handle
   std::printf("%d %d\n", threw ? 1 : 0, bad_ordering ? 1 : 0);
+  // default options: the reference constructor's supernode cap of 150 columns, lifted
+  // by SetMaxSize(0); a dense 300 x 300 matrix is one supernode without the cap
+  const int nd = 300;
+  std::vector<long long> dcp(1, 1);
+  std::vector<int> dri;
+  for (int c = 0; c < nd; ++c) {
+    for (int r = c; r < nd; ++r) dri.push_back(r + 1);
+    dcp.push_back((long long)dri.size() + 1);
+  }
+  for (int cap = 0; cap < 2; ++cap) {
+    sympack_b200::symPACKOptions od;
+    od.device = -1;
+    if (cap) std::printf("%d %d %d %d ", od.relax.maxSize, od.relax.nrelax0, od.relax.nrelax1, od.relax.nrelax2);
+    else od.relax.SetMaxSize(0);
+    sympack_b200::symPACKMatrix2D D;
+    D.Init(od);
+    D.SymbolicFactorization(nd, reinterpret_cast<const int64_t*>(dcp.data()), dri.data());
+    std::vector<int> xs = D.GetSupernodalPartition();
+    int widest = 0;
+    for (size_t s = 0; s + 1 < xs.size(); ++s) widest = std::max(widest, xs[s + 1] - xs[s]);
+    std::printf("%d\n", widest);
+  }
   return 0;
 }
 """
@@ -153,6 +175,9 @@ def test_cpp_class_over_the_library(tmp_path):
     assert int(out[3]) == M.GetETree()[-1]
     assert out[4] == "1"
     assert out[5] == "1"  # an ordering the solver does not have is a logic_error, as in the reference
+    assert int(out[6]) == 300  # relax.SetMaxSize(0): no cap, the dense block is one supernode
+    assert out[7:11] == ["150", "8", "32", "64"]  # symPACKOptions() defaults (Types.hpp:158-188)
+    assert int(out[11]) == 150  # ... which cap supernodes at 150 columns
 
 
 CPP_DEVICE_PROGRAM = r"""
