@@ -15,6 +15,10 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <iomanip>
+#include <iostream>
+#include <limits>
+#include <ostream>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -98,6 +102,44 @@ struct symPACKOptions {
   }
 };
 
+// The factor as a MATLAB expression, the form of symPACKMatrix2D::DumpMatlab
+// (2D.hpp:6762-6854): +sparse([rows],[cols],[values],n,n) over the stored entries of the
+// lower triangle, supernode by supernode and row by row, in the permuted ordering
+// (1-based), values with 17 significant digits.  xsuper / xlindx / lindx: supernodal
+// partition and row structure (1-based); panels: per supernode its h x w panel
+// column-major with leading dimension h (spb_get_factor's layout).
+inline void write_matlab_sparse(std::ostream& os, int n, const std::vector<int32_t>& xsuper,
+                                const std::vector<int64_t>& xlindx, const std::vector<int32_t>& lindx,
+                                const double* panels) {
+  const int nsuper = (int)xsuper.size() - 1;
+  const std::ios_base::fmtflags flags = os.flags();
+  const std::streamsize prec = os.precision();
+  for (int pass = 0; pass < 3; ++pass) {
+    os << (pass == 0 ? "+sparse([" : "],[");
+    if (pass == 2) os << std::scientific << std::setprecision(std::numeric_limits<double>::max_digits10 - 1);
+    const double* p = panels;
+    bool first = true;
+    for (int s = 0; s < nsuper; ++s) {
+      const int fc = xsuper[s], w = xsuper[s + 1] - xsuper[s];
+      const int64_t r0 = xlindx[s] - 1, h = xlindx[s + 1] - xlindx[s];
+      for (int64_t i = 0; i < h; ++i)
+        for (int j = 0; j < w; ++j) {
+          const int row = lindx[r0 + i], col = fc + j;
+          if (row < col) continue;  // the diagonal block's upper part is not stored
+          if (!first) os << ' ';
+          first = false;
+          if (pass == 0) os << row;
+          else if (pass == 1) os << col;
+          else os << p[(int64_t)j * h + i];
+        }
+      p += h * w;
+    }
+  }
+  os << "]," << n << ',' << n << ")\n";
+  os.flags(flags);
+  os.precision(prec);
+}
+
 class symPACKMatrix2D {
  public:
   symPACKMatrix2D() = default;
@@ -108,7 +150,10 @@ class symPACKMatrix2D {
   }
 
   // symPACKMatrix2D::Init(symPACKOptions&) (2D.hpp:2649).
-  void Init(symPACKOptions& options) { Init(options.to_c()); }
+  void Init(symPACKOptions& options) {
+    Init(options.to_c());
+    options_ = options;
+  }
   // Options as spb_options (spb_default_options gives the reference's defaults).
   void Init(const spb_options& o) {
     if (h_) spb_destroy(h_);
@@ -174,6 +219,28 @@ class symPACKMatrix2D {
     check(spb_get_supernodes(need(), xsuper.data(), sup.data()));
     return sup;
   }
+  // symPACKMatrixMeta accessors (symPACKMatrixBase.hpp:96-103): order of the matrix, the
+  // options given to Init, number of supernodes.
+  int Size() const { return n_; }
+  symPACKOptions GetOptions() const { return options_; }
+  int TotalSupernodeCnt() { return n_ ? info().nsuper : 0; }
+
+  // symPACKMatrix2D::DumpMatlab (2D.hpp:6762-6854), after Factorize: the factor as
+  // +sparse([rows],[cols],[values],n,n) (write_matlab_sparse) on os.
+  void DumpMatlab(std::ostream& os = std::cout) {
+    const spb_info inf = info();
+    std::vector<int32_t> xsuper(inf.nsuper + 1), lindx(inf.lindx_size);
+    std::vector<int64_t> xlindx(inf.nsuper + 1);
+    check(spb_get_supernodes(need(), xsuper.data(), nullptr));
+    check(spb_get_structure(need(), xlindx.data(), lindx.data()));
+    size_t total = 0;
+    for (int s = 0; s < inf.nsuper; ++s)
+      total += (size_t)(xlindx[s + 1] - xlindx[s]) * (size_t)(xsuper[s + 1] - xsuper[s]);
+    std::vector<double> panels(total);
+    check(spb_get_factor(need(), panels.data()));
+    write_matlab_sparse(os, n_, xsuper, xlindx, lindx, panels.data());
+  }
+
   spb_info info() {
     spb_info i;
     check(spb_get_info(need(), &i));
@@ -191,6 +258,7 @@ class symPACKMatrix2D {
   }
   spb_handle* h_ = nullptr;
   int32_t n_ = 0;
+  symPACKOptions options_;
   std::vector<int64_t> colptr_;
   std::vector<int32_t> rowind_;
 };

@@ -201,6 +201,38 @@ def _d(a):
     return a.ctypes.data_as(N._DP)
 
 
+def matlab_sparse(n: int, xsuper, xlindx, lindx, panels) -> str:
+    """The factor as a MATLAB expression, the form of symPACKMatrix2D::DumpMatlab
+    (2D.hpp:6762-6854): ``+sparse([rows],[cols],[values],n,n)`` over the stored entries of
+    the lower triangle, supernode by supernode and row by row, in the permuted ordering
+    (1-based), values with 17 significant digits.  ``xsuper`` / ``xlindx`` / ``lindx`` are
+    the supernodal partition and row structure (1-based) and ``panels`` the factor, per
+    supernode its h x w panel column-major with leading dimension h."""
+    xsuper = np.asarray(xsuper, np.int64)
+    xlindx = np.asarray(xlindx, np.int64)
+    lindx = np.asarray(lindx, np.int64)
+    panels = np.asarray(panels, np.float64)
+    rows, cols, vals = [], [], []
+    off = 0
+    for s in range(len(xsuper) - 1):
+        fc, w = int(xsuper[s]), int(xsuper[s + 1] - xsuper[s])
+        r = lindx[xlindx[s] - 1:xlindx[s + 1] - 1]
+        h = len(r)
+        P = panels[off:off + h * w].reshape(w, h).T  # P[i, j]: row r[i], column fc + j
+        off += h * w
+        c = fc + np.arange(w)
+        keep = r[:, None] >= c[None, :]  # lower triangle (the diagonal block's upper part is not stored)
+        ii, jj = np.nonzero(keep)  # row-major: row by row, its columns in order
+        rows.append(r[ii])
+        cols.append(c[jj])
+        vals.append(P[ii, jj])
+    rows = np.concatenate(rows) if rows else np.empty(0, np.int64)
+    cols = np.concatenate(cols) if cols else np.empty(0, np.int64)
+    vals = np.concatenate(vals) if vals else np.empty(0)
+    return ("+sparse([" + " ".join(map(str, rows.tolist())) + "],[" + " ".join(map(str, cols.tolist())) + "],["
+            + " ".join(f"{v:.16e}" for v in vals.tolist()) + f"],{n},{n})\n")
+
+
 class symPACKMatrix2D:
     """One supernodal Cholesky factorization held on one GPU."""
 
@@ -425,6 +457,34 @@ class symPACKMatrix2D:
         out = np.empty(total, np.float64)
         _raise(self._lib.spb_get_factor(self._need(), _d(out)), "GetFactor", self._h)
         return out
+
+    def DumpMatlab(self, file=None) -> None:
+        """symPACKMatrix2D::DumpMatlab (2D.hpp:6762-6854): write the factor as
+        ``+sparse([rows],[cols],[values],n,n)`` (see ``matlab_sparse``) to ``file`` (a path
+        or a text stream; default standard output) after Factorize."""
+        import sys
+        xl, li = self.GetStructure()
+        text = matlab_sparse(self._n, self.GetSupernodalPartition(), xl, li, self.GetFactor())
+        if file is None:
+            sys.stdout.write(text)
+        elif isinstance(file, (str, bytes)) or hasattr(file, "__fspath__"):
+            with open(file, "w") as f:
+                f.write(text)
+        else:
+            file.write(text)
+
+    # symPACKMatrixMeta accessors (symPACKMatrixBase.hpp:96-103)
+    def Size(self) -> int:
+        """Order of the analysed matrix (iSize_)."""
+        return self._n
+
+    def GetOptions(self) -> "symPACKOptions | None":
+        """The options given to Init."""
+        return self.options
+
+    def TotalSupernodeCnt(self) -> int:
+        """Number of supernodes (0 before the symbolic factorization)."""
+        return int(self.info().nsuper) if self._h and self._n else 0
 
     def GetStatus(self):
         a, b, c = C.c_int32(), C.c_int32(), C.c_int32()

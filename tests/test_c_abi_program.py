@@ -9,6 +9,7 @@ import numpy as np
 import pytest
 
 from sympack_b200 import DistSparseMatrix, generators as G, symPACKMatrix2D, symPACKOptions
+from sympack_b200.solver import matlab_sparse
 from sympack_b200 import _native as N
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -83,6 +84,7 @@ def test_c_program_against_the_library(tmp_path):
 
 CPP_PROGRAM = r"""
 #include <cstdio>
+#include <fstream>
 #include <vector>
 #include "sympack_b200.hpp"
 
@@ -90,7 +92,7 @@ CPP_PROGRAM = r"""
 struct Graph { std::vector<long long> colptr; std::vector<int> rowind; };
 struct DistSparseMatrix { int size; Graph Localg_; std::vector<double> nzvalLocal; };
 
-int main() {
+int main(int argc, char** argv) {
   const int k = 20, n = k * k;
   DistSparseMatrix A;
   A.size = n;
@@ -146,6 +148,18 @@ int main() {
     for (size_t s = 0; s + 1 < xs.size(); ++s) widest = std::max(widest, xs[s + 1] - xs[s]);
     std::printf("%d\n", widest);
   }
+  // accessors, and the MATLAB text of a made-up factor (value = 1000 row + column)
+  std::printf("%d %d %d\n", M.Size(), M.TotalSupernodeCnt(), M.GetOptions().relax.maxSize);
+  const spb_info inf = M.info();
+  std::vector<int64_t> xl(inf.nsuper + 1);
+  std::vector<int32_t> li(inf.lindx_size);
+  if (spb_get_structure(M.handle(), xl.data(), li.data()) != SPB_OK) return 1;
+  std::vector<double> panels;
+  for (int s = 0; s < inf.nsuper; ++s)
+    for (int j = xsuper[s]; j < xsuper[s + 1]; ++j)
+      for (int64_t i = xl[s] - 1; i < xl[s + 1] - 1; ++i) panels.push_back(1000.0 * li[i] + j);
+  std::ofstream out(argv[argc - 1]);
+  sympack_b200::write_matlab_sparse(out, n, xsuper, xl, li, panels.data());
   return 0;
 }
 """
@@ -164,7 +178,8 @@ def test_cpp_class_over_the_library(tmp_path):
     env = dict(os.environ)
     env["LD_LIBRARY_PATH"] = os.path.join(os.path.dirname(cr.__file__), "lib") + os.pathsep + env.get(
         "LD_LIBRARY_PATH", "")
-    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True, env=env).stdout.split()
+    dump = tmp_path / "L.m"
+    out = subprocess.run([str(exe), str(dump)], check=True, capture_output=True, text=True, env=env).stdout.split()
     n, cp, ri, v = G.laplacian_2d(20, 20)
     M = symPACKMatrix2D()
     M.Init(symPACKOptions(device=-1))
@@ -178,6 +193,13 @@ def test_cpp_class_over_the_library(tmp_path):
     assert int(out[6]) == 300  # relax.SetMaxSize(0): no cap, the dense block is one supernode
     assert out[7:11] == ["150", "8", "32", "64"]  # symPACKOptions() defaults (Types.hpp:158-188)
     assert int(out[11]) == 150  # ... which cap supernodes at 150 columns
+    assert [int(x) for x in out[12:15]] == [n, M.info().nsuper, 0]  # Size, TotalSupernodeCnt, GetOptions
+    # DumpMatlab's text: the same as the Python class writes for the same panels
+    xs = M.GetSupernodalPartition()
+    xl, li = M.GetStructure()
+    panels = np.concatenate([(1000.0 * li[xl[s] - 1:xl[s + 1] - 1][:, None]
+                              + np.arange(xs[s], xs[s + 1])[None, :]).T.ravel() for s in range(len(xs) - 1)])
+    assert dump.read_text() == matlab_sparse(n, xs, xl, li, panels)
 
 
 CPP_DEVICE_PROGRAM = r"""

@@ -399,3 +399,36 @@ def test_degenerate_matrices(case, decomposition):
     M.Solve(b)
     x = M.GetSolution(nrhs=2)
     assert relerr(x, np.linalg.solve(D, b)) <= TOL
+
+
+def test_dump_matlab_of_the_device_factor_matches_the_oracle(tmp_path):
+    """symPACKMatrix2D::DumpMatlab (2D.hpp:6762-6854): the device factor as MATLAB text,
+    read back, equals the oracle's factor in the same form."""
+    import io
+    from sympack_b200.solver import matlab_sparse
+    n, cp, ri, v = G.laplacian_3d(9, 8, 7, 1e-2)
+    A = DistSparseMatrix.from_lower_csc(n, cp, ri, v)
+    M = setup(A)
+    buf = io.StringIO()
+    M.DumpMatlab(buf)
+    path = tmp_path / "L.m"
+    M.DumpMatlab(str(path))
+    assert path.read_text() == buf.getvalue()
+    f = oracle_for(M, A)
+    xl, li = M.GetStructure()
+    ref = matlab_sparse(n, M.GetSupernodalPartition(), xl, li, f.factor())
+
+    def parse(text):
+        head, tail = text.split("],[", 2)[:2], text.split("],[", 2)[2]
+        rows = np.array(head[0][len("+sparse(["):].split(), np.int64)
+        cols = np.array(head[1].split(), np.int64)
+        vals = np.array(tail.split("]")[0].split(), np.float64)
+        return rows, cols, vals
+
+    rg, cg, vg = parse(buf.getvalue())
+    ro, co, vo = parse(ref)
+    np.testing.assert_array_equal(rg, ro)
+    np.testing.assert_array_equal(cg, co)
+    assert relerr(vg, vo) <= TOL
+    assert buf.getvalue().endswith(f"],{n},{n})\n")
+    M.close()
