@@ -243,6 +243,13 @@ int spb_debug_stall_factor(spb_handle* h, int32_t supernode);
  * (0 small panel, 1 diagonal block, 2 TRSM tile, 3 64 x 64 tile, 4 128 x 128 tile). */
 int spb_set_factor_trace(spb_handle* h, int32_t on);
 int spb_get_factor_trace(spb_handle* h, uint64_t* out, int64_t cap, int64_t* ntasks, int32_t* kinds);
+/* Profile-guided task order of the persistent factorization: after a factorization
+ * traced with spb_set_factor_trace(h, 1), re-order the tasks by the same list scheduling
+ * with each task's measured duration in place of the cost model (the plan's
+ * factor_sched_us becomes the new prediction).  Later factorizations of this handle use
+ * the new order; the tasks, their dependencies and the results do not change.
+ * SPB_ERR_STATE without a fresh trace or when the persistent schedule is not in use. */
+int spb_reorder_factor_from_trace(spb_handle* h);
 /* Reset the device status word (after a reported failure). */
 int spb_clear_status(spb_handle* h);
 

@@ -134,6 +134,7 @@ SIGNATURES = [
     ("spb_debug_stall_factor", C.c_int, [_P, C.c_int32]),
     ("spb_set_factor_trace", C.c_int, [_P, C.c_int32]),
     ("spb_get_factor_trace", C.c_int, [_P, C.POINTER(C.c_uint64), C.c_int64, C.POINTER(C.c_int64), _I32P]),
+    ("spb_reorder_factor_from_trace", C.c_int, [_P]),
     ("spb_clear_status", C.c_int, [_P]),
     ("spb_set_stream", C.c_int, [_P, _P]),
     ("spb_set_profiling", C.c_int, [_P, C.c_int]),

@@ -72,6 +72,7 @@ struct spb_handle {
   int32_t* dfctr = nullptr;        // nfctr counters + the task counter
   unsigned long long* dftrace = nullptr;  // factor trace (spb_set_factor_trace): 4 per task
   bool factor_trace = false;
+  bool trace_fresh = false;        // the last factorization was traced in the current task order
   int32_t* dinvp0 = nullptr;
   int32_t* dlevel_sn = nullptr;
   spb::SolveTask* dfwd = nullptr;
@@ -1005,6 +1006,7 @@ int install_device(spb_handle* h) {
   SPB_CK(h, up(h->dftasks, P.ftasks.data(), P.ftasks.size() * sizeof(spb::FTask)));
   SPB_CK(h, up(h->dfwaits, P.fwaits.data(), P.fwaits.size() * sizeof(spb::FWait)));
   SPB_CK(h, up(h->dfsigs, P.fsigs.data(), P.fsigs.size() * 4));
+  h->trace_fresh = false;
   SPB_CK(h, cudaMemsetAsync(h->dstatus, 0, sizeof(Status), h->stream));
   if (h->fp32 && h->opt.fp32_engine == 3) {
     const int rc = build_tile_maps(h);
@@ -1263,6 +1265,7 @@ int spb_factorize(spb_handle* h) {
   if (!h->have_values) return fail(h, SPB_ERR_STATE, "factorize: call spb_distribute first");
   if (h->factored) return fail(h, SPB_ERR_STATE, "factorize: values already factored; distribute again");
   SPB_CK(h, cudaSetDevice(h->device));
+  h->trace_fresh = false;
   if (h->profiling) {
     int rc = factor_profiled(h);
     if (rc) return rc;
@@ -1302,6 +1305,7 @@ int spb_factorize(spb_handle* h) {
     return fail(h, SPB_ERR_TIMEOUT, "factorize: a device wait expired");
   }
   if (st.code != 0) return fail(h, SPB_ERR_STRUCTURE, "factorize: update row missing from target structure");
+  h->trace_fresh = h->factor_trace && !h->profiling && persistent_factor(h) && !h->plan.ftasks.empty();
   return SPB_OK;
 }
 
@@ -1551,6 +1555,38 @@ int spb_get_factor_trace(spb_handle* h, uint64_t* out, int64_t cap, int64_t* nta
   SPB_CK(h, cudaMemcpy(out, h->dftrace, 4 * n * sizeof(uint64_t), cudaMemcpyDeviceToHost));
   if (kinds)
     for (int64_t i = 0; i < n; ++i) kinds[i] = h->plan.ftasks[i].kind;
+  return SPB_OK;
+}
+
+int spb_reorder_factor_from_trace(spb_handle* h) {
+  if (check_handle(h)) return SPB_ERR_INVALID;
+  if (!h->have_symbolic || h->device < 0) return fail(h, SPB_ERR_STATE, "reorder: needs an analysed device handle");
+  if (!persistent_factor(h) || h->plan.ftasks.empty())
+    return fail(h, SPB_ERR_STATE, "reorder: the factorization does not use the persistent schedule");
+  if (!h->trace_fresh || !h->dftrace)
+    return fail(h, SPB_ERR_STATE, "reorder: factorize once with spb_set_factor_trace(h, 1) first");
+  SPB_CK(h, cudaSetDevice(h->device));
+  spb::Plan& P = h->plan;
+  const size_t n = P.ftasks.size();
+  std::vector<unsigned long long> tr(4 * n);
+  SPB_CK(h, cudaMemcpy(tr.data(), h->dftrace, tr.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+  std::vector<double> us(n);
+  for (size_t i = 0; i < n; ++i) {  // dependencies met -> done, nanoseconds of the global timer
+    const unsigned long long met = tr[4 * i + 1], done = tr[4 * i + 2];
+    us[i] = done > met ? (double)(done - met) * 1e-3 : 0.0;
+  }
+  try {
+    spb::reorder_factor_tasks(P, plan_params_of(h->opt), us);
+  } catch (const std::exception& e) {
+    return fail(h, SPB_ERR_INVALID, e.what());
+  }
+  // same sizes: the arrays are rewritten in place, so a captured factorization stays valid
+  SPB_CK(h, cudaMemcpyAsync(h->dftasks, P.ftasks.data(), n * sizeof(spb::FTask), cudaMemcpyHostToDevice, h->stream));
+  SPB_CK(h, cudaMemcpyAsync(h->dfwaits, P.fwaits.data(), P.fwaits.size() * sizeof(spb::FWait), cudaMemcpyHostToDevice,
+                            h->stream));
+  SPB_CK(h, cudaMemcpyAsync(h->dfsigs, P.fsigs.data(), P.fsigs.size() * 4, cudaMemcpyHostToDevice, h->stream));
+  SPB_CK(h, cudaStreamSynchronize(h->stream));
+  h->trace_fresh = false;
   return SPB_OK;
 }
 

@@ -9,7 +9,7 @@ namespace spb {
 
 static int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
 
-static void build_factor_dag(Plan& P, const PlanParams& prm);
+static void build_factor_dag(Plan& P, const PlanParams& prm, const std::vector<double>* measured_us = nullptr);
 
 Plan build_plan(const Symbolic& sym, const PlanParams& prm) {
   Plan P;
@@ -424,7 +424,14 @@ std::vector<int64_t> build_assembly_map(const Symbolic& sym, const Plan& P, cons
 // block granularity).  The dispatch order comes from a list-scheduling simulation on
 // the SMs with estimated task times, highest bottom level first, and is topological:
 // a CTA only ever waits for tasks handed out before its own.
-static void build_factor_dag(Plan& P, const PlanParams& prm) {
+void reorder_factor_tasks(Plan& P, const PlanParams& prm, const std::vector<double>& us) {
+  if (us.size() != P.ftasks.size()) throw std::invalid_argument("reorder: one duration per factor task");
+  build_factor_dag(P, prm, &us);
+}
+
+// measured_us: durations of the current tasks, in their dispatch order (P.ftasks), used in
+// place of the cost model for the tasks they name.
+static void build_factor_dag(Plan& P, const PlanParams& prm, const std::vector<double>* measured_us) {
   const int ns = P.nsuper, nb = P.nblk_total;
   const int EXT = 0, SDONE = ns, BLK = 2 * ns, COL = 2 * ns + nb;
   P.nfctr = 2 * ns + 2 * nb;
@@ -447,7 +454,7 @@ static void build_factor_dag(Plan& P, const PlanParams& prm) {
         r.s = s;
         r.sig = {SDONE + s};
         const double w = m.w, mm = m.h - m.w;
-        r.us = 3.0 + 2.0 * (w * w * w / 3.0 + mm * w * w) / 20e3;
+        r.us = 2.2 + 13.0 * (w * w * w / 3.0 + mm * w * w) / 20e3;
         e_sdone[s] += 1;
       } else if (st.kind == StepKind::PotrfDiag || st.kind == StepKind::TrsmRows) {
         const PanelItem& it = P.panel_items[i];
@@ -464,10 +471,12 @@ static void build_factor_dag(Plan& P, const PlanParams& prm) {
         r.kind = st.tile == 128 ? 4 : 3;
         r.s = t.s;
         const double fl = 2.0 * t.mrows * t.ncols * t.kn;
-        // per-CTA rates (FP64 128 x 64 tiles at two CTAs per SM, FP32 3xTF32 tiles at one),
-        // like the diagonal-block and TRSM times above, from the task timeline of a traced
-        // factorization (spb_get_factor_trace)
-        r.us = st.tile == 128 ? 3.0 + fl / (prm.fp32 ? 600e3 : 90e3) : 2.0 + fl / 30e3;
+        // fixed cost + per-CTA rate (FP64 128 x 64 tiles at two CTAs per SM, FP32 3xTF32
+        // tiles at one).  The FP64 figures, like the small-panel, diagonal-block and TRSM
+        // times above, fit the per-kind duration quantiles of the task timeline of a traced
+        // 60^3 Laplacian factorization (spb_get_factor_trace): a 128 x 64 tile costs about
+        // 11 us before its first flop (pipeline fill, dependency reads, atomic epilogue)
+        r.us = st.tile == 128 ? (prm.fp32 ? 3.0 + fl / 600e3 : 11.0 + fl / 105e3) : 5.0 + fl / 16.7e3;
         if (t.mode == 0) {
           for (int c = t.b_row0 / 64; c <= (t.b_row0 + t.ncols - 1) / 64; ++c) {
             r.sig.push_back(COL + m.boff + c);
@@ -487,6 +496,22 @@ static void build_factor_dag(Plan& P, const PlanParams& prm) {
         }
       }
       raw.push_back(std::move(r));
+    }
+  }
+  if (measured_us) {  // (kind, item) names a task: items index small_items, panel_items or tile_items
+    std::vector<int32_t> of_small(P.small_items.size(), -1), of_panel(P.panel_items.size(), -1),
+        of_tile(P.tile_items.size(), -1);
+    for (size_t k = 0; k < raw.size(); ++k) {
+      std::vector<int32_t>& of = raw[k].kind == 0 ? of_small : raw[k].kind <= 2 ? of_panel : of_tile;
+      of[raw[k].item] = (int32_t)k;
+    }
+    for (size_t i = 0; i < P.ftasks.size(); ++i) {
+      const FTask& t = P.ftasks[i];
+      const std::vector<int32_t>& of = t.kind == 0 ? of_small : t.kind <= 2 ? of_panel : of_tile;
+      const int32_t k = t.item >= 0 && t.item < (int32_t)of.size() ? of[t.item] : -1;
+      if (k < 0 || raw[k].kind != t.kind) throw std::invalid_argument("reorder: tasks do not match the plan");
+      const double d = (*measured_us)[i];
+      if (d > 0.0 && d < 1e7) raw[k].us = d;  // else keep the model's estimate
     }
   }
   // waits of every task

@@ -269,6 +269,12 @@ struct PlanParams {
 
 Plan build_plan(const Symbolic& s, const PlanParams& p = PlanParams());
 
+// Re-order the persistent factorization's tasks (P.ftasks, fwaits, fsigs, fsim_us) by the
+// same list scheduling with measured durations in place of the cost model: us[i] is the
+// duration of task P.ftasks[i] in microseconds (<= 0 keeps the model's estimate).  The
+// counts of tasks, waits and signals do not change; the dependency counters neither.
+void reorder_factor_tasks(Plan& P, const PlanParams& prm, const std::vector<double>& us);
+
 // int32 counters one persistent solve pass uses: two task counters, then per
 // supernode arrivals and forward / backward done blocks, then per super-block
 // forward / backward update counts.  Sized by 64-column blocks (at least as many

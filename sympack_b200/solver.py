@@ -369,6 +369,30 @@ class symPACKMatrix2D:
                                               kinds.ctypes.data_as(C.POINTER(C.c_int32))), "GetFactorTrace", h)
         return out, kinds
 
+    def ReorderFactorFromTrace(self) -> None:
+        """Re-order the persistent factorization's tasks by the durations the last traced
+        factorization measured (spb_reorder_factor_from_trace)."""
+        h = self._need()
+        _raise(self._lib.spb_reorder_factor_from_trace(h), "ReorderFactorFromTrace", h)
+
+    def TuneFactorOrder(self, A: "DistSparseMatrix", rounds: int = 2) -> list:
+        """Profile-guided task order: ``rounds`` times, factor A with the task timeline on
+        and re-order the tasks by their measured durations.  Leaves A distributed, ready
+        for Factorize, and the trace off.  Returns the ordering simulation's predicted
+        makespan (microseconds) after each round."""
+        pred = []
+        self.SetFactorTrace(True)
+        try:
+            for _ in range(rounds):
+                self.DistributeMatrix(A)
+                self.Factorize()
+                self.ReorderFactorFromTrace()
+                pred.append(float(self.info().factor_sched_us))
+        finally:
+            self.SetFactorTrace(False)
+        self.DistributeMatrix(A)
+        return pred
+
     def DebugStallFactor(self, supernode: int) -> None:
         """Failure-detection test hook: the persistent factorization waits for an update nobody sends."""
         _raise(self._lib.spb_debug_stall_factor(self._need(), int(supernode)), "DebugStallFactor", self._h)

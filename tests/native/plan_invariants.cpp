@@ -5,6 +5,7 @@
 #include <cstdio>
 #include <algorithm>
 #include <cstdlib>
+#include <map>
 #include <set>
 #include <vector>
 
@@ -113,6 +114,45 @@ static void check_plan(const Symbolic& sym, const PlanParams& prm, const char* w
         ++ctr[c];
       }
     }
+  }
+  // re-ordered by measured durations (here pseudo-random ones): the same tasks with the
+  // same waits and signals, and again no task waits for one handed out after it
+  if (prm.factor_dag) {
+    Plan R = P;
+    std::vector<double> us(R.ftasks.size());
+    unsigned long long x = 88172645463325252ULL;
+    for (double& u : us) {
+      x ^= x << 13; x ^= x >> 7; x ^= x << 17;
+      u = 0.5 + (double)(x % 100000) / 1000.0;
+    }
+    reorder_factor_tasks(R, prm, us);
+    CHECK(R.ftasks.size() == P.ftasks.size() && R.fwaits.size() == P.fwaits.size() &&
+          R.fsigs.size() == P.fsigs.size() && R.nfctr == P.nfctr, "%s: re-ordering changed the counts", what);
+    auto key = [](const FTask& t) { return ((long long)(t.kind == 0 ? 0 : t.kind <= 2 ? 1 : 2) << 32) | t.item; };
+    std::map<long long, size_t> pos;
+    for (size_t i = 0; i < P.ftasks.size(); ++i) pos[key(P.ftasks[i])] = i;
+    std::vector<int64_t> ctr(R.nfctr, 0);
+    for (size_t i = 0; i < R.ftasks.size(); ++i) {
+      const FTask& t = R.ftasks[i];
+      auto it = pos.find(key(t));
+      CHECK(it != pos.end(), "%s: re-ordering made a new task", what);
+      if (it == pos.end()) continue;
+      const FTask& o = P.ftasks[it->second];
+      CHECK(o.kind == t.kind && o.nwait == t.nwait && o.nsig == t.nsig, "%s: re-ordered task differs", what);
+      for (int w = 0; w < t.nwait && o.nwait == t.nwait; ++w)
+        CHECK(R.fwaits[t.wait0 + w].ctr == P.fwaits[o.wait0 + w].ctr &&
+                  R.fwaits[t.wait0 + w].target == P.fwaits[o.wait0 + w].target,
+              "%s: re-ordered task waits differ", what);
+      for (int q = 0; q < t.nsig && o.nsig == t.nsig; ++q)
+        CHECK(R.fsigs[t.sig0 + q] == P.fsigs[o.sig0 + q], "%s: re-ordered task signals differ", what);
+      for (int w = 0; w < t.nwait; ++w) {
+        const FWait& fw = R.fwaits[t.wait0 + w];
+        CHECK(ctr[fw.ctr] >= fw.target, "%s: re-ordered task %zu waits for a task handed out after it", what, i);
+      }
+      for (int q = 0; q < t.nsig; ++q) ++ctr[R.fsigs[t.sig0 + q]];
+      pos.erase(it);
+    }
+    CHECK(pos.empty(), "%s: re-ordering lost tasks", what);
   }
   // solve: tiny leaves first (forward) and last (backward), each in exactly one batch
   std::vector<int> seen(P.nsuper, 0);

@@ -432,3 +432,25 @@ def test_dump_matlab_of_the_device_factor_matches_the_oracle(tmp_path):
     assert relerr(vg, vo) <= TOL
     assert buf.getvalue().endswith(f"],{n},{n})\n")
     M.close()
+
+
+def test_profile_guided_task_order_keeps_the_factor():
+    """spb_reorder_factor_from_trace: the persistent factorization re-ordered by the
+    measured task durations of a traced run gives the same factor (within the FP64
+    tolerance: the atomic update order may differ) and matches the oracle."""
+    n, cp, ri, v = G.laplacian_3d(20, 20, 20, 1e-3)
+    A = DistSparseMatrix.from_lower_csc(n, cp, ri, v)
+    M = setup(A)
+    L0 = M.GetFactor()
+    with pytest.raises(StateError):
+        M.ReorderFactorFromTrace()  # no traced factorization yet
+    pred = M.TuneFactorOrder(A, rounds=2)
+    assert len(pred) == 2 and all(p > 0 for p in pred)
+    with pytest.raises(StateError):
+        M.ReorderFactorFromTrace()  # the trace is used up
+    M.Factorize()
+    L1 = M.GetFactor()
+    assert relerr(L1, L0) <= TOL
+    f = oracle_for(M, A)
+    assert relerr(L1, f.factor()) <= TOL
+    M.close()
