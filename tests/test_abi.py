@@ -37,7 +37,8 @@ def test_host_only_handle_rejects_numeric_calls():
     M = symPACKMatrix2D()
     M.Init(symPACKOptions(device=-1))
     M.SymbolicFactorization(A)
-    for call in (lambda: M.DistributeMatrix(A), M.Factorize, lambda: M.Solve(np.ones(n))):
+    for call in (lambda: M.DistributeMatrix(A), M.Factorize, lambda: M.Solve(np.ones(n)),
+                 M.ReorderFactorFromTrace, lambda: M.SetFactorTrace(True)):
         with pytest.raises(StateError):
             call()
 
