@@ -1597,7 +1597,11 @@ int spb_debug_stall_factor(spb_handle* h, int32_t supernode) {
   std::vector<spb::FWait> w = h->plan.fwaits;
   for (spb::FWait& x : w)
     if (supernode >= 0 && x.ctr == supernode) x.target += 1;  // ext counters come first
+  std::vector<spb::FTask> t = h->plan.ftasks;  // and the tasks' copies of their first wait
+  for (spb::FTask& x : t)
+    if (supernode >= 0 && x.nwait > 0 && x.w0_ctr == supernode) x.w0_target += 1;
   SPB_CK(h, cudaMemcpyAsync(h->dfwaits, w.data(), w.size() * sizeof(spb::FWait), cudaMemcpyHostToDevice, h->stream));
+  SPB_CK(h, cudaMemcpyAsync(h->dftasks, t.data(), t.size() * sizeof(spb::FTask), cudaMemcpyHostToDevice, h->stream));
   SPB_CK(h, cudaStreamSynchronize(h->stream));
   return SPB_OK;
 }

@@ -1590,7 +1590,7 @@ __global__ void __launch_bounds__(256, std::is_same<T, float>::value ? 1 : 2)
       if (go) {
         const FTask t = f.tasks[tk];
         for (int w = 0; w < t.nwait && go; ++w) {
-          const FWait fw = f.waits[t.wait0 + w];
+          const FWait fw = w == 0 ? FWait{t.w0_ctr, t.w0_target} : f.waits[t.wait0 + w];
           const int32_t* c = f.ctr + fw.ctr;
           if (ld_acquire_i(c) >= fw.target) continue;
           go = 0;

@@ -650,6 +650,8 @@ static void build_factor_dag(Plan& P, const PlanParams& prm, const std::vector<d
     for (const FWait& w : waits[k])
       if (w.target > 0) P.fwaits.push_back(w);
     t.nwait = (int32_t)P.fwaits.size() - t.wait0;
+    t.w0_ctr = t.nwait > 0 ? P.fwaits[t.wait0].ctr : 0;
+    t.w0_target = t.nwait > 0 ? P.fwaits[t.wait0].target : 0;
     t.sig0 = (int32_t)P.fsigs.size();
     P.fsigs.insert(P.fsigs.end(), raw[k].sig.begin(), raw[k].sig.end());
     t.nsig = (int32_t)raw[k].sig.size();

@@ -98,6 +98,8 @@ struct FTask {
   int32_t nwait;
   int32_t sig0;   // fsigs[sig0 .. sig0 + nsig)
   int32_t nsig;
+  int32_t w0_ctr;     // copy of the first wait, fwaits[wait0] (when nwait > 0), so that
+  int32_t w0_target;  // dispatch reads it with the task instead of after it
 };
 struct FWait {
   int32_t ctr;

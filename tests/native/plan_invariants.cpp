@@ -103,6 +103,8 @@ static void check_plan(const Symbolic& sym, const PlanParams& prm, const char* w
     std::vector<int64_t> ctr(P.nfctr, 0);
     for (size_t i = 0; i < P.ftasks.size(); ++i) {
       const FTask& t = P.ftasks[i];
+      CHECK(t.nwait == 0 || (t.w0_ctr == P.fwaits[t.wait0].ctr && t.w0_target == P.fwaits[t.wait0].target),
+            "%s: task %zu's copy of its first wait differs from its wait list", what, i);
       for (int w = 0; w < t.nwait; ++w) {
         const FWait& fw = P.fwaits[t.wait0 + w];
         CHECK(fw.ctr >= 0 && fw.ctr < P.nfctr, "%s: wait on a counter out of range", what);
@@ -139,6 +141,8 @@ static void check_plan(const Symbolic& sym, const PlanParams& prm, const char* w
       if (it == pos.end()) continue;
       const FTask& o = P.ftasks[it->second];
       CHECK(o.kind == t.kind && o.nwait == t.nwait && o.nsig == t.nsig, "%s: re-ordered task differs", what);
+      CHECK(t.nwait == 0 || (t.w0_ctr == R.fwaits[t.wait0].ctr && t.w0_target == R.fwaits[t.wait0].target),
+            "%s: re-ordered task's copy of its first wait differs", what);
       for (int w = 0; w < t.nwait && o.nwait == t.nwait; ++w)
         CHECK(R.fwaits[t.wait0 + w].ctr == P.fwaits[o.wait0 + w].ctr &&
                   R.fwaits[t.wait0 + w].target == P.fwaits[o.wait0 + w].target,
