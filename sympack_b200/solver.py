@@ -375,15 +375,15 @@ class symPACKMatrix2D:
         h = self._need()
         _raise(self._lib.spb_reorder_factor_from_trace(h), "ReorderFactorFromTrace", h)
 
-    def TuneFactorOrder(self, A: "DistSparseMatrix", rounds: int = 2) -> list:
-        """Profile-guided task order: ``rounds`` times, factor A with the task timeline on
+    def TuneFactorOrder(self, A: "DistSparseMatrix", passes: int = 2) -> list:
+        """Profile-guided task order: ``passes`` times, factor A with the task timeline on
         and re-order the tasks by their measured durations.  Leaves A distributed, ready
         for Factorize, and the trace off.  Returns the ordering simulation's predicted
-        makespan (microseconds) after each round."""
+        makespan (microseconds) after each pass."""
         pred = []
         self.SetFactorTrace(True)
         try:
-            for _ in range(rounds):
+            for _ in range(passes):
                 self.DistributeMatrix(A)
                 self.Factorize()
                 self.ReorderFactorFromTrace()

@@ -444,7 +444,7 @@ def test_profile_guided_task_order_keeps_the_factor():
     L0 = M.GetFactor()
     with pytest.raises(StateError):
         M.ReorderFactorFromTrace()  # no traced factorization yet
-    pred = M.TuneFactorOrder(A, rounds=2)
+    pred = M.TuneFactorOrder(A, passes=2)
     assert len(pred) == 2 and all(p > 0 for p in pred)
     with pytest.raises(StateError):
         M.ReorderFactorFromTrace()  # the trace is used up
