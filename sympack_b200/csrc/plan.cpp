@@ -1,8 +1,11 @@
 #include "plan.hpp"
 
 #include <algorithm>
+#include <atomic>
 #include <queue>
 #include <stdexcept>
+#include <system_error>
+#include <thread>
 #include <utility>
 
 namespace spb {
@@ -217,30 +220,64 @@ Plan build_plan(const Symbolic& sym, const PlanParams& prm) {
     }
     flush_gemm(Lane::Join, 0);
   }
-  // relative indices of the external updates: groups of off-diagonal rows by
-  // target, positions found by merging the sorted row lists
+  // relative indices of the external updates: groups of off-diagonal rows by target
+  // (every row of s from a group's first one on is in its target's row list), the
+  // group's positions in the target found by merging the sorted row lists from the
+  // first row's place.  The groups and their offsets first, then the positions,
+  // groups spread over host threads (batches of many systems have 1e8+ positions).
   P.row_group.assign(P.rows.size(), -1);
+  int64_t nrel = 0;
+  std::vector<int32_t> group_s;  // source supernode of each group
   for (int s = 0; s < ns; ++s) {
     const SnMeta& m = P.meta[s];
     const int32_t* rl = P.rows.data() + m.lidx;
     int r = m.w;
     while (r < m.h) {
       const int t = P.supmember0[rl[r]];
-      const SnMeta& mt = P.meta[t];
-      const int32_t* tl = P.rows.data() + mt.lidx;
-      RelGroup g{t, r, (int64_t)P.rel.size()};
       const int gid = (int)P.groups.size();
-      P.groups.push_back(g);
-      int q = 0;
-      for (int i = r; i < m.h; ++i) {
-        while (q < mt.h && tl[q] < rl[i]) ++q;
-        if (q == mt.h || tl[q] != rl[i]) throw std::runtime_error("plan: update row missing from its target's structure");
-        P.rel.push_back(q);
-      }
+      P.groups.push_back(RelGroup{t, r, nrel});
+      group_s.push_back(s);
+      nrel += m.h - r;
       int e = r;
       while (e < m.h && P.supmember0[rl[e]] == t) P.row_group[m.lidx + e++] = gid;
       r = e;
     }
+  }
+  P.rel.resize((size_t)nrel);
+  {
+    std::atomic<int64_t> next{0};
+    std::atomic<bool> missing{false};
+    const int64_t ngroups = (int64_t)P.groups.size(), chunk = 256;
+    auto fill = [&]() {
+      for (int64_t g0 = next.fetch_add(chunk); g0 < ngroups; g0 = next.fetch_add(chunk)) {
+        for (int64_t g = g0; g < std::min(ngroups, g0 + chunk); ++g) {
+          const RelGroup& gr = P.groups[g];
+          const SnMeta& m = P.meta[group_s[g]];
+          const SnMeta& mt = P.meta[gr.t];
+          const int32_t* rl = P.rows.data() + m.lidx;
+          const int32_t* tl = P.rows.data() + mt.lidx;
+          int32_t* out = P.rel.data() + gr.rel_off;
+          int q = (int)(std::lower_bound(tl, tl + mt.h, rl[gr.j0]) - tl);
+          for (int i = gr.j0; i < m.h; ++i) {
+            while (q < mt.h && tl[q] < rl[i]) ++q;
+            if (q == mt.h || tl[q] != rl[i]) {
+              missing = true;
+              return;
+            }
+            out[i - gr.j0] = q;
+          }
+        }
+      }
+    };
+    const unsigned nth = nrel < (1 << 20) ? 1u : std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    std::vector<std::thread> pool;
+    try {
+      for (unsigned k = 1; k < nth; ++k) pool.emplace_back(fill);
+    } catch (const std::system_error&) {  // fewer threads: the ones started and this one share the groups
+    }
+    fill();
+    for (std::thread& th : pool) th.join();
+    if (missing) throw std::runtime_error("plan: update row missing from its target's structure");
   }
 
   // algorithmic flops per step
@@ -262,13 +299,13 @@ Plan build_plan(const Symbolic& sym, const PlanParams& prm) {
         f += rows * it.nb * it.nb;
       } else {
         const TileItem& t = P.tile_items[i];
-        // pairs (r, c) of the tile with panel row >= panel column
-        double pairs = 0.0;
-        for (int c = 0; c < t.ncols; ++c) {
-          int lo = std::max(0, t.b_row0 + c - t.a_row0);
-          if (lo < t.mrows) pairs += t.mrows - lo;
-        }
-        f += 2.0 * t.kn * pairs;
+        // pairs (r, c) of the tile with panel row >= panel column: column c (panel row
+        // b_row0 + c) pairs with the tile rows from max(0, d + c) on, d = b_row0 - a_row0
+        const int64_t d = t.b_row0 - t.a_row0, mr = t.mrows, nc = t.ncols;
+        const int64_t c0 = std::min(nc, std::max<int64_t>(0, 1 - d));  // columns paired with every row
+        const int64_t k = std::max<int64_t>(0, std::min(nc, mr - d) - c0);  // then mr - d - c rows each
+        const int64_t pairs = c0 * mr + k * (mr - d) - (k * c0 + k * (k - 1) / 2);
+        f += 2.0 * t.kn * (double)pairs;
       }
     }
     P.step_flops[k] = f;
@@ -438,21 +475,28 @@ static void build_factor_dag(Plan& P, const PlanParams& prm, const std::vector<d
   std::vector<int32_t> e_ext(ns, 0), e_sdone(ns, 0), e_blk(nb, 0), e_col(nb, 0);
   struct Raw {
     int kind, item, s;
-    std::vector<int32_t> sig;
+    int32_t nsig;
+    int64_t sig0;  // signals sigv[sig0 .. sig0 + nsig)
     double us;
   };
   std::vector<Raw> raw;
+  std::vector<int32_t> sigv;  // every task's signals, flat (millions of tasks in a batch)
+  size_t ntask_all = 0;
+  for (const Step& st : P.steps) ntask_all += (size_t)st.count;
+  raw.reserve(ntask_all);
+  sigv.reserve(ntask_all * 2);
   // tasks of each step in step order (already topological), signals first
   for (const Step& st : P.steps) {
     for (int i = st.begin; i < st.begin + st.count; ++i) {
       Raw r;
       r.item = i;
+      r.sig0 = (int64_t)sigv.size();
       if (st.kind == StepKind::FactorSmall) {
         const int s = P.small_items[i];
         const SnMeta& m = P.meta[s];
         r.kind = 0;
         r.s = s;
-        r.sig = {SDONE + s};
+        sigv.push_back(SDONE + s);
         const double w = m.w, mm = m.h - m.w;
         r.us = 2.2 + 13.0 * (w * w * w / 3.0 + mm * w * w) / 20e3;
         e_sdone[s] += 1;
@@ -461,7 +505,8 @@ static void build_factor_dag(Plan& P, const PlanParams& prm, const std::vector<d
         const int b = P.meta[it.s].boff + it.c0 / 64;
         r.kind = st.kind == StepKind::PotrfDiag ? 1 : 2;
         r.s = it.s;
-        r.sig = {BLK + b, SDONE + it.s};
+        sigv.push_back(BLK + b);
+        sigv.push_back(SDONE + it.s);
         r.us = r.kind == 1 ? 24.0 : 12.0;
         e_blk[b] += 1;
         e_sdone[it.s] += 1;
@@ -479,7 +524,7 @@ static void build_factor_dag(Plan& P, const PlanParams& prm, const std::vector<d
         r.us = st.tile == 128 ? (prm.fp32 ? 3.0 + fl / 600e3 : 11.0 + fl / 105e3) : 5.0 + fl / 16.7e3;
         if (t.mode == 0) {
           for (int c = t.b_row0 / 64; c <= (t.b_row0 + t.ncols - 1) / 64; ++c) {
-            r.sig.push_back(COL + m.boff + c);
+            sigv.push_back(COL + m.boff + c);
             e_col[m.boff + c] += 1;
           }
         } else {
@@ -488,14 +533,15 @@ static void build_factor_dag(Plan& P, const PlanParams& prm, const std::vector<d
             const int g = P.row_group[m.lidx + t.b_row0 + c];
             const int tgt = P.groups[g].t;
             if (tgt != last) {
-              r.sig.push_back(EXT + tgt);
+              sigv.push_back(EXT + tgt);
               e_ext[tgt] += 1;
             }
             last = tgt;
           }
         }
       }
-      raw.push_back(std::move(r));
+      r.nsig = (int32_t)((int64_t)sigv.size() - r.sig0);
+      raw.push_back(r);
     }
   }
   if (measured_us) {  // (kind, item) names a task: items index small_items, panel_items or tile_items
@@ -514,27 +560,35 @@ static void build_factor_dag(Plan& P, const PlanParams& prm, const std::vector<d
       if (d > 0.0 && d < 1e7) raw[k].us = d;  // else keep the model's estimate
     }
   }
-  // waits of every task
-  std::vector<std::vector<FWait>> waits(raw.size());
+  // waits of every task, flat: task k's are wv[woff[k] .. woff[k + 1])
+  std::vector<FWait> wv;
+  std::vector<int64_t> woff(raw.size() + 1, 0);
+  wv.reserve(raw.size() * 2);
   for (size_t k = 0; k < raw.size(); ++k) {
     const Raw& r = raw[k];
+    woff[k] = (int64_t)wv.size();
     if (r.kind == 0) {
-      waits[k] = {{EXT + r.s, e_ext[r.s]}};
+      wv.push_back({EXT + r.s, e_ext[r.s]});
     } else if (r.kind == 1 || r.kind == 2) {
       const PanelItem& it = P.panel_items[r.item];
       const int b = P.meta[it.s].boff + it.c0 / 64;
-      if (r.kind == 1) waits[k] = {{EXT + r.s, e_ext[r.s]}, {COL + b, e_col[b]}};
-      else waits[k] = {{BLK + b, 1}};
+      if (r.kind == 1) {
+        wv.push_back({EXT + r.s, e_ext[r.s]});
+        wv.push_back({COL + b, e_col[b]});
+      } else {
+        wv.push_back({BLK + b, 1});
+      }
     } else {
       const TileItem& t = P.tile_items[r.item];
       const SnMeta& m = P.meta[t.s];
       if (t.mode == 0) {
-        for (int c = t.k0 / 64; c <= (t.k0 + t.kn - 1) / 64; ++c) waits[k].push_back({BLK + m.boff + c, e_blk[m.boff + c]});
+        for (int c = t.k0 / 64; c <= (t.k0 + t.kn - 1) / 64; ++c) wv.push_back({BLK + m.boff + c, e_blk[m.boff + c]});
       } else {
-        waits[k] = {{SDONE + t.s, e_sdone[t.s]}};
+        wv.push_back({SDONE + t.s, e_sdone[t.s]});
       }
     }
   }
+  woff[raw.size()] = (int64_t)wv.size();
   // dependency graph for the simulation: every counter is a zero-time join node whose
   // predecessors are its signalling tasks; a task depends on the joins it waits for
   // (a TRSM tile waits for its block's POTRF only).  Successor lists in CSR form.
@@ -546,8 +600,9 @@ static void build_factor_dag(Plan& P, const PlanParams& prm, const std::vector<d
   std::vector<int32_t> npred(nn, 0);
   auto for_edges = [&](auto&& edge) {
     for (int k = 0; k < nt; ++k) {
-      for (int32_t c : raw[k].sig) edge(k, nt + c);
-      for (const FWait& w : waits[k]) {
+      for (int64_t q = raw[k].sig0; q < raw[k].sig0 + raw[k].nsig; ++q) edge(k, nt + sigv[q]);
+      for (int64_t q = woff[k]; q < woff[k + 1]; ++q) {
+        const FWait& w = wv[q];
         if (w.target <= 0) continue;
         edge(raw[k].kind == 2 ? potrf_of[w.ctr - BLK] : nt + w.ctr, k);
       }
@@ -594,8 +649,10 @@ static void build_factor_dag(Plan& P, const PlanParams& prm, const std::vector<d
   // list scheduling on the SMs' CTA slots (two per SM for FP64, one for FP32)
   const int workers = std::max(1, prm.sms) * (prm.fp32 ? 1 : 2);
   std::vector<int32_t> pend = npred;
-  auto cmp = [&](int32_t x, int32_t y) { return blev[x] < blev[y] || (blev[x] == blev[y] && x > y); };
-  std::priority_queue<int32_t, std::vector<int32_t>, decltype(cmp)> ready(cmp);
+  // ready tasks by bottom level, ties to the lower index; the key travels with the task
+  using Key = std::pair<double, int32_t>;
+  auto cmp = [](const Key& x, const Key& y) { return x.first < y.first || (x.first == y.first && x.second > y.second); };
+  std::priority_queue<Key, std::vector<Key>, decltype(cmp)> ready(cmp);
   using Ev = std::pair<double, int32_t>;
   std::priority_queue<Ev, std::vector<Ev>, std::greater<Ev>> running;
   std::vector<int32_t> dispatch;
@@ -609,19 +666,19 @@ static void build_factor_dag(Plan& P, const PlanParams& prm, const std::vector<d
       for (int32_t u : succ_of(x))
         if (--pend[u] == 0) {
           if (u >= nt) stack.push_back(u);
-          else ready.push(u);
+          else ready.push({blev[u], u});
         }
     }
   };
   for (int v = nt; v < nn; ++v)
     if (!pend[v]) complete(v);
   for (int v = 0; v < nt; ++v)
-    if (!pend[v]) ready.push(v);
+    if (!pend[v]) ready.push({blev[v], v});
   double now = 0.0;
   int busy = 0;
   while ((int)dispatch.size() < nt) {
     while (busy < workers && !ready.empty()) {
-      const int32_t v = ready.top();
+      const int32_t v = ready.top().second;
       ready.pop();
       dispatch.push_back(v);
       running.push({now + dur[v], v});
@@ -642,19 +699,22 @@ static void build_factor_dag(Plan& P, const PlanParams& prm, const std::vector<d
   P.ftasks.clear();
   P.fwaits.clear();
   P.fsigs.clear();
+  P.ftasks.reserve(dispatch.size());
+  P.fwaits.reserve(wv.size());
+  P.fsigs.reserve(sigv.size());
   for (int32_t k : dispatch) {
     FTask t;
     t.kind = raw[k].kind;
     t.item = raw[k].item;
     t.wait0 = (int32_t)P.fwaits.size();
-    for (const FWait& w : waits[k])
-      if (w.target > 0) P.fwaits.push_back(w);
+    for (int64_t q = woff[k]; q < woff[k + 1]; ++q)
+      if (wv[q].target > 0) P.fwaits.push_back(wv[q]);
     t.nwait = (int32_t)P.fwaits.size() - t.wait0;
     t.w0_ctr = t.nwait > 0 ? P.fwaits[t.wait0].ctr : 0;
     t.w0_target = t.nwait > 0 ? P.fwaits[t.wait0].target : 0;
     t.sig0 = (int32_t)P.fsigs.size();
-    P.fsigs.insert(P.fsigs.end(), raw[k].sig.begin(), raw[k].sig.end());
-    t.nsig = (int32_t)raw[k].sig.size();
+    P.fsigs.insert(P.fsigs.end(), sigv.begin() + raw[k].sig0, sigv.begin() + raw[k].sig0 + raw[k].nsig);
+    t.nsig = raw[k].nsig;
     P.ftasks.push_back(t);
   }
 }

@@ -72,8 +72,39 @@ static void path_matrix(int n, std::vector<int64_t>& cp, std::vector<int32_t>& r
   }
 }
 
+static long long n_rel = 0;
+
 static void check_plan(const Symbolic& sym, const PlanParams& prm, const char* what) {
   const Plan P = build_plan(sym, prm);
+  // relative indices (filled by host threads on large plans): every group's positions
+  // equal a merge of its rows with its target's from the start
+  n_rel += (long long)P.rel.size();
+  {
+    std::vector<int32_t> src(P.groups.size(), -1);
+    for (int s = 0; s < P.nsuper; ++s) {
+      const SnMeta& m = P.meta[s];
+      for (int r = m.w; r < m.h; ++r) {
+        const int g = P.row_group[m.lidx + r];
+        CHECK(g >= 0 && g < (int)P.groups.size(), "%s: off-diagonal row without a group", what);
+        if (g >= 0 && g < (int)P.groups.size() && src[g] < 0) src[g] = s;
+      }
+    }
+    bool bad = false;
+    for (size_t g = 0; g < P.groups.size() && !bad; ++g) {
+      const RelGroup& gr = P.groups[g];
+      if (src[g] < 0) { bad = true; break; }
+      const SnMeta& m = P.meta[src[g]];
+      const SnMeta& mt = P.meta[gr.t];
+      const int32_t* rl = P.rows.data() + m.lidx;
+      const int32_t* tl = P.rows.data() + mt.lidx;
+      int q = 0;
+      for (int i = gr.j0; i < m.h && !bad; ++i) {
+        while (q < mt.h && tl[q] < rl[i]) ++q;
+        bad = q == mt.h || tl[q] != rl[i] || P.rel[gr.rel_off + (i - gr.j0)] != q;
+      }
+    }
+    CHECK(!bad, "%s: relative indices differ from a merge of the row lists", what);
+  }
   // tiles
   for (const Step& st : P.steps) {
     if (st.kind != StepKind::Gemm) continue;
@@ -363,6 +394,17 @@ int main() {
       std::snprintf(what, sizeof what, "%s %d^3 FP64 small blocks", full ? "27-point" : "7-point", k);
       check_plan(sym, small, what);
     }
+  // a plan large enough (over 2^20 relative indices) for its relative indices to be
+  // filled by several host threads
+  {
+    std::vector<int64_t> cp;
+    std::vector<int32_t> ri;
+    grid_matrix(44, true, cp, ri);
+    const Symbolic sym = symbolic_factorization(44 * 44 * 44, cp.data(), ri.data(), OrderingKind::MMD, RelaxParams());
+    const long long before = n_rel;
+    check_plan(sym, PlanParams(), "27-point 44^3 FP64");
+    CHECK(n_rel - before > (1 << 20), "27-point 44^3: only %lld relative indices", n_rel - before);
+  }
   // a block-diagonal batch (a forest of elimination trees, merged as the batch analysis
   // merges its systems): grids, a dense block wider than one outer block, a path, and
   // many one-column systems
@@ -408,7 +450,7 @@ int main() {
     std::fprintf(stderr, "%d violations\n", fails);
     return 1;
   }
-  std::printf("ok: %lld tiles (%lld tensor-core), %lld factor tasks, %lld tiny leaves\n", n_tiles, n_big_tiles,
-              n_ftasks, n_tiny);
+  std::printf("ok: %lld tiles (%lld tensor-core), %lld factor tasks, %lld tiny leaves, %lld relative indices\n",
+              n_tiles, n_big_tiles, n_ftasks, n_tiny, n_rel);
   return 0;
 }

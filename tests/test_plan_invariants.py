@@ -6,7 +6,10 @@ order, no task ever waits), the tiny-leaf solve batches (first forward, last bac
 every tiny leaf in exactly one), the forward solve's arrival counts (what the tasks
 signal equals what each supernode waits for), and both solve sweeps run one task at a time
 in dispatch order with the kernels' wait targets and signals (no task waits for one handed
-out after it, and every supernode ends done).  The matrices: 7- and 27-point grids, and a
+out after it, and every supernode ends done), the relative indices of the external updates
+(filled by host threads on large plans) against a merge of the row lists, and the task
+order re-built from measured durations (same tasks, waits and signals; still never
+waiting for a later task).  The matrices: 7- and 27-point grids, and a
 block-diagonal batch merged as the batch analysis merges its systems (grids, a dense block,
 a path, one-column systems), each planned in FP64, FP32 and with small blocks."""
 import os
