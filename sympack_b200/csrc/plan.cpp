@@ -436,18 +436,37 @@ std::vector<int64_t> build_assembly_map(const Symbolic& sym, const Plan& P, cons
   const int n = sym.n;
   const int64_t nnz = colptr[n] - 1;
   std::vector<int64_t> dst(nnz);
-  for (int c = 1; c <= n; ++c)
-    for (int64_t p = colptr[c - 1]; p < colptr[c]; ++p) {
-      int r = rowind[p - 1];
-      int pr = sym.invp[r - 1] - 1, pc = sym.invp[c - 1] - 1;
-      if (pr < pc) std::swap(pr, pc);
-      int s = P.supmember0[pc];
-      const SnMeta& m = P.meta[s];
-      const int32_t* rl = P.rows.data() + m.lidx;
-      const int32_t* it = std::lower_bound(rl, rl + m.h, pr);
-      if (it == rl + m.h || *it != pr) throw std::runtime_error("assembly: entry outside the symbolic structure");
-      dst[p - 1] = m.off + (int64_t)(pc - m.fc) * m.ld + (it - rl);
+  std::atomic<int> next{1};
+  std::atomic<bool> outside{false};
+  const int chunk = 4096;
+  auto fill = [&]() {  // columns in chunks; every entry's place is independent of the others
+    for (int c0 = next.fetch_add(chunk); c0 <= n; c0 = next.fetch_add(chunk)) {
+      for (int c = c0; c < std::min(n + 1, c0 + chunk); ++c)
+        for (int64_t p = colptr[c - 1]; p < colptr[c]; ++p) {
+          int r = rowind[p - 1];
+          int pr = sym.invp[r - 1] - 1, pc = sym.invp[c - 1] - 1;
+          if (pr < pc) std::swap(pr, pc);
+          int s = P.supmember0[pc];
+          const SnMeta& m = P.meta[s];
+          const int32_t* rl = P.rows.data() + m.lidx;
+          const int32_t* it = std::lower_bound(rl, rl + m.h, pr);
+          if (it == rl + m.h || *it != pr) {
+            outside = true;
+            return;
+          }
+          dst[p - 1] = m.off + (int64_t)(pc - m.fc) * m.ld + (it - rl);
+        }
     }
+  };
+  const unsigned nth = nnz < (1 << 20) ? 1u : std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+  std::vector<std::thread> pool;
+  try {
+    for (unsigned k = 1; k < nth; ++k) pool.emplace_back(fill);
+  } catch (const std::system_error&) {  // fewer threads: the ones started and this one share the columns
+  }
+  fill();
+  for (std::thread& th : pool) th.join();
+  if (outside) throw std::runtime_error("assembly: entry outside the symbolic structure");
   return dst;
 }
 

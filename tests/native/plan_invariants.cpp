@@ -404,6 +404,23 @@ int main() {
     const long long before = n_rel;
     check_plan(sym, PlanParams(), "27-point 44^3 FP64");
     CHECK(n_rel - before > (1 << 20), "27-point 44^3: only %lld relative indices", n_rel - before);
+    // the assembly map (filled by host threads above 2^20 entries): every entry of A lands
+    // on its (row, column) of the permuted factor inside its supernode's panel
+    PlanParams np;
+    np.factor_dag = false;
+    const Plan P = build_plan(sym, np);
+    const std::vector<int64_t> amap = build_assembly_map(sym, P, cp.data(), ri.data());
+    CHECK((int64_t)amap.size() == cp.back() - 1 && amap.size() > (1u << 20), "assembly map size %zu", amap.size());
+    bool bad = false;
+    for (int c = 1; c <= sym.n && !bad; ++c)
+      for (int64_t p = cp[c - 1]; p < cp[c] && !bad; ++p) {
+        int pr = sym.invp[ri[p - 1] - 1] - 1, pc = sym.invp[c - 1] - 1;
+        if (pr < pc) std::swap(pr, pc);
+        const SnMeta& m = P.meta[P.supmember0[pc]];
+        const int64_t d = amap[p - 1] - m.off, col = d / m.ld, pos = d % m.ld;
+        bad = d < 0 || col != pc - m.fc || pos >= m.h || P.rows[m.lidx + pos] != pr;
+      }
+    CHECK(!bad, "27-point 44^3: an assembly map entry is not its (row, column) in the panel");
   }
   // a block-diagonal batch (a forest of elimination trees, merged as the batch analysis
   // merges its systems): grids, a dense block wider than one outer block, a path, and
